@@ -1,0 +1,278 @@
+"""Benchmark of the matrix-free octree FEM hot path on B200.
+
+Workload (one GPU): 1,048,576 log-normal points (seed 2, maxDepth 14),
+points2Octree + 2:1 balance on the GPU, the mesh, and the FP64
+variable-coefficient operator -div(a grad u) + u with a = 1e4 inside the
+sphere of radius 0.25 about the centre and 1 outside.  A step is one
+operator application (y = A x) over the whole mesh.  The solve leg reports
+the FP64 V(2,2)-preconditioned CG time to ||b - A x|| <= 1e-8 ||b||.
+
+    python bench.py --gpus N --steps K --warmup W [--impl reference]
+
+N > 1 runs under torchrun, one rank per GPU; each rank processes its own
+mesh (independent work, no data-path collective: weak scaling) and rank 0
+prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time to FP64 rel. residual 1e-8 & matvec GDoF/s: chosen vs plain FP64, 1 B200"
+WORKLOAD = "lognormal1m_d14"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="dendro_b200", choices=["dendro_b200", "reference"])
+    p.add_argument("--workload", default=WORKLOAD)
+    p.add_argument("--scale", type=float, default=1.0, help="fraction of the workload's points (testing)")
+    p.add_argument("--no-solve", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=10.0)
+    return p.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(gpu_index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        med = float(np.median(sm)) if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload(name, scale):
+    from dendro_b200 import inputs as I
+    pts, depth = I.workload_points(name, scale)
+    return pts, depth
+
+
+def run_dendro(args, rank, world):
+    import torch
+
+    import dendro_b200 as dg
+    from dendro_b200 import inputs as I
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    pts, depth = build_workload(args.workload, args.scale)
+    t0 = time.time()
+    bal = dg.balanceOctree(dg.points2Octree(pts, depth, 1))
+    da = dg.DA(bal)
+    torch.cuda.synchronize()
+    setup_s = time.time() - t0
+    coef = I.sphere_coefficients(da.elementCenters())
+    A = dg.Jacobian2(da, coef)
+    E, N = da.E, da.N
+    x = torch.tensor(I.uniform_rhs(N, 3), device=dev)
+    y = torch.empty_like(x)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+    stream = torch.cuda.current_stream(dev)
+
+    for _ in range(args.warmup):
+        A.mult(x, y, stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(dev.index)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        flush.fill_(float(i))  # evict the mesh and vectors from L2 between steps
+        ev[i][0].record(stream)
+        A.mult(x, y, stream)
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+        torch.distributed.barrier()
+    ms_per_step = total_ms / args.steps
+    gdofs = world * N * args.steps / (total_ms * 1e-3) / 1e9
+
+    # roofline of the operator kernel: algorithmic bytes per launch
+    alg_bytes = 36 * E + 16 * E + 16 * N  # element record + (a, b) FP64 + x read + y written
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ms_per_step * 1e-3) / 1e9
+
+    # end to end through the host entry point (pinned host x, y)
+    xh = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    xh.copy_(x.cpu())
+    yh = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    A.mult(xh.numpy(), yh.numpy())
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(args.steps):
+        A.mult(xh.numpy(), yh.numpy())
+    e2e_s = time.perf_counter() - t1
+    e2e = {"value": world * N * args.steps / e2e_s / 1e9, "unit": "GDoF/s", "h2d_bytes_per_step": 8 * N,
+           "d2h_bytes_per_step": 8 * N}
+
+    solve = None
+    if not args.no_solve:
+        m = dg.DAMG(bal)
+        m.setKSP(coef)
+        b = torch.tensor(I.uniform_rhs(N, 3), device=dev)
+        m.solve(b, allow_unconverged=True)
+        xs, rep = m.solve(b, allow_unconverged=True)
+        solve = {"ms_to_1e-8": rep["solve_ms"], "iterations": rep["iterations"],
+                 "rel_residual": rep["rel_residual"], "converged": rep["converged"], "levels": int(m.nlevels),
+                 "precision": "fp64 V(2,2) + fp64 CG"}
+    return dict(E=E, N=N, setup_s=setup_s, ms_per_step=ms_per_step, gdofs=gdofs, achieved=achieved, peak=peak,
+                peak_kind=peak_kind, alg_bytes=alg_bytes, clocks=clk, e2e=e2e, solve=solve, bal=bal, depth=depth,
+                coef=coef, x=x.cpu().numpy(), y=y.cpu().numpy())
+
+
+def cpu_baseline(octs, depth, coef, x, seconds):
+    """Reference CPU matvec on the same mesh, timed on this host."""
+    from oracle import oracle as O
+    kind = "port"
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "dendro_ref_matvec")
+    mesh = O.Mesh(octs, depth)
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        mesh.matvec(x, coef)
+        n += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    del ref_bin
+    return {"value": mesh.N * n / dt / 1e9, "unit": "GDoF/s", "cores": 1, "kind": kind,
+            "sample": f"{n} full matvecs of the same mesh (E={mesh.E}, N={mesh.N}) in {dt:.1f} s, 1 thread"}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        return main_reference(args, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    r = run_dendro(args, rank, world)
+    line = {
+        "metric": METRIC, "value": round(r["gdofs"], 4), "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(r["ms_per_step"], 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded point cloud)",
+        "config": {"workload": args.workload, "points": int(1048576 * args.scale), "maxDepth": r["depth"],
+                   "elements": r["E"], "nodes": r["N"], "operator": "FP64 -div(a grad u)+u, a=1e4 in r<0.25",
+                   "l2": "flushed between steps (256 MB write)", "parallelism": f"independent mesh per GPU x{world}"},
+        "roofline": {"bound": "hbm", "achieved": round(r["achieved"], 1), "peak": r["peak"], "unit": "GB/s",
+                     "frac": round(r["achieved"] / r["peak"], 4), "traffic": None,
+                     "peak_source": r["peak_kind"], "algorithmic_bytes": int(r["alg_bytes"])},
+        "e2e": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r["e2e"].items()},
+        "gpu_launches": args.steps,
+        "clocks": r["clocks"],
+        "solve": r["solve"],
+        "setup_s": round(r["setup_s"], 3),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        octs = r["bal"].to_numpy()
+        line["cpu_baseline"] = cpu_baseline(octs, r["depth"], r["coef"], r["x"], args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+def main_reference(args, rank, world):
+    """Reference arm: the reference algorithm's CPU matvec on this host."""
+    if rank != 0:
+        return
+    from dendro_b200 import inputs as I
+    from oracle import oracle as O
+    pts, depth = build_workload(args.workload, args.scale)
+    octs = O.balance(O.points2octree(pts, depth, 1), depth)
+    mesh = O.Mesh(octs, depth)
+    cen = np.empty((mesh.E, 3))
+    s = 2.0 ** -(mesh.elev.astype(np.float64) - 1)
+    xyz = np.stack([mesh.octs["x"][:mesh.E], mesh.octs["y"][:mesh.E], mesh.octs["z"][:mesh.E]], 1).astype(float)
+    cen[:] = xyz / 2.0 ** depth + 0.5 * s[:, None]
+    coef = I.sphere_coefficients(cen)
+    x = I.uniform_rhs(mesh.N, 3)
+    for _ in range(max(0, min(args.warmup, 3))):
+        mesh.matvec(x, coef)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        mesh.matvec(x, coef)
+    dt = time.perf_counter() - t0
+    v = mesh.N * args.steps / dt / 1e9
+    line = {"metric": METRIC, "value": round(v, 5), "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * dt / args.steps, 3), "higher_is_better": True,
+            "impl": "reference", "dtype": "f64", "data": "synthetic (seeded point cloud)",
+            "config": {"workload": args.workload, "elements": mesh.E, "nodes": mesh.N},
+            "cpu_baseline": {"value": round(v, 5), "unit": "GDoF/s", "cores": 1, "kind": "port",
+                             "sample": f"{args.steps} full matvecs, 1 thread"},
+            "e2e": {"value": round(v, 5), "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,257 @@
+"""Python classes over the C ABI, named after the reference's interfaces.
+
+Arrays may be numpy (host) or torch CUDA tensors (device); the operators take
+device tensors for the resident path and host arrays for the end-to-end path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import OCT_DTYPE, DamgConfig, SolveReport, check, lib, ptr
+
+
+def _is_device(a) -> bool:
+    return not isinstance(a, np.ndarray) and getattr(a, "is_cuda", False)
+
+
+class Octree:
+    """Device-resident sorted linear octree (a vector<ot::TreeNode>)."""
+
+    def __init__(self, handle):
+        self.h = C.c_void_p(handle) if not isinstance(handle, C.c_void_p) else handle
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().dg_octree_destroy(self.h)
+            self.h = None
+
+    def __len__(self):
+        return int(lib().dg_octree_size(self.h))
+
+    @property
+    def maxDepth(self) -> int:
+        return int(lib().dg_octree_max_depth(self.h))
+
+    def to_numpy(self) -> np.ndarray:
+        out = np.empty(len(self), OCT_DTYPE)
+        check(lib().dg_octree_export(self.h, ptr(out)), "octree_export")
+        return out
+
+    @classmethod
+    def from_octants(cls, octs, maxDepth: int) -> "Octree":
+        h = C.c_void_p()
+        if _is_device(octs):
+            check(lib().dg_octree_from_octants(ptr(octs), octs.numel() // 4, 1, maxDepth, C.byref(h)),
+                  "octree_from_octants")
+        else:
+            a = np.ascontiguousarray(octs, OCT_DTYPE)
+            check(lib().dg_octree_from_octants(ptr(a), len(a), 0, maxDepth, C.byref(h)), "octree_from_octants")
+        return cls(h)
+
+
+def points2Octree(pts, maxDepth: int, maxNumPts: int = 1) -> Octree:
+    """ot::points2Octree (src/oct/Construct.C:727): points in [0,1)^3 -> octree."""
+    h = C.c_void_p()
+    if _is_device(pts):
+        n = pts.numel() // 3
+        check(lib().dg_points2octree(ptr(pts), n, 1, maxDepth, maxNumPts, C.byref(h)), "points2octree")
+    else:
+        a = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+        check(lib().dg_points2octree(ptr(a), len(a), 0, maxDepth, maxNumPts, C.byref(h)), "points2octree")
+    return Octree(h)
+
+
+def balanceOctree(octree: Octree) -> Octree:
+    """ot::balanceOctree with incCorner = true (src/oct/Balance.C:31)."""
+    h = C.c_void_p()
+    check(lib().dg_balance_octree(octree.h, C.byref(h)), "balance_octree")
+    return Octree(h)
+
+
+def coarsenOctree(octree: Octree) -> Octree:
+    """ot::coarsenOctree (src/oct/Coarsen.C:53-104)."""
+    h = C.c_void_p()
+    check(lib().dg_coarsen_octree(octree.h, C.byref(h)), "coarsen_octree")
+    return Octree(h)
+
+
+class DA:
+    """ot::DA: the mesh of a balanced octree, resident on the GPU."""
+
+    def __init__(self, octree: Octree = None, handle=None, owner=None):
+        self._owner = owner
+        if handle is None:
+            h = C.c_void_p()
+            check(lib().dg_da_create(octree.h, C.byref(h)), "da_create")
+            handle = h
+        self.h = handle if isinstance(handle, C.c_void_p) else C.c_void_p(handle)
+        E, N, P = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().dg_da_sizes(self.h, C.byref(E), C.byref(N), C.byref(P)), "da_sizes")
+        self.E, self.N, self.P = E.value, N.value, P.value
+        self.maxDepth = int(lib().dg_da_max_depth(self.h))  # embedded depth
+
+    @classmethod
+    def from_maps(cls, max_depth, nlist, level, cnum, hmask, node_xyz, elem_xyz) -> "DA":
+        arrs = [np.ascontiguousarray(a, dt) for a, dt in
+                ((nlist, np.uint32), (level, np.uint8), (cnum, np.uint8), (hmask, np.uint8),
+                 (node_xyz, np.uint32), (elem_xyz, np.uint32))]
+        h = C.c_void_p()
+        check(lib().dg_da_create_from_maps(len(arrs[1]), len(arrs[4]), max_depth, *[ptr(a) for a in arrs],
+                                           C.byref(h)), "da_create_from_maps")
+        return cls(handle=h)
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and self._owner is None and self.h.value:
+            lib().dg_da_destroy(self.h)
+            self.h = None
+
+    def getElementSize(self) -> int:
+        return self.E
+
+    def getNodeSize(self) -> int:
+        """Nodes including the positive-boundary nodes (getNodeSize + getBoundaryNodeSize)."""
+        return self.N
+
+    def export(self) -> dict:
+        E, N = self.E, self.N
+        out = dict(nlist=np.empty((E, 8), np.uint32), hmask=np.empty(E, np.uint8), cnum=np.empty(E, np.uint8),
+                   etype=np.empty(E, np.uint8), level=np.empty(E, np.uint8),
+                   node_xyz=np.empty((N, 3), np.uint32), elem_xyz=np.empty((E, 3), np.uint32),
+                   node_bdy=np.empty(N, np.uint8))
+        check(lib().dg_da_export(self.h, *[ptr(out[k]) for k in ("nlist", "hmask", "cnum", "etype", "level",
+                                                                  "node_xyz", "elem_xyz", "node_bdy")]),
+              "da_export")
+        return out
+
+    def elementCenters(self) -> np.ndarray:
+        """CalculateCenters (examples/src/backend/omgNeumann.C:788-820), [E, 3] in [0,1]."""
+        c = np.empty((self.E, 3))
+        check(lib().dg_da_element_centers(self.h, ptr(c)), "element_centers")
+        return c
+
+
+class _Mat:
+    def __init__(self, da: DA, h):
+        self.da = da
+        self.h = h
+        self.n = int(lib().dg_mat_size(self.h))
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().dg_mat_destroy(self.h)
+            self.h = None
+
+    def mult(self, x, y=None, stream=None):
+        """y = A x.  Device tensors run on `stream` (a torch stream or None);
+        host numpy arrays go through the copy-in / copy-out entry point."""
+        if _is_device(x):
+            import torch
+            if y is None:
+                y = torch.empty_like(x)
+            s = None if stream is None else C.c_void_p(stream.cuda_stream)
+            if x.dtype == torch.float64:
+                check(lib().dg_mat_mult(self.h, ptr(x), ptr(y), s), "mat_mult")
+            elif x.dtype == torch.float32:
+                check(lib().dg_mat_mult_f32(self.h, ptr(x), ptr(y), s), "mat_mult_f32")
+            else:
+                raise TypeError("x must be float64 or float32")
+            return y
+        xa = np.ascontiguousarray(x, np.float64)
+        ya = np.empty(self.n) if y is None else y
+        check(lib().dg_mat_mult_host(self.h, ptr(xa), ptr(ya)), "mat_mult_host")
+        return ya
+
+    def getDiagonal(self, d=None, stream=None):
+        import torch
+        if d is None:
+            d = torch.empty(self.n, dtype=torch.float64, device="cuda")
+        s = None if stream is None else C.c_void_p(stream.cuda_stream)
+        check(lib().dg_mat_get_diagonal(self.h, ptr(d), s), "mat_get_diagonal")
+        return d
+
+
+class Jacobian2(_Mat):
+    """-div(a grad u) + b u (CreateJacobian2 / Jacobian2MatMult,
+    examples/src/backend/omgNeumann.C:533,643); coef = [a0, b0, a1, b1, ...]
+    per element, or None for a = b = 1."""
+
+    def __init__(self, da: DA, coef=None):
+        h = C.c_void_p()
+        c = None if coef is None else np.ascontiguousarray(coef, np.float64).reshape(-1)
+        if c is not None and len(c) != 2 * da.E:
+            raise ValueError("coef must hold 2 values per element")
+        check(lib().dg_mat_create_lapmass(da.h, ptr(c), C.byref(h)), "mat_create_lapmass")
+        super().__init__(da, h)
+
+
+class Elasticity(_Mat):
+    """3-dof linear elasticity (ElasticityMatMult, examples/src/backend/elasticityJac.C:212)."""
+
+    def __init__(self, da: DA, mu: float, lam: float, dirichlet=None):
+        h = C.c_void_p()
+        d = None if dirichlet is None else np.ascontiguousarray(dirichlet, np.uint8)
+        check(lib().dg_mat_create_elasticity(da.h, mu, lam, ptr(d), C.byref(h)), "mat_create_elasticity")
+        super().__init__(da, h)
+
+
+class DAMG:
+    """ot::DAMG: level hierarchy + V-cycle preconditioned CG on the GPU."""
+
+    def __init__(self, finest: Octree, nlevels: int = 30, nu_pre: int = 2, nu_post: int = 2,
+                 omega: float = 2.0 / 3.0, rtol: float = 1e-8, maxit: int = 200, inner_prec: int = 0,
+                 use_graph: bool = False):
+        cfg = DamgConfig()
+        lib().dg_damg_default_config(C.byref(cfg))
+        cfg.nlevels, cfg.nu_pre, cfg.nu_post, cfg.omega = nlevels, nu_pre, nu_post, omega
+        cfg.rtol, cfg.maxit, cfg.inner_prec, cfg.use_graph = rtol, maxit, inner_prec, int(use_graph)
+        h = C.c_void_p()
+        check(lib().dg_damg_create(finest.h, C.byref(cfg), C.byref(h)), "damg_create")
+        self.h = h
+        self.nlevels = int(lib().dg_damg_levels(self.h))
+        E = np.empty(self.nlevels, np.int64)
+        N = np.empty(self.nlevels, np.int64)
+        check(lib().dg_damg_level_sizes(self.h, ptr(E), ptr(N)), "damg_level_sizes")
+        self.E, self.N = E, N
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().dg_damg_destroy(self.h)
+            self.h = None
+
+    def level_da(self, l: int) -> DA:
+        return DA(handle=lib().dg_damg_level_da(self.h, l), owner=self)
+
+    def setKSP(self, coef=None):
+        """DAMGSetKSP with the Jacobian2 operator (include/omg/omg.h:488)."""
+        c = None if coef is None else np.ascontiguousarray(coef, np.float64).reshape(-1)
+        check(lib().dg_damg_set_lapmass(self.h, ptr(c)), "damg_set_lapmass")
+
+    def solve(self, b, x=None, allow_unconverged: bool = False):
+        """DAMGSolve (include/omg/omg.h:492): returns (x, report dict)."""
+        rep = SolveReport()
+        if _is_device(b):
+            import torch
+            x = torch.empty_like(b) if x is None else x
+            st = lib().dg_damg_solve(self.h, ptr(b), ptr(x), 1, C.byref(rep))
+        else:
+            ba = np.ascontiguousarray(b, np.float64)
+            x = np.empty_like(ba) if x is None else x
+            st = lib().dg_damg_solve(self.h, ptr(ba), ptr(x), 0, C.byref(rep))
+        if not (allow_unconverged and st == 4):
+            check(st, "damg_solve")
+        return x, dict(iterations=rep.iterations, converged=bool(rep.converged), rel_residual=rep.rel_residual,
+                       solve_ms=rep.solve_ms)
+
+    def prolong(self, level: int, xc: np.ndarray, xf: np.ndarray) -> np.ndarray:
+        xc = np.ascontiguousarray(xc, np.float64)
+        xf = np.ascontiguousarray(xf, np.float64).copy()
+        check(lib().dg_damg_prolong(self.h, level, ptr(xc), ptr(xf), 0), "damg_prolong")
+        return xf
+
+    def restrict(self, level: int, rf: np.ndarray) -> np.ndarray:
+        rf = np.ascontiguousarray(rf, np.float64)
+        rc = np.empty(int(self.N[level + 1]))
+        check(lib().dg_damg_restrict(self.h, level, ptr(rf), ptr(rc), 0), "damg_restrict")
+        return rc

@@ -1,0 +1,74 @@
+// Internal device-side objects behind the opaque C-ABI handles.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "dg_common.cuh"
+
+struct dg_octree {
+  uint32_t max_depth = 0;
+  int64_t n = 0;
+  dg::DBuf<uint64_t> keys;  // octant keys (Morton anchor << 5 | level), sorted
+};
+
+struct dg_da {
+  uint32_t D = 0;        // embedded depth = maxDepth + 1
+  int64_t E = 0, N = 0, P = 0;
+  dg::DBuf<uint32_t> nl;     // [8][E] node ids, vertex-major
+  dg::DBuf<uint32_t> meta;   // [E] packed level / child number / hanging mask / type
+  dg::DBuf<uint64_t> ekey;   // [E] element octant keys (embedded space)
+  dg::DBuf<uint64_t> nkey;   // [N] node anchor Morton keys (embedded space), sorted
+  // Element tiles for the shared-memory matvec: per tile of kTile elements the
+  // smallest node id it touches and the window width actually needed.
+  dg::DBuf<uint32_t> tile_lo;
+  dg::DBuf<uint32_t> tile_span;
+  int64_t ntiles = 0;
+  uint32_t max_span = 0;
+};
+
+struct dg_mat {
+  dg_da* da = nullptr;
+  int kind = 0;  // 0 lap+mass, 1 elasticity
+  int dof = 1;
+  bool has_coef = false;
+  dg::DBuf<double> coef;       // [2][E] (a then b), FP64
+  dg::DBuf<float> coef32;      // [2][E] FP32 copy for the inner solver
+  double mu = 0, lam = 0;
+  dg::DBuf<uint8_t> dirichlet; // [N]
+  dg::DBuf<double> host_x, host_y;  // device staging of dg_mat_mult_host, kept between calls
+};
+
+namespace dg {
+
+// ---- primitives (prim.cu) ----
+// Device-wide exclusive scan of n uint32 values into out (out may alias in);
+// returns the total through *total (host) when not null.
+dg_status scan_u32(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, cudaStream_t s);
+// Keys-only stable LSD radix sort of n uint64 keys on bits
+// [start_bit, start_bit + bits).  Sorted keys end in `keys`; tmp holds n keys.
+dg_status radix_sort_u64(uint64_t* keys, uint64_t* tmp, int64_t n, int bits, cudaStream_t s,
+                         int start_bit = 0);
+// Remove adjacent duplicates in place; returns the new length.
+dg_status unique_u64(uint64_t* keys, int64_t n, int64_t* n_out, cudaStream_t s);
+
+// ---- octree (octree.cu) ----
+dg_status points_to_octree(const double* d_pts, int64_t n, uint32_t D, uint32_t m, dg_octree* out,
+                           cudaStream_t s);
+dg_status balance_octree(const dg_octree* in, dg_octree* out, cudaStream_t s);
+dg_status coarsen_octree(const dg_octree* in, dg_octree* out, cudaStream_t s);
+
+// ---- mesh (mesh.cu) ----
+dg_status build_mesh(const dg_octree* tree, dg_da* da, cudaStream_t s);
+dg_status build_tiles(dg_da* da, cudaStream_t s);
+
+// ---- operators (matvec.cu) ----
+dg_status lapmass_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
+dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStream_t s);
+dg_status lapmass_diag(const dg_mat* A, double* d, cudaStream_t s);
+dg_status elasticity_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
+dg_status elasticity_diag(const dg_mat* A, double* d, cudaStream_t s);
+// Dense assembled operator (row-major n x n) of a small level.
+dg_status lapmass_assemble_dense(const dg_mat* A, double* dense, cudaStream_t s);
+
+}  // namespace dg

@@ -1,0 +1,625 @@
+// Multigrid hierarchy and solver on the GPU (ot::DAMG):
+//  * levels by coarsenOctree + balanceOctree until the requested count or a
+//    level below 500 octants (DAMGCreateAndSetDA, src/omg/omg.C:1306-1420);
+//  * coarse coefficients copied or averaged from the 8 children
+//    (ASSIGN_MAT_PROP_FINE_TO_COARSE_ELEM_BLOCK, omgNeumann.C:73-113);
+//  * prolongation P = the coarse conforming FE function at the fine nodes,
+//    restriction R = P^T (prolongMatVecType1 / restrictMatVecType1,
+//    src/omg/ProlongMatVec.C:154-284, RestrictMatVec.C:486-619);
+//  * V(nu_pre, nu_post) cycle with Richardson(omega)+Jacobi smoothing and a
+//    dense FP64 direct coarse solve, inside CG (bin/options:50-53,182-207).
+#include <chrono>
+#include <cmath>
+#include <memory>
+#include <vector>
+
+#include "dg_internal.h"
+
+namespace dg {
+dg_status node_boundary_flags(const dg_da* da, uint8_t* d_out, cudaStream_t s);
+dg_status convert_f64_to_f32(const double* a, float* b, int64_t n, cudaStream_t s);
+}  // namespace dg
+
+using namespace dg;
+
+namespace {
+
+__device__ __forceinline__ int64_t gtid() { return blockIdx.x * int64_t(blockDim.x) + threadIdx.x; }
+__device__ __forceinline__ int64_t gstride() { return int64_t(gridDim.x) * blockDim.x; }
+
+__device__ __forceinline__ int64_t lower_bound(const uint64_t* __restrict__ a, int64_t n, uint64_t key) {
+  int64_t lo = 0, hi = n;  // first index with a[i] >= key
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    if (a[mid] < key) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int64_t max_lower_bound(const uint64_t* __restrict__ a, int64_t n, uint64_t key) {
+  int64_t lo = 0, hi = n;  // first index with a[i] > key
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    if (a[mid] <= key) lo = mid + 1; else hi = mid;
+  }
+  return lo - 1;
+}
+
+// ---------------------------------------------------------- coefficients --
+__global__ void coarse_coef_kernel(const uint64_t* __restrict__ fk, int64_t Ef, const double* __restrict__ fc,
+                                   const uint64_t* __restrict__ ck, int64_t Ec, double* __restrict__ cc,
+                                   uint32_t* __restrict__ err) {
+  for (int64_t e = gtid(); e < Ec; e += gstride()) {
+    uint64_t m = okey_m(ck[e]);
+    uint32_t l = okey_l(ck[e]);
+    int64_t f = lower_bound(fk, Ef, okey(m, 0));  // first fine element anchored at or after m
+    if (f >= Ef || okey_m(fk[f]) != m) {
+      atomicOr(err, 1u);
+      continue;
+    }
+    if (okey_l(fk[f]) == l) {
+      cc[e] = fc[f];
+      cc[Ec + e] = fc[Ef + f];
+    } else {
+      double a = 0, b = 0;
+      for (int k = 0; k < 8 && f + k < Ef; ++k) {
+        a += fc[f + k];
+        b += fc[Ef + f + k];
+      }
+      cc[e] = a / 8.0;
+      cc[Ec + e] = b / 8.0;
+    }
+  }
+}
+
+// ----------------------------------------------------------- prolongation --
+// Weights of the coarse element holding fine node f: the 8 trilinear values
+// at the node, mapped through T^T to the element's node slots.
+__device__ __forceinline__ bool prolong_row(const uint64_t* __restrict__ fnk, int64_t f, const uint64_t* __restrict__ cek,
+                                            int64_t Ec, const uint32_t* __restrict__ cmeta, uint32_t top, uint32_t Dp,
+                                            int64_t& e, double (&w)[8]) {
+  uint32_t px, py, pz;
+  demorton(fnk[f], px, py, pz);
+  uint32_t qx = px == top ? px - 1 : px, qy = py == top ? py - 1 : py, qz = pz == top ? pz - 1 : pz;
+  e = max_lower_bound(cek, Ec, okey(morton(qx, qy, qz), 31));
+  if (e < 0) return false;
+  uint32_t ox, oy, oz;
+  demorton(okey_m(cek[e]), ox, oy, oz);
+  uint32_t s = 1u << (Dp - okey_l(cek[e]));
+  if (qx < ox || qy < oy || qz < oz || qx >= ox + s || qy >= oy + s || qz >= oz + s) return false;
+  double inv = 1.0 / double(s);
+  double lx = double(px - ox) * inv, ly = double(py - oy) * inv, lz = double(pz - oz) * inv;
+  double phi[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v)
+    phi[v] = ((v & 1) ? lx : 1 - lx) * ((v & 2) ? ly : 1 - ly) * ((v & 4) ? lz : 1 - lz);
+  uint32_t m = cmeta[e], c = meta_cnum(m), mask = meta_mask(m);
+#pragma unroll
+  for (int v = 0; v < 8; ++v) w[v] = ((mask >> v) & 1u) ? 0.0 : phi[v];
+  for (int i = 0; i < 8; ++i) {
+    if (!((mask >> i) & 1u)) continue;
+    uint32_t mid = (uint32_t(i) ^ c) & 7u;
+    double wi = phi[i] * (__popc(mid) == 1 ? 0.5 : 0.25);
+    for (uint32_t sub = mid;; sub = (sub - 1) & mid) {
+      w[i ^ sub] += wi;
+      if (!sub) break;
+    }
+  }
+  return true;
+}
+
+__global__ void prolong_count(const uint64_t* __restrict__ fnk, int64_t Nf, const uint64_t* __restrict__ cek, int64_t Ec,
+                              const uint32_t* __restrict__ cmeta, uint32_t top, uint32_t Dp, uint32_t* __restrict__ cnt,
+                              uint32_t* __restrict__ err) {
+  for (int64_t f = gtid(); f < Nf; f += gstride()) {
+    int64_t e;
+    double w[8];
+    uint32_t c = 0;
+    if (!prolong_row(fnk, f, cek, Ec, cmeta, top, Dp, e, w)) {
+      atomicOr(err, 1u);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) c += w[j] != 0.0;
+    }
+    cnt[f] = c;
+  }
+}
+
+__global__ void prolong_fill(const uint64_t* __restrict__ fnk, int64_t Nf, const uint64_t* __restrict__ cek, int64_t Ec,
+                             const uint32_t* __restrict__ cmeta, const uint32_t* __restrict__ cnl, uint32_t top,
+                             uint32_t Dp, const uint32_t* __restrict__ ptr, uint32_t* __restrict__ col,
+                             double* __restrict__ val) {
+  for (int64_t f = gtid(); f < Nf; f += gstride()) {
+    int64_t e;
+    double w[8];
+    if (!prolong_row(fnk, f, cek, Ec, cmeta, top, Dp, e, w)) continue;
+    uint32_t p = ptr[f];
+    for (int j = 0; j < 8; ++j)
+      if (w[j] != 0.0) {
+        col[p] = cnl[int64_t(j) * Ec + e];
+        val[p] = w[j];
+        ++p;
+      }
+  }
+}
+
+// xf += P xc
+__global__ void prolong_add(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+                            const double* __restrict__ val, int64_t Nf, const double* __restrict__ xc,
+                            double* __restrict__ xf) {
+  for (int64_t f = gtid(); f < Nf; f += gstride()) {
+    double s = 0;
+    for (uint32_t k = ptr[f]; k < ptr[f + 1]; ++k) s += val[k] * xc[col[k]];
+    xf[f] += s;
+  }
+}
+
+// rc = P^T (b - t) (restriction of the residual, fused)
+__global__ void restrict_residual(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+                                  const double* __restrict__ val, int64_t Nf, const double* __restrict__ b,
+                                  const double* __restrict__ t, double* __restrict__ rc) {
+  for (int64_t f = gtid(); f < Nf; f += gstride()) {
+    double r = t ? b[f] - t[f] : b[f];
+    if (r == 0.0) continue;
+    for (uint32_t k = ptr[f]; k < ptr[f + 1]; ++k) atomicAdd(rc + col[k], val[k] * r);
+  }
+}
+
+// --------------------------------------------------------------- smoother --
+__global__ void jacobi_first(double* __restrict__ x, const double* __restrict__ b, const double* __restrict__ dinv,
+                             double omega, int64_t n) {
+  for (int64_t i = gtid(); i < n; i += gstride()) x[i] = omega * dinv[i] * b[i];
+}
+__global__ void jacobi_update(double* __restrict__ x, const double* __restrict__ b, const double* __restrict__ t,
+                              const double* __restrict__ dinv, double omega, int64_t n) {
+  for (int64_t i = gtid(); i < n; i += gstride()) x[i] += omega * dinv[i] * (b[i] - t[i]);
+}
+__global__ void invert(double* __restrict__ d, int64_t n) {
+  for (int64_t i = gtid(); i < n; i += gstride()) d[i] = 1.0 / d[i];
+}
+
+// ------------------------------------------------------------ coarse solve --
+__global__ void gj_col(const double* __restrict__ A, int64_t n, int64_t k, double* __restrict__ colk) {
+  for (int64_t i = gtid(); i < n; i += gstride()) colk[i] = A[i * n + k];
+}
+__global__ void gj_row(double* __restrict__ A, int64_t n, int64_t k, const double* __restrict__ colk) {
+  const double piv = colk[k];
+  for (int64_t j = gtid(); j < n; j += gstride()) A[k * n + j] = (j == k ? 1.0 : A[k * n + j]) / piv;
+}
+__global__ void gj_elim(double* __restrict__ A, int64_t n, int64_t k, const double* __restrict__ colk) {
+  for (int64_t t = gtid(); t < n * n; t += gstride()) {
+    int64_t i = t / n, j = t - i * n;
+    if (i == k) continue;
+    A[t] = (j == k ? 0.0 : A[t]) - colk[i] * A[k * n + j];
+  }
+}
+// x = Ainv b, one warp per row
+__global__ void dense_gemv(const double* __restrict__ A, int64_t n, const double* __restrict__ b, double* __restrict__ x) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t row = gtid() >> 5; row < n; row += gstride() >> 5) {
+    double s = 0;
+    for (int64_t j = lane; j < n; j += 32) s += A[row * n + j] * b[j];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (!lane) x[row] = s;
+  }
+}
+
+// -------------------------------------------------------------- reductions --
+constexpr int kRedBlocks = 296;  // 2 x 148 SMs
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double ws[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) ws[w] = v;
+  __syncthreads();
+  v = 0;
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  __syncthreads();
+  return v;
+}
+// deterministic second stage: one block sums the partials in a fixed order
+__global__ void finish_sum(const double* __restrict__ part, int np, double* __restrict__ out) {
+  double v = 0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) v += part[i];
+  v = block_sum(v);
+  if (threadIdx.x == 0) *out = v;
+}
+__global__ void dot_partial(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
+                            double* __restrict__ part) {
+  double v = 0;
+  for (int64_t i = gtid(); i < n; i += gstride()) v += a[i] * b[i];
+  v = block_sum(v);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+// x += alpha p; r -= alpha q; partial (r, r); alpha = num / den read on device
+__global__ void cg_update(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                          const double* __restrict__ q, int64_t n, const double* __restrict__ num,
+                          const double* __restrict__ den, double* __restrict__ part) {
+  const double alpha = *num / *den;
+  double v = 0;
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    x[i] += alpha * p[i];
+    double ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    v += ri * ri;
+  }
+  v = block_sum(v);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+// p = z + beta p with beta = num / den
+__global__ void cg_direction(double* __restrict__ p, const double* __restrict__ z, int64_t n,
+                             const double* __restrict__ num, const double* __restrict__ den) {
+  const double beta = *num / *den;
+  for (int64_t i = gtid(); i < n; i += gstride()) p[i] = z[i] + beta * p[i];
+}
+
+}  // namespace
+
+// --------------------------------------------------------------- hierarchy --
+struct Level {
+  std::unique_ptr<dg_octree> tree;
+  std::unique_ptr<dg_da> da;
+  std::unique_ptr<dg_mat> A;
+  DBuf<double> dinv, x, b, t;
+  // P to this level from level + 1 (CSR over this level's nodes)
+  DBuf<uint32_t> pptr, pcol;
+  DBuf<double> pval;
+};
+
+struct dg_damg {
+  dg_damg_config cfg;
+  std::vector<Level> lv;
+  DBuf<double> Ainv;  // dense inverse of the coarsest operator
+  int64_t nc = 0;
+  // PCG work vectors on the finest level and device scalars
+  DBuf<double> r, z, p, q, part, scal;
+  cudaStream_t s = nullptr;
+};
+
+namespace {
+
+dg_status build_prolongation(Level& F, Level& C, cudaStream_t s) {
+  const dg_da* fd = F.da.get();
+  const dg_da* cd = C.da.get();
+  DG_CHECK(fd->D == cd->D, DG_EINVAL, "levels with different depths");
+  const uint32_t top = 1u << (fd->D - 1);
+  DBuf<uint32_t> err;
+  DG_TRY(err.alloc(1));
+  DG_CUDA(cudaMemsetAsync(err.p, 0, 4, s));
+  DG_TRY(F.pptr.alloc(fd->N + 1));
+  prolong_count<<<grid_for(fd->N, 256), 256, 0, s>>>(fd->nkey.p, fd->N, cd->ekey.p, cd->E, cd->meta.p, top, fd->D,
+                                                      F.pptr.p, err.p);
+  DG_CUDA(cudaMemsetAsync(F.pptr.p + fd->N, 0, 4, s));
+  uint32_t nnz = 0;
+  DG_TRY(scan_u32(F.pptr.p, F.pptr.p, fd->N + 1, &nnz, s));
+  uint32_t herr = 0;
+  DG_CUDA(cudaMemcpyAsync(&herr, err.p, 4, cudaMemcpyDeviceToHost, s));
+  DG_CUDA(cudaStreamSynchronize(s));
+  DG_CHECK(!herr, DG_EUNBALANCED, "fine node outside every coarse element");
+  DG_TRY(F.pcol.alloc(nnz));
+  DG_TRY(F.pval.alloc(nnz));
+  prolong_fill<<<grid_for(fd->N, 256), 256, 0, s>>>(fd->nkey.p, fd->N, cd->ekey.p, cd->E, cd->meta.p, cd->nl.p, top,
+                                                     fd->D, F.pptr.p, F.pcol.p, F.pval.p);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status setup_level_vectors(Level& L, cudaStream_t s) {
+  const int64_t N = L.da->N;
+  DG_TRY(L.dinv.alloc(N));
+  DG_TRY(L.x.alloc(N));
+  DG_TRY(L.b.alloc(N));
+  DG_TRY(L.t.alloc(N));
+  DG_TRY(lapmass_diag(L.A.get(), L.dinv.p, s));
+  invert<<<grid_for(N, 256), 256, 0, s>>>(L.dinv.p, N);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status setup_coarse(dg_damg* m) {
+  Level& L = m->lv.back();
+  const int64_t n = L.da->N;
+  DG_CHECK(n <= 16384, DG_EINVAL, "coarsest level too large for the dense direct solve (> 16384 nodes)");
+  m->nc = n;
+  DG_TRY(m->Ainv.alloc(n * n));
+  DG_TRY(lapmass_assemble_dense(L.A.get(), m->Ainv.p, m->s));
+  DBuf<double> colk;
+  DG_TRY(colk.alloc(n));
+  const unsigned g1 = grid_for(n, 256), g2 = grid_for(n * n, 256);
+  for (int64_t k = 0; k < n; ++k) {
+    gj_col<<<g1, 256, 0, m->s>>>(m->Ainv.p, n, k, colk.p);
+    gj_row<<<g1, 256, 0, m->s>>>(m->Ainv.p, n, k, colk.p);
+    gj_elim<<<g2, 256, 0, m->s>>>(m->Ainv.p, n, k, colk.p);
+  }
+  DG_CUDA(cudaGetLastError());
+  DG_CUDA(cudaStreamSynchronize(m->s));
+  return DG_OK;
+}
+
+dg_status set_operators(dg_damg* m, const double* coef) {
+  cudaStream_t s = m->s;
+  for (size_t l = 0; l < m->lv.size(); ++l) {
+    Level& L = m->lv[l];
+    auto A = std::make_unique<dg_mat>();
+    A->da = L.da.get();
+    A->kind = 0;
+    A->dof = 1;
+    if (coef) {
+      A->has_coef = true;
+      DG_TRY(A->coef.alloc(2 * L.da->E));
+      if (l == 0) {
+        std::vector<double> soa(2 * L.da->E);
+        for (int64_t e = 0; e < L.da->E; ++e) {
+          soa[e] = coef[2 * e];
+          soa[L.da->E + e] = coef[2 * e + 1];
+        }
+        DG_CUDA(cudaMemcpyAsync(A->coef.p, soa.data(), 16 * L.da->E, cudaMemcpyHostToDevice, s));
+        DG_CUDA(cudaStreamSynchronize(s));
+      } else {
+        Level& F = m->lv[l - 1];
+        DBuf<uint32_t> err;
+        DG_TRY(err.alloc(1));
+        DG_CUDA(cudaMemsetAsync(err.p, 0, 4, s));
+        coarse_coef_kernel<<<grid_for(L.da->E, 256), 256, 0, s>>>(F.da->ekey.p, F.da->E, F.A->coef.p, L.da->ekey.p,
+                                                                   L.da->E, A->coef.p, err.p);
+        uint32_t herr = 0;
+        DG_CUDA(cudaMemcpyAsync(&herr, err.p, 4, cudaMemcpyDeviceToHost, s));
+        DG_CUDA(cudaStreamSynchronize(s));
+        DG_CHECK(!herr, DG_EINVAL, "coarse element without fine elements");
+      }
+      DG_TRY(A->coef32.alloc(2 * L.da->E));
+      DG_TRY(convert_f64_to_f32(A->coef.p, A->coef32.p, 2 * L.da->E, s));
+    }
+    L.A = std::move(A);
+    DG_TRY(setup_level_vectors(L, s));
+  }
+  return setup_coarse(m);
+}
+
+// z = V(b) on level l (x of level l holds the result)
+dg_status vcycle(dg_damg* m, size_t l, const double* b, double* x) {
+  cudaStream_t s = m->s;
+  Level& L = m->lv[l];
+  const int64_t n = L.da->N;
+  const unsigned g = grid_for(n, 256);
+  if (l + 1 == m->lv.size()) {
+    dense_gemv<<<grid_for(n * 32, 256), 256, 0, s>>>(m->Ainv.p, n, b, x);
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+  }
+  const double w = m->cfg.omega;
+  // pre-smoothing from a zero initial guess
+  if (m->cfg.nu_pre > 0) {
+    jacobi_first<<<g, 256, 0, s>>>(x, b, L.dinv.p, w, n);
+    for (int k = 1; k < m->cfg.nu_pre; ++k) {
+      DG_TRY(lapmass_apply_f64(L.A.get(), x, L.t.p, s));
+      jacobi_update<<<g, 256, 0, s>>>(x, b, L.t.p, L.dinv.p, w, n);
+    }
+    DG_TRY(lapmass_apply_f64(L.A.get(), x, L.t.p, s));
+  } else {
+    DG_CUDA(cudaMemsetAsync(x, 0, 8 * n, s));
+  }
+  Level& C = m->lv[l + 1];
+  DG_CUDA(cudaMemsetAsync(C.b.p, 0, 8 * C.da->N, s));
+  restrict_residual<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval.p, n, b, m->cfg.nu_pre > 0 ? L.t.p : nullptr, C.b.p);
+  DG_TRY(vcycle(m, l + 1, C.b.p, C.x.p));
+  prolong_add<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval.p, n, C.x.p, x);
+  for (int k = 0; k < m->cfg.nu_post; ++k) {
+    DG_TRY(lapmass_apply_f64(L.A.get(), x, L.t.p, s));
+    jacobi_update<<<g, 256, 0, s>>>(x, b, L.t.p, L.dinv.p, w, n);
+  }
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status dot(dg_damg* m, const double* a, const double* b, int64_t n, double* out) {
+  dot_partial<<<kRedBlocks, 256, 0, m->s>>>(a, b, n, m->part.p);
+  finish_sum<<<1, 256, 0, m->s>>>(m->part.p, kRedBlocks, out);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void dg_damg_default_config(dg_damg_config* c) {
+  c->nlevels = 30;
+  c->nu_pre = 2;
+  c->nu_post = 2;
+  c->omega = 2.0 / 3.0;
+  c->rtol = 1e-8;
+  c->maxit = 200;
+  c->inner_prec = DG_PREC_F64;
+  c->use_graph = 0;
+}
+
+dg_status dg_damg_create(const dg_octree* finest, const dg_damg_config* cfg, dg_damg** out) {
+  DG_CHECK(finest && out, DG_EINVAL, "damg_create: bad arguments");
+  auto m = std::make_unique<dg_damg>();
+  if (cfg) m->cfg = *cfg; else dg_damg_default_config(&m->cfg);
+  DG_CHECK(m->cfg.nlevels >= 1, DG_EINVAL, "damg_create: nlevels must be >= 1");
+  cudaStream_t s = nullptr;
+  m->s = s;
+  // level octrees: coarsen + balance (omg.C:1376-1420)
+  std::vector<std::unique_ptr<dg_octree>> trees;
+  auto t0 = std::make_unique<dg_octree>();
+  t0->max_depth = finest->max_depth;
+  t0->n = finest->n;
+  DG_TRY(t0->keys.alloc(finest->n));
+  DG_CUDA(cudaMemcpy(t0->keys.p, finest->keys.p, 8 * finest->n, cudaMemcpyDeviceToDevice));
+  trees.push_back(std::move(t0));
+  int idx = -1;
+  bool repeat = m->cfg.nlevels > 1;
+  while (idx < m->cfg.nlevels - 2 && repeat) {
+    dg_octree tmp;
+    DG_TRY(coarsen_octree(trees.back().get(), &tmp, s));
+    auto c = std::make_unique<dg_octree>();
+    DG_TRY(balance_octree(&tmp, c.get(), s));
+    ++idx;
+    if (c->n < 500) repeat = false;
+    trees.push_back(std::move(c));
+  }
+  m->lv.resize(trees.size());
+  for (size_t l = 0; l < trees.size(); ++l) {
+    m->lv[l].tree = std::move(trees[l]);
+    m->lv[l].da = std::make_unique<dg_da>();
+    DG_TRY(build_mesh(m->lv[l].tree.get(), m->lv[l].da.get(), s));
+  }
+  for (size_t l = 0; l + 1 < m->lv.size(); ++l) DG_TRY(build_prolongation(m->lv[l], m->lv[l + 1], s));
+  const int64_t N = m->lv[0].da->N;
+  DG_TRY(m->r.alloc(N));
+  DG_TRY(m->z.alloc(N));
+  DG_TRY(m->p.alloc(N));
+  DG_TRY(m->q.alloc(N));
+  DG_TRY(m->part.alloc(kRedBlocks));
+  DG_TRY(m->scal.alloc(8));
+  DG_TRY(set_operators(m.get(), nullptr));
+  *out = m.release();
+  return DG_OK;
+}
+
+dg_status dg_damg_set_lapmass(dg_damg* m, const double* coef) {
+  DG_CHECK(m, DG_EINVAL, "damg_set_lapmass: null handle");
+  return set_operators(m, coef);
+}
+
+int dg_damg_levels(const dg_damg* m) { return m ? int(m->lv.size()) : 0; }
+
+dg_status dg_damg_level_sizes(const dg_damg* m, int64_t* E, int64_t* N) {
+  DG_CHECK(m, DG_EINVAL, "damg_level_sizes: null handle");
+  for (size_t l = 0; l < m->lv.size(); ++l) {
+    if (E) E[l] = m->lv[l].da->E;
+    if (N) N[l] = m->lv[l].da->N;
+  }
+  return DG_OK;
+}
+
+dg_da* dg_damg_level_da(dg_damg* m, int level) {
+  if (!m || level < 0 || level >= int(m->lv.size())) return nullptr;
+  return m->lv[level].da.get();
+}
+
+dg_status dg_damg_prolong(dg_damg* m, int level, const double* xc, double* xf, int on_device) {
+  DG_CHECK(m && level >= 0 && level + 1 < int(m->lv.size()), DG_EINVAL, "damg_prolong: bad level");
+  Level& F = m->lv[level];
+  Level& C = m->lv[level + 1];
+  const int64_t nf = F.da->N, nc = C.da->N;
+  DBuf<double> dc, df;
+  const double* pc = xc;
+  double* pf = xf;
+  if (!on_device) {
+    DG_TRY(dc.alloc(nc));
+    DG_TRY(df.alloc(nf));
+    DG_CUDA(cudaMemcpy(dc.p, xc, 8 * nc, cudaMemcpyHostToDevice));
+    DG_CUDA(cudaMemcpy(df.p, xf, 8 * nf, cudaMemcpyHostToDevice));
+    pc = dc.p;
+    pf = df.p;
+  }
+  prolong_add<<<grid_for(nf, 256), 256, 0, m->s>>>(F.pptr.p, F.pcol.p, F.pval.p, nf, pc, pf);
+  DG_CUDA(cudaGetLastError());
+  if (!on_device) DG_CUDA(cudaMemcpy(xf, df.p, 8 * nf, cudaMemcpyDeviceToHost));
+  return DG_OK;
+}
+
+dg_status dg_damg_restrict(dg_damg* m, int level, const double* rf, double* rc, int on_device) {
+  DG_CHECK(m && level >= 0 && level + 1 < int(m->lv.size()), DG_EINVAL, "damg_restrict: bad level");
+  Level& F = m->lv[level];
+  Level& C = m->lv[level + 1];
+  const int64_t nf = F.da->N, nc = C.da->N;
+  DBuf<double> dc, df;
+  const double* pf = rf;
+  double* pc = rc;
+  if (!on_device) {
+    DG_TRY(dc.alloc(nc));
+    DG_TRY(df.alloc(nf));
+    DG_CUDA(cudaMemcpy(df.p, rf, 8 * nf, cudaMemcpyHostToDevice));
+    pf = df.p;
+    pc = dc.p;
+  }
+  DG_CUDA(cudaMemsetAsync(pc, 0, 8 * nc, m->s));
+  restrict_residual<<<grid_for(nf, 256), 256, 0, m->s>>>(F.pptr.p, F.pcol.p, F.pval.p, nf, pf, nullptr, pc);
+  DG_CUDA(cudaGetLastError());
+  if (!on_device) DG_CUDA(cudaMemcpy(rc, dc.p, 8 * nc, cudaMemcpyDeviceToHost));
+  return DG_OK;
+}
+
+// Preconditioned CG, zero initial guess, stop on ||b - A x||_2 <= rtol ||b||_2.
+dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, dg_solve_report* rep) {
+  DG_CHECK(m && b && x, DG_EINVAL, "damg_solve: bad arguments");
+  cudaStream_t s = m->s;
+  Level& L = m->lv[0];
+  const int64_t n = L.da->N;
+  const unsigned g = grid_for(n, 256);
+  DBuf<double> db, dx;
+  const double* pb = b;
+  double* px = x;
+  if (!on_device) {
+    DG_TRY(db.alloc(n));
+    DG_TRY(dx.alloc(n));
+    DG_CUDA(cudaMemcpyAsync(db.p, b, 8 * n, cudaMemcpyHostToDevice, s));
+    pb = db.p;
+    px = dx.p;
+  }
+  cudaEvent_t e0, e1;
+  DG_CUDA(cudaEventCreate(&e0));
+  DG_CUDA(cudaEventCreate(&e1));
+  DG_CUDA(cudaEventRecord(e0, s));
+  double* sc = m->scal.p;  // [0] bb, [1] rz, [2] pq, [3] rr, [4] rz_new
+  DG_CUDA(cudaMemsetAsync(px, 0, 8 * n, s));
+  DG_CUDA(cudaMemcpyAsync(m->r.p, pb, 8 * n, cudaMemcpyDeviceToDevice, s));
+  DG_TRY(dot(m, pb, pb, n, sc + 0));
+  double hb = 0;
+  DG_CUDA(cudaMemcpyAsync(&hb, sc + 0, 8, cudaMemcpyDeviceToHost, s));
+  DG_CUDA(cudaStreamSynchronize(s));
+  const double bnorm = std::sqrt(hb);
+  int it = 0;
+  double rel = bnorm > 0 ? 1.0 : 0.0;
+  bool conv = bnorm == 0;
+  if (!conv) {
+    DG_TRY(vcycle(m, 0, m->r.p, m->z.p));
+    DG_CUDA(cudaMemcpyAsync(m->p.p, m->z.p, 8 * n, cudaMemcpyDeviceToDevice, s));
+    DG_TRY(dot(m, m->r.p, m->z.p, n, sc + 1));
+    for (it = 1; it <= m->cfg.maxit; ++it) {
+      DG_TRY(lapmass_apply_f64(L.A.get(), m->p.p, m->q.p, s));
+      DG_TRY(dot(m, m->p.p, m->q.p, n, sc + 2));
+      cg_update<<<kRedBlocks, 256, 0, s>>>(px, m->r.p, m->p.p, m->q.p, n, sc + 1, sc + 2, m->part.p);
+      finish_sum<<<1, 256, 0, s>>>(m->part.p, kRedBlocks, sc + 3);
+      double hr = 0;
+      DG_CUDA(cudaMemcpyAsync(&hr, sc + 3, 8, cudaMemcpyDeviceToHost, s));
+      DG_CUDA(cudaStreamSynchronize(s));
+      rel = std::sqrt(hr) / bnorm;
+      if (!(rel == rel)) break;  // NaN: stop and report
+      if (rel <= m->cfg.rtol) {
+        conv = true;
+        break;
+      }
+      DG_TRY(vcycle(m, 0, m->r.p, m->z.p));
+      DG_TRY(dot(m, m->r.p, m->z.p, n, sc + 4));
+      cg_direction<<<g, 256, 0, s>>>(m->p.p, m->z.p, n, sc + 4, sc + 1);
+      DG_CUDA(cudaMemcpyAsync(sc + 1, sc + 4, 8, cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  DG_CUDA(cudaEventRecord(e1, s));
+  DG_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!on_device) DG_CUDA(cudaMemcpy(x, dx.p, 8 * n, cudaMemcpyDeviceToHost));
+  if (rep) {
+    rep->iterations = it > m->cfg.maxit ? m->cfg.maxit : it;
+    rep->converged = conv ? 1 : 0;
+    rep->rel_residual = rel;
+    rep->solve_ms = ms;
+  }
+  return conv ? DG_OK : DG_ENOTCONVERGED;
+}
+
+void dg_damg_destroy(dg_damg* m) { delete m; }
+
+}  // extern "C"

@@ -1,0 +1,195 @@
+/*
+ * dendro_b200 -- C ABI of the B200 matrix-free octree finite-element path.
+ *
+ * Plain pointers and sizes only.  Every entry point returns a dg_status
+ * (0 = OK) and never traps; a failed call leaves a message retrievable with
+ * dg_last_error().  Handles are opaque, owned by the library, and are not to
+ * be shared between host threads; calls on different handles are reentrant.
+ *
+ * Each declaration names the reference (hsundar/dendro) interface it stands
+ * in for, by file:line within that project.
+ */
+#ifndef DENDRO_B200_H
+#define DENDRO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Errors: PetscErrorCode / CHKERRQ (include/oda/oda.h:26-28) and the
+ * assert(false) paths (include/oda/odaUtils.txx:89-91) become status codes. */
+typedef enum dg_status {
+  DG_OK = 0,
+  DG_EINVAL = 1,          /* bad argument, size or pointer kind */
+  DG_ENOMEM = 2,          /* device allocation failed */
+  DG_ECUDA = 3,           /* a CUDA runtime call failed */
+  DG_ENOTCONVERGED = 4,   /* iteration cap reached before the tolerance */
+  DG_ETIMEOUT = 5,        /* a bounded device wait ran out */
+  DG_EUNBALANCED = 6,     /* octree not linear / complete / 2:1 balanced */
+  DG_EDEPTH = 7,          /* maxDepth outside the supported range */
+  DG_ENOTIMPL = 8
+} dg_status;
+
+/* Octant record: anchor and level|flags with the reference's flag bits
+ * (ot::TreeNode, include/oct/TreeNode.h:40,77-78: level mask 31,
+ * BOUNDARY 64, NODE 128). */
+typedef struct dg_octant {
+  uint32_t x, y, z, level_flags;
+} dg_octant;
+
+typedef struct dg_octree dg_octree; /* device-resident sorted linear octree */
+typedef struct dg_da dg_da;         /* device-resident mesh (ot::DA)         */
+typedef struct dg_mat dg_mat;       /* operator on a mesh (PETSc MatShell)   */
+typedef struct dg_damg dg_damg;     /* multigrid hierarchy (ot::DAMG)        */
+
+const char* dg_status_string(dg_status s);
+/* Copies the last error message of the calling thread into buf. */
+void dg_last_error(char* buf, size_t n);
+/* Number of CUDA devices visible (0 on a host without a GPU). */
+int dg_device_count(void);
+
+/* ------------------------------------------------------------- octree --- */
+
+/* ot::points2Octree / points2OctreeSeq (src/oct/Construct.C:727,880):
+ * quantise n points in [0,1)^3 (xyz interleaved FP64) at maxDepth, sort by
+ * Morton key and emit the coarsest leaves holding <= maxNumPts points.
+ * pts_on_device: 1 when pts is a device pointer, 0 for host memory. */
+dg_status dg_points2octree(const double* pts, int64_t n, int pts_on_device, uint32_t max_depth,
+                           uint32_t max_num_pts, dg_octree** out);
+
+/* Wrap an existing sorted linear octree (e.g. read from an .ot file). */
+dg_status dg_octree_from_octants(const dg_octant* octs, int64_t n, int on_device, uint32_t max_depth,
+                                 dg_octree** out);
+
+/* ot::balanceOctree with incCorner = true (src/oct/Balance.C:31): the
+ * coarsest 2:1 (face, edge and corner) balanced refinement. */
+dg_status dg_balance_octree(const dg_octree* in, dg_octree** out);
+
+/* ot::coarsenOctree, sequential form (src/oct/Coarsen.C:53-104). */
+dg_status dg_coarsen_octree(const dg_octree* in, dg_octree** out);
+
+int64_t dg_octree_size(const dg_octree* t);
+uint32_t dg_octree_max_depth(const dg_octree* t);
+/* Copy the octants to host memory (n = dg_octree_size entries). */
+dg_status dg_octree_export(const dg_octree* t, dg_octant* host_out);
+void dg_octree_destroy(dg_octree* t);
+
+/* ---------------------------------------------------------------- mesh --- */
+
+/* ot::DA::DA (include/oda/oda.h:500; src/oda/oda.C:175 -> DA_FactoryPart0..3,
+ * src/oda/private/odaFactory.C:100-880) on one GPU: embeds the balanced
+ * octree at maxDepth+1 with positive-boundary pseudo-octants
+ * (addBoundaryNodesType1, src/oct/OctFunctions.C:636), flags non-hanging
+ * anchors (flagNodesType3, OctFunctions.C:1501) and builds the element->node
+ * map with hanging masks, child numbers and element types (buildNodeList,
+ * src/oda/private/odaBuildNlist.C:47-856).  The input octree is not consumed. */
+dg_status dg_da_create(const dg_octree* balanced, dg_da** out);
+
+/* Build a mesh from maps computed elsewhere (host arrays): nlist [E][8] node
+ * ids, level [E] (embedded level), cnum [E], hmask [E], node anchors
+ * [N][3] (embedded coordinates), element anchors [E][3]. */
+dg_status dg_da_create_from_maps(int64_t E, int64_t N, uint32_t max_depth, const uint32_t* nlist,
+                                 const uint8_t* level, const uint8_t* cnum, const uint8_t* hmask,
+                                 const uint32_t* node_xyz, const uint32_t* elem_xyz, dg_da** out);
+
+/* Sizes: elements (getElementSize), nodes (getNodeSize + getBoundaryNodeSize,
+ * include/oda/oda.h:668-684) and positive-boundary pseudo-octants. */
+dg_status dg_da_sizes(const dg_da* da, int64_t* elements, int64_t* nodes, int64_t* pseudo_octants);
+uint32_t dg_da_max_depth(const dg_da* da); /* embedded depth (maxDepth + 1) */
+
+/* Copy the maps to host memory; any pointer may be NULL.  nlist [E][8]
+ * (getNodeIndices, include/oda/oda.txx:1111), hmask [E]
+ * (getHangingNodeIndex, src/oda/oda.C:784), cnum [E] (getChildNumber,
+ * oda.txx:1087), etype [E] (GET_ETYPE_BLOCK, include/oda/odaUtils.h:334),
+ * level [E] (getLevel), node anchors [N][3], element anchors [E][3],
+ * node_bdy [N] (1 on the domain boundary). */
+dg_status dg_da_export(const dg_da* da, uint32_t* nlist, uint8_t* hmask, uint8_t* cnum, uint8_t* etype,
+                       uint8_t* level, uint32_t* node_xyz, uint32_t* elem_xyz, uint8_t* node_bdy);
+
+/* Element centres in [0,1]^3, xyz interleaved (CalculateCenters,
+ * examples/src/backend/omgNeumann.C:788-820); out is host memory [E][3]. */
+dg_status dg_da_element_centers(const dg_da* da, double* host_out);
+void dg_da_destroy(dg_da* da);
+
+/* ----------------------------------------------------------- operators --- */
+
+typedef enum dg_prec {
+  DG_PREC_F64 = 0,        /* FP64 vectors and arithmetic                      */
+  DG_PREC_F32 = 1,        /* FP32 vectors, FP32 coefficients and accumulation */
+  DG_PREC_F32_BF16COEF = 2 /* FP32 vectors, BF16-stored coefficients          */
+} dg_prec;
+
+/* CreateJacobian2 / Jacobian2MatMult (examples/src/backend/omgNeumann.C:533,
+ * 643-745): -div(a grad u) + b u with per-element coefficients
+ * coef[2*e] = a_e, coef[2*e+1] = b_e (host memory), or a = b = 1 when coef is
+ * NULL (Jacobian1, examples/src/backend/odaJac.C:271-290). */
+dg_status dg_mat_create_lapmass(dg_da* da, const double* coef, dg_mat** out);
+
+/* ElasticityMatMult (examples/src/backend/elasticityJac.C:130-230): 3 dof per
+ * node, mu h/2 (L x I3) + (mu+lambda) h/2 GD, Dirichlet rows set to the input
+ * and Dirichlet columns skipped.  dirichlet: host [N] flags, or NULL for all
+ * domain-boundary nodes. */
+dg_status dg_mat_create_elasticity(dg_da* da, double mu, double lambda, const uint8_t* dirichlet,
+                                   dg_mat** out);
+
+/* MatMult (MATOP_MULT of the MatShell, omgNeumann.C:700-710): y = A x with
+ * device pointers on the given CUDA stream (NULL = default stream). */
+dg_status dg_mat_mult(dg_mat* A, const double* x, double* y, void* stream);
+/* FP32 inner-solver form of the same operator. */
+dg_status dg_mat_mult_f32(dg_mat* A, const float* x, float* y, void* stream);
+/* MATOP_GET_DIAGONAL (Jacobian2MatGetDiagonal, omgNeumann.C:442-465). */
+dg_status dg_mat_get_diagonal(dg_mat* A, double* d, void* stream);
+/* Same as dg_mat_mult with host x and y: copies in, applies, copies out and
+ * synchronises (the call a PETSc MatShell callback makes on host Vec arrays). */
+dg_status dg_mat_mult_host(dg_mat* A, const double* x, double* y);
+int64_t dg_mat_size(const dg_mat* A); /* rows = dof * nodes */
+void dg_mat_destroy(dg_mat* A);
+
+/* ------------------------------------------------------------ multigrid --- */
+
+typedef struct dg_damg_config {
+  int nlevels;          /* requested levels; fewer when a level drops below 500 octants */
+  int nu_pre, nu_post;  /* damped-Jacobi sweeps (bin/options:187-194) */
+  double omega;         /* Richardson scale (bin/options: 0.667) */
+  double rtol;          /* ||b - A x||_2 <= rtol ||b||_2 */
+  int maxit;            /* outer iteration cap */
+  int inner_prec;       /* dg_prec of the V-cycle (F64, or F32 inside FP64 outer) */
+  int use_graph;        /* capture the V-cycle in a CUDA graph */
+} dg_damg_config;
+
+typedef struct dg_solve_report {
+  int iterations;
+  int converged;
+  double rel_residual;  /* FP64 ||b - A x||_2 / ||b||_2 at exit */
+  double solve_ms;      /* device time of the solve */
+} dg_solve_report;
+
+void dg_damg_default_config(dg_damg_config* cfg);
+
+/* DAMGCreateAndSetDA (include/omg/omg.h:470; src/omg/omg.C:1306-1420): level
+ * hierarchy by coarsenOctree + balanceOctree, a mesh per level, and the
+ * transfer operators of createInterpolationType1 (omg.C:2234-2290). */
+dg_status dg_damg_create(const dg_octree* finest_balanced, const dg_damg_config* cfg, dg_damg** out);
+/* DAMGSetKSP with CreateJacobian2 (omg.h:488; omgNeumann.C:643): finest-level
+ * coefficients (host, 2 per element or NULL), coarse levels averaged as
+ * SetPDECoefFromPts (omgNeumann.C:73-113,188-297). */
+dg_status dg_damg_set_lapmass(dg_damg* m, const double* coef);
+/* DAMGSolve (omg.h:492; omg.C:1121-1169): CG with V(nu_pre, nu_post)
+ * preconditioning.  b and x are host arrays when on_device = 0. */
+dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, dg_solve_report* rep);
+int dg_damg_levels(const dg_damg* m);
+dg_status dg_damg_level_sizes(const dg_damg* m, int64_t* elements, int64_t* nodes);
+dg_da* dg_damg_level_da(dg_damg* m, int level); /* 0 = finest; owned by m */
+/* P (fine level l from level l+1) applied to host or device vectors. */
+dg_status dg_damg_prolong(dg_damg* m, int level, const double* xc, double* xf, int on_device);
+dg_status dg_damg_restrict(dg_damg* m, int level, const double* rf, double* rc, int on_device);
+void dg_damg_destroy(dg_damg* m);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DENDRO_B200_H */

@@ -1,0 +1,77 @@
+"""GPU elemental operators against the oracle (FP64: 1e-12 relative)."""
+import numpy as np
+import pytest
+
+from dendro_b200 import inputs as I
+from tests.cases import points
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12   # FP64 matvec vs the reference-form oracle, relative 2-norm
+TOL32 = 2e-6    # FP32 matvec vs the FP64 oracle, relative 2-norm
+
+
+def setup(gpu, oracle, name):
+    pts, d, m = points(name)
+    bal = oracle.balance(oracle.points2octree(pts, d, m), d)
+    ref = oracle.Mesh(bal, d)
+    da = gpu.DA(gpu.Octree.from_octants(bal, d))
+    return ref, da
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("name", ["gauss2k_d8", "gauss20k_d10", "lognormal20k_d12", "corner_points_d5"])
+def test_lapmass_f64(gpu, oracle, name):
+    import torch
+    ref, da = setup(gpu, oracle, name)
+    x = I.uniform_rhs(ref.N, 1)
+    y_ref = ref.matvec(x)
+    A = gpu.Jacobian2(da)
+    y = A.mult(torch.tensor(x, device="cuda")).cpu().numpy()
+    assert rel(y, y_ref) < TOL64
+    y_host = A.mult(x)
+    assert rel(y_host, y_ref) < TOL64
+
+
+@pytest.mark.parametrize("name", ["gauss20k_d10", "lognormal20k_d12"])
+def test_lapmass_variable_coef_f64(gpu, oracle, name):
+    import torch
+    ref, da = setup(gpu, oracle, name)
+    coef = I.sphere_coefficients(da.elementCenters())
+    x = I.uniform_rhs(ref.N, 3)
+    y_ref = ref.matvec(x, coef)
+    y = gpu.Jacobian2(da, coef).mult(torch.tensor(x, device="cuda")).cpu().numpy()
+    assert rel(y, y_ref) < TOL64
+
+
+def test_lapmass_f32(gpu, oracle):
+    import torch
+    ref, da = setup(gpu, oracle, "lognormal20k_d12")
+    x = I.uniform_rhs(ref.N, 1)
+    y_ref = ref.matvec(x)
+    y = gpu.Jacobian2(da).mult(torch.tensor(x, device="cuda", dtype=torch.float32)).double().cpu().numpy()
+    assert rel(y, y_ref) < TOL32
+
+
+def test_diagonal(gpu, oracle):
+    ref, da = setup(gpu, oracle, "lognormal20k_d12")
+    coef = I.sphere_coefficients(da.elementCenters())
+    d = gpu.Jacobian2(da, coef).getDiagonal().cpu().numpy()
+    assert rel(d, ref.diagonal(coef)) < TOL64
+
+
+def test_constant_and_symmetry(gpu, oracle):
+    """A 1 integrates to the unit-cube volume; (Ax, y) == (x, Ay)."""
+    import torch
+    _, da = setup(gpu, oracle, "gauss20k_d10")
+    A = gpu.Jacobian2(da)
+    one = torch.ones(da.N, dtype=torch.float64, device="cuda")
+    assert abs(A.mult(one).sum().item() - 1.0) < 1e-12
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.rand(da.N, dtype=torch.float64, device="cuda", generator=g)
+    y = torch.rand(da.N, dtype=torch.float64, device="cuda", generator=g)
+    a, b = torch.dot(A.mult(x), y).item(), torch.dot(x, A.mult(y)).item()
+    assert abs(a - b) < 1e-12 * abs(a)

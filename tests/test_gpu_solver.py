@@ -1,0 +1,58 @@
+"""GPU multigrid hierarchy, transfer operators and PCG solve against the oracle."""
+import numpy as np
+import pytest
+
+from dendro_b200 import inputs as I
+from tests.cases import points
+
+pytestmark = pytest.mark.gpu
+
+
+def hierarchy(gpu, oracle, name, nlevels):
+    pts, d, m = points(name)
+    bal = oracle.balance(oracle.points2octree(pts, d, m), d)
+    ref = oracle.DAMG(bal, d, nlevels)
+    got = gpu.DAMG(gpu.Octree.from_octants(bal, d), nlevels=nlevels)
+    return ref, got
+
+
+@pytest.mark.parametrize("name", ["gauss20k_d10", "lognormal20k_d12"])
+def test_level_sizes_and_transfer(gpu, oracle, name):
+    ref, got = hierarchy(gpu, oracle, name, 4)
+    assert got.nlevels == ref.nlevels
+    assert np.array_equal(got.E, ref.E) and np.array_equal(got.N, ref.N)
+    for l in range(ref.nlevels - 1):
+        fm, cm = ref.level_mesh(l), ref.level_mesh(l + 1)
+        ptr, col, val = oracle.prolongation(fm, cm)
+        P = np.zeros((fm.N, cm.N))
+        for f in range(fm.N):
+            P[f, col[ptr[f]:ptr[f + 1]]] += val[ptr[f]:ptr[f + 1]]
+        xc = I.uniform_rhs(cm.N, 10 + l)
+        xf0 = I.uniform_rhs(fm.N, 20 + l)
+        assert np.linalg.norm(got.prolong(l, xc, xf0) - (xf0 + P @ xc)) < 1e-12 * np.linalg.norm(P @ xc)
+        assert np.linalg.norm(got.restrict(l, xf0) - P.T @ xf0) < 1e-12 * np.linalg.norm(P.T @ xf0)
+
+
+def test_pcg_solution_matches_oracle(gpu, oracle):
+    ref, got = hierarchy(gpu, oracle, "gauss20k_d10", 4)
+    b = I.uniform_rhs(int(ref.N[0]), 1)
+    xr, itr, _ = ref.pcg(b, 1e-10, 100)
+    x, rep = got.solve(b)
+    assert rep["converged"] and rep["rel_residual"] <= 1e-8
+    fm = ref.level_mesh(0)
+    assert np.linalg.norm(fm.matvec(x) - b) <= 1.01e-8 * np.linalg.norm(b)
+    assert np.linalg.norm(x - xr) <= 1e-6 * np.linalg.norm(xr)
+    assert abs(rep["iterations"] - len(_) + 1) <= 3 or rep["iterations"] <= itr
+
+
+def test_pcg_variable_coefficients(gpu, oracle):
+    pts, d, m = points("lognormal20k_d12")
+    bal = oracle.balance(oracle.points2octree(pts, d, m), d)
+    got = gpu.DAMG(gpu.Octree.from_octants(bal, d))
+    coef = I.sphere_coefficients(got.level_da(0).elementCenters())
+    got.setKSP(coef)
+    b = I.uniform_rhs(int(got.N[0]), 3)
+    x, rep = got.solve(b)
+    assert rep["converged"]
+    fm = oracle.Mesh(bal, d)
+    assert np.linalg.norm(fm.matvec(x, coef) - b) <= 1.01e-8 * np.linalg.norm(b)

@@ -1,0 +1,97 @@
+"""Compile the reference's own octree / mesh / operator / transfer sources
+(from /root/reference, read-only) into oracle/_ref/, single-rank, against
+the project-written MPI and PETSc stand-ins in oracle/ref_build/shim.
+
+The reference at its HEAD forces Hilbert ordering inside TreeNode::operator<
+(include/oct/TreeNode.txx:198-202) while its mesh layer is Morton-only; the
+build therefore uses a copy of TreeNode.h / TreeNode.txx, generated into
+oracle/_ref/patched/ by this script, with those five lines removed so that
+the Morton comparator is used throughout.  Nothing under /root/reference is
+modified and nothing it contains is committed.
+
+Outputs (git-ignored; they travel to the GPU box with the snapshot):
+  oracle/_ref/dendro_ref       driver binary
+  oracle/_ref/stencils/*.inp   the reference's stencil tables (read from cwd)
+"""
+import os
+import re
+import shutil
+import subprocess
+import sys
+
+REF = "/root/reference"
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(os.path.dirname(HERE), "_ref")
+
+SOURCES = [
+    "src/oct/TreeNode.C", "src/oct/Construct.C", "src/oct/Balance.C", "src/oct/Coarsen.C",
+    "src/oct/OctFunctions.C", "src/oct/pickBdy.C", "src/oct/BlockPart.C", "src/oct/TreeNodePointer.C",
+    "src/oda/oda.C", "src/oda/odaUtils.C", "src/oda/odaPartition.C", "src/oda/private/odaFactory.C",
+    "src/oda/private/odaBuildNlist.C", "src/par/parUtils.C", "src/binOps/binUtils.C", "src/point/Point.C",
+    "src/hilbert/morton.cpp", "src/hilbert/sfc.cpp", "src/hilbert/hilbert.cpp", "src/hilbert/rotation.cpp",
+    "src/omg/RestrictMatVec.C", "src/omg/ProlongMatVec.C", "src/omg/VtxMaps.C", "src/omg/RmatType1StencilsAux.C",
+    "src/omg/RmatType2StencilsAux.C", "src/omg/omg.C", "src/test/testUtils.C",
+    "examples/src/backend/omgNeumann.C", "examples/src/backend/handleType2Stencils.C",
+    "examples/src/backend/elasticityJac.C",
+]
+INCLUDE_DIRS = ["include", "include/oct", "include/oda", "include/omg", "include/par", "include/seq",
+                "include/omp_par", "include/binOps", "include/point", "include/hilbert", "include/test",
+                "include/sys", "include/fem", "include/pc", "examples/include"]
+
+
+def patched_headers():
+    pdir = os.path.join(OUT, "patched")
+    os.makedirs(pdir, exist_ok=True)
+    txx = open(os.path.join(REF, "include/oct/TreeNode.txx")).read().split("\n")
+    # drop the forced "#ifdef HILBERT_ORDERING / #undef / #endif / #define HILBERT_ORDERING /
+    # #define USE_NCA_PROPERTY" block inside operator< (lines 198-202)
+    block = [l.strip() for l in txx[197:202]]
+    assert block[0].startswith("#ifdef HILBERT_ORDERING") and block[4].startswith("#define USE_NCA_PROPERTY"), block
+    txx = txx[:197] + txx[202:]
+    open(os.path.join(pdir, "TreeNode.txx"), "w").write("\n".join(txx))
+    h = open(os.path.join(REF, "include/oct/TreeNode.h")).read()
+    h = re.sub(r'#include "\.\./([a-zA-Z]+)/', lambda m: '#include "' + os.path.join(REF, "include", m.group(1)) + "/", h)
+    open(os.path.join(pdir, "TreeNode.h"), "w").write(h)
+    return pdir
+
+
+def main():
+    if not os.path.isdir(REF):
+        print("reference tree not present; skipping the reference build")
+        return 0
+    os.makedirs(os.path.join(OUT, "obj"), exist_ok=True)
+    pdir = patched_headers()
+    inc = ["-I" + os.path.join(HERE, "shim"), "-I" + pdir] + ["-I" + os.path.join(REF, d) for d in INCLUDE_DIRS]
+    flags = ["-O2", "-std=c++11", "-fopenmp", "-w", "-fpermissive", "-D__USE_PVT_DA_IN_MG__", "-D__SILENT_MODE__",
+             "-include", os.path.join(pdir, "TreeNode.h")]
+    objs, procs = [], []
+    for src in SOURCES + [os.path.join(HERE, "ref_driver.cpp")]:
+        path = src if os.path.isabs(src) else os.path.join(REF, src)
+        obj = os.path.join(OUT, "obj", os.path.basename(src) + ".o")
+        objs.append(obj)
+        if os.path.exists(obj) and os.path.getmtime(obj) > max(os.path.getmtime(path), os.path.getmtime(__file__),
+                                                             *[os.path.getmtime(os.path.join(HERE, "shim", f))
+                                                               for f in os.listdir(os.path.join(HERE, "shim"))]):
+            continue
+        procs.append((subprocess.Popen(["g++", *flags, *inc, "-c", path, "-o", obj], stdout=subprocess.PIPE,
+                                       stderr=subprocess.STDOUT), src))
+    bad = []
+    for p, src in procs:
+        out, _ = p.communicate()
+        if p.returncode:
+            bad.append(src)
+            sys.stderr.write(f"==== {src}\n" + out.decode()[-6000:])
+    if bad:
+        print("reference build failed:", bad)
+        return 1
+    subprocess.check_call(["g++", "-fopenmp", "-o", os.path.join(OUT, "dendro_ref"), *objs])
+    sdir = os.path.join(OUT, "stencils")
+    os.makedirs(sdir, exist_ok=True)
+    for f in os.listdir(os.path.join(REF, "Stencils")):
+        shutil.copy(os.path.join(REF, "Stencils", f), sdir)
+    print(os.path.join(OUT, "dendro_ref"))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,2 @@
+/* oracle build stand-in: see petsc.h */
+#include "petsc.h"

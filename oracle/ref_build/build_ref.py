@@ -6,7 +6,9 @@ The reference at its HEAD forces Hilbert ordering inside TreeNode::operator<
 (include/oct/TreeNode.txx:198-202) while its mesh layer is Morton-only; the
 build therefore uses a copy of TreeNode.h / TreeNode.txx, generated into
 oracle/_ref/patched/ by this script, with those five lines removed so that
-the Morton comparator is used throughout.  Nothing under /root/reference is
+the Morton comparator is used throughout.  A copy of include/hilbert/rotation.h
+gets one more byte in two sprintf buffers (the Hilbert tables that every
+TreeNode constructor reads overflow them by the terminator).  Nothing under /root/reference is
 modified and nothing it contains is committed.
 
 Outputs (git-ignored; they travel to the GPU box with the snapshot):
@@ -31,8 +33,8 @@ SOURCES = [
     "src/hilbert/morton.cpp", "src/hilbert/sfc.cpp", "src/hilbert/hilbert.cpp", "src/hilbert/rotation.cpp",
     "src/omg/RestrictMatVec.C", "src/omg/ProlongMatVec.C", "src/omg/VtxMaps.C", "src/omg/RmatType1StencilsAux.C",
     "src/omg/RmatType2StencilsAux.C", "src/omg/omg.C", "src/test/testUtils.C",
-    "examples/src/backend/omgNeumann.C", "examples/src/backend/handleType2Stencils.C",
-    "examples/src/backend/elasticityJac.C",
+    "examples/src/backend/omgJac.C", "examples/src/backend/handleType2Stencils.C",
+    "examples/src/backend/elasticityJac.C", "examples/src/backend/odaJac.C", "examples/src/backend/vecMass.C",
 ]
 INCLUDE_DIRS = ["include", "include/oct", "include/oda", "include/omg", "include/par", "include/seq",
                 "include/omp_par", "include/binOps", "include/point", "include/hilbert", "include/test",
@@ -52,6 +54,14 @@ def patched_headers():
     h = open(os.path.join(REF, "include/oct/TreeNode.h")).read()
     h = re.sub(r'#include "\.\./([a-zA-Z]+)/', lambda m: '#include "' + os.path.join(REF, "include", m.group(1)) + "/", h)
     open(os.path.join(pdir, "TreeNode.h"), "w").write(h)
+    # include/hilbert/rotation.h:72-143 formats 4 (8) digits into char[4]
+    # (char[8]) with sprintf, writing the terminator past the buffer; the
+    # copy gives the buffers room for it (Hilbert-only code, unused here)
+    r = open(os.path.join(REF, "include/hilbert/rotation.h")).read()
+    n4, n8 = r.count("char str[4];"), r.count("char str[8];")
+    assert n4 == 2 and n8 == 2, (n4, n8)
+    r = r.replace("char str[4];", "char str[5];").replace("char str[8];", "char str[9];")
+    open(os.path.join(pdir, "rotation.h"), "w").write(r)
     return pdir
 
 
@@ -62,8 +72,8 @@ def main():
     os.makedirs(os.path.join(OUT, "obj"), exist_ok=True)
     pdir = patched_headers()
     inc = ["-I" + os.path.join(HERE, "shim"), "-I" + pdir] + ["-I" + os.path.join(REF, d) for d in INCLUDE_DIRS]
-    flags = ["-O2", "-std=c++11", "-fopenmp", "-w", "-fpermissive", "-D__USE_PVT_DA_IN_MG__", "-D__SILENT_MODE__",
-             "-include", os.path.join(pdir, "TreeNode.h")]
+    flags = ["-O1", "-g", "-std=c++11", "-fopenmp", "-w", "-fpermissive", "-D__USE_PVT_DA_IN_MG__", "-D__SILENT_MODE__",
+             "-include", os.path.join(pdir, "rotation.h"), "-include", os.path.join(pdir, "TreeNode.h")]
     objs, procs = [], []
     for src in SOURCES + [os.path.join(HERE, "ref_driver.cpp")]:
         path = src if os.path.isabs(src) else os.path.join(REF, src)
@@ -84,7 +94,7 @@ def main():
     if bad:
         print("reference build failed:", bad)
         return 1
-    subprocess.check_call(["g++", "-fopenmp", "-o", os.path.join(OUT, "dendro_ref"), *objs])
+    subprocess.check_call(["g++", "-fopenmp", "-rdynamic", "-o", os.path.join(OUT, "dendro_ref"), *objs])
     sdir = os.path.join(OUT, "stencils")
     os.makedirs(sdir, exist_ok=True)
     for f in os.listdir(os.path.join(REF, "Stencils")):

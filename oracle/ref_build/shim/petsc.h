@@ -66,6 +66,12 @@ typedef const char* PetscRandomType;
 #define PETSC_MAX_PATH_LEN 4096
 #define PETSC_VIEWER_STDOUT_WORLD ((PetscViewer)0)
 #define PETSC_VIEWER_STDOUT_SELF ((PetscViewer)0)
+#define PETSC_VIEWER_DRAW_(c) ((PetscViewer)0)
+#define PETSC_ERR_ARG_NULL 85
+#define PETSC_ERR_ORDER 73
+#define PETSC_ERR_ARG_INCOMP 75
+#define MATDAAD "daad"
+#define MATMFFD "mffd"
 
 #define VECMPI "mpi"
 #define VECSEQ "seq"
@@ -287,20 +293,28 @@ static inline PetscErrorCode MatSetOption(Mat, int, PetscBool) { return 0; }
 DG_SHIM_NOOP(KSPSetType) DG_SHIM_NOOP(KSPSetOperators) DG_SHIM_NOOP(KSPSetFromOptions) DG_SHIM_NOOP(KSPSetUp)
 DG_SHIM_NOOP(KSPSolve) DG_SHIM_NOOP(KSPSetTolerances) DG_SHIM_NOOP(KSPSetOptionsPrefix) DG_SHIM_NOOP(KSPAppendOptionsPrefix)
 DG_SHIM_NOOP(KSPSetInitialGuessNonzero) DG_SHIM_NOOP(KSPSetInitialGuessKnoll) DG_SHIM_NOOP(KSPSetNormType)
-DG_SHIM_NOOP(KSPSetPCSide) DG_SHIM_NOOP(KSPSetNullSpace) DG_SHIM_NOOP(KSPMonitorSet) DG_SHIM_NOOP(KSPRichardsonSetScale)
-DG_SHIM_NOOP(KSPSetConvergenceTest) DG_SHIM_NOOP(KSPGetIterationNumber) DG_SHIM_NOOP(KSPGetConvergedReason)
+DG_SHIM_NOOP(KSPSetPCSide) DG_SHIM_NOOP(KSPSetNullSpace)  DG_SHIM_NOOP(KSPRichardsonSetScale)
+ DG_SHIM_NOOP(KSPGetIterationNumber) DG_SHIM_NOOP(KSPGetConvergedReason)
 DG_SHIM_NOOP(KSPView) DG_SHIM_NOOP(PCSetType) DG_SHIM_NOOP(PCSetOperators) DG_SHIM_NOOP(PCMGSetLevels)
 DG_SHIM_NOOP(PCMGSetType) DG_SHIM_NOOP(PCMGSetCycleType) DG_SHIM_NOOP(PCMGSetInterpolation) DG_SHIM_NOOP(PCMGSetRestriction)
-DG_SHIM_NOOP(PCMGSetResidual) DG_SHIM_NOOP(PCMGSetX) DG_SHIM_NOOP(PCMGSetRhs) DG_SHIM_NOOP(PCMGSetR)
+ DG_SHIM_NOOP(PCMGSetX) DG_SHIM_NOOP(PCMGSetRhs) DG_SHIM_NOOP(PCMGSetR)
 DG_SHIM_NOOP(PCMGSetNumberSmoothUp) DG_SHIM_NOOP(PCMGSetNumberSmoothDown) DG_SHIM_NOOP(PCSetFromOptions)
 DG_SHIM_NOOP(PCSetOptionsPrefix) DG_SHIM_NOOP(PCAppendOptionsPrefix) DG_SHIM_NOOP(PCGetOptionsPrefix)
 DG_SHIM_NOOP(KSPGetOptionsPrefix) DG_SHIM_NOOP(PCShellSetSetUp) DG_SHIM_NOOP(PCShellSetName) DG_SHIM_NOOP(PCShellSetDestroy)
 DG_SHIM_NOOP(PCShellSetContext) DG_SHIM_NOOP(PCShellSetApply) DG_SHIM_NOOP(PCFactorSetShiftType)
 DG_SHIM_NOOP(PCFactorSetShiftPd) DG_SHIM_NOOP(PCSetUp) DG_SHIM_NOOP(PCApply) DG_SHIM_NOOP(PCGetOperators)
 DG_SHIM_NOOP(PCRedundantGetPC) DG_SHIM_NOOP(PCRedundantGetKSP) DG_SHIM_NOOP(KSPSetDM) DG_SHIM_NOOP(PetscViewerASCIIOpen)
-DG_SHIM_NOOP(PetscViewerDestroy) DG_SHIM_NOOP(PetscViewerASCIISetTab) DG_SHIM_NOOP(PCMGResidualDefault)
-DG_SHIM_NOOP(KSPMonitorDefault) DG_SHIM_NOOP(KSPConvergedSkip) DG_SHIM_NOOP(KSPDefaultConverged) DG_SHIM_NOOP(PCMGDefaultResidual)
+DG_SHIM_NOOP(PetscViewerDestroy) DG_SHIM_NOOP(PetscViewerASCIISetTab) 
+   
 DG_SHIM_NOOP(PetscObjectReference) DG_SHIM_NOOP(PetscObjectDereference) DG_SHIM_NOOP(PCShellGetContext)
+static inline PetscErrorCode KSPMonitorDefault(KSP, PetscInt, PetscReal, void*) { return 0; }
+static inline PetscErrorCode KSPConvergedSkip(KSP, PetscInt, PetscReal, KSPConvergedReason*, void*) { return 0; }
+static inline PetscErrorCode KSPDefaultConverged(KSP, PetscInt, PetscReal, KSPConvergedReason*, void*) { return 0; }
+static inline PetscErrorCode PCMGResidualDefault(Mat, Vec, Vec, Vec) { return 0; }
+#define PCMGDefaultResidual PCMGResidualDefault
+template <class... A> static inline PetscErrorCode KSPSetConvergenceTest(A...) { return 0; }
+template <class... A> static inline PetscErrorCode KSPMonitorSet(A...) { return 0; }
+template <class... A> static inline PetscErrorCode PCMGSetResidual(A...) { return 0; }
 static inline PetscErrorCode KSPCreate(MPI_Comm, KSP* k) { *k = new _p_KSP(); return 0; }
 static inline PetscErrorCode KSPDestroy(KSP* k) { delete *k; *k = 0; return 0; }
 static inline PetscErrorCode KSPDestroy(KSP k) { delete k; return 0; }

@@ -1,0 +1,179 @@
+"""Generate the golden fixtures of tests/golden/ from the reference itself.
+
+Runs oracle/_ref/dendro_ref -- the reference's own octree, mesh, operator and
+transfer sources compiled single-rank by oracle/ref_build/build_ref.py -- on
+seeded inputs and stores its outputs as compressed .npz files, plus digests
+of the reference's stencil tables (Stencils/*.inp).  Needs the reference
+tree and the reference build; the fixtures it writes are committed and the
+tests read only them.
+
+    python tests/golden/make_golden.py
+
+Inputs whose linear octree the reference cannot produce (its points2Octree
+does not terminate above 8 points at its HEAD) start from the oracle's
+linear octree; the reference then balances, coarsens, meshes, applies the
+operators and the transfers.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from dendro_b200 import inputs as I  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "dendro_ref")
+REF_CWD = os.path.join(ROOT, "oracle", "_ref", "stencils")
+STENCILS = "/root/reference/Stencils"
+
+MU, LAM = 1.0 / (2.0 * 1.3), 0.3 / (1.3 * 0.4)  # E = 1, nu = 0.3
+
+
+def run(*args, timeout=3600):
+    r = subprocess.run([REF_BIN, *map(str, args)], cwd=REF_CWD, capture_output=True, text=True, timeout=timeout)
+    if r.returncode:
+        raise RuntimeError(f"reference run {args[0]} failed ({r.returncode}): {r.stderr[-2000:]}")
+    return r.stderr
+
+
+def octs_to_u32(o):
+    return np.stack([o["x"], o["y"], o["z"], o["lf"] & 31], 1).astype(np.uint32)
+
+
+def read_octs(path):
+    return np.fromfile(path, np.uint32).reshape(-1, 4)
+
+
+P2O_CASES = [(n, seed, depth) for n in (4, 8) for seed in range(4) for depth in (6, 10)]
+
+MESH_CASES = {
+    "corner_points_d5": lambda: (np.array([[0, 0, 0], [1 - 2.0 ** -6] * 3, [0.5, 0.5, 0.5], [0.49, 0.51, 0.5]]), 5),
+    "uniform600_d7": lambda: (I.clamp_unit(I.uniform_cloud(600, 11), 7), 7),
+    "gauss1k_d8": lambda: (I.clamp_unit(I.gaussian_cloud(1000, 12), 8), 8),
+    "lognormal1k_d10": lambda: (I.clamp_unit(I.lognormal_cloud(1000, 13), 10), 10),
+}
+TRANSFER_CASE = ("gauss1k_d8", 3)
+
+
+def p2o_fixture(tmp):
+    rec = {}
+    for n, seed, depth in P2O_CASES:
+        pts = np.random.default_rng(1000 + 17 * n + seed).uniform(0, 1, (n, 3))
+        pts.tofile(os.path.join(tmp, "pts.f64"))
+        try:
+            run("octree", os.path.join(tmp, "pts.f64"), depth, 1, tmp, timeout=20)
+        except subprocess.TimeoutExpired:
+            print(f"points2Octree did not terminate: n={n} seed={seed} depth={depth}")
+            continue
+        key = f"n{n}_s{seed}_d{depth}"
+        rec[key + "_pts"] = pts
+        rec[key + "_p2o"] = read_octs(os.path.join(tmp, "p2o.u32"))
+        rec[key + "_bal"] = read_octs(os.path.join(tmp, "bal.u32"))
+    np.savez_compressed(os.path.join(OUT, "p2o_tiny.npz"), **rec)
+
+
+def mesh_fixture(tmp, name):
+    pts, depth = MESH_CASES[name]()
+    lin = O.points2octree(pts, depth, 1)
+    octs_to_u32(lin).tofile(os.path.join(tmp, "lin.u32"))
+    run("balance", os.path.join(tmp, "lin.u32"), depth, tmp)
+    bal = read_octs(os.path.join(tmp, "bal.u32"))
+    coarse = read_octs(os.path.join(tmp, "coarse.u32"))
+    bal.tofile(os.path.join(tmp, "bal_in.u32"))
+    run("mesh", os.path.join(tmp, "bal_in.u32"), depth, tmp)
+    elem = np.fromfile(os.path.join(tmp, "elem.u32"), np.uint32).reshape(-1, 14)
+    node_xyz = np.fromfile(os.path.join(tmp, "node_xyz.u32"), np.uint32).reshape(-1, 3)
+    N = len(node_xyz)
+    x = np.random.default_rng(7).uniform(-1, 1, N)
+    x.tofile(os.path.join(tmp, "x.f64"))
+    run("matvec", os.path.join(tmp, "bal_in.u32"), depth, os.path.join(tmp, "x.f64"), "none",
+        os.path.join(tmp, "y.f64"))
+    y = np.fromfile(os.path.join(tmp, "y.f64"))
+    # variable coefficients: a = 1e4 inside the sphere r < 0.25, b = 1
+    s = 2.0 ** -(elem[:, 3].astype(np.float64) - 1)
+    cen = elem[:, :3] / 2.0 ** depth + 0.5 * s[:, None]
+    coef = I.sphere_coefficients(cen)
+    coef.tofile(os.path.join(tmp, "coef.f64"))
+    run("matvec", os.path.join(tmp, "bal_in.u32"), depth, os.path.join(tmp, "x.f64"), os.path.join(tmp, "coef.f64"),
+        os.path.join(tmp, "yc.f64"))
+    yc = np.fromfile(os.path.join(tmp, "yc.f64"))
+    x3 = np.random.default_rng(8).uniform(-1, 1, 3 * N)
+    x3.tofile(os.path.join(tmp, "x3.f64"))
+    run("elastic", os.path.join(tmp, "bal_in.u32"), depth, os.path.join(tmp, "x3.f64"), os.path.join(tmp, "y3.f64"))
+    y3 = np.fromfile(os.path.join(tmp, "y3.f64"))
+    np.savez_compressed(os.path.join(OUT, f"mesh_{name}.npz"), depth=depth, lin=octs_to_u32(lin), bal=bal,
+                        coarse=coarse, elem=elem, node_xyz=node_xyz, x=x, y=y, coef=coef, yc=yc, x3=x3, y3=y3,
+                        mu=MU, lam=LAM)
+
+
+def transfer_fixture(tmp):
+    name, nlevels = TRANSFER_CASE
+    pts, depth = MESH_CASES[name]()
+    bal = O.balance(O.points2octree(pts, depth, 1), depth)
+    octs_to_u32(bal).tofile(os.path.join(tmp, "bal_t.u32"))
+    dm = O.DAMG(bal, depth, nlevels)
+    rec = {"depth": depth, "nlevels": dm.nlevels}
+    for l in range(dm.nlevels - 1):
+        xf = np.random.default_rng(30 + l).uniform(-1, 1, int(dm.N[l]))
+        xc = np.random.default_rng(40 + l).uniform(-1, 1, int(dm.N[l + 1]))
+        xf.tofile(os.path.join(tmp, f"level{l}_in.f64"))
+        xc.tofile(os.path.join(tmp, f"coarse{l}_in.f64"))
+        rec[f"xf{l}"], rec[f"xc{l}"] = xf, xc
+    run("transfer", os.path.join(tmp, "bal_t.u32"), depth, nlevels, tmp)
+    for l in range(dm.nlevels):
+        rec[f"elem{l}"] = np.fromfile(os.path.join(tmp, f"level{l}_elem.u32"), np.uint32).reshape(-1, 14)
+        rec[f"node_xyz{l}"] = np.fromfile(os.path.join(tmp, f"level{l}_node_xyz.u32"), np.uint32).reshape(-1, 3)
+    for l in range(dm.nlevels - 1):
+        rec[f"restrict{l}"] = np.fromfile(os.path.join(tmp, f"restrict{l}.f64"))
+        rec[f"prolong{l}"] = np.fromfile(os.path.join(tmp, f"prolong{l}.f64"))
+    rec["bal"] = octs_to_u32(bal)
+    np.savez_compressed(os.path.join(OUT, f"transfer_{name}.npz"), **rec)
+
+
+def table_digest(a):
+    """Checksums of each (child number, type) table: sum, sum of squares,
+    sum of magnitudes and a position-weighted sum."""
+    m = a.shape[-1]
+    w = (7.0 * np.arange(m)[:, None] + 3.0 * np.arange(m)[None, :] + 1.0) / (10.0 * m)
+    return np.stack([a.sum(axis=(2, 3)), (a * a).sum(axis=(2, 3)), np.abs(a).sum(axis=(2, 3)),
+                     (a * w).sum(axis=(2, 3))], -1)
+
+
+def stencil_digests():
+    """Checksums of the reference's Laplacian, mass, grad-div and same-level
+    restriction tables (Stencils/*Type2Stencils.inp)."""
+    rec = {}
+    for tag, fname, m in (("lap", "LapType2Stencils.inp", 8), ("mass", "MassType2Stencils.inp", 8),
+                          ("gd", "GDType2Stencils.inp", 24), ("rmat2", "RmatType2Stencils.inp", 8)):
+        a = np.array(open(os.path.join(STENCILS, fname)).read().split(), float).reshape(8, 18, m, m)
+        rec[tag] = table_digest(a)
+    np.savez_compressed(os.path.join(OUT, "stencil_digests.npz"), **rec)
+
+
+def main():
+    if not os.path.exists(REF_BIN):
+        sys.exit("build the reference first: python oracle/ref_build/build_ref.py")
+    if "--stencils-only" in sys.argv:
+        stencil_digests()
+        return
+    with tempfile.TemporaryDirectory() as tmp:
+        p2o_fixture(tmp)
+        for name in MESH_CASES:
+            mesh_fixture(tmp, name)
+        transfer_fixture(tmp)
+    stencil_digests()
+    for f in sorted(os.listdir(OUT)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(OUT, f)))
+
+
+if __name__ == "__main__":
+    main()

@@ -255,3 +255,12 @@ class DAMG:
         rc = np.empty(int(self.N[level + 1]))
         check(lib().dg_damg_restrict(self.h, level, ptr(rf), ptr(rc), 0), "damg_restrict")
         return rc
+
+
+def vecDot(x, y, stream=None) -> float:
+    """FP64 inner product of two device vectors (PETSc VecDot stand-in)."""
+    import torch
+    out = torch.empty(1, dtype=torch.float64, device=x.device)
+    s = None if stream is None else C.c_void_p(stream.cuda_stream)
+    check(lib().dg_vec_dot(ptr(x), ptr(y), x.numel(), ptr(out), s), "vec_dot")
+    return float(out.item())

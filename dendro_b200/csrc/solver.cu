@@ -622,4 +622,17 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
 
 void dg_damg_destroy(dg_damg* m) { delete m; }
 
+dg_status dg_vec_dot(const double* x, const double* y, int64_t n, double* result, void* stream) {
+  DG_CHECK(x && y && result && n >= 0, DG_EINVAL, "vec_dot: bad arguments");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  DBuf<double> part;  // one partial sum per reduction block
+  DG_TRY(part.alloc(kRedBlocks));
+  dot_partial<<<kRedBlocks, 256, 0, s>>>(x, y, n, part.p);
+  finish_sum<<<1, 256, 0, s>>>(part.p, kRedBlocks, result);
+  DG_CUDA(cudaGetLastError());
+  // the partials are released when this call returns
+  DG_CUDA(cudaStreamSynchronize(s));
+  return DG_OK;
+}
+
 }  // extern "C"

@@ -188,6 +188,14 @@ dg_status dg_damg_prolong(dg_damg* m, int level, const double* xc, double* xf, i
 dg_status dg_damg_restrict(dg_damg* m, int level, const double* rf, double* rc, int on_device);
 void dg_damg_destroy(dg_damg* m);
 
+/* -------------------------------------------------------- vector kernels --- */
+
+/* VecDot / VecNorm^2 as PETSc's KSPCG calls them (KSPSolve, src/omg/omg.C:1166,
+ * with bin/options:50 -ksp_type cg): *result = sum_i x[i] y[i] in FP64 with a
+ * fixed-order (deterministic) two-stage reduction.  x, y and result are device
+ * pointers; the call synchronises the stream before returning. */
+dg_status dg_vec_dot(const double* x, const double* y, int64_t n, double* result, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

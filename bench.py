@@ -34,7 +34,7 @@ WORKLOAD = "lognormal1m_d14"
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="dendro_b200", choices=["dendro_b200", "reference"])
     p.add_argument("--workload", default=WORKLOAD)
@@ -127,12 +127,12 @@ def run_dendro(args, rank, world):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
     stream = torch.cuda.current_stream(dev)
 
+    clocks = ClockSampler(dev.index)
     for _ in range(args.warmup):
         A.mult(x, y, stream)
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    clocks = ClockSampler(dev.index)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     torch.cuda.synchronize()
     for i in range(args.steps):
@@ -172,14 +172,23 @@ def run_dendro(args, rank, world):
 
     solve = None
     if not args.no_solve:
-        m = dg.DAMG(bal)
-        m.setKSP(coef)
         b = torch.tensor(I.uniform_rhs(N, 3), device=dev)
-        m.solve(b, allow_unconverged=True)
-        xs, rep = m.solve(b, allow_unconverged=True)
-        solve = {"ms_to_1e-8": rep["solve_ms"], "iterations": rep["iterations"],
-                 "rel_residual": rep["rel_residual"], "converged": rep["converged"], "levels": int(m.nlevels),
-                 "precision": "fp64 V(2,2) + fp64 CG"}
+        solve = {}
+        for tag, kw in (("plain_fp64", dict(inner_prec=0, use_graph=False)),
+                        ("chosen", dict(inner_prec=1, use_graph=True))):
+            m = dg.DAMG(bal, **kw)
+            m.setKSP(coef)
+            m.solve(b, allow_unconverged=True)  # warm-up (captures the graph)
+            reps = [m.solve(b, allow_unconverged=True)[1] for _ in range(3)]
+            rep = min(reps, key=lambda r: r["solve_ms"])
+            solve[tag] = {"ms_to_1e-8": round(rep["solve_ms"], 3), "iterations": rep["iterations"],
+                          "rel_residual": rep["rel_residual"], "converged": rep["converged"],
+                          "levels": int(m.nlevels)}
+            del m
+        solve["plain_fp64"]["method"] = "FP64 CG + FP64 V(2,2) damped Jacobi, dense FP64 coarse solve"
+        solve["chosen"]["method"] = ("FP64 flexible CG + FP32 V(2,2) (FP32 operator, smoother, transfers), "
+                                     "FP64 coarse solve, V-cycle replayed from a CUDA graph")
+        solve["speedup_chosen_vs_plain"] = round(solve["plain_fp64"]["ms_to_1e-8"] / solve["chosen"]["ms_to_1e-8"], 3)
     return dict(E=E, N=N, setup_s=setup_s, ms_per_step=ms_per_step, gdofs=gdofs, achieved=achieved, peak=peak,
                 peak_kind=peak_kind, alg_bytes=alg_bytes, clocks=clk, e2e=e2e, solve=solve, bal=bal, depth=depth,
                 coef=coef, x=x.cpu().numpy(), y=y.cpu().numpy())
@@ -230,6 +239,7 @@ def main():
         "gpu_launches": args.steps,
         "clocks": r["clocks"],
         "solve": r["solve"],
+        "matvec_kernel": os.environ.get("DG_MATVEC_KERNEL", "tiled"),
         "setup_s": round(r["setup_s"], 3),
     }
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -24,6 +24,7 @@ struct dg_da {
   dg::DBuf<uint32_t> tile_lo;
   dg::DBuf<uint32_t> tile_span;
   int64_t ntiles = 0;
+  int tile_elems = 0;
   uint32_t max_span = 0;
 };
 

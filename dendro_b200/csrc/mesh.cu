@@ -154,16 +154,16 @@ __global__ void tile_ranges(const uint32_t* __restrict__ nl, int64_t E, int tile
                             uint32_t* __restrict__ lo_out, uint32_t* __restrict__ span_out) {
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     uint32_t lo = 0xffffffffu, hi = 0;
-    int64_t e0 = t * tile;
-    for (int64_t i = threadIdx.x; i < int64_t(tile) * 8; i += blockDim.x) {
-      int64_t e = e0 + (i % tile);
-      int v = int(i / tile);
-      if (e < E) {
-        uint32_t id = nl[int64_t(v) * E + e];
-        lo = min(lo, id);
-        hi = max(hi, id);
+    const int64_t e0 = t * tile;
+    for (int v = 0; v < 8; ++v)
+      for (int i = threadIdx.x; i < tile; i += blockDim.x) {
+        const int64_t e = e0 + i;
+        if (e < E) {
+          const uint32_t id = nl[int64_t(v) * E + e];
+          lo = min(lo, id);
+          hi = max(hi, id);
+        }
       }
-    }
     for (int o = 16; o > 0; o >>= 1) {
       lo = min(lo, __shfl_down_sync(0xffffffffu, lo, o));
       hi = max(hi, __shfl_down_sync(0xffffffffu, hi, o));
@@ -255,7 +255,8 @@ dg_status build_mesh(const dg_octree* tree, dg_da* da, cudaStream_t s) {
 }
 
 dg_status build_tiles(dg_da* da, cudaStream_t s) {
-  const int tile = 256;
+  const int tile = 512;  // elements per tile of the shared-memory operator kernel
+  da->tile_elems = tile;
   da->ntiles = (da->E + tile - 1) / tile;
   DG_TRY(da->tile_lo.alloc(da->ntiles));
   DG_TRY(da->tile_span.alloc(da->ntiles));

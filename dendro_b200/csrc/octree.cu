@@ -106,12 +106,17 @@ __global__ void emit_gaps(const uint64_t* __restrict__ lk, int64_t u, uint32_t D
 // -------------------------------------------------------------- balance --
 __global__ void level_composite(const uint64_t* __restrict__ ok, int64_t n, uint32_t D, uint64_t* __restrict__ out,
                                 uint32_t* __restrict__ hist) {
+  __shared__ uint32_t h[32];
+  if (threadIdx.x < 32) h[threadIdx.x] = 0;
+  __syncthreads();
   for (int64_t i = gtid(); i < n; i += gstride()) {
     uint32_t l = okey_l(ok[i]);
     uint64_t lk = okey_m(ok[i]) >> (3u * (D - l));
     out[i] = (uint64_t(l) << 59) | lk;
-    atomicAdd(&hist[l], 1u);
+    atomicAdd(&h[l], 1u);
   }
+  __syncthreads();
+  if (threadIdx.x < 32 && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
 }
 
 __global__ void strip_level(uint64_t* __restrict__ k, int64_t n) {

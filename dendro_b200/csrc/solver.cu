@@ -15,6 +15,8 @@
 
 #include "dg_internal.h"
 
+#include <cuda_bf16.h>
+
 namespace dg {
 dg_status node_boundary_flags(const dg_da* da, uint8_t* d_out, cudaStream_t s);
 dg_status convert_f64_to_f32(const double* a, float* b, int64_t n, cudaStream_t s);
@@ -144,35 +146,46 @@ __global__ void prolong_fill(const uint64_t* __restrict__ fnk, int64_t Nf, const
 }
 
 // xf += P xc
+template <class T>
 __global__ void prolong_add(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
-                            const double* __restrict__ val, int64_t Nf, const double* __restrict__ xc,
-                            double* __restrict__ xf) {
+                            const T* __restrict__ val, int64_t Nf, const T* __restrict__ xc, T* __restrict__ xf) {
   for (int64_t f = gtid(); f < Nf; f += gstride()) {
-    double s = 0;
+    T s = 0;
     for (uint32_t k = ptr[f]; k < ptr[f + 1]; ++k) s += val[k] * xc[col[k]];
     xf[f] += s;
   }
 }
 
 // rc = P^T (b - t) (restriction of the residual, fused)
+template <class T>
 __global__ void restrict_residual(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
-                                  const double* __restrict__ val, int64_t Nf, const double* __restrict__ b,
-                                  const double* __restrict__ t, double* __restrict__ rc) {
+                                  const T* __restrict__ val, int64_t Nf, const T* __restrict__ b,
+                                  const T* __restrict__ t, T* __restrict__ rc) {
   for (int64_t f = gtid(); f < Nf; f += gstride()) {
-    double r = t ? b[f] - t[f] : b[f];
-    if (r == 0.0) continue;
+    T r = t ? b[f] - t[f] : b[f];
+    if (r == T(0)) continue;
     for (uint32_t k = ptr[f]; k < ptr[f + 1]; ++k) atomicAdd(rc + col[k], val[k] * r);
   }
 }
 
 // --------------------------------------------------------------- smoother --
-__global__ void jacobi_first(double* __restrict__ x, const double* __restrict__ b, const double* __restrict__ dinv,
-                             double omega, int64_t n) {
+template <class T>
+__global__ void jacobi_first(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ dinv, T omega,
+                             int64_t n) {
   for (int64_t i = gtid(); i < n; i += gstride()) x[i] = omega * dinv[i] * b[i];
 }
-__global__ void jacobi_update(double* __restrict__ x, const double* __restrict__ b, const double* __restrict__ t,
-                              const double* __restrict__ dinv, double omega, int64_t n) {
+template <class T>
+__global__ void jacobi_update(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ t,
+                              const T* __restrict__ dinv, T omega, int64_t n) {
   for (int64_t i = gtid(); i < n; i += gstride()) x[i] += omega * dinv[i] * (b[i] - t[i]);
+}
+template <class A, class B>
+__global__ void convert(const A* __restrict__ a, B* __restrict__ b, int64_t n) {
+  for (int64_t i = gtid(); i < n; i += gstride()) b[i] = B(a[i]);
+}
+// Coefficients stored in BF16: round the FP32 copy to the nearest BF16 value.
+__global__ void to_bf16_values(float* __restrict__ a, int64_t n) {
+  for (int64_t i = gtid(); i < n; i += gstride()) a[i] = __bfloat162float(__float2bfloat16_rn(a[i]));
 }
 __global__ void invert(double* __restrict__ d, int64_t n) {
   for (int64_t i = gtid(); i < n; i += gstride()) d[i] = 1.0 / d[i];
@@ -250,6 +263,14 @@ __global__ void cg_update(double* __restrict__ x, double* __restrict__ r, const 
   v = block_sum(v);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
 }
+// flexible (Polak-Ribiere) direction: p = z + beta p,
+// beta = ((r, z) - (r, z_old)) / (r_old, z_old)
+__global__ void cg_direction_flex(double* __restrict__ p, const double* __restrict__ z, int64_t n,
+                                  const double* __restrict__ rz, const double* __restrict__ rzo,
+                                  const double* __restrict__ den) {
+  const double beta = (*rz - *rzo) / *den;
+  for (int64_t i = gtid(); i < n; i += gstride()) p[i] = z[i] + beta * p[i];
+}
 // p = z + beta p with beta = num / den
 __global__ void cg_direction(double* __restrict__ p, const double* __restrict__ z, int64_t n,
                              const double* __restrict__ num, const double* __restrict__ den) {
@@ -268,6 +289,8 @@ struct Level {
   // P to this level from level + 1 (CSR over this level's nodes)
   DBuf<uint32_t> pptr, pcol;
   DBuf<double> pval;
+  // FP32 inner V-cycle
+  DBuf<float> dinv32, x32, b32, t32, pval32;
 };
 
 struct dg_damg {
@@ -276,8 +299,14 @@ struct dg_damg {
   DBuf<double> Ainv;  // dense inverse of the coarsest operator
   int64_t nc = 0;
   // PCG work vectors on the finest level and device scalars
-  DBuf<double> r, z, p, q, part, scal;
+  DBuf<double> r, z, zold, p, q, part, scal;
+  DBuf<float> r32, z32;
   cudaStream_t s = nullptr;
+  cudaGraphExec_t precond_graph = nullptr;
+  ~dg_damg() {
+    if (precond_graph) cudaGraphExecDestroy(precond_graph);
+    if (s) cudaStreamDestroy(s);
+  }
 };
 
 namespace {
@@ -316,6 +345,31 @@ dg_status setup_level_vectors(Level& L, cudaStream_t s) {
   DG_TRY(L.t.alloc(N));
   DG_TRY(lapmass_diag(L.A.get(), L.dinv.p, s));
   invert<<<grid_for(N, 256), 256, 0, s>>>(L.dinv.p, N);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status round_coef_bf16(float* c, int64_t n, cudaStream_t s) {
+  to_bf16_values<<<grid_for(n, 256), 256, 0, s>>>(c, n);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+// FP32 copies for the inner V-cycle: smoother diagonal, prolongation weights
+// and (optionally BF16-rounded) coefficients.
+dg_status setup_level_f32(dg_damg* m, Level& L, cudaStream_t s) {
+  const int64_t N = L.da->N;
+  DG_TRY(L.dinv32.alloc(N));
+  DG_TRY(L.x32.alloc(N));
+  DG_TRY(L.b32.alloc(N));
+  DG_TRY(L.t32.alloc(N));
+  convert<double, float><<<grid_for(N, 256), 256, 0, s>>>(L.dinv.p, L.dinv32.p, N);
+  if (L.pval.n) {
+    DG_TRY(L.pval32.alloc(L.pval.n));
+    convert<double, float><<<grid_for(L.pval.n, 256), 256, 0, s>>>(L.pval.p, L.pval32.p, L.pval.n);
+  }
+  if (L.A->has_coef && m->cfg.inner_prec == DG_PREC_F32_BF16COEF)
+    DG_TRY(round_coef_bf16(L.A->coef32.p, 2 * L.da->E, s));
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }
@@ -376,6 +430,11 @@ dg_status set_operators(dg_damg* m, const double* coef) {
     }
     L.A = std::move(A);
     DG_TRY(setup_level_vectors(L, s));
+    if (m->cfg.inner_prec != DG_PREC_F64) DG_TRY(setup_level_f32(m, L, s));
+  }
+  if (m->precond_graph) {  // operators changed: capture again on the next solve
+    cudaGraphExecDestroy(m->precond_graph);
+    m->precond_graph = nullptr;
   }
   return setup_coarse(m);
 }
@@ -405,7 +464,8 @@ dg_status vcycle(dg_damg* m, size_t l, const double* b, double* x) {
   }
   Level& C = m->lv[l + 1];
   DG_CUDA(cudaMemsetAsync(C.b.p, 0, 8 * C.da->N, s));
-  restrict_residual<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval.p, n, b, m->cfg.nu_pre > 0 ? L.t.p : nullptr, C.b.p);
+  restrict_residual<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval.p, n, b,
+                                      m->cfg.nu_pre > 0 ? (const double*)L.t.p : (const double*)nullptr, C.b.p);
   DG_TRY(vcycle(m, l + 1, C.b.p, C.x.p));
   prolong_add<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval.p, n, C.x.p, x);
   for (int k = 0; k < m->cfg.nu_post; ++k) {
@@ -413,6 +473,79 @@ dg_status vcycle(dg_damg* m, size_t l, const double* b, double* x) {
     jacobi_update<<<g, 256, 0, s>>>(x, b, L.t.p, L.dinv.p, w, n);
   }
   DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+// FP32 V-cycle; the coarsest solve stays FP64 (the dense inverse).
+dg_status vcycle32(dg_damg* m, size_t l, const float* b, float* x) {
+  cudaStream_t s = m->s;
+  Level& L = m->lv[l];
+  const int64_t n = L.da->N;
+  const unsigned g = grid_for(n, 256);
+  if (l + 1 == m->lv.size()) {
+    convert<float, double><<<g, 256, 0, s>>>(b, L.b.p, n);
+    dense_gemv<<<grid_for(n * 32, 256), 256, 0, s>>>(m->Ainv.p, n, L.b.p, L.x.p);
+    convert<double, float><<<g, 256, 0, s>>>(L.x.p, x, n);
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+  }
+  const float w = float(m->cfg.omega);
+  if (m->cfg.nu_pre > 0) {
+    jacobi_first<<<g, 256, 0, s>>>(x, b, L.dinv32.p, w, n);
+    for (int k = 1; k < m->cfg.nu_pre; ++k) {
+      DG_TRY(lapmass_apply_f32(L.A.get(), x, L.t32.p, s));
+      jacobi_update<<<g, 256, 0, s>>>(x, b, L.t32.p, L.dinv32.p, w, n);
+    }
+    DG_TRY(lapmass_apply_f32(L.A.get(), x, L.t32.p, s));
+  } else {
+    DG_CUDA(cudaMemsetAsync(x, 0, 4 * n, s));
+  }
+  Level& C = m->lv[l + 1];
+  DG_CUDA(cudaMemsetAsync(C.b32.p, 0, 4 * C.da->N, s));
+  restrict_residual<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval32.p, n, b,
+                                      m->cfg.nu_pre > 0 ? (const float*)L.t32.p : (const float*)nullptr, C.b32.p);
+  DG_TRY(vcycle32(m, l + 1, C.b32.p, C.x32.p));
+  prolong_add<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval32.p, n, C.x32.p, x);
+  for (int k = 0; k < m->cfg.nu_post; ++k) {
+    DG_TRY(lapmass_apply_f32(L.A.get(), x, L.t32.p, s));
+    jacobi_update<<<g, 256, 0, s>>>(x, b, L.t32.p, L.dinv32.p, w, n);
+  }
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+// z = M^-1 r on the finest level: the FP64 V-cycle, or the FP32 one between
+// conversions of r and z.
+dg_status precond_body(dg_damg* m) {
+  if (m->cfg.inner_prec == DG_PREC_F64) return vcycle(m, 0, m->r.p, m->z.p);
+  const int64_t n = m->lv[0].da->N;
+  const unsigned g = grid_for(n, 256);
+  convert<double, float><<<g, 256, 0, m->s>>>(m->r.p, m->r32.p, n);
+  DG_TRY(vcycle32(m, 0, m->r32.p, m->z32.p));
+  convert<float, double><<<g, 256, 0, m->s>>>(m->z32.p, m->z.p, n);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+// Apply the preconditioner, replaying it from a CUDA graph when enabled (the
+// graph is captured on the first application).
+dg_status precond(dg_damg* m) {
+  if (!m->cfg.use_graph) return precond_body(m);
+  if (!m->precond_graph) {
+    cudaGraph_t graph = nullptr;
+    DG_CUDA(cudaStreamBeginCapture(m->s, cudaStreamCaptureModeThreadLocal));
+    dg_status st = precond_body(m);
+    cudaError_t e = cudaStreamEndCapture(m->s, &graph);
+    if (st != DG_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    DG_CUDA(e);
+    e = cudaGraphInstantiate(&m->precond_graph, graph, 0);
+    cudaGraphDestroy(graph);
+    DG_CUDA(e);
+  }
+  DG_CUDA(cudaGraphLaunch(m->precond_graph, m->s));
   return DG_OK;
 }
 
@@ -443,8 +576,8 @@ dg_status dg_damg_create(const dg_octree* finest, const dg_damg_config* cfg, dg_
   auto m = std::make_unique<dg_damg>();
   if (cfg) m->cfg = *cfg; else dg_damg_default_config(&m->cfg);
   DG_CHECK(m->cfg.nlevels >= 1, DG_EINVAL, "damg_create: nlevels must be >= 1");
-  cudaStream_t s = nullptr;
-  m->s = s;
+  DG_CUDA(cudaStreamCreateWithFlags(&m->s, cudaStreamNonBlocking));
+  cudaStream_t s = m->s;
   // level octrees: coarsen + balance (omg.C:1376-1420)
   std::vector<std::unique_ptr<dg_octree>> trees;
   auto t0 = std::make_unique<dg_octree>();
@@ -476,6 +609,11 @@ dg_status dg_damg_create(const dg_octree* finest, const dg_damg_config* cfg, dg_
   DG_TRY(m->z.alloc(N));
   DG_TRY(m->p.alloc(N));
   DG_TRY(m->q.alloc(N));
+  DG_TRY(m->zold.alloc(N));
+  if (m->cfg.inner_prec != DG_PREC_F64) {
+    DG_TRY(m->r32.alloc(N));
+    DG_TRY(m->z32.alloc(N));
+  }
   DG_TRY(m->part.alloc(kRedBlocks));
   DG_TRY(m->scal.alloc(8));
   DG_TRY(set_operators(m.get(), nullptr));
@@ -520,8 +658,10 @@ dg_status dg_damg_prolong(dg_damg* m, int level, const double* xc, double* xf, i
     pc = dc.p;
     pf = df.p;
   }
+  if (on_device) DG_CUDA(cudaDeviceSynchronize());
   prolong_add<<<grid_for(nf, 256), 256, 0, m->s>>>(F.pptr.p, F.pcol.p, F.pval.p, nf, pc, pf);
   DG_CUDA(cudaGetLastError());
+  DG_CUDA(cudaStreamSynchronize(m->s));
   if (!on_device) DG_CUDA(cudaMemcpy(xf, df.p, 8 * nf, cudaMemcpyDeviceToHost));
   return DG_OK;
 }
@@ -541,9 +681,12 @@ dg_status dg_damg_restrict(dg_damg* m, int level, const double* rf, double* rc, 
     pf = df.p;
     pc = dc.p;
   }
+  if (on_device) DG_CUDA(cudaDeviceSynchronize());
   DG_CUDA(cudaMemsetAsync(pc, 0, 8 * nc, m->s));
-  restrict_residual<<<grid_for(nf, 256), 256, 0, m->s>>>(F.pptr.p, F.pcol.p, F.pval.p, nf, pf, nullptr, pc);
+  restrict_residual<<<grid_for(nf, 256), 256, 0, m->s>>>(F.pptr.p, F.pcol.p, F.pval.p, nf, pf, (const double*)nullptr,
+                                                          pc);
   DG_CUDA(cudaGetLastError());
+  DG_CUDA(cudaStreamSynchronize(m->s));
   if (!on_device) DG_CUDA(cudaMemcpy(rc, dc.p, 8 * nc, cudaMemcpyDeviceToHost));
   return DG_OK;
 }
@@ -558,6 +701,8 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
   DBuf<double> db, dx;
   const double* pb = b;
   double* px = x;
+  // the caller's device data may come from any stream
+  if (on_device) DG_CUDA(cudaDeviceSynchronize());
   if (!on_device) {
     DG_TRY(db.alloc(n));
     DG_TRY(dx.alloc(n));
@@ -580,8 +725,9 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
   int it = 0;
   double rel = bnorm > 0 ? 1.0 : 0.0;
   bool conv = bnorm == 0;
+  const bool flexible = m->cfg.inner_prec != DG_PREC_F64;
   if (!conv) {
-    DG_TRY(vcycle(m, 0, m->r.p, m->z.p));
+    DG_TRY(precond(m));
     DG_CUDA(cudaMemcpyAsync(m->p.p, m->z.p, 8 * n, cudaMemcpyDeviceToDevice, s));
     DG_TRY(dot(m, m->r.p, m->z.p, n, sc + 1));
     for (it = 1; it <= m->cfg.maxit; ++it) {
@@ -598,9 +744,15 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
         conv = true;
         break;
       }
-      DG_TRY(vcycle(m, 0, m->r.p, m->z.p));
+      if (flexible) DG_CUDA(cudaMemcpyAsync(m->zold.p, m->z.p, 8 * n, cudaMemcpyDeviceToDevice, s));
+      DG_TRY(precond(m));
       DG_TRY(dot(m, m->r.p, m->z.p, n, sc + 4));
-      cg_direction<<<g, 256, 0, s>>>(m->p.p, m->z.p, n, sc + 4, sc + 1);
+      if (flexible) {
+        DG_TRY(dot(m, m->r.p, m->zold.p, n, sc + 5));
+        cg_direction_flex<<<g, 256, 0, s>>>(m->p.p, m->z.p, n, sc + 4, sc + 5, sc + 1);
+      } else {
+        cg_direction<<<g, 256, 0, s>>>(m->p.p, m->z.p, n, sc + 4, sc + 1);
+      }
       DG_CUDA(cudaMemcpyAsync(sc + 1, sc + 4, 8, cudaMemcpyDeviceToDevice, s));
     }
   }
@@ -623,7 +775,7 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
 void dg_damg_destroy(dg_damg* m) { delete m; }
 
 dg_status dg_vec_dot(const double* x, const double* y, int64_t n, double* result, void* stream) {
-  DG_CHECK(x && y && result && n >= 0, DG_EINVAL, "vec_dot: bad arguments");
+  DG_CHECK(result && n >= 0 && (n == 0 || (x && y)), DG_EINVAL, "vec_dot: bad arguments");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   DBuf<double> part;  // one partial sum per reduction block
   DG_TRY(part.alloc(kRedBlocks));

@@ -35,6 +35,9 @@ def test_balance_coarsen_mesh_operators(gpu, name):
     x = torch.tensor(g["x"], device="cuda")
     assert rel(gpu.Jacobian2(da).mult(x).cpu().numpy(), g["y"]) < TOL
     assert rel(gpu.Jacobian2(da, g["coef"]).mult(x).cpu().numpy(), g["yc"]) < TOL
+    x3 = torch.tensor(g["x3"], device="cuda")
+    y3 = gpu.Elasticity(da, float(g["mu"]), float(g["lam"])).mult(x3).cpu().numpy()
+    assert rel(y3, g["y3"]) < TOL
 
 
 def test_transfer(gpu):

@@ -75,3 +75,25 @@ def test_constant_and_symmetry(gpu, oracle):
     y = torch.rand(da.N, dtype=torch.float64, device="cuda", generator=g)
     a, b = torch.dot(A.mult(x), y).item(), torch.dot(x, A.mult(y)).item()
     assert abs(a - b) < 1e-12 * abs(a)
+
+
+@pytest.mark.parametrize("name", ["gauss2k_d8", "lognormal20k_d12"])
+def test_elasticity_f64(gpu, oracle, name):
+    import torch
+    ref, da = setup(gpu, oracle, name)
+    mu, lam = 1.0 / (2.0 * 1.3), 0.3 / (1.3 * 0.4)
+    x = I.uniform_rhs(3 * ref.N, 5)
+    y_ref = ref.elasticity_matvec(x, mu, lam)
+    y = gpu.Elasticity(da, mu, lam).mult(torch.tensor(x, device="cuda")).cpu().numpy()
+    assert rel(y, y_ref) < TOL64
+
+
+def test_elasticity_diagonal_matches_unit_vectors(gpu, oracle):
+    import torch
+    ref, da = setup(gpu, oracle, "corner_points_d5")
+    mu, lam = 0.4, 0.6
+    A = gpu.Elasticity(da, mu, lam)
+    d = A.getDiagonal().cpu().numpy()
+    n = 3 * ref.N
+    cols = np.array([ref.elasticity_matvec(np.eye(n)[j], mu, lam)[j] for j in range(n)])
+    assert rel(d, cols) < TOL64

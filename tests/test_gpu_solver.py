@@ -56,3 +56,21 @@ def test_pcg_variable_coefficients(gpu, oracle):
     assert rep["converged"]
     fm = oracle.Mesh(bal, d)
     assert np.linalg.norm(fm.matvec(x, coef) - b) <= 1.01e-8 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("inner_prec,use_graph", [(0, True), (1, False), (1, True), (2, True)])
+def test_pcg_precision_and_graph(gpu, oracle, inner_prec, use_graph):
+    """FP32 (or BF16-coefficient) inner V-cycle inside FP64 flexible PCG, with
+    and without the CUDA-graph preconditioner: the FP64 true residual reaches 1e-8."""
+    pts, d, m = points("lognormal20k_d12")
+    bal = oracle.balance(oracle.points2octree(pts, d, m), d)
+    got = gpu.DAMG(gpu.Octree.from_octants(bal, d), inner_prec=inner_prec, use_graph=use_graph)
+    coef = I.sphere_coefficients(got.level_da(0).elementCenters())
+    got.setKSP(coef)
+    b = I.uniform_rhs(int(got.N[0]), 3)
+    x, rep = got.solve(b)
+    x2, rep2 = got.solve(b)  # second solve replays the captured graph
+    assert rep["converged"] and rep2["converged"]
+    fm = oracle.Mesh(bal, d)
+    for xx in (x, x2):
+        assert np.linalg.norm(fm.matvec(xx, coef) - b) <= 1.01e-8 * np.linalg.norm(b)

@@ -199,16 +199,23 @@ class Elasticity(_Mat):
 class DAMG:
     """ot::DAMG: level hierarchy + V-cycle preconditioned CG on the GPU."""
 
-    def __init__(self, finest: Octree, nlevels: int = 30, nu_pre: int = 2, nu_post: int = 2,
+    def __init__(self, finest, nlevels: int = 30, nu_pre: int = 2, nu_post: int = 2,
                  omega: float = 2.0 / 3.0, rtol: float = 1e-8, maxit: int = 200, inner_prec: int = 0,
                  use_graph: bool = False):
+        """`finest` is one balanced Octree, or a list of them for the batched
+        form (independent meshes solved together, one launch per kernel)."""
         cfg = DamgConfig()
         lib().dg_damg_default_config(C.byref(cfg))
         cfg.nlevels, cfg.nu_pre, cfg.nu_post, cfg.omega = nlevels, nu_pre, nu_post, omega
         cfg.rtol, cfg.maxit, cfg.inner_prec, cfg.use_graph = rtol, maxit, inner_prec, int(use_graph)
         h = C.c_void_p()
-        check(lib().dg_damg_create(finest.h, C.byref(cfg), C.byref(h)), "damg_create")
+        if isinstance(finest, (list, tuple)):
+            arr = (C.c_void_p * len(finest))(*[t.h.value for t in finest])
+            check(lib().dg_damg_create_batch(arr, len(finest), C.byref(cfg), C.byref(h)), "damg_create_batch")
+        else:
+            check(lib().dg_damg_create(finest.h, C.byref(cfg), C.byref(h)), "damg_create")
         self.h = h
+        self.count = int(lib().dg_damg_batch_count(self.h))
         self.nlevels = int(lib().dg_damg_levels(self.h))
         E = np.empty(self.nlevels, np.int64)
         N = np.empty(self.nlevels, np.int64)
@@ -219,6 +226,13 @@ class DAMG:
         if getattr(self, "h", None) is not None and self.h.value:
             lib().dg_damg_destroy(self.h)
             self.h = None
+
+    def batch_offsets(self, level: int = 0):
+        """(element offsets, node offsets) of each mesh on a level, count + 1 entries."""
+        eo = np.empty(self.count + 1, np.int64)
+        no = np.empty(self.count + 1, np.int64)
+        check(lib().dg_damg_batch_offsets(self.h, level, ptr(eo), ptr(no)), "damg_batch_offsets")
+        return eo, no
 
     def level_da(self, l: int) -> DA:
         return DA(handle=lib().dg_damg_level_da(self.h, l), owner=self)

@@ -69,7 +69,10 @@ dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStrea
 dg_status lapmass_diag(const dg_mat* A, double* d, cudaStream_t s);
 dg_status elasticity_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status elasticity_diag(const dg_mat* A, double* d, cudaStream_t s);
-// Dense assembled operator (row-major n x n) of a small level.
-dg_status lapmass_assemble_dense(const dg_mat* A, double* dense, cudaStream_t s);
+// Dense assembled operator of a small level as row-major blocks, one per
+// independent mesh: node r belongs to block row_blk[r] with node offset
+// boff[b], size bn[b] and storage offset baoff[b].
+dg_status lapmass_assemble_dense(const dg_mat* A, double* dense, int64_t dense_size, const uint32_t* row_blk,
+                                 const int64_t* boff, const int64_t* bn, const int64_t* baoff, cudaStream_t s);
 
 }  // namespace dg

@@ -228,10 +228,13 @@ __global__ void lapmass_diag_kernel(const uint32_t* __restrict__ nl, const uint3
   }
 }
 
-// Dense assembly of a small level (row-major N x N).
+// Dense assembly of a small level into per-mesh row-major blocks: node r of
+// block b = row_blk[r] lands at dense[aoff[b] + (r - off[b]) * n[b] + ...].
 template <class CT>
 __global__ void lapmass_dense_kernel(const uint32_t* __restrict__ nl, const uint32_t* __restrict__ meta,
-                                     const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E, int64_t N,
+                                     const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
+                                     const uint32_t* __restrict__ row_blk, const int64_t* __restrict__ boff,
+                                     const int64_t* __restrict__ bn, const int64_t* __restrict__ baoff,
                                      double* __restrict__ A) {
   for (int64_t t = gtid(); t < E * 8; t += gstride()) {
     int64_t e = t >> 3;
@@ -248,7 +251,11 @@ __global__ void lapmass_dense_kernel(const uint32_t* __restrict__ nl, const uint
     lapmass_ref(u, f1, f2, r);
     if (mask) scatter_hanging(r, c, mask);
     const uint32_t col = nl[int64_t(j) * E + e];
-    for (int k = 0; k < 8; ++k) atomicAdd(A + int64_t(nl[int64_t(k) * E + e]) * N + col, r[k]);
+    const uint32_t blk = row_blk[col];
+    const int64_t o = boff[blk], n = bn[blk];
+    double* Ab = A + baoff[blk];
+    for (int k = 0; k < 8; ++k)
+      atomicAdd(Ab + (int64_t(nl[int64_t(k) * E + e]) - o) * n + (int64_t(col) - o), r[k]);
   }
 }
 
@@ -301,13 +308,14 @@ dg_status lapmass_diag(const dg_mat* A, double* d, cudaStream_t s) {
   return DG_OK;
 }
 
-dg_status lapmass_assemble_dense(const dg_mat* A, double* dense, cudaStream_t s) {
+dg_status lapmass_assemble_dense(const dg_mat* A, double* dense, int64_t dense_size, const uint32_t* row_blk,
+                                 const int64_t* boff, const int64_t* bn, const int64_t* baoff, cudaStream_t s) {
   const dg_da* da = A->da;
-  DG_CUDA(cudaMemsetAsync(dense, 0, sizeof(double) * da->N * da->N, s));
+  DG_CUDA(cudaMemsetAsync(dense, 0, sizeof(double) * dense_size, s));
   const double* ca = A->has_coef ? A->coef.p : nullptr;
   const double* cb = A->has_coef ? A->coef.p + da->E : nullptr;
   lapmass_dense_kernel<double><<<grid_for(da->E * 8, 256, 8), 256, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E,
-                                                                          da->N, dense);
+                                                                          row_blk, boff, bn, baoff, dense);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }

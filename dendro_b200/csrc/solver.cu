@@ -8,6 +8,7 @@
 //    src/omg/ProlongMatVec.C:154-284, RestrictMatVec.C:486-619);
 //  * V(nu_pre, nu_post) cycle with Richardson(omega)+Jacobi smoothing and a
 //    dense FP64 direct coarse solve, inside CG (bin/options:50-53,182-207).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <memory>
@@ -48,9 +49,9 @@ __device__ __forceinline__ int64_t max_lower_bound(const uint64_t* __restrict__ 
 }
 
 // ---------------------------------------------------------- coefficients --
-__global__ void coarse_coef_kernel(const uint64_t* __restrict__ fk, int64_t Ef, const double* __restrict__ fc,
-                                   const uint64_t* __restrict__ ck, int64_t Ec, double* __restrict__ cc,
-                                   uint32_t* __restrict__ err) {
+__global__ void coarse_coef_kernel(const uint64_t* __restrict__ fk, int64_t Ef, const double* __restrict__ fa,
+                                   const double* __restrict__ fb, const uint64_t* __restrict__ ck, int64_t Ec,
+                                   double* __restrict__ ca, double* __restrict__ cb, uint32_t* __restrict__ err) {
   for (int64_t e = gtid(); e < Ec; e += gstride()) {
     uint64_t m = okey_m(ck[e]);
     uint32_t l = okey_l(ck[e]);
@@ -60,18 +61,37 @@ __global__ void coarse_coef_kernel(const uint64_t* __restrict__ fk, int64_t Ef, 
       continue;
     }
     if (okey_l(fk[f]) == l) {
-      cc[e] = fc[f];
-      cc[Ec + e] = fc[Ef + f];
+      ca[e] = fa[f];
+      cb[e] = fb[f];
     } else {
       double a = 0, b = 0;
       for (int k = 0; k < 8 && f + k < Ef; ++k) {
-        a += fc[f + k];
-        b += fc[Ef + f + k];
+        a += fa[f + k];
+        b += fb[f + k];
       }
-      cc[e] = a / 8.0;
-      cc[Ec + e] = b / 8.0;
+      ca[e] = a / 8.0;
+      cb[e] = b / 8.0;
     }
   }
+}
+
+// concatenation helpers for batches of meshes
+__global__ void copy_add_u32(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, int64_t n, uint32_t add) {
+  for (int64_t i = gtid(); i < n; i += gstride()) dst[i] = src[i] + add;
+}
+__global__ void fill_u16(uint16_t* __restrict__ d, int64_t n0, int64_t n1, uint16_t v) {
+  for (int64_t i = n0 + gtid(); i < n1; i += gstride()) d[i] = v;
+}
+// per-mesh squared norms (acc zeroed by the caller), one shared slot per mesh
+__global__ void seg_sqnorm(const double* __restrict__ r, int64_t n, const uint16_t* __restrict__ node_mesh, int nmesh,
+                           double* __restrict__ acc) {
+  extern __shared__ double sh[];
+  for (int i = threadIdx.x; i < nmesh; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  for (int64_t i = gtid(); i < n; i += gstride()) atomicAdd(sh + node_mesh[i], r[i] * r[i]);
+  __syncthreads();
+  for (int i = threadIdx.x; i < nmesh; i += blockDim.x)
+    if (sh[i] != 0.0) atomicAdd(acc + i, sh[i]);
 }
 
 // ----------------------------------------------------------- prolongation --
@@ -192,27 +212,48 @@ __global__ void invert(double* __restrict__ d, int64_t n) {
 }
 
 // ------------------------------------------------------------ coarse solve --
-__global__ void gj_col(const double* __restrict__ A, int64_t n, int64_t k, double* __restrict__ colk) {
-  for (int64_t i = gtid(); i < n; i += gstride()) colk[i] = A[i * n + k];
+// Gauss-Jordan inversion of SPD blocks, all blocks advancing one pivot k per
+// launch (blockIdx.y = block; blocks with n <= k skip).
+__global__ void gj_col(double* __restrict__ A, const int64_t* __restrict__ bn, const int64_t* __restrict__ baoff,
+                       int64_t k, double* __restrict__ colk, const int64_t* __restrict__ boff) {
+  const int64_t n = bn[blockIdx.y];
+  if (k >= n) return;
+  const double* Ab = A + baoff[blockIdx.y];
+  double* ck = colk + boff[blockIdx.y];
+  for (int64_t i = gtid(); i < n; i += gstride()) ck[i] = Ab[i * n + k];
 }
-__global__ void gj_row(double* __restrict__ A, int64_t n, int64_t k, const double* __restrict__ colk) {
-  const double piv = colk[k];
-  for (int64_t j = gtid(); j < n; j += gstride()) A[k * n + j] = (j == k ? 1.0 : A[k * n + j]) / piv;
+__global__ void gj_row(double* __restrict__ A, const int64_t* __restrict__ bn, const int64_t* __restrict__ baoff,
+                       int64_t k, const double* __restrict__ colk, const int64_t* __restrict__ boff) {
+  const int64_t n = bn[blockIdx.y];
+  if (k >= n) return;
+  double* Ab = A + baoff[blockIdx.y];
+  const double piv = colk[boff[blockIdx.y] + k];
+  for (int64_t j = gtid(); j < n; j += gstride()) Ab[k * n + j] = (j == k ? 1.0 : Ab[k * n + j]) / piv;
 }
-__global__ void gj_elim(double* __restrict__ A, int64_t n, int64_t k, const double* __restrict__ colk) {
+__global__ void gj_elim(double* __restrict__ A, const int64_t* __restrict__ bn, const int64_t* __restrict__ baoff,
+                        int64_t k, const double* __restrict__ colk, const int64_t* __restrict__ boff) {
+  const int64_t n = bn[blockIdx.y];
+  if (k >= n) return;
+  double* Ab = A + baoff[blockIdx.y];
+  const double* ck = colk + boff[blockIdx.y];
   for (int64_t t = gtid(); t < n * n; t += gstride()) {
     int64_t i = t / n, j = t - i * n;
     if (i == k) continue;
-    A[t] = (j == k ? 0.0 : A[t]) - colk[i] * A[k * n + j];
+    Ab[t] = (j == k ? 0.0 : Ab[t]) - ck[i] * Ab[k * n + j];
   }
 }
-// x = Ainv b, one warp per row
-__global__ void dense_gemv(const double* __restrict__ A, int64_t n, const double* __restrict__ b, double* __restrict__ x) {
+// x = Ainv b with block-diagonal Ainv, one warp per row
+__global__ void dense_gemv(const double* __restrict__ A, int64_t N, const uint32_t* __restrict__ row_blk,
+                           const int64_t* __restrict__ boff, const int64_t* __restrict__ bn,
+                           const int64_t* __restrict__ baoff, const double* __restrict__ b, double* __restrict__ x) {
   const int lane = threadIdx.x & 31;
-  for (int64_t row = gtid() >> 5; row < n; row += gstride() >> 5) {
+  for (int64_t row = gtid() >> 5; row < N; row += gstride() >> 5) {
+    const uint32_t blk = row_blk[row];
+    const int64_t o = boff[blk], n = bn[blk];
+    const double* Ar = A + baoff[blk] + (row - o) * n;
     double s = 0;
-    for (int64_t j = lane; j < n; j += 32) s += A[row * n + j] * b[j];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    for (int64_t j = lane; j < n; j += 32) s += Ar[j] * b[o + j];
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
     if (!lane) x[row] = s;
   }
 }
@@ -296,8 +337,17 @@ struct Level {
 struct dg_damg {
   dg_damg_config cfg;
   std::vector<Level> lv;
-  DBuf<double> Ainv;  // dense inverse of the coarsest operator
+  DBuf<double> Ainv;  // dense inverses of the coarsest operator, one block per mesh
   int64_t nc = 0;
+  // block structure of the coarsest level (one block per independent mesh)
+  std::vector<int64_t> cb_off, cb_n, cb_aoff;
+  DBuf<int64_t> d_cb_off, d_cb_n, d_cb_aoff;
+  DBuf<uint32_t> d_crow_blk;
+  // batches: mesh offsets of elements / nodes on every level
+  int nmesh = 1;
+  std::vector<std::vector<int64_t>> mesh_elem_off, mesh_node_off;  // [level][mesh + 1]
+  DBuf<uint16_t> d_node_mesh;   // finest-level node -> mesh
+  DBuf<double> mesh_part;       // per-mesh squared norms
   // PCG work vectors on the finest level and device scalars
   DBuf<double> r, z, zold, p, q, part, scal;
   DBuf<float> r32, z32;
@@ -374,20 +424,46 @@ dg_status setup_level_f32(dg_damg* m, Level& L, cudaStream_t s) {
   return DG_OK;
 }
 
+__global__ void fill_row_blk(uint32_t* __restrict__ rb, int64_t n0, int64_t n1, uint32_t b) {
+  for (int64_t i = n0 + gtid(); i < n1; i += gstride()) rb[i] = b;
+}
+
 dg_status setup_coarse(dg_damg* m) {
   Level& L = m->lv.back();
-  const int64_t n = L.da->N;
-  DG_CHECK(n <= 16384, DG_EINVAL, "coarsest level too large for the dense direct solve (> 16384 nodes)");
-  m->nc = n;
-  DG_TRY(m->Ainv.alloc(n * n));
-  DG_TRY(lapmass_assemble_dense(L.A.get(), m->Ainv.p, m->s));
+  const int64_t N = L.da->N;
+  const std::vector<int64_t>& noff = m->mesh_node_off.back();
+  const int nb = int(noff.size()) - 1;
+  m->cb_off.assign(noff.begin(), noff.end() - 1);
+  m->cb_n.resize(nb);
+  m->cb_aoff.resize(nb);
+  int64_t total = 0, maxn = 0;
+  for (int b = 0; b < nb; ++b) {
+    m->cb_n[b] = noff[b + 1] - noff[b];
+    DG_CHECK(m->cb_n[b] <= 16384, DG_EINVAL, "coarsest level too large for the dense direct solve (> 16384 nodes)");
+    m->cb_aoff[b] = total;
+    total += m->cb_n[b] * m->cb_n[b];
+    maxn = m->cb_n[b] > maxn ? m->cb_n[b] : maxn;
+  }
+  m->nc = N;
+  DG_TRY(m->Ainv.alloc(total));
+  DG_TRY(m->d_cb_off.alloc(nb));
+  DG_TRY(m->d_cb_n.alloc(nb));
+  DG_TRY(m->d_cb_aoff.alloc(nb));
+  DG_TRY(m->d_crow_blk.alloc(N));
+  DG_CUDA(cudaMemcpyAsync(m->d_cb_off.p, m->cb_off.data(), 8 * nb, cudaMemcpyHostToDevice, m->s));
+  DG_CUDA(cudaMemcpyAsync(m->d_cb_n.p, m->cb_n.data(), 8 * nb, cudaMemcpyHostToDevice, m->s));
+  DG_CUDA(cudaMemcpyAsync(m->d_cb_aoff.p, m->cb_aoff.data(), 8 * nb, cudaMemcpyHostToDevice, m->s));
+  for (int b = 0; b < nb; ++b)
+    fill_row_blk<<<grid_for(m->cb_n[b], 256), 256, 0, m->s>>>(m->d_crow_blk.p, noff[b], noff[b + 1], uint32_t(b));
+  DG_TRY(lapmass_assemble_dense(L.A.get(), m->Ainv.p, total, m->d_crow_blk.p, m->d_cb_off.p, m->d_cb_n.p,
+                                m->d_cb_aoff.p, m->s));
   DBuf<double> colk;
-  DG_TRY(colk.alloc(n));
-  const unsigned g1 = grid_for(n, 256), g2 = grid_for(n * n, 256);
-  for (int64_t k = 0; k < n; ++k) {
-    gj_col<<<g1, 256, 0, m->s>>>(m->Ainv.p, n, k, colk.p);
-    gj_row<<<g1, 256, 0, m->s>>>(m->Ainv.p, n, k, colk.p);
-    gj_elim<<<g2, 256, 0, m->s>>>(m->Ainv.p, n, k, colk.p);
+  DG_TRY(colk.alloc(N));
+  const dim3 g1(grid_for(maxn, 256), unsigned(nb)), g2(grid_for(maxn * maxn, 256), unsigned(nb));
+  for (int64_t k = 0; k < maxn; ++k) {
+    gj_col<<<g1, 256, 0, m->s>>>(m->Ainv.p, m->d_cb_n.p, m->d_cb_aoff.p, k, colk.p, m->d_cb_off.p);
+    gj_row<<<g1, 256, 0, m->s>>>(m->Ainv.p, m->d_cb_n.p, m->d_cb_aoff.p, k, colk.p, m->d_cb_off.p);
+    gj_elim<<<g2, 256, 0, m->s>>>(m->Ainv.p, m->d_cb_n.p, m->d_cb_aoff.p, k, colk.p, m->d_cb_off.p);
   }
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaStreamSynchronize(m->s));
@@ -418,8 +494,15 @@ dg_status set_operators(dg_damg* m, const double* coef) {
         DBuf<uint32_t> err;
         DG_TRY(err.alloc(1));
         DG_CUDA(cudaMemsetAsync(err.p, 0, 4, s));
-        coarse_coef_kernel<<<grid_for(L.da->E, 256), 256, 0, s>>>(F.da->ekey.p, F.da->E, F.A->coef.p, L.da->ekey.p,
-                                                                   L.da->E, A->coef.p, err.p);
+        // per mesh: element keys are sorted within each mesh's segment
+        const std::vector<int64_t>& fo = m->mesh_elem_off[l - 1];
+        const std::vector<int64_t>& co = m->mesh_elem_off[l];
+        for (int i = 0; i < m->nmesh; ++i) {
+          const int64_t ef = fo[i + 1] - fo[i], ec = co[i + 1] - co[i];
+          coarse_coef_kernel<<<grid_for(ec, 256), 256, 0, s>>>(
+              F.da->ekey.p + fo[i], ef, F.A->coef.p + fo[i], F.A->coef.p + F.da->E + fo[i], L.da->ekey.p + co[i],
+              ec, A->coef.p + co[i], A->coef.p + L.da->E + co[i], err.p);
+        }
         uint32_t herr = 0;
         DG_CUDA(cudaMemcpyAsync(&herr, err.p, 4, cudaMemcpyDeviceToHost, s));
         DG_CUDA(cudaStreamSynchronize(s));
@@ -446,7 +529,8 @@ dg_status vcycle(dg_damg* m, size_t l, const double* b, double* x) {
   const int64_t n = L.da->N;
   const unsigned g = grid_for(n, 256);
   if (l + 1 == m->lv.size()) {
-    dense_gemv<<<grid_for(n * 32, 256), 256, 0, s>>>(m->Ainv.p, n, b, x);
+    dense_gemv<<<grid_for(n * 32, 256), 256, 0, s>>>(m->Ainv.p, n, m->d_crow_blk.p, m->d_cb_off.p, m->d_cb_n.p,
+                                                     m->d_cb_aoff.p, b, x);
     DG_CUDA(cudaGetLastError());
     return DG_OK;
   }
@@ -484,7 +568,8 @@ dg_status vcycle32(dg_damg* m, size_t l, const float* b, float* x) {
   const unsigned g = grid_for(n, 256);
   if (l + 1 == m->lv.size()) {
     convert<float, double><<<g, 256, 0, s>>>(b, L.b.p, n);
-    dense_gemv<<<grid_for(n * 32, 256), 256, 0, s>>>(m->Ainv.p, n, L.b.p, L.x.p);
+    dense_gemv<<<grid_for(n * 32, 256), 256, 0, s>>>(m->Ainv.p, n, m->d_crow_blk.p, m->d_cb_off.p, m->d_cb_n.p,
+                                                     m->d_cb_aoff.p, L.b.p, L.x.p);
     convert<double, float><<<g, 256, 0, s>>>(L.x.p, x, n);
     DG_CUDA(cudaGetLastError());
     return DG_OK;
@@ -571,14 +656,13 @@ void dg_damg_default_config(dg_damg_config* c) {
   c->use_graph = 0;
 }
 
-dg_status dg_damg_create(const dg_octree* finest, const dg_damg_config* cfg, dg_damg** out) {
-  DG_CHECK(finest && out, DG_EINVAL, "damg_create: bad arguments");
-  auto m = std::make_unique<dg_damg>();
-  if (cfg) m->cfg = *cfg; else dg_damg_default_config(&m->cfg);
-  DG_CHECK(m->cfg.nlevels >= 1, DG_EINVAL, "damg_create: nlevels must be >= 1");
-  DG_CUDA(cudaStreamCreateWithFlags(&m->s, cudaStreamNonBlocking));
-  cudaStream_t s = m->s;
-  // level octrees: coarsen + balance (omg.C:1376-1420)
+}  // extern "C"
+
+namespace {
+
+// Level hierarchy of one mesh: coarsen + balance (omg.C:1376-1420), a mesh
+// and the prolongation per level.
+dg_status build_hierarchy(const dg_octree* finest, int nlevels, cudaStream_t s, std::vector<Level>& lv) {
   std::vector<std::unique_ptr<dg_octree>> trees;
   auto t0 = std::make_unique<dg_octree>();
   t0->max_depth = finest->max_depth;
@@ -587,8 +671,8 @@ dg_status dg_damg_create(const dg_octree* finest, const dg_damg_config* cfg, dg_
   DG_CUDA(cudaMemcpy(t0->keys.p, finest->keys.p, 8 * finest->n, cudaMemcpyDeviceToDevice));
   trees.push_back(std::move(t0));
   int idx = -1;
-  bool repeat = m->cfg.nlevels > 1;
-  while (idx < m->cfg.nlevels - 2 && repeat) {
+  bool repeat = nlevels > 1;
+  while (idx < nlevels - 2 && repeat) {
     dg_octree tmp;
     DG_TRY(coarsen_octree(trees.back().get(), &tmp, s));
     auto c = std::make_unique<dg_octree>();
@@ -597,13 +681,17 @@ dg_status dg_damg_create(const dg_octree* finest, const dg_damg_config* cfg, dg_
     if (c->n < 500) repeat = false;
     trees.push_back(std::move(c));
   }
-  m->lv.resize(trees.size());
+  lv.resize(trees.size());
   for (size_t l = 0; l < trees.size(); ++l) {
-    m->lv[l].tree = std::move(trees[l]);
-    m->lv[l].da = std::make_unique<dg_da>();
-    DG_TRY(build_mesh(m->lv[l].tree.get(), m->lv[l].da.get(), s));
+    lv[l].tree = std::move(trees[l]);
+    lv[l].da = std::make_unique<dg_da>();
+    DG_TRY(build_mesh(lv[l].tree.get(), lv[l].da.get(), s));
   }
-  for (size_t l = 0; l + 1 < m->lv.size(); ++l) DG_TRY(build_prolongation(m->lv[l], m->lv[l + 1], s));
+  for (size_t l = 0; l + 1 < lv.size(); ++l) DG_TRY(build_prolongation(lv[l], lv[l + 1], s));
+  return DG_OK;
+}
+
+dg_status finish_create(dg_damg* m) {
   const int64_t N = m->lv[0].da->N;
   DG_TRY(m->r.alloc(N));
   DG_TRY(m->z.alloc(N));
@@ -616,8 +704,148 @@ dg_status dg_damg_create(const dg_octree* finest, const dg_damg_config* cfg, dg_
   }
   DG_TRY(m->part.alloc(kRedBlocks));
   DG_TRY(m->scal.alloc(8));
-  DG_TRY(set_operators(m.get(), nullptr));
+  DG_TRY(m->d_node_mesh.alloc(N));
+  DG_TRY(m->mesh_part.alloc(m->nmesh));
+  const std::vector<int64_t>& no = m->mesh_node_off[0];
+  for (int i = 0; i < m->nmesh; ++i)
+    fill_u16<<<grid_for(no[i + 1] - no[i], 256), 256, 0, m->s>>>(m->d_node_mesh.p, no[i], no[i + 1], uint16_t(i));
+  DG_CUDA(cudaGetLastError());
+  return set_operators(m, nullptr);
+}
+
+// Concatenate per-mesh meshes of one level into one mesh (node ids offset).
+dg_status concat_das(const std::vector<dg_da*>& in, dg_da* out, cudaStream_t s) {
+  out->D = in[0]->D;
+  int64_t E = 0, N = 0, P = 0;
+  for (dg_da* d : in) {
+    DG_CHECK(d->D == out->D, DG_EINVAL, "batched meshes must share maxDepth");
+    E += d->E;
+    N += d->N;
+    P += d->P;
+  }
+  DG_CHECK(N < (int64_t(1) << 32), DG_EINVAL, "batch too large for 32-bit node ids");
+  out->E = E;
+  out->N = N;
+  out->P = P;
+  DG_TRY(out->nl.alloc(8 * E));
+  DG_TRY(out->meta.alloc(E));
+  DG_TRY(out->ekey.alloc(E));
+  DG_TRY(out->nkey.alloc(N));
+  int64_t eo = 0, no = 0;
+  for (dg_da* d : in) {
+    for (int v = 0; v < 8; ++v)
+      copy_add_u32<<<grid_for(d->E, 256), 256, 0, s>>>(out->nl.p + int64_t(v) * E + eo, d->nl.p + int64_t(v) * d->E,
+                                                        d->E, uint32_t(no));
+    DG_CUDA(cudaMemcpyAsync(out->meta.p + eo, d->meta.p, 4 * d->E, cudaMemcpyDeviceToDevice, s));
+    DG_CUDA(cudaMemcpyAsync(out->ekey.p + eo, d->ekey.p, 8 * d->E, cudaMemcpyDeviceToDevice, s));
+    DG_CUDA(cudaMemcpyAsync(out->nkey.p + no, d->nkey.p, 8 * d->N, cudaMemcpyDeviceToDevice, s));
+    eo += d->E;
+    no += d->N;
+  }
+  DG_CUDA(cudaGetLastError());
+  return build_tiles(out, s);
+}
+
+// Concatenate per-mesh prolongations (block diagonal).
+dg_status concat_prolong(const std::vector<Level*>& fine, const std::vector<int64_t>& coarse_node_off, Level& out,
+                         cudaStream_t s) {
+  int64_t rows = 0, nnz = 0;
+  for (Level* f : fine) {
+    rows += f->da->N;
+    nnz += f->pval.n;
+  }
+  DG_TRY(out.pptr.alloc(rows + 1));
+  DG_TRY(out.pcol.alloc(nnz > 0 ? nnz : 1));
+  DG_TRY(out.pval.alloc(nnz > 0 ? nnz : 1));
+  int64_t ro = 0, zo = 0;
+  for (size_t i = 0; i < fine.size(); ++i) {
+    Level* f = fine[i];
+    const int64_t r = f->da->N, z = f->pval.n;
+    copy_add_u32<<<grid_for(r + 1, 256), 256, 0, s>>>(out.pptr.p + ro, f->pptr.p, r + 1, uint32_t(zo));
+    if (z) {
+      copy_add_u32<<<grid_for(z, 256), 256, 0, s>>>(out.pcol.p + zo, f->pcol.p, z, uint32_t(coarse_node_off[i]));
+      DG_CUDA(cudaMemcpyAsync(out.pval.p + zo, f->pval.p, 8 * z, cudaMemcpyDeviceToDevice, s));
+    }
+    ro += r;
+    zo += z;
+  }
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+dg_status dg_damg_create(const dg_octree* finest, const dg_damg_config* cfg, dg_damg** out) {
+  DG_CHECK(finest && out, DG_EINVAL, "damg_create: bad arguments");
+  return dg_damg_create_batch(&finest, 1, cfg, out);
+}
+
+dg_status dg_damg_create_batch(const dg_octree* const* finest, int count, const dg_damg_config* cfg, dg_damg** out) {
+  DG_CHECK(finest && out && count >= 1 && count <= 65535, DG_EINVAL, "damg_create_batch: bad arguments");
+  auto m = std::make_unique<dg_damg>();
+  if (cfg) m->cfg = *cfg; else dg_damg_default_config(&m->cfg);
+  DG_CHECK(m->cfg.nlevels >= 1, DG_EINVAL, "damg_create: nlevels must be >= 1");
+  DG_CUDA(cudaStreamCreateWithFlags(&m->s, cudaStreamNonBlocking));
+  cudaStream_t s = m->s;
+  m->nmesh = count;
+  if (count == 1) {
+    DG_TRY(build_hierarchy(finest[0], m->cfg.nlevels, s, m->lv));
+    for (Level& L : m->lv) {
+      m->mesh_elem_off.push_back({0, L.da->E});
+      m->mesh_node_off.push_back({0, L.da->N});
+    }
+  } else {
+    // every mesh gets the same number of levels: the smallest natural count
+    std::vector<std::vector<Level>> per(count);
+    size_t L = size_t(-1);
+    for (int i = 0; i < count; ++i) {
+      DG_CHECK(finest[i], DG_EINVAL, "damg_create_batch: null octree");
+      DG_TRY(build_hierarchy(finest[i], m->cfg.nlevels, s, per[i]));
+      L = per[i].size() < L ? per[i].size() : L;
+    }
+    for (int i = 0; i < count; ++i) {
+      per[i].resize(L);
+      Level& last = per[i].back();  // no transfer below the common coarsest level
+      last.pptr.reset();
+      last.pcol.reset();
+      last.pval.reset();
+    }
+    m->lv.resize(L);
+    for (size_t l = 0; l < L; ++l) {
+      std::vector<dg_da*> das;
+      std::vector<int64_t> eo{0}, no{0};
+      for (int i = 0; i < count; ++i) {
+        das.push_back(per[i][l].da.get());
+        eo.push_back(eo.back() + per[i][l].da->E);
+        no.push_back(no.back() + per[i][l].da->N);
+      }
+      m->lv[l].da = std::make_unique<dg_da>();
+      DG_TRY(concat_das(das, m->lv[l].da.get(), s));
+      m->mesh_elem_off.push_back(eo);
+      m->mesh_node_off.push_back(no);
+    }
+    for (size_t l = 0; l + 1 < L; ++l) {
+      std::vector<Level*> fine;
+      for (int i = 0; i < count; ++i) fine.push_back(&per[i][l]);
+      DG_TRY(concat_prolong(fine, m->mesh_node_off[l + 1], m->lv[l], s));
+    }
+    DG_CUDA(cudaStreamSynchronize(s));
+  }
+  DG_TRY(finish_create(m.get()));
   *out = m.release();
+  return DG_OK;
+}
+
+int dg_damg_batch_count(const dg_damg* m) { return m ? m->nmesh : 0; }
+
+dg_status dg_damg_batch_offsets(const dg_damg* m, int level, int64_t* elem_off, int64_t* node_off) {
+  DG_CHECK(m && level >= 0 && level < int(m->lv.size()), DG_EINVAL, "damg_batch_offsets: bad level");
+  for (int i = 0; i <= m->nmesh; ++i) {
+    if (elem_off) elem_off[i] = m->mesh_elem_off[level][i];
+    if (node_off) node_off[i] = m->mesh_node_off[level][i];
+  }
   return DG_OK;
 }
 
@@ -722,6 +950,18 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
   DG_CUDA(cudaMemcpyAsync(&hb, sc + 0, 8, cudaMemcpyDeviceToHost, s));
   DG_CUDA(cudaStreamSynchronize(s));
   const double bnorm = std::sqrt(hb);
+  // independent meshes: each must reach the tolerance on its own ||b_i||
+  const int nm = m->nmesh;
+  std::vector<double> bb(nm, hb), rr(nm);
+  auto mesh_norms = [&](const double* v, std::vector<double>& out) -> dg_status {
+    DG_CUDA(cudaMemsetAsync(m->mesh_part.p, 0, 8 * nm, s));
+    seg_sqnorm<<<kRedBlocks, 256, 8 * nm, s>>>(v, n, m->d_node_mesh.p, nm, m->mesh_part.p);
+    DG_CUDA(cudaGetLastError());
+    DG_CUDA(cudaMemcpyAsync(out.data(), m->mesh_part.p, 8 * nm, cudaMemcpyDeviceToHost, s));
+    DG_CUDA(cudaStreamSynchronize(s));
+    return DG_OK;
+  };
+  if (nm > 1) DG_TRY(mesh_norms(pb, bb));
   int it = 0;
   double rel = bnorm > 0 ? 1.0 : 0.0;
   bool conv = bnorm == 0;
@@ -735,10 +975,17 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
       DG_TRY(dot(m, m->p.p, m->q.p, n, sc + 2));
       cg_update<<<kRedBlocks, 256, 0, s>>>(px, m->r.p, m->p.p, m->q.p, n, sc + 1, sc + 2, m->part.p);
       finish_sum<<<1, 256, 0, s>>>(m->part.p, kRedBlocks, sc + 3);
-      double hr = 0;
-      DG_CUDA(cudaMemcpyAsync(&hr, sc + 3, 8, cudaMemcpyDeviceToHost, s));
-      DG_CUDA(cudaStreamSynchronize(s));
-      rel = std::sqrt(hr) / bnorm;
+      if (nm > 1) {
+        DG_TRY(mesh_norms(m->r.p, rr));
+        rel = 0;
+        for (int i = 0; i < nm; ++i)
+          if (bb[i] > 0) rel = std::max(rel, std::sqrt(rr[i] / bb[i]));
+      } else {
+        double hr = 0;
+        DG_CUDA(cudaMemcpyAsync(&hr, sc + 3, 8, cudaMemcpyDeviceToHost, s));
+        DG_CUDA(cudaStreamSynchronize(s));
+        rel = std::sqrt(hr) / bnorm;
+      }
       if (!(rel == rel)) break;  // NaN: stop and report
       if (rel <= m->cfg.rtol) {
         conv = true;

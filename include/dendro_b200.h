@@ -173,6 +173,19 @@ void dg_damg_default_config(dg_damg_config* cfg);
  * hierarchy by coarsenOctree + balanceOctree, a mesh per level, and the
  * transfer operators of createInterpolationType1 (omg.C:2234-2290). */
 dg_status dg_damg_create(const dg_octree* finest_balanced, const dg_damg_config* cfg, dg_damg** out);
+/* Many independent meshes as one hierarchy (the batched form): every mesh gets
+ * the same number of levels (the smallest natural count over the meshes),
+ * level l of all meshes is concatenated into one mesh with per-mesh node-id
+ * offsets, transfers are block diagonal and the coarsest level is solved with
+ * one dense block per mesh.  One kernel launch then serves all meshes; the
+ * solve stops when every mesh reaches rtol on its own ||b_i||.  Vectors and
+ * coefficients are the per-mesh arrays concatenated in mesh order. */
+dg_status dg_damg_create_batch(const dg_octree* const* finest_balanced, int count, const dg_damg_config* cfg,
+                               dg_damg** out);
+int dg_damg_batch_count(const dg_damg* m);
+/* Element and node offsets of each mesh on a level (count + 1 entries each). */
+dg_status dg_damg_batch_offsets(const dg_damg* m, int level, int64_t* elem_off, int64_t* node_off);
+
 /* DAMGSetKSP with CreateJacobian2 (omg.h:488; omgNeumann.C:643): finest-level
  * coefficients (host, 2 per element or NULL), coarse levels averaged as
  * SetPDECoefFromPts (omgNeumann.C:73-113,188-297). */

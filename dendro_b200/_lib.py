@@ -92,6 +92,7 @@ def lib():
         "dg_damg_create_batch": ([P, I, C.POINTER(DamgConfig), PP], I),
         "dg_damg_batch_count": ([P], I),
         "dg_damg_batch_offsets": ([P, I, P, P], I),
+        "dg_vec_dot_noalloc": ([P, P, I64, P, P], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -113,6 +114,7 @@ def exported_symbols():
         "dg_damg_set_lapmass", "dg_damg_solve", "dg_damg_levels", "dg_damg_level_sizes", "dg_damg_level_da",
         "dg_damg_prolong", "dg_damg_restrict", "dg_damg_destroy", "dg_vec_dot",
         "dg_damg_create_batch", "dg_damg_batch_count", "dg_damg_batch_offsets",
+        "dg_vec_dot_noalloc",
     ]
 
 

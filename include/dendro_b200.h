@@ -209,6 +209,21 @@ void dg_damg_destroy(dg_damg* m);
  * pointers; the call synchronises the stream before returning. */
 dg_status dg_vec_dot(const double* x, const double* y, int64_t n, double* result, void* stream);
 
+/* The same inner product without any device allocation, for callers that
+ * cannot allocate: a convergence test or monitor run every iteration inside
+ * a solver whose device memory belongs to another allocator (a caching pool
+ * that already holds the free HBM, or a process under an MPS memory cap), or
+ * a loop that cannot take the device-wide synchronisation of cudaMalloc /
+ * cudaFree.  It has no counterpart in the reference.  Limit: n <= 268435456.
+ * The partial sums live in a fixed 512 KiB array inside the library's device
+ * memory, held by every GPU that loads the library until the process exits.
+ * The first call on each device looks up that array's address (with the
+ * device current), so make that first call before any stream capture.  The
+ * result is written asynchronously on `stream` (no synchronisation).  All
+ * calls share the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race on it and must be serialised by the caller. */
+dg_status dg_vec_dot_noalloc(const double* x, const double* y, int64_t n, double* result, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -189,7 +189,8 @@ def run_dendro(args, rank, world):
         solve["chosen"]["method"] = ("FP64 flexible CG + FP32 V(2,2) (FP32 operator, smoother, transfers), "
                                      "FP64 coarse solve, V-cycle replayed from a CUDA graph")
         solve["speedup_chosen_vs_plain"] = round(solve["plain_fp64"]["ms_to_1e-8"] / solve["chosen"]["ms_to_1e-8"], 3)
-    return dict(E=E, N=N, setup_s=setup_s, ms_per_step=ms_per_step, gdofs=gdofs, achieved=achieved, peak=peak,
+    kernel = A.kernel_name(0)
+    return dict(kernel=kernel, E=E, N=N, setup_s=setup_s, ms_per_step=ms_per_step, gdofs=gdofs, achieved=achieved, peak=peak,
                 peak_kind=peak_kind, alg_bytes=alg_bytes, clocks=clk, e2e=e2e, solve=solve, bal=bal, depth=depth,
                 coef=coef, x=x.cpu().numpy(), y=y.cpu().numpy())
 
@@ -239,7 +240,7 @@ def main():
         "gpu_launches": args.steps,
         "clocks": r["clocks"],
         "solve": r["solve"],
-        "matvec_kernel": os.environ.get("DG_MATVEC_KERNEL", "tiled"),
+        "matvec_kernel": r["kernel"],
         "setup_s": round(r["setup_s"], 3),
     }
     if rank == 0 and world == 1 and not args.no_cpu:

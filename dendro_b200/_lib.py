@@ -77,6 +77,7 @@ def lib():
         "dg_mat_get_diagonal": ([P, P, P], I),
         "dg_mat_mult_host": ([P, P, P], I),
         "dg_mat_size": ([P], I64),
+        "dg_mat_kernel_name": ([P, I], C.c_char_p),
         "dg_mat_destroy": ([P], None),
         "dg_damg_default_config": ([C.POINTER(DamgConfig)], None),
         "dg_damg_create": ([P, C.POINTER(DamgConfig), PP], I),
@@ -110,7 +111,7 @@ def exported_symbols():
         "dg_octree_destroy", "dg_da_create", "dg_da_create_from_maps", "dg_da_sizes", "dg_da_max_depth",
         "dg_da_export", "dg_da_element_centers", "dg_da_destroy", "dg_mat_create_lapmass",
         "dg_mat_create_elasticity", "dg_mat_mult", "dg_mat_mult_f32", "dg_mat_get_diagonal",
-        "dg_mat_mult_host", "dg_mat_size", "dg_mat_destroy", "dg_damg_default_config", "dg_damg_create",
+        "dg_mat_mult_host", "dg_mat_size", "dg_mat_kernel_name", "dg_mat_destroy", "dg_damg_default_config", "dg_damg_create",
         "dg_damg_set_lapmass", "dg_damg_solve", "dg_damg_levels", "dg_damg_level_sizes", "dg_damg_level_da",
         "dg_damg_prolong", "dg_damg_restrict", "dg_damg_destroy", "dg_vec_dot",
         "dg_damg_create_batch", "dg_damg_batch_count", "dg_damg_batch_offsets",

@@ -163,6 +163,10 @@ class _Mat:
         check(lib().dg_mat_mult_host(self.h, ptr(xa), ptr(ya)), "mat_mult_host")
         return ya
 
+    def kernel_name(self, prec: int = 0) -> str:
+        """Launch shape the autotuner chose for this mesh (after the first mult)."""
+        return lib().dg_mat_kernel_name(self.h, prec).decode()
+
     def getDiagonal(self, d=None, stream=None):
         import torch
         if d is None:

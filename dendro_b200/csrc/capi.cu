@@ -400,6 +400,11 @@ dg_status dg_mat_mult_host(dg_mat* A, const double* x, double* y) {
 
 int64_t dg_mat_size(const dg_mat* A) { return A ? int64_t(A->dof) * A->da->N : 0; }
 
+const char* dg_mat_kernel_name(const dg_mat* A, int prec) {
+  if (!A || A->kind != 0) return "elasticity";
+  return matvec_variant_name(prec == DG_PREC_F64 ? A->da->tuned_f64 : A->da->tuned_f32);
+}
+
 void dg_mat_destroy(dg_mat* A) { delete A; }
 
 }  // extern "C"

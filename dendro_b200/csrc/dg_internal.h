@@ -25,6 +25,8 @@ struct dg_da {
   dg::DBuf<uint32_t> tile_span;
   int64_t ntiles = 0;
   int tile_elems = 0;
+  // operator launch shape picked by the autotuner on first use (-1: not yet)
+  int tuned_f64 = -1, tuned_f32 = -1;
   uint32_t max_span = 0;
 };
 
@@ -67,6 +69,7 @@ dg_status build_tiles(dg_da* da, cudaStream_t s);
 dg_status lapmass_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStream_t s);
 dg_status lapmass_diag(const dg_mat* A, double* d, cudaStream_t s);
+const char* matvec_variant_name(int v);
 dg_status elasticity_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status elasticity_diag(const dg_mat* A, double* d, cudaStream_t s);
 // Dense assembled operator of a small level as row-major blocks, one per

@@ -113,11 +113,13 @@ __device__ __forceinline__ void scatter_hanging(T (&r)[8], uint32_t c, uint32_t 
   for (int v = 0; v < 8; ++v) r[v] = rn[v];
 }
 
-// One thread per element: gather, apply, scatter with atomics.
-template <class T, class CT>
-__global__ void __launch_bounds__(256) lapmass_kernel(const uint32_t* __restrict__ nl, const uint32_t* __restrict__ meta,
-                                                      const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
-                                                      const T* __restrict__ x, T* __restrict__ y) {
+// One thread per element: gather, apply, scatter with atomics.  BLOCK and
+// MINB set the launch bounds (registers per thread) of each tuned variant.
+template <class T, class CT, int BLOCK = 256, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB) lapmass_kernel(const uint32_t* __restrict__ nl,
+                                                              const uint32_t* __restrict__ meta,
+                                                              const CT* __restrict__ ca, const CT* __restrict__ cb,
+                                                              int64_t E, const T* __restrict__ x, T* __restrict__ y) {
   for (int64_t e = gtid(); e < E; e += gstride()) {
     const uint32_t m = meta[e];
     const uint32_t lev = meta_lev(m), c = meta_cnum(m), mask = meta_mask(m);
@@ -261,41 +263,110 @@ __global__ void lapmass_dense_kernel(const uint32_t* __restrict__ nl, const uint
 
 }  // namespace
 
-static int matvec_variant() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = getenv("DG_MATVEC_KERNEL");
-    v = (e && !strcmp(e, "atomic")) ? 0 : 1;
-  }
-  return v;
-}
+// Launch shapes tried by the autotuner: one thread per element with
+// different block sizes / register caps / grid sizes, and the tiled
+// shared-memory form.  The first application on a mesh times each once
+// (after one untimed launch) and keeps the fastest for that mesh and
+// precision; DG_MATVEC_KERNEL=<index> forces one (testing).
+struct MatvecVariant {
+  int block, per_sm;  // threads per CTA, CTAs per SM in the grid (0: one thread per element)
+  int kind;           // 0 atomic (BLOCK, MINB), 1 tiled
+  int minb;
+  const char* name;
+};
+constexpr MatvecVariant kVariants[] = {
+    {256, 8, 0, 1, "atomic b256 grid 8/SM"},  {256, 0, 0, 1, "atomic b256 grid E"},
+    {256, 8, 0, 4, "atomic b256 minB4"},      {128, 16, 0, 8, "atomic b128 minB8"},
+    {512, 4, 0, 2, "atomic b512 minB2"},      {256, 0, 1, 1, "tiled 512 elems / 2048-node window"},
+};
+constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 
 template <class T, class CT>
-static dg_status lapmass_launch(const dg_da* da, const CT* ca, const CT* cb, const T* x, T* y, cudaStream_t s) {
-  DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
-  if (matvec_variant() == 1 && da->tile_elems == kTileElems && da->ntiles > 0) {
-    const unsigned g = unsigned(da->ntiles < int64_t(sm_count()) * 16 ? da->ntiles : int64_t(sm_count()) * 16);
-    lapmass_tiled_kernel<T, CT><<<g, kTileThreads, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E, da->N,
-                                                          da->tile_lo.p, da->ntiles, x, y);
+static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* cb, const T* x, T* y,
+                                cudaStream_t s) {
+  const MatvecVariant& V = kVariants[v];
+  const unsigned g = V.per_sm ? grid_for(da->E, V.block, V.per_sm)
+                              : unsigned((da->E + V.block - 1) / V.block > 0 ? (da->E + V.block - 1) / V.block : 1);
+  if (V.kind == 1) {
+    const unsigned gt = unsigned(da->ntiles < int64_t(sm_count()) * 16 ? da->ntiles : int64_t(sm_count()) * 16);
+    lapmass_tiled_kernel<T, CT><<<gt > 0 ? gt : 1, kTileThreads, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E, da->N,
+                                                                      da->tile_lo.p, da->ntiles, x, y);
+  } else if (V.block == 256 && V.minb == 1) {
+    lapmass_kernel<T, CT, 256, 1><<<g, 256, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E, x, y);
+  } else if (V.block == 256 && V.minb == 4) {
+    lapmass_kernel<T, CT, 256, 4><<<g, 256, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E, x, y);
+  } else if (V.block == 128) {
+    lapmass_kernel<T, CT, 128, 8><<<g, 128, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E, x, y);
   } else {
-    lapmass_kernel<T, CT><<<grid_for(da->E, 256, 8), 256, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E, x, y);
+    lapmass_kernel<T, CT, 512, 2><<<g, 512, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E, x, y);
   }
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }
 
+static int forced_variant() {
+  static int v = -2;
+  if (v == -2) {
+    const char* e = getenv("DG_MATVEC_KERNEL");
+    v = -1;
+    if (e && *e) {
+      if (!strcmp(e, "atomic")) v = 0;
+      else if (!strcmp(e, "tiled")) v = kNumVariants - 1;
+      else v = atoi(e) % kNumVariants;
+    }
+  }
+  return v;
+}
+
+template <class T, class CT>
+static dg_status lapmass_launch(const dg_da* da, int& choice, const CT* ca, const CT* cb, const T* x, T* y,
+                                cudaStream_t s) {
+  DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
+  if (forced_variant() >= 0) return launch_variant<T, CT>(forced_variant(), da, ca, cb, x, y, s);
+  if (choice < 0) {
+    // autotune: one untimed launch, then one timed launch per variant
+    cudaEvent_t e0, e1;
+    DG_CUDA(cudaEventCreate(&e0));
+    DG_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bi = 0;
+    DG_TRY((launch_variant<T, CT>(0, da, ca, cb, x, y, s)));
+    for (int v = 0; v < kNumVariants; ++v) {
+      if (kVariants[v].kind == 1 && da->ntiles == 0) continue;
+      DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
+      DG_CUDA(cudaEventRecord(e0, s));
+      DG_TRY((launch_variant<T, CT>(v, da, ca, cb, x, y, s)));
+      DG_CUDA(cudaEventRecord(e1, s));
+      DG_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      DG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best) {
+        best = ms;
+        bi = v;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    choice = bi;
+    DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
+  }
+  return launch_variant<T, CT>(choice, da, ca, cb, x, y, s);
+}
+
+const char* matvec_variant_name(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].name : "untuned"; }
+
 dg_status lapmass_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s) {
-  const dg_da* da = A->da;
+  dg_da* da = A->da;
   const double* ca = A->has_coef ? A->coef.p : nullptr;
   const double* cb = A->has_coef ? A->coef.p + da->E : nullptr;
-  return lapmass_launch<double, double>(da, ca, cb, x, y, s);
+  return lapmass_launch<double, double>(da, da->tuned_f64, ca, cb, x, y, s);
 }
 
 dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStream_t s) {
-  const dg_da* da = A->da;
+  dg_da* da = A->da;
   const float* ca = A->has_coef ? A->coef32.p : nullptr;
   const float* cb = A->has_coef ? A->coef32.p + da->E : nullptr;
-  return lapmass_launch<float, float>(da, ca, cb, x, y, s);
+  return lapmass_launch<float, float>(da, da->tuned_f32, ca, cb, x, y, s);
 }
 
 dg_status lapmass_diag(const dg_mat* A, double* d, cudaStream_t s) {

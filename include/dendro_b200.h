@@ -146,6 +146,9 @@ dg_status dg_mat_get_diagonal(dg_mat* A, double* d, void* stream);
  * synchronises (the call a PETSc MatShell callback makes on host Vec arrays). */
 dg_status dg_mat_mult_host(dg_mat* A, const double* x, double* y);
 int64_t dg_mat_size(const dg_mat* A); /* rows = dof * nodes */
+/* Launch shape of the scalar operator kernel that the autotuner picked on the
+ * first application in the given precision ("untuned" before it). */
+const char* dg_mat_kernel_name(const dg_mat* A, int prec);
 void dg_mat_destroy(dg_mat* A);
 
 /* ------------------------------------------------------------ multigrid --- */

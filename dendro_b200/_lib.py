@@ -28,7 +28,7 @@ class DendroError(RuntimeError):
 
 class SolveReport(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("rel_residual", C.c_double),
-                ("solve_ms", C.c_double)]
+                ("solve_ms", C.c_double), ("smoother_fallbacks", C.c_int)]
 
 
 class DamgConfig(C.Structure):
@@ -91,6 +91,17 @@ def lib():
         "dg_damg_destroy": ([P], None),
         "dg_vec_dot": ([P, P, I64, P, P], I),
         "dg_damg_create_batch": ([P, I, C.POINTER(DamgConfig), PP], I),
+        "dg_damg_vcycle": ([P, P, P], I),
+        "dg_mlp_param_count": ([], I),
+        "dg_mlp_create": ([P, PP], I),
+        "dg_mlp_get_params": ([P, P], I),
+        "dg_mlp_set_params": ([P, P], I),
+        "dg_mlp_forward": ([P, P, I64, P, I, P], I),
+        "dg_mlp_gradient": ([P, P, P, I64, I, P, C.POINTER(C.c_double)], I),
+        "dg_mlp_train_step": ([P, P, P, I64, C.c_float, C.POINTER(C.c_double)], I),
+        "dg_mlp_destroy": ([P], None),
+        "dg_damg_set_smoother": ([P, P, I, C.c_double], I),
+        "dg_damg_features": ([P, P, P, C.POINTER(C.c_float)], I),
         "dg_damg_batch_count": ([P], I),
         "dg_damg_batch_offsets": ([P, I, P, P], I),
         "dg_vec_dot_noalloc": ([P, P, I64, P, P], I),
@@ -114,7 +125,9 @@ def exported_symbols():
         "dg_mat_mult_host", "dg_mat_size", "dg_mat_kernel_name", "dg_mat_destroy", "dg_damg_default_config", "dg_damg_create",
         "dg_damg_set_lapmass", "dg_damg_solve", "dg_damg_levels", "dg_damg_level_sizes", "dg_damg_level_da",
         "dg_damg_prolong", "dg_damg_restrict", "dg_damg_destroy", "dg_vec_dot",
-        "dg_damg_create_batch", "dg_damg_batch_count", "dg_damg_batch_offsets",
+        "dg_damg_create_batch", "dg_damg_batch_count", "dg_damg_batch_offsets", "dg_damg_vcycle",
+        "dg_mlp_param_count", "dg_mlp_create", "dg_mlp_get_params", "dg_mlp_set_params", "dg_mlp_forward",
+        "dg_mlp_gradient", "dg_mlp_train_step", "dg_mlp_destroy", "dg_damg_set_smoother", "dg_damg_features",
         "dg_vec_dot_noalloc",
     ]
 

@@ -260,7 +260,14 @@ class DAMG:
         if not (allow_unconverged and st == 4):
             check(st, "damg_solve")
         return x, dict(iterations=rep.iterations, converged=bool(rep.converged), rel_residual=rep.rel_residual,
-                       solve_ms=rep.solve_ms)
+                       solve_ms=rep.solve_ms, smoother_fallbacks=rep.smoother_fallbacks)
+
+    def setSmoother(self, mlp=None, sweeps: int = 2, fallback_ratio: float = 0.7):
+        """Finest-level post-smoother: a learned MLP (dendro_b200.learned.MLP)
+        or None for damped Jacobi; needs the FP32 inner V-cycle (inner_prec=1)."""
+        self._mlp = mlp  # keep the network alive while the hierarchy uses it
+        check(lib().dg_damg_set_smoother(self.h, None if mlp is None else mlp.h, sweeps, fallback_ratio),
+              "damg_set_smoother")
 
     def prolong(self, level: int, xc: np.ndarray, xf: np.ndarray) -> np.ndarray:
         xc = np.ascontiguousarray(xc, np.float64)

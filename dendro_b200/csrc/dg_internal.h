@@ -30,6 +30,11 @@ struct dg_da {
   uint32_t max_span = 0;
 };
 
+struct dg_mlp {
+  dg::DBuf<float> params, grad, m1, m2, loss;
+  int step = 0;
+};
+
 struct dg_mat {
   dg_da* da = nullptr;
   int kind = 0;  // 0 lap+mass, 1 elasticity
@@ -44,7 +49,23 @@ struct dg_mat {
 
 namespace dg {
 
+// ---- learned smoother (mlp.cu): 6 -> 64 -> 64 -> 1, packed FP32 parameters ----
+constexpr int kMlpIn = 6;
+constexpr int kMlpHidden = 64;
+constexpr int kOffW1 = 0;
+constexpr int kOffB1 = kOffW1 + kMlpHidden * kMlpIn;
+constexpr int kOffW2 = kOffB1 + kMlpHidden;
+constexpr int kOffB2 = kOffW2 + kMlpHidden * kMlpHidden;
+constexpr int kOffW3 = kOffB2 + kMlpHidden;
+constexpr int kOffB3 = kOffW3 + kMlpHidden;
+constexpr int kMlpParams = kOffB3 + 1;
+dg_status mlp_forward(const float* params, const float* F, int64_t n, float* out, bool exact, cudaStream_t s);
+dg_status mlp_gradient(const float* params, const float* F, const float* T, int64_t n, float* grad, float* loss_acc,
+                       bool exact, cudaStream_t s);
+dg_status mlp_adam(float* p, const float* g, float* m1, float* m2, int step, float lr, cudaStream_t s);
+
 // ---- primitives (prim.cu) ----
+
 // Device-wide exclusive scan of n uint32 values into out (out may alias in);
 // returns the total through *total (host) when not null.
 dg_status scan_u32(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, cudaStream_t s);

@@ -21,6 +21,14 @@
 namespace dg {
 dg_status node_boundary_flags(const dg_da* da, uint8_t* d_out, cudaStream_t s);
 dg_status convert_f64_to_f32(const double* a, float* b, int64_t n, cudaStream_t s);
+dg_status smoother_node_data(const dg_da* da, const float* dinv32, float* refs, float* hang, float* dlogbar,
+                             cudaStream_t s);
+dg_status mlp_smooth_step(const float* params, const dg_da* da, const float* r, float* s2, const float* dinv32,
+                          float dlogbar, float level_feat, const float* hang, const float* inv_refs, float* nsum,
+                          float* nmax, float* x, cudaStream_t s);
+dg_status mlp_features_f64(const dg_da* da, const double* r, float* s2, const float* dinv32, float dlogbar,
+                           float level_feat, const float* hang, const float* inv_refs, float* nsum, float* nmax,
+                           float* F, float* scale_out, cudaStream_t s);
 }  // namespace dg
 
 using namespace dg;
@@ -199,6 +207,10 @@ __global__ void jacobi_update(T* __restrict__ x, const T* __restrict__ b, const 
                               const T* __restrict__ dinv, T omega, int64_t n) {
   for (int64_t i = gtid(); i < n; i += gstride()) x[i] += omega * dinv[i] * (b[i] - t[i]);
 }
+template <class T>
+__global__ void residual_kernel(const T* __restrict__ b, const T* __restrict__ t, T* __restrict__ r, int64_t n) {
+  for (int64_t i = gtid(); i < n; i += gstride()) r[i] = b[i] - t[i];
+}
 template <class A, class B>
 __global__ void convert(const A* __restrict__ a, B* __restrict__ b, int64_t n) {
   for (int64_t i = gtid(); i < n; i += gstride()) b[i] = B(a[i]);
@@ -332,6 +344,10 @@ struct Level {
   DBuf<double> pval;
   // FP32 inner V-cycle
   DBuf<float> dinv32, x32, b32, t32, pval32;
+  // learned smoother data (finest level): residual, neighbour stats,
+  // 1 / element references, hanging share, mean log2 diagonal
+  DBuf<float> sm_r, sm_nsum, sm_nmax, sm_refs, sm_hang;
+  float sm_dlogbar = 0.f;
 };
 
 struct dg_damg {
@@ -348,6 +364,12 @@ struct dg_damg {
   std::vector<std::vector<int64_t>> mesh_elem_off, mesh_node_off;  // [level][mesh + 1]
   DBuf<uint16_t> d_node_mesh;   // finest-level node -> mesh
   DBuf<double> mesh_part;       // per-mesh squared norms
+  // learned post-smoother on the finest level (FP32 inner V-cycle only)
+  dg_mlp* mlp = nullptr;
+  int mlp_sweeps = 2;
+  double mlp_fallback = 0.7;
+  bool mlp_active = false;
+  DBuf<float> sm_s2;
   // PCG work vectors on the finest level and device scalars
   DBuf<double> r, z, zold, p, q, part, scal;
   DBuf<float> r32, z32;
@@ -591,9 +613,19 @@ dg_status vcycle32(dg_damg* m, size_t l, const float* b, float* x) {
                                       m->cfg.nu_pre > 0 ? (const float*)L.t32.p : (const float*)nullptr, C.b32.p);
   DG_TRY(vcycle32(m, l + 1, C.b32.p, C.x32.p));
   prolong_add<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval32.p, n, C.x32.p, x);
-  for (int k = 0; k < m->cfg.nu_post; ++k) {
-    DG_TRY(lapmass_apply_f32(L.A.get(), x, L.t32.p, s));
-    jacobi_update<<<g, 256, 0, s>>>(x, b, L.t32.p, L.dinv32.p, w, n);
+  if (l == 0 && m->mlp && m->mlp_active) {
+    const float level_feat = 0.f;  // finest level
+    for (int k = 0; k < m->mlp_sweeps; ++k) {
+      DG_TRY(lapmass_apply_f32(L.A.get(), x, L.t32.p, s));
+      residual_kernel<<<g, 256, 0, s>>>(b, (const float*)L.t32.p, L.sm_r.p, n);
+      DG_TRY(mlp_smooth_step(m->mlp->params.p, L.da.get(), L.sm_r.p, m->sm_s2.p, L.dinv32.p, L.sm_dlogbar,
+                             level_feat, L.sm_hang.p, L.sm_refs.p, L.sm_nsum.p, L.sm_nmax.p, x, s));
+    }
+  } else {
+    for (int k = 0; k < m->cfg.nu_post; ++k) {
+      DG_TRY(lapmass_apply_f32(L.A.get(), x, L.t32.p, s));
+      jacobi_update<<<g, 256, 0, s>>>(x, b, L.t32.p, L.dinv32.p, w, n);
+    }
   }
   DG_CUDA(cudaGetLastError());
   return DG_OK;
@@ -617,6 +649,9 @@ dg_status precond_body(dg_damg* m) {
 dg_status precond(dg_damg* m) {
   if (!m->cfg.use_graph) return precond_body(m);
   if (!m->precond_graph) {
+    // one plain application first: operator autotuning and lazy set-up
+    // happen outside the capture
+    DG_TRY(precond_body(m));
     cudaGraph_t graph = nullptr;
     DG_CUDA(cudaStreamBeginCapture(m->s, cudaStreamCaptureModeThreadLocal));
     dg_status st = precond_body(m);
@@ -631,6 +666,28 @@ dg_status precond(dg_damg* m) {
     DG_CUDA(e);
   }
   DG_CUDA(cudaGraphLaunch(m->precond_graph, m->s));
+  return DG_OK;
+}
+
+// Finest-level node data of the learned smoother (allocated on first use).
+dg_status ensure_smoother_data(dg_damg* m) {
+  Level& L = m->lv[0];
+  if (L.sm_r.n == L.da->N && L.sm_refs.n == L.da->N) return DG_OK;
+  const int64_t N = L.da->N;
+  DG_TRY(L.sm_r.alloc(N));
+  DG_TRY(L.sm_nsum.alloc(N));
+  DG_TRY(L.sm_nmax.alloc(N));
+  DG_TRY(L.sm_refs.alloc(N));
+  DG_TRY(L.sm_hang.alloc(N));
+  DG_TRY(m->sm_s2.alloc(1));
+  DBuf<float> d32;
+  const float* dinv32 = L.dinv32.p;
+  if (!dinv32) {
+    DG_TRY(d32.alloc(N));
+    convert<double, float><<<grid_for(N, 256), 256, 0, m->s>>>(L.dinv.p, d32.p, N);
+    dinv32 = d32.p;
+  }
+  DG_TRY(smoother_node_data(L.da.get(), dinv32, L.sm_refs.p, L.sm_hang.p, &L.sm_dlogbar, m->s));
   return DG_OK;
 }
 
@@ -966,6 +1023,15 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
   double rel = bnorm > 0 ? 1.0 : 0.0;
   bool conv = bnorm == 0;
   const bool flexible = m->cfg.inner_prec != DG_PREC_F64;
+  int fallbacks = 0;
+  double prev_rel = 1.0;
+  if (m->mlp && !m->mlp_active) {  // a new solve starts with the learned smoother again
+    m->mlp_active = true;
+    if (m->precond_graph) {
+      cudaGraphExecDestroy(m->precond_graph);
+      m->precond_graph = nullptr;
+    }
+  }
   if (!conv) {
     DG_TRY(precond(m));
     DG_CUDA(cudaMemcpyAsync(m->p.p, m->z.p, 8 * n, cudaMemcpyDeviceToDevice, s));
@@ -991,6 +1057,17 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
         conv = true;
         break;
       }
+      // the FP64 residual judges the learned smoother: when it fails to fall
+      // by the set factor, plain damped Jacobi takes over for this solve
+      if (m->mlp && m->mlp_active && rel > m->mlp_fallback * prev_rel) {
+        m->mlp_active = false;
+        ++fallbacks;
+        if (m->precond_graph) {
+          cudaGraphExecDestroy(m->precond_graph);
+          m->precond_graph = nullptr;
+        }
+      }
+      prev_rel = rel;
       if (flexible) DG_CUDA(cudaMemcpyAsync(m->zold.p, m->z.p, 8 * n, cudaMemcpyDeviceToDevice, s));
       DG_TRY(precond(m));
       DG_TRY(dot(m, m->r.p, m->z.p, n, sc + 4));
@@ -1015,6 +1092,7 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
     rep->converged = conv ? 1 : 0;
     rep->rel_residual = rel;
     rep->solve_ms = ms;
+    rep->smoother_fallbacks = fallbacks;
   }
   return conv ? DG_OK : DG_ENOTCONVERGED;
 }
@@ -1031,6 +1109,55 @@ dg_status dg_vec_dot(const double* x, const double* y, int64_t n, double* result
   DG_CUDA(cudaGetLastError());
   // the partials are released when this call returns
   DG_CUDA(cudaStreamSynchronize(s));
+  return DG_OK;
+}
+
+dg_status dg_damg_set_smoother(dg_damg* m, dg_mlp* mlp, int sweeps, double fallback_ratio) {
+  DG_CHECK(m && sweeps >= 1 && fallback_ratio > 0, DG_EINVAL, "damg_set_smoother: bad arguments");
+  DG_CHECK(!mlp || m->cfg.inner_prec != DG_PREC_F64, DG_EINVAL,
+           "damg_set_smoother: the learned smoother runs in the FP32 inner V-cycle (inner_prec F32)");
+  if (mlp) DG_TRY(ensure_smoother_data(m));
+  m->mlp = mlp;
+  m->mlp_sweeps = sweeps;
+  m->mlp_fallback = fallback_ratio;
+  m->mlp_active = mlp != nullptr;
+  if (m->precond_graph) {
+    cudaGraphExecDestroy(m->precond_graph);
+    m->precond_graph = nullptr;
+  }
+  return DG_OK;
+}
+
+dg_status dg_damg_features(dg_damg* m, const double* r, float* F, float* scale) {
+  DG_CHECK(m && r && F, DG_EINVAL, "damg_features: bad arguments");
+  DG_CUDA(cudaDeviceSynchronize());
+  DG_TRY(ensure_smoother_data(m));
+  Level& L = m->lv[0];
+  DBuf<float> d32, sc;
+  const float* dinv32 = L.dinv32.p;
+  if (!dinv32) {
+    DG_TRY(d32.alloc(L.da->N));
+    convert<double, float><<<grid_for(L.da->N, 256), 256, 0, m->s>>>(L.dinv.p, d32.p, L.da->N);
+    dinv32 = d32.p;
+  }
+  DG_TRY(sc.alloc(1));
+  DG_TRY(mlp_features_f64(L.da.get(), r, m->sm_s2.p, dinv32, L.sm_dlogbar, 0.f, L.sm_hang.p, L.sm_refs.p,
+                          L.sm_nsum.p, L.sm_nmax.p, F, sc.p, m->s));
+  float h = 0;
+  DG_CUDA(cudaMemcpyAsync(&h, sc.p, 4, cudaMemcpyDeviceToHost, m->s));
+  DG_CUDA(cudaStreamSynchronize(m->s));
+  if (scale) *scale = h;
+  return DG_OK;
+}
+
+dg_status dg_damg_vcycle(dg_damg* m, const double* b, double* x) {
+  DG_CHECK(m && b && x, DG_EINVAL, "damg_vcycle: bad arguments");
+  const int64_t n = m->lv[0].da->N;
+  DG_CUDA(cudaDeviceSynchronize());
+  DG_CUDA(cudaMemcpyAsync(m->r.p, b, 8 * n, cudaMemcpyDeviceToDevice, m->s));
+  DG_TRY(precond_body(m));
+  DG_CUDA(cudaMemcpyAsync(x, m->z.p, 8 * n, cudaMemcpyDeviceToDevice, m->s));
+  DG_CUDA(cudaStreamSynchronize(m->s));
   return DG_OK;
 }
 

@@ -44,6 +44,7 @@ typedef struct dg_octree dg_octree; /* device-resident sorted linear octree */
 typedef struct dg_da dg_da;         /* device-resident mesh (ot::DA)         */
 typedef struct dg_mat dg_mat;       /* operator on a mesh (PETSc MatShell)   */
 typedef struct dg_damg dg_damg;     /* multigrid hierarchy (ot::DAMG)        */
+typedef struct dg_mlp dg_mlp;       /* learned post-smoother (no reference counterpart) */
 
 const char* dg_status_string(dg_status s);
 /* Copies the last error message of the calling thread into buf. */
@@ -168,6 +169,7 @@ typedef struct dg_solve_report {
   int converged;
   double rel_residual;  /* FP64 ||b - A x||_2 / ||b||_2 at exit */
   double solve_ms;      /* device time of the solve */
+  int smoother_fallbacks; /* learned smoother replaced by damped Jacobi during the solve */
 } dg_solve_report;
 
 void dg_damg_default_config(dg_damg_config* cfg);
@@ -203,6 +205,38 @@ dg_da* dg_damg_level_da(dg_damg* m, int level); /* 0 = finest; owned by m */
 dg_status dg_damg_prolong(dg_damg* m, int level, const double* xc, double* xf, int on_device);
 dg_status dg_damg_restrict(dg_damg* m, int level, const double* rf, double* rc, int on_device);
 void dg_damg_destroy(dg_damg* m);
+
+/* PCApply of the multigrid preconditioner: one V-cycle on device vectors. */
+dg_status dg_damg_vcycle(dg_damg* m, const double* b, double* x);
+
+/* ------------------------------------------------------- learned smoother --- */
+/* No reference counterpart (the reference smooths with damped Jacobi,
+ * bin/options:187-194).  A per-node MLP 6 -> 64 -> 64 -> 1 (GELU), BF16
+ * weights in the forward pass, FP32 accumulation, FP32 master parameters
+ * packed as W1[64][6] | b1[64] | W2[64][64] | b2[64] | w3[64] | b3.
+ * Features of node i for a residual r (s = RMS of r): r_i/s, log2 d_i minus
+ * its mean (d = operator diagonal), level, share of hanging references,
+ * mean and max |r| over the surrounding elements / s.  It replaces the
+ * post-smoothing of the finest level, x_i += y_i s / d_i, inside the FP32
+ * inner V-cycle; the FP64 outer residual judges it and damped Jacobi takes
+ * over for the rest of a solve when that residual falls by less than
+ * fallback_ratio in one iteration. */
+int dg_mlp_param_count(void);
+dg_status dg_mlp_create(const float* params_host /* NULL: zeros */, dg_mlp** out);
+dg_status dg_mlp_get_params(const dg_mlp* m, float* host);
+dg_status dg_mlp_set_params(dg_mlp* m, const float* host);
+/* out[i] = MLP(F[i][0..5]) for device F, out; exact_fp32 = 1 skips BF16 rounding. */
+dg_status dg_mlp_forward(dg_mlp* m, const float* F, int64_t n, float* out, int exact_fp32, void* stream);
+/* Gradient of mean (MLP(F_i) - T_i)^2 over n device rows (host grad, loss). */
+dg_status dg_mlp_gradient(dg_mlp* m, const float* F, const float* T, int64_t n, int exact_fp32, float* grad_host,
+                          double* loss_host);
+/* One Adam step (beta 0.9/0.999) on that loss. */
+dg_status dg_mlp_train_step(dg_mlp* m, const float* F, const float* T, int64_t n, float lr, double* loss_host);
+void dg_mlp_destroy(dg_mlp* m);
+/* Use the MLP (or NULL for damped Jacobi) as finest-level post-smoother. */
+dg_status dg_damg_set_smoother(dg_damg* m, dg_mlp* mlp, int sweeps, double fallback_ratio);
+/* Features of a finest-level residual r (device) into F [N][6] (device); *scale = s. */
+dg_status dg_damg_features(dg_damg* m, const double* r, float* F, float* scale);
 
 /* -------------------------------------------------------- vector kernels --- */
 

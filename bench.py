@@ -145,9 +145,8 @@ def run_dendro(args, rank, world):
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = float(sum(step_ms))
     if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+        from dendro_b200.parallel import max_over_ranks
+        total_ms = max_over_ranks(total_ms, dev)
         torch.distributed.barrier()
     ms_per_step = total_ms / args.steps
     gdofs = world * N * args.steps / (total_ms * 1e-3) / 1e9

@@ -163,9 +163,31 @@ class _Mat:
         check(lib().dg_mat_mult_host(self.h, ptr(xa), ptr(ya)), "mat_mult_host")
         return ya
 
+    def mult_multi(self, X, Y=None, split: int = 3, stream=None):
+        """Y = A X for the columns of X, a CUDA float32 tensor [N, nrhs]
+        (nrhs a multiple of 16), on the tensor cores (split 3: FP32-level
+        accuracy from three TF32 products; 1: one TF32 product)."""
+        import torch
+        if not (X.is_cuda and X.dtype == torch.float32 and X.dim() == 2 and X.is_contiguous()):
+            raise TypeError("X must be a contiguous CUDA float32 tensor [N, nrhs]")
+        if Y is None:
+            Y = torch.empty_like(X)
+        s = None if stream is None else C.c_void_p(stream.cuda_stream)
+        check(lib().dg_mat_mult_multi(self.h, ptr(X), ptr(Y), X.shape[1], split, s), "mat_mult_multi")
+        return Y
+
     def kernel_name(self, prec: int = 0) -> str:
         """Launch shape the autotuner chose for this mesh (after the first mult)."""
         return lib().dg_mat_kernel_name(self.h, prec).decode()
+
+    @staticmethod
+    def kernel_count() -> int:
+        """Number of operator launch shapes the autotuner chooses from."""
+        return lib().dg_mat_kernel_count()
+
+    def set_kernel(self, variant: int, prec: int = 0) -> None:
+        """Fix the operator launch shape for this mesh and precision (no timing)."""
+        check(lib().dg_mat_set_kernel(self.h, prec, variant), "dg_mat_set_kernel")
 
     def getDiagonal(self, d=None, stream=None):
         import torch

@@ -405,6 +405,21 @@ const char* dg_mat_kernel_name(const dg_mat* A, int prec) {
   return matvec_variant_name(prec == DG_PREC_F64 ? A->da->tuned_f64 : A->da->tuned_f32);
 }
 
+int dg_mat_kernel_count(void) { return matvec_variant_count(); }
+
+dg_status dg_mat_mult_multi(dg_mat* A, const float* X, float* Y, int nrhs, int split, void* stream) {
+  DG_CHECK(A && X && Y, DG_EINVAL, "mat_mult_multi: null argument");
+  return mrhs_apply(A, X, Y, nrhs, split, static_cast<cudaStream_t>(stream));
+}
+
+dg_status dg_mat_set_kernel(dg_mat* A, int prec, int variant) {
+  DG_CHECK(A && A->kind == 0, DG_EINVAL, "set_kernel: scalar operator expected");
+  DG_CHECK(variant >= 0 && variant < matvec_variant_count(), DG_EINVAL, "set_kernel: variant out of range");
+  DG_CHECK(prec == DG_PREC_F64 || prec == DG_PREC_F32, DG_EINVAL, "set_kernel: precision");
+  (prec == DG_PREC_F64 ? A->da->tuned_f64 : A->da->tuned_f32) = variant;
+  return DG_OK;
+}
+
 void dg_mat_destroy(dg_mat* A) { delete A; }
 
 }  // extern "C"

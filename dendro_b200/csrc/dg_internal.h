@@ -6,6 +6,24 @@
 
 #include "dg_common.cuh"
 
+namespace dg {
+// Tiles of `te` consecutive elements for the shared-memory operator kernels.
+// Per tile: its distinct node ids (ascending; bit 31 set when another tile
+// also references the node) and, grouped by node, the tile's references to
+// them, each as position v * te + element of its (element, vertex) slot.
+struct TileSet {
+  int te = 0;                // elements per tile
+  int64_t ntiles = 0;
+  uint32_t max_nodes = 0;    // largest node count of a tile
+  DBuf<uint32_t> ptr;        // [ntiles + 1] offsets of the tiles' node lists
+  DBuf<uint32_t> nodes;      // [ptr[ntiles]]
+  DBuf<uint16_t> nend;       // [ntiles * 8 te]: tile t, node k -> end of its run in inc
+  DBuf<uint16_t> inc;        // [ntiles * 8 te]: tile t -> references ordered by node
+  DBuf<uint32_t> shared;     // ascending ids of the nodes several tiles reference
+  int64_t nshared = 0;
+};
+}  // namespace dg
+
 struct dg_octree {
   uint32_t max_depth = 0;
   int64_t n = 0;
@@ -19,15 +37,12 @@ struct dg_da {
   dg::DBuf<uint32_t> meta;   // [E] packed level / child number / hanging mask / type
   dg::DBuf<uint64_t> ekey;   // [E] element octant keys (embedded space)
   dg::DBuf<uint64_t> nkey;   // [N] node anchor Morton keys (embedded space), sorted
-  // Element tiles for the shared-memory matvec: per tile of kTile elements the
-  // smallest node id it touches and the window width actually needed.
-  dg::DBuf<uint32_t> tile_lo;
-  dg::DBuf<uint32_t> tile_span;
-  int64_t ntiles = 0;
-  int tile_elems = 0;
+  // element tiles of the shared-memory operator kernels: the scalar operator's
+  // (kLocalTile elements per tile) and the multi-right-hand-side one's
+  // (kMultiTile elements per tile, built on first use)
+  dg::TileSet tiles, tiles_mr;
   // operator launch shape picked by the autotuner on first use (-1: not yet)
   int tuned_f64 = -1, tuned_f32 = -1;
-  uint32_t max_span = 0;
 };
 
 struct dg_mlp {
@@ -48,6 +63,11 @@ struct dg_mat {
 };
 
 namespace dg {
+
+// elements per tile of the scalar shared-memory operator kernel (one thread
+// each) and of the multi-right-hand-side kernel
+constexpr int kLocalTile = 512;
+constexpr int kMultiTile = 128;
 
 // ---- learned smoother (mlp.cu): 6 -> 64 -> 64 -> 1, packed FP32 parameters ----
 constexpr int kMlpIn = 6;
@@ -84,13 +104,32 @@ dg_status coarsen_octree(const dg_octree* in, dg_octree* out, cudaStream_t s);
 
 // ---- mesh (mesh.cu) ----
 dg_status build_mesh(const dg_octree* tree, dg_da* da, cudaStream_t s);
-dg_status build_tiles(dg_da* da, cudaStream_t s);
+dg_status build_tiles(dg_da* da, cudaStream_t s);  // da->tiles (kLocalTile)
+dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s);
+// Hanging mask of element type t (0..17) for child number c
+// (include/oda/cnumEtypes.h:19-229).
+uint32_t etype_mask(int c, int t);
 
 // ---- operators (matvec.cu) ----
 dg_status lapmass_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStream_t s);
 dg_status lapmass_diag(const dg_mat* A, double* d, cudaStream_t s);
+// Fused tile-local forms: one damped-Jacobi sweep x <- x + omega dinv (b - A x)
+// in place, and the residual r = b - A x.  acc is an N-vector that must be
+// zero on entry and is zero again on return (sums of the shared nodes).
+dg_status lapmass_smooth_f64(const dg_mat* A, double* x, const double* b, const double* dinv, double omega,
+                             double* acc, cudaStream_t s);
+dg_status lapmass_smooth_f32(const dg_mat* A, float* x, const float* b, const float* dinv, float omega, float* acc,
+                             cudaStream_t s);
+dg_status lapmass_residual_f64(const dg_mat* A, const double* x, const double* b, double* r, double* acc,
+                               cudaStream_t s);
+dg_status lapmass_residual_f32(const dg_mat* A, const float* x, const float* b, float* r, float* acc,
+                               cudaStream_t s);
 const char* matvec_variant_name(int v);
+int matvec_variant_count();
+// Y = A X for nrhs vectors (node-major [N][nrhs], FP32) on the tensor cores;
+// split 1: TF32 products, 3: high/low TF32 split (FP32-level accuracy).
+dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int nrhs, int split, cudaStream_t s);
 dg_status elasticity_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status elasticity_diag(const dg_mat* A, double* d, cudaStream_t s);
 // Dense assembled operator of a small level as row-major blocks, one per

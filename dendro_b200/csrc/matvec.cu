@@ -10,8 +10,12 @@
 // T^T A T, where A is the reference-cube Q1 matrix and T interpolates the
 // element's vertex values from its node values (a hanging vertex takes the
 // mean of the parent vertices on its edge or face).  The kernels apply T,
-// the tensor-product form of A on [-1,1]^3, then T^T, which needs no tables
-// and about 150 flops per scalar element instead of 256.
+// A on [-1,1]^3, then T^T, which needs no tables.  A itself is applied in the
+// basis where it is diagonal: along each axis the 1D mass and stiffness
+// matrices M1 = [[2,1],[1,2]]/3 and K1 = [[1,-1],[-1,1]]/2 share the
+// eigenvectors (1,1) and (1,-1), so A = f1 K + f2 M = W diag(l) W / 8 with W
+// the 8-point Walsh-Hadamard transform and l depending only on the number of
+// (1,-1) factors; 56 flops per scalar element instead of 256.
 #include <cstdlib>
 #include <cstring>
 
@@ -30,48 +34,48 @@ __device__ __forceinline__ T elem_h(uint32_t lev) {
   return T(__longlong_as_double(int64_t(1023 + 1 - int(lev)) << 52));
 }
 
-// 1D reference matrices on [-1,1]: mass M1 = [[2,1],[1,2]]/3, stiffness
-// K1 = [[1,-1],[-1,1]]/2, applied along the axis whose vertex bit is B.
-template <int B, class T>
-__device__ __forceinline__ void mass1(const T (&u)[8], T (&o)[8]) {
-  const T third = T(1.0 / 3.0);
+// In-place 8-point Walsh-Hadamard transform over the vertex bits x=1, y=2, z=4.
+template <class T>
+__device__ __forceinline__ void wht8(T (&u)[8]) {
 #pragma unroll
-  for (int v = 0; v < 8; ++v) {
-    if (v & B) continue;
-    T s = u[v] + u[v | B];
-    o[v] = (s + u[v]) * third;
-    o[v | B] = (s + u[v | B]) * third;
-  }
-}
-template <int B, class T>
-__device__ __forceinline__ void stiff1(const T (&u)[8], T (&o)[8]) {
+  for (int B = 1; B < 8; B <<= 1)
 #pragma unroll
-  for (int v = 0; v < 8; ++v) {
-    if (v & B) continue;
-    T d = (u[v] - u[v | B]) * T(0.5);
-    o[v] = d;
-    o[v | B] = -d;
-  }
+    for (int v = 0; v < 8; ++v)
+      if (!(v & B)) {
+        const T a = u[v], b = u[v | B];
+        u[v] = a + b;
+        u[v | B] = a - b;
+      }
 }
 
-// r = f1 * K u + f2 * M u with K = K1(x)M1(x)M1 + M1(x)K1(x)M1 + M1(x)M1(x)K1
-// and M = M1(x)M1(x)M1 on the reference cube.
+// u <- (f1 K + f2 M) u on the reference cube, K = K1(x)M1(x)M1 + M1(x)K1(x)M1
+// + M1(x)M1(x)K1 and M = M1(x)M1(x)M1.  In the Walsh basis M1 -> diag(1, 1/3)
+// and K1 -> diag(0, 1), so a component with n (1,-1) factors is scaled by
+// f2 3^-n + f1 n 3^(1-n); the 1/8 of the inverse transform is folded in.
 template <class T>
-__device__ __forceinline__ void lapmass_ref(const T (&u)[8], T f1, T f2, T (&r)[8]) {
-  T P[8], Q[8], A[8], B[8];
-  mass1<1>(u, P);   // Mx u
-  mass1<2>(P, Q);   // My Mx u
-  mass1<4>(Q, A);   // Mz My Mx u        (mass)
-  stiff1<4>(Q, B);  // Kz My Mx u
+__device__ __forceinline__ void lapmass_ref(T (&u)[8], T f1, T f2) {
+  wht8(u);
+  const T l0 = f2 * T(0.125);
+  const T l1 = (f2 * T(1.0 / 3.0) + f1) * T(0.125);
+  const T l2 = (f2 * T(1.0 / 9.0) + f1 * T(2.0 / 3.0)) * T(0.125);
+  const T l3 = (f2 * T(1.0 / 27.0) + f1 * T(1.0 / 3.0)) * T(0.125);
+  u[0] *= l0;
+  u[1] *= l1;
+  u[2] *= l1;
+  u[4] *= l1;
+  u[3] *= l2;
+  u[5] *= l2;
+  u[6] *= l2;
+  u[7] *= l3;
+  wht8(u);
+}
+
+// r = (f1 K + f2 M) u, u unchanged.
+template <class T>
+__device__ __forceinline__ void lapmass_ref_to(const T (&u)[8], T f1, T f2, T (&r)[8]) {
 #pragma unroll
-  for (int v = 0; v < 8; ++v) r[v] = f2 * A[v] + f1 * B[v];
-  mass1<4>(P, Q);   // Mz Mx u
-  stiff1<2>(Q, A);  // Ky Mz Mx u
-  mass1<2>(u, P);   // My u
-  mass1<4>(P, Q);   // Mz My u
-  stiff1<1>(Q, B);  // Kx Mz My u
-#pragma unroll
-  for (int v = 0; v < 8; ++v) r[v] += f1 * (A[v] + B[v]);
+  for (int v = 0; v < 8; ++v) r[v] = u[v];
+  lapmass_ref(r, f1, f2);
 }
 
 // Hanging interpolation u_vertex = T u_node, in place.  A hanging vertex i
@@ -113,6 +117,59 @@ __device__ __forceinline__ void scatter_hanging(T (&r)[8], uint32_t c, uint32_t 
   for (int v = 0; v < 8; ++v) r[v] = rn[v];
 }
 
+// XOR relabelling of a vertex-indexed array by the child number: a[j] <- a[j ^ c]
+// (an involution).  In this frame the element's own corner of its parent is
+// vertex 0 and the hanging-vertex structure no longer depends on c.
+template <class T>
+__device__ __forceinline__ void xor_perm(T (&a)[8], uint32_t c) {
+#pragma unroll
+  for (int B = 1; B < 8; B <<= 1) {
+    const bool f = (c & B) != 0;
+#pragma unroll
+    for (int v = 0; v < 8; ++v)
+      if (!(v & B)) {
+        const T p = a[v], q = a[v | B];
+        a[v] = f ? q : p;
+        a[v | B] = f ? p : q;
+      }
+  }
+}
+// The hanging mask in the same frame: bit j <- bit j ^ c.
+__device__ __forceinline__ uint32_t xor_perm_mask(uint32_t m, uint32_t c) {
+  if (c & 1u) m = ((m & 0x55u) << 1) | ((m & 0xAAu) >> 1);
+  if (c & 2u) m = ((m & 0x33u) << 2) | ((m & 0xCCu) >> 2);
+  if (c & 4u) m = ((m & 0x0Fu) << 4) | ((m & 0xF0u) >> 4);
+  return m;
+}
+// T and T^T in the child-number frame.  A hanging vertex j lies on the
+// parent's edge (j = 1, 2, 4) or face (j = 3, 5, 6) through the shared corner
+// 0 and takes the mean of the node values of the vertices j' with j' a bit
+// subset of j; vertices 0 and 7 are never hanging.
+template <class T>
+__device__ __forceinline__ void interp_frame(T (&w)[8], uint32_t mp) {
+  const T w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3], w4 = w[4], w5 = w[5], w6 = w[6];
+  if (mp & 0x02u) w[1] = (w0 + w1) * T(0.5);
+  if (mp & 0x04u) w[2] = (w0 + w2) * T(0.5);
+  if (mp & 0x10u) w[4] = (w0 + w4) * T(0.5);
+  if (mp & 0x08u) w[3] = ((w0 + w1) + (w2 + w3)) * T(0.25);
+  if (mp & 0x20u) w[5] = ((w0 + w1) + (w4 + w5)) * T(0.25);
+  if (mp & 0x40u) w[6] = ((w0 + w2) + (w4 + w6)) * T(0.25);
+}
+template <class T>
+__device__ __forceinline__ void scatter_frame(T (&r)[8], uint32_t mp) {
+  const T h1 = (mp & 0x02u) ? r[1] * T(0.5) : T(0), h2 = (mp & 0x04u) ? r[2] * T(0.5) : T(0);
+  const T h4 = (mp & 0x10u) ? r[4] * T(0.5) : T(0);
+  const T q3 = (mp & 0x08u) ? r[3] * T(0.25) : T(0), q5 = (mp & 0x20u) ? r[5] * T(0.25) : T(0);
+  const T q6 = (mp & 0x40u) ? r[6] * T(0.25) : T(0);
+  r[0] += (h1 + h2) + (h4 + q3) + (q5 + q6);
+  r[1] = ((mp & 0x02u) ? h1 : r[1]) + (q3 + q5);
+  r[2] = ((mp & 0x04u) ? h2 : r[2]) + (q3 + q6);
+  r[4] = ((mp & 0x10u) ? h4 : r[4]) + (q5 + q6);
+  if (mp & 0x08u) r[3] = q3;
+  if (mp & 0x20u) r[5] = q5;
+  if (mp & 0x40u) r[6] = q6;
+}
+
 // One thread per element: gather, apply, scatter with atomics.  BLOCK and
 // MINB set the launch bounds (registers per thread) of each tuned variant.
 template <class T, class CT, int BLOCK = 256, int MINB = 1>
@@ -130,81 +187,118 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_kernel(const uint32_t* __
     T u[8];
 #pragma unroll
     for (int v = 0; v < 8; ++v) id[v] = __ldg(nl + int64_t(v) * E + e);
+    xor_perm(id, c);  // child-number frame: id[j] is the node of vertex j ^ c
 #pragma unroll
-    for (int v = 0; v < 8; ++v) u[v] = __ldg(x + id[v]);
-    if (mask) interp_hanging(u, c, mask);
-    T r[8];
-    lapmass_ref(u, f1, f2, r);
-    if (mask) scatter_hanging(r, c, mask);
+    for (int j = 0; j < 8; ++j) u[j] = __ldg(x + id[j]);
+    const uint32_t mp = xor_perm_mask(mask, c);
+    if (mp) interp_frame(u, mp);
+    lapmass_ref(u, f1, f2);
+    if (mp) scatter_frame(u, mp);
 #pragma unroll
-    for (int v = 0; v < 8; ++v) atomicAdd(y + id[v], r[v]);
+    for (int j = 0; j < 8; ++j) atomicAdd(y + id[j], u[j]);
   }
 }
 
-// Tiled variant: a CTA owns kTileElems consecutive elements (Morton order) and
-// a window of kWindow consecutive node ids starting at the tile's smallest
-// node id.  x over the window is staged in shared memory with coalesced
-// loads; element results for window nodes accumulate in shared memory and are
-// flushed with one global atomic per touched node.  References outside the
-// window (about 8% on log-normal meshes) go straight to global memory.
-constexpr int kTileThreads = 256;
-constexpr int kTileElems = 512;
-constexpr int kWindow = 2048;
+// Output of the tile-local kernel.  MODE 0: y = A x (y zeroed beforehand for
+// the shared nodes).  MODE 1: one damped-Jacobi sweep in place, y = x <- x +
+// omega dinv (b - A x).  MODE 2: residual y = r = b - A x.  In modes 1 and 2
+// the exclusive nodes are finished in the kernel and the shared ones collect
+// their sums in acc (zero on entry) for local_shared_finish.
+template <class T>
+struct LocalOut {
+  T* y;
+  const T* b;
+  const T* dinv;
+  T omega;
+  T* acc;
+};
 
-template <class T, class CT>
-__global__ void __launch_bounds__(kTileThreads) lapmass_tiled_kernel(
-    const uint32_t* __restrict__ nl, const uint32_t* __restrict__ meta, const CT* __restrict__ ca,
-    const CT* __restrict__ cb, int64_t E, int64_t N, const uint32_t* __restrict__ tile_lo, int64_t ntiles,
-    const T* __restrict__ x, T* __restrict__ y) {
-  __shared__ T xs[kWindow];
-  __shared__ T ys[kWindow];
-  __shared__ uint32_t touched[kWindow / 32];
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const uint32_t lo = tile_lo[tile];
-    const int64_t wn = (N - int64_t(lo)) < kWindow ? (N - int64_t(lo)) : kWindow;
-    for (int i = threadIdx.x; i < kWindow; i += kTileThreads) {
-      xs[i] = i < wn ? x[lo + i] : T(0);
-      ys[i] = T(0);
+// Tile-local variant: a CTA of kLocalTile threads owns one tile of kLocalTile
+// consecutive elements (one each), its distinct nodes and, per node, the
+// tile's (element, vertex) references to it.  The node-parallel phases copy x
+// from each node to its references in shared memory and, after the element
+// phase, sum each node's references; a node's sum leaves with one store (node
+// used by this tile only) or one global atomic (node shared with other
+// tiles).  No shared-memory atomics and two barriers per tile.
+template <class T, class CT, int MODE>
+__global__ void __launch_bounds__(kLocalTile, 2) lapmass_local_kernel(
+    const uint32_t* __restrict__ meta, const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
+    const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_nodes,
+    const uint16_t* __restrict__ nend, const uint16_t* __restrict__ inc, const T* x, LocalOut<T> o) {
+  constexpr int S = 8 * kLocalTile;
+  __shared__ T buf[S];  // per (vertex, element) slot: x in, element result out
+  const int tid = threadIdx.x;
+  const int64_t tile = blockIdx.x;
+  const int64_t e = tile * kLocalTile + tid;
+  const bool live = e < E;
+  uint32_t m = 0;
+  T a = T(1), b = T(1);
+  if (live) {
+    m = __ldg(meta + e);
+    if (ca) {
+      a = T(__ldg(ca + e));
+      b = T(__ldg(cb + e));
     }
-    for (int i = threadIdx.x; i < kWindow / 32; i += kTileThreads) touched[i] = 0;
-    __syncthreads();
-#pragma unroll 1
-    for (int k = 0; k < kTileElems / kTileThreads; ++k) {
-      const int64_t e = tile * kTileElems + k * kTileThreads + threadIdx.x;
-      if (e >= E) break;
-      const uint32_t m = meta[e];
-      const uint32_t lev = meta_lev(m), c = meta_cnum(m), mask = meta_mask(m);
-      const T h = elem_h<T>(lev);
-      const T a = ca ? T(ca[e]) : T(1), b = cb ? T(cb[e]) : T(1);
-      const T f1 = a * h / T(2), f2 = b * h * h * h / T(8);
-      uint32_t id[8];
-      T u[8];
+  }
+  const uint32_t p0 = __ldg(tile_ptr + tile), nt = __ldg(tile_ptr + tile + 1) - p0;
+  const uint16_t* tinc = inc + tile * S;
+  const uint16_t* tend = nend + tile * S;
+  // x at each node to the slots that reference it
+  for (uint32_t k = tid; k < nt; k += kLocalTile) {
+    const uint32_t n = __ldg(tile_nodes + p0 + k) & 0x7fffffffu;
+    // the smoothing form updates x in place (other tiles' exclusive nodes),
+    // so x is read through the coherent path there
+    const T xv = MODE == 1 ? x[n] : __ldg(x + n);
+    const uint32_t end = __ldg(tend + k);
+    for (uint32_t j = k ? __ldg(tend + k - 1) : 0u; j < end; ++j) buf[__ldg(tinc + j)] = xv;
+  }
+  __syncthreads();
+  if (live) {
+    const uint32_t c = meta_cnum(m);
+    const T h = elem_h<T>(meta_lev(m));
+    const T f1 = a * h * T(0.5), f2 = b * h * h * h * T(0.125);
+    // work in the child-number frame: w[j] is vertex j ^ c
+    T w[8];
 #pragma unroll
-      for (int v = 0; v < 8; ++v) id[v] = __ldg(nl + int64_t(v) * E + e);
+    for (int j = 0; j < 8; ++j) w[j] = buf[(uint32_t(j) ^ c) * kLocalTile + tid];
+    const uint32_t mp = xor_perm_mask(meta_mask(m), c);
+    if (mp) interp_frame(w, mp);
+    lapmass_ref(w, f1, f2);  // the reference-cube operator is invariant under the relabelling
+    if (mp) scatter_frame(w, mp);
 #pragma unroll
-      for (int v = 0; v < 8; ++v) {
-        const uint32_t o = id[v] - lo;
-        u[v] = o < uint32_t(wn) ? xs[o] : __ldg(x + id[v]);
-      }
-      if (mask) interp_hanging(u, c, mask);
-      T r[8];
-      lapmass_ref(u, f1, f2, r);
-      if (mask) scatter_hanging(r, c, mask);
-#pragma unroll
-      for (int v = 0; v < 8; ++v) {
-        const uint32_t o = id[v] - lo;
-        if (o < uint32_t(wn)) {
-          atomicAdd(ys + o, r[v]);
-          atomicOr(touched + (o >> 5), 1u << (o & 31));
-        } else {
-          atomicAdd(y + id[v], r[v]);
-        }
-      }
+    for (int j = 0; j < 8; ++j) buf[(uint32_t(j) ^ c) * kLocalTile + tid] = w[j];
+  }
+  __syncthreads();
+  // each node sums its references
+  for (uint32_t k = tid; k < nt; k += kLocalTile) {
+    const uint32_t id = __ldg(tile_nodes + p0 + k);
+    const uint32_t n = id & 0x7fffffffu;
+    const uint32_t end = __ldg(tend + k);
+    T sum = T(0);
+    for (uint32_t j = k ? __ldg(tend + k - 1) : 0u; j < end; ++j) sum += buf[__ldg(tinc + j)];
+    if (MODE == 0) {
+      if (id & 0x80000000u) atomicAdd(o.y + n, sum);
+      else o.y[n] = sum;
+    } else if (id & 0x80000000u) {
+      atomicAdd(o.acc + n, sum);
+    } else if (MODE == 1) {
+      o.y[n] = o.y[n] + o.omega * o.dinv[n] * (o.b[n] - sum);
+    } else {
+      o.y[n] = o.b[n] - sum;
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kWindow; i += kTileThreads)
-      if ((touched[i >> 5] >> (i & 31)) & 1u) atomicAdd(y + lo + i, ys[i]);
-    __syncthreads();
+  }
+}
+
+// Second pass of the smoothing / residual forms over the nodes that several
+// tiles share, once every tile has added its part to acc (acc is left zero).
+template <class T, int MODE>
+__global__ void local_shared_finish(const uint32_t* __restrict__ list, int64_t ns, LocalOut<T> o) {
+  for (int64_t i = gtid(); i < ns; i += gstride()) {
+    const uint32_t n = list[i];
+    const T a = o.acc[n];
+    o.acc[n] = T(0);
+    if (MODE == 1) o.y[n] += o.omega * o.dinv[n] * (o.b[n] - a);
+    else o.y[n] = o.b[n] - a;
   }
 }
 
@@ -219,13 +313,13 @@ __global__ void lapmass_diag_kernel(const uint32_t* __restrict__ nl, const uint3
     const double a = ca ? double(ca[e]) : 1.0, b = cb ? double(cb[e]) : 1.0;
     const double f1 = a * h / 2.0, f2 = b * h * h * h / 8.0;
     for (int j = 0; j < 8; ++j) {
-      double u[8], r[8];
+      double u[8];
 #pragma unroll
       for (int v = 0; v < 8; ++v) u[v] = v == j ? 1.0 : 0.0;
       if (mask) interp_hanging(u, c, mask);
-      lapmass_ref(u, f1, f2, r);
-      if (mask) scatter_hanging(r, c, mask);
-      atomicAdd(d + nl[int64_t(j) * E + e], r[j]);
+      lapmass_ref(u, f1, f2);
+      if (mask) scatter_hanging(u, c, mask);
+      atomicAdd(d + nl[int64_t(j) * E + e], u[j]);
     }
   }
 }
@@ -246,38 +340,38 @@ __global__ void lapmass_dense_kernel(const uint32_t* __restrict__ nl, const uint
     const double h = elem_h<double>(lev);
     const double a = ca ? double(ca[e]) : 1.0, b = cb ? double(cb[e]) : 1.0;
     const double f1 = a * h / 2.0, f2 = b * h * h * h / 8.0;
-    double u[8], r[8];
+    double u[8];
 #pragma unroll
     for (int v = 0; v < 8; ++v) u[v] = v == j ? 1.0 : 0.0;
     if (mask) interp_hanging(u, c, mask);
-    lapmass_ref(u, f1, f2, r);
-    if (mask) scatter_hanging(r, c, mask);
+    lapmass_ref(u, f1, f2);
+    if (mask) scatter_hanging(u, c, mask);
     const uint32_t col = nl[int64_t(j) * E + e];
     const uint32_t blk = row_blk[col];
     const int64_t o = boff[blk], n = bn[blk];
     double* Ab = A + baoff[blk];
     for (int k = 0; k < 8; ++k)
-      atomicAdd(Ab + (int64_t(nl[int64_t(k) * E + e]) - o) * n + (int64_t(col) - o), r[k]);
+      atomicAdd(Ab + (int64_t(nl[int64_t(k) * E + e]) - o) * n + (int64_t(col) - o), u[k]);
   }
 }
 
 }  // namespace
 
 // Launch shapes tried by the autotuner: one thread per element with
-// different block sizes / register caps / grid sizes, and the tiled
+// different block sizes / register caps / grid sizes, and the tile-local
 // shared-memory form.  The first application on a mesh times each once
 // (after one untimed launch) and keeps the fastest for that mesh and
 // precision; DG_MATVEC_KERNEL=<index> forces one (testing).
 struct MatvecVariant {
   int block, per_sm;  // threads per CTA, CTAs per SM in the grid (0: one thread per element)
-  int kind;           // 0 atomic (BLOCK, MINB), 1 tiled
+  int kind;           // 0 atomic (BLOCK, MINB), 1 tile-local
   int minb;
   const char* name;
 };
 constexpr MatvecVariant kVariants[] = {
     {256, 8, 0, 1, "atomic b256 grid 8/SM"},  {256, 0, 0, 1, "atomic b256 grid E"},
     {256, 8, 0, 4, "atomic b256 minB4"},      {128, 16, 0, 8, "atomic b128 minB8"},
-    {512, 4, 0, 2, "atomic b512 minB2"},      {256, 0, 1, 1, "tiled 512 elems / 2048-node window"},
+    {512, 4, 0, 2, "atomic b512 minB2"},      {kLocalTile, 0, 1, 2, "tile-local 512 elems"},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 
@@ -288,9 +382,10 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
   const unsigned g = V.per_sm ? grid_for(da->E, V.block, V.per_sm)
                               : unsigned((da->E + V.block - 1) / V.block > 0 ? (da->E + V.block - 1) / V.block : 1);
   if (V.kind == 1) {
-    const unsigned gt = unsigned(da->ntiles < int64_t(sm_count()) * 16 ? da->ntiles : int64_t(sm_count()) * 16);
-    lapmass_tiled_kernel<T, CT><<<gt > 0 ? gt : 1, kTileThreads, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E, da->N,
-                                                                      da->tile_lo.p, da->ntiles, x, y);
+    const TileSet& ts = da->tiles;
+    LocalOut<T> o{y, nullptr, nullptr, T(0), nullptr};
+    lapmass_local_kernel<T, CT, 0><<<unsigned(ts.ntiles), kLocalTile, 0, s>>>(
+        da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p, ts.nend.p, ts.inc.p, x, o);
   } else if (V.block == 256 && V.minb == 1) {
     lapmass_kernel<T, CT, 256, 1><<<g, 256, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E, x, y);
   } else if (V.block == 256 && V.minb == 4) {
@@ -311,7 +406,7 @@ static int forced_variant() {
     v = -1;
     if (e && *e) {
       if (!strcmp(e, "atomic")) v = 0;
-      else if (!strcmp(e, "tiled")) v = kNumVariants - 1;
+      else if (!strcmp(e, "local")) v = kNumVariants - 1;
       else v = atoi(e) % kNumVariants;
     }
   }
@@ -341,7 +436,7 @@ static dg_status lapmass_launch(const dg_da* da, int& choice, const CT* ca, cons
     int bi = 0;
     DG_TRY((launch_variant<T, CT>(0, da, ca, cb, x, y, s)));
     for (int v = 0; v < kNumVariants; ++v) {
-      if (kVariants[v].kind == 1 && da->ntiles == 0) continue;
+      if (kVariants[v].kind == 1 && da->tiles.ntiles == 0) continue;
       for (int trial = 0; trial < 2; ++trial) {
         DG_CUDA(cudaMemsetAsync(flush.p, trial + 1, flush_bytes, s));
         DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
@@ -365,6 +460,8 @@ static dg_status lapmass_launch(const dg_da* da, int& choice, const CT* ca, cons
   return launch_variant<T, CT>(choice, da, ca, cb, x, y, s);
 }
 
+int matvec_variant_count() { return kNumVariants; }
+
 const char* matvec_variant_name(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].name : "untuned"; }
 
 dg_status lapmass_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s) {
@@ -379,6 +476,37 @@ dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStrea
   const float* ca = A->has_coef ? A->coef32.p : nullptr;
   const float* cb = A->has_coef ? A->coef32.p + da->E : nullptr;
   return lapmass_launch<float, float>(da, da->tuned_f32, ca, cb, x, y, s);
+}
+
+template <class T, class CT, int MODE>
+static dg_status lapmass_fused(const dg_mat* A, const CT* coef, const T* x, LocalOut<T> o, cudaStream_t s) {
+  const dg_da* da = A->da;
+  const CT* ca = A->has_coef ? coef : nullptr;
+  const CT* cb = A->has_coef ? coef + da->E : nullptr;
+  const TileSet& ts = da->tiles;
+  lapmass_local_kernel<T, CT, MODE><<<unsigned(ts.ntiles), kLocalTile, 0, s>>>(
+      da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p, ts.nend.p, ts.inc.p, x, o);
+  if (ts.nshared)
+    local_shared_finish<T, MODE><<<grid_for(ts.nshared, 256, 8), 256, 0, s>>>(ts.shared.p, ts.nshared, o);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status lapmass_smooth_f64(const dg_mat* A, double* x, const double* b, const double* dinv, double omega,
+                             double* acc, cudaStream_t s) {
+  return lapmass_fused<double, double, 1>(A, A->coef.p, x, LocalOut<double>{x, b, dinv, omega, acc}, s);
+}
+dg_status lapmass_smooth_f32(const dg_mat* A, float* x, const float* b, const float* dinv, float omega, float* acc,
+                             cudaStream_t s) {
+  return lapmass_fused<float, float, 1>(A, A->coef32.p, x, LocalOut<float>{x, b, dinv, omega, acc}, s);
+}
+dg_status lapmass_residual_f64(const dg_mat* A, const double* x, const double* b, double* r, double* acc,
+                               cudaStream_t s) {
+  return lapmass_fused<double, double, 2>(A, A->coef.p, x, LocalOut<double>{r, b, nullptr, 0.0, acc}, s);
+}
+dg_status lapmass_residual_f32(const dg_mat* A, const float* x, const float* b, float* r, float* acc,
+                               cudaStream_t s) {
+  return lapmass_fused<float, float, 2>(A, A->coef32.p, x, LocalOut<float>{r, b, nullptr, 0.f, acc}, s);
 }
 
 dg_status lapmass_diag(const dg_mat* A, double* d, cudaStream_t s) {
@@ -480,9 +608,9 @@ __global__ void __launch_bounds__(128) elasticity_kernel(const uint32_t* __restr
     }
     double r0[8], r1[8], r2[8];
     const double wl = mu * fac, wg = (mu + lam) * fac;
-    lapmass_ref(u0, wl, 0.0, r0);
-    lapmass_ref(u1, wl, 0.0, r1);
-    lapmass_ref(u2, wl, 0.0, r2);
+    lapmass_ref_to(u0, wl, 0.0, r0);
+    lapmass_ref_to(u1, wl, 0.0, r1);
+    lapmass_ref_to(u2, wl, 0.0, r2);
     graddiv_block<0, 0>(u0, wg, r0);
     graddiv_block<0, 1>(u1, wg, r0);
     graddiv_block<0, 2>(u2, wg, r0);
@@ -537,7 +665,7 @@ __global__ void elasticity_diag_kernel(const uint32_t* __restrict__ nl, const ui
     if (mask)
       for (int a = 0; a < 3; ++a) interp_hanging(u[a], c, mask);
     const double wl = mu * fac, wg = (mu + lam) * fac;
-    for (int a = 0; a < 3; ++a) lapmass_ref(u[a], wl, 0.0, r[a]);
+    for (int a = 0; a < 3; ++a) lapmass_ref_to(u[a], wl, 0.0, r[a]);
     graddiv_block<0, 0>(u[0], wg, r[0]);
     graddiv_block<0, 1>(u[1], wg, r[0]);
     graddiv_block<0, 2>(u[2], wg, r[0]);

@@ -149,42 +149,124 @@ __global__ void build_nlist(const uint64_t* __restrict__ ekey, int64_t E, uint32
   }
 }
 
-// Per tile of kTile consecutive elements: min node id and the window span.
-__global__ void tile_ranges(const uint32_t* __restrict__ nl, int64_t E, int tile, int64_t ntiles,
-                            uint32_t* __restrict__ lo_out, uint32_t* __restrict__ span_out) {
+// Exclusive scan of one value per thread over a block of TE threads (every
+// thread calls it); the block total is returned through `total`.
+template <int TE>
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* wsum, uint32_t& total) {
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  uint32_t incl = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t n = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += n;
+  }
+  if (lane == 31) wsum[w] = incl;
+  __syncthreads();
+  uint32_t base = 0;
+  total = 0;
+  for (int i = 0; i < TE / 32; ++i) {
+    if (i < w) base += wsum[i];
+    total += wsum[i];
+  }
+  __syncthreads();
+  return base + incl - v;
+}
+
+// Per tile of TE consecutive elements (one CTA of TE threads per tile): the
+// 8 TE (node id, position v * TE + element) pairs are sorted in shared memory
+// by a bitonic network; the sorted positions are the tile's references
+// grouped by node (inc), the distinct ids its node list (to tmp, count to
+// cnt) and the run ends per node nend.
+template <int TE>
+__global__ void __launch_bounds__(TE) tile_lists(const uint32_t* __restrict__ nl, int64_t E, int64_t ntiles,
+                                                 uint32_t* __restrict__ tmp, uint32_t* __restrict__ cnt,
+                                                 uint16_t* __restrict__ nend, uint16_t* __restrict__ inc) {
+  constexpr int S = 8 * TE;
+  constexpr int kPer = 8;  // sorted entries per thread
+  static_assert(S <= 4096, "positions are 12-bit");
+  extern __shared__ __align__(16) unsigned char tl_smem[];
+  uint64_t* key = reinterpret_cast<uint64_t*>(tl_smem);
+  __shared__ uint32_t wsum[TE / 32];
+  const int tid = threadIdx.x;
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    uint32_t lo = 0xffffffffu, hi = 0;
-    const int64_t e0 = t * tile;
-    for (int v = 0; v < 8; ++v)
-      for (int i = threadIdx.x; i < tile; i += blockDim.x) {
-        const int64_t e = e0 + i;
-        if (e < E) {
-          const uint32_t id = nl[int64_t(v) * E + e];
-          lo = min(lo, id);
-          hi = max(hi, id);
-        }
-      }
-    for (int o = 16; o > 0; o >>= 1) {
-      lo = min(lo, __shfl_down_sync(0xffffffffu, lo, o));
-      hi = max(hi, __shfl_down_sync(0xffffffffu, hi, o));
-    }
-    __shared__ uint32_t slo[32], shi[32];
-    int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
-      slo[w] = lo;
-      shi[w] = hi;
+    for (int i = tid; i < S; i += TE) {
+      const int v = i / TE, el = i % TE;
+      const int64_t e = t * TE + el;
+      key[i] = e < E ? (uint64_t(nl[int64_t(v) * E + e]) << 12) | uint64_t(i) : ~0ull;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int i = 1; i < int(blockDim.x >> 5); ++i) {
-        lo = min(lo, slo[i]);
-        hi = max(hi, shi[i]);
+    for (int k = 2; k <= S; k <<= 1)
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int p = tid; p < S / 2; p += TE) {
+          const int i = 2 * p - (p & (j - 1));  // lower index of the pair, bit j clear
+          const int l = i + j;
+          const bool up = (i & k) == 0;
+          const uint64_t a = key[i], b = key[l];
+          if ((a > b) == up) {
+            key[i] = b;
+            key[l] = a;
+          }
+        }
+        __syncthreads();
       }
-      lo_out[t] = lo;
-      span_out[t] = hi >= lo ? hi - lo + 1 : 0;
+    uint32_t first_f = 0, nfirst = 0;
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+      const int j = tid * kPer + q;
+      const uint64_t kj = key[j];
+      const bool first = kj != ~0ull && (j == 0 || (key[j - 1] >> 12) != (kj >> 12));
+      first_f |= uint32_t(first) << q;
+      nfirst += first;
     }
+    uint32_t total = 0;
+    uint32_t run = block_excl_scan<TE>(nfirst, wsum, total);
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+      const int j = tid * kPer + q;
+      const uint64_t kj = key[j];
+      if (kj == ~0ull) continue;
+      if ((first_f >> q) & 1u) {
+        tmp[t * S + run] = uint32_t(kj >> 12);
+        ++run;
+      }
+      inc[t * S + j] = uint16_t(kj & 4095u);
+      const bool last = j + 1 == S || (key[j + 1] >> 12) != (kj >> 12);  // padding keys end every run
+      if (last) nend[t * S + run - 1] = uint16_t(j + 1);
+    }
+    if (tid == 0) cnt[t] = total;
     __syncthreads();
   }
+}
+
+// Copy each tile's node list (capacity S per tile) to its final place.
+__global__ void tile_compact(const uint32_t* __restrict__ tmp, int S, const uint32_t* __restrict__ ptr,
+                             int64_t ntiles, uint32_t* __restrict__ out) {
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint32_t p0 = ptr[t], n = ptr[t + 1] - p0;
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) out[p0 + k] = tmp[t * S + k];
+  }
+}
+
+// Per node, the number of tiles whose list holds it.
+__global__ void tile_touch(const uint32_t* __restrict__ nodes, int64_t n, uint32_t* __restrict__ touch) {
+  for (int64_t i = gtid(); i < n; i += gstride()) atomicAdd(touch + nodes[i], 1u);
+}
+
+// Bit 31 of a list entry: the node is referenced by more than one tile, so its
+// sum must be accumulated with a global atomic.  The shared nodes are also
+// flagged per node for the compact list of them.
+__global__ void tile_local_mark(uint32_t* __restrict__ nodes, int64_t n, const uint32_t* __restrict__ touch) {
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    const uint32_t id = nodes[i];
+    if (touch[id] > 1u) nodes[i] = id | 0x80000000u;
+  }
+}
+__global__ void shared_flag(uint32_t* __restrict__ touch, int64_t N) {
+  for (int64_t i = gtid(); i < N; i += gstride()) touch[i] = touch[i] > 1u ? 1u : 0u;
+}
+__global__ void shared_emit(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos, int64_t N,
+                            uint32_t* __restrict__ out) {
+  for (int64_t i = gtid(); i < N; i += gstride())
+    if (flag[i]) out[pos[i]] = uint32_t(i);
 }
 
 }  // namespace
@@ -254,17 +336,65 @@ dg_status build_mesh(const dg_octree* tree, dg_da* da, cudaStream_t s) {
   return build_tiles(da, s);
 }
 
-dg_status build_tiles(dg_da* da, cudaStream_t s) {
-  const int tile = 512;  // elements per tile of the shared-memory operator kernel
-  da->tile_elems = tile;
-  da->ntiles = (da->E + tile - 1) / tile;
-  DG_TRY(da->tile_lo.alloc(da->ntiles));
-  DG_TRY(da->tile_span.alloc(da->ntiles));
-  tile_ranges<<<grid_for(da->ntiles, 256, 16), 256, 0, s>>>(da->nl.p, da->E, tile, da->ntiles, da->tile_lo.p,
-                                                             da->tile_span.p);
+template <int TE>
+static dg_status launch_tile_lists(const dg_da* da, int64_t nt, uint32_t* tmp, uint32_t* cnt, uint16_t* nend,
+                                   uint16_t* inc, cudaStream_t s) {
+  const size_t smem = size_t(8) * 8 * TE;
+  static bool set = false;
+  if (!set && smem > 48 * 1024) {
+    DG_CUDA(cudaFuncSetAttribute(tile_lists<TE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  }
+  set = true;
+  tile_lists<TE><<<grid_for(nt, TE, 2048 / TE), TE, smem, s>>>(da->nl.p, da->E, nt, tmp, cnt, nend, inc);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s) {
+  DG_CHECK(da->N < (int64_t(1) << 31), DG_EINVAL, "mesh above 2^31 nodes");
+  DG_CHECK(te == kLocalTile || te == kMultiTile, DG_EINVAL, "unsupported tile size");
+  const int64_t E = da->E, nt = (E + te - 1) / te, S = 8 * int64_t(te);
+  ts.te = te;
+  ts.ntiles = nt;
+  DBuf<uint32_t> tmp, cnt, touch;
+  DG_TRY(tmp.alloc(nt * S));
+  DG_TRY(cnt.alloc(nt));
+  DG_TRY(ts.nend.alloc(nt * S));
+  DG_TRY(ts.inc.alloc(nt * S));
+  if (te == kLocalTile) DG_TRY(launch_tile_lists<kLocalTile>(da, nt, tmp.p, cnt.p, ts.nend.p, ts.inc.p, s));
+  else DG_TRY(launch_tile_lists<kMultiTile>(da, nt, tmp.p, cnt.p, ts.nend.p, ts.inc.p, s));
+  std::vector<uint32_t> hc(nt);
+  DG_CUDA(cudaMemcpyAsync(hc.data(), cnt.p, 4 * nt, cudaMemcpyDeviceToHost, s));
+  uint32_t total = 0;
+  DG_TRY(ts.ptr.alloc(nt + 1));
+  DG_TRY(scan_u32(cnt.p, ts.ptr.p, nt, &total, s));
+  DG_CUDA(cudaMemcpyAsync(ts.ptr.p + nt, &total, 4, cudaMemcpyHostToDevice, s));
+  DG_CUDA(cudaStreamSynchronize(s));
+  uint32_t mx = 0;
+  for (uint32_t c : hc) mx = c > mx ? c : mx;
+  ts.max_nodes = mx;
+  DG_TRY(ts.nodes.alloc(total));
+  tile_compact<<<grid_for(nt, 256, 8), 256, 0, s>>>(tmp.p, int(S), ts.ptr.p, nt, ts.nodes.p);
+  DG_TRY(touch.alloc(da->N));
+  DG_CUDA(cudaMemsetAsync(touch.p, 0, 4 * da->N, s));
+  tile_touch<<<grid_for(total, 256), 256, 0, s>>>(ts.nodes.p, total, touch.p);
+  tile_local_mark<<<grid_for(total, 256), 256, 0, s>>>(ts.nodes.p, total, touch.p);
+  shared_flag<<<grid_for(da->N, 256), 256, 0, s>>>(touch.p, da->N);
+  DG_CUDA(cudaGetLastError());
+  DBuf<uint32_t> pos;
+  DG_TRY(pos.alloc(da->N));
+  uint32_t ns = 0;
+  DG_TRY(scan_u32(touch.p, pos.p, da->N, &ns, s));
+  ts.nshared = ns;
+  DG_TRY(ts.shared.alloc(ns > 0 ? ns : 1));
+  shared_emit<<<grid_for(da->N, 256), 256, 0, s>>>(touch.p, pos.p, da->N, ts.shared.p);
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaStreamSynchronize(s));
   return DG_OK;
 }
+
+dg_status build_tiles(dg_da* da, cudaStream_t s) { return build_tile_set(da, kLocalTile, da->tiles, s); }
+
+uint32_t etype_mask(int c, int t) { return kEtypeMask[c & 7][t % 18]; }
 
 }  // namespace dg

@@ -1,0 +1,253 @@
+// Multi-right-hand-side operator Y = A X on the tensor cores: the scalar
+// Laplacian + mass operator (JAC_TYPE2_ELEM_MULT_BLOCK,
+// examples/src/backend/omgNeumann.C:468-488) applied to nrhs vectors at once,
+// X and Y node-major [N][nrhs] in FP32.  The reference applies MatMult to one
+// vector at a time; the batching has no reference counterpart.
+//
+// Per element the contraction D (16 rhs x 8 vertices) = X_e (16 x 8) A_e^T is
+// one mma.sync.m16n8k8 with TF32 inputs and FP32 accumulation (or three, with
+// each input split into a TF32 high part and a TF32 remainder, which keeps
+// FP32-level accuracy).  A_e = f1 L[c][t] + f2 M[c][t], where L and M are the
+// per (child number, element type) tables T^T K T and T^T M T
+// (Stencils/LapType2Stencils.inp, MassType2Stencils.inp; here computed from T
+// and the reference-cube matrices), stored per MMA lane so that each lane
+// loads its B-fragment entries with one 16-byte load.
+//
+// A CTA owns a tile of kMultiTile elements (its distinct nodes and, grouped by
+// node, the (element, vertex) references to them) and walks the right-hand
+// sides in chunks of 16: x rows go from each node to its references in shared
+// memory, each warp contracts its elements in place, and each node sums its
+// references and leaves with one store (node used by this tile only) or one
+// float4 global atomic (node shared with other tiles).
+#include <vector>
+
+#include "dg_internal.h"
+
+namespace dg {
+
+namespace {
+
+constexpr int kMT = kMultiTile;     // elements per tile, one thread each
+constexpr int kMS = 8 * kMT;        // references per tile
+constexpr int kRC = 16;             // right-hand sides per chunk (the MMA's M)
+constexpr int kBufFloats = kMS * kRC + 8 * 32 + 32;
+
+static_assert(kMT == 128, "slot_row assumes 128 elements per tile");
+
+// Shared-memory row of reference pos = v * kMT + element: 16 floats per row;
+// each vertex block starts at its own bank offset so that the MMA fragment
+// reads (vertices tq and tq + 4) and writes (vertices 2 tq and 2 tq + 1) of
+// one element hit distinct banks.
+__device__ __forceinline__ int slot_row(int pos) {
+  const int v = pos >> 7;
+  return pos * kRC + v * 32 + 8 * ((v + (v >> 2)) & 3);
+}
+
+__device__ __forceinline__ float elem_hf(uint32_t lev) { return __int_as_float(int(127 + 1 - int(lev)) << 23); }
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// d += A (16 x 8, row) * B (8 x 8, col), TF32 inputs, FP32 accumulation.
+__device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// NS = 1: TF32 products.  NS = 3: x = hi + lo for both inputs and
+// D = A_lo B_hi + A_hi B_lo + A_hi B_hi.
+template <int NS>
+__global__ void __launch_bounds__(kMT) mrhs_kernel(const uint32_t* __restrict__ meta, const float* __restrict__ ca,
+                                                   const float* __restrict__ cb, int64_t E,
+                                                   const uint32_t* __restrict__ tile_ptr,
+                                                   const uint32_t* __restrict__ tile_nodes,
+                                                   const uint16_t* __restrict__ nend, const uint16_t* __restrict__ inc,
+                                                   const float4* __restrict__ tbl, int R, const float* __restrict__ X,
+                                                   float* __restrict__ Y) {
+  extern __shared__ __align__(16) float mr_buf[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, tq = lane & 3;
+  const int64_t tile = blockIdx.x;
+  const uint32_t p0 = __ldg(tile_ptr + tile), nt = __ldg(tile_ptr + tile + 1) - p0;
+  const uint16_t* tinc = inc + tile * kMS;
+  const uint16_t* tend = nend + tile * kMS;
+  for (int r0 = 0; r0 < R; r0 += kRC) {
+    // x rows of the chunk to the references (4 threads per node, float4 each)
+    for (uint32_t i = tid; i < 4 * nt; i += kMT) {
+      const uint32_t k = i >> 2, q = i & 3;
+      const uint32_t n = __ldg(tile_nodes + p0 + k) & 0x7fffffffu;
+      const float4 xv = __ldg(reinterpret_cast<const float4*>(X + int64_t(n) * R + r0) + q);
+      const uint32_t end = __ldg(tend + k);
+      for (uint32_t j = k ? __ldg(tend + k - 1) : 0u; j < end; ++j)
+        *reinterpret_cast<float4*>(mr_buf + slot_row(__ldg(tinc + j)) + 4 * q) = xv;
+    }
+    __syncthreads();
+    for (int el = warp; el < kMT; el += kMT / 32) {
+      const int64_t e = tile * kMT + el;
+      if (e >= E) break;
+      const uint32_t m = __ldg(meta + e);
+      const float h = elem_hf(meta_lev(m));
+      const float a = ca ? __ldg(ca + e) : 1.f, b = cb ? __ldg(cb + e) : 1.f;
+      const float f1 = a * h * 0.5f, f2 = b * h * h * h * 0.125f;
+      const float4 t = __ldg(tbl + (meta_cnum(m) * 18 + meta_type(m)) * 32 + lane);
+      const float bf0 = f1 * t.x + f2 * t.z, bf1 = f1 * t.y + f2 * t.w;
+      float* r_lo = mr_buf + slot_row(tq * kMT + el);        // vertex tq
+      float* r_hi = mr_buf + slot_row((tq + 4) * kMT + el);  // vertex tq + 4
+      const float x0 = r_lo[g], x1 = r_lo[g + 8], x2 = r_hi[g], x3 = r_hi[g + 8];
+      float d[4] = {0.f, 0.f, 0.f, 0.f};
+      if (NS == 1) {
+        mma_tf32(d, to_tf32(x0), to_tf32(x1), to_tf32(x2), to_tf32(x3), to_tf32(bf0), to_tf32(bf1));
+      } else {
+        const uint32_t ah0 = to_tf32(x0), ah1 = to_tf32(x1), ah2 = to_tf32(x2), ah3 = to_tf32(x3);
+        const uint32_t bh0 = to_tf32(bf0), bh1 = to_tf32(bf1);
+        const uint32_t al0 = to_tf32(x0 - __uint_as_float(ah0)), al1 = to_tf32(x1 - __uint_as_float(ah1));
+        const uint32_t al2 = to_tf32(x2 - __uint_as_float(ah2)), al3 = to_tf32(x3 - __uint_as_float(ah3));
+        const uint32_t bl0 = to_tf32(bf0 - __uint_as_float(bh0)), bl1 = to_tf32(bf1 - __uint_as_float(bh1));
+        mma_tf32(d, al0, al1, al2, al3, bh0, bh1);
+        mma_tf32(d, ah0, ah1, ah2, ah3, bl0, bl1);
+        mma_tf32(d, ah0, ah1, ah2, ah3, bh0, bh1);
+      }
+      // D (rhs g / g + 8, vertices 2 tq / 2 tq + 1) back into the element's
+      // rows; every lane's reads above precede the warp-wide mma
+      float* w0 = mr_buf + slot_row(2 * tq * kMT + el);
+      float* w1 = mr_buf + slot_row((2 * tq + 1) * kMT + el);
+      __syncwarp();
+      w0[g] = d[0];
+      w1[g] = d[1];
+      w0[g + 8] = d[2];
+      w1[g + 8] = d[3];
+    }
+    __syncthreads();
+    for (uint32_t i = tid; i < 4 * nt; i += kMT) {
+      const uint32_t k = i >> 2, q = i & 3;
+      const uint32_t id = __ldg(tile_nodes + p0 + k);
+      const uint32_t end = __ldg(tend + k);
+      float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (uint32_t j = k ? __ldg(tend + k - 1) : 0u; j < end; ++j) {
+        const float4 v = *reinterpret_cast<const float4*>(mr_buf + slot_row(__ldg(tinc + j)) + 4 * q);
+        sum.x += v.x;
+        sum.y += v.y;
+        sum.z += v.z;
+        sum.w += v.w;
+      }
+      float4* dst = reinterpret_cast<float4*>(Y + int64_t(id & 0x7fffffffu) * R + r0) + q;
+      if (id & 0x80000000u) atomicAdd(dst, sum);
+      else *dst = sum;
+    }
+    __syncthreads();
+  }
+}
+
+// Zero the rows of the nodes that several tiles share (their sums arrive by atomics).
+__global__ void zero_shared_rows(const uint32_t* __restrict__ shared, int64_t ns, int R4, float4* __restrict__ Y) {
+  const int64_t n = ns * R4;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    Y[int64_t(shared[i / R4]) * R4 + i % R4] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// Element matrices T^T K T and T^T M T per (child number, element type), in
+// the per-lane layout of the B fragment: lane (g = lane / 4, tq = lane % 4)
+// holds {L[g][tq], L[g][tq + 4], M[g][tq], M[g][tq + 4]}.
+std::vector<float> stencil_tables() {
+  const double M1[2][2] = {{2.0 / 3.0, 1.0 / 3.0}, {1.0 / 3.0, 2.0 / 3.0}};
+  const double K1[2][2] = {{0.5, -0.5}, {-0.5, 0.5}};
+  double K[8][8], Mm[8][8];
+  for (int i = 0; i < 8; ++i)
+    for (int j = 0; j < 8; ++j) {
+      const int ix = i & 1, iy = (i >> 1) & 1, iz = i >> 2, jx = j & 1, jy = (j >> 1) & 1, jz = j >> 2;
+      Mm[i][j] = M1[ix][jx] * M1[iy][jy] * M1[iz][jz];
+      K[i][j] = K1[ix][jx] * M1[iy][jy] * M1[iz][jz] + M1[ix][jx] * K1[iy][jy] * M1[iz][jz] +
+                M1[ix][jx] * M1[iy][jy] * K1[iz][jz];
+    }
+  std::vector<float> out(size_t(8) * 18 * 32 * 4);
+  for (int c = 0; c < 8; ++c)
+    for (int t = 0; t < 18; ++t) {
+      const uint32_t mask = etype_mask(c, t);
+      double T[8][8] = {};
+      for (int i = 0; i < 8; ++i) {
+        if (!((mask >> i) & 1u)) {
+          T[i][i] = 1.0;
+          continue;
+        }
+        const uint32_t keep = ~(uint32_t(i) ^ uint32_t(c)) & 7u;
+        const double w = __builtin_popcount(keep) == 2 ? 0.5 : 0.25;
+        for (int j = 0; j < 8; ++j)
+          if (((uint32_t(j ^ i)) & keep) == 0u) T[i][j] = w;
+      }
+      double L[8][8], MM[8][8];
+      for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < 8; ++j) {
+          double sl = 0, sm = 0;
+          for (int p = 0; p < 8; ++p)
+            for (int q = 0; q < 8; ++q) {
+              sl += T[p][i] * K[p][q] * T[q][j];
+              sm += T[p][i] * Mm[p][q] * T[q][j];
+            }
+          L[i][j] = sl;
+          MM[i][j] = sm;
+        }
+      for (int lane = 0; lane < 32; ++lane) {
+        const int g = lane >> 2, tq = lane & 3;
+        float* o = out.data() + ((size_t(c) * 18 + t) * 32 + lane) * 4;
+        o[0] = float(L[g][tq]);
+        o[1] = float(L[g][tq + 4]);
+        o[2] = float(MM[g][tq]);
+        o[3] = float(MM[g][tq + 4]);
+      }
+    }
+  return out;
+}
+
+}  // namespace
+
+dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int R, int split, cudaStream_t s) {
+  dg_da* da = A->da;
+  DG_CHECK(A->kind == 0, DG_EINVAL, "mat_mult_multi: scalar operator expected");
+  DG_CHECK(R > 0 && R % kRC == 0, DG_EINVAL, "mat_mult_multi: nrhs must be a positive multiple of 16");
+  DG_CHECK(split == 1 || split == 3, DG_EINVAL, "mat_mult_multi: split must be 1 or 3");
+  DG_CHECK((reinterpret_cast<uintptr_t>(X) & 15) == 0 && (reinterpret_cast<uintptr_t>(Y) & 15) == 0, DG_EINVAL,
+           "mat_mult_multi: X and Y must be 16-byte aligned");
+  static float4* tbls[64] = {};  // one table per device, kept for the process
+  int dev = 0;
+  DG_CUDA(cudaGetDevice(&dev));
+  DG_CHECK(dev >= 0 && dev < 64, DG_EINVAL, "device index");
+  if (!tbls[dev]) {
+    std::vector<float> h = stencil_tables();
+    float4* p = nullptr;
+    DG_CUDA(cudaMalloc(&p, h.size() * sizeof(float)));
+    DG_CUDA(cudaMemcpy(p, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+    tbls[dev] = p;
+  }
+  const float4* tbl = tbls[dev];
+  if (!da->tiles_mr.ntiles) DG_TRY(build_tile_set(da, kMultiTile, da->tiles_mr, s));
+  const TileSet& ts = da->tiles_mr;
+  if (ts.nshared)
+    zero_shared_rows<<<grid_for(ts.nshared * (R / 4), 256, 8), 256, 0, s>>>(ts.shared.p, ts.nshared, R / 4,
+                                                                           reinterpret_cast<float4*>(Y));
+  const float* ca = A->has_coef ? A->coef32.p : nullptr;
+  const float* cb = A->has_coef ? A->coef32.p + da->E : nullptr;
+  const int smem = int(kBufFloats * sizeof(float));
+  static bool attr = false;
+  if (!attr) {
+    DG_CUDA(cudaFuncSetAttribute(mrhs_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    DG_CUDA(cudaFuncSetAttribute(mrhs_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  if (split == 1)
+    mrhs_kernel<1><<<unsigned(ts.ntiles), kMT, smem, s>>>(da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p, ts.nend.p,
+                                                         ts.inc.p, tbl, R, X, Y);
+  else
+    mrhs_kernel<3><<<unsigned(ts.ntiles), kMT, smem, s>>>(da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p, ts.nend.p,
+                                                         ts.inc.p, tbl, R, X, Y);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+}  // namespace dg

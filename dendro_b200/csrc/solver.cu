@@ -184,13 +184,13 @@ __global__ void prolong_add(const uint32_t* __restrict__ ptr, const uint32_t* __
   }
 }
 
-// rc = P^T (b - t) (restriction of the residual, fused)
+// rc += P^T r (restriction; rc zeroed beforehand)
 template <class T>
 __global__ void restrict_residual(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
-                                  const T* __restrict__ val, int64_t Nf, const T* __restrict__ b,
-                                  const T* __restrict__ t, T* __restrict__ rc) {
+                                  const T* __restrict__ val, int64_t Nf, const T* __restrict__ rf,
+                                  T* __restrict__ rc) {
   for (int64_t f = gtid(); f < Nf; f += gstride()) {
-    T r = t ? b[f] - t[f] : b[f];
+    const T r = rf[f];
     if (r == T(0)) continue;
     for (uint32_t k = ptr[f]; k < ptr[f + 1]; ++k) atomicAdd(rc + col[k], val[k] * r);
   }
@@ -201,15 +201,6 @@ template <class T>
 __global__ void jacobi_first(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ dinv, T omega,
                              int64_t n) {
   for (int64_t i = gtid(); i < n; i += gstride()) x[i] = omega * dinv[i] * b[i];
-}
-template <class T>
-__global__ void jacobi_update(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ t,
-                              const T* __restrict__ dinv, T omega, int64_t n) {
-  for (int64_t i = gtid(); i < n; i += gstride()) x[i] += omega * dinv[i] * (b[i] - t[i]);
-}
-template <class T>
-__global__ void residual_kernel(const T* __restrict__ b, const T* __restrict__ t, T* __restrict__ r, int64_t n) {
-  for (int64_t i = gtid(); i < n; i += gstride()) r[i] = b[i] - t[i];
 }
 template <class A, class B>
 __global__ void convert(const A* __restrict__ a, B* __restrict__ b, int64_t n) {
@@ -339,11 +330,12 @@ struct Level {
   std::unique_ptr<dg_da> da;
   std::unique_ptr<dg_mat> A;
   DBuf<double> dinv, x, b, t;
+  DBuf<double> acc;   // shared-node sums of the fused sweeps (kept zero between uses)
   // P to this level from level + 1 (CSR over this level's nodes)
   DBuf<uint32_t> pptr, pcol;
   DBuf<double> pval;
   // FP32 inner V-cycle
-  DBuf<float> dinv32, x32, b32, t32, pval32;
+  DBuf<float> dinv32, x32, b32, t32, pval32, acc32;
   // learned smoother data (finest level): residual, neighbour stats,
   // 1 / element references, hanging share, mean log2 diagonal
   DBuf<float> sm_r, sm_nsum, sm_nmax, sm_refs, sm_hang;
@@ -415,6 +407,8 @@ dg_status setup_level_vectors(Level& L, cudaStream_t s) {
   DG_TRY(L.x.alloc(N));
   DG_TRY(L.b.alloc(N));
   DG_TRY(L.t.alloc(N));
+  DG_TRY(L.acc.alloc(N));
+  DG_CUDA(cudaMemsetAsync(L.acc.p, 0, 8 * N, s));
   DG_TRY(lapmass_diag(L.A.get(), L.dinv.p, s));
   invert<<<grid_for(N, 256), 256, 0, s>>>(L.dinv.p, N);
   DG_CUDA(cudaGetLastError());
@@ -435,6 +429,8 @@ dg_status setup_level_f32(dg_damg* m, Level& L, cudaStream_t s) {
   DG_TRY(L.x32.alloc(N));
   DG_TRY(L.b32.alloc(N));
   DG_TRY(L.t32.alloc(N));
+  DG_TRY(L.acc32.alloc(N));
+  DG_CUDA(cudaMemsetAsync(L.acc32.p, 0, 4 * N, s));
   convert<double, float><<<grid_for(N, 256), 256, 0, s>>>(L.dinv.p, L.dinv32.p, N);
   if (L.pval.n) {
     DG_TRY(L.pval32.alloc(L.pval.n));
@@ -557,27 +553,22 @@ dg_status vcycle(dg_damg* m, size_t l, const double* b, double* x) {
     return DG_OK;
   }
   const double w = m->cfg.omega;
-  // pre-smoothing from a zero initial guess
+  // pre-smoothing from a zero initial guess; the sweeps after the first and
+  // the residual are fused tile-local operator applications
   if (m->cfg.nu_pre > 0) {
     jacobi_first<<<g, 256, 0, s>>>(x, b, L.dinv.p, w, n);
-    for (int k = 1; k < m->cfg.nu_pre; ++k) {
-      DG_TRY(lapmass_apply_f64(L.A.get(), x, L.t.p, s));
-      jacobi_update<<<g, 256, 0, s>>>(x, b, L.t.p, L.dinv.p, w, n);
-    }
-    DG_TRY(lapmass_apply_f64(L.A.get(), x, L.t.p, s));
+    for (int k = 1; k < m->cfg.nu_pre; ++k) DG_TRY(lapmass_smooth_f64(L.A.get(), x, b, L.dinv.p, w, L.acc.p, s));
+    DG_TRY(lapmass_residual_f64(L.A.get(), x, b, L.t.p, L.acc.p, s));
   } else {
     DG_CUDA(cudaMemsetAsync(x, 0, 8 * n, s));
   }
   Level& C = m->lv[l + 1];
   DG_CUDA(cudaMemsetAsync(C.b.p, 0, 8 * C.da->N, s));
-  restrict_residual<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval.p, n, b,
-                                      m->cfg.nu_pre > 0 ? (const double*)L.t.p : (const double*)nullptr, C.b.p);
+  restrict_residual<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval.p, n, m->cfg.nu_pre > 0 ? (const double*)L.t.p : b,
+                                      C.b.p);
   DG_TRY(vcycle(m, l + 1, C.b.p, C.x.p));
   prolong_add<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval.p, n, C.x.p, x);
-  for (int k = 0; k < m->cfg.nu_post; ++k) {
-    DG_TRY(lapmass_apply_f64(L.A.get(), x, L.t.p, s));
-    jacobi_update<<<g, 256, 0, s>>>(x, b, L.t.p, L.dinv.p, w, n);
-  }
+  for (int k = 0; k < m->cfg.nu_post; ++k) DG_TRY(lapmass_smooth_f64(L.A.get(), x, b, L.dinv.p, w, L.acc.p, s));
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }
@@ -599,33 +590,27 @@ dg_status vcycle32(dg_damg* m, size_t l, const float* b, float* x) {
   const float w = float(m->cfg.omega);
   if (m->cfg.nu_pre > 0) {
     jacobi_first<<<g, 256, 0, s>>>(x, b, L.dinv32.p, w, n);
-    for (int k = 1; k < m->cfg.nu_pre; ++k) {
-      DG_TRY(lapmass_apply_f32(L.A.get(), x, L.t32.p, s));
-      jacobi_update<<<g, 256, 0, s>>>(x, b, L.t32.p, L.dinv32.p, w, n);
-    }
-    DG_TRY(lapmass_apply_f32(L.A.get(), x, L.t32.p, s));
+    for (int k = 1; k < m->cfg.nu_pre; ++k) DG_TRY(lapmass_smooth_f32(L.A.get(), x, b, L.dinv32.p, w, L.acc32.p, s));
+    DG_TRY(lapmass_residual_f32(L.A.get(), x, b, L.t32.p, L.acc32.p, s));
   } else {
     DG_CUDA(cudaMemsetAsync(x, 0, 4 * n, s));
   }
   Level& C = m->lv[l + 1];
   DG_CUDA(cudaMemsetAsync(C.b32.p, 0, 4 * C.da->N, s));
-  restrict_residual<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval32.p, n, b,
-                                      m->cfg.nu_pre > 0 ? (const float*)L.t32.p : (const float*)nullptr, C.b32.p);
+  restrict_residual<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval32.p, n, m->cfg.nu_pre > 0 ? (const float*)L.t32.p : b,
+                                      C.b32.p);
   DG_TRY(vcycle32(m, l + 1, C.b32.p, C.x32.p));
   prolong_add<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval32.p, n, C.x32.p, x);
   if (l == 0 && m->mlp && m->mlp_active) {
     const float level_feat = 0.f;  // finest level
     for (int k = 0; k < m->mlp_sweeps; ++k) {
-      DG_TRY(lapmass_apply_f32(L.A.get(), x, L.t32.p, s));
-      residual_kernel<<<g, 256, 0, s>>>(b, (const float*)L.t32.p, L.sm_r.p, n);
+      DG_TRY(lapmass_residual_f32(L.A.get(), x, b, L.sm_r.p, L.acc32.p, s));
       DG_TRY(mlp_smooth_step(m->mlp->params.p, L.da.get(), L.sm_r.p, m->sm_s2.p, L.dinv32.p, L.sm_dlogbar,
                              level_feat, L.sm_hang.p, L.sm_refs.p, L.sm_nsum.p, L.sm_nmax.p, x, s));
     }
   } else {
-    for (int k = 0; k < m->cfg.nu_post; ++k) {
-      DG_TRY(lapmass_apply_f32(L.A.get(), x, L.t32.p, s));
-      jacobi_update<<<g, 256, 0, s>>>(x, b, L.t32.p, L.dinv32.p, w, n);
-    }
+    for (int k = 0; k < m->cfg.nu_post; ++k)
+      DG_TRY(lapmass_smooth_f32(L.A.get(), x, b, L.dinv32.p, w, L.acc32.p, s));
   }
   DG_CUDA(cudaGetLastError());
   return DG_OK;
@@ -968,7 +953,7 @@ dg_status dg_damg_restrict(dg_damg* m, int level, const double* rf, double* rc, 
   }
   if (on_device) DG_CUDA(cudaDeviceSynchronize());
   DG_CUDA(cudaMemsetAsync(pc, 0, 8 * nc, m->s));
-  restrict_residual<<<grid_for(nf, 256), 256, 0, m->s>>>(F.pptr.p, F.pcol.p, F.pval.p, nf, pf, (const double*)nullptr,
+  restrict_residual<<<grid_for(nf, 256), 256, 0, m->s>>>(F.pptr.p, F.pcol.p, F.pval.p, nf, pf,
                                                           pc);
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaStreamSynchronize(m->s));

@@ -150,6 +150,19 @@ int64_t dg_mat_size(const dg_mat* A); /* rows = dof * nodes */
 /* Launch shape of the scalar operator kernel that the autotuner picked on the
  * first application in the given precision ("untuned" before it). */
 const char* dg_mat_kernel_name(const dg_mat* A, int prec);
+/* Number of launch shapes the autotuner chooses from, and a way to fix one
+ * (0 <= variant < count) for a mesh and precision instead of timing them
+ * (no reference counterpart; testing and benchmarking). */
+int dg_mat_kernel_count(void);
+/* Y = A X for nrhs right-hand sides at once (no reference counterpart: the
+ * reference's Jacobian2MatMult, omgNeumann.C:533, takes one Vec).  X and Y are
+ * device arrays, node-major [N][nrhs] FP32, 16-byte aligned; nrhs a multiple
+ * of 16.  The element contraction runs on the tensor cores with TF32 inputs
+ * and FP32 accumulation; split = 3 splits each input into a TF32 high part and
+ * a TF32 remainder (three products, FP32-level accuracy), split = 1 uses one
+ * TF32 product.  Scalar Laplacian + mass operators only. */
+dg_status dg_mat_mult_multi(dg_mat* A, const float* X, float* Y, int nrhs, int split, void* stream);
+dg_status dg_mat_set_kernel(dg_mat* A, int prec, int variant);
 void dg_mat_destroy(dg_mat* A);
 
 /* ------------------------------------------------------------ multigrid --- */

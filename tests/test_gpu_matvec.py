@@ -47,6 +47,24 @@ def test_lapmass_variable_coef_f64(gpu, oracle, name):
     assert rel(y, y_ref) < TOL64
 
 
+@pytest.mark.parametrize("name", ["gauss20k_d10", "lognormal20k_d12", "corner_points_d5"])
+def test_every_launch_shape(gpu, oracle, name):
+    """Each operator kernel the autotuner may pick, fixed in turn, FP64 and FP32."""
+    import torch
+    ref, da = setup(gpu, oracle, name)
+    coef = I.sphere_coefficients(da.elementCenters())
+    x = I.uniform_rhs(ref.N, 5)
+    y_ref = ref.matvec(x, coef)
+    A = gpu.Jacobian2(da, coef)
+    xd = torch.tensor(x, device="cuda")
+    for v in range(A.kernel_count()):
+        A.set_kernel(v, 0)
+        A.set_kernel(v, 1)
+        assert rel(A.mult(xd).cpu().numpy(), y_ref) < TOL64, v
+        y32 = A.mult(xd.float()).double().cpu().numpy()
+        assert rel(y32, y_ref) < TOL32, v
+
+
 def test_lapmass_f32(gpu, oracle):
     import torch
     ref, da = setup(gpu, oracle, "lognormal20k_d12")

@@ -80,8 +80,8 @@ def test_trained_smoother_gain_is_measured(gpu, oracle):
     with and without the learned post-smoother on the same system."""
     from dendro_b200 import inputs as I
     from dendro_b200 import learned as Lrn
-    net, hist = Lrn.train(n_pairs=40, steps_per_pair=2, batch=16384, mesh_points=(15000,), log=None)
-    assert hist[-1] < hist[0]
+    net, hist = Lrn.train(n_pairs=60, steps_per_pair=2, batch=16384, mesh_points=(15000,), log=None)
+    assert np.mean(hist[-10:]) < 0.5 * np.mean(hist[:3])
     pts, d, m = points("lognormal20k_d12")
     bal = oracle.balance(oracle.points2octree(pts, d, m), d)
     b = I.uniform_rhs(len(bal), 9)

@@ -1,0 +1,42 @@
+"""Multi-right-hand-side operator on the tensor cores against the oracle's
+FP64 operator applied column by column."""
+import numpy as np
+import pytest
+
+from dendro_b200 import inputs as I
+from tests.cases import points
+
+pytestmark = pytest.mark.gpu
+
+TOL_SPLIT3 = 2e-6   # three TF32 products: FP32-level, relative 2-norm per column
+TOL_SPLIT1 = 2e-3   # one TF32 product (10-bit mantissa inputs)
+
+
+def setup(gpu, oracle, name):
+    pts, d, m = points(name)
+    bal = oracle.balance(oracle.points2octree(pts, d, m), d)
+    return oracle.Mesh(bal, d), gpu.DA(gpu.Octree.from_octants(bal, d))
+
+
+@pytest.mark.parametrize("name,nrhs,coef", [("lognormal20k_d12", 32, True), ("gauss20k_d10", 16, False),
+                                             ("corner_points_d5", 48, True)])
+def test_multi_rhs_matches_oracle(gpu, oracle, name, nrhs, coef):
+    import torch
+    ref, da = setup(gpu, oracle, name)
+    c = I.sphere_coefficients(da.elementCenters()) if coef else None
+    A = gpu.Jacobian2(da, c)
+    X = np.random.default_rng(6).uniform(-1, 1, (ref.N, nrhs))
+    Yr = np.stack([ref.matvec(X[:, j], c) for j in range(nrhs)], 1)
+    Xd = torch.tensor(X, dtype=torch.float32, device="cuda")
+    for split, tol in ((3, TOL_SPLIT3), (1, TOL_SPLIT1)):
+        Y = A.mult_multi(Xd, split=split).double().cpu().numpy()
+        err = np.linalg.norm(Y - Yr, axis=0) / np.linalg.norm(Yr, axis=0)
+        assert err.max() < tol, (split, err.max())
+
+
+def test_multi_rhs_rejects_bad_shapes(gpu, oracle):
+    import torch
+    ref, da = setup(gpu, oracle, "corner_points_d5")
+    A = gpu.Jacobian2(da)
+    with pytest.raises(gpu.DendroError):
+        A.mult_multi(torch.zeros((ref.N, 20), dtype=torch.float32, device="cuda"))

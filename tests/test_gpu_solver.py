@@ -74,3 +74,19 @@ def test_pcg_precision_and_graph(gpu, oracle, inner_prec, use_graph):
     fm = oracle.Mesh(bal, d)
     for xx in (x, x2):
         assert np.linalg.norm(fm.matvec(xx, coef) - b) <= 1.01e-8 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("inner_prec,tol", [(0, 1e-11), (1, 2e-5)])
+def test_vcycle_matches_oracle(gpu, oracle, inner_prec, tol):
+    """One V(2,2) application (fused tile-local sweeps and residuals on the
+    GPU) against the oracle's V-cycle on the same hierarchy."""
+    import torch
+    from dendro_b200.learned import vcycle
+    pts, d, m = points("lognormal20k_d12")
+    bal = oracle.balance(oracle.points2octree(pts, d, m), d)
+    ref = oracle.DAMG(bal, d, 4)
+    got = gpu.DAMG(gpu.Octree.from_octants(bal, d), nlevels=4, inner_prec=inner_prec, use_graph=False)
+    b = I.uniform_rhs(int(ref.N[0]), 4)
+    zr = ref.vcycle(b)
+    z = vcycle(got, torch.tensor(b, device="cuda")).cpu().numpy()
+    assert np.linalg.norm(z - zr) <= tol * np.linalg.norm(zr)

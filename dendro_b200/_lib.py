@@ -81,6 +81,7 @@ def lib():
         "dg_mat_kernel_count": ([], I),
         "dg_mat_set_kernel": ([P, I, I], I),
         "dg_mat_mult_multi": ([P, P, P, I, I, P], I),
+        "dg_damg_set_tolerances": ([P, C.c_double, I], I),
         "dg_mat_destroy": ([P], None),
         "dg_damg_default_config": ([C.POINTER(DamgConfig)], None),
         "dg_damg_create": ([P, C.POINTER(DamgConfig), PP], I),
@@ -132,7 +133,7 @@ def exported_symbols():
         "dg_mlp_param_count", "dg_mlp_create", "dg_mlp_get_params", "dg_mlp_set_params", "dg_mlp_forward",
         "dg_mlp_gradient", "dg_mlp_train_step", "dg_mlp_destroy", "dg_damg_set_smoother", "dg_damg_features",
         "dg_vec_dot_noalloc", "dg_mat_kernel_count", "dg_mat_set_kernel",
-        "dg_mat_mult_multi",
+        "dg_mat_mult_multi", "dg_damg_set_tolerances",
     ]
 
 

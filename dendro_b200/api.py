@@ -260,6 +260,10 @@ class DAMG:
         check(lib().dg_damg_batch_offsets(self.h, level, ptr(eo), ptr(no)), "damg_batch_offsets")
         return eo, no
 
+    def setTolerances(self, rtol: float, maxit: int = 200) -> None:
+        """KSPSetTolerances: relative residual target and iteration limit."""
+        check(lib().dg_damg_set_tolerances(self.h, rtol, maxit), "damg_set_tolerances")
+
     def level_da(self, l: int) -> DA:
         return DA(handle=lib().dg_damg_level_da(self.h, l), owner=self)
 

@@ -19,6 +19,7 @@ struct TileSet {
   DBuf<uint32_t> nodes;      // [ptr[ntiles]]
   DBuf<uint16_t> nend;       // [ntiles * 8 te]: tile t, node k -> end of its run in inc
   DBuf<uint16_t> inc;        // [ntiles * 8 te]: tile t -> references ordered by node
+  DBuf<uint4> eloc;          // [E] per element the node positions of its 8 vertices (multi-RHS set only)
   DBuf<uint32_t> shared;     // ascending ids of the nodes several tiles reference
   int64_t nshared = 0;
 };

@@ -224,13 +224,18 @@ template <class T, class CT, int MODE>
 __global__ void __launch_bounds__(kLocalTile, 2) lapmass_local_kernel(
     const uint32_t* __restrict__ meta, const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
     const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_nodes,
-    const uint16_t* __restrict__ nend, const uint16_t* __restrict__ inc, const T* x, LocalOut<T> o) {
+    const uint16_t* __restrict__ nend, const uint16_t* __restrict__ inc, uint32_t cap, const T* x, LocalOut<T> o) {
   constexpr int S = 8 * kLocalTile;
-  __shared__ T buf[S];  // per (vertex, element) slot: x in, element result out
+  extern __shared__ __align__(16) unsigned char dg_smem[];
+  T* buf = reinterpret_cast<T*>(dg_smem);                    // [S] per (vertex, element) slot: x in, result out
+  uint16_t* s_inc = reinterpret_cast<uint16_t*>(buf + S);    // [S] the tile's references, grouped by node
+  uint16_t* s_end = s_inc + S;                               // [cap rounded up to 8] run ends
+  uint32_t* s_nodes = reinterpret_cast<uint32_t*>(s_end + ((cap + 7) & ~7u));  // [cap]
   const int tid = threadIdx.x;
   const int64_t tile = blockIdx.x;
   const int64_t e = tile * kLocalTile + tid;
   const bool live = e < E;
+  // independent loads first: the element's record and the tile's lists
   uint32_t m = 0;
   T a = T(1), b = T(1);
   if (live) {
@@ -241,16 +246,19 @@ __global__ void __launch_bounds__(kLocalTile, 2) lapmass_local_kernel(
     }
   }
   const uint32_t p0 = __ldg(tile_ptr + tile), nt = __ldg(tile_ptr + tile + 1) - p0;
-  const uint16_t* tinc = inc + tile * S;
-  const uint16_t* tend = nend + tile * S;
+  reinterpret_cast<uint4*>(s_inc)[tid] = __ldg(reinterpret_cast<const uint4*>(inc + tile * S) + tid);
+  if (uint32_t(tid) < (nt + 7) / 8)
+    reinterpret_cast<uint4*>(s_end)[tid] = __ldg(reinterpret_cast<const uint4*>(nend + tile * S) + tid);
+  for (uint32_t k = tid; k < nt; k += kLocalTile) s_nodes[k] = __ldg(tile_nodes + p0 + k);
+  __syncthreads();
   // x at each node to the slots that reference it
   for (uint32_t k = tid; k < nt; k += kLocalTile) {
-    const uint32_t n = __ldg(tile_nodes + p0 + k) & 0x7fffffffu;
+    const uint32_t n = s_nodes[k] & 0x7fffffffu;
     // the smoothing form updates x in place (other tiles' exclusive nodes),
     // so x is read through the coherent path there
     const T xv = MODE == 1 ? x[n] : __ldg(x + n);
-    const uint32_t end = __ldg(tend + k);
-    for (uint32_t j = k ? __ldg(tend + k - 1) : 0u; j < end; ++j) buf[__ldg(tinc + j)] = xv;
+    const uint32_t end = s_end[k];
+    for (uint32_t j = k ? s_end[k - 1] : 0u; j < end; ++j) buf[s_inc[j]] = xv;
   }
   __syncthreads();
   if (live) {
@@ -271,11 +279,11 @@ __global__ void __launch_bounds__(kLocalTile, 2) lapmass_local_kernel(
   __syncthreads();
   // each node sums its references
   for (uint32_t k = tid; k < nt; k += kLocalTile) {
-    const uint32_t id = __ldg(tile_nodes + p0 + k);
+    const uint32_t id = s_nodes[k];
     const uint32_t n = id & 0x7fffffffu;
-    const uint32_t end = __ldg(tend + k);
+    const uint32_t end = s_end[k];
     T sum = T(0);
-    for (uint32_t j = k ? __ldg(tend + k - 1) : 0u; j < end; ++j) sum += buf[__ldg(tinc + j)];
+    for (uint32_t j = k ? s_end[k - 1] : 0u; j < end; ++j) sum += buf[s_inc[j]];
     if (MODE == 0) {
       if (id & 0x80000000u) atomicAdd(o.y + n, sum);
       else o.y[n] = sum;
@@ -287,6 +295,24 @@ __global__ void __launch_bounds__(kLocalTile, 2) lapmass_local_kernel(
       o.y[n] = o.b[n] - sum;
     }
   }
+}
+
+// Dynamic shared memory of the tile-local kernel for a tile set's largest node count.
+template <class T>
+static int local_smem_bytes(uint32_t cap) {
+  return int(sizeof(T) * 8 * kLocalTile + 2 * 8 * kLocalTile + 2 * ((cap + 7) & ~7u) + 4 * cap);
+}
+
+// Opt in to more than 48 KB of dynamic shared memory once per instantiation.
+template <class T, class CT, int MODE>
+static dg_status local_smem_optin(int smem) {
+  static int granted = 48 * 1024;
+  if (smem > granted) {
+    DG_CUDA(cudaFuncSetAttribute(lapmass_local_kernel<T, CT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem));
+    granted = smem;
+  }
+  return DG_OK;
 }
 
 // Second pass of the smoothing / residual forms over the nodes that several
@@ -384,8 +410,10 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
   if (V.kind == 1) {
     const TileSet& ts = da->tiles;
     LocalOut<T> o{y, nullptr, nullptr, T(0), nullptr};
-    lapmass_local_kernel<T, CT, 0><<<unsigned(ts.ntiles), kLocalTile, 0, s>>>(
-        da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p, ts.nend.p, ts.inc.p, x, o);
+    const int smem = local_smem_bytes<T>(ts.max_nodes);
+    DG_TRY((local_smem_optin<T, CT, 0>(smem)));
+    lapmass_local_kernel<T, CT, 0><<<unsigned(ts.ntiles), kLocalTile, smem, s>>>(
+        da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p, ts.nend.p, ts.inc.p, ts.max_nodes, x, o);
   } else if (V.block == 256 && V.minb == 1) {
     lapmass_kernel<T, CT, 256, 1><<<g, 256, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E, x, y);
   } else if (V.block == 256 && V.minb == 4) {
@@ -484,8 +512,10 @@ static dg_status lapmass_fused(const dg_mat* A, const CT* coef, const T* x, Loca
   const CT* ca = A->has_coef ? coef : nullptr;
   const CT* cb = A->has_coef ? coef + da->E : nullptr;
   const TileSet& ts = da->tiles;
-  lapmass_local_kernel<T, CT, MODE><<<unsigned(ts.ntiles), kLocalTile, 0, s>>>(
-      da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p, ts.nend.p, ts.inc.p, x, o);
+  const int smem = local_smem_bytes<T>(ts.max_nodes);
+  DG_TRY((local_smem_optin<T, CT, MODE>(smem)));
+  lapmass_local_kernel<T, CT, MODE><<<unsigned(ts.ntiles), kLocalTile, smem, s>>>(
+      da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p, ts.nend.p, ts.inc.p, ts.max_nodes, x, o);
   if (ts.nshared)
     local_shared_finish<T, MODE><<<grid_for(ts.nshared, 256, 8), 256, 0, s>>>(ts.shared.p, ts.nshared, o);
   DG_CUDA(cudaGetLastError());

@@ -179,12 +179,14 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* wsum, 
 template <int TE>
 __global__ void __launch_bounds__(TE) tile_lists(const uint32_t* __restrict__ nl, int64_t E, int64_t ntiles,
                                                  uint32_t* __restrict__ tmp, uint32_t* __restrict__ cnt,
-                                                 uint16_t* __restrict__ nend, uint16_t* __restrict__ inc) {
+                                                 uint16_t* __restrict__ nend, uint16_t* __restrict__ inc,
+                                                 uint4* __restrict__ eloc) {
   constexpr int S = 8 * TE;
   constexpr int kPer = 8;  // sorted entries per thread
   static_assert(S <= 4096, "positions are 12-bit");
   extern __shared__ __align__(16) unsigned char tl_smem[];
   uint64_t* key = reinterpret_cast<uint64_t*>(tl_smem);
+  uint16_t* slot = reinterpret_cast<uint16_t*>(key + S);  // position -> node rank
   __shared__ uint32_t wsum[TE / 32];
   const int tid = threadIdx.x;
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -229,11 +231,24 @@ __global__ void __launch_bounds__(TE) tile_lists(const uint32_t* __restrict__ nl
         ++run;
       }
       inc[t * S + j] = uint16_t(kj & 4095u);
+      slot[kj & 4095u] = uint16_t(run - 1);
       const bool last = j + 1 == S || (key[j + 1] >> 12) != (kj >> 12);  // padding keys end every run
       if (last) nend[t * S + run - 1] = uint16_t(j + 1);
     }
     if (tid == 0) cnt[t] = total;
     __syncthreads();
+    if (eloc) {  // per element the node ranks of its eight vertices
+      const int64_t e = t * TE + tid;
+      if (e < E) {
+        uint4 o;
+        o.x = uint32_t(slot[0 * TE + tid]) | (uint32_t(slot[1 * TE + tid]) << 16);
+        o.y = uint32_t(slot[2 * TE + tid]) | (uint32_t(slot[3 * TE + tid]) << 16);
+        o.z = uint32_t(slot[4 * TE + tid]) | (uint32_t(slot[5 * TE + tid]) << 16);
+        o.w = uint32_t(slot[6 * TE + tid]) | (uint32_t(slot[7 * TE + tid]) << 16);
+        eloc[e] = o;
+      }
+      __syncthreads();
+    }
   }
 }
 
@@ -338,14 +353,14 @@ dg_status build_mesh(const dg_octree* tree, dg_da* da, cudaStream_t s) {
 
 template <int TE>
 static dg_status launch_tile_lists(const dg_da* da, int64_t nt, uint32_t* tmp, uint32_t* cnt, uint16_t* nend,
-                                   uint16_t* inc, cudaStream_t s) {
-  const size_t smem = size_t(8) * 8 * TE;
+                                   uint16_t* inc, uint4* eloc, cudaStream_t s) {
+  const size_t smem = size_t(8 + 2) * 8 * TE;
   static bool set = false;
   if (!set && smem > 48 * 1024) {
     DG_CUDA(cudaFuncSetAttribute(tile_lists<TE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   }
   set = true;
-  tile_lists<TE><<<grid_for(nt, TE, 2048 / TE), TE, smem, s>>>(da->nl.p, da->E, nt, tmp, cnt, nend, inc);
+  tile_lists<TE><<<grid_for(nt, TE, 2048 / TE), TE, smem, s>>>(da->nl.p, da->E, nt, tmp, cnt, nend, inc, eloc);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }
@@ -361,8 +376,12 @@ dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s) {
   DG_TRY(cnt.alloc(nt));
   DG_TRY(ts.nend.alloc(nt * S));
   DG_TRY(ts.inc.alloc(nt * S));
-  if (te == kLocalTile) DG_TRY(launch_tile_lists<kLocalTile>(da, nt, tmp.p, cnt.p, ts.nend.p, ts.inc.p, s));
-  else DG_TRY(launch_tile_lists<kMultiTile>(da, nt, tmp.p, cnt.p, ts.nend.p, ts.inc.p, s));
+  if (te == kLocalTile) {
+    DG_TRY(launch_tile_lists<kLocalTile>(da, nt, tmp.p, cnt.p, ts.nend.p, ts.inc.p, nullptr, s));
+  } else {
+    DG_TRY(ts.eloc.alloc(E));
+    DG_TRY(launch_tile_lists<kMultiTile>(da, nt, tmp.p, cnt.p, ts.nend.p, ts.inc.p, ts.eloc.p, s));
+  }
   std::vector<uint32_t> hc(nt);
   DG_CUDA(cudaMemcpyAsync(hc.data(), cnt.p, 4 * nt, cudaMemcpyDeviceToHost, s));
   uint32_t total = 0;

@@ -13,12 +13,14 @@
 // and the reference-cube matrices), stored per MMA lane so that each lane
 // loads its B-fragment entries with one 16-byte load.
 //
-// A CTA owns a tile of kMultiTile elements (its distinct nodes and, grouped by
-// node, the (element, vertex) references to them) and walks the right-hand
-// sides in chunks of 16: x rows go from each node to its references in shared
-// memory, each warp contracts its elements in place, and each node sums its
-// references and leaves with one store (node used by this tile only) or one
-// float4 global atomic (node shared with other tiles).
+// A CTA owns a tile of kMultiTile elements (its distinct nodes and, per
+// element, the positions of its vertices' nodes in that list) and walks the
+// right-hand sides in chunks of 16: the chunk's rows of x at the tile's nodes
+// are staged in shared memory with coalesced float4 loads, each warp reads its
+// elements' MMA fragments from those rows and adds the results into shared
+// rows of y with shared-memory atomics, and each node's row leaves with float4
+// stores (node used by this tile only) or float4 global atomics (node shared
+// with other tiles).
 #include <vector>
 
 #include "dg_internal.h"
@@ -28,20 +30,7 @@ namespace dg {
 namespace {
 
 constexpr int kMT = kMultiTile;     // elements per tile, one thread each
-constexpr int kMS = 8 * kMT;        // references per tile
 constexpr int kRC = 16;             // right-hand sides per chunk (the MMA's M)
-constexpr int kBufFloats = kMS * kRC + 8 * 32 + 32;
-
-static_assert(kMT == 128, "slot_row assumes 128 elements per tile");
-
-// Shared-memory row of reference pos = v * kMT + element: 16 floats per row;
-// each vertex block starts at its own bank offset so that the MMA fragment
-// reads (vertices tq and tq + 4) and writes (vertices 2 tq and 2 tq + 1) of
-// one element hit distinct banks.
-__device__ __forceinline__ int slot_row(int pos) {
-  const int v = pos >> 7;
-  return pos * kRC + v * 32 + 8 * ((v + (v >> 2)) & 3);
-}
 
 __device__ __forceinline__ float elem_hf(uint32_t lev) { return __int_as_float(int(127 + 1 - int(lev)) << 23); }
 
@@ -61,46 +50,54 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
+constexpr int kMThreads = 256;  // 8 warps per tile
+constexpr int kRW = kRC + 4;     // shared row of one node: 16 floats + pad, float4-aligned
+
 // NS = 1: TF32 products.  NS = 3: x = hi + lo for both inputs and
 // D = A_lo B_hi + A_hi B_lo + A_hi B_hi.
 template <int NS>
-__global__ void __launch_bounds__(kMT) mrhs_kernel(const uint32_t* __restrict__ meta, const float* __restrict__ ca,
-                                                   const float* __restrict__ cb, int64_t E,
-                                                   const uint32_t* __restrict__ tile_ptr,
-                                                   const uint32_t* __restrict__ tile_nodes,
-                                                   const uint16_t* __restrict__ nend, const uint16_t* __restrict__ inc,
-                                                   const float4* __restrict__ tbl, int R, const float* __restrict__ X,
-                                                   float* __restrict__ Y) {
-  extern __shared__ __align__(16) float mr_buf[];
+__global__ void __launch_bounds__(kMThreads) mrhs_kernel(const uint32_t* __restrict__ meta,
+                                                         const float* __restrict__ ca, const float* __restrict__ cb,
+                                                         int64_t E, const uint32_t* __restrict__ tile_ptr,
+                                                         const uint32_t* __restrict__ tile_nodes,
+                                                         const uint4* __restrict__ eloc,
+                                                         const float4* __restrict__ tbl, int R, uint32_t cap,
+                                                         const float* __restrict__ X, float* __restrict__ Y) {
+  extern __shared__ __align__(16) float mr_smem[];
+  float* Xs = mr_smem;           // [cap][kRW] x rows of the chunk
+  float* Ys = Xs + cap * kRW;    // [cap][kRW] y rows of the chunk
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, tq = lane & 3;
   const int64_t tile = blockIdx.x;
   const uint32_t p0 = __ldg(tile_ptr + tile), nt = __ldg(tile_ptr + tile + 1) - p0;
-  const uint16_t* tinc = inc + tile * kMS;
-  const uint16_t* tend = nend + tile * kMS;
   for (int r0 = 0; r0 < R; r0 += kRC) {
-    // x rows of the chunk to the references (4 threads per node, float4 each)
-    for (uint32_t i = tid; i < 4 * nt; i += kMT) {
+    for (uint32_t i = tid; i < 4 * nt; i += kMThreads) {
       const uint32_t k = i >> 2, q = i & 3;
       const uint32_t n = __ldg(tile_nodes + p0 + k) & 0x7fffffffu;
-      const float4 xv = __ldg(reinterpret_cast<const float4*>(X + int64_t(n) * R + r0) + q);
-      const uint32_t end = __ldg(tend + k);
-      for (uint32_t j = k ? __ldg(tend + k - 1) : 0u; j < end; ++j)
-        *reinterpret_cast<float4*>(mr_buf + slot_row(__ldg(tinc + j)) + 4 * q) = xv;
+      reinterpret_cast<float4*>(Xs + k * kRW)[q] =
+          __ldg(reinterpret_cast<const float4*>(X + int64_t(n) * R + r0) + q);
+      reinterpret_cast<float4*>(Ys + k * kRW)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
-    for (int el = warp; el < kMT; el += kMT / 32) {
+    for (int el = warp; el < kMT; el += kMThreads / 32) {
       const int64_t e = tile * kMT + el;
       if (e >= E) break;
       const uint32_t m = __ldg(meta + e);
+      const uint4 L = __ldg(eloc + e);
       const float h = elem_hf(meta_lev(m));
       const float a = ca ? __ldg(ca + e) : 1.f, b = cb ? __ldg(cb + e) : 1.f;
       const float f1 = a * h * 0.5f, f2 = b * h * h * h * 0.125f;
       const float4 t = __ldg(tbl + (meta_cnum(m) * 18 + meta_type(m)) * 32 + lane);
       const float bf0 = f1 * t.x + f2 * t.z, bf1 = f1 * t.y + f2 * t.w;
-      float* r_lo = mr_buf + slot_row(tq * kMT + el);        // vertex tq
-      float* r_hi = mr_buf + slot_row((tq + 4) * kMT + el);  // vertex tq + 4
-      const float x0 = r_lo[g], x1 = r_lo[g + 8], x2 = r_hi[g], x3 = r_hi[g + 8];
+      // node positions of vertices tq, tq + 4 (A columns) and 2 tq, 2 tq + 1 (D columns)
+      const uint32_t lo = tq < 2 ? L.x : L.y, hi = tq < 2 ? L.z : L.w;
+      const uint32_t sh = (tq & 1) * 16;
+      const uint32_t s_a = (lo >> sh) & 0xffffu, s_b = (hi >> sh) & 0xffffu;
+      const uint32_t dw = tq == 0 ? L.x : tq == 1 ? L.y : tq == 2 ? L.z : L.w;
+      const uint32_t s_c = dw & 0xffffu, s_d = dw >> 16;
+      const float* xa = Xs + s_a * kRW;
+      const float* xb = Xs + s_b * kRW;
+      const float x0 = xa[g], x1 = xa[g + 8], x2 = xb[g], x3 = xb[g + 8];
       float d[4] = {0.f, 0.f, 0.f, 0.f};
       if (NS == 1) {
         mma_tf32(d, to_tf32(x0), to_tf32(x1), to_tf32(x2), to_tf32(x3), to_tf32(bf0), to_tf32(bf1));
@@ -114,32 +111,22 @@ __global__ void __launch_bounds__(kMT) mrhs_kernel(const uint32_t* __restrict__ 
         mma_tf32(d, ah0, ah1, ah2, ah3, bl0, bl1);
         mma_tf32(d, ah0, ah1, ah2, ah3, bh0, bh1);
       }
-      // D (rhs g / g + 8, vertices 2 tq / 2 tq + 1) back into the element's
-      // rows; every lane's reads above precede the warp-wide mma
-      float* w0 = mr_buf + slot_row(2 * tq * kMT + el);
-      float* w1 = mr_buf + slot_row((2 * tq + 1) * kMT + el);
-      __syncwarp();
-      w0[g] = d[0];
-      w1[g] = d[1];
-      w0[g + 8] = d[2];
-      w1[g + 8] = d[3];
+      // D: rhs g / g + 8 at vertices 2 tq (node s_c) and 2 tq + 1 (node s_d)
+      float* yc = Ys + s_c * kRW;
+      float* yd = Ys + s_d * kRW;
+      atomicAdd(yc + g, d[0]);
+      atomicAdd(yd + g, d[1]);
+      atomicAdd(yc + g + 8, d[2]);
+      atomicAdd(yd + g + 8, d[3]);
     }
     __syncthreads();
-    for (uint32_t i = tid; i < 4 * nt; i += kMT) {
+    for (uint32_t i = tid; i < 4 * nt; i += kMThreads) {
       const uint32_t k = i >> 2, q = i & 3;
       const uint32_t id = __ldg(tile_nodes + p0 + k);
-      const uint32_t end = __ldg(tend + k);
-      float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
-      for (uint32_t j = k ? __ldg(tend + k - 1) : 0u; j < end; ++j) {
-        const float4 v = *reinterpret_cast<const float4*>(mr_buf + slot_row(__ldg(tinc + j)) + 4 * q);
-        sum.x += v.x;
-        sum.y += v.y;
-        sum.z += v.z;
-        sum.w += v.w;
-      }
+      const float4 v = reinterpret_cast<const float4*>(Ys + k * kRW)[q];
       float4* dst = reinterpret_cast<float4*>(Y + int64_t(id & 0x7fffffffu) * R + r0) + q;
-      if (id & 0x80000000u) atomicAdd(dst, sum);
-      else *dst = sum;
+      if (id & 0x80000000u) atomicAdd(dst, v);
+      else *dst = v;
     }
     __syncthreads();
   }
@@ -233,19 +220,21 @@ dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int R, int split
                                                                            reinterpret_cast<float4*>(Y));
   const float* ca = A->has_coef ? A->coef32.p : nullptr;
   const float* cb = A->has_coef ? A->coef32.p + da->E : nullptr;
-  const int smem = int(kBufFloats * sizeof(float));
-  static bool attr = false;
-  if (!attr) {
+  const uint32_t cap = ts.max_nodes;
+  const int smem = int(2 * size_t(cap) * kRW * sizeof(float));
+  DG_CHECK(smem <= 220 * 1024, DG_EINVAL, "mat_mult_multi: tile node count too large");
+  static int granted = 48 * 1024;
+  if (smem > granted) {
     DG_CUDA(cudaFuncSetAttribute(mrhs_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     DG_CUDA(cudaFuncSetAttribute(mrhs_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr = true;
+    granted = smem;
   }
   if (split == 1)
-    mrhs_kernel<1><<<unsigned(ts.ntiles), kMT, smem, s>>>(da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p, ts.nend.p,
-                                                         ts.inc.p, tbl, R, X, Y);
+    mrhs_kernel<1><<<unsigned(ts.ntiles), kMThreads, smem, s>>>(da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p,
+                                                               ts.eloc.p, tbl, R, cap, X, Y);
   else
-    mrhs_kernel<3><<<unsigned(ts.ntiles), kMT, smem, s>>>(da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p, ts.nend.p,
-                                                         ts.inc.p, tbl, R, X, Y);
+    mrhs_kernel<3><<<unsigned(ts.ntiles), kMThreads, smem, s>>>(da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p,
+                                                               ts.eloc.p, tbl, R, cap, X, Y);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }

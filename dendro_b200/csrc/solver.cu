@@ -366,9 +366,18 @@ struct dg_damg {
   DBuf<double> r, z, zold, p, q, part, scal;
   DBuf<float> r32, z32;
   cudaStream_t s = nullptr;
-  cudaGraphExec_t precond_graph = nullptr;
+  // captured preconditioner, one per post-smoother (0 Jacobi, 1 learned), so
+  // that a fallback inside a solve switches graphs instead of capturing again
+  cudaGraphExec_t precond_graph[2] = {nullptr, nullptr};
+  void drop_graphs() {
+    for (cudaGraphExec_t& g : precond_graph)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  }
   ~dg_damg() {
-    if (precond_graph) cudaGraphExecDestroy(precond_graph);
+    drop_graphs();
     if (s) cudaStreamDestroy(s);
   }
 };
@@ -533,10 +542,7 @@ dg_status set_operators(dg_damg* m, const double* coef) {
     DG_TRY(setup_level_vectors(L, s));
     if (m->cfg.inner_prec != DG_PREC_F64) DG_TRY(setup_level_f32(m, L, s));
   }
-  if (m->precond_graph) {  // operators changed: capture again on the next solve
-    cudaGraphExecDestroy(m->precond_graph);
-    m->precond_graph = nullptr;
-  }
+  m->drop_graphs();  // operators changed: capture again on the next solve
   return setup_coarse(m);
 }
 
@@ -633,7 +639,8 @@ dg_status precond_body(dg_damg* m) {
 // graph is captured on the first application).
 dg_status precond(dg_damg* m) {
   if (!m->cfg.use_graph) return precond_body(m);
-  if (!m->precond_graph) {
+  cudaGraphExec_t& ge = m->precond_graph[(m->mlp && m->mlp_active) ? 1 : 0];
+  if (!ge) {
     // one plain application first: operator autotuning and lazy set-up
     // happen outside the capture
     DG_TRY(precond_body(m));
@@ -646,11 +653,11 @@ dg_status precond(dg_damg* m) {
       return st;
     }
     DG_CUDA(e);
-    e = cudaGraphInstantiate(&m->precond_graph, graph, 0);
+    e = cudaGraphInstantiate(&ge, graph, 0);
     cudaGraphDestroy(graph);
     DG_CUDA(e);
   }
-  DG_CUDA(cudaGraphLaunch(m->precond_graph, m->s));
+  DG_CUDA(cudaGraphLaunch(ge, m->s));
   return DG_OK;
 }
 
@@ -896,6 +903,14 @@ dg_status dg_damg_set_lapmass(dg_damg* m, const double* coef) {
   return set_operators(m, coef);
 }
 
+dg_status dg_damg_set_tolerances(dg_damg* m, double rtol, int maxit) {
+  DG_CHECK(m, DG_EINVAL, "damg_set_tolerances: null handle");
+  DG_CHECK(rtol > 0.0 && rtol < 1.0 && maxit > 0, DG_EINVAL, "damg_set_tolerances: rtol in (0,1), maxit > 0");
+  m->cfg.rtol = rtol;
+  m->cfg.maxit = maxit;
+  return DG_OK;
+}
+
 int dg_damg_levels(const dg_damg* m) { return m ? int(m->lv.size()) : 0; }
 
 dg_status dg_damg_level_sizes(const dg_damg* m, int64_t* E, int64_t* N) {
@@ -1010,13 +1025,7 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
   const bool flexible = m->cfg.inner_prec != DG_PREC_F64;
   int fallbacks = 0;
   double prev_rel = 1.0;
-  if (m->mlp && !m->mlp_active) {  // a new solve starts with the learned smoother again
-    m->mlp_active = true;
-    if (m->precond_graph) {
-      cudaGraphExecDestroy(m->precond_graph);
-      m->precond_graph = nullptr;
-    }
-  }
+  if (m->mlp) m->mlp_active = true;  // a new solve starts with the learned smoother again
   if (!conv) {
     DG_TRY(precond(m));
     DG_CUDA(cudaMemcpyAsync(m->p.p, m->z.p, 8 * n, cudaMemcpyDeviceToDevice, s));
@@ -1047,10 +1056,6 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
       if (m->mlp && m->mlp_active && rel > m->mlp_fallback * prev_rel) {
         m->mlp_active = false;
         ++fallbacks;
-        if (m->precond_graph) {
-          cudaGraphExecDestroy(m->precond_graph);
-          m->precond_graph = nullptr;
-        }
       }
       prev_rel = rel;
       if (flexible) DG_CUDA(cudaMemcpyAsync(m->zold.p, m->z.p, 8 * n, cudaMemcpyDeviceToDevice, s));
@@ -1106,10 +1111,7 @@ dg_status dg_damg_set_smoother(dg_damg* m, dg_mlp* mlp, int sweeps, double fallb
   m->mlp_sweeps = sweeps;
   m->mlp_fallback = fallback_ratio;
   m->mlp_active = mlp != nullptr;
-  if (m->precond_graph) {
-    cudaGraphExecDestroy(m->precond_graph);
-    m->precond_graph = nullptr;
-  }
+  m->drop_graphs();
   return DG_OK;
 }
 

@@ -211,6 +211,10 @@ dg_status dg_damg_set_lapmass(dg_damg* m, const double* coef);
 /* DAMGSolve (omg.h:492; omg.C:1121-1169): CG with V(nu_pre, nu_post)
  * preconditioning.  b and x are host arrays when on_device = 0. */
 dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, dg_solve_report* rep);
+/* Relative residual target and iteration limit of later solves (the
+ * reference sets them through PETSc, KSPSetTolerances / -ksp_rtol,
+ * bin/options:50-53). */
+dg_status dg_damg_set_tolerances(dg_damg* m, double rtol, int maxit);
 int dg_damg_levels(const dg_damg* m);
 dg_status dg_damg_level_sizes(const dg_damg* m, int64_t* elements, int64_t* nodes);
 dg_da* dg_damg_level_da(dg_damg* m, int level); /* 0 = finest; owned by m */

@@ -1,11 +1,15 @@
 """Benchmark of the matrix-free octree FEM hot path on B200.
 
-Workload (one GPU): 1,048,576 log-normal points (seed 2, maxDepth 14),
-points2Octree + 2:1 balance on the GPU, the mesh, and the FP64
+Matvec leg (the JSON line's value): 1,048,576 log-normal points (seed 2,
+maxDepth 14), points2Octree + 2:1 balance on the GPU, the mesh, and the FP64
 variable-coefficient operator -div(a grad u) + u with a = 1e4 inside the
-sphere of radius 0.25 about the centre and 1 outside.  A step is one
-operator application (y = A x) over the whole mesh.  The solve leg reports
-the FP64 V(2,2)-preconditioned CG time to ||b - A x|| <= 1e-8 ||b||.
+sphere of radius 0.25 about the centre and 1 outside.  A step is one operator
+application (y = A x) over the whole mesh; the L2 cache is flushed before
+every step.  Extra legs (in the same line): the solve leg on 4,194,304
+log-normal points (seed 4, maxDepth 16) -- time to FP64 relative residual
+1e-8 for the plain FP64 V(2,2)-preconditioned CG and the mixed-precision
+methods -- and a 64-right-hand-side tensor-core leg on 524,288 uniform points
+(seed 5, maxDepth 12).
 
     python bench.py --gpus N --steps K --warmup W [--impl reference]
 
@@ -29,6 +33,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "time to FP64 rel. residual 1e-8 & matvec GDoF/s: chosen vs plain FP64, 1 B200"
 WORKLOAD = "lognormal1m_d14"
+# DRAM bytes (read + write) of one operator launch on the default workload,
+# from one ncu capture per kernel (profiles/lapmass_warp_lognormal1m_d14.md)
+TRAFFIC = {"warp-tile": 332613888 + 21873408}
 
 
 def parse():
@@ -41,6 +48,7 @@ def parse():
     p.add_argument("--scale", type=float, default=1.0, help="fraction of the workload's points (testing)")
     p.add_argument("--no-solve", action="store_true")
     p.add_argument("--no-multi", action="store_true")
+    p.add_argument("--no-batch", action="store_true")
     p.add_argument("--solve-workload", default="lognormal4m_d16")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -174,7 +182,8 @@ def run_dendro(args, rank, world):
     solve = None if args.no_solve else run_solve(dev, args.solve_workload)
     kernel = A.kernel_name(0)
     multi = None if args.no_multi else run_multi(dev, min(args.steps, 50))
-    return dict(multi=multi, kernel=kernel, E=E, N=N, setup_s=setup_s, ms_per_step=ms_per_step, gdofs=gdofs, achieved=achieved, peak=peak,
+    batch = None if args.no_batch else run_batch(dev)
+    return dict(multi=multi, batch=batch, kernel=kernel, E=E, N=N, setup_s=setup_s, ms_per_step=ms_per_step, gdofs=gdofs, achieved=achieved, peak=peak,
                 peak_kind=peak_kind, alg_bytes=alg_bytes, clocks=clk, e2e=e2e, solve=solve, bal=bal, depth=depth,
                 coef=coef, x=x.cpu().numpy(), y=y.cpu().numpy())
 
@@ -233,6 +242,41 @@ def run_solve(dev, workload):
         "mixed_fp32_learned": "mixed_fp32 with the trained MLP post-smoother on the finest level, Jacobi fallback "
                               "when the FP64 residual stalls"}
     return out
+
+
+def run_batch(dev):
+    """Batched leg: 32 independent Gaussian clouds (seeds 100-131, point counts
+    log-uniform in [10K, 500K], maxDepth 12), -Laplace u + u, f = U[-1,1]
+    (seed 7); one concatenated hierarchy solved with the FP32 V-cycle replayed
+    from a CUDA graph (one launch per kernel for all meshes, per-mesh
+    convergence to 1e-8), against the 32 meshes solved one after another."""
+    import torch
+
+    import dendro_b200 as dg
+    from dendro_b200 import inputs as I
+    clouds, depth = I.batch_clouds()
+    trees = [dg.balanceOctree(dg.points2Octree(p, depth, 1)) for p in clouds]
+    m = dg.DAMG(trees, inner_prec=1, use_graph=True)
+    n = int(m.N[0])
+    b = torch.tensor(I.uniform_rhs(n, 7), device=dev)
+    m.solve(b, allow_unconverged=True)
+    reps = [m.solve(b, allow_unconverged=True)[1] for _ in range(2)]
+    rep = min(reps, key=lambda r: r["solve_ms"])
+    _, no = m.batch_offsets(0)
+    seq_ms, seq_its = 0.0, []
+    for i, t in enumerate(trees):
+        mi = dg.DAMG(t, inner_prec=1, use_graph=True)
+        bi = b[int(no[i]):int(no[i + 1])].contiguous()
+        mi.solve(bi, allow_unconverged=True)
+        ri = min((mi.solve(bi, allow_unconverged=True)[1] for _ in range(2)), key=lambda r: r["solve_ms"])
+        seq_ms += ri["solve_ms"]
+        seq_its.append(ri["iterations"])
+        del mi
+    return {"meshes": len(trees), "elements": int(m.E[0]), "nodes": n, "levels": int(m.nlevels),
+            "batched_ms": round(rep["solve_ms"], 3), "batched_iterations": rep["iterations"],
+            "converged": rep["converged"], "rel_residual_max_over_meshes": rep["rel_residual"],
+            "one_by_one_ms": round(seq_ms, 3), "one_by_one_iterations_max": int(max(seq_its)),
+            "speedup_batched": round(seq_ms / rep["solve_ms"], 3)}
 
 
 def run_multi(dev, steps, nrhs=64):
@@ -310,7 +354,9 @@ def main():
                    "elements": r["E"], "nodes": r["N"], "operator": "FP64 -div(a grad u)+u, a=1e4 in r<0.25",
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"independent mesh per GPU x{world}"},
         "roofline": {"bound": "hbm", "achieved": round(r["achieved"], 1), "peak": r["peak"], "unit": "GB/s",
-                     "frac": round(r["achieved"] / r["peak"], 4), "traffic": None,
+                     "frac": round(r["achieved"] / r["peak"], 4),
+                     "traffic": next((v for k, v in TRAFFIC.items() if r["kernel"].startswith(k)), None)
+                     if args.workload == WORKLOAD and args.scale == 1.0 else None,
                      "peak_source": r["peak_kind"], "algorithmic_bytes": int(r["alg_bytes"])},
         "e2e": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r["e2e"].items()},
         "gpu_launches": args.steps,
@@ -318,6 +364,7 @@ def main():
         "solve": r["solve"],
         "matvec_kernel": r["kernel"],
         "multi_rhs": r["multi"],
+        "batch": r["batch"],
         "setup_s": round(r["setup_s"], 3),
     }
     if rank == 0 and world == 1 and not args.no_cpu:

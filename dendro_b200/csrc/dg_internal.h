@@ -20,6 +20,8 @@ struct TileSet {
   DBuf<uint16_t> nend;       // [ntiles * 8 te]: tile t, node k -> end of its run in inc
   DBuf<uint16_t> inc;        // [ntiles * 8 te]: tile t -> references ordered by node
   DBuf<uint4> eloc;          // [E] per element the node positions of its 8 vertices (multi-RHS set only)
+  DBuf<uint8_t> eloc8;       // [8 E] the same as bytes (warp tiles, at most 256 nodes per tile)
+  DBuf<uint8_t> ref8;        // [ntiles * 24 te] warp tiles: sorted positions, node ranks, segmented-sum flags
   DBuf<uint32_t> shared;     // ascending ids of the nodes several tiles reference
   int64_t nshared = 0;
 };
@@ -38,10 +40,10 @@ struct dg_da {
   dg::DBuf<uint32_t> meta;   // [E] packed level / child number / hanging mask / type
   dg::DBuf<uint64_t> ekey;   // [E] element octant keys (embedded space)
   dg::DBuf<uint64_t> nkey;   // [N] node anchor Morton keys (embedded space), sorted
-  // element tiles of the shared-memory operator kernels: the scalar operator's
-  // (kLocalTile elements per tile) and the multi-right-hand-side one's
-  // (kMultiTile elements per tile, built on first use)
-  dg::TileSet tiles, tiles_mr;
+  // element tiles of the shared-memory operator kernels: the scalar warp-tile
+  // operator's (kWarpTile elements per tile, built with the mesh) and the
+  // multi-right-hand-side one's (kMultiTile elements per tile, built on first use)
+  dg::TileSet tiles_w, tiles_mr;
   // operator launch shape picked by the autotuner on first use (-1: not yet)
   int tuned_f64 = -1, tuned_f32 = -1;
 };
@@ -65,10 +67,10 @@ struct dg_mat {
 
 namespace dg {
 
-// elements per tile of the scalar shared-memory operator kernel (one thread
-// each) and of the multi-right-hand-side kernel
-constexpr int kLocalTile = 512;
+// elements per tile of the multi-right-hand-side kernel and of the scalar
+// warp-tile kernel (one lane each)
 constexpr int kMultiTile = 128;
+constexpr int kWarpTile = 32;
 
 // ---- learned smoother (mlp.cu): 6 -> 64 -> 64 -> 1, packed FP32 parameters ----
 constexpr int kMlpIn = 6;
@@ -105,7 +107,7 @@ dg_status coarsen_octree(const dg_octree* in, dg_octree* out, cudaStream_t s);
 
 // ---- mesh (mesh.cu) ----
 dg_status build_mesh(const dg_octree* tree, dg_da* da, cudaStream_t s);
-dg_status build_tiles(dg_da* da, cudaStream_t s);  // da->tiles (kLocalTile)
+dg_status build_tiles(dg_da* da, cudaStream_t s);  // da->tiles_w (kWarpTile)
 dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s);
 // Hanging mask of element type t (0..17) for child number c
 // (include/oda/cnumEtypes.h:19-229).
@@ -115,9 +117,9 @@ uint32_t etype_mask(int c, int t);
 dg_status lapmass_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStream_t s);
 dg_status lapmass_diag(const dg_mat* A, double* d, cudaStream_t s);
-// Fused tile-local forms: one damped-Jacobi sweep x <- x + omega dinv (b - A x)
-// in place, and the residual r = b - A x.  acc is an N-vector that must be
-// zero on entry and is zero again on return (sums of the shared nodes).
+// One damped-Jacobi sweep x <- x + omega dinv (b - A x) in place, and the
+// residual r = b - A x: the warp-tile operator into acc (an N-vector that must
+// be zero on entry and is zero again on return), then one elementwise pass.
 dg_status lapmass_smooth_f64(const dg_mat* A, double* x, const double* b, const double* dinv, double omega,
                              double* acc, cudaStream_t s);
 dg_status lapmass_smooth_f32(const dg_mat* A, float* x, const float* b, const float* dinv, float omega, float* acc,

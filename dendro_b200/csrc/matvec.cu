@@ -199,132 +199,162 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_kernel(const uint32_t* __
   }
 }
 
-// Output of the tile-local kernel.  MODE 0: y = A x (y zeroed beforehand for
-// the shared nodes).  MODE 1: one damped-Jacobi sweep in place, y = x <- x +
-// omega dinv (b - A x).  MODE 2: residual y = r = b - A x.  In modes 1 and 2
-// the exclusive nodes are finished in the kernel and the shared ones collect
-// their sums in acc (zero on entry) for local_shared_finish.
+// Jacobi update and residual from an operator application t = A x, which
+// they read and zero again (t stays zero between uses, as the warp-tile
+// kernel's atomics need).
 template <class T>
-struct LocalOut {
-  T* y;
-  const T* b;
-  const T* dinv;
-  T omega;
-  T* acc;
+__global__ void jacobi_from(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ dinv,
+                            T* __restrict__ t, T omega, int64_t n) {
+  #pragma unroll 4
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    const T ti = t[i];
+    t[i] = T(0);
+    x[i] += omega * dinv[i] * (b[i] - ti);
+  }
+}
+template <class T>
+__global__ void residual_from(const T* __restrict__ b, T* __restrict__ t, T* __restrict__ r, int64_t n) {
+  #pragma unroll 4
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    const T ti = t[i];
+    t[i] = T(0);
+    r[i] = b[i] - ti;
+  }
+}
+
+// Warp-tile variant: each warp owns tiles of kWarpTile consecutive elements
+// (one per lane) with warp-private shared buffers, so the phases of a tile
+// synchronise with __syncwarp only and the warps of an SM progress
+// independently.  Per tile: x at the tile's nodes is staged once; each lane
+// applies its element operator, reading x through its 8 node ranks (one
+// 8-byte load), and writes its 8 results by (vertex, element) position; the
+// tile's 256 references, sorted by node, are then summed 8 consecutive ones
+// per lane, following per-reference flags built with the mesh (start a sum,
+// let it leave, as a store or an atomic).  A sum leaves with a store when the
+// node's whole run lies in one lane and no other tile uses the node, else
+// with an FP64 global atomic (y is zeroed first).
+constexpr int kWarpCta = 8;  // warps per CTA
+
+// bytes j <- j ^ c of a vertex-indexed byte vector (8 node ranks in a uint2)
+__device__ __forceinline__ uint2 xor_perm_bytes(uint2 r, uint32_t c) {
+  if (c & 1u) {
+    r.x = __byte_perm(r.x, 0, 0x2301);
+    r.y = __byte_perm(r.y, 0, 0x2301);
+  }
+  if (c & 2u) {
+    r.x = __byte_perm(r.x, 0, 0x1032);
+    r.y = __byte_perm(r.y, 0, 0x1032);
+  }
+  if (c & 4u) {
+    const uint32_t t = r.x;
+    r.x = r.y;
+    r.y = t;
+  }
+  return r;
+}
+__device__ __forceinline__ uint32_t byte_of(uint2 r, int j) { return ((j < 4 ? r.x : r.y) >> ((j & 3) * 8)) & 0xffu; }
+
+// Per-lane record of one tile: the lane's element and its 8 sorted references.
+template <class T>
+struct WarpTileLoad {
+  uint32_t m, p0, nt;
+  uint2 L, pp, rr, ff;
+  T a, b;
 };
-
-// Tile-local variant: a CTA of kLocalTile threads owns one tile of kLocalTile
-// consecutive elements (one each), its distinct nodes and, per node, the
-// tile's (element, vertex) references to it.  The node-parallel phases copy x
-// from each node to its references in shared memory and, after the element
-// phase, sum each node's references; a node's sum leaves with one store (node
-// used by this tile only) or one global atomic (node shared with other
-// tiles).  No shared-memory atomics and two barriers per tile.
-template <class T, class CT, int MODE>
-__global__ void __launch_bounds__(kLocalTile, 2) lapmass_local_kernel(
-    const uint32_t* __restrict__ meta, const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
-    const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_nodes,
-    const uint16_t* __restrict__ nend, const uint16_t* __restrict__ inc, uint32_t cap, const T* x, LocalOut<T> o) {
-  constexpr int S = 8 * kLocalTile;
-  extern __shared__ __align__(16) unsigned char dg_smem[];
-  T* buf = reinterpret_cast<T*>(dg_smem);                    // [S] per (vertex, element) slot: x in, result out
-  uint16_t* s_inc = reinterpret_cast<uint16_t*>(buf + S);    // [S] the tile's references, grouped by node
-  uint16_t* s_end = s_inc + S;                               // [cap rounded up to 8] run ends
-  uint32_t* s_nodes = reinterpret_cast<uint32_t*>(s_end + ((cap + 7) & ~7u));  // [cap]
-  const int tid = threadIdx.x;
-  const int64_t tile = blockIdx.x;
-  const int64_t e = tile * kLocalTile + tid;
-  const bool live = e < E;
-  // independent loads first: the element's record and the tile's lists
-  uint32_t m = 0;
-  T a = T(1), b = T(1);
-  if (live) {
-    m = __ldg(meta + e);
+template <class T, class CT>
+__device__ __forceinline__ void load_warp_tile(WarpTileLoad<T>& d, int64_t t, int lane, int64_t E,
+                                               const uint32_t* __restrict__ meta, const CT* __restrict__ ca,
+                                               const CT* __restrict__ cb, const uint32_t* __restrict__ tile_ptr,
+                                               const uint2* __restrict__ eloc8, const uint8_t* __restrict__ ref8) {
+  constexpr int S = 8 * kWarpTile;
+  const int64_t e = t * kWarpTile + lane;
+  d.m = 0;
+  d.L = make_uint2(0, 0);
+  d.a = T(1);
+  d.b = T(1);
+  if (e < E) {
+    d.m = __ldg(meta + e);
+    d.L = __ldg(eloc8 + e);
     if (ca) {
-      a = T(__ldg(ca + e));
-      b = T(__ldg(cb + e));
+      d.a = T(__ldg(ca + e));
+      d.b = T(__ldg(cb + e));
     }
   }
-  const uint32_t p0 = __ldg(tile_ptr + tile), nt = __ldg(tile_ptr + tile + 1) - p0;
-  reinterpret_cast<uint4*>(s_inc)[tid] = __ldg(reinterpret_cast<const uint4*>(inc + tile * S) + tid);
-  if (uint32_t(tid) < (nt + 7) / 8)
-    reinterpret_cast<uint4*>(s_end)[tid] = __ldg(reinterpret_cast<const uint4*>(nend + tile * S) + tid);
-  for (uint32_t k = tid; k < nt; k += kLocalTile) s_nodes[k] = __ldg(tile_nodes + p0 + k);
-  __syncthreads();
-  // x at each node to the slots that reference it
-  for (uint32_t k = tid; k < nt; k += kLocalTile) {
-    const uint32_t n = s_nodes[k] & 0x7fffffffu;
-    // the smoothing form updates x in place (other tiles' exclusive nodes),
-    // so x is read through the coherent path there
-    const T xv = MODE == 1 ? x[n] : __ldg(x + n);
-    const uint32_t end = s_end[k];
-    for (uint32_t j = k ? s_end[k - 1] : 0u; j < end; ++j) buf[s_inc[j]] = xv;
-  }
-  __syncthreads();
-  if (live) {
-    const uint32_t c = meta_cnum(m);
-    const T h = elem_h<T>(meta_lev(m));
-    const T f1 = a * h * T(0.5), f2 = b * h * h * h * T(0.125);
-    // work in the child-number frame: w[j] is vertex j ^ c
-    T w[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) w[j] = buf[(uint32_t(j) ^ c) * kLocalTile + tid];
-    const uint32_t mp = xor_perm_mask(meta_mask(m), c);
-    if (mp) interp_frame(w, mp);
-    lapmass_ref(w, f1, f2);  // the reference-cube operator is invariant under the relabelling
-    if (mp) scatter_frame(w, mp);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) buf[(uint32_t(j) ^ c) * kLocalTile + tid] = w[j];
-  }
-  __syncthreads();
-  // each node sums its references
-  for (uint32_t k = tid; k < nt; k += kLocalTile) {
-    const uint32_t id = s_nodes[k];
-    const uint32_t n = id & 0x7fffffffu;
-    const uint32_t end = s_end[k];
-    T sum = T(0);
-    for (uint32_t j = k ? s_end[k - 1] : 0u; j < end; ++j) sum += buf[s_inc[j]];
-    if (MODE == 0) {
-      if (id & 0x80000000u) atomicAdd(o.y + n, sum);
-      else o.y[n] = sum;
-    } else if (id & 0x80000000u) {
-      atomicAdd(o.acc + n, sum);
-    } else if (MODE == 1) {
-      o.y[n] = o.y[n] + o.omega * o.dinv[n] * (o.b[n] - sum);
+  const uint8_t* tr = ref8 + t * 3 * S;
+  d.pp = __ldg(reinterpret_cast<const uint2*>(tr) + lane);
+  d.rr = __ldg(reinterpret_cast<const uint2*>(tr + S) + lane);
+  d.ff = __ldg(reinterpret_cast<const uint2*>(tr + 2 * S) + lane);
+  d.p0 = __ldg(tile_ptr + t);
+  d.nt = __ldg(tile_ptr + t + 1) - d.p0;
+}
+
+// MINB: CTAs per SM the register budget is set for.  PF: load the next
+// tile's records before working on the current one (more registers, the
+// loads' latency hidden behind the current tile).
+template <class T, class CT, int MINB, bool PF>
+__global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_kernel(
+    const uint32_t* __restrict__ meta, const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
+    int64_t ntiles, const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_nodes,
+    const uint2* __restrict__ eloc8, const uint8_t* __restrict__ ref8, const T* __restrict__ x,
+    T* __restrict__ y) {
+  constexpr int S = 8 * kWarpTile;
+  __shared__ T s_x[kWarpCta][S];  // x at the tile's nodes by rank, then element results by position
+  __shared__ uint32_t s_nodes[kWarpCta][S];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  T* sx = s_x[w];
+  uint32_t* sn = s_nodes[w];
+  const int64_t nw = int64_t(gridDim.x) * kWarpCta;
+  int64_t t = blockIdx.x * int64_t(kWarpCta) + w;
+  WarpTileLoad<T> cur, nxt;
+  if (PF && t < ntiles) load_warp_tile<T, CT>(cur, t, lane, E, meta, ca, cb, tile_ptr, eloc8, ref8);
+  for (; t < ntiles; t += nw) {
+    if (PF) {
+      if (t + nw < ntiles) load_warp_tile<T, CT>(nxt, t + nw, lane, E, meta, ca, cb, tile_ptr, eloc8, ref8);
     } else {
-      o.y[n] = o.b[n] - sum;
+      load_warp_tile<T, CT>(cur, t, lane, E, meta, ca, cb, tile_ptr, eloc8, ref8);
     }
-  }
-}
-
-// Dynamic shared memory of the tile-local kernel for a tile set's largest node count.
-template <class T>
-static int local_smem_bytes(uint32_t cap) {
-  return int(sizeof(T) * 8 * kLocalTile + 2 * 8 * kLocalTile + 2 * ((cap + 7) & ~7u) + 4 * cap);
-}
-
-// Opt in to more than 48 KB of dynamic shared memory once per instantiation.
-template <class T, class CT, int MODE>
-static dg_status local_smem_optin(int smem) {
-  static int granted = 48 * 1024;
-  if (smem > granted) {
-    DG_CUDA(cudaFuncSetAttribute(lapmass_local_kernel<T, CT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 smem));
-    granted = smem;
-  }
-  return DG_OK;
-}
-
-// Second pass of the smoothing / residual forms over the nodes that several
-// tiles share, once every tile has added its part to acc (acc is left zero).
-template <class T, int MODE>
-__global__ void local_shared_finish(const uint32_t* __restrict__ list, int64_t ns, LocalOut<T> o) {
-  for (int64_t i = gtid(); i < ns; i += gstride()) {
-    const uint32_t n = list[i];
-    const T a = o.acc[n];
-    o.acc[n] = T(0);
-    if (MODE == 1) o.y[n] += o.omega * o.dinv[n] * (o.b[n] - a);
-    else o.y[n] = o.b[n] - a;
+    const bool live = t * kWarpTile + lane < E;
+    for (uint32_t k = lane; k < cur.nt; k += 32) {
+      const uint32_t id = __ldg(tile_nodes + cur.p0 + k);
+      sn[k] = id;
+      sx[k] = __ldg(x + (id & 0x7fffffffu));
+    }
+    __syncwarp();
+    T wv[8];
+    const uint32_t c = meta_cnum(cur.m);
+    if (live) {
+      const T h = elem_h<T>(meta_lev(cur.m));
+      const T f1 = cur.a * h * T(0.5), f2 = cur.b * h * h * h * T(0.125);
+      const uint2 Lf = xor_perm_bytes(cur.L, c);  // child-number frame: byte j is vertex j ^ c
+#pragma unroll
+      for (int j = 0; j < 8; ++j) wv[j] = sx[byte_of(Lf, j)];
+      const uint32_t mp = xor_perm_mask(meta_mask(cur.m), c);
+      if (mp) interp_frame(wv, mp);
+      lapmass_ref(wv, f1, f2);
+      if (mp) scatter_frame(wv, mp);
+    }
+    __syncwarp();  // every lane has read x: its buffer now takes the results
+    if (live) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) sx[(uint32_t(j) ^ c) * kWarpTile + lane] = wv[j];
+    }
+    __syncwarp();
+    T sum = T(0);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const uint32_t f = byte_of(cur.ff, q);
+      if (f & 8u) {
+        const T v = sx[byte_of(cur.pp, q)];
+        sum = (f & 1u) ? v : sum + v;
+        if (f & 2u) {
+          const uint32_t id = sn[byte_of(cur.rr, q)];
+          if (f & 4u) y[id] = sum;  // the node's whole sum, node used by this tile only
+          else atomicAdd(y + (id & 0x7fffffffu), sum);
+        }
+      }
+    }
+    __syncwarp();
+    if (PF) cur = nxt;
   }
 }
 
@@ -384,20 +414,22 @@ __global__ void lapmass_dense_kernel(const uint32_t* __restrict__ nl, const uint
 }  // namespace
 
 // Launch shapes tried by the autotuner: one thread per element with
-// different block sizes / register caps / grid sizes, and the tile-local
+// different block sizes / register caps / grid sizes, and the warp-tile
 // shared-memory form.  The first application on a mesh times each once
 // (after one untimed launch) and keeps the fastest for that mesh and
 // precision; DG_MATVEC_KERNEL=<index> forces one (testing).
 struct MatvecVariant {
   int block, per_sm;  // threads per CTA, CTAs per SM in the grid (0: one thread per element)
-  int kind;           // 0 atomic (BLOCK, MINB), 1 tile-local
+  int kind;           // 0 atomic (BLOCK, MINB), 2 warp-tile, 3 warp-tile with prefetch
   int minb;
   const char* name;
 };
 constexpr MatvecVariant kVariants[] = {
     {256, 8, 0, 1, "atomic b256 grid 8/SM"},  {256, 0, 0, 1, "atomic b256 grid E"},
     {256, 8, 0, 4, "atomic b256 minB4"},      {128, 16, 0, 8, "atomic b128 minB8"},
-    {512, 4, 0, 2, "atomic b512 minB2"},      {kLocalTile, 0, 1, 2, "tile-local 512 elems"},
+    {512, 4, 0, 2, "atomic b512 minB2"},
+    {32 * kWarpCta, 5, 2, 5, "warp-tile 32 elems, 5 CTAs/SM"}, {32 * kWarpCta, 6, 2, 6, "warp-tile 32 elems, 6 CTAs/SM"},
+    {32 * kWarpCta, 4, 3, 4, "warp-tile 32 elems, 4 CTAs/SM, next tile prefetched"},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 
@@ -407,13 +439,19 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
   const MatvecVariant& V = kVariants[v];
   const unsigned g = V.per_sm ? grid_for(da->E, V.block, V.per_sm)
                               : unsigned((da->E + V.block - 1) / V.block > 0 ? (da->E + V.block - 1) / V.block : 1);
-  if (V.kind == 1) {
-    const TileSet& ts = da->tiles;
-    LocalOut<T> o{y, nullptr, nullptr, T(0), nullptr};
-    const int smem = local_smem_bytes<T>(ts.max_nodes);
-    DG_TRY((local_smem_optin<T, CT, 0>(smem)));
-    lapmass_local_kernel<T, CT, 0><<<unsigned(ts.ntiles), kLocalTile, smem, s>>>(
-        da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p, ts.nend.p, ts.inc.p, ts.max_nodes, x, o);
+  if (V.kind >= 2) {
+    const TileSet& ts = da->tiles_w;
+    const unsigned gw = grid_for(ts.ntiles * 32, 32 * kWarpCta, V.per_sm);
+    const uint2* e8 = reinterpret_cast<const uint2*>(ts.eloc8.p);
+    if (V.kind == 3)
+      lapmass_warp_kernel<T, CT, 4, true><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
+                                                                      ts.nodes.p, e8, ts.ref8.p, x, y);
+    else if (V.minb == 6)
+      lapmass_warp_kernel<T, CT, 6, false><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles,
+                                                                       ts.ptr.p, ts.nodes.p, e8, ts.ref8.p, x, y);
+    else
+      lapmass_warp_kernel<T, CT, 5, false><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles,
+                                                                       ts.ptr.p, ts.nodes.p, e8, ts.ref8.p, x, y);
   } else if (V.block == 256 && V.minb == 1) {
     lapmass_kernel<T, CT, 256, 1><<<g, 256, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E, x, y);
   } else if (V.block == 256 && V.minb == 4) {
@@ -433,27 +471,39 @@ static int forced_variant() {
     const char* e = getenv("DG_MATVEC_KERNEL");
     v = -1;
     if (e && *e) {
-      if (!strcmp(e, "atomic")) v = 0;
-      else if (!strcmp(e, "local")) v = kNumVariants - 1;
-      else v = atoi(e) % kNumVariants;
+      const int kind = !strcmp(e, "atomic") ? 0 : !strcmp(e, "warp") ? 2 : -1;
+      if (kind >= 0) {
+        for (int i = kNumVariants - 1; i >= 0; --i)
+          if (kVariants[i].kind == kind) v = i;
+      } else {
+        v = atoi(e) % kNumVariants;
+      }
     }
   }
   return v;
 }
 
+// The launch shape for a mesh and precision: the forced one, the tuned one,
+// or -- on first use outside a stream capture -- tune now: one untimed launch,
+// then per variant the best of two timed launches, each after overwriting a
+// buffer larger than L2 so that the mesh streams from HBM as it does for
+// meshes larger than L2.  y is used as scratch and left zero.  Inside a
+// capture an untuned mesh gets the default warp-tile shape.
+constexpr int kDefaultVariant = 5;  // "warp-tile 32 elems, 5 CTAs/SM"
 template <class T, class CT>
-static dg_status lapmass_launch(const dg_da* da, int& choice, const CT* ca, const CT* cb, const T* x, T* y,
-                                cudaStream_t s) {
-  DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
-  if (forced_variant() >= 0) return launch_variant<T, CT>(forced_variant(), da, ca, cb, x, y, s);
+static dg_status pick_variant(const dg_da* da, int& choice, const CT* ca, const CT* cb, const T* x, T* y,
+                              cudaStream_t s, int* v_out) {
+  if (forced_variant() >= 0) {
+    *v_out = forced_variant();
+    return DG_OK;
+  }
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   DG_CUDA(cudaStreamIsCapturing(s, &cap));
-  if (choice < 0 && cap != cudaStreamCaptureStatusNone)  // no timing inside a graph capture
-    return launch_variant<T, CT>(0, da, ca, cb, x, y, s);
+  if (choice < 0 && cap != cudaStreamCaptureStatusNone) {  // no timing inside a graph capture
+    *v_out = kDefaultVariant;
+    return DG_OK;
+  }
   if (choice < 0) {
-    // autotune: one untimed launch, then per variant the best of two timed
-    // launches, each after overwriting a buffer larger than L2 so that the
-    // mesh streams from HBM as it does for meshes larger than L2
     cudaEvent_t e0, e1;
     DG_CUDA(cudaEventCreate(&e0));
     DG_CUDA(cudaEventCreate(&e1));
@@ -461,10 +511,11 @@ static dg_status lapmass_launch(const dg_da* da, int& choice, const CT* ca, cons
     const int64_t flush_bytes = int64_t(192) << 20;
     DG_TRY(flush.alloc(flush_bytes));
     float best = 1e30f;
-    int bi = 0;
+    int bi = kDefaultVariant;
+    DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
     DG_TRY((launch_variant<T, CT>(0, da, ca, cb, x, y, s)));
     for (int v = 0; v < kNumVariants; ++v) {
-      if (kVariants[v].kind == 1 && da->tiles.ntiles == 0) continue;
+      if (kVariants[v].kind >= 2 && da->tiles_w.ntiles == 0) continue;
       for (int trial = 0; trial < 2; ++trial) {
         DG_CUDA(cudaMemsetAsync(flush.p, trial + 1, flush_bytes, s));
         DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
@@ -485,7 +536,18 @@ static dg_status lapmass_launch(const dg_da* da, int& choice, const CT* ca, cons
     choice = bi;
     DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
   }
-  return launch_variant<T, CT>(choice, da, ca, cb, x, y, s);
+  *v_out = choice;
+  return DG_OK;
+}
+
+// y = A x with the mesh's launch shape.
+template <class T, class CT>
+static dg_status lapmass_launch(dg_da* da, int& choice, const CT* ca, const CT* cb, const T* x, T* y,
+                                cudaStream_t s) {
+  int v = 0;
+  DG_TRY((pick_variant<T, CT>(da, choice, ca, cb, x, y, s, &v)));
+  DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
+  return launch_variant<T, CT>(v, da, ca, cb, x, y, s);
 }
 
 int matvec_variant_count() { return kNumVariants; }
@@ -506,37 +568,53 @@ dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStrea
   return lapmass_launch<float, float>(da, da->tuned_f32, ca, cb, x, y, s);
 }
 
-template <class T, class CT, int MODE>
-static dg_status lapmass_fused(const dg_mat* A, const CT* coef, const T* x, LocalOut<T> o, cudaStream_t s) {
-  const dg_da* da = A->da;
+// t = A x into a zero-kept accumulator (every launch shape only adds into y
+// or stores whole sums, so no memset), with the mesh's tuned shape.
+template <class T, class CT>
+static dg_status apply_to_zeroed(const dg_mat* A, const CT* coef, const T* x, T* t, cudaStream_t s) {
+  dg_da* da = A->da;
   const CT* ca = A->has_coef ? coef : nullptr;
   const CT* cb = A->has_coef ? coef + da->E : nullptr;
-  const TileSet& ts = da->tiles;
-  const int smem = local_smem_bytes<T>(ts.max_nodes);
-  DG_TRY((local_smem_optin<T, CT, MODE>(smem)));
-  lapmass_local_kernel<T, CT, MODE><<<unsigned(ts.ntiles), kLocalTile, smem, s>>>(
-      da->meta.p, ca, cb, da->E, ts.ptr.p, ts.nodes.p, ts.nend.p, ts.inc.p, ts.max_nodes, x, o);
-  if (ts.nshared)
-    local_shared_finish<T, MODE><<<grid_for(ts.nshared, 256, 8), 256, 0, s>>>(ts.shared.p, ts.nshared, o);
+  int& choice = sizeof(T) == 8 ? da->tuned_f64 : da->tuned_f32;
+  int v = 0;
+  DG_TRY((pick_variant<T, CT>(da, choice, ca, cb, x, t, s, &v)));
+  return launch_variant<T, CT>(v, da, ca, cb, x, t, s);
+}
+
+template <class T, class CT>
+static dg_status smooth_sweep(const dg_mat* A, const CT* coef, T* x, const T* b, const T* dinv, T omega, T* t,
+                              cudaStream_t s) {
+  DG_TRY((apply_to_zeroed<T, CT>(A, coef, x, t, s)));
+  const int64_t n = A->da->N;
+  jacobi_from<T><<<grid_for(n, 256, 16), 256, 0, s>>>(x, b, dinv, t, omega, n);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+template <class T, class CT>
+static dg_status residual(const dg_mat* A, const CT* coef, const T* x, const T* b, T* r, T* t, cudaStream_t s) {
+  DG_TRY((apply_to_zeroed<T, CT>(A, coef, x, t, s)));
+  const int64_t n = A->da->N;
+  residual_from<T><<<grid_for(n, 256, 16), 256, 0, s>>>(b, t, r, n);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }
 
 dg_status lapmass_smooth_f64(const dg_mat* A, double* x, const double* b, const double* dinv, double omega,
                              double* acc, cudaStream_t s) {
-  return lapmass_fused<double, double, 1>(A, A->coef.p, x, LocalOut<double>{x, b, dinv, omega, acc}, s);
+  return smooth_sweep<double, double>(A, A->coef.p, x, b, dinv, omega, acc, s);
 }
 dg_status lapmass_smooth_f32(const dg_mat* A, float* x, const float* b, const float* dinv, float omega, float* acc,
                              cudaStream_t s) {
-  return lapmass_fused<float, float, 1>(A, A->coef32.p, x, LocalOut<float>{x, b, dinv, omega, acc}, s);
+  return smooth_sweep<float, float>(A, A->coef32.p, x, b, dinv, omega, acc, s);
 }
 dg_status lapmass_residual_f64(const dg_mat* A, const double* x, const double* b, double* r, double* acc,
                                cudaStream_t s) {
-  return lapmass_fused<double, double, 2>(A, A->coef.p, x, LocalOut<double>{r, b, nullptr, 0.0, acc}, s);
+  return residual<double, double>(A, A->coef.p, x, b, r, acc, s);
 }
 dg_status lapmass_residual_f32(const dg_mat* A, const float* x, const float* b, float* r, float* acc,
                                cudaStream_t s) {
-  return lapmass_fused<float, float, 2>(A, A->coef32.p, x, LocalOut<float>{r, b, nullptr, 0.f, acc}, s);
+  return residual<float, float>(A, A->coef32.p, x, b, r, acc, s);
 }
 
 dg_status lapmass_diag(const dg_mat* A, double* d, cudaStream_t s) {

@@ -180,7 +180,7 @@ template <int TE>
 __global__ void __launch_bounds__(TE) tile_lists(const uint32_t* __restrict__ nl, int64_t E, int64_t ntiles,
                                                  uint32_t* __restrict__ tmp, uint32_t* __restrict__ cnt,
                                                  uint16_t* __restrict__ nend, uint16_t* __restrict__ inc,
-                                                 uint4* __restrict__ eloc) {
+                                                 uint4* __restrict__ eloc, uint8_t* __restrict__ eloc8) {
   constexpr int S = 8 * TE;
   constexpr int kPer = 8;  // sorted entries per thread
   static_assert(S <= 4096, "positions are 12-bit");
@@ -249,6 +249,18 @@ __global__ void __launch_bounds__(TE) tile_lists(const uint32_t* __restrict__ nl
       }
       __syncthreads();
     }
+    if (eloc8) {  // the same as bytes (tiles of at most 256 nodes)
+      const int64_t e = t * TE + tid;
+      if (e < E) {
+        uint2 o;
+        o.x = uint32_t(slot[0 * TE + tid]) | (uint32_t(slot[1 * TE + tid]) << 8) |
+              (uint32_t(slot[2 * TE + tid]) << 16) | (uint32_t(slot[3 * TE + tid]) << 24);
+        o.y = uint32_t(slot[4 * TE + tid]) | (uint32_t(slot[5 * TE + tid]) << 8) |
+              (uint32_t(slot[6 * TE + tid]) << 16) | (uint32_t(slot[7 * TE + tid]) << 24);
+        reinterpret_cast<uint2*>(eloc8)[e] = o;
+      }
+      __syncthreads();
+    }
   }
 }
 
@@ -261,9 +273,66 @@ __global__ void tile_compact(const uint32_t* __restrict__ tmp, int S, const uint
   }
 }
 
+// Warp-tile reference lists in bytes, per tile of kWarpTile elements (768
+// bytes): the 8 * kWarpTile references sorted by node as positions
+// v * kWarpTile + element, the node's rank in the tile list, and flags for
+// the kernel's segmented sum, which gives each lane 8 consecutive references:
+// 1 = a new sum starts here, 2 = the sum leaves after this reference, 4 = it
+// leaves as a store (the node's whole run lies in this lane and no other
+// tile uses the node), 8 = valid reference.  One warp per tile, one lane per
+// node; runs after the nodes shared between tiles are marked.
+__global__ void warp_refs(const uint16_t* __restrict__ inc, const uint16_t* __restrict__ nend,
+                          const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ nodes, int64_t ntiles,
+                          uint8_t* __restrict__ out) {
+  constexpr int S = 8 * kWarpTile;
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = int64_t(gridDim.x) * (blockDim.x / 32);
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x / 32) + (threadIdx.x >> 5); t < ntiles; t += nw) {
+    uint8_t* o = out + t * 3 * S;
+    for (int j = lane; j < S; j += 32) o[2 * S + j] = 0;  // invalid until written
+    __syncwarp();
+    const uint32_t p0 = ptr[t], nt = ptr[t + 1] - p0;
+    for (uint32_t k = lane; k < nt; k += 32) {
+      const uint32_t beg = k ? nend[t * S + k - 1] : 0u, end = nend[t * S + k];
+      const bool excl = !(nodes[p0 + k] & 0x80000000u);
+      for (uint32_t j = beg; j < end; ++j) {
+        o[j] = uint8_t(inc[t * S + j]);
+        o[S + j] = uint8_t(k);
+        const bool lane_first = (j & 7u) == 0u, lane_last = (j & 7u) == 7u;
+        const bool start = j == beg || lane_first;
+        const bool flush = j + 1 == end || lane_last;
+        const bool whole = (beg >> 3) == ((end - 1) >> 3);  // the run does not cross a lane boundary
+        o[2 * S + j] = uint8_t(8u | (start ? 1u : 0u) | (flush ? 2u : 0u) | (flush && whole && excl ? 4u : 0u));
+      }
+    }
+  }
+}
+
 // Per node, the number of tiles whose list holds it.
+// An entry whose bit 31 is already set (a warp-tile node whose references
+// span two lanes of the segmented sum) counts twice, so that it is treated
+// like a node shared between tiles.
 __global__ void tile_touch(const uint32_t* __restrict__ nodes, int64_t n, uint32_t* __restrict__ touch) {
-  for (int64_t i = gtid(); i < n; i += gstride()) atomicAdd(touch + nodes[i], 1u);
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    const uint32_t id = nodes[i];
+    atomicAdd(touch + (id & 0x7fffffffu), (id & 0x80000000u) ? 2u : 1u);
+  }
+}
+
+// Warp tiles: mark (bit 31) the nodes whose run of sorted references crosses
+// a boundary between two lanes' groups of 8, since their sums arrive in parts.
+__global__ void warp_split_runs(const uint16_t* __restrict__ nend, const uint32_t* __restrict__ ptr, int64_t ntiles,
+                                uint32_t* __restrict__ nodes) {
+  constexpr int S = 8 * kWarpTile;
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = int64_t(gridDim.x) * (blockDim.x / 32);
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x / 32) + (threadIdx.x >> 5); t < ntiles; t += nw) {
+    const uint32_t p0 = ptr[t], nt = ptr[t + 1] - p0;
+    for (uint32_t k = lane; k < nt; k += 32) {
+      const uint32_t beg = k ? nend[t * S + k - 1] : 0u, end = nend[t * S + k];
+      if ((beg >> 3) != ((end - 1) >> 3)) nodes[p0 + k] |= 0x80000000u;
+    }
+  }
 }
 
 // Bit 31 of a list entry: the node is referenced by more than one tile, so its
@@ -271,7 +340,7 @@ __global__ void tile_touch(const uint32_t* __restrict__ nodes, int64_t n, uint32
 // flagged per node for the compact list of them.
 __global__ void tile_local_mark(uint32_t* __restrict__ nodes, int64_t n, const uint32_t* __restrict__ touch) {
   for (int64_t i = gtid(); i < n; i += gstride()) {
-    const uint32_t id = nodes[i];
+    const uint32_t id = nodes[i] & 0x7fffffffu;
     if (touch[id] > 1u) nodes[i] = id | 0x80000000u;
   }
 }
@@ -353,21 +422,21 @@ dg_status build_mesh(const dg_octree* tree, dg_da* da, cudaStream_t s) {
 
 template <int TE>
 static dg_status launch_tile_lists(const dg_da* da, int64_t nt, uint32_t* tmp, uint32_t* cnt, uint16_t* nend,
-                                   uint16_t* inc, uint4* eloc, cudaStream_t s) {
+                                   uint16_t* inc, uint4* eloc, uint8_t* eloc8, cudaStream_t s) {
   const size_t smem = size_t(8 + 2) * 8 * TE;
   static bool set = false;
   if (!set && smem > 48 * 1024) {
     DG_CUDA(cudaFuncSetAttribute(tile_lists<TE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   }
   set = true;
-  tile_lists<TE><<<grid_for(nt, TE, 2048 / TE), TE, smem, s>>>(da->nl.p, da->E, nt, tmp, cnt, nend, inc, eloc);
+  tile_lists<TE><<<grid_for(nt, TE, 2048 / TE), TE, smem, s>>>(da->nl.p, da->E, nt, tmp, cnt, nend, inc, eloc, eloc8);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }
 
 dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s) {
   DG_CHECK(da->N < (int64_t(1) << 31), DG_EINVAL, "mesh above 2^31 nodes");
-  DG_CHECK(te == kLocalTile || te == kMultiTile, DG_EINVAL, "unsupported tile size");
+  DG_CHECK(te == kMultiTile || te == kWarpTile, DG_EINVAL, "unsupported tile size");
   const int64_t E = da->E, nt = (E + te - 1) / te, S = 8 * int64_t(te);
   ts.te = te;
   ts.ntiles = nt;
@@ -376,11 +445,12 @@ dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s) {
   DG_TRY(cnt.alloc(nt));
   DG_TRY(ts.nend.alloc(nt * S));
   DG_TRY(ts.inc.alloc(nt * S));
-  if (te == kLocalTile) {
-    DG_TRY(launch_tile_lists<kLocalTile>(da, nt, tmp.p, cnt.p, ts.nend.p, ts.inc.p, nullptr, s));
+  if (te == kWarpTile) {
+    DG_TRY(ts.eloc8.alloc(8 * E));
+    DG_TRY(launch_tile_lists<kWarpTile>(da, nt, tmp.p, cnt.p, ts.nend.p, ts.inc.p, nullptr, ts.eloc8.p, s));
   } else {
     DG_TRY(ts.eloc.alloc(E));
-    DG_TRY(launch_tile_lists<kMultiTile>(da, nt, tmp.p, cnt.p, ts.nend.p, ts.inc.p, ts.eloc.p, s));
+    DG_TRY(launch_tile_lists<kMultiTile>(da, nt, tmp.p, cnt.p, ts.nend.p, ts.inc.p, ts.eloc.p, nullptr, s));
   }
   std::vector<uint32_t> hc(nt);
   DG_CUDA(cudaMemcpyAsync(hc.data(), cnt.p, 4 * nt, cudaMemcpyDeviceToHost, s));
@@ -396,6 +466,8 @@ dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s) {
   tile_compact<<<grid_for(nt, 256, 8), 256, 0, s>>>(tmp.p, int(S), ts.ptr.p, nt, ts.nodes.p);
   DG_TRY(touch.alloc(da->N));
   DG_CUDA(cudaMemsetAsync(touch.p, 0, 4 * da->N, s));
+  if (te == kWarpTile)
+    warp_split_runs<<<grid_for(nt * 32, 256, 8), 256, 0, s>>>(ts.nend.p, ts.ptr.p, nt, ts.nodes.p);
   tile_touch<<<grid_for(total, 256), 256, 0, s>>>(ts.nodes.p, total, touch.p);
   tile_local_mark<<<grid_for(total, 256), 256, 0, s>>>(ts.nodes.p, total, touch.p);
   shared_flag<<<grid_for(da->N, 256), 256, 0, s>>>(touch.p, da->N);
@@ -407,12 +479,20 @@ dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s) {
   ts.nshared = ns;
   DG_TRY(ts.shared.alloc(ns > 0 ? ns : 1));
   shared_emit<<<grid_for(da->N, 256), 256, 0, s>>>(touch.p, pos.p, da->N, ts.shared.p);
+  if (te == kWarpTile) {  // byte lists with flags replace the uint16 ones
+    DG_TRY(ts.ref8.alloc(nt * 3 * S));
+    warp_refs<<<grid_for(nt * 32, 256, 8), 256, 0, s>>>(ts.inc.p, ts.nend.p, ts.ptr.p, ts.nodes.p, nt, ts.ref8.p);
+  }
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaStreamSynchronize(s));
+  if (te == kWarpTile) {
+    ts.inc.reset();
+    ts.nend.reset();
+  }
   return DG_OK;
 }
 
-dg_status build_tiles(dg_da* da, cudaStream_t s) { return build_tile_set(da, kLocalTile, da->tiles, s); }
+dg_status build_tiles(dg_da* da, cudaStream_t s) { return build_tile_set(da, kWarpTile, da->tiles_w, s); }
 
 uint32_t etype_mask(int c, int t) { return kEtypeMask[c & 7][t % 18]; }
 

@@ -177,6 +177,7 @@ __global__ void prolong_fill(const uint64_t* __restrict__ fnk, int64_t Nf, const
 template <class T>
 __global__ void prolong_add(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
                             const T* __restrict__ val, int64_t Nf, const T* __restrict__ xc, T* __restrict__ xf) {
+  #pragma unroll 4
   for (int64_t f = gtid(); f < Nf; f += gstride()) {
     T s = 0;
     for (uint32_t k = ptr[f]; k < ptr[f + 1]; ++k) s += val[k] * xc[col[k]];
@@ -189,6 +190,7 @@ template <class T>
 __global__ void restrict_residual(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
                                   const T* __restrict__ val, int64_t Nf, const T* __restrict__ rf,
                                   T* __restrict__ rc) {
+  #pragma unroll 4
   for (int64_t f = gtid(); f < Nf; f += gstride()) {
     const T r = rf[f];
     if (r == T(0)) continue;
@@ -200,10 +202,12 @@ __global__ void restrict_residual(const uint32_t* __restrict__ ptr, const uint32
 template <class T>
 __global__ void jacobi_first(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ dinv, T omega,
                              int64_t n) {
+  #pragma unroll 4
   for (int64_t i = gtid(); i < n; i += gstride()) x[i] = omega * dinv[i] * b[i];
 }
 template <class A, class B>
 __global__ void convert(const A* __restrict__ a, B* __restrict__ b, int64_t n) {
+  #pragma unroll 4
   for (int64_t i = gtid(); i < n; i += gstride()) b[i] = B(a[i]);
 }
 // Coefficients stored in BF16: round the FP32 copy to the nearest BF16 value.
@@ -288,6 +292,7 @@ __global__ void finish_sum(const double* __restrict__ part, int np, double* __re
 __global__ void dot_partial(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
                             double* __restrict__ part) {
   double v = 0;
+  #pragma unroll 4
   for (int64_t i = gtid(); i < n; i += gstride()) v += a[i] * b[i];
   v = block_sum(v);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
@@ -298,6 +303,7 @@ __global__ void cg_update(double* __restrict__ x, double* __restrict__ r, const 
                           const double* __restrict__ den, double* __restrict__ part) {
   const double alpha = *num / *den;
   double v = 0;
+  #pragma unroll 4
   for (int64_t i = gtid(); i < n; i += gstride()) {
     x[i] += alpha * p[i];
     double ri = r[i] - alpha * q[i];
@@ -313,12 +319,14 @@ __global__ void cg_direction_flex(double* __restrict__ p, const double* __restri
                                   const double* __restrict__ rz, const double* __restrict__ rzo,
                                   const double* __restrict__ den) {
   const double beta = (*rz - *rzo) / *den;
+  #pragma unroll 4
   for (int64_t i = gtid(); i < n; i += gstride()) p[i] = z[i] + beta * p[i];
 }
 // p = z + beta p with beta = num / den
 __global__ void cg_direction(double* __restrict__ p, const double* __restrict__ z, int64_t n,
                              const double* __restrict__ num, const double* __restrict__ den) {
   const double beta = *num / *den;
+  #pragma unroll 4
   for (int64_t i = gtid(); i < n; i += gstride()) p[i] = z[i] + beta * p[i];
 }
 
@@ -551,7 +559,7 @@ dg_status vcycle(dg_damg* m, size_t l, const double* b, double* x) {
   cudaStream_t s = m->s;
   Level& L = m->lv[l];
   const int64_t n = L.da->N;
-  const unsigned g = grid_for(n, 256);
+  const unsigned g = grid_for(n, 256, 16);
   if (l + 1 == m->lv.size()) {
     dense_gemv<<<grid_for(n * 32, 256), 256, 0, s>>>(m->Ainv.p, n, m->d_crow_blk.p, m->d_cb_off.p, m->d_cb_n.p,
                                                      m->d_cb_aoff.p, b, x);
@@ -560,7 +568,7 @@ dg_status vcycle(dg_damg* m, size_t l, const double* b, double* x) {
   }
   const double w = m->cfg.omega;
   // pre-smoothing from a zero initial guess; the sweeps after the first and
-  // the residual are fused tile-local operator applications
+  // the residual are fused warp-tile operator applications
   if (m->cfg.nu_pre > 0) {
     jacobi_first<<<g, 256, 0, s>>>(x, b, L.dinv.p, w, n);
     for (int k = 1; k < m->cfg.nu_pre; ++k) DG_TRY(lapmass_smooth_f64(L.A.get(), x, b, L.dinv.p, w, L.acc.p, s));
@@ -584,7 +592,7 @@ dg_status vcycle32(dg_damg* m, size_t l, const float* b, float* x) {
   cudaStream_t s = m->s;
   Level& L = m->lv[l];
   const int64_t n = L.da->N;
-  const unsigned g = grid_for(n, 256);
+  const unsigned g = grid_for(n, 256, 16);
   if (l + 1 == m->lv.size()) {
     convert<float, double><<<g, 256, 0, s>>>(b, L.b.p, n);
     dense_gemv<<<grid_for(n * 32, 256), 256, 0, s>>>(m->Ainv.p, n, m->d_crow_blk.p, m->d_cb_off.p, m->d_cb_n.p,
@@ -740,6 +748,25 @@ dg_status build_hierarchy(const dg_octree* finest, int nlevels, cudaStream_t s, 
   return DG_OK;
 }
 
+// Coarsen the coarsest level further until the hierarchy has L levels (a
+// batch gives every mesh the depth of the deepest one; a mesh coarsened to
+// the root stays there, with identity transfers).
+dg_status extend_hierarchy(std::vector<Level>& lv, size_t L, cudaStream_t s) {
+  while (lv.size() < L) {
+    Level& last = lv.back();
+    dg_octree tmp;
+    DG_TRY(coarsen_octree(last.tree.get(), &tmp, s));
+    Level next;
+    next.tree = std::make_unique<dg_octree>();
+    DG_TRY(balance_octree(&tmp, next.tree.get(), s));
+    next.da = std::make_unique<dg_da>();
+    DG_TRY(build_mesh(next.tree.get(), next.da.get(), s));
+    lv.push_back(std::move(next));
+    DG_TRY(build_prolongation(lv[lv.size() - 2], lv.back(), s));
+  }
+  return DG_OK;
+}
+
 dg_status finish_create(dg_damg* m) {
   const int64_t N = m->lv[0].da->N;
   DG_TRY(m->r.alloc(N));
@@ -846,21 +873,17 @@ dg_status dg_damg_create_batch(const dg_octree* const* finest, int count, const 
       m->mesh_node_off.push_back({0, L.da->N});
     }
   } else {
-    // every mesh gets the same number of levels: the smallest natural count
+    // every mesh gets the same number of levels: the largest natural count,
+    // the shallower hierarchies coarsened further (so that every coarsest
+    // level stays small enough for the dense direct solve)
     std::vector<std::vector<Level>> per(count);
-    size_t L = size_t(-1);
+    size_t L = 0;
     for (int i = 0; i < count; ++i) {
       DG_CHECK(finest[i], DG_EINVAL, "damg_create_batch: null octree");
       DG_TRY(build_hierarchy(finest[i], m->cfg.nlevels, s, per[i]));
-      L = per[i].size() < L ? per[i].size() : L;
+      L = per[i].size() > L ? per[i].size() : L;
     }
-    for (int i = 0; i < count; ++i) {
-      per[i].resize(L);
-      Level& last = per[i].back();  // no transfer below the common coarsest level
-      last.pptr.reset();
-      last.pcol.reset();
-      last.pval.reset();
-    }
+    for (int i = 0; i < count; ++i) DG_TRY(extend_hierarchy(per[i], L, s));
     m->lv.resize(L);
     for (size_t l = 0; l < L; ++l) {
       std::vector<dg_da*> das;

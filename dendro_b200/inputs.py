@@ -60,6 +60,20 @@ def workload_points(name: str, scale: float = 1.0):
     raise KeyError(name)
 
 
+def batch_clouds(count: int = 32, first_seed: int = 100, depth: int = 12, n_lo: float = 1e4, n_hi: float = 5e5):
+    """Independent Gaussian clouds: per seed, n log-uniform in [n_lo, n_hi],
+    sigma U[0.05, 0.2], centre U[0.3, 0.7]^3, coordinates N(centre, sigma),
+    clamped to [0, 1)."""
+    out = []
+    for i in range(count):
+        rng = np.random.default_rng(first_seed + i)
+        n = int(round(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi)))))
+        sigma = rng.uniform(0.05, 0.2)
+        c = rng.uniform(0.3, 0.7, 3)
+        out.append(clamp_unit(rng.normal(c, sigma, (n, 3)), depth))
+    return out, depth
+
+
 def sphere_coefficients(centers: np.ndarray, inside=1.0e4, outside=1.0, radius=0.25) -> np.ndarray:
     """Per-element [alpha, beta]: alpha = `inside` when the element centre lies
     within `radius` of (0.5,0.5,0.5), else `outside`; beta = 1."""

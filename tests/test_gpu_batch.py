@@ -45,3 +45,22 @@ def test_batch_matvec_and_solve(gpu, oracle):
         bi = b[no[i]:no[i + 1]]
         ri = mm.matvec(xs[no[i]:no[i + 1]], coef[2 * eo[i]:2 * eo[i + 1]]) - bi
         assert np.linalg.norm(ri) <= 1.01e-8 * np.linalg.norm(bi), i
+
+
+def test_batch_of_uneven_meshes_takes_the_deepest_hierarchy(gpu, oracle):
+    """Meshes of very different sizes: the batch has the deepest mesh's level
+    count (shallower hierarchies coarsened further) and every mesh converges."""
+    from dendro_b200 import inputs as I
+    clouds, d = I.batch_clouds(count=4, first_seed=200, depth=10, n_lo=500, n_hi=60000)
+    trees = [gpu.balanceOctree(gpu.points2Octree(p, d, 1)) for p in clouds]
+    natural = [gpu.DAMG(t).nlevels for t in trees]
+    m = gpu.DAMG(trees, inner_prec=1, use_graph=True)
+    assert m.nlevels == max(natural)
+    _, no = m.batch_offsets(0)
+    b = I.uniform_rhs(int(no[-1]), 11)
+    x, rep = m.solve(b)
+    assert rep["converged"]
+    for i, t in enumerate(trees):
+        mm = oracle.Mesh(t.to_numpy(), d)
+        bi = b[no[i]:no[i + 1]]
+        assert np.linalg.norm(mm.matvec(x[no[i]:no[i + 1]]) - bi) <= 1.01e-8 * np.linalg.norm(bi), i

@@ -236,7 +236,7 @@ def run_solve(dev, workload):
     best = min(out[t]["1e-08"]["ms"] for t, _, _, _ in methods[1:])
     out["speedup_chosen_vs_plain_at_1e-8"] = round(out["plain_fp64"]["1e-08"]["ms"] / best, 3)
     out["methods"] = {
-        "plain_fp64": "FP64 CG + FP64 V(2,2) damped Jacobi (fused tile-local sweeps), dense FP64 coarse solve",
+        "plain_fp64": "FP64 CG + FP64 V(2,2) damped Jacobi (warp-tile operator), dense FP64 coarse solve",
         "mixed_fp32": "FP64 flexible CG + FP32 V(2,2) (FP32 operator, smoother, transfers), FP64 coarse solve, "
                       "V-cycle replayed from a CUDA graph",
         "mixed_fp32_learned": "mixed_fp32 with the trained MLP post-smoother on the finest level, Jacobi fallback "

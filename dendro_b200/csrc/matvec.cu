@@ -18,6 +18,7 @@
 // (1,-1) factors; 56 flops per scalar element instead of 256.
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 
 #include "dg_internal.h"
 
@@ -219,6 +220,52 @@ __global__ void residual_from(const T* __restrict__ b, T* __restrict__ t, T* __r
     const T ti = t[i];
     t[i] = T(0);
     r[i] = b[i] - ti;
+  }
+}
+
+// 16-byte forms (4 floats or 2 doubles per step) for vectors that are whole
+// allocations (16-byte aligned); the callers check the alignment.
+template <class T>
+using Vec16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+template <class T>
+__global__ void jacobi_from_v(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ dinv,
+                              T* __restrict__ t, T omega, int64_t nv) {
+  using V = Vec16<T>;
+  constexpr int W = 16 / sizeof(T);
+  for (int64_t i = gtid(); i < nv; i += gstride()) {
+    V tv = reinterpret_cast<V*>(t)[i], xv = reinterpret_cast<V*>(x)[i];
+    const V bv = reinterpret_cast<const V*>(b)[i], dv = reinterpret_cast<const V*>(dinv)[i];
+    T* tp = reinterpret_cast<T*>(&tv);
+    T* xp = reinterpret_cast<T*>(&xv);
+    const T* bp = reinterpret_cast<const T*>(&bv);
+    const T* dp = reinterpret_cast<const T*>(&dv);
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      xp[k] += omega * dp[k] * (bp[k] - tp[k]);
+      tp[k] = T(0);
+    }
+    reinterpret_cast<V*>(t)[i] = tv;
+    reinterpret_cast<V*>(x)[i] = xv;
+  }
+}
+template <class T>
+__global__ void residual_from_v(const T* __restrict__ b, T* __restrict__ t, T* __restrict__ r, int64_t nv) {
+  using V = Vec16<T>;
+  constexpr int W = 16 / sizeof(T);
+  for (int64_t i = gtid(); i < nv; i += gstride()) {
+    V tv = reinterpret_cast<V*>(t)[i];
+    const V bv = reinterpret_cast<const V*>(b)[i];
+    V rv;
+    T* tp = reinterpret_cast<T*>(&tv);
+    T* rp = reinterpret_cast<T*>(&rv);
+    const T* bp = reinterpret_cast<const T*>(&bv);
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      rp[k] = bp[k] - tp[k];
+      tp[k] = T(0);
+    }
+    reinterpret_cast<V*>(t)[i] = tv;
+    reinterpret_cast<V*>(r)[i] = rv;
   }
 }
 
@@ -430,6 +477,7 @@ constexpr MatvecVariant kVariants[] = {
     {512, 4, 0, 2, "atomic b512 minB2"},
     {32 * kWarpCta, 5, 2, 5, "warp-tile 32 elems, 5 CTAs/SM"}, {32 * kWarpCta, 6, 2, 6, "warp-tile 32 elems, 6 CTAs/SM"},
     {32 * kWarpCta, 4, 3, 4, "warp-tile 32 elems, 4 CTAs/SM, next tile prefetched"},
+    {32 * kWarpCta, 8, 2, 8, "warp-tile 32 elems, 8 CTAs/SM"},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 
@@ -448,6 +496,9 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
                                                                       ts.nodes.p, e8, ts.ref8.p, x, y);
     else if (V.minb == 6)
       lapmass_warp_kernel<T, CT, 6, false><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles,
+                                                                       ts.ptr.p, ts.nodes.p, e8, ts.ref8.p, x, y);
+    else if (V.minb == 8)
+      lapmass_warp_kernel<T, CT, 8, false><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles,
                                                                        ts.ptr.p, ts.nodes.p, e8, ts.ref8.p, x, y);
     else
       lapmass_warp_kernel<T, CT, 5, false><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles,
@@ -568,6 +619,8 @@ dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStrea
   return lapmass_launch<float, float>(da, da->tuned_f32, ca, cb, x, y, s);
 }
 
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 // t = A x into a zero-kept accumulator (every launch shape only adds into y
 // or stores whole sums, so no memset), with the mesh's tuned shape.
 template <class T, class CT>
@@ -586,7 +639,12 @@ static dg_status smooth_sweep(const dg_mat* A, const CT* coef, T* x, const T* b,
                               cudaStream_t s) {
   DG_TRY((apply_to_zeroed<T, CT>(A, coef, x, t, s)));
   const int64_t n = A->da->N;
-  jacobi_from<T><<<grid_for(n, 256, 16), 256, 0, s>>>(x, b, dinv, t, omega, n);
+  constexpr int W = 16 / sizeof(T);
+  const int64_t nv = (aligned16(x) && aligned16(b) && aligned16(dinv) && aligned16(t)) ? n / W : 0;
+  if (nv) jacobi_from_v<T><<<grid_for(nv, 256, 16), 256, 0, s>>>(x, b, dinv, t, omega, nv);
+  if (n > nv * W)
+    jacobi_from<T><<<grid_for(n - nv * W, 256, 16), 256, 0, s>>>(x + nv * W, b + nv * W, dinv + nv * W, t + nv * W,
+                                                                omega, n - nv * W);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }
@@ -595,7 +653,11 @@ template <class T, class CT>
 static dg_status residual(const dg_mat* A, const CT* coef, const T* x, const T* b, T* r, T* t, cudaStream_t s) {
   DG_TRY((apply_to_zeroed<T, CT>(A, coef, x, t, s)));
   const int64_t n = A->da->N;
-  residual_from<T><<<grid_for(n, 256, 16), 256, 0, s>>>(b, t, r, n);
+  constexpr int W = 16 / sizeof(T);
+  const int64_t nv = (aligned16(b) && aligned16(t) && aligned16(r)) ? n / W : 0;
+  if (nv) residual_from_v<T><<<grid_for(nv, 256, 16), 256, 0, s>>>(b, t, r, nv);
+  if (n > nv * W)
+    residual_from<T><<<grid_for(n - nv * W, 256, 16), 256, 0, s>>>(b + nv * W, t + nv * W, r + nv * W, n - nv * W);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }

@@ -14,6 +14,8 @@
 #include <memory>
 #include <vector>
 
+#include <type_traits>
+
 #include "dg_internal.h"
 
 #include <cuda_bf16.h>
@@ -185,30 +187,74 @@ __global__ void prolong_add(const uint32_t* __restrict__ ptr, const uint32_t* __
   }
 }
 
-// rc += P^T r (restriction; rc zeroed beforehand)
+// rc = R rf with R = P^T stored by coarse rows (a gather: no atomics, and the
+// sum order is the same on every run)
 template <class T>
-__global__ void restrict_residual(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
-                                  const T* __restrict__ val, int64_t Nf, const T* __restrict__ rf,
-                                  T* __restrict__ rc) {
-  #pragma unroll 4
-  for (int64_t f = gtid(); f < Nf; f += gstride()) {
-    const T r = rf[f];
-    if (r == T(0)) continue;
-    for (uint32_t k = ptr[f]; k < ptr[f + 1]; ++k) atomicAdd(rc + col[k], val[k] * r);
+__global__ void restrict_gather(const uint32_t* __restrict__ rptr, const uint32_t* __restrict__ rcol,
+                                const T* __restrict__ rval, int64_t Nc, const T* __restrict__ rf,
+                                T* __restrict__ rc) {
+  for (int64_t c = gtid(); c < Nc; c += gstride()) {
+    T acc = T(0);
+    for (uint32_t k = rptr[c]; k < rptr[c + 1]; ++k) acc += rval[k] * rf[rcol[k]];
+    rc[c] = acc;
+  }
+}
+// transpose of P: keys (coarse column << 32 | entry index) and counts per column
+__global__ void ptrans_keys(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col, int64_t Nf,
+                            uint64_t* __restrict__ keys, uint32_t* __restrict__ frow, uint32_t* __restrict__ cnt) {
+  for (int64_t f = gtid(); f < Nf; f += gstride())
+    for (uint32_t k = ptr[f]; k < ptr[f + 1]; ++k) {
+      keys[k] = (uint64_t(col[k]) << 32) | k;
+      frow[k] = uint32_t(f);
+      atomicAdd(cnt + col[k], 1u);
+    }
+}
+__global__ void ptrans_fill(const uint64_t* __restrict__ keys, int64_t nnz, const uint32_t* __restrict__ frow,
+                            const double* __restrict__ pval, uint32_t* __restrict__ rcol,
+                            double* __restrict__ rval) {
+  for (int64_t j = gtid(); j < nnz; j += gstride()) {
+    const uint32_t k = uint32_t(keys[j] & 0xffffffffu);
+    rcol[j] = frow[k];
+    rval[j] = pval[k];
   }
 }
 
 // --------------------------------------------------------------- smoother --
+// x = omega dinv b on 16-byte chunks (4 floats or 2 doubles; level vectors
+// are whole allocations, so 16-byte aligned); the remainder by thread 0.
 template <class T>
 __global__ void jacobi_first(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ dinv, T omega,
                              int64_t n) {
-  #pragma unroll 4
-  for (int64_t i = gtid(); i < n; i += gstride()) x[i] = omega * dinv[i] * b[i];
+  constexpr int W = 16 / sizeof(T);
+  using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  const int64_t nv = n / W;
+  for (int64_t i = gtid(); i < nv; i += gstride()) {
+    V bv = reinterpret_cast<const V*>(b)[i];
+    const V dv = reinterpret_cast<const V*>(dinv)[i];
+    T* bp = reinterpret_cast<T*>(&bv);
+    const T* dp = reinterpret_cast<const T*>(&dv);
+#pragma unroll
+    for (int k = 0; k < W; ++k) bp[k] = omega * dp[k] * bp[k];
+    reinterpret_cast<V*>(x)[i] = bv;
+  }
+  if (gtid() == 0)
+    for (int64_t i = nv * W; i < n; ++i) x[i] = omega * dinv[i] * b[i];
 }
+// b = a converted, two values per thread and step (whole allocations)
 template <class A, class B>
 __global__ void convert(const A* __restrict__ a, B* __restrict__ b, int64_t n) {
-  #pragma unroll 4
-  for (int64_t i = gtid(); i < n; i += gstride()) b[i] = B(a[i]);
+  using VA = typename std::conditional<sizeof(A) == 4, float2, double2>::type;
+  using VB = typename std::conditional<sizeof(B) == 4, float2, double2>::type;
+  const int64_t n2 = n / 2;
+  #pragma unroll 2
+  for (int64_t i = gtid(); i < n2; i += gstride()) {
+    const VA v = reinterpret_cast<const VA*>(a)[i];
+    VB o;
+    o.x = B(v.x);
+    o.y = B(v.y);
+    reinterpret_cast<VB*>(b)[i] = o;
+  }
+  if (gtid() == 0 && (n & 1)) b[n - 1] = B(a[n - 1]);
 }
 // Coefficients stored in BF16: round the FP32 copy to the nearest BF16 value.
 __global__ void to_bf16_values(float* __restrict__ a, int64_t n) {
@@ -266,7 +312,7 @@ __global__ void dense_gemv(const double* __restrict__ A, int64_t N, const uint32
 }
 
 // -------------------------------------------------------------- reductions --
-constexpr int kRedBlocks = 296;  // 2 x 148 SMs
+constexpr int kRedBlocks = 1184;  // 8 x 148 SMs: enough loads in flight for HBM
 
 __device__ __forceinline__ double block_sum(double v) {
   __shared__ double ws[32];
@@ -289,12 +335,32 @@ __global__ void finish_sum(const double* __restrict__ part, int np, double* __re
   v = block_sum(v);
   if (threadIdx.x == 0) *out = v;
 }
+// The FP64 vector kernels of the outer CG read 16-byte pairs (the solver's
+// vectors are whole allocations, so 16-byte aligned); an odd last element is
+// handled by thread 0.
 __global__ void dot_partial(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
                             double* __restrict__ part) {
-  double v = 0;
+  const double2* a2 = reinterpret_cast<const double2*>(a);
+  const double2* b2 = reinterpret_cast<const double2*>(b);
+  const int64_t n2 = n / 2;
+  double v0 = 0, v1 = 0;
+  #pragma unroll 2
+  for (int64_t i = gtid(); i < n2; i += gstride()) {
+    const double2 x = a2[i], y = b2[i];
+    v0 = fma(x.x, y.x, v0);
+    v1 = fma(x.y, y.y, v1);
+  }
+  if (gtid() == 0 && (n & 1)) v0 = fma(a[n - 1], b[n - 1], v0);
+  const double v = block_sum(v0 + v1);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+// the same for arrays of any alignment (caller-provided vectors)
+__global__ void dot_partial_any(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
+                                double* __restrict__ part) {
+  double v0 = 0;
   #pragma unroll 4
-  for (int64_t i = gtid(); i < n; i += gstride()) v += a[i] * b[i];
-  v = block_sum(v);
+  for (int64_t i = gtid(); i < n; i += gstride()) v0 = fma(a[i], b[i], v0);
+  const double v = block_sum(v0);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
 }
 // x += alpha p; r -= alpha q; partial (r, r); alpha = num / den read on device
@@ -302,32 +368,61 @@ __global__ void cg_update(double* __restrict__ x, double* __restrict__ r, const 
                           const double* __restrict__ q, int64_t n, const double* __restrict__ num,
                           const double* __restrict__ den, double* __restrict__ part) {
   const double alpha = *num / *den;
-  double v = 0;
-  #pragma unroll 4
-  for (int64_t i = gtid(); i < n; i += gstride()) {
-    x[i] += alpha * p[i];
-    double ri = r[i] - alpha * q[i];
-    r[i] = ri;
-    v += ri * ri;
+  double2* x2 = reinterpret_cast<double2*>(x);
+  double2* r2 = reinterpret_cast<double2*>(r);
+  const double2* p2 = reinterpret_cast<const double2*>(p);
+  const double2* q2 = reinterpret_cast<const double2*>(q);
+  const int64_t n2 = n / 2;
+  double v0 = 0, v1 = 0;
+  #pragma unroll 2
+  for (int64_t i = gtid(); i < n2; i += gstride()) {
+    double2 xi = x2[i], ri = r2[i];
+    const double2 pi = p2[i], qi = q2[i];
+    xi.x += alpha * pi.x;
+    xi.y += alpha * pi.y;
+    ri.x -= alpha * qi.x;
+    ri.y -= alpha * qi.y;
+    x2[i] = xi;
+    r2[i] = ri;
+    v0 = fma(ri.x, ri.x, v0);
+    v1 = fma(ri.y, ri.y, v1);
   }
-  v = block_sum(v);
+  if (gtid() == 0 && (n & 1)) {
+    x[n - 1] += alpha * p[n - 1];
+    const double rl = r[n - 1] - alpha * q[n - 1];
+    r[n - 1] = rl;
+    v0 = fma(rl, rl, v0);
+  }
+  const double v = block_sum(v0 + v1);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+// p = z + beta p on 16-byte pairs
+__device__ __forceinline__ void axpby_pairs(double* __restrict__ p, const double* __restrict__ z, int64_t n,
+                                            double beta) {
+  double2* p2 = reinterpret_cast<double2*>(p);
+  const double2* z2 = reinterpret_cast<const double2*>(z);
+  const int64_t n2 = n / 2;
+  #pragma unroll 2
+  for (int64_t i = gtid(); i < n2; i += gstride()) {
+    double2 pi = p2[i];
+    const double2 zi = z2[i];
+    pi.x = zi.x + beta * pi.x;
+    pi.y = zi.y + beta * pi.y;
+    p2[i] = pi;
+  }
+  if (gtid() == 0 && (n & 1)) p[n - 1] = z[n - 1] + beta * p[n - 1];
 }
 // flexible (Polak-Ribiere) direction: p = z + beta p,
 // beta = ((r, z) - (r, z_old)) / (r_old, z_old)
 __global__ void cg_direction_flex(double* __restrict__ p, const double* __restrict__ z, int64_t n,
                                   const double* __restrict__ rz, const double* __restrict__ rzo,
                                   const double* __restrict__ den) {
-  const double beta = (*rz - *rzo) / *den;
-  #pragma unroll 4
-  for (int64_t i = gtid(); i < n; i += gstride()) p[i] = z[i] + beta * p[i];
+  axpby_pairs(p, z, n, (*rz - *rzo) / *den);
 }
 // p = z + beta p with beta = num / den
 __global__ void cg_direction(double* __restrict__ p, const double* __restrict__ z, int64_t n,
                              const double* __restrict__ num, const double* __restrict__ den) {
-  const double beta = *num / *den;
-  #pragma unroll 4
-  for (int64_t i = gtid(); i < n; i += gstride()) p[i] = z[i] + beta * p[i];
+  axpby_pairs(p, z, n, *num / *den);
 }
 
 }  // namespace
@@ -339,11 +434,12 @@ struct Level {
   std::unique_ptr<dg_mat> A;
   DBuf<double> dinv, x, b, t;
   DBuf<double> acc;   // shared-node sums of the fused sweeps (kept zero between uses)
-  // P to this level from level + 1 (CSR over this level's nodes)
-  DBuf<uint32_t> pptr, pcol;
-  DBuf<double> pval;
+  // P to this level from level + 1 (CSR over this level's nodes) and R = P^T
+  // (CSR over the coarse nodes, entries in fine-node order)
+  DBuf<uint32_t> pptr, pcol, rptr, rcol;
+  DBuf<double> pval, rval;
   // FP32 inner V-cycle
-  DBuf<float> dinv32, x32, b32, t32, pval32, acc32;
+  DBuf<float> dinv32, x32, b32, t32, pval32, rval32, acc32;
   // learned smoother data (finest level): residual, neighbour stats,
   // 1 / element references, hanging share, mean log2 diagonal
   DBuf<float> sm_r, sm_nsum, sm_nmax, sm_refs, sm_hang;
@@ -418,6 +514,33 @@ dg_status build_prolongation(Level& F, Level& C, cudaStream_t s) {
   return DG_OK;
 }
 
+// R = P^T by coarse rows, entries in fine-node order (a stable sort of the
+// entries by their coarse column).
+dg_status build_restriction(Level& F, int64_t Nc, cudaStream_t s) {
+  const int64_t Nf = F.da->N, nnz = F.pcol.n;
+  DBuf<uint64_t> keys, tmp;
+  DBuf<uint32_t> frow;
+  DG_TRY(keys.alloc(nnz));
+  DG_TRY(tmp.alloc(nnz));
+  DG_TRY(frow.alloc(nnz));
+  DG_TRY(F.rptr.alloc(Nc + 1));
+  DG_CUDA(cudaMemsetAsync(F.rptr.p, 0, 4 * (Nc + 1), s));
+  ptrans_keys<<<grid_for(Nf, 256), 256, 0, s>>>(F.pptr.p, F.pcol.p, Nf, keys.p, frow.p, F.rptr.p);
+  DG_CUDA(cudaGetLastError());
+  int bits = 1;
+  while ((int64_t(1) << bits) < Nc) ++bits;
+  DG_TRY(radix_sort_u64(keys.p, tmp.p, nnz, bits, s, 32));
+  uint32_t total = 0;
+  DG_TRY(scan_u32(F.rptr.p, F.rptr.p, Nc + 1, &total, s));
+  DG_CHECK(int64_t(total) == nnz, DG_EINVAL, "restriction: entry count mismatch");
+  DG_TRY(F.rcol.alloc(nnz));
+  DG_TRY(F.rval.alloc(nnz));
+  ptrans_fill<<<grid_for(nnz, 256), 256, 0, s>>>(keys.p, nnz, frow.p, F.pval.p, F.rcol.p, F.rval.p);
+  DG_CUDA(cudaGetLastError());
+  DG_CUDA(cudaStreamSynchronize(s));
+  return DG_OK;
+}
+
 dg_status setup_level_vectors(Level& L, cudaStream_t s) {
   const int64_t N = L.da->N;
   DG_TRY(L.dinv.alloc(N));
@@ -452,6 +575,8 @@ dg_status setup_level_f32(dg_damg* m, Level& L, cudaStream_t s) {
   if (L.pval.n) {
     DG_TRY(L.pval32.alloc(L.pval.n));
     convert<double, float><<<grid_for(L.pval.n, 256), 256, 0, s>>>(L.pval.p, L.pval32.p, L.pval.n);
+    DG_TRY(L.rval32.alloc(L.rval.n));
+    convert<double, float><<<grid_for(L.rval.n, 256), 256, 0, s>>>(L.rval.p, L.rval32.p, L.rval.n);
   }
   if (L.A->has_coef && m->cfg.inner_prec == DG_PREC_F32_BF16COEF)
     DG_TRY(round_coef_bf16(L.A->coef32.p, 2 * L.da->E, s));
@@ -577,9 +702,8 @@ dg_status vcycle(dg_damg* m, size_t l, const double* b, double* x) {
     DG_CUDA(cudaMemsetAsync(x, 0, 8 * n, s));
   }
   Level& C = m->lv[l + 1];
-  DG_CUDA(cudaMemsetAsync(C.b.p, 0, 8 * C.da->N, s));
-  restrict_residual<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval.p, n, m->cfg.nu_pre > 0 ? (const double*)L.t.p : b,
-                                      C.b.p);
+  restrict_gather<<<grid_for(C.da->N, 256, 16), 256, 0, s>>>(L.rptr.p, L.rcol.p, L.rval.p, C.da->N,
+                                                            m->cfg.nu_pre > 0 ? (const double*)L.t.p : b, C.b.p);
   DG_TRY(vcycle(m, l + 1, C.b.p, C.x.p));
   prolong_add<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval.p, n, C.x.p, x);
   for (int k = 0; k < m->cfg.nu_post; ++k) DG_TRY(lapmass_smooth_f64(L.A.get(), x, b, L.dinv.p, w, L.acc.p, s));
@@ -610,9 +734,8 @@ dg_status vcycle32(dg_damg* m, size_t l, const float* b, float* x) {
     DG_CUDA(cudaMemsetAsync(x, 0, 4 * n, s));
   }
   Level& C = m->lv[l + 1];
-  DG_CUDA(cudaMemsetAsync(C.b32.p, 0, 4 * C.da->N, s));
-  restrict_residual<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval32.p, n, m->cfg.nu_pre > 0 ? (const float*)L.t32.p : b,
-                                      C.b32.p);
+  restrict_gather<<<grid_for(C.da->N, 256, 16), 256, 0, s>>>(L.rptr.p, L.rcol.p, L.rval32.p, C.da->N,
+                                                            m->cfg.nu_pre > 0 ? (const float*)L.t32.p : b, C.b32.p);
   DG_TRY(vcycle32(m, l + 1, C.b32.p, C.x32.p));
   prolong_add<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval32.p, n, C.x32.p, x);
   if (l == 0 && m->mlp && m->mlp_active) {
@@ -786,6 +909,7 @@ dg_status finish_create(dg_damg* m) {
   for (int i = 0; i < m->nmesh; ++i)
     fill_u16<<<grid_for(no[i + 1] - no[i], 256), 256, 0, m->s>>>(m->d_node_mesh.p, no[i], no[i + 1], uint16_t(i));
   DG_CUDA(cudaGetLastError());
+  for (size_t l = 0; l + 1 < m->lv.size(); ++l) DG_TRY(build_restriction(m->lv[l], m->lv[l + 1].da->N, m->s));
   return set_operators(m, nullptr);
 }
 
@@ -990,9 +1114,7 @@ dg_status dg_damg_restrict(dg_damg* m, int level, const double* rf, double* rc, 
     pc = dc.p;
   }
   if (on_device) DG_CUDA(cudaDeviceSynchronize());
-  DG_CUDA(cudaMemsetAsync(pc, 0, 8 * nc, m->s));
-  restrict_residual<<<grid_for(nf, 256), 256, 0, m->s>>>(F.pptr.p, F.pcol.p, F.pval.p, nf, pf,
-                                                          pc);
+  restrict_gather<<<grid_for(nc, 256, 16), 256, 0, m->s>>>(F.rptr.p, F.rcol.p, F.rval.p, nc, pf, pc);
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaStreamSynchronize(m->s));
   if (!on_device) DG_CUDA(cudaMemcpy(rc, dc.p, 8 * nc, cudaMemcpyDeviceToHost));
@@ -1011,10 +1133,13 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
   double* px = x;
   // the caller's device data may come from any stream
   if (on_device) DG_CUDA(cudaDeviceSynchronize());
-  if (!on_device) {
+  // the vector kernels read 16-byte pairs: host data, and device data not
+  // 16-byte aligned, go through the solver's own buffers
+  const bool staged = !on_device || ((reinterpret_cast<uintptr_t>(b) | reinterpret_cast<uintptr_t>(x)) & 15) != 0;
+  if (staged) {
     DG_TRY(db.alloc(n));
     DG_TRY(dx.alloc(n));
-    DG_CUDA(cudaMemcpyAsync(db.p, b, 8 * n, cudaMemcpyHostToDevice, s));
+    DG_CUDA(cudaMemcpyAsync(db.p, b, 8 * n, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
     pb = db.p;
     px = dx.p;
   }
@@ -1099,7 +1224,10 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (!on_device) DG_CUDA(cudaMemcpy(x, dx.p, 8 * n, cudaMemcpyDeviceToHost));
+  if (staged) {
+    DG_CUDA(cudaMemcpyAsync(x, dx.p, 8 * n, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    DG_CUDA(cudaStreamSynchronize(s));
+  }
   if (rep) {
     rep->iterations = it > m->cfg.maxit ? m->cfg.maxit : it;
     rep->converged = conv ? 1 : 0;
@@ -1117,7 +1245,10 @@ dg_status dg_vec_dot(const double* x, const double* y, int64_t n, double* result
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   DBuf<double> part;  // one partial sum per reduction block
   DG_TRY(part.alloc(kRedBlocks));
-  dot_partial<<<kRedBlocks, 256, 0, s>>>(x, y, n, part.p);
+  if (((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0)
+    dot_partial<<<kRedBlocks, 256, 0, s>>>(x, y, n, part.p);
+  else
+    dot_partial_any<<<kRedBlocks, 256, 0, s>>>(x, y, n, part.p);
   finish_sum<<<1, 256, 0, s>>>(part.p, kRedBlocks, result);
   DG_CUDA(cudaGetLastError());
   // the partials are released when this call returns

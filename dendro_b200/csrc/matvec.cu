@@ -405,6 +405,113 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_kernel(
   }
 }
 
+
+// Deeper software pipeline over a warp's tiles: while tile t is worked on,
+// the records of tile t + 1 (loaded at the top), then its node ids (issued
+// after the element phase of t) and then x at those nodes (issued after the
+// segmented sum of t) travel in registers, so that of the three dependent
+// global round trips of a tile (list offsets, node ids, x) only the last is
+// exposed.  Up to kPipeIds node ids per lane ride along (tiles of up to
+// 32 kPipeIds nodes); larger tiles load the rest in place.
+constexpr int kPipeIds = 3;
+template <class T, class CT, int MINB>
+__global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_pipe_kernel(
+    const uint32_t* __restrict__ meta, const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
+    int64_t ntiles, const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_nodes,
+    const uint2* __restrict__ eloc8, const uint8_t* __restrict__ ref8, const T* __restrict__ x,
+    T* __restrict__ y) {
+  constexpr int S = 8 * kWarpTile;
+  __shared__ T s_x[kWarpCta][S];
+  __shared__ uint32_t s_nodes[kWarpCta][S];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  T* sx = s_x[w];
+  uint32_t* sn = s_nodes[w];
+  const int64_t nw = int64_t(gridDim.x) * kWarpCta;
+  int64_t t = blockIdx.x * int64_t(kWarpCta) + w;
+  WarpTileLoad<T> cur, nxt;
+  uint32_t idc[kPipeIds];
+  T xc[kPipeIds];
+  if (t < ntiles) {
+    load_warp_tile<T, CT>(cur, t, lane, E, meta, ca, cb, tile_ptr, eloc8, ref8);
+#pragma unroll
+    for (int j = 0; j < kPipeIds; ++j) {
+      const uint32_t k = lane + 32 * j;
+      idc[j] = k < cur.nt ? __ldg(tile_nodes + cur.p0 + k) : 0u;
+    }
+#pragma unroll
+    for (int j = 0; j < kPipeIds; ++j) {
+      const uint32_t k = lane + 32 * j;
+      xc[j] = k < cur.nt ? __ldg(x + (idc[j] & 0x7fffffffu)) : T(0);
+    }
+  }
+  for (; t < ntiles; t += nw) {
+    const bool has_next = t + nw < ntiles;
+    if (has_next) load_warp_tile<T, CT>(nxt, t + nw, lane, E, meta, ca, cb, tile_ptr, eloc8, ref8);
+#pragma unroll
+    for (int j = 0; j < kPipeIds; ++j) {
+      const uint32_t k = lane + 32 * j;
+      if (k < cur.nt) {
+        sn[k] = idc[j];
+        sx[k] = xc[j];
+      }
+    }
+    for (uint32_t k = lane + 32 * kPipeIds; k < cur.nt; k += 32) {
+      const uint32_t id = __ldg(tile_nodes + cur.p0 + k);
+      sn[k] = id;
+      sx[k] = __ldg(x + (id & 0x7fffffffu));
+    }
+    __syncwarp();
+    const bool live = t * kWarpTile + lane < E;
+    T wv[8];
+    const uint32_t c = meta_cnum(cur.m);
+    if (live) {
+      const T h = elem_h<T>(meta_lev(cur.m));
+      const T f1 = cur.a * h * T(0.5), f2 = cur.b * h * h * h * T(0.125);
+      const uint2 Lf = xor_perm_bytes(cur.L, c);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) wv[j] = sx[byte_of(Lf, j)];
+      const uint32_t mp = xor_perm_mask(meta_mask(cur.m), c);
+      if (mp) interp_frame(wv, mp);
+      lapmass_ref(wv, f1, f2);
+      if (mp) scatter_frame(wv, mp);
+    }
+    // the next tile's node ids: its record has had the element phase to arrive
+#pragma unroll
+    for (int j = 0; j < kPipeIds; ++j) {
+      const uint32_t k = lane + 32 * j;
+      idc[j] = (has_next && k < nxt.nt) ? __ldg(tile_nodes + nxt.p0 + k) : 0u;
+    }
+    __syncwarp();
+    if (live) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) sx[(uint32_t(j) ^ c) * kWarpTile + lane] = wv[j];
+    }
+    __syncwarp();
+    T sum = T(0);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const uint32_t f = byte_of(cur.ff, q);
+      if (f & 8u) {
+        const T v = sx[byte_of(cur.pp, q)];
+        sum = (f & 1u) ? v : sum + v;
+        if (f & 2u) {
+          const uint32_t id = sn[byte_of(cur.rr, q)];
+          if (f & 4u) y[id] = sum;
+          else atomicAdd(y + (id & 0x7fffffffu), sum);
+        }
+      }
+    }
+    // x at the next tile's nodes: the ids have had the segmented sum to arrive
+#pragma unroll
+    for (int j = 0; j < kPipeIds; ++j) {
+      const uint32_t k = lane + 32 * j;
+      xc[j] = (has_next && k < nxt.nt) ? __ldg(x + (idc[j] & 0x7fffffffu)) : T(0);
+    }
+    __syncwarp();
+    if (has_next) cur = nxt;
+  }
+}
+
 template <class CT>
 __global__ void lapmass_diag_kernel(const uint32_t* __restrict__ nl, const uint32_t* __restrict__ meta,
                                     const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
@@ -467,7 +574,7 @@ __global__ void lapmass_dense_kernel(const uint32_t* __restrict__ nl, const uint
 // precision; DG_MATVEC_KERNEL=<index> forces one (testing).
 struct MatvecVariant {
   int block, per_sm;  // threads per CTA, CTAs per SM in the grid (0: one thread per element)
-  int kind;           // 0 atomic (BLOCK, MINB), 2 warp-tile, 3 warp-tile with prefetch
+  int kind;           // 0 atomic (BLOCK, MINB), 2 warp-tile, 3 + records prefetched, 4 + ids and x too
   int minb;
   const char* name;
 };
@@ -478,6 +585,8 @@ constexpr MatvecVariant kVariants[] = {
     {32 * kWarpCta, 5, 2, 5, "warp-tile 32 elems, 5 CTAs/SM"}, {32 * kWarpCta, 6, 2, 6, "warp-tile 32 elems, 6 CTAs/SM"},
     {32 * kWarpCta, 4, 3, 4, "warp-tile 32 elems, 4 CTAs/SM, next tile prefetched"},
     {32 * kWarpCta, 8, 2, 8, "warp-tile 32 elems, 8 CTAs/SM"},
+    {32 * kWarpCta, 3, 4, 3, "warp-tile 32 elems, 3 CTAs/SM, ids and x of the next tile in flight"},
+    {32 * kWarpCta, 4, 4, 4, "warp-tile 32 elems, 4 CTAs/SM, ids and x of the next tile in flight"},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 
@@ -491,7 +600,13 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
     const TileSet& ts = da->tiles_w;
     const unsigned gw = grid_for(ts.ntiles * 32, 32 * kWarpCta, V.per_sm);
     const uint2* e8 = reinterpret_cast<const uint2*>(ts.eloc8.p);
-    if (V.kind == 3)
+    if (V.kind == 4 && V.minb == 3)
+      lapmass_warp_pipe_kernel<T, CT, 3><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
+                                                                     ts.nodes.p, e8, ts.ref8.p, x, y);
+    else if (V.kind == 4)
+      lapmass_warp_pipe_kernel<T, CT, 4><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
+                                                                     ts.nodes.p, e8, ts.ref8.p, x, y);
+    else if (V.kind == 3)
       lapmass_warp_kernel<T, CT, 4, true><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
                                                                       ts.nodes.p, e8, ts.ref8.p, x, y);
     else if (V.minb == 6)

@@ -21,6 +21,8 @@
 // rows of y with shared-memory atomics, and each node's row leaves with float4
 // stores (node used by this tile only) or float4 global atomics (node shared
 // with other tiles).
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "dg_internal.h"
@@ -132,6 +134,106 @@ __global__ void __launch_bounds__(kMThreads) mrhs_kernel(const uint32_t* __restr
   }
 }
 
+// Warp-tile form: each warp owns tiles of kWarpTile elements (the scalar
+// operator's tiles) and a private shared accumulator of the tile's node rows
+// for one 16-RHS chunk, so the elements of a tile add their D fragments with
+// plain read-modify-writes, one element after the other (no atomics, no
+// other warp touching the rows).  A fragments come straight from the
+// node-major X rows (8 lanes read 32 contiguous bytes of a row; rows shared by
+// neighbouring elements hit L1).  Each lane keeps its own element's scaling,
+// table index and node ranks; the warp walks the tile's elements taking them
+// by shuffle.  Rows leave with float4 stores (node whole in this tile) or
+// float4 global atomics.
+constexpr int kMWarps = 4;       // warps per CTA
+constexpr int kYW = kRC + 4;     // accumulator row: 16 floats + pad, float4-aligned
+// Floats of shared memory per warp: the rows, then the node ids padded to a
+// multiple of 4, so that every warp's rows start on a 16-byte boundary.
+__host__ __device__ constexpr size_t mrhs_warp_stride(uint32_t cap) {
+  return size_t(cap) * kYW + ((size_t(cap) + 3) & ~size_t(3));
+}
+__device__ __forceinline__ uint32_t rank_of(uint2 r, int v) { return ((v < 4 ? r.x : r.y) >> ((v & 3) * 8)) & 0xffu; }
+
+template <int NS>
+__global__ void __launch_bounds__(32 * kMWarps) mrhs_warp_kernel(
+    const uint32_t* __restrict__ meta, const float* __restrict__ ca, const float* __restrict__ cb, int64_t E,
+    int64_t ntiles, const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_nodes,
+    const uint2* __restrict__ eloc8, const float4* __restrict__ tbl, int R, uint32_t cap,
+    const float* __restrict__ X, float* __restrict__ Y) {
+  extern __shared__ __align__(16) float mw_smem[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = lane >> 2, tq = lane & 3;
+  float* Ys = mw_smem + size_t(w) * mrhs_warp_stride(cap);  // [cap][kYW] rows, then the node ids
+  uint32_t* sn = reinterpret_cast<uint32_t*>(Ys + size_t(cap) * kYW);
+  const int64_t nw = int64_t(gridDim.x) * kMWarps;
+  for (int64_t t = blockIdx.x * int64_t(kMWarps) + w; t < ntiles; t += nw) {
+    const uint32_t p0 = __ldg(tile_ptr + t), nt = __ldg(tile_ptr + t + 1) - p0;
+    for (uint32_t k = lane; k < nt; k += 32) sn[k] = __ldg(tile_nodes + p0 + k);
+    // this lane's element: scaling, table row and node ranks
+    const int64_t e_own = t * kWarpTile + lane;
+    const int nel = int(E - t * kWarpTile < kWarpTile ? E - t * kWarpTile : kWarpTile);
+    float f1o = 0.f, f2o = 0.f;
+    uint32_t combo_o = 0;
+    uint2 Lo = make_uint2(0, 0);
+    if (e_own < E) {
+      const uint32_t m = __ldg(meta + e_own);
+      const float h = elem_hf(meta_lev(m));
+      const float a = ca ? __ldg(ca + e_own) : 1.f, b = cb ? __ldg(cb + e_own) : 1.f;
+      f1o = a * h * 0.5f;
+      f2o = b * h * h * h * 0.125f;
+      combo_o = (meta_cnum(m) * 18 + meta_type(m)) * 32;
+      Lo = __ldg(eloc8 + e_own);
+    }
+    __syncwarp();
+    for (int r0 = 0; r0 < R; r0 += kRC) {
+      for (uint32_t i = lane; i < 4 * nt; i += 32)
+        reinterpret_cast<float4*>(Ys + (i >> 2) * kYW)[i & 3] = make_float4(0.f, 0.f, 0.f, 0.f);
+      __syncwarp();
+      for (int el = 0; el < nel; ++el) {
+        const float f1 = __shfl_sync(0xffffffffu, f1o, el), f2 = __shfl_sync(0xffffffffu, f2o, el);
+        const uint32_t combo = __shfl_sync(0xffffffffu, combo_o, el);
+        uint2 L;
+        L.x = __shfl_sync(0xffffffffu, Lo.x, el);
+        L.y = __shfl_sync(0xffffffffu, Lo.y, el);
+        const float4 tb = __ldg(tbl + combo + lane);
+        const float bf0 = f1 * tb.x + f2 * tb.z, bf1 = f1 * tb.y + f2 * tb.w;
+        const float* xa = X + int64_t(sn[rank_of(L, tq)] & 0x7fffffffu) * R + r0;
+        const float* xb = X + int64_t(sn[rank_of(L, tq + 4)] & 0x7fffffffu) * R + r0;
+        const float x0 = __ldg(xa + g), x1 = __ldg(xa + g + 8), x2 = __ldg(xb + g), x3 = __ldg(xb + g + 8);
+        float d[4] = {0.f, 0.f, 0.f, 0.f};
+        if (NS == 1) {
+          mma_tf32(d, to_tf32(x0), to_tf32(x1), to_tf32(x2), to_tf32(x3), to_tf32(bf0), to_tf32(bf1));
+        } else {
+          const uint32_t ah0 = to_tf32(x0), ah1 = to_tf32(x1), ah2 = to_tf32(x2), ah3 = to_tf32(x3);
+          const uint32_t bh0 = to_tf32(bf0), bh1 = to_tf32(bf1);
+          const uint32_t al0 = to_tf32(x0 - __uint_as_float(ah0)), al1 = to_tf32(x1 - __uint_as_float(ah1));
+          const uint32_t al2 = to_tf32(x2 - __uint_as_float(ah2)), al3 = to_tf32(x3 - __uint_as_float(ah3));
+          const uint32_t bl0 = to_tf32(bf0 - __uint_as_float(bh0)), bl1 = to_tf32(bf1 - __uint_as_float(bh1));
+          mma_tf32(d, al0, al1, al2, al3, bh0, bh1);
+          mma_tf32(d, ah0, ah1, ah2, ah3, bl0, bl1);
+          mma_tf32(d, ah0, ah1, ah2, ah3, bh0, bh1);
+        }
+        // D: rhs g / g + 8 at vertices 2 tq and 2 tq + 1 (distinct nodes of one element)
+        float* yc = Ys + rank_of(L, 2 * tq) * kYW;
+        float* yd = Ys + rank_of(L, 2 * tq + 1) * kYW;
+        yc[g] += d[0];
+        yd[g] += d[1];
+        yc[g + 8] += d[2];
+        yd[g + 8] += d[3];
+        __syncwarp();  // the next element may add into the same rows
+      }
+      for (uint32_t i = lane; i < 4 * nt; i += 32) {
+        const uint32_t k = i >> 2, q = i & 3;
+        const uint32_t id = sn[k];
+        const float4 v = reinterpret_cast<const float4*>(Ys + k * kYW)[q];
+        float4* dst = reinterpret_cast<float4*>(Y + int64_t(id & 0x7fffffffu) * R + r0) + q;
+        if (id & 0x80000000u) atomicAdd(dst, v);
+        else *dst = v;
+      }
+      __syncwarp();
+    }
+  }
+}
+
 // Zero the rows of the nodes that several tiles share (their sums arrive by atomics).
 __global__ void zero_shared_rows(const uint32_t* __restrict__ shared, int64_t ns, int R4, float4* __restrict__ Y) {
   const int64_t n = ns * R4;
@@ -213,13 +315,43 @@ dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int R, int split
     tbls[dev] = p;
   }
   const float4* tbl = tbls[dev];
+  const float* ca = A->has_coef ? A->coef32.p : nullptr;
+  const float* cb = A->has_coef ? A->coef32.p + da->E : nullptr;
+  static int form = -1;  // DG_MRHS_KERNEL=cta selects the 128-element CTA-tile form (testing)
+  if (form < 0) {
+    const char* e = getenv("DG_MRHS_KERNEL");
+    form = (e && !strcmp(e, "cta")) ? 1 : 0;
+  }
+  if (form == 0) {
+    const TileSet& ts = da->tiles_w;
+    if (ts.nshared)
+      zero_shared_rows<<<grid_for(ts.nshared * (R / 4), 256, 8), 256, 0, s>>>(ts.shared.p, ts.nshared, R / 4,
+                                                                             reinterpret_cast<float4*>(Y));
+    const uint32_t cap = ts.max_nodes;
+    const int smem = int(kMWarps * mrhs_warp_stride(cap) * sizeof(float));
+    DG_CHECK(smem <= 220 * 1024, DG_EINVAL, "mat_mult_multi: tile node count too large");
+    static int granted_w = 48 * 1024;
+    if (smem > granted_w) {
+      DG_CUDA(cudaFuncSetAttribute(mrhs_warp_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      DG_CUDA(cudaFuncSetAttribute(mrhs_warp_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      granted_w = smem;
+    }
+    const unsigned grid = grid_for(ts.ntiles * 32, 32 * kMWarps, 16);
+    const uint2* e8 = reinterpret_cast<const uint2*>(ts.eloc8.p);
+    if (split == 1)
+      mrhs_warp_kernel<1><<<grid, 32 * kMWarps, smem, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
+                                                           ts.nodes.p, e8, tbl, R, cap, X, Y);
+    else
+      mrhs_warp_kernel<3><<<grid, 32 * kMWarps, smem, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
+                                                           ts.nodes.p, e8, tbl, R, cap, X, Y);
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+  }
   if (!da->tiles_mr.ntiles) DG_TRY(build_tile_set(da, kMultiTile, da->tiles_mr, s));
   const TileSet& ts = da->tiles_mr;
   if (ts.nshared)
     zero_shared_rows<<<grid_for(ts.nshared * (R / 4), 256, 8), 256, 0, s>>>(ts.shared.p, ts.nshared, R / 4,
                                                                            reinterpret_cast<float4*>(Y));
-  const float* ca = A->has_coef ? A->coef32.p : nullptr;
-  const float* cb = A->has_coef ? A->coef32.p + da->E : nullptr;
   const uint32_t cap = ts.max_nodes;
   const int smem = int(2 * size_t(cap) * kRW * sizeof(float));
   DG_CHECK(smem <= 220 * 1024, DG_EINVAL, "mat_mult_multi: tile node count too large");

@@ -93,6 +93,39 @@ __host__ __device__ __forceinline__ uint32_t meta_cnum(uint32_t m) { return (m >
 __host__ __device__ __forceinline__ uint32_t meta_mask(uint32_t m) { return (m >> 8) & 255u; }
 __host__ __device__ __forceinline__ uint32_t meta_type(uint32_t m) { return (m >> 16) & 31u; }
 
+// Child-number frame of the warp-tile kernels: frame vertex j is vertex j ^ c
+// of the element (c its child number), so the element's own corner of its
+// parent is frame vertex 0 and the hanging structure no longer depends on c.
+// Bytes j <- j ^ c of a vertex-indexed byte vector (8 node ranks in a uint2).
+__device__ __forceinline__ uint2 xor_perm_bytes(uint2 r, uint32_t c) {
+  if (c & 1u) {
+    r.x = __byte_perm(r.x, 0, 0x2301);
+    r.y = __byte_perm(r.y, 0, 0x2301);
+  }
+  if (c & 2u) {
+    r.x = __byte_perm(r.x, 0, 0x1032);
+    r.y = __byte_perm(r.y, 0, 0x1032);
+  }
+  if (c & 4u) {
+    const uint32_t t = r.x;
+    r.x = r.y;
+    r.y = t;
+  }
+  return r;
+}
+// The hanging mask in the same frame: bit j <- bit j ^ c.
+__host__ __device__ __forceinline__ uint32_t xor_perm_mask(uint32_t m, uint32_t c) {
+  if (c & 1u) m = ((m & 0x55u) << 1) | ((m & 0xAAu) >> 1);
+  if (c & 2u) m = ((m & 0x33u) << 2) | ((m & 0xCCu) >> 2);
+  if (c & 4u) m = ((m & 0x0Fu) << 4) | ((m & 0xF0u) >> 4);
+  return m;
+}
+// Per-element word of the warp-tile kernels: level | frame hanging mask << 8.
+__host__ __device__ __forceinline__ uint32_t wmeta_pack(uint32_t m) {
+  return meta_lev(m) | (xor_perm_mask(meta_mask(m), meta_cnum(m)) << 8);
+}
+__host__ __device__ __forceinline__ uint32_t wmeta_mask(uint32_t w) { return (w >> 8) & 255u; }
+
 // ----------------------------------------------------------------- launch --
 int sm_count();
 inline unsigned grid_for(int64_t n, int block, int per_sm = 8) {

@@ -20,8 +20,13 @@ struct TileSet {
   DBuf<uint16_t> nend;       // [ntiles * 8 te]: tile t, node k -> end of its run in inc
   DBuf<uint16_t> inc;        // [ntiles * 8 te]: tile t -> references ordered by node
   DBuf<uint4> eloc;          // [E] per element the node positions of its 8 vertices (multi-RHS set only)
-  DBuf<uint8_t> eloc8;       // [8 E] the same as bytes (warp tiles, at most 256 nodes per tile)
-  DBuf<uint8_t> ref8;        // [ntiles * 24 te] warp tiles: sorted positions, node ranks, segmented-sum flags
+  // warp tiles (at most 256 nodes per tile), all in the child-number frame
+  // (frame vertex j = vertex j ^ c of the element):
+  DBuf<uint8_t> eloc8;       // [8 E] per element byte j = node rank of frame vertex j
+  DBuf<uint32_t> wmeta;      // [E] level | frame hanging mask << 8
+  DBuf<uint8_t> ref8;        // [ntiles * kWarpRefBytes] per tile: the references sorted by node as frame
+                             // positions j * te + element [8 te], their node ranks [8 te], then per lane
+                             // one flag word [32 x u32] (bit q valid, 8 + q start, 16 + q leave, 24 + q store)
   DBuf<uint32_t> shared;     // ascending ids of the nodes several tiles reference
   int64_t nshared = 0;
 };
@@ -71,6 +76,7 @@ namespace dg {
 // warp-tile kernel (one lane each)
 constexpr int kMultiTile = 128;
 constexpr int kWarpTile = 32;
+constexpr int kWarpRefBytes = 16 * kWarpTile + 4 * 32;  // per warp tile in TileSet::ref8
 
 // ---- learned smoother (mlp.cu): 6 -> 64 -> 64 -> 1, packed FP32 parameters ----
 constexpr int kMlpIn = 6;

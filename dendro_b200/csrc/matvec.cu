@@ -135,13 +135,6 @@ __device__ __forceinline__ void xor_perm(T (&a)[8], uint32_t c) {
       }
   }
 }
-// The hanging mask in the same frame: bit j <- bit j ^ c.
-__device__ __forceinline__ uint32_t xor_perm_mask(uint32_t m, uint32_t c) {
-  if (c & 1u) m = ((m & 0x55u) << 1) | ((m & 0xAAu) >> 1);
-  if (c & 2u) m = ((m & 0x33u) << 2) | ((m & 0xCCu) >> 2);
-  if (c & 4u) m = ((m & 0x0Fu) << 4) | ((m & 0xF0u) >> 4);
-  return m;
-}
 // T and T^T in the child-number frame.  A hanging vertex j lies on the
 // parent's edge (j = 1, 2, 4) or face (j = 3, 5, 6) through the shared corner
 // 0 and takes the mean of the node values of the vertices j' with j' a bit
@@ -277,40 +270,27 @@ __global__ void residual_from_v(const T* __restrict__ b, T* __restrict__ t, T* _
 // 8-byte load), and writes its 8 results by (vertex, element) position; the
 // tile's 256 references, sorted by node, are then summed 8 consecutive ones
 // per lane, following per-reference flags built with the mesh (start a sum,
-// let it leave, as a store or an atomic).  A sum leaves with a store when the
+// let it leave, as a store or an atomic).  Node ranks, hanging masks and
+// result positions are stored in the child-number frame, so an element needs
+// no relabelling at run time.  A sum leaves with a store when the
 // node's whole run lies in one lane and no other tile uses the node, else
 // with an FP64 global atomic (y is zeroed first).
 constexpr int kWarpCta = 8;  // warps per CTA
 
-// bytes j <- j ^ c of a vertex-indexed byte vector (8 node ranks in a uint2)
-__device__ __forceinline__ uint2 xor_perm_bytes(uint2 r, uint32_t c) {
-  if (c & 1u) {
-    r.x = __byte_perm(r.x, 0, 0x2301);
-    r.y = __byte_perm(r.y, 0, 0x2301);
-  }
-  if (c & 2u) {
-    r.x = __byte_perm(r.x, 0, 0x1032);
-    r.y = __byte_perm(r.y, 0, 0x1032);
-  }
-  if (c & 4u) {
-    const uint32_t t = r.x;
-    r.x = r.y;
-    r.y = t;
-  }
-  return r;
-}
-__device__ __forceinline__ uint32_t byte_of(uint2 r, int j) { return ((j < 4 ? r.x : r.y) >> ((j & 3) * 8)) & 0xffu; }
+// byte j of a uint2, zero-extended (one byte permute)
+__device__ __forceinline__ uint32_t byte_of(uint2 r, int j) { return __byte_perm(j < 4 ? r.x : r.y, 0u, 0x4440u | uint32_t(j & 3)); }
 
 // Per-lane record of one tile: the lane's element and its 8 sorted references.
 template <class T>
 struct WarpTileLoad {
   uint32_t m, p0, nt;
-  uint2 L, pp, rr, ff;
+  uint2 L, pp, rr;
+  uint32_t ff;  // bit q: reference q valid; 8 + q: starts a sum; 16 + q: sum leaves; 24 + q: as a store
   T a, b;
 };
 template <class T, class CT>
 __device__ __forceinline__ void load_warp_tile(WarpTileLoad<T>& d, int64_t t, int lane, int64_t E,
-                                               const uint32_t* __restrict__ meta, const CT* __restrict__ ca,
+                                               const uint32_t* __restrict__ wmeta, const CT* __restrict__ ca,
                                                const CT* __restrict__ cb, const uint32_t* __restrict__ tile_ptr,
                                                const uint2* __restrict__ eloc8, const uint8_t* __restrict__ ref8) {
   constexpr int S = 8 * kWarpTile;
@@ -320,17 +300,17 @@ __device__ __forceinline__ void load_warp_tile(WarpTileLoad<T>& d, int64_t t, in
   d.a = T(1);
   d.b = T(1);
   if (e < E) {
-    d.m = __ldg(meta + e);
+    d.m = __ldg(wmeta + e);
     d.L = __ldg(eloc8 + e);
     if (ca) {
       d.a = T(__ldg(ca + e));
       d.b = T(__ldg(cb + e));
     }
   }
-  const uint8_t* tr = ref8 + t * 3 * S;
+  const uint8_t* tr = ref8 + t * kWarpRefBytes;
   d.pp = __ldg(reinterpret_cast<const uint2*>(tr) + lane);
   d.rr = __ldg(reinterpret_cast<const uint2*>(tr + S) + lane);
-  d.ff = __ldg(reinterpret_cast<const uint2*>(tr + 2 * S) + lane);
+  d.ff = __ldg(reinterpret_cast<const uint32_t*>(tr + 2 * S) + lane);
   d.p0 = __ldg(tile_ptr + t);
   d.nt = __ldg(tile_ptr + t + 1) - d.p0;
 }
@@ -340,7 +320,7 @@ __device__ __forceinline__ void load_warp_tile(WarpTileLoad<T>& d, int64_t t, in
 // loads' latency hidden behind the current tile).
 template <class T, class CT, int MINB, bool PF>
 __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_kernel(
-    const uint32_t* __restrict__ meta, const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
+    const uint32_t* __restrict__ wmeta, const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
     int64_t ntiles, const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_nodes,
     const uint2* __restrict__ eloc8, const uint8_t* __restrict__ ref8, const T* __restrict__ x,
     T* __restrict__ y) {
@@ -353,12 +333,12 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_kernel(
   const int64_t nw = int64_t(gridDim.x) * kWarpCta;
   int64_t t = blockIdx.x * int64_t(kWarpCta) + w;
   WarpTileLoad<T> cur, nxt;
-  if (PF && t < ntiles) load_warp_tile<T, CT>(cur, t, lane, E, meta, ca, cb, tile_ptr, eloc8, ref8);
+  if (PF && t < ntiles) load_warp_tile<T, CT>(cur, t, lane, E, wmeta, ca, cb, tile_ptr, eloc8, ref8);
   for (; t < ntiles; t += nw) {
     if (PF) {
-      if (t + nw < ntiles) load_warp_tile<T, CT>(nxt, t + nw, lane, E, meta, ca, cb, tile_ptr, eloc8, ref8);
+      if (t + nw < ntiles) load_warp_tile<T, CT>(nxt, t + nw, lane, E, wmeta, ca, cb, tile_ptr, eloc8, ref8);
     } else {
-      load_warp_tile<T, CT>(cur, t, lane, E, meta, ca, cb, tile_ptr, eloc8, ref8);
+      load_warp_tile<T, CT>(cur, t, lane, E, wmeta, ca, cb, tile_ptr, eloc8, ref8);
     }
     const bool live = t * kWarpTile + lane < E;
     for (uint32_t k = lane; k < cur.nt; k += 32) {
@@ -368,14 +348,12 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_kernel(
     }
     __syncwarp();
     T wv[8];
-    const uint32_t c = meta_cnum(cur.m);
     if (live) {
       const T h = elem_h<T>(meta_lev(cur.m));
       const T f1 = cur.a * h * T(0.5), f2 = cur.b * h * h * h * T(0.125);
-      const uint2 Lf = xor_perm_bytes(cur.L, c);  // child-number frame: byte j is vertex j ^ c
 #pragma unroll
-      for (int j = 0; j < 8; ++j) wv[j] = sx[byte_of(Lf, j)];
-      const uint32_t mp = xor_perm_mask(meta_mask(cur.m), c);
+      for (int j = 0; j < 8; ++j) wv[j] = sx[byte_of(cur.L, j)];  // byte j: rank of frame vertex j
+      const uint32_t mp = wmeta_mask(cur.m);
       if (mp) interp_frame(wv, mp);
       lapmass_ref(wv, f1, f2);
       if (mp) scatter_frame(wv, mp);
@@ -383,19 +361,18 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_kernel(
     __syncwarp();  // every lane has read x: its buffer now takes the results
     if (live) {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) sx[(uint32_t(j) ^ c) * kWarpTile + lane] = wv[j];
+      for (int j = 0; j < 8; ++j) sx[j * kWarpTile + lane] = wv[j];
     }
     __syncwarp();
     T sum = T(0);
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const uint32_t f = byte_of(cur.ff, q);
-      if (f & 8u) {
+      if (cur.ff & (1u << q)) {
         const T v = sx[byte_of(cur.pp, q)];
-        sum = (f & 1u) ? v : sum + v;
-        if (f & 2u) {
+        sum = (cur.ff & (0x100u << q)) ? v : sum + v;
+        if (cur.ff & (0x10000u << q)) {
           const uint32_t id = sn[byte_of(cur.rr, q)];
-          if (f & 4u) y[id] = sum;  // the node's whole sum, node used by this tile only
+          if (cur.ff & (0x1000000u << q)) y[id] = sum;  // the node's whole sum, node used by this tile only
           else atomicAdd(y + (id & 0x7fffffffu), sum);
         }
       }
@@ -416,7 +393,7 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_kernel(
 constexpr int kPipeIds = 3;
 template <class T, class CT, int MINB>
 __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_pipe_kernel(
-    const uint32_t* __restrict__ meta, const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
+    const uint32_t* __restrict__ wmeta, const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
     int64_t ntiles, const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_nodes,
     const uint2* __restrict__ eloc8, const uint8_t* __restrict__ ref8, const T* __restrict__ x,
     T* __restrict__ y) {
@@ -432,7 +409,7 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_pipe_kernel(
   uint32_t idc[kPipeIds];
   T xc[kPipeIds];
   if (t < ntiles) {
-    load_warp_tile<T, CT>(cur, t, lane, E, meta, ca, cb, tile_ptr, eloc8, ref8);
+    load_warp_tile<T, CT>(cur, t, lane, E, wmeta, ca, cb, tile_ptr, eloc8, ref8);
 #pragma unroll
     for (int j = 0; j < kPipeIds; ++j) {
       const uint32_t k = lane + 32 * j;
@@ -446,7 +423,7 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_pipe_kernel(
   }
   for (; t < ntiles; t += nw) {
     const bool has_next = t + nw < ntiles;
-    if (has_next) load_warp_tile<T, CT>(nxt, t + nw, lane, E, meta, ca, cb, tile_ptr, eloc8, ref8);
+    if (has_next) load_warp_tile<T, CT>(nxt, t + nw, lane, E, wmeta, ca, cb, tile_ptr, eloc8, ref8);
 #pragma unroll
     for (int j = 0; j < kPipeIds; ++j) {
       const uint32_t k = lane + 32 * j;
@@ -463,14 +440,12 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_pipe_kernel(
     __syncwarp();
     const bool live = t * kWarpTile + lane < E;
     T wv[8];
-    const uint32_t c = meta_cnum(cur.m);
     if (live) {
       const T h = elem_h<T>(meta_lev(cur.m));
       const T f1 = cur.a * h * T(0.5), f2 = cur.b * h * h * h * T(0.125);
-      const uint2 Lf = xor_perm_bytes(cur.L, c);
 #pragma unroll
-      for (int j = 0; j < 8; ++j) wv[j] = sx[byte_of(Lf, j)];
-      const uint32_t mp = xor_perm_mask(meta_mask(cur.m), c);
+      for (int j = 0; j < 8; ++j) wv[j] = sx[byte_of(cur.L, j)];  // byte j: rank of frame vertex j
+      const uint32_t mp = wmeta_mask(cur.m);
       if (mp) interp_frame(wv, mp);
       lapmass_ref(wv, f1, f2);
       if (mp) scatter_frame(wv, mp);
@@ -484,19 +459,18 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_pipe_kernel(
     __syncwarp();
     if (live) {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) sx[(uint32_t(j) ^ c) * kWarpTile + lane] = wv[j];
+      for (int j = 0; j < 8; ++j) sx[j * kWarpTile + lane] = wv[j];
     }
     __syncwarp();
     T sum = T(0);
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const uint32_t f = byte_of(cur.ff, q);
-      if (f & 8u) {
+      if (cur.ff & (1u << q)) {
         const T v = sx[byte_of(cur.pp, q)];
-        sum = (f & 1u) ? v : sum + v;
-        if (f & 2u) {
+        sum = (cur.ff & (0x100u << q)) ? v : sum + v;
+        if (cur.ff & (0x10000u << q)) {
           const uint32_t id = sn[byte_of(cur.rr, q)];
-          if (f & 4u) y[id] = sum;
+          if (cur.ff & (0x1000000u << q)) y[id] = sum;
           else atomicAdd(y + (id & 0x7fffffffu), sum);
         }
       }
@@ -601,22 +575,22 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
     const unsigned gw = grid_for(ts.ntiles * 32, 32 * kWarpCta, V.per_sm);
     const uint2* e8 = reinterpret_cast<const uint2*>(ts.eloc8.p);
     if (V.kind == 4 && V.minb == 3)
-      lapmass_warp_pipe_kernel<T, CT, 3><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
+      lapmass_warp_pipe_kernel<T, CT, 3><<<gw, 32 * kWarpCta, 0, s>>>(ts.wmeta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
                                                                      ts.nodes.p, e8, ts.ref8.p, x, y);
     else if (V.kind == 4)
-      lapmass_warp_pipe_kernel<T, CT, 4><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
+      lapmass_warp_pipe_kernel<T, CT, 4><<<gw, 32 * kWarpCta, 0, s>>>(ts.wmeta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
                                                                      ts.nodes.p, e8, ts.ref8.p, x, y);
     else if (V.kind == 3)
-      lapmass_warp_kernel<T, CT, 4, true><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
+      lapmass_warp_kernel<T, CT, 4, true><<<gw, 32 * kWarpCta, 0, s>>>(ts.wmeta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
                                                                       ts.nodes.p, e8, ts.ref8.p, x, y);
     else if (V.minb == 6)
-      lapmass_warp_kernel<T, CT, 6, false><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles,
+      lapmass_warp_kernel<T, CT, 6, false><<<gw, 32 * kWarpCta, 0, s>>>(ts.wmeta.p, ca, cb, da->E, ts.ntiles,
                                                                        ts.ptr.p, ts.nodes.p, e8, ts.ref8.p, x, y);
     else if (V.minb == 8)
-      lapmass_warp_kernel<T, CT, 8, false><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles,
+      lapmass_warp_kernel<T, CT, 8, false><<<gw, 32 * kWarpCta, 0, s>>>(ts.wmeta.p, ca, cb, da->E, ts.ntiles,
                                                                        ts.ptr.p, ts.nodes.p, e8, ts.ref8.p, x, y);
     else
-      lapmass_warp_kernel<T, CT, 5, false><<<gw, 32 * kWarpCta, 0, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles,
+      lapmass_warp_kernel<T, CT, 5, false><<<gw, 32 * kWarpCta, 0, s>>>(ts.wmeta.p, ca, cb, da->E, ts.ntiles,
                                                                        ts.ptr.p, ts.nodes.p, e8, ts.ref8.p, x, y);
   } else if (V.block == 256 && V.minb == 1) {
     lapmass_kernel<T, CT, 256, 1><<<g, 256, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E, x, y);

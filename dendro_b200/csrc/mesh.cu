@@ -282,13 +282,14 @@ __global__ void tile_compact(const uint32_t* __restrict__ tmp, int S, const uint
 // tile uses the node), 8 = valid reference.  One warp per tile, one lane per
 // node; runs after the nodes shared between tiles are marked.
 __global__ void warp_refs(const uint16_t* __restrict__ inc, const uint16_t* __restrict__ nend,
-                          const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ nodes, int64_t ntiles,
+                          const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ nodes,
+                          const uint32_t* __restrict__ meta, int64_t ntiles, uint8_t* __restrict__ tmp,
                           uint8_t* __restrict__ out) {
   constexpr int S = 8 * kWarpTile;
   const int lane = threadIdx.x & 31;
   const int64_t nw = int64_t(gridDim.x) * (blockDim.x / 32);
   for (int64_t t = blockIdx.x * int64_t(blockDim.x / 32) + (threadIdx.x >> 5); t < ntiles; t += nw) {
-    uint8_t* o = out + t * 3 * S;
+    uint8_t* o = tmp + t * 3 * S;  // positions, ranks, flag bytes (8 valid, 1 start, 2 leave, 4 store)
     for (int j = lane; j < S; j += 32) o[2 * S + j] = 0;  // invalid until written
     __syncwarp();
     const uint32_t p0 = ptr[t], nt = ptr[t + 1] - p0;
@@ -305,6 +306,38 @@ __global__ void warp_refs(const uint16_t* __restrict__ inc, const uint16_t* __re
         o[2 * S + j] = uint8_t(8u | (start ? 1u : 0u) | (flush ? 2u : 0u) | (flush && whole && excl ? 4u : 0u));
       }
     }
+    __syncwarp();
+    // per lane its 8 references: positions v * 32 + element become frame
+    // positions (v ^ c) * 32 + element, the flag bytes one word of bit masks
+    uint8_t* f = out + t * kWarpRefBytes;
+    uint32_t word = 0;
+    for (int q = 0; q < 8; ++q) {
+      const int j = lane * 8 + q;
+      const uint32_t fl = o[2 * S + j];
+      uint32_t pf = 0, rk = 0;
+      if (fl & 8u) {
+        const uint32_t pos = o[j];
+        const uint32_t c = meta_cnum(meta[t * kWarpTile + (pos & 31u)]);
+        pf = (((pos >> 5) ^ c) << 5) | (pos & 31u);
+        rk = o[S + j];
+        word |= (1u << q) | ((fl & 1u) << (8 + q)) | (((fl >> 1) & 1u) << (16 + q)) | (((fl >> 2) & 1u) << (24 + q));
+      }
+      f[j] = uint8_t(pf);
+      f[S + j] = uint8_t(rk);
+    }
+    reinterpret_cast<uint32_t*>(f + 2 * S)[lane] = word;
+    __syncwarp();
+  }
+}
+
+// Warp tiles: node ranks in the child-number frame and the per-element word
+// (level, frame hanging mask).
+__global__ void warp_frame(const uint32_t* __restrict__ meta, int64_t E, uint2* __restrict__ eloc8,
+                           uint32_t* __restrict__ wmeta) {
+  for (int64_t e = gtid(); e < E; e += gstride()) {
+    const uint32_t m = meta[e];
+    eloc8[e] = xor_perm_bytes(eloc8[e], meta_cnum(m));
+    wmeta[e] = wmeta_pack(m);
   }
 }
 
@@ -480,8 +513,15 @@ dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s) {
   DG_TRY(ts.shared.alloc(ns > 0 ? ns : 1));
   shared_emit<<<grid_for(da->N, 256), 256, 0, s>>>(touch.p, pos.p, da->N, ts.shared.p);
   if (te == kWarpTile) {  // byte lists with flags replace the uint16 ones
-    DG_TRY(ts.ref8.alloc(nt * 3 * S));
-    warp_refs<<<grid_for(nt * 32, 256, 8), 256, 0, s>>>(ts.inc.p, ts.nend.p, ts.ptr.p, ts.nodes.p, nt, ts.ref8.p);
+    DBuf<uint8_t> r3;
+    DG_TRY(r3.alloc(nt * 3 * S));
+    DG_TRY(ts.ref8.alloc(nt * kWarpRefBytes));
+    warp_refs<<<grid_for(nt * 32, 256, 8), 256, 0, s>>>(ts.inc.p, ts.nend.p, ts.ptr.p, ts.nodes.p, da->meta.p, nt,
+                                                         r3.p, ts.ref8.p);
+    DG_TRY(ts.wmeta.alloc(E));
+    warp_frame<<<grid_for(E, 256), 256, 0, s>>>(da->meta.p, E, reinterpret_cast<uint2*>(ts.eloc8.p), ts.wmeta.p);
+    DG_CUDA(cudaGetLastError());
+    DG_CUDA(cudaStreamSynchronize(s));  // r3 is freed on return
   }
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaStreamSynchronize(s));

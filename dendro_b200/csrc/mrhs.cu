@@ -148,12 +148,16 @@ constexpr int kMWarps = 4;       // warps per CTA
 constexpr int kYW = kRC + 4;     // accumulator row: 16 floats + pad, float4-aligned
 // Floats of shared memory per warp: the rows, then the node ids padded to a
 // multiple of 4, so that every warp's rows start on a 16-byte boundary.
-__host__ __device__ constexpr size_t mrhs_warp_stride(uint32_t cap) {
-  return size_t(cap) * kYW + ((size_t(cap) + 3) & ~size_t(3));
+// STAGE adds a second block of rows for the chunk's x values.
+__host__ __device__ constexpr size_t mrhs_warp_stride(uint32_t cap, bool stage) {
+  return size_t(cap) * kYW * (stage ? 2 : 1) + ((size_t(cap) + 3) & ~size_t(3));
 }
-__device__ __forceinline__ uint32_t rank_of(uint2 r, int v) { return ((v < 4 ? r.x : r.y) >> ((v & 3) * 8)) & 0xffu; }
+__device__ __forceinline__ uint32_t rank_of(uint2 r, uint32_t v) { return __byte_perm(v < 4 ? r.x : r.y, 0u, 0x4440u | (v & 3u)); }
 
-template <int NS>
+// STAGE: the chunk's x rows of the tile are first copied into shared memory
+// with every lane's float4 loads in flight together, so the element walk
+// reads shared memory only; otherwise each element loads its A fragment from X.
+template <int NS, bool STAGE>
 __global__ void __launch_bounds__(32 * kMWarps) mrhs_warp_kernel(
     const uint32_t* __restrict__ meta, const float* __restrict__ ca, const float* __restrict__ cb, int64_t E,
     int64_t ntiles, const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_nodes,
@@ -162,8 +166,10 @@ __global__ void __launch_bounds__(32 * kMWarps) mrhs_warp_kernel(
   extern __shared__ __align__(16) float mw_smem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int g = lane >> 2, tq = lane & 3;
-  float* Ys = mw_smem + size_t(w) * mrhs_warp_stride(cap);  // [cap][kYW] rows, then the node ids
-  uint32_t* sn = reinterpret_cast<uint32_t*>(Ys + size_t(cap) * kYW);
+  // [cap][kYW] y rows, ([cap][kYW] x rows,) then the node ids
+  float* Ys = mw_smem + size_t(w) * mrhs_warp_stride(cap, STAGE);
+  float* Xs = Ys + size_t(cap) * kYW;
+  uint32_t* sn = reinterpret_cast<uint32_t*>(Ys + size_t(cap) * kYW * (STAGE ? 2 : 1));
   const int64_t nw = int64_t(gridDim.x) * kMWarps;
   for (int64_t t = blockIdx.x * int64_t(kMWarps) + w; t < ntiles; t += nw) {
     const uint32_t p0 = __ldg(tile_ptr + t), nt = __ldg(tile_ptr + t + 1) - p0;
@@ -180,25 +186,37 @@ __global__ void __launch_bounds__(32 * kMWarps) mrhs_warp_kernel(
       const float a = ca ? __ldg(ca + e_own) : 1.f, b = cb ? __ldg(cb + e_own) : 1.f;
       f1o = a * h * 0.5f;
       f2o = b * h * h * h * 0.125f;
-      combo_o = (meta_cnum(m) * 18 + meta_type(m)) * 32;
+      combo_o = ((meta_cnum(m) * 18 + meta_type(m)) * 32) | (meta_cnum(m) << 16);
       Lo = __ldg(eloc8 + e_own);
     }
     __syncwarp();
     for (int r0 = 0; r0 < R; r0 += kRC) {
-      for (uint32_t i = lane; i < 4 * nt; i += 32)
+      for (uint32_t i = lane; i < 4 * nt; i += 32) {
         reinterpret_cast<float4*>(Ys + (i >> 2) * kYW)[i & 3] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (STAGE)
+          reinterpret_cast<float4*>(Xs + (i >> 2) * kYW)[i & 3] =
+              __ldg(reinterpret_cast<const float4*>(X + int64_t(sn[i >> 2] & 0x7fffffffu) * R + r0) + (i & 3));
+      }
       __syncwarp();
       for (int el = 0; el < nel; ++el) {
         const float f1 = __shfl_sync(0xffffffffu, f1o, el), f2 = __shfl_sync(0xffffffffu, f2o, el);
-        const uint32_t combo = __shfl_sync(0xffffffffu, combo_o, el);
+        const uint32_t cw = __shfl_sync(0xffffffffu, combo_o, el);
+        const uint32_t combo = cw & 0xffffu, c = cw >> 16;  // table row; child number (ranks are in its frame)
         uint2 L;
         L.x = __shfl_sync(0xffffffffu, Lo.x, el);
         L.y = __shfl_sync(0xffffffffu, Lo.y, el);
         const float4 tb = __ldg(tbl + combo + lane);
         const float bf0 = f1 * tb.x + f2 * tb.z, bf1 = f1 * tb.y + f2 * tb.w;
-        const float* xa = X + int64_t(sn[rank_of(L, tq)] & 0x7fffffffu) * R + r0;
-        const float* xb = X + int64_t(sn[rank_of(L, tq + 4)] & 0x7fffffffu) * R + r0;
-        const float x0 = __ldg(xa + g), x1 = __ldg(xa + g + 8), x2 = __ldg(xb + g), x3 = __ldg(xb + g + 8);
+        float x0, x1, x2, x3;
+        if (STAGE) {
+          const float* xa = Xs + rank_of(L, tq ^ c) * kYW;
+          const float* xb = Xs + rank_of(L, (tq + 4) ^ c) * kYW;
+          x0 = xa[g], x1 = xa[g + 8], x2 = xb[g], x3 = xb[g + 8];
+        } else {
+          const float* xa = X + int64_t(sn[rank_of(L, tq ^ c)] & 0x7fffffffu) * R + r0;
+          const float* xb = X + int64_t(sn[rank_of(L, (tq + 4) ^ c)] & 0x7fffffffu) * R + r0;
+          x0 = __ldg(xa + g), x1 = __ldg(xa + g + 8), x2 = __ldg(xb + g), x3 = __ldg(xb + g + 8);
+        }
         float d[4] = {0.f, 0.f, 0.f, 0.f};
         if (NS == 1) {
           mma_tf32(d, to_tf32(x0), to_tf32(x1), to_tf32(x2), to_tf32(x3), to_tf32(bf0), to_tf32(bf1));
@@ -213,8 +231,8 @@ __global__ void __launch_bounds__(32 * kMWarps) mrhs_warp_kernel(
           mma_tf32(d, ah0, ah1, ah2, ah3, bh0, bh1);
         }
         // D: rhs g / g + 8 at vertices 2 tq and 2 tq + 1 (distinct nodes of one element)
-        float* yc = Ys + rank_of(L, 2 * tq) * kYW;
-        float* yd = Ys + rank_of(L, 2 * tq + 1) * kYW;
+        float* yc = Ys + rank_of(L, (2 * tq) ^ c) * kYW;
+        float* yd = Ys + rank_of(L, (2 * tq + 1) ^ c) * kYW;
         yc[g] += d[0];
         yd[g] += d[1];
         yc[g + 8] += d[2];
@@ -317,33 +335,31 @@ dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int R, int split
   const float4* tbl = tbls[dev];
   const float* ca = A->has_coef ? A->coef32.p : nullptr;
   const float* cb = A->has_coef ? A->coef32.p + da->E : nullptr;
-  static int form = -1;  // DG_MRHS_KERNEL=cta selects the 128-element CTA-tile form (testing)
-  if (form < 0) {
+  static int form = -1;
+  if (form < 0) {  // DG_MRHS_KERNEL: direct (default) | stage | cta
     const char* e = getenv("DG_MRHS_KERNEL");
-    form = (e && !strcmp(e, "cta")) ? 1 : 0;
+    form = (e && !strcmp(e, "cta")) ? 2 : (e && !strcmp(e, "stage")) ? 1 : 0;
   }
-  if (form == 0) {
+  if (form < 2) {
     const TileSet& ts = da->tiles_w;
     if (ts.nshared)
       zero_shared_rows<<<grid_for(ts.nshared * (R / 4), 256, 8), 256, 0, s>>>(ts.shared.p, ts.nshared, R / 4,
                                                                              reinterpret_cast<float4*>(Y));
     const uint32_t cap = ts.max_nodes;
-    const int smem = int(kMWarps * mrhs_warp_stride(cap) * sizeof(float));
+    const bool stage = form == 1;
+    const int smem = int(kMWarps * mrhs_warp_stride(cap, stage) * sizeof(float));
     DG_CHECK(smem <= 220 * 1024, DG_EINVAL, "mat_mult_multi: tile node count too large");
-    static int granted_w = 48 * 1024;
-    if (smem > granted_w) {
-      DG_CUDA(cudaFuncSetAttribute(mrhs_warp_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-      DG_CUDA(cudaFuncSetAttribute(mrhs_warp_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-      granted_w = smem;
+    auto kern = stage ? (split == 1 ? mrhs_warp_kernel<1, true> : mrhs_warp_kernel<3, true>)
+                      : (split == 1 ? mrhs_warp_kernel<1, false> : mrhs_warp_kernel<3, false>);
+    static int granted_w[4] = {48 * 1024, 48 * 1024, 48 * 1024, 48 * 1024};
+    int& gr = granted_w[(stage ? 2 : 0) + (split == 1 ? 0 : 1)];
+    if (smem > gr) {
+      DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      gr = smem;
     }
     const unsigned grid = grid_for(ts.ntiles * 32, 32 * kMWarps, 16);
-    const uint2* e8 = reinterpret_cast<const uint2*>(ts.eloc8.p);
-    if (split == 1)
-      mrhs_warp_kernel<1><<<grid, 32 * kMWarps, smem, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
-                                                           ts.nodes.p, e8, tbl, R, cap, X, Y);
-    else
-      mrhs_warp_kernel<3><<<grid, 32 * kMWarps, smem, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
-                                                           ts.nodes.p, e8, tbl, R, cap, X, Y);
+    kern<<<grid, 32 * kMWarps, smem, s>>>(da->meta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p, ts.nodes.p,
+                                          reinterpret_cast<const uint2*>(ts.eloc8.p), tbl, R, cap, X, Y);
     DG_CUDA(cudaGetLastError());
     return DG_OK;
   }

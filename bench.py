@@ -35,7 +35,14 @@ METRIC = "time to FP64 rel. residual 1e-8 & matvec GDoF/s: chosen vs plain FP64,
 WORKLOAD = "lognormal1m_d14"
 # DRAM bytes (read + write) of one operator launch on the default workload,
 # from one ncu capture per kernel (profiles/lapmass_warp_lognormal1m_d14.md)
-TRAFFIC = {"warp-tile": 332613888 + 21873408}
+# DRAM bytes per operator launch on the bench mesh, by launch shape (ncu:
+# dram__bytes.sum.per_second x gpu__time_duration.sum of one launch; the
+# summaries under profiles/ give the commands).  First matching prefix wins.
+TRAFFIC = {
+    "warp-tile 32 elems, 3 CTAs/SM, ids and x of the next tile in flight": 337146106,
+    "warp-tile 32 elems, records by bulk copy": 336114385,
+    "warp-tile": 332613888 + 21873408,
+}
 
 
 def parse():

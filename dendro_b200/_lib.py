@@ -109,6 +109,8 @@ def lib():
         "dg_damg_batch_count": ([P], I),
         "dg_damg_batch_offsets": ([P, I, P, P], I),
         "dg_vec_dot_noalloc": ([P, P, I64, P, P], I),
+        "dg_device_check": ([P], I),
+        "dg_set_device_wait_limit": ([I64], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -132,7 +134,8 @@ def exported_symbols():
         "dg_damg_create_batch", "dg_damg_batch_count", "dg_damg_batch_offsets", "dg_damg_vcycle",
         "dg_mlp_param_count", "dg_mlp_create", "dg_mlp_get_params", "dg_mlp_set_params", "dg_mlp_forward",
         "dg_mlp_gradient", "dg_mlp_train_step", "dg_mlp_destroy", "dg_damg_set_smoother", "dg_damg_features",
-        "dg_vec_dot_noalloc", "dg_mat_kernel_count", "dg_mat_set_kernel",
+        "dg_vec_dot_noalloc", "dg_mat_kernel_count", "dg_mat_set_kernel", "dg_device_check",
+        "dg_set_device_wait_limit",
         "dg_mat_mult_multi", "dg_damg_set_tolerances",
     ]
 

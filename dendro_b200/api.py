@@ -315,3 +315,17 @@ def vecDot(x, y, stream=None) -> float:
     s = None if stream is None else C.c_void_p(stream.cuda_stream)
     check(lib().dg_vec_dot(ptr(x), ptr(y), x.numel(), ptr(out), s), "vec_dot")
     return float(out.item())
+
+
+def deviceCheck(stream=None) -> None:
+    """Synchronise `stream` (a torch stream or None) and raise DendroError
+    (DG_ETIMEOUT) when a bounded device wait of an operator kernel ran out
+    since the last check; the launches concerned produced no valid result."""
+    s = None if stream is None else C.c_void_p(stream.cuda_stream)
+    check(lib().dg_device_check(s), "device_check")
+
+
+def setDeviceWaitLimit(cycles: int) -> None:
+    """Test hook: clock64 cycles a staged operator kernel waits for its copies
+    before giving up (<= 0 restores the default of 2^31 cycles)."""
+    check(lib().dg_set_device_wait_limit(int(cycles)), "set_device_wait_limit")

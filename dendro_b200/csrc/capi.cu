@@ -338,8 +338,12 @@ dg_status dg_mat_create_lapmass(dg_da* da, const double* coef, dg_mat** out) {
       soa[e] = coef[2 * e];
       soa[da->E + e] = coef[2 * e + 1];
     }
-    dg_status st = upload(A->coef, soa.data(), 2 * da->E);
-    if (!st) st = A->coef32.alloc(2 * da->E);
+    dg_status st = A->coef.alloc(2 * da->E + kCoefPad);
+    if (!st && cudaMemcpy(A->coef.p, soa.data(), 16 * da->E, cudaMemcpyHostToDevice) != cudaSuccess) {
+      set_error(__FILE__, __LINE__, "cudaMemcpy of the coefficients");
+      st = DG_ECUDA;
+    }
+    if (!st) st = A->coef32.alloc(2 * da->E + kCoefPad);
     if (!st) st = convert_f64_to_f32(A->coef.p, A->coef32.p, 2 * da->E, nullptr);
     if (st) { delete A; return st; }
   }
@@ -394,7 +398,13 @@ dg_status dg_mat_mult_host(dg_mat* A, const double* x, double* y) {
   DG_CUDA(cudaMemcpyAsync(A->host_x.p, x, 8 * n, cudaMemcpyHostToDevice, nullptr));
   DG_TRY(dg_mat_mult(A, A->host_x.p, A->host_y.p, nullptr));
   DG_CUDA(cudaMemcpyAsync(y, A->host_y.p, 8 * n, cudaMemcpyDeviceToHost, nullptr));
-  DG_CUDA(cudaStreamSynchronize(nullptr));
+  return device_wait_status(nullptr);  // synchronises
+}
+
+dg_status dg_device_check(void* stream) { return device_wait_status(as_stream(stream)); }
+
+dg_status dg_set_device_wait_limit(int64_t cycles) {
+  set_wait_limit(static_cast<long long>(cycles));
   return DG_OK;
 }
 

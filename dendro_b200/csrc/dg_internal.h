@@ -77,6 +77,12 @@ namespace dg {
 constexpr int kMultiTile = 128;
 constexpr int kWarpTile = 32;
 constexpr int kWarpRefBytes = 16 * kWarpTile + 4 * 32;  // per warp tile in TileSet::ref8
+// Slack after per-element arrays that the bulk-copy operator kernel reads in
+// whole 32-element windows starting on 16-byte boundaries: the [2 E]
+// coefficient arrays get kCoefPad extra elements, the warp tiles' node lists
+// kNodePad extra entries; eloc8 and wmeta are allocated for whole tiles.
+constexpr int64_t kCoefPad = 64;
+constexpr int64_t kNodePad = 8;
 
 // ---- learned smoother (mlp.cu): 6 -> 64 -> 64 -> 1, packed FP32 parameters ----
 constexpr int kMlpIn = 6;
@@ -113,6 +119,11 @@ dg_status coarsen_octree(const dg_octree* in, dg_octree* out, cudaStream_t s);
 
 // ---- mesh (mesh.cu) ----
 dg_status build_mesh(const dg_octree* tree, dg_da* da, cudaStream_t s);
+// Bounded device waits of the operator kernels: the wait limit in clock64
+// cycles (<= 0: the default) and the check that synchronises s and reports
+// DG_ETIMEOUT (then clears it) when a wait has run out.
+void set_wait_limit(long long cycles);
+dg_status device_wait_status(cudaStream_t s);
 dg_status build_tiles(dg_da* da, cudaStream_t s);  // da->tiles_w (kWarpTile)
 dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s);
 // Hanging mask of element type t (0..17) for child number c

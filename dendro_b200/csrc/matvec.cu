@@ -16,6 +16,7 @@
 // eigenvectors (1,1) and (1,-1), so A = f1 K + f2 M = W diag(l) W / 8 with W
 // the 8-point Walsh-Hadamard transform and l depending only on the number of
 // (1,-1) factors; 56 flops per scalar element instead of 256.
+#include <cstddef>
 #include <cstdlib>
 #include <cstring>
 #include <type_traits>
@@ -486,6 +487,284 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_pipe_kernel(
   }
 }
 
+// ---------------------------------------------------- bulk-copy staging --
+// The warp-tile operator with its tile records staged by the copy engine:
+// one lane per warp issues cp.async.bulk copies of a tile's contiguous
+// records (sorted references, frame ranks, element words, coefficients and
+// the window of its node ids) into the warp's shared memory, completing on an
+// mbarrier; two stages per warp, tile t + 2 issued as soon as tile t has been
+// summed, x at the next tile's nodes gathered into registers as soon as its
+// stage has landed.  The records never occupy registers in flight and the
+// lanes issue no global loads for them.
+//
+// Every copy starts on a 16-byte boundary: per-tile offsets of the reference
+// lists (kWarpRefBytes), ranks (256 B), element words (128 B) and first
+// coefficients (32 per tile) are multiples of 16; the second coefficient
+// array and the node list are copied from the 16-byte boundary at or below
+// their start (lead-in skipped when read), and the arrays carry slack so
+// that whole-tile windows stay inside their allocations.
+//
+// Waits are bounded: lane 0 polls the stage's mbarrier until a clock64
+// deadline; past it the warp records DG_ETIMEOUT in a device status word,
+// waits (bounded again) for its copies still in flight, and returns.
+constexpr int kTmaWarps = 4;  // warps per CTA
+constexpr long long kDefaultWaitLimit = 1ll << 31;  // clock64 cycles, about a second
+static long long g_wait_limit = kDefaultWaitLimit;
+
+__device__ int g_wait_status;  // DG_ETIMEOUT once a bounded wait has run out
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+template <class CT>
+struct alignas(16) TmaStage {
+  uint8_t ref[kWarpRefBytes];                 // sorted frame positions, their node ranks, flag words
+  uint2 eloc[kWarpTile];                      // per element the ranks of its frame vertices
+  uint32_t wm[kWarpTile];                     // per element level | frame hanging mask << 8
+  CT ca[kWarpTile];                           // first coefficient
+  CT cb[kWarpTile + 16 / sizeof(CT)];         // second coefficient, from the 16-byte boundary below
+  uint32_t nodes[8 * kWarpTile + kNodePad];   // node ids, from the 16-byte boundary below
+};
+template <class T, class CT>
+struct alignas(16) TmaWarp {
+  TmaStage<CT> st[2];
+  T sx[8 * kWarpTile];  // x at the tile's nodes by rank, then element results by frame position
+  uint64_t bar[2];
+  uint32_t info[2][4];  // per stage: node count, node lead-in, second-coefficient lead-in
+};
+static_assert(sizeof(TmaStage<double>) % 16 == 0 && sizeof(TmaStage<float>) % 16 == 0, "stage alignment");
+static_assert(offsetof(TmaStage<double>, cb) % 16 == 0 && offsetof(TmaStage<double>, nodes) % 16 == 0, "fields");
+static_assert(offsetof(TmaStage<float>, cb) % 16 == 0 && offsetof(TmaStage<float>, nodes) % 16 == 0, "fields");
+
+// Lane 0: copy tile tt's records into stage st (p0, p1: its node list offsets).
+template <class T, class CT>
+__device__ __forceinline__ void tma_issue(TmaWarp<T, CT>& W, int st, int64_t tt, uint32_t p0, uint32_t p1,
+                                          const CT* ca, const CT* cb, const uint32_t* tile_nodes,
+                                          const uint2* eloc8, const uint32_t* wmeta, const uint8_t* ref8) {
+  TmaStage<CT>& S = W.st[st];
+  const uint32_t n0 = p0 & ~3u;
+  const uint32_t nbytes = ((p1 - n0 + 3u) & ~3u) * 4u;
+  uint32_t total = kWarpRefBytes + 8 * kWarpTile + 4 * kWarpTile + nbytes;
+  uintptr_t cb0 = 0;
+  uint32_t cbbytes = 0, cblead = 0;
+  if (ca) {
+    const uintptr_t cbs = reinterpret_cast<uintptr_t>(cb + tt * kWarpTile);
+    cb0 = cbs & ~uintptr_t(15);
+    cblead = uint32_t(cbs - cb0) / sizeof(CT);
+    cbbytes = (uint32_t(cbs - cb0) + kWarpTile * sizeof(CT) + 15u) & ~15u;
+    total += kWarpTile * sizeof(CT) + cbbytes;
+  }
+  W.info[st][0] = p1 - p0;
+  W.info[st][1] = p0 - n0;
+  W.info[st][2] = cblead;
+  mbar_expect_tx(&W.bar[st], total);
+  bulk_g2s(S.ref, ref8 + tt * kWarpRefBytes, kWarpRefBytes, &W.bar[st]);
+  bulk_g2s(S.eloc, eloc8 + tt * kWarpTile, 8 * kWarpTile, &W.bar[st]);
+  bulk_g2s(S.wm, wmeta + tt * kWarpTile, 4 * kWarpTile, &W.bar[st]);
+  if (ca) {
+    bulk_g2s(S.ca, ca + tt * kWarpTile, kWarpTile * sizeof(CT), &W.bar[st]);
+    bulk_g2s(S.cb, reinterpret_cast<const void*>(cb0), cbbytes, &W.bar[st]);
+  }
+  bulk_g2s(S.nodes, tile_nodes + n0, nbytes, &W.bar[st]);
+}
+
+// Warp-uniform bounded wait for the phase `parity` of bar.  try_wait
+// suspends the warp in hardware until the phase completes or a short
+// hardware limit passes; every lane sees the completed phase itself (its own
+// acquire of the staged data) before the warp goes on, and the warp gives up
+// together once lane clocks pass `limit` cycles.
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool tma_wait(uint64_t* bar, uint32_t parity, int /*lane*/, long long limit) {
+  const long long t0 = clock64();
+  while (true) {
+    if (__any_sync(0xffffffffu, clock64() - t0 > limit)) return false;
+    const bool done = mbar_try(bar, parity);
+    if (__all_sync(0xffffffffu, done)) return true;
+  }
+}
+
+template <class T, class CT, int MINB>
+__global__ void __launch_bounds__(32 * kTmaWarps, MINB) lapmass_warp_tma_kernel(
+    const uint32_t* __restrict__ wmeta, const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
+    int64_t ntiles, const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_nodes,
+    const uint2* __restrict__ eloc8, const uint8_t* __restrict__ ref8, const T* __restrict__ x, T* __restrict__ y,
+    long long wait_limit) {
+  extern __shared__ __align__(16) unsigned char tma_smem[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  TmaWarp<T, CT>& W = reinterpret_cast<TmaWarp<T, CT>*>(tma_smem)[w];
+  const int64_t nw = int64_t(gridDim.x) * kTmaWarps;
+  int64_t t = blockIdx.x * int64_t(kTmaWarps) + w;
+  if (t >= ntiles) return;
+  if (lane == 0) {
+    mbar_init(&W.bar[0], 1);
+    mbar_init(&W.bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncwarp();
+  // lane 0 keeps the node-list offsets of the tile after next (read early)
+  uint32_t q0 = 0, q1 = 0;
+  bool pend0 = false, pend1 = false;  // stage has copies not yet waited for
+  if (lane == 0) {
+    tma_issue(W, 0, t, __ldg(tile_ptr + t), __ldg(tile_ptr + t + 1), ca, cb, tile_nodes, eloc8, wmeta, ref8);
+    pend0 = true;
+    if (t + nw < ntiles) {
+      tma_issue(W, 1, t + nw, __ldg(tile_ptr + t + nw), __ldg(tile_ptr + t + nw + 1), ca, cb, tile_nodes, eloc8,
+                wmeta, ref8);
+      pend1 = true;
+    }
+    if (t + 2 * nw < ntiles) {
+      q0 = __ldg(tile_ptr + t + 2 * nw);
+      q1 = __ldg(tile_ptr + t + 2 * nw + 1);
+    }
+  }
+  __syncwarp();  // lane 0's stage info words are visible to the warp
+  uint32_t par0 = 0, par1 = 0;
+  bool failed = !tma_wait(&W.bar[0], par0, lane, wait_limit);
+  if (!failed) {
+    pend0 = false;
+    par0 ^= 1u;
+  }
+  T xc[kPipeIds];
+  if (!failed) {
+    const uint32_t nt = W.info[0][0], nl = W.info[0][1];
+#pragma unroll
+    for (int j = 0; j < kPipeIds; ++j) {
+      const uint32_t k = lane + 32 * j;
+      xc[j] = k < nt ? __ldg(x + (W.st[0].nodes[nl + k] & 0x7fffffffu)) : T(0);
+    }
+  }
+  int st = 0;
+  for (; !failed && t < ntiles; t += nw, st ^= 1) {
+    TmaStage<CT>& S = W.st[st];
+    T* sx = W.sx;
+    const uint32_t nt = W.info[st][0], nl = W.info[st][1], cbl = W.info[st][2];
+    const uint32_t* sn = S.nodes + nl;
+#pragma unroll
+    for (int j = 0; j < kPipeIds; ++j) {
+      const uint32_t k = lane + 32 * j;
+      if (k < nt) sx[k] = xc[j];
+    }
+    for (uint32_t k = lane + 32 * kPipeIds; k < nt; k += 32) sx[k] = __ldg(x + (sn[k] & 0x7fffffffu));
+    __syncwarp();
+    const bool live = t * kWarpTile + lane < E;
+    T wv[8];
+    if (live) {
+      const uint32_t m = S.wm[lane];
+      const uint2 L = S.eloc[lane];
+      const T a = ca ? T(S.ca[lane]) : T(1), b = ca ? T(S.cb[cbl + lane]) : T(1);
+      const T h = elem_h<T>(meta_lev(m));
+      const T f1 = a * h * T(0.5), f2 = b * h * h * h * T(0.125);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) wv[j] = sx[byte_of(L, j)];
+      const uint32_t mp = wmeta_mask(m);
+      if (mp) interp_frame(wv, mp);
+      lapmass_ref(wv, f1, f2);
+      if (mp) scatter_frame(wv, mp);
+    }
+    // x at the next tile's nodes, once its stage has landed
+    const bool has_next = t + nw < ntiles;
+    if (has_next) {
+      uint64_t* nb = &W.bar[st ^ 1];
+      if (!tma_wait(nb, st ? par0 : par1, lane, wait_limit)) {
+        failed = true;
+      } else {
+        if (st) {
+          pend0 = false;
+          par0 ^= 1u;
+        } else {
+          pend1 = false;
+          par1 ^= 1u;
+        }
+        const uint32_t nt2 = W.info[st ^ 1][0], nl2 = W.info[st ^ 1][1];
+        const uint32_t* sn2 = W.st[st ^ 1].nodes + nl2;
+#pragma unroll
+        for (int j = 0; j < kPipeIds; ++j) {
+          const uint32_t k = lane + 32 * j;
+          xc[j] = k < nt2 ? __ldg(x + (sn2[k] & 0x7fffffffu)) : T(0);
+        }
+      }
+    }
+    __syncwarp();  // every lane has read x: the buffer now takes the results
+    if (live) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) sx[j * kWarpTile + lane] = wv[j];
+    }
+    __syncwarp();
+    const uint2 pp = reinterpret_cast<const uint2*>(S.ref)[lane];
+    const uint2 rr = reinterpret_cast<const uint2*>(S.ref + 8 * kWarpTile)[lane];
+    const uint32_t ff = reinterpret_cast<const uint32_t*>(S.ref + 16 * kWarpTile)[lane];
+    T sum = T(0);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      if (ff & (1u << q)) {
+        const T v = sx[byte_of(pp, q)];
+        sum = (ff & (0x100u << q)) ? v : sum + v;
+        if (ff & (0x10000u << q)) {
+          const uint32_t id = sn[byte_of(rr, q)];
+          if (ff & (0x1000000u << q)) y[id] = sum;
+          else atomicAdd(y + (id & 0x7fffffffu), sum);
+        }
+      }
+    }
+    __syncwarp();  // stage st and the result buffer are free
+    if (failed) break;
+    if (lane == 0 && t + 2 * nw < ntiles) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      tma_issue(W, st, t + 2 * nw, q0, q1, ca, cb, tile_nodes, eloc8, wmeta, ref8);
+      if (st) pend1 = true;
+      else pend0 = true;
+      if (t + 3 * nw < ntiles) {
+        q0 = __ldg(tile_ptr + t + 3 * nw);
+        q1 = __ldg(tile_ptr + t + 3 * nw + 1);
+      }
+    }
+  }
+  if (failed) {
+    // record the timeout and let the copies still in flight land before the
+    // warp's shared memory can be reused
+    if (lane == 0) {
+      atomicExch(&g_wait_status, int(DG_ETIMEOUT));
+      const long long drain = wait_limit > (1ll << 31) ? wait_limit : (1ll << 31);
+      const long long t0 = clock64();
+      while ((pend0 && !mbar_test(&W.bar[0], par0)) || (pend1 && !mbar_test(&W.bar[1], par1)))
+        if (clock64() - t0 > drain) break;
+    }
+    __syncwarp();
+  }
+}
+
 template <class CT>
 __global__ void lapmass_diag_kernel(const uint32_t* __restrict__ nl, const uint32_t* __restrict__ meta,
                                     const CT* __restrict__ ca, const CT* __restrict__ cb, int64_t E,
@@ -548,7 +827,8 @@ __global__ void lapmass_dense_kernel(const uint32_t* __restrict__ nl, const uint
 // precision; DG_MATVEC_KERNEL=<index> forces one (testing).
 struct MatvecVariant {
   int block, per_sm;  // threads per CTA, CTAs per SM in the grid (0: one thread per element)
-  int kind;           // 0 atomic (BLOCK, MINB), 2 warp-tile, 3 + records prefetched, 4 + ids and x too
+  int kind;           // 0 atomic (BLOCK, MINB), 2 warp-tile, 3 + records prefetched, 4 + ids and x too,
+                      // 5 records staged by bulk copies
   int minb;
   const char* name;
 };
@@ -561,6 +841,9 @@ constexpr MatvecVariant kVariants[] = {
     {32 * kWarpCta, 8, 2, 8, "warp-tile 32 elems, 8 CTAs/SM"},
     {32 * kWarpCta, 3, 4, 3, "warp-tile 32 elems, 3 CTAs/SM, ids and x of the next tile in flight"},
     {32 * kWarpCta, 4, 4, 4, "warp-tile 32 elems, 4 CTAs/SM, ids and x of the next tile in flight"},
+    {32 * kTmaWarps, 5, 5, 5, "warp-tile 32 elems, records by bulk copy, 5 CTAs of 4 warps/SM"},
+    {32 * kTmaWarps, 6, 5, 6, "warp-tile 32 elems, records by bulk copy, 6 CTAs of 4 warps/SM"},
+    {32 * kTmaWarps, 7, 5, 7, "warp-tile 32 elems, records by bulk copy, 7 CTAs of 4 warps/SM"},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 
@@ -570,7 +853,22 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
   const MatvecVariant& V = kVariants[v];
   const unsigned g = V.per_sm ? grid_for(da->E, V.block, V.per_sm)
                               : unsigned((da->E + V.block - 1) / V.block > 0 ? (da->E + V.block - 1) / V.block : 1);
-  if (V.kind >= 2) {
+  if (V.kind == 5) {
+    const TileSet& ts = da->tiles_w;
+    const unsigned gt = grid_for(ts.ntiles * 32, 32 * kTmaWarps, V.per_sm);
+    const uint2* e8 = reinterpret_cast<const uint2*>(ts.eloc8.p);
+    const size_t smem = kTmaWarps * sizeof(TmaWarp<T, CT>);
+    const long long lim = g_wait_limit;
+    if (V.minb == 5)
+      lapmass_warp_tma_kernel<T, CT, 5><<<gt, 32 * kTmaWarps, smem, s>>>(ts.wmeta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
+                                                                        ts.nodes.p, e8, ts.ref8.p, x, y, lim);
+    else if (V.minb == 6)
+      lapmass_warp_tma_kernel<T, CT, 6><<<gt, 32 * kTmaWarps, smem, s>>>(ts.wmeta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
+                                                                        ts.nodes.p, e8, ts.ref8.p, x, y, lim);
+    else
+      lapmass_warp_tma_kernel<T, CT, 7><<<gt, 32 * kTmaWarps, smem, s>>>(ts.wmeta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p,
+                                                                        ts.nodes.p, e8, ts.ref8.p, x, y, lim);
+  } else if (V.kind >= 2) {
     const TileSet& ts = da->tiles_w;
     const unsigned gw = grid_for(ts.ntiles * 32, 32 * kWarpCta, V.per_sm);
     const uint2* e8 = reinterpret_cast<const uint2*>(ts.eloc8.p);
@@ -691,6 +989,20 @@ static dg_status lapmass_launch(dg_da* da, int& choice, const CT* ca, const CT* 
 }
 
 int matvec_variant_count() { return kNumVariants; }
+
+void set_wait_limit(long long cycles) { g_wait_limit = cycles > 0 ? cycles : kDefaultWaitLimit; }
+
+dg_status device_wait_status(cudaStream_t s) {
+  DG_CUDA(cudaStreamSynchronize(s));
+  int v = 0;
+  DG_CUDA(cudaMemcpyFromSymbol(&v, g_wait_status, sizeof(int)));
+  if (v) {
+    const int z = 0;
+    DG_CUDA(cudaMemcpyToSymbol(g_wait_status, &z, sizeof(int)));
+    DG_CHECK(false, DG_ETIMEOUT, "a bounded device wait of an operator kernel ran out");
+  }
+  return DG_OK;
+}
 
 const char* matvec_variant_name(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].name : "untuned"; }
 

@@ -479,7 +479,7 @@ dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s) {
   DG_TRY(ts.nend.alloc(nt * S));
   DG_TRY(ts.inc.alloc(nt * S));
   if (te == kWarpTile) {
-    DG_TRY(ts.eloc8.alloc(8 * E));
+    DG_TRY(ts.eloc8.alloc(8 * nt * kWarpTile));  // whole tiles
     DG_TRY(launch_tile_lists<kWarpTile>(da, nt, tmp.p, cnt.p, ts.nend.p, ts.inc.p, nullptr, ts.eloc8.p, s));
   } else {
     DG_TRY(ts.eloc.alloc(E));
@@ -495,7 +495,7 @@ dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s) {
   uint32_t mx = 0;
   for (uint32_t c : hc) mx = c > mx ? c : mx;
   ts.max_nodes = mx;
-  DG_TRY(ts.nodes.alloc(total));
+  DG_TRY(ts.nodes.alloc(total + kNodePad));
   tile_compact<<<grid_for(nt, 256, 8), 256, 0, s>>>(tmp.p, int(S), ts.ptr.p, nt, ts.nodes.p);
   DG_TRY(touch.alloc(da->N));
   DG_CUDA(cudaMemsetAsync(touch.p, 0, 4 * da->N, s));
@@ -518,7 +518,7 @@ dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s) {
     DG_TRY(ts.ref8.alloc(nt * kWarpRefBytes));
     warp_refs<<<grid_for(nt * 32, 256, 8), 256, 0, s>>>(ts.inc.p, ts.nend.p, ts.ptr.p, ts.nodes.p, da->meta.p, nt,
                                                          r3.p, ts.ref8.p);
-    DG_TRY(ts.wmeta.alloc(E));
+    DG_TRY(ts.wmeta.alloc(nt * kWarpTile));  // whole tiles
     warp_frame<<<grid_for(E, 256), 256, 0, s>>>(da->meta.p, E, reinterpret_cast<uint2*>(ts.eloc8.p), ts.wmeta.p);
     DG_CUDA(cudaGetLastError());
     DG_CUDA(cudaStreamSynchronize(s));  // r3 is freed on return

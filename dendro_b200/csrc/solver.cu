@@ -640,7 +640,7 @@ dg_status set_operators(dg_damg* m, const double* coef) {
     A->dof = 1;
     if (coef) {
       A->has_coef = true;
-      DG_TRY(A->coef.alloc(2 * L.da->E));
+      DG_TRY(A->coef.alloc(2 * L.da->E + kCoefPad));
       if (l == 0) {
         std::vector<double> soa(2 * L.da->E);
         for (int64_t e = 0; e < L.da->E; ++e) {
@@ -668,7 +668,7 @@ dg_status set_operators(dg_damg* m, const double* coef) {
         DG_CUDA(cudaStreamSynchronize(s));
         DG_CHECK(!herr, DG_EINVAL, "coarse element without fine elements");
       }
-      DG_TRY(A->coef32.alloc(2 * L.da->E));
+      DG_TRY(A->coef32.alloc(2 * L.da->E + kCoefPad));
       DG_TRY(convert_f64_to_f32(A->coef.p, A->coef32.p, 2 * L.da->E, s));
     }
     L.A = std::move(A);
@@ -1235,6 +1235,7 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
     rep->solve_ms = ms;
     rep->smoother_fallbacks = fallbacks;
   }
+  DG_TRY(device_wait_status(s));  // an operator kernel gave up waiting: the result is not valid
   return conv ? DG_OK : DG_ENOTCONVERGED;
 }
 

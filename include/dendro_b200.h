@@ -146,6 +146,16 @@ dg_status dg_mat_get_diagonal(dg_mat* A, double* d, void* stream);
 /* Same as dg_mat_mult with host x and y: copies in, applies, copies out and
  * synchronises (the call a PETSc MatShell callback makes on host Vec arrays). */
 dg_status dg_mat_mult_host(dg_mat* A, const double* x, double* y);
+/* Synchronise `stream`; DG_ETIMEOUT when a bounded device wait of an
+ * operator kernel (the bulk-copy staged launch shape waits for its copies)
+ * has run out since the last check, which clears it.  The results of the
+ * launches concerned are not valid.  dg_mat_mult_host and dg_damg_solve make
+ * the same check.  No reference counterpart: PETSc's MatMult reports errors
+ * through its return code (Jacobian2MatMult, omgNeumann.C:533-556, returns 0). */
+dg_status dg_device_check(void* stream);
+/* Test hook: the clock64 cycles such a wait lasts before it gives up
+ * (<= 0 restores the default of 2^31 cycles, about one second). */
+dg_status dg_set_device_wait_limit(int64_t cycles);
 int64_t dg_mat_size(const dg_mat* A); /* rows = dof * nodes */
 /* Launch shape of the scalar operator kernel that the autotuner picked on the
  * first application in the given precision ("untuned" before it). */

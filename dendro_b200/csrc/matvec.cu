@@ -281,6 +281,51 @@ constexpr int kWarpCta = 8;  // warps per CTA
 // byte j of a uint2, zero-extended (one byte permute)
 __device__ __forceinline__ uint32_t byte_of(uint2 r, int j) { return __byte_perm(j < 4 ? r.x : r.y, 0u, 0x4440u | uint32_t(j & 3)); }
 
+// Predicated global store / reduction-add (no branch; c == 0 skips the access).
+__device__ __forceinline__ void st_if(double* p, double v, uint32_t c) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.global.f64 [%0], %1;\n}" ::"l"(p), "d"(v),
+               "r"(c)
+               : "memory");
+}
+__device__ __forceinline__ void st_if(float* p, float v, uint32_t c) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.global.f32 [%0], %1;\n}" ::"l"(p), "f"(v),
+               "r"(c)
+               : "memory");
+}
+__device__ __forceinline__ void red_add_if(double* p, double v, uint32_t c) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q red.global.add.f64 [%0], %1;\n}" ::"l"(p),
+               "d"(v), "r"(c)
+               : "memory");
+}
+__device__ __forceinline__ void red_add_if(float* p, float v, uint32_t c) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q red.global.add.f32 [%0], %1;\n}" ::"l"(p),
+               "f"(v), "r"(c)
+               : "memory");
+}
+
+// The segmented sum of a lane's 8 sorted references, without branches:
+// sx holds the element results by frame position, sn the tile's node ids by
+// rank.  A reference that starts a sum replaces it; one whose flag says the
+// sum leaves stores it (node whole in this lane and tile) or adds it with a
+// global reduction.  Padding references (after a lane's last real one) point
+// at position 0 and rank 0 and carry no flags, so they read valid slots and
+// never leave.
+template <class T>
+__device__ __forceinline__ void warp_seg_sum(const T* sx, const uint32_t* sn, uint2 pp, uint2 rr, uint32_t ff,
+                                             T* __restrict__ y) {
+  T sum = T(0);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const T v = sx[byte_of(pp, q)];
+    sum = (ff & (0x100u << q)) ? v : sum + v;
+    const uint32_t id = sn[byte_of(rr, q)];
+    T* dst = y + (id & 0x7fffffffu);
+    const uint32_t leave = ff & (0x10000u << q), store = ff & (0x1000000u << q);
+    st_if(dst, sum, store);
+    red_add_if(dst, sum, leave && !store);
+  }
+}
+
 // Per-lane record of one tile: the lane's element and its 8 sorted references.
 template <class T>
 struct WarpTileLoad {
@@ -365,19 +410,7 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_kernel(
       for (int j = 0; j < 8; ++j) sx[j * kWarpTile + lane] = wv[j];
     }
     __syncwarp();
-    T sum = T(0);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      if (cur.ff & (1u << q)) {
-        const T v = sx[byte_of(cur.pp, q)];
-        sum = (cur.ff & (0x100u << q)) ? v : sum + v;
-        if (cur.ff & (0x10000u << q)) {
-          const uint32_t id = sn[byte_of(cur.rr, q)];
-          if (cur.ff & (0x1000000u << q)) y[id] = sum;  // the node's whole sum, node used by this tile only
-          else atomicAdd(y + (id & 0x7fffffffu), sum);
-        }
-      }
-    }
+    warp_seg_sum(sx, sn, cur.pp, cur.rr, cur.ff, y);
     __syncwarp();
     if (PF) cur = nxt;
   }
@@ -463,19 +496,7 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_pipe_kernel(
       for (int j = 0; j < 8; ++j) sx[j * kWarpTile + lane] = wv[j];
     }
     __syncwarp();
-    T sum = T(0);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      if (cur.ff & (1u << q)) {
-        const T v = sx[byte_of(cur.pp, q)];
-        sum = (cur.ff & (0x100u << q)) ? v : sum + v;
-        if (cur.ff & (0x10000u << q)) {
-          const uint32_t id = sn[byte_of(cur.rr, q)];
-          if (cur.ff & (0x1000000u << q)) y[id] = sum;
-          else atomicAdd(y + (id & 0x7fffffffu), sum);
-        }
-      }
-    }
+    warp_seg_sum(sx, sn, cur.pp, cur.rr, cur.ff, y);
     // x at the next tile's nodes: the ids have had the segmented sum to arrive
 #pragma unroll
     for (int j = 0; j < kPipeIds; ++j) {
@@ -725,19 +746,7 @@ __global__ void __launch_bounds__(32 * kTmaWarps, MINB) lapmass_warp_tma_kernel(
     const uint2 pp = reinterpret_cast<const uint2*>(S.ref)[lane];
     const uint2 rr = reinterpret_cast<const uint2*>(S.ref + 8 * kWarpTile)[lane];
     const uint32_t ff = reinterpret_cast<const uint32_t*>(S.ref + 16 * kWarpTile)[lane];
-    T sum = T(0);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      if (ff & (1u << q)) {
-        const T v = sx[byte_of(pp, q)];
-        sum = (ff & (0x100u << q)) ? v : sum + v;
-        if (ff & (0x10000u << q)) {
-          const uint32_t id = sn[byte_of(rr, q)];
-          if (ff & (0x1000000u << q)) y[id] = sum;
-          else atomicAdd(y + (id & 0x7fffffffu), sum);
-        }
-      }
-    }
+    warp_seg_sum(sx, sn, pp, rr, ff, y);
     __syncwarp();  // stage st and the result buffer are free
     if (failed) break;
     if (lane == 0 && t + 2 * nw < ntiles) {

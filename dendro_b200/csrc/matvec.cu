@@ -318,9 +318,9 @@ __device__ __forceinline__ void warp_seg_sum(const T* sx, const uint32_t* sn, ui
   for (int q = 0; q < 8; ++q) {
     const T v = sx[byte_of(pp, q)];
     sum = (ff & (0x100u << q)) ? v : sum + v;
-    const uint32_t id = sn[byte_of(rr, q)];
-    T* dst = y + (id & 0x7fffffffu);
     const uint32_t leave = ff & (0x10000u << q), store = ff & (0x1000000u << q);
+    const uint32_t id = leave ? sn[byte_of(rr, q)] : 0u;  // shared load only where the sum leaves
+    T* dst = y + (id & 0x7fffffffu);
     st_if(dst, sum, store);
     red_add_if(dst, sum, leave && !store);
   }

@@ -58,6 +58,9 @@ def parse():
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--solve-workload", default="lognormal4m_d16")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--vcycle-profile", metavar="WORKLOAD", default=None,
+                   help="only: one FP64 and one FP32 V(2,2) cycle on WORKLOAD's hierarchy between "
+                        "cudaProfilerStart/Stop (for ncu --profile-from-start off), then exit")
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     return p.parse_args()
 
@@ -318,7 +321,8 @@ def run_multi(dev, steps, nrhs=64):
                                 "achieved_gbs": round(alg / (ms * 1e-3) / 1e9, 1),
                                 "tflops": round(2 * 64 * nrhs * E * split / (ms * 1e-3) / 1e12, 2)}
     out["algorithmic_bytes"] = int(36 * E + 8 * nrhs * N)
-    out["method"] = "mma.sync m16n8k8 TF32 (split3: hi/lo TF32 split, three products), FP32 accumulation"
+    out["method"] = ("mma.sync m16n8k8 TF32, 32 right-hand sides per element pass on the warp tiles "
+                     "(split3: hi/lo TF32 split, three products), FP32 accumulation")
     return out
 
 
@@ -341,10 +345,44 @@ def cpu_baseline(octs, depth, coef, x, seconds):
             "sample": f"{n} full matvecs of the same mesh (E={mesh.E}, N={mesh.N}) in {dt:.1f} s, 1 thread"}
 
 
+def run_vcycle_profile(workload):
+    """One V(2,2) cycle of the FP64 and of the FP32 hierarchy on `workload`,
+    after three warm-up cycles each (operator shapes tuned per level and
+    precision), bracketed by cudaProfilerStart / cudaProfilerStop; prints
+    their times (CUDA events around the synchronising call)."""
+    import torch
+
+    import dendro_b200 as dg
+    from dendro_b200 import inputs as I
+    from dendro_b200.learned import vcycle
+    pts, depth = build_workload(workload, 1.0)
+    bal = dg.balanceOctree(dg.points2Octree(pts, depth, 1))
+    out = {"workload": workload}
+    for prec, name in ((0, "fp64"), (1, "fp32")):
+        m = dg.DAMG(bal, inner_prec=prec, use_graph=False)
+        b = torch.tensor(I.uniform_rhs(int(m.N[0]), 3), device="cuda")
+        for _ in range(3):
+            vcycle(m, b)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.profiler.start()
+        e0.record()
+        vcycle(m, b)
+        e1.record()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        out[name] = {"levels": m.nlevels, "elements": int(m.E[0]), "nodes": int(m.N[0]),
+                     "vcycle_ms": round(e0.elapsed_time(e1), 4)}
+        del m
+    print(json.dumps({"vcycle_profile": out}), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.vcycle_profile:
+        return run_vcycle_profile(args.vcycle_profile)
     if args.impl == "reference":
         return main_reference(args, rank, world)
     if world > 1:

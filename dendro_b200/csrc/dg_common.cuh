@@ -113,6 +113,10 @@ __device__ __forceinline__ uint2 xor_perm_bytes(uint2 r, uint32_t c) {
   }
   return r;
 }
+// byte j of a uint2, zero-extended (one byte permute)
+__device__ __forceinline__ uint32_t byte_of(uint2 r, int j) {
+  return __byte_perm(j < 4 ? r.x : r.y, 0u, 0x4440u | uint32_t(j & 3));
+}
 // The hanging mask in the same frame: bit j <- bit j ^ c.
 __host__ __device__ __forceinline__ uint32_t xor_perm_mask(uint32_t m, uint32_t c) {
   if (c & 1u) m = ((m & 0x55u) << 1) | ((m & 0xAAu) >> 1);
@@ -120,10 +124,25 @@ __host__ __device__ __forceinline__ uint32_t xor_perm_mask(uint32_t m, uint32_t 
   if (c & 4u) m = ((m & 0x0Fu) << 4) | ((m & 0xF0u) >> 4);
   return m;
 }
-// Per-element word of the warp-tile kernels: level | frame hanging mask << 8.
-__host__ __device__ __forceinline__ uint32_t wmeta_pack(uint32_t m) {
-  return meta_lev(m) | (xor_perm_mask(meta_mask(m), meta_cnum(m)) << 8);
+// The 18 element types are 18 hanging patterns in the child-number frame
+// (the same set for every child number, listed in a different order per
+// child), so an element's stencil in that frame depends on the pattern only.
+constexpr uint8_t kFrameMasks[18] = {0, 2, 4, 6, 14, 16, 18, 20, 22, 30, 50, 54, 62, 84, 86, 94, 118, 126};
+__host__ __device__ __forceinline__ uint32_t frame_type(uint32_t mp) {
+  const uint8_t fm[18] = {0, 2, 4, 6, 14, 16, 18, 20, 22, 30, 50, 54, 62, 84, 86, 94, 118, 126};
+  uint32_t t = 0;
+#pragma unroll
+  for (uint32_t i = 0; i < 18; ++i)
+    if (fm[i] == mp) t = i;
+  return t;
 }
+// Per-element word of the warp-tile kernels: level | frame hanging mask << 8
+// | frame type (index into kFrameMasks) << 16.
+__host__ __device__ __forceinline__ uint32_t wmeta_pack(uint32_t m) {
+  const uint32_t mp = xor_perm_mask(meta_mask(m), meta_cnum(m));
+  return meta_lev(m) | (mp << 8) | (frame_type(mp) << 16);
+}
+__host__ __device__ __forceinline__ uint32_t wmeta_ftype(uint32_t w) { return (w >> 16) & 31u; }
 __host__ __device__ __forceinline__ uint32_t wmeta_mask(uint32_t w) { return (w >> 8) & 255u; }
 
 // ----------------------------------------------------------------- launch --

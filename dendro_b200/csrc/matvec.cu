@@ -278,8 +278,6 @@ __global__ void residual_from_v(const T* __restrict__ b, T* __restrict__ t, T* _
 // with an FP64 global atomic (y is zeroed first).
 constexpr int kWarpCta = 8;  // warps per CTA
 
-// byte j of a uint2, zero-extended (one byte permute)
-__device__ __forceinline__ uint32_t byte_of(uint2 r, int j) { return __byte_perm(j < 4 ? r.x : r.y, 0u, 0x4440u | uint32_t(j & 3)); }
 
 // Predicated global store / reduction-add (no branch; c == 0 skips the access).
 __device__ __forceinline__ void st_if(double* p, double v, uint32_t c) {

@@ -252,6 +252,155 @@ __global__ void __launch_bounds__(32 * kMWarps) mrhs_warp_kernel(
   }
 }
 
+// Block form: per element the whole block of W right-hand sides of a pass
+// (W = 32 or 64, W / 16 MMAs sharing one B fragment), all in the
+// child-number frame: an element's node ranks come frame-ordered from the
+// warp tiles and its stencil fragment from the 18-entry frame table (9 KB,
+// read through L1).  The rows of the MMA map to right-hand sides
+// so that a lane's A values at a vertex are the F = W / 8 consecutive floats
+// F g .. F g + F - 1 of the node's row (chunk c, row g: rhs F g + 2c; row g + 8:
+// F g + 2c + 1): 16-byte loads straight from X; its D values at a vertex land
+// on the same F consecutive floats of the accumulator row as 16-byte
+// read-modify-writes.  The next PD elements' X values travel in a ring of
+// registers, walked PD elements at a time so that every slot is a
+// compile-time register.
+constexpr int kBWarps = 4;
+__host__ __device__ constexpr size_t mrhs_block_stride(uint32_t cap, int W) {
+  return size_t(cap) * (W + 4) + ((size_t(cap) + 3) & ~size_t(3));
+}
+
+template <int NS, int W, int PD>
+__global__ void __launch_bounds__(32 * kBWarps) mrhs_block_kernel(
+    const uint32_t* __restrict__ wmeta, const float* __restrict__ ca, const float* __restrict__ cb, int64_t E,
+    int64_t ntiles, const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_nodes,
+    const uint2* __restrict__ eloc8, const float4* __restrict__ ftbl, int R, uint32_t cap,
+    const float* __restrict__ X, float* __restrict__ Y) {
+  constexpr int F = W / 8, NV = F / 4, NC = W / 16, RW = W + 4;
+  extern __shared__ __align__(16) float mb_smem[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = lane >> 2, tq = lane & 3;
+  float* Ys = mb_smem + size_t(w) * mrhs_block_stride(cap, W);  // [cap][RW] rows, then the node ids
+  uint32_t* sn = reinterpret_cast<uint32_t*>(Ys + size_t(cap) * RW);
+  const int64_t nw = int64_t(gridDim.x) * kBWarps;
+  for (int64_t t = blockIdx.x * int64_t(kBWarps) + w; t < ntiles; t += nw) {
+    const uint32_t p0 = __ldg(tile_ptr + t), nt = __ldg(tile_ptr + t + 1) - p0;
+    for (uint32_t k = lane; k < nt; k += 32) sn[k] = __ldg(tile_nodes + p0 + k);
+    const int64_t e_own = t * kWarpTile + lane;
+    const int nel = int(E - t * kWarpTile < kWarpTile ? E - t * kWarpTile : kWarpTile);
+    float f1o = 0.f, f2o = 0.f;
+    uint32_t ft_o = 0;
+    uint2 Lo = make_uint2(0, 0);
+    if (e_own < E) {
+      const uint32_t m = __ldg(wmeta + e_own);
+      const float h = elem_hf(meta_lev(m));
+      const float a = ca ? __ldg(ca + e_own) : 1.f, b = cb ? __ldg(cb + e_own) : 1.f;
+      f1o = a * h * 0.5f;
+      f2o = b * h * h * h * 0.125f;
+      ft_o = wmeta_ftype(m) * 32;
+      Lo = __ldg(eloc8 + e_own);  // byte j: rank of frame vertex j
+    }
+    __syncwarp();
+    for (int r0 = 0; r0 < R; r0 += W) {
+      for (uint32_t i = lane; i < (W / 4) * nt; i += 32)
+        reinterpret_cast<float4*>(Ys + (i / (W / 4)) * RW)[i % (W / 4)] = make_float4(0.f, 0.f, 0.f, 0.f);
+      __syncwarp();
+      float4 ra[PD][NV], rb[PD][NV];
+      uint2 rL[PD];
+      uint32_t rf[PD];
+      auto fetch = [&](int slot, int el) {  // el < 32; beyond the tile's elements nothing is loaded
+        uint2 Ln;
+        Ln.x = __shfl_sync(0xffffffffu, Lo.x, el);
+        Ln.y = __shfl_sync(0xffffffffu, Lo.y, el);
+        rf[slot] = __shfl_sync(0xffffffffu, ft_o, el);
+        rL[slot] = Ln;
+        if (el < nel) {
+          const float4* a4 =
+              reinterpret_cast<const float4*>(X + int64_t(sn[byte_of(Ln, tq)] & 0x7fffffffu) * R + r0 + F * g);
+          const float4* b4 =
+              reinterpret_cast<const float4*>(X + int64_t(sn[byte_of(Ln, tq + 4)] & 0x7fffffffu) * R + r0 + F * g);
+#pragma unroll
+          for (int k = 0; k < NV; ++k) {
+            ra[slot][k] = __ldg(a4 + k);
+            rb[slot][k] = __ldg(b4 + k);
+          }
+        }
+      };
+#pragma unroll
+      for (int q = 0; q < PD; ++q) fetch(q, q);
+      for (int el0 = 0; el0 < nel; el0 += PD) {
+#pragma unroll
+        for (int q = 0; q < PD; ++q) {
+          const int el = el0 + q;
+          if (el >= nel) break;
+          float4 xa[NV], xb[NV];
+#pragma unroll
+          for (int k = 0; k < NV; ++k) {
+            xa[k] = ra[q][k];
+            xb[k] = rb[q][k];
+          }
+          const uint2 L = rL[q];
+          const float4 tb = __ldg(ftbl + rf[q] + lane);
+          const float f1 = __shfl_sync(0xffffffffu, f1o, el), f2 = __shfl_sync(0xffffffffu, f2o, el);
+          fetch(q, el + PD < 32 ? el + PD : 31);  // this slot now carries element el + PD
+          const float bf0 = f1 * tb.x + f2 * tb.z, bf1 = f1 * tb.y + f2 * tb.w;
+          const uint32_t bh0 = to_tf32(bf0), bh1 = to_tf32(bf1);
+          const uint32_t bl0 = to_tf32(bf0 - __uint_as_float(bh0)), bl1 = to_tf32(bf1 - __uint_as_float(bh1));
+          float d[NC][4];
+#pragma unroll
+          for (int cc = 0; cc < NC; ++cc) {
+            const float4& qa = xa[cc / 2];
+            const float4& qb = xb[cc / 2];
+            const float x0 = (cc & 1) ? qa.z : qa.x, x1 = (cc & 1) ? qa.w : qa.y;
+            const float x2 = (cc & 1) ? qb.z : qb.x, x3 = (cc & 1) ? qb.w : qb.y;
+            d[cc][0] = d[cc][1] = d[cc][2] = d[cc][3] = 0.f;
+            const uint32_t ah0 = to_tf32(x0), ah1 = to_tf32(x1), ah2 = to_tf32(x2), ah3 = to_tf32(x3);
+            if (NS == 1) {
+              mma_tf32(d[cc], ah0, ah1, ah2, ah3, bh0, bh1);
+            } else {
+              const uint32_t al0 = to_tf32(x0 - __uint_as_float(ah0)), al1 = to_tf32(x1 - __uint_as_float(ah1));
+              const uint32_t al2 = to_tf32(x2 - __uint_as_float(ah2)), al3 = to_tf32(x3 - __uint_as_float(ah3));
+              float e[4] = {0.f, 0.f, 0.f, 0.f};  // the two correction products, a chain of their own
+              mma_tf32(e, al0, al1, al2, al3, bh0, bh1);
+              mma_tf32(d[cc], ah0, ah1, ah2, ah3, bh0, bh1);
+              mma_tf32(e, ah0, ah1, ah2, ah3, bl0, bl1);
+#pragma unroll
+              for (int r = 0; r < 4; ++r) d[cc][r] += e[r];
+            }
+          }
+          // D: rows g / g + 8 of chunk cc are right-hand sides F g + 2 cc / F g + 2 cc + 1,
+          // at frame vertices 2 tq and 2 tq + 1
+          float4* yc = reinterpret_cast<float4*>(Ys + byte_of(L, 2 * tq) * RW + F * g);
+          float4* yd = reinterpret_cast<float4*>(Ys + byte_of(L, 2 * tq + 1) * RW + F * g);
+#pragma unroll
+          for (int k = 0; k < NV; ++k) {
+            float4 u = yc[k], v = yd[k];
+            u.x += d[2 * k][0];
+            u.y += d[2 * k][2];
+            u.z += d[2 * k + 1][0];
+            u.w += d[2 * k + 1][2];
+            v.x += d[2 * k][1];
+            v.y += d[2 * k][3];
+            v.z += d[2 * k + 1][1];
+            v.w += d[2 * k + 1][3];
+            yc[k] = u;
+            yd[k] = v;
+          }
+          __syncwarp();  // the next element may add into the same rows
+        }
+      }
+      for (uint32_t i = lane; i < (W / 4) * nt; i += 32) {
+        const uint32_t k = i / (W / 4), q = i % (W / 4);
+        const uint32_t id = sn[k];
+        const float4 v = reinterpret_cast<const float4*>(Ys + k * RW)[q];
+        float4* dst = reinterpret_cast<float4*>(Y + int64_t(id & 0x7fffffffu) * R + r0) + q;
+        if (id & 0x80000000u) atomicAdd(dst, v);
+        else *dst = v;
+      }
+      __syncwarp();
+    }
+  }
+}
+
 // Zero the rows of the nodes that several tiles share (their sums arrive by atomics).
 __global__ void zero_shared_rows(const uint32_t* __restrict__ shared, int64_t ns, int R4, float4* __restrict__ Y) {
   const int64_t n = ns * R4;
@@ -312,6 +461,53 @@ std::vector<float> stencil_tables() {
   return out;
 }
 
+// The 18 frame stencils (child number 0 frame, kFrameMasks order) in the
+// same per-lane fragment layout: T for a frame mask has vertex 0's frame
+// parent corner and hanging vertex i averages the nodes j with j a bit subset
+// of i (2 on an edge, 4 on a face).
+std::vector<float> frame_stencil_tables() {
+  const double M1[2][2] = {{2.0 / 3.0, 1.0 / 3.0}, {1.0 / 3.0, 2.0 / 3.0}};
+  const double K1[2][2] = {{0.5, -0.5}, {-0.5, 0.5}};
+  double K[8][8], Mm[8][8];
+  for (int i = 0; i < 8; ++i)
+    for (int j = 0; j < 8; ++j) {
+      const int ix = i & 1, iy = (i >> 1) & 1, iz = i >> 2, jx = j & 1, jy = (j >> 1) & 1, jz = j >> 2;
+      Mm[i][j] = M1[ix][jx] * M1[iy][jy] * M1[iz][jz];
+      K[i][j] = K1[ix][jx] * M1[iy][jy] * M1[iz][jz] + M1[ix][jx] * K1[iy][jy] * M1[iz][jz] +
+                M1[ix][jx] * M1[iy][jy] * K1[iz][jz];
+    }
+  std::vector<float> out(size_t(18) * 32 * 4);
+  for (int t = 0; t < 18; ++t) {
+    const uint32_t mask = kFrameMasks[t];
+    double T[8][8] = {};
+    for (int i = 0; i < 8; ++i) {
+      if (!((mask >> i) & 1u)) {
+        T[i][i] = 1.0;
+        continue;
+      }
+      const double w = __builtin_popcount(uint32_t(i)) == 1 ? 0.5 : 0.25;
+      for (int j = 0; j < 8; ++j)
+        if ((uint32_t(j) & ~uint32_t(i)) == 0u) T[i][j] = w;
+    }
+    for (int lane = 0; lane < 32; ++lane) {
+      const int g = lane >> 2, tq = lane & 3;
+      const int rows[2] = {tq, tq + 4};
+      float* o = out.data() + (size_t(t) * 32 + lane) * 4;
+      for (int h = 0; h < 2; ++h) {
+        double sl = 0, sm = 0;
+        for (int p = 0; p < 8; ++p)
+          for (int q = 0; q < 8; ++q) {
+            sl += T[p][g] * K[p][q] * T[q][rows[h]];
+            sm += T[p][g] * Mm[p][q] * T[q][rows[h]];
+          }
+        o[h] = float(sl);
+        o[2 + h] = float(sm);
+      }
+    }
+  }
+  return out;
+}
+
 }  // namespace
 
 dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int R, int split, cudaStream_t s) {
@@ -336,11 +532,46 @@ dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int R, int split
   const float* ca = A->has_coef ? A->coef32.p : nullptr;
   const float* cb = A->has_coef ? A->coef32.p + da->E : nullptr;
   static int form = -1;
-  if (form < 0) {  // DG_MRHS_KERNEL: direct (default) | stage | cta
+  if (form < 0) {  // DG_MRHS_KERNEL: block (default, 32 per pass) | block64 | direct | stage | cta
     const char* e = getenv("DG_MRHS_KERNEL");
-    form = (e && !strcmp(e, "cta")) ? 2 : (e && !strcmp(e, "stage")) ? 1 : 0;
+    form = (e && !strcmp(e, "cta"))       ? 2
+           : (e && !strcmp(e, "stage"))   ? 1
+           : (e && !strcmp(e, "direct"))  ? 0
+           : (e && !strcmp(e, "block64")) ? 4
+                                          : 3;
   }
-  if (form < 2) {
+  if (form >= 3 && R % 32 == 0) {
+    static float4* ftbls[64] = {};  // frame tables, one per device, kept for the process
+    if (!ftbls[dev]) {
+      std::vector<float> h = frame_stencil_tables();
+      float4* p = nullptr;
+      DG_CUDA(cudaMalloc(&p, h.size() * sizeof(float)));
+      DG_CUDA(cudaMemcpy(p, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+      ftbls[dev] = p;
+    }
+    const TileSet& ts = da->tiles_w;
+    if (ts.nshared)
+      zero_shared_rows<<<grid_for(ts.nshared * (R / 4), 256, 8), 256, 0, s>>>(ts.shared.p, ts.nshared, R / 4,
+                                                                             reinterpret_cast<float4*>(Y));
+    const uint32_t cap = ts.max_nodes;
+    const int W = (R % 64 == 0 && form == 4) ? 64 : 32;
+    const int smem = int(kBWarps * mrhs_block_stride(cap, W) * sizeof(float));
+    DG_CHECK(smem <= 220 * 1024, DG_EINVAL, "mat_mult_multi: tile node count too large");
+    auto kern = W == 64 ? (split == 1 ? mrhs_block_kernel<1, 64, 2> : mrhs_block_kernel<3, 64, 2>)
+                        : (split == 1 ? mrhs_block_kernel<1, 32, 3> : mrhs_block_kernel<3, 32, 3>);
+    static int granted_b[4] = {48 * 1024, 48 * 1024, 48 * 1024, 48 * 1024};
+    int& gr = granted_b[(W == 64 ? 2 : 0) + (split == 1 ? 0 : 1)];
+    if (smem > gr) {
+      DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      gr = smem;
+    }
+    const unsigned grid = grid_for(ts.ntiles * 32, 32 * kBWarps, 16);
+    kern<<<grid, 32 * kBWarps, smem, s>>>(ts.wmeta.p, ca, cb, da->E, ts.ntiles, ts.ptr.p, ts.nodes.p,
+                                          reinterpret_cast<const uint2*>(ts.eloc8.p), ftbls[dev], R, cap, X, Y);
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+  }
+  if (form != 2) {  // warp tiles, 16 right-hand sides per pass
     const TileSet& ts = da->tiles_w;
     if (ts.nshared)
       zero_shared_rows<<<grid_for(ts.nshared * (R / 4), 256, 8), 256, 0, s>>>(ts.shared.p, ts.nshared, R / 4,

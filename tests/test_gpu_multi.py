@@ -18,8 +18,11 @@ def setup(gpu, oracle, name):
     return oracle.Mesh(bal, d), gpu.DA(gpu.Octree.from_octants(bal, d))
 
 
+# 16 and 48 right-hand sides take the 16-per-pass kernel, multiples of 32 the
+# 32-wide block kernel (DG_MRHS_KERNEL=block64: 64-wide where they divide)
 @pytest.mark.parametrize("name,nrhs,coef", [("lognormal20k_d12", 32, True), ("gauss20k_d10", 16, False),
-                                             ("corner_points_d5", 48, True)])
+                                             ("corner_points_d5", 48, True), ("lognormal20k_d12", 64, True),
+                                             ("gauss20k_d10", 96, False), ("uniform8k_d9_m4", 64, False)])
 def test_multi_rhs_matches_oracle(gpu, oracle, name, nrhs, coef):
     import torch
     ref, da = setup(gpu, oracle, name)

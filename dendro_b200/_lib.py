@@ -110,6 +110,13 @@ def lib():
         "dg_damg_batch_offsets": ([P, I, P, P], I),
         "dg_vec_dot_noalloc": ([P, P, I64, P, P], I),
         "dg_device_check": ([P], I),
+        "dg_write_pts": ([C.c_char_p, P, I64], I),
+        "dg_read_pts": ([C.c_char_p, P, I64, I64P], I),
+        "dg_write_data_pts": ([C.c_char_p, P, P, I64], I),
+        "dg_read_data_pts": ([C.c_char_p, P, P, I64, I64P], I),
+        "dg_octree_write": ([P, C.c_char_p], I),
+        "dg_octree_read": ([C.c_char_p, PP], I),
+        "dg_da_dump_mesh": ([P, C.c_char_p], I),
         "dg_set_device_wait_limit": ([I64], I),
     }
     for name, (args, res) in sig.items():
@@ -135,7 +142,8 @@ def exported_symbols():
         "dg_mlp_param_count", "dg_mlp_create", "dg_mlp_get_params", "dg_mlp_set_params", "dg_mlp_forward",
         "dg_mlp_gradient", "dg_mlp_train_step", "dg_mlp_destroy", "dg_damg_set_smoother", "dg_damg_features",
         "dg_vec_dot_noalloc", "dg_mat_kernel_count", "dg_mat_set_kernel", "dg_device_check",
-        "dg_set_device_wait_limit",
+        "dg_set_device_wait_limit", "dg_write_pts", "dg_read_pts", "dg_write_data_pts", "dg_read_data_pts",
+        "dg_octree_write", "dg_octree_read", "dg_da_dump_mesh",
         "dg_mat_mult_multi", "dg_damg_set_tolerances",
     ]
 

@@ -6,6 +6,7 @@ device tensors for the resident path and host arrays for the end-to-end path.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -60,6 +61,51 @@ def points2Octree(pts, maxDepth: int, maxNumPts: int = 1) -> Octree:
     else:
         a = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
         check(lib().dg_points2octree(ptr(a), len(a), 0, maxDepth, maxNumPts, C.byref(h)), "points2octree")
+    return Octree(h)
+
+
+def writePtsToFile(path, pts) -> None:
+    """ot::writePtsToFile (src/oct/OctFunctions.C:370): uint32 count + xyz FP64."""
+    a = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+    check(lib().dg_write_pts(os.fsencode(path), ptr(a), len(a)), "write_pts")
+
+
+def readPtsFromFile(path) -> np.ndarray:
+    """ot::readPtsFromFile (src/oct/OctFunctions.C:313): the points, [n, 3]."""
+    n = C.c_int64()
+    check(lib().dg_read_pts(os.fsencode(path), None, 0, C.byref(n)), "read_pts")
+    out = np.empty((n.value, 3))
+    check(lib().dg_read_pts(os.fsencode(path), ptr(out), n.value, C.byref(n)), "read_pts")
+    return out
+
+
+def writeDataPtsToFile(path, pts, vals) -> None:
+    """ot::writeDataPtsToFile (src/oct/OctFunctions.C:387): count, xyz, one value per point."""
+    a = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+    v = np.ascontiguousarray(vals, np.float64).reshape(-1)
+    if len(v) != len(a):
+        raise ValueError("one value per point")
+    check(lib().dg_write_data_pts(os.fsencode(path), ptr(a), ptr(v), len(a)), "write_data_pts")
+
+
+def readDataPtsFromFile(path):
+    """ot::readDataPtsFromFile (src/oct/OctFunctions.C:343): (points [n, 3], values [n])."""
+    n = C.c_int64()
+    check(lib().dg_read_data_pts(os.fsencode(path), None, None, 0, C.byref(n)), "read_data_pts")
+    pts, vals = np.empty((n.value, 3)), np.empty(n.value)
+    check(lib().dg_read_data_pts(os.fsencode(path), ptr(pts), ptr(vals), n.value, C.byref(n)), "read_data_pts")
+    return pts, vals
+
+
+def writeNodesToFile(path, octree: Octree) -> None:
+    """ot::writeNodesToFile (src/oct/OctFunctions.C:424): the .ot text format."""
+    check(lib().dg_octree_write(octree.h, os.fsencode(path)), "octree_write")
+
+
+def readNodesFromFile(path) -> Octree:
+    """ot::readNodesFromFile (src/oct/OctFunctions.C:403): an .ot file as an octree on the GPU."""
+    h = C.c_void_p()
+    check(lib().dg_octree_read(os.fsencode(path), C.byref(h)), "octree_read")
     return Octree(h)
 
 
@@ -130,6 +176,11 @@ class DA:
         c = np.empty((self.E, 3))
         check(lib().dg_da_element_centers(self.h, ptr(c)), "element_centers")
         return c
+
+    def dumpMesh(self, prefix: str) -> None:
+        """The files of examples/src/drivers/dumpMesh.C for one rank:
+        <prefix>_NL_0_1.out, <prefix>_EL_0_1.out, <prefix>_M_0_1.out."""
+        check(lib().dg_da_dump_mesh(self.h, os.fsencode(prefix)), "da_dump_mesh")
 
 
 class _Mat:

@@ -78,6 +78,26 @@ uint32_t dg_octree_max_depth(const dg_octree* t);
 dg_status dg_octree_export(const dg_octree* t, dg_octant* host_out);
 void dg_octree_destroy(dg_octree* t);
 
+/* ------------------------------------------------------------ files --- */
+/* The reference drivers' file formats, on the host (no GPU needed for the
+ * point files).  Point files: readPtsFromFile / writePtsToFile
+ * (src/oct/OctFunctions.C:313-341, 370-385): uint32 count, then xyz FP64
+ * interleaved; the writer leaves the file empty for no points, and an empty
+ * file reads as no points.  dg_read_pts with pts == NULL only returns the
+ * count; otherwise capacity (in points) must hold it. */
+dg_status dg_write_pts(const char* path, const double* pts, int64_t n);
+dg_status dg_read_pts(const char* path, double* pts, int64_t capacity, int64_t* n);
+/* Points with one value each: readDataPtsFromFile / writeDataPtsToFile
+ * (OctFunctions.C:343-368, 387-401): the count, the coordinates, the values. */
+dg_status dg_write_data_pts(const char* path, const double* pts, const double* vals, int64_t n);
+dg_status dg_read_data_pts(const char* path, double* pts, double* vals, int64_t capacity, int64_t* n);
+/* Octree files (.ot): writeNodesToFile / readNodesFromFile
+ * (OctFunctions.C:403-439): "3 maxDepth", the count, "x y z level" per octant
+ * (flags are not written).  The reader rejects a file that is not a sorted
+ * linear octree (DG_EUNBALANCED), as dg_octree_from_octants does. */
+dg_status dg_octree_write(const dg_octree* t, const char* path);
+dg_status dg_octree_read(const char* path, dg_octree** out);
+
 /* ---------------------------------------------------------------- mesh --- */
 
 /* ot::DA::DA (include/oda/oda.h:500; src/oda/oda.C:175 -> DA_FactoryPart0..3,
@@ -113,6 +133,14 @@ dg_status dg_da_export(const dg_da* da, uint32_t* nlist, uint8_t* hmask, uint8_t
 /* Element centres in [0,1]^3, xyz interleaved (CalculateCenters,
  * examples/src/backend/omgNeumann.C:788-820); out is host memory [E][3]. */
 dg_status dg_da_element_centers(const dg_da* da, double* host_out);
+/* The files of examples/src/drivers/dumpMesh.C for one rank of one:
+ * <prefix>_NL_0_1.out (node count; per node, in order of first visit over
+ * the elements, anchor x y z and global id), <prefix>_EL_0_1.out (maxDepth,
+ * element count; per element anchor x y z, level - 1, global id) and
+ * <prefix>_M_0_1.out (element count; per element its id and 8 node ids);
+ * 4-byte integers, embedded coordinates.  Byte-identical to the reference's
+ * output on the same balanced octree. */
+dg_status dg_da_dump_mesh(const dg_da* da, const char* prefix);
 void dg_da_destroy(dg_da* da);
 
 /* ----------------------------------------------------------- operators --- */

@@ -13,6 +13,7 @@ modified and nothing it contains is committed.
 
 Outputs (git-ignored; they travel to the GPU box with the snapshot):
   oracle/_ref/dendro_ref       driver binary
+  oracle/_ref/dendro_ref_dumpmesh  the reference's examples/src/drivers/dumpMesh.C, single rank
   oracle/_ref/stencils/*.inp   the reference's stencil tables (read from cwd)
 """
 import os
@@ -75,7 +76,8 @@ def main():
     flags = ["-O1", "-g", "-std=c++11", "-fopenmp", "-w", "-fpermissive", "-D__USE_PVT_DA_IN_MG__", "-D__SILENT_MODE__",
              "-include", os.path.join(pdir, "rotation.h"), "-include", os.path.join(pdir, "TreeNode.h")]
     objs, procs = [], []
-    for src in SOURCES + [os.path.join(HERE, "ref_driver.cpp")]:
+    for src in SOURCES + [os.path.join(HERE, "ref_driver.cpp"), os.path.join(HERE, "dump_stubs.cpp"),
+                          "examples/src/drivers/dumpMesh.C"]:
         path = src if os.path.isabs(src) else os.path.join(REF, src)
         obj = os.path.join(OUT, "obj", os.path.basename(src) + ".o")
         objs.append(obj)
@@ -94,7 +96,14 @@ def main():
     if bad:
         print("reference build failed:", bad)
         return 1
-    subprocess.check_call(["g++", "-fopenmp", "-rdynamic", "-o", os.path.join(OUT, "dendro_ref"), *objs])
+    lib_objs, driver_obj, stub_obj, dump_obj = objs[:-3], objs[-3], objs[-2], objs[-1]
+    subprocess.check_call(["g++", "-fopenmp", "-rdynamic", "-o", os.path.join(OUT, "dendro_ref"), *lib_objs,
+                           driver_obj])
+    # the mesh dump needs the octree, mesh and support sources only
+    mesh_objs = [o for o, src in zip(lib_objs, SOURCES) if src.split("/")[1] in ("oct", "oda", "par", "binOps",
+                                                                                   "point", "hilbert")]
+    subprocess.check_call(["g++", "-fopenmp", "-rdynamic", "-o", os.path.join(OUT, "dendro_ref_dumpmesh"),
+                           *mesh_objs, stub_obj, dump_obj])
     sdir = os.path.join(OUT, "stencils")
     os.makedirs(sdir, exist_ok=True)
     for f in os.listdir(os.path.join(REF, "Stencils")):

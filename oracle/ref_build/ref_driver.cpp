@@ -19,6 +19,11 @@
 //       DAMGCreateAndSetDA + DAMGSetUp; per level the node anchors, and the
 //       restriction / prolongation of the vectors level<l>_in.f64 /
 //       coarse<l>_in.f64 found in outdir
+//   dendro_ref io <octs.u32> <maxDepth> <pts.f64> <vals.f64> <outdir>
+//       the reference's file writers (src/oct/OctFunctions.C:313-440):
+//       writeNodesToFile -> octs.ot, writePtsToFile -> pts.pts,
+//       writeDataPtsToFile -> data.pts; then its readers on those files:
+//       octs_rt.u32, pts_rt.f64, data_pts_rt.f64, data_vals_rt.f64
 //
 // Octant files hold 4 x uint32 per octant (x, y, z, level); run from a
 // directory that holds the reference's Stencils/*.inp (they are read from the
@@ -217,6 +222,26 @@ int main(int argc, char** argv) {
     write_octs(dir + "/bal.u32", bal);
     ot::coarsenOctree(bal, coarse);
     write_octs(dir + "/coarse.u32", coarse);
+    return 0;
+  }
+  if (mode == "io" && argc >= 7) {
+    unsigned D = atoi(argv[3]);
+    std::vector<ot::TreeNode> octs = read_octs(argv[2], D);
+    std::vector<double> pts = read_raw<double>(argv[4]), vals = read_raw<double>(argv[5]);
+    std::string dir = argv[6];
+    std::string fo = dir + "/octs.ot", fp = dir + "/pts.pts", fd = dir + "/data.pts";
+    ot::writeNodesToFile(&fo[0], octs);
+    ot::writePtsToFile(&fp[0], pts);
+    ot::writeDataPtsToFile(&fd[0], pts, vals);
+    std::vector<ot::TreeNode> o2;
+    ot::readNodesFromFile(&fo[0], o2);
+    write_octs(dir + "/octs_rt.u32", o2);
+    std::vector<double> p2, p3, v3;
+    if (!pts.empty()) ot::readPtsFromFile(&fp[0], p2);  // its writer leaves no header for no points
+    write_raw(dir + "/pts_rt.f64", p2.data(), p2.size());
+    ot::readDataPtsFromFile(&fd[0], p3, v3);
+    write_raw(dir + "/data_pts_rt.f64", p3.data(), p3.size());
+    write_raw(dir + "/data_vals_rt.f64", v3.data(), v3.size());
     return 0;
   }
   if (mode == "mesh" && argc >= 5) {

@@ -7,7 +7,11 @@ of the reference's stencil tables (Stencils/*.inp).  Needs the reference
 tree and the reference build; the fixtures it writes are committed and the
 tests read only them.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # everything
+    python tests/golden/make_golden.py --io-only  # the file-format fixtures io_*.npz
+
+The file-format fixtures also run oracle/_ref/dendro_ref_dumpmesh, the
+reference's examples/src/drivers/dumpMesh.C built single-rank.
 
 Inputs whose linear octree the reference cannot produce (its points2Octree
 does not terminate above 8 points at its HEAD) start from the oracle's
@@ -17,6 +21,7 @@ operators and the transfers.
 from __future__ import annotations
 
 import os
+import shutil
 import subprocess
 import sys
 import tempfile
@@ -138,6 +143,35 @@ def transfer_fixture(tmp):
     np.savez_compressed(os.path.join(OUT, f"transfer_{name}.npz"), **rec)
 
 
+IO_CASES = ["corner_points_d5", "uniform600_d7", "gauss1k_d8"]
+DUMP_BIN = os.path.join(ROOT, "oracle", "_ref", "dendro_ref_dumpmesh")
+
+
+def io_fixture(tmp, name):
+    """The reference's file writers and readers (src/oct/OctFunctions.C:313-439)
+    on the mesh case's points and balanced octree, and its mesh dump
+    (examples/src/drivers/dumpMesh.C, one rank) of that octree."""
+    z = np.load(os.path.join(OUT, f"mesh_{name}.npz"))
+    bal, depth = z["bal"], int(z["depth"])
+    pts = MESH_CASES[name]()[0]
+    vals = np.random.default_rng(21).uniform(-1, 1, len(pts))
+    bal.astype(np.uint32).tofile(os.path.join(tmp, "octs.u32"))
+    pts.astype(np.float64).tofile(os.path.join(tmp, "pts.f64"))
+    vals.tofile(os.path.join(tmp, "vals.f64"))
+    run("io", os.path.join(tmp, "octs.u32"), depth, os.path.join(tmp, "pts.f64"), os.path.join(tmp, "vals.f64"), tmp)
+    rd = lambda f, dt=np.uint8: np.fromfile(os.path.join(tmp, f), dt)  # noqa: E731
+    assert np.array_equal(rd("octs_rt.u32", np.uint32).reshape(-1, 4), bal)
+    assert np.array_equal(rd("pts_rt.f64", np.float64).reshape(-1, 3), pts)
+    assert np.array_equal(rd("data_vals_rt.f64", np.float64), vals)
+    shutil.copy(os.path.join(tmp, "octs.ot"), os.path.join(tmp, "m0_1.ot"))
+    r = subprocess.run([DUMP_BIN, os.path.join(tmp, "m")], cwd=REF_CWD, capture_output=True, text=True, timeout=600)
+    if r.returncode:
+        raise RuntimeError(f"reference dumpMesh failed ({r.returncode}): {r.stderr[-2000:]}")
+    np.savez_compressed(os.path.join(OUT, f"io_{name}.npz"), depth=depth, bal=bal, pts=pts, vals=vals,
+                        ot=rd("octs.ot"), pts_file=rd("pts.pts"), data_file=rd("data.pts"),
+                        nl=rd("m_NL_0_1.out"), el=rd("m_EL_0_1.out"), m=rd("m_M_0_1.out"))
+
+
 def table_digest(a):
     """Checksums of each (child number, type) table: sum, sum of squares,
     sum of magnitudes and a position-weighted sum."""
@@ -164,11 +198,18 @@ def main():
     if "--stencils-only" in sys.argv:
         stencil_digests()
         return
+    if "--io-only" in sys.argv:
+        with tempfile.TemporaryDirectory() as tmp:
+            for name in IO_CASES:
+                io_fixture(tmp, name)
+        return
     with tempfile.TemporaryDirectory() as tmp:
         p2o_fixture(tmp)
         for name in MESH_CASES:
             mesh_fixture(tmp, name)
         transfer_fixture(tmp)
+        for name in IO_CASES:
+            io_fixture(tmp, name)
     stencil_digests()
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):

@@ -447,6 +447,65 @@ const Tables& tables() {
   return *g_tables;
 }
 
+// Type-1 tables (LapType1Stencils.inp / MassType1Stencils.inp, loaded by
+// createLmatType1 / createMmatType1, examples/src/backend/handleType1Stencils.C:
+// [coarse child number][element type][fine child][8][8]): the stiffness and mass
+// of fine child f of a coarse element in the coarse element's vertex basis,
+// T^T P_f^T (K/2) P_f T and T^T P_f^T (M/8) P_f T, with P_f the trilinear
+// interpolation from the coarse vertices to child f's vertices and the
+// factors 1/2, 1/8 the child's h/2 and h^3/8 against the coarse ones.
+struct Tables1 {
+  double L[8][18][8][8][8], Ms[8][18][8][8][8];
+  Tables1() {
+    const RefMats& R = refmats();
+    for (uint32_t f = 0; f < 8; ++f) {
+      double P[8][8];  // child vertex v <- coarse vertex w
+      for (int v = 0; v < 8; ++v)
+        for (int w = 0; w < 8; ++w) {
+          double p = 1.0;
+          for (int d = 0; d < 3; ++d) {
+            const double s = 0.5 * (((f >> d) & 1) + ((v >> d) & 1));  // coordinate in [0, 1]
+            p *= ((w >> d) & 1) ? s : 1.0 - s;
+          }
+          P[v][w] = p;
+        }
+      double Kf[8][8], Mf[8][8];  // P^T K P / 2, P^T M P / 8
+      for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < 8; ++j) {
+          double k = 0, m = 0;
+          for (int a = 0; a < 8; ++a)
+            for (int b = 0; b < 8; ++b) {
+              k += P[a][i] * R.K[a][b] * P[b][j];
+              m += P[a][i] * R.M[a][b] * P[b][j];
+            }
+          Kf[i][j] = k / 2.0;
+          Mf[i][j] = m / 8.0;
+        }
+      for (uint32_t c = 0; c < 8; ++c)
+        for (int t = 0; t < 18; ++t) {
+          double T[8][8];
+          hanging_T(c, kEtypeMask[c][t], T);
+          for (int i = 0; i < 8; ++i)
+            for (int j = 0; j < 8; ++j) {
+              double l = 0, m = 0;
+              for (int a = 0; a < 8; ++a)
+                for (int b = 0; b < 8; ++b) {
+                  l += T[a][i] * Kf[a][b] * T[b][j];
+                  m += T[a][i] * Mf[a][b] * T[b][j];
+                }
+              L[c][t][f][i][j] = l;
+              Ms[c][t][f][i][j] = m;
+            }
+        }
+    }
+  }
+};
+Tables1* g_tables1 = nullptr;
+const Tables1& tables1() {
+  if (!g_tables1) g_tables1 = new Tables1();
+  return *g_tables1;
+}
+
 // -------------------------------------------------------------- operators --
 // JAC_TYPE2_ELEM_MULT_BLOCK / JAC_TYPE2_MULT_BLOCK (examples/src/backend/
 // omgNeumann.C:468-530): y = sum_e (a_e h/2 L[c][t] + b_e h^3/8 M[c][t]) x_e,
@@ -594,6 +653,66 @@ int coarse_coef(const Mesh& F, const double* fc, const Mesh& C, std::vector<doub
   return 0;
 }
 
+// JAC_TYPE3_MULT_BLOCK (examples/src/backend/omgJac.C:2139-2233): the
+// operator of a coarse level from the next finer level's coefficients fc.
+// A coarse element that is also a fine element uses its coefficients with the
+// type-2 tables; one split into 8 fine children uses their mean with the
+// type-2 tables when the children's a and b each vary by at most tol times
+// their maximum (-tolToCoarsenMatProp, default 1e-12), else the sum over the
+// children of their own a, b with the type-1 tables.
+int jacobian3(const Mesh& F, const double* fc, const Mesh& C, const double* x, double* y, double tol = 1e-12) {
+  const Tables& T2 = tables();
+  const Tables1& T1 = tables1();
+  std::fill(y, y + C.N, 0.0);
+  size_t f = 0;
+  for (size_t e = 0; e < C.E; ++e) {
+    const Oct& o = C.oct[e];
+    while (f < F.E && !(F.oct[f].x == o.x && F.oct[f].y == o.y && F.oct[f].z == o.z)) ++f;
+    if (f >= F.E) return -1;
+    const double h = std::ldexp(1.0, 1 - int(C.elev[e]));
+    const uint32_t* idx = &C.nlist[8 * e];
+    const uint32_t c = C.cnum[e], t = C.etype[e];
+    double A[8][8];
+    if (F.oct[f].lev() == o.lev()) {
+      const double f1 = fc[2 * f] * h / 2.0, f2 = fc[2 * f + 1] * h * h * h / 8.0;
+      for (int k = 0; k < 8; ++k)
+        for (int j = 0; j < 8; ++j) A[k][j] = f1 * T2.L[c][t][k][j] + f2 * T2.Ms[c][t][k][j];
+      ++f;
+    } else {
+      double p1[8], p2[8];
+      for (int k = 0; k < 8; ++k, ++f) {
+        p1[k] = fc[2 * f];
+        p2[k] = fc[2 * f + 1];
+      }
+      double mx1 = p1[0], mn1 = p1[0], mx2 = p2[0], mn2 = p2[0], s1 = 0, s2 = 0;
+      for (int k = 0; k < 8; ++k) {
+        mx1 = std::max(mx1, p1[k]);
+        mn1 = std::min(mn1, p1[k]);
+        mx2 = std::max(mx2, p2[k]);
+        mn2 = std::min(mn2, p2[k]);
+        s1 += p1[k];
+        s2 += p2[k];
+      }
+      if (mx1 - mn1 <= tol * mx1 && mx2 - mn2 <= tol * mx2) {
+        const double f1 = s1 * h / 16.0, f2 = s2 * h * h * h / 64.0;
+        for (int k = 0; k < 8; ++k)
+          for (int j = 0; j < 8; ++j) A[k][j] = f1 * T2.L[c][t][k][j] + f2 * T2.Ms[c][t][k][j];
+      } else {
+        for (int k = 0; k < 8; ++k)
+          for (int j = 0; j < 8; ++j) A[k][j] = 0.0;
+        for (int q = 0; q < 8; ++q) {
+          const double f1 = p1[q] * h / 2.0, f2 = p2[q] * h * h * h / 8.0;
+          for (int k = 0; k < 8; ++k)
+            for (int j = 0; j < 8; ++j) A[k][j] += f1 * T1.L[c][t][q][k][j] + f2 * T1.Ms[c][t][q][k][j];
+        }
+      }
+    }
+    for (int k = 0; k < 8; ++k)
+      for (int j = 0; j < 8; ++j) y[idx[k]] += A[k][j] * x[idx[j]];
+  }
+  return 0;
+}
+
 // ------------------------------------------------------------------ solver --
 // DAMGSolve with the options of bin/options:50-53,182-207: CG outer,
 // multiplicative V-cycle, Richardson(omega)+Jacobi smoothing with zero initial
@@ -610,11 +729,23 @@ struct Level {
 
 struct Hierarchy {
   std::vector<Level> lv;  // lv[0] finest
+  int coarse_op = 0;      // 1: levels below the finest apply Jacobian3 (J); diag stays type 2 (B)
   std::vector<double> chol;  // dense Cholesky of the coarsest operator
   size_t nc = 0;
   int nu_pre = 2, nu_post = 2;
   double omega = 2.0 / 3.0;
 };
+
+// The operator J of level l: type 2 with the level's coefficients, or with
+// coarse_op 1 below the finest level Jacobian3 from the finer level's.
+void level_apply(const Hierarchy& H, size_t l, const double* x, double* y) {
+  const Level& L = H.lv[l];
+  if (H.coarse_op == 1 && l > 0 && !H.lv[l - 1].coef.empty()) {
+    jacobian3(H.lv[l - 1].mesh, H.lv[l - 1].coef.data(), L.mesh, x, y);
+    return;
+  }
+  matvec(L.mesh, L.coef.empty() ? nullptr : L.coef.data(), x, y);
+}
 
 int assemble_and_factor(Hierarchy& H) {
   Level& L = H.lv.back();
@@ -624,7 +755,7 @@ int assemble_and_factor(Hierarchy& H) {
   std::vector<double> e(n, 0.0), col(n);
   for (size_t j = 0; j < n; ++j) {
     e[j] = 1.0;
-    matvec(L.mesh, L.coef.empty() ? nullptr : L.coef.data(), e.data(), col.data());
+    level_apply(H, H.lv.size() - 1, e.data(), col.data());
     e[j] = 0.0;
     for (size_t i = 0; i < n; ++i) H.chol[i * n + j] = col[i];
   }
@@ -666,20 +797,19 @@ void vcycle(Hierarchy& H, size_t l, const double* b, double* x) {
     chol_solve(H, b, x);
     return;
   }
-  const double* cf = L.coef.empty() ? nullptr : L.coef.data();
   std::fill(x, x + n, 0.0);
   for (int s = 0; s < H.nu_pre; ++s) {
-    matvec(L.mesh, cf, x, L.t.data());
+    level_apply(H, l, x, L.t.data());
     for (size_t i = 0; i < n; ++i) x[i] += H.omega * (b[i] - L.t[i]) / L.diag[i];
   }
-  matvec(L.mesh, cf, x, L.t.data());
+  level_apply(H, l, x, L.t.data());
   for (size_t i = 0; i < n; ++i) L.r[i] = b[i] - L.t[i];
   Level& C = H.lv[l + 1];
   restrict_(L.P, n, C.mesh.N, L.r.data(), C.b.data());
   vcycle(H, l + 1, C.b.data(), C.x.data());
   prolong_add(L.P, n, C.x.data(), x);
   for (int s = 0; s < H.nu_post; ++s) {
-    matvec(L.mesh, cf, x, L.t.data());
+    level_apply(H, l, x, L.t.data());
     for (size_t i = 0; i < n; ++i) x[i] += H.omega * (b[i] - L.t[i]) / L.diag[i];
   }
 }
@@ -871,6 +1001,21 @@ void* orc_damg_create(const orc_octant* finest, int64_t n, uint32_t maxDepth, in
   return H;
 }
 void orc_damg_destroy(void* h) { delete (Hierarchy*)h; }
+// coarse_op 1: Jacobian3 below the finest level (the coarsest is re-factored)
+int orc_damg_set_coarse_op(void* h, int op) {
+  Hierarchy* H = (Hierarchy*)h;
+  H->coarse_op = op;
+  return assemble_and_factor(*H);
+}
+void orc_damg_level_apply(void* h, int l, const double* x, double* y) { level_apply(*(Hierarchy*)h, l, x, y); }
+void orc_type1_stencils(double* L, double* M) {
+  const Tables1& T = tables1();
+  std::memcpy(L, T.L, sizeof T.L);
+  std::memcpy(M, T.Ms, sizeof T.Ms);
+}
+int orc_jacobian3(void* fine, const double* fc, void* coarse, const double* x, double* y) {
+  return jacobian3(*(Mesh*)fine, fc, *(Mesh*)coarse, x, y);
+}
 void orc_damg_level_sizes(void* h, int64_t* E, int64_t* N) {
   Hierarchy* H = (Hierarchy*)h;
   for (size_t l = 0; l < H->lv.size(); ++l) {

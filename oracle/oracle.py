@@ -63,6 +63,10 @@ def lib():
         L.orc_damg_level_mesh.restype = P
         L.orc_damg_vcycle.argtypes = [P, P, P]
         L.orc_damg_pcg.argtypes = [P, P, P, C.c_double, C.c_int, P]
+        L.orc_damg_set_coarse_op.argtypes = [P, C.c_int]
+        L.orc_damg_level_apply.argtypes = [P, C.c_int, P, P]
+        L.orc_type1_stencils.argtypes = [P, P]
+        L.orc_jacobian3.argtypes = [P, P, P, P, P]
         _lib = L
     return _lib
 
@@ -168,6 +172,26 @@ def stencils():
     return L, M, G
 
 
+def type1_stencils():
+    """The oracle's type-1 tables (L1, M1), each [8][18][8][8][8]:
+    [coarse child number][element type][fine child][i][j]."""
+    L = np.empty((8, 18, 8, 8, 8))
+    M = np.empty((8, 18, 8, 8, 8))
+    lib().orc_type1_stencils(_ptr(L), _ptr(M))
+    return L, M
+
+
+def jacobian3(fine: Mesh, fine_coef, coarse: Mesh, x):
+    """Jacobian3MatMult (examples/src/backend/omgJac.C:2235): the coarse mesh's
+    operator from the fine mesh's coefficients (a, b per element)."""
+    fc = np.ascontiguousarray(fine_coef, np.float64)
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.empty_like(x)
+    if lib().orc_jacobian3(fine.h, _ptr(fc), coarse.h, _ptr(x), _ptr(y)):
+        raise ValueError("coarse element without fine elements")
+    return y
+
+
 def prolongation(fine: Mesh, coarse: Mesh):
     """CSR (ptr, col, val) of P: fine nodes x coarse nodes."""
     p, c, v, nnz = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_int64()
@@ -218,6 +242,18 @@ class DAMG:
 
     def level_mesh(self, l: int) -> Mesh:
         return Mesh(None, 0, handle=lib().orc_damg_level_mesh(self.h, l), owner=self)
+
+    def set_coarse_op(self, op: int):
+        """1: Jacobian3 below the finest level (J), Jacobi diagonal from the
+        level's own averaged coefficients (B); 0: type 2 throughout."""
+        if lib().orc_damg_set_coarse_op(self.h, op):
+            raise ValueError("coarsest operator not positive definite")
+
+    def level_apply(self, l: int, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty_like(x)
+        lib().orc_damg_level_apply(self.h, l, _ptr(x), _ptr(y))
+        return y
 
     def vcycle(self, b):
         b = np.ascontiguousarray(b, np.float64)

@@ -35,6 +35,7 @@ SOURCES = [
     "src/omg/RestrictMatVec.C", "src/omg/ProlongMatVec.C", "src/omg/VtxMaps.C", "src/omg/RmatType1StencilsAux.C",
     "src/omg/RmatType2StencilsAux.C", "src/omg/omg.C", "src/test/testUtils.C",
     "examples/src/backend/omgJac.C", "examples/src/backend/handleType2Stencils.C",
+    "examples/src/backend/handleType1Stencils.C",
     "examples/src/backend/elasticityJac.C", "examples/src/backend/odaJac.C", "examples/src/backend/vecMass.C",
 ]
 INCLUDE_DIRS = ["include", "include/oct", "include/oda", "include/omg", "include/par", "include/seq",

@@ -19,6 +19,12 @@
 //       DAMGCreateAndSetDA + DAMGSetUp; per level the node anchors, and the
 //       restriction / prolongation of the vectors level<l>_in.f64 /
 //       coarse<l>_in.f64 found in outdir
+//   dendro_ref jac3 <octs.u32> <maxDepth> <nlevels> <outdir>
+//       DAMGCreateAndSetDA + DAMGSetUp, then per coarse level l (1 = next to
+//       the finest) Jacobian3MatMult (examples/src/backend/omgJac.C:2235) with
+//       the Jacobian-3 context of that level: the next finer level's DA and
+//       its coefficients coef<l-1>.f64 (a, b per element), applied to
+//       jin<l>.f64 -> jout<l>.f64 (files in outdir)
 //   dendro_ref io <octs.u32> <maxDepth> <pts.f64> <vals.f64> <outdir>
 //       the reference's file writers (src/oct/OctFunctions.C:313-440):
 //       writeNodesToFile -> octs.ot, writePtsToFile -> pts.pts,
@@ -222,6 +228,45 @@ int main(int argc, char** argv) {
     write_octs(dir + "/bal.u32", bal);
     ot::coarsenOctree(bal, coarse);
     write_octs(dir + "/coarse.u32", coarse);
+    return 0;
+  }
+  if (mode == "jac3" && argc >= 6) {
+    unsigned D = atoi(argv[3]);
+    int nlevels = atoi(argv[4]);
+    std::string dir = argv[5];
+    std::vector<ot::TreeNode> octs = read_octs(argv[2], D);
+    ot::DAMG* damg = NULL;
+    ot::DAMG_Initialize(MPI_COMM_WORLD);
+    ot::DAMGCreateAndSetDA(MPI_COMM_WORLD, nlevels, NULL, &damg, octs, 1, 1.5, false, true);
+    ot::DAMGSetUp(damg);
+    createLmatType2(LaplacianType2Stencil);
+    createMmatType2(MassType2Stencil);
+    createLmatType1(LaplacianType1Stencil);
+    createMmatType1(MassType1Stencil);
+    for (int l = 1; l < nlevels; ++l) {
+      ot::DAMG fine = damg[nlevels - l], coarse = damg[nlevels - 1 - l];
+      std::vector<double> coef = read_raw<double>(dir + "/coef" + std::to_string(l - 1) + ".f64");
+      std::vector<double> matProp;
+      fine->da->createVector(matProp, true, true, 2);
+      for (size_t i = 0; i < matProp.size() && i < coef.size(); ++i) matProp[i] = coef[i];
+      Jac3MFreeData data;
+      std::memset((void*)&data, 0, sizeof(data));
+      data.daf = fine->da;
+      data.matPropFine = &matProp;
+      data.isFinestLevel = false;
+      data.isCoarsestLevel = (l == nlevels - 1);
+      data.changedPartition = false;
+      void* saved = coarse->user;
+      coarse->user = &data;
+      std::vector<double> x = read_raw<double>(dir + "/jin" + std::to_string(l) + ".f64");
+      Mat J;
+      MatCreateShell(MPI_COMM_WORLD, int(x.size()), int(x.size()), PETSC_DETERMINE, PETSC_DETERMINE, coarse, &J);
+      Vec in = make_vec(x), out = make_vec(x);
+      Jacobian3MatMult(J, in, out);
+      std::vector<double> y = vec_data(out);
+      write_raw(dir + "/jout" + std::to_string(l) + ".f64", y.data(), y.size());
+      coarse->user = saved;
+    }
     return 0;
   }
   if (mode == "io" && argc >= 7) {

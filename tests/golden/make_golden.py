@@ -9,6 +9,7 @@ tests read only them.
 
     python tests/golden/make_golden.py            # everything
     python tests/golden/make_golden.py --io-only  # the file-format fixtures io_*.npz
+    python tests/golden/make_golden.py --jac3-only  # Jacobian3 fixture + stencil digests
 
 The file-format fixtures also run oracle/_ref/dendro_ref_dumpmesh, the
 reference's examples/src/drivers/dumpMesh.C built single-rank.
@@ -143,6 +144,35 @@ def transfer_fixture(tmp):
     np.savez_compressed(os.path.join(OUT, f"transfer_{name}.npz"), **rec)
 
 
+def jac3_fixture(tmp):
+    """Jacobian3MatMult (examples/src/backend/omgJac.C:2235) on the coarse
+    levels of the transfer case's hierarchy, from the next finer level's
+    coefficients: the sphere coefficients (a = 1e4 inside r < 0.25) on the
+    finest level, their per-level means below."""
+    name, nlevels = TRANSFER_CASE
+    z = np.load(os.path.join(OUT, f"transfer_{name}.npz"))
+    depth, bal = int(z["depth"]), z["bal"]
+    nl = int(z["nlevels"])
+    bal.tofile(os.path.join(tmp, "bal_j.u32"))
+    dm = O.DAMG(bal.view(np.uint32).reshape(-1, 4).astype(np.uint32).view(O.OCT_DTYPE).reshape(-1), depth, nlevels)
+    assert dm.nlevels == nl
+    rec = {"depth": depth, "nlevels": nl, "bal": bal}
+    e0 = z["elem0"]
+    s0 = 2.0 ** -(e0[:, 3].astype(np.float64) - 1)
+    coef = I.sphere_coefficients(e0[:, :3] / 2.0 ** depth + 0.5 * s0[:, None]).reshape(-1)
+    for l in range(nl - 1):
+        rec[f"coef{l}"] = coef
+        coef.tofile(os.path.join(tmp, f"coef{l}.f64"))
+        x = np.random.default_rng(50 + l).uniform(-1, 1, int(dm.N[l + 1]))
+        rec[f"jin{l + 1}"] = x
+        x.tofile(os.path.join(tmp, f"jin{l + 1}.f64"))
+        coef = O.coarse_coef(dm.level_mesh(l), coef, dm.level_mesh(l + 1)).reshape(-1)
+    run("jac3", os.path.join(tmp, "bal_j.u32"), depth, nl, tmp)
+    for l in range(1, nl):
+        rec[f"jout{l}"] = np.fromfile(os.path.join(tmp, f"jout{l}.f64"))
+    np.savez_compressed(os.path.join(OUT, f"jac3_{name}.npz"), **rec)
+
+
 IO_CASES = ["corner_points_d5", "uniform600_d7", "gauss1k_d8"]
 DUMP_BIN = os.path.join(ROOT, "oracle", "_ref", "dendro_ref_dumpmesh")
 
@@ -189,6 +219,10 @@ def stencil_digests():
                           ("gd", "GDType2Stencils.inp", 24), ("rmat2", "RmatType2Stencils.inp", 8)):
         a = np.array(open(os.path.join(STENCILS, fname)).read().split(), float).reshape(8, 18, m, m)
         rec[tag] = table_digest(a)
+    # type-1 tables [coarse child][type][fine child][8][8], digested per (type, fine child)
+    for tag, fname in (("lap1", "LapType1Stencils.inp"), ("mass1", "MassType1Stencils.inp")):
+        a = np.array(open(os.path.join(STENCILS, fname)).read().split(), float).reshape(8, 18 * 8, 8, 8)
+        rec[tag] = table_digest(a)
     np.savez_compressed(os.path.join(OUT, "stencil_digests.npz"), **rec)
 
 
@@ -196,6 +230,11 @@ def main():
     if not os.path.exists(REF_BIN):
         sys.exit("build the reference first: python oracle/ref_build/build_ref.py")
     if "--stencils-only" in sys.argv:
+        stencil_digests()
+        return
+    if "--jac3-only" in sys.argv:
+        with tempfile.TemporaryDirectory() as tmp:
+            jac3_fixture(tmp)
         stencil_digests()
         return
     if "--io-only" in sys.argv:
@@ -208,6 +247,7 @@ def main():
         for name in MESH_CASES:
             mesh_fixture(tmp, name)
         transfer_fixture(tmp)
+        jac3_fixture(tmp)
         for name in IO_CASES:
             io_fixture(tmp, name)
     stencil_digests()

@@ -33,7 +33,8 @@ class SolveReport(C.Structure):
 
 class DamgConfig(C.Structure):
     _fields_ = [("nlevels", C.c_int), ("nu_pre", C.c_int), ("nu_post", C.c_int), ("omega", C.c_double),
-                ("rtol", C.c_double), ("maxit", C.c_int), ("inner_prec", C.c_int), ("use_graph", C.c_int)]
+                ("rtol", C.c_double), ("maxit", C.c_int), ("inner_prec", C.c_int), ("use_graph", C.c_int),
+                ("coarse_op", C.c_int)]
 
 
 _lib = None
@@ -117,6 +118,7 @@ def lib():
         "dg_octree_write": ([P, C.c_char_p], I),
         "dg_octree_read": ([C.c_char_p, PP], I),
         "dg_da_dump_mesh": ([P, C.c_char_p], I),
+        "dg_damg_level_apply": ([P, I, P, P, I], I),
         "dg_set_device_wait_limit": ([I64], I),
     }
     for name, (args, res) in sig.items():
@@ -143,7 +145,7 @@ def exported_symbols():
         "dg_mlp_gradient", "dg_mlp_train_step", "dg_mlp_destroy", "dg_damg_set_smoother", "dg_damg_features",
         "dg_vec_dot_noalloc", "dg_mat_kernel_count", "dg_mat_set_kernel", "dg_device_check",
         "dg_set_device_wait_limit", "dg_write_pts", "dg_read_pts", "dg_write_data_pts", "dg_read_data_pts",
-        "dg_octree_write", "dg_octree_read", "dg_da_dump_mesh",
+        "dg_octree_write", "dg_octree_read", "dg_da_dump_mesh", "dg_damg_level_apply",
         "dg_mat_mult_multi", "dg_damg_set_tolerances",
     ]
 

@@ -278,13 +278,16 @@ class DAMG:
 
     def __init__(self, finest, nlevels: int = 30, nu_pre: int = 2, nu_post: int = 2,
                  omega: float = 2.0 / 3.0, rtol: float = 1e-8, maxit: int = 200, inner_prec: int = 0,
-                 use_graph: bool = False):
+                 use_graph: bool = False, coarse_op: int = 0):
         """`finest` is one balanced Octree, or a list of them for the batched
-        form (independent meshes solved together, one launch per kernel)."""
+        form (independent meshes solved together, one launch per kernel).
+        coarse_op 1: operators below the finest level from the next finer
+        level's coefficients (Jacobian3) instead of the level's averaged ones."""
         cfg = DamgConfig()
         lib().dg_damg_default_config(C.byref(cfg))
         cfg.nlevels, cfg.nu_pre, cfg.nu_post, cfg.omega = nlevels, nu_pre, nu_post, omega
         cfg.rtol, cfg.maxit, cfg.inner_prec, cfg.use_graph = rtol, maxit, inner_prec, int(use_graph)
+        cfg.coarse_op = int(coarse_op)
         h = C.c_void_p()
         if isinstance(finest, (list, tuple)):
             arr = (C.c_void_p * len(finest))(*[t.h.value for t in finest])
@@ -351,6 +354,18 @@ class DAMG:
         xf = np.ascontiguousarray(xf, np.float64).copy()
         check(lib().dg_damg_prolong(self.h, level, ptr(xc), ptr(xf), 0), "damg_prolong")
         return xf
+
+    def levelApply(self, level: int, x):
+        """y = J x on one level (0 = finest), host numpy or device tensor."""
+        if _is_device(x):
+            import torch
+            y = torch.empty_like(x)
+            check(lib().dg_damg_level_apply(self.h, level, ptr(x), ptr(y), 1), "damg_level_apply")
+            return y
+        xa = np.ascontiguousarray(x, np.float64)
+        y = np.empty_like(xa)
+        check(lib().dg_damg_level_apply(self.h, level, ptr(xa), ptr(y), 0), "damg_level_apply")
+        return y
 
     def restrict(self, level: int, rf: np.ndarray) -> np.ndarray:
         rf = np.ascontiguousarray(rf, np.float64)

@@ -131,20 +131,39 @@ dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s);
 uint32_t etype_mask(int c, int t);
 
 // ---- operators (matvec.cu) ----
+// Coarse elements of a level whose operator, with the coarse operator taken
+// from the next finer level's coefficients (Jacobian3, examples/src/backend/
+// omgJac.C:2139-2233), is the sum over their 8 children with the children's
+// own coefficients (type-1 tables) because those differ.
+struct Type1Set {
+  int64_t n = 0;
+  DBuf<uint32_t> elem;  // [n] element ids
+  DBuf<double> coef;    // [n][16]: a of children 0..7 (child-number order), then b
+  DBuf<float> coef32;
+};
+// The J operator of a level: coef (a then b, [2][E]) with the elements of t1
+// zeroed, plus t1's children sums; coef == nullptr / t1 == nullptr: the
+// operator's own coefficients / no type-1 elements.
 dg_status lapmass_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
+dg_status lapmass_apply_j_f64(const dg_mat* A, const double* coef, const Type1Set* t1, const double* x, double* y,
+                              cudaStream_t s);
 dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStream_t s);
 dg_status lapmass_diag(const dg_mat* A, double* d, cudaStream_t s);
 // One damped-Jacobi sweep x <- x + omega dinv (b - A x) in place, and the
 // residual r = b - A x: the warp-tile operator into acc (an N-vector that must
 // be zero on entry and is zero again on return), then one elementwise pass.
 dg_status lapmass_smooth_f64(const dg_mat* A, double* x, const double* b, const double* dinv, double omega,
-                             double* acc, cudaStream_t s);
+                             double* acc, cudaStream_t s, const double* coef = nullptr,
+                             const Type1Set* t1 = nullptr);
 dg_status lapmass_smooth_f32(const dg_mat* A, float* x, const float* b, const float* dinv, float omega, float* acc,
-                             cudaStream_t s);
+                             cudaStream_t s, const float* coef = nullptr,
+                             const Type1Set* t1 = nullptr);
 dg_status lapmass_residual_f64(const dg_mat* A, const double* x, const double* b, double* r, double* acc,
-                               cudaStream_t s);
+                               cudaStream_t s, const double* coef = nullptr,
+                               const Type1Set* t1 = nullptr);
 dg_status lapmass_residual_f32(const dg_mat* A, const float* x, const float* b, float* r, float* acc,
-                               cudaStream_t s);
+                               cudaStream_t s, const float* coef = nullptr,
+                               const Type1Set* t1 = nullptr);
 const char* matvec_variant_name(int v);
 int matvec_variant_count();
 // Y = A X for nrhs vectors (node-major [N][nrhs], FP32) on the tensor cores;
@@ -156,6 +175,7 @@ dg_status elasticity_diag(const dg_mat* A, double* d, cudaStream_t s);
 // independent mesh: node r belongs to block row_blk[r] with node offset
 // boff[b], size bn[b] and storage offset baoff[b].
 dg_status lapmass_assemble_dense(const dg_mat* A, double* dense, int64_t dense_size, const uint32_t* row_blk,
-                                 const int64_t* boff, const int64_t* bn, const int64_t* baoff, cudaStream_t s);
+                                 const int64_t* boff, const int64_t* bn, const int64_t* baoff, cudaStream_t s,
+                                 const double* coef = nullptr, const Type1Set* t1 = nullptr);
 
 }  // namespace dg

@@ -825,6 +825,162 @@ __global__ void lapmass_dense_kernel(const uint32_t* __restrict__ nl, const uint
   }
 }
 
+// Type-1 element operator (JAC_TYPE3_MULT_BLOCK's children sum,
+// examples/src/backend/omgJac.C:2206-2230): u (natural vertex order) <- the
+// sum over the element's 8 children of their operators with their own
+// coefficients (cf: a of children 0..7, then b), in the coarse element's
+// vertex basis, with the hanging interpolation T on both sides.  Worked in the
+// child-number frame: T applied, the frame corner values interpolated
+// trilinearly to the 3x3x3 points of the children, each child's Walsh-form
+// operator at half the size (f1 = a h/4, f2 = b h^3/64), the children's results
+// summed at the points and restricted back to the corners (the transpose of
+// the interpolation), then T^T.  Equal to the type-1 tables
+// T^T P_f^T (a_f K h/4 + b_f M h^3/64) P_f T (LapType1Stencils.inp /
+// MassType1Stencils.inp).
+template <int P, int W>
+__host__ __device__ constexpr double t1_weight() {  // trilinear weight of corner W at sub-grid point P
+  return ((W & 1) ? 0.5 * (P % 3) : 1.0 - 0.5 * (P % 3)) * ((W & 2) ? 0.5 * ((P / 3) % 3) : 1.0 - 0.5 * ((P / 3) % 3)) *
+         ((W & 4) ? 0.5 * (P / 9) : 1.0 - 0.5 * (P / 9));
+}
+template <int F, int V>
+__host__ __device__ constexpr int t1_point() {  // sub-grid point of vertex V of frame child F
+  return ((F & 1) + (V & 1)) + 3 * (((F >> 1) & 1) + ((V >> 1) & 1)) + 9 * (((F >> 2) & 1) + ((V >> 2) & 1));
+}
+template <class T, int P>
+__device__ __forceinline__ T t1_interp(const T (&w)[8]) {
+  T s = T(0);
+  if (t1_weight<P, 0>() != 0.0) s += T(t1_weight<P, 0>()) * w[0];
+  if (t1_weight<P, 1>() != 0.0) s += T(t1_weight<P, 1>()) * w[1];
+  if (t1_weight<P, 2>() != 0.0) s += T(t1_weight<P, 2>()) * w[2];
+  if (t1_weight<P, 3>() != 0.0) s += T(t1_weight<P, 3>()) * w[3];
+  if (t1_weight<P, 4>() != 0.0) s += T(t1_weight<P, 4>()) * w[4];
+  if (t1_weight<P, 5>() != 0.0) s += T(t1_weight<P, 5>()) * w[5];
+  if (t1_weight<P, 6>() != 0.0) s += T(t1_weight<P, 6>()) * w[6];
+  if (t1_weight<P, 7>() != 0.0) s += T(t1_weight<P, 7>()) * w[7];
+  return s;
+}
+template <class T, int P>
+__device__ __forceinline__ void t1_restrict(const T (&R)[27], T (&r)[8]) {
+  if constexpr (P < 27) {
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+      const double wt = (w == 0)   ? t1_weight<P, 0>()
+                        : (w == 1) ? t1_weight<P, 1>()
+                        : (w == 2) ? t1_weight<P, 2>()
+                        : (w == 3) ? t1_weight<P, 3>()
+                        : (w == 4) ? t1_weight<P, 4>()
+                        : (w == 5) ? t1_weight<P, 5>()
+                        : (w == 6) ? t1_weight<P, 6>()
+                                   : t1_weight<P, 7>();
+      if (wt != 0.0) r[w] += T(wt) * R[P];
+    }
+    t1_restrict<T, P + 1>(R, r);
+  }
+}
+template <class T, int P>
+__device__ __forceinline__ void t1_interp_all(const T (&w)[8], T (&S)[27]) {
+  if constexpr (P < 27) {
+    S[P] = t1_interp<T, P>(w);
+    t1_interp_all<T, P + 1>(w, S);
+  }
+}
+template <class T, int F>
+__device__ __forceinline__ void t1_children(const T (&S)[27], T (&R)[27], uint32_t c, T h, const T* __restrict__ a,
+                                            const T* __restrict__ b) {
+  if constexpr (F < 8) {
+    const uint32_t k = uint32_t(F) ^ c;  // the child's number
+    const T f1 = a[k] * h * T(0.25), f2 = b[k] * h * h * h * T(1.0 / 64.0);
+    T v[8];
+    v[0] = S[t1_point<F, 0>()];
+    v[1] = S[t1_point<F, 1>()];
+    v[2] = S[t1_point<F, 2>()];
+    v[3] = S[t1_point<F, 3>()];
+    v[4] = S[t1_point<F, 4>()];
+    v[5] = S[t1_point<F, 5>()];
+    v[6] = S[t1_point<F, 6>()];
+    v[7] = S[t1_point<F, 7>()];
+    lapmass_ref(v, f1, f2);
+    R[t1_point<F, 0>()] += v[0];
+    R[t1_point<F, 1>()] += v[1];
+    R[t1_point<F, 2>()] += v[2];
+    R[t1_point<F, 3>()] += v[3];
+    R[t1_point<F, 4>()] += v[4];
+    R[t1_point<F, 5>()] += v[5];
+    R[t1_point<F, 6>()] += v[6];
+    R[t1_point<F, 7>()] += v[7];
+    t1_children<T, F + 1>(S, R, c, h, a, b);
+  }
+}
+template <class T>
+__device__ __forceinline__ void type1_elem(T (&u)[8], uint32_t m, const T (&a)[8], const T (&b)[8]) {
+  const uint32_t c = meta_cnum(m);
+  const T h = elem_h<T>(meta_lev(m));
+  T w[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) w[j] = u[j ^ c];  // frame
+  const uint32_t mp = xor_perm_mask(meta_mask(m), c);
+  if (mp) interp_frame(w, mp);
+  T S[27], R[27];
+  t1_interp_all<T, 0>(w, S);
+#pragma unroll
+  for (int p = 0; p < 27; ++p) R[p] = T(0);
+  t1_children<T, 0>(S, R, c, h, a, b);
+  T r[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) r[j] = T(0);
+  t1_restrict<T, 0>(R, r);
+  if (mp) scatter_frame(r, mp);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) u[j ^ c] = r[j];
+}
+
+// y += the type-1 operators of the listed elements applied to x (atomics).
+template <class T, class CT>
+__global__ void type1_add_kernel(const uint32_t* __restrict__ nl, const uint32_t* __restrict__ meta, int64_t E,
+                                 const uint32_t* __restrict__ elems, const CT* __restrict__ cf, int64_t n,
+                                 const T* __restrict__ x, T* __restrict__ y) {
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    const uint32_t e = elems[i];
+    T u[8], a[8], b[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      u[v] = x[nl[int64_t(v) * E + e]];
+      a[v] = T(cf[16 * i + v]);
+      b[v] = T(cf[16 * i + 8 + v]);
+    }
+    type1_elem(u, meta[e], a, b);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) atomicAdd(y + nl[int64_t(v) * E + e], u[v]);
+  }
+}
+
+// The listed elements' type-1 operators added into the dense blocks (one
+// thread per element and column), like lapmass_dense_kernel.
+__global__ void type1_dense_kernel(const uint32_t* __restrict__ nl, const uint32_t* __restrict__ meta, int64_t E,
+                                   const uint32_t* __restrict__ elems, const double* __restrict__ cf, int64_t n,
+                                   const uint32_t* __restrict__ row_blk, const int64_t* __restrict__ boff,
+                                   const int64_t* __restrict__ bn, const int64_t* __restrict__ baoff,
+                                   double* __restrict__ A) {
+  for (int64_t t = gtid(); t < n * 8; t += gstride()) {
+    const int64_t i = t >> 3;
+    const int j = int(t & 7);
+    const uint32_t e = elems[i];
+    double u[8], a[8], b[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      u[v] = v == j ? 1.0 : 0.0;
+      a[v] = cf[16 * i + v];
+      b[v] = cf[16 * i + 8 + v];
+    }
+    type1_elem(u, meta[e], a, b);
+    const uint32_t col = nl[int64_t(j) * E + e];
+    const uint32_t blk = row_blk[col];
+    const int64_t o = boff[blk], nb = bn[blk];
+    double* Ab = A + baoff[blk];
+    for (int k = 0; k < 8; ++k) atomicAdd(Ab + (int64_t(nl[int64_t(k) * E + e]) - o) * nb + (int64_t(col) - o), u[k]);
+  }
+}
+
 }  // namespace
 
 // Launch shapes tried by the autotuner: one thread per element with
@@ -1043,9 +1199,22 @@ static dg_status apply_to_zeroed(const dg_mat* A, const CT* coef, const T* x, T*
 }
 
 template <class T, class CT>
+static dg_status type1_add(const dg_mat* A, const Type1Set* t1, const T* x, T* y, cudaStream_t s) {
+  if (!t1 || !t1->n) return DG_OK;
+  const CT* cf;
+  if constexpr (sizeof(CT) == 8) cf = t1->coef.p;
+  else cf = t1->coef32.p;
+  type1_add_kernel<T, CT><<<grid_for(t1->n, 128, 8), 128, 0, s>>>(A->da->nl.p, A->da->meta.p, A->da->E, t1->elem.p, cf,
+                                                                   t1->n, x, y);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+template <class T, class CT>
 static dg_status smooth_sweep(const dg_mat* A, const CT* coef, T* x, const T* b, const T* dinv, T omega, T* t,
-                              cudaStream_t s) {
+                              cudaStream_t s, const Type1Set* t1 = nullptr) {
   DG_TRY((apply_to_zeroed<T, CT>(A, coef, x, t, s)));
+  DG_TRY((type1_add<T, CT>(A, t1, x, t, s)));
   const int64_t n = A->da->N;
   constexpr int W = 16 / sizeof(T);
   const int64_t nv = (aligned16(x) && aligned16(b) && aligned16(dinv) && aligned16(t)) ? n / W : 0;
@@ -1058,8 +1227,10 @@ static dg_status smooth_sweep(const dg_mat* A, const CT* coef, T* x, const T* b,
 }
 
 template <class T, class CT>
-static dg_status residual(const dg_mat* A, const CT* coef, const T* x, const T* b, T* r, T* t, cudaStream_t s) {
+static dg_status residual(const dg_mat* A, const CT* coef, const T* x, const T* b, T* r, T* t, cudaStream_t s,
+                          const Type1Set* t1 = nullptr) {
   DG_TRY((apply_to_zeroed<T, CT>(A, coef, x, t, s)));
+  DG_TRY((type1_add<T, CT>(A, t1, x, t, s)));
   const int64_t n = A->da->N;
   constexpr int W = 16 / sizeof(T);
   const int64_t nv = (aligned16(b) && aligned16(t) && aligned16(r)) ? n / W : 0;
@@ -1071,20 +1242,27 @@ static dg_status residual(const dg_mat* A, const CT* coef, const T* x, const T* 
 }
 
 dg_status lapmass_smooth_f64(const dg_mat* A, double* x, const double* b, const double* dinv, double omega,
-                             double* acc, cudaStream_t s) {
-  return smooth_sweep<double, double>(A, A->coef.p, x, b, dinv, omega, acc, s);
+                             double* acc, cudaStream_t s, const double* coef, const Type1Set* t1) {
+  return smooth_sweep<double, double>(A, coef ? coef : A->coef.p, x, b, dinv, omega, acc, s, t1);
 }
 dg_status lapmass_smooth_f32(const dg_mat* A, float* x, const float* b, const float* dinv, float omega, float* acc,
-                             cudaStream_t s) {
-  return smooth_sweep<float, float>(A, A->coef32.p, x, b, dinv, omega, acc, s);
+                             cudaStream_t s, const float* coef, const Type1Set* t1) {
+  return smooth_sweep<float, float>(A, coef ? coef : A->coef32.p, x, b, dinv, omega, acc, s, t1);
 }
 dg_status lapmass_residual_f64(const dg_mat* A, const double* x, const double* b, double* r, double* acc,
-                               cudaStream_t s) {
-  return residual<double, double>(A, A->coef.p, x, b, r, acc, s);
+                               cudaStream_t s, const double* coef, const Type1Set* t1) {
+  return residual<double, double>(A, coef ? coef : A->coef.p, x, b, r, acc, s, t1);
 }
 dg_status lapmass_residual_f32(const dg_mat* A, const float* x, const float* b, float* r, float* acc,
-                               cudaStream_t s) {
-  return residual<float, float>(A, A->coef32.p, x, b, r, acc, s);
+                               cudaStream_t s, const float* coef, const Type1Set* t1) {
+  return residual<float, float>(A, coef ? coef : A->coef32.p, x, b, r, acc, s, t1);
+}
+
+dg_status lapmass_apply_j_f64(const dg_mat* A, const double* coef, const Type1Set* t1, const double* x, double* y,
+                              cudaStream_t s) {
+  DG_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * A->da->N, s));
+  DG_TRY((apply_to_zeroed<double, double>(A, coef ? coef : A->coef.p, x, y, s)));
+  return type1_add<double, double>(A, t1, x, y, s);
 }
 
 dg_status lapmass_diag(const dg_mat* A, double* d, cudaStream_t s) {
@@ -1098,13 +1276,18 @@ dg_status lapmass_diag(const dg_mat* A, double* d, cudaStream_t s) {
 }
 
 dg_status lapmass_assemble_dense(const dg_mat* A, double* dense, int64_t dense_size, const uint32_t* row_blk,
-                                 const int64_t* boff, const int64_t* bn, const int64_t* baoff, cudaStream_t s) {
+                                 const int64_t* boff, const int64_t* bn, const int64_t* baoff, cudaStream_t s,
+                                 const double* coef, const Type1Set* t1) {
   const dg_da* da = A->da;
   DG_CUDA(cudaMemsetAsync(dense, 0, sizeof(double) * dense_size, s));
-  const double* ca = A->has_coef ? A->coef.p : nullptr;
-  const double* cb = A->has_coef ? A->coef.p + da->E : nullptr;
+  const double* c0 = coef ? coef : A->coef.p;
+  const double* ca = A->has_coef ? c0 : nullptr;
+  const double* cb = A->has_coef ? c0 + da->E : nullptr;
   lapmass_dense_kernel<double><<<grid_for(da->E * 8, 256, 8), 256, 0, s>>>(da->nl.p, da->meta.p, ca, cb, da->E,
                                                                           row_blk, boff, bn, baoff, dense);
+  if (t1 && t1->n)
+    type1_dense_kernel<<<grid_for(t1->n * 8, 128, 8), 128, 0, s>>>(da->nl.p, da->meta.p, da->E, t1->elem.p,
+                                                                   t1->coef.p, t1->n, row_blk, boff, bn, baoff, dense);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }

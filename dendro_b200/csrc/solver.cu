@@ -85,6 +85,44 @@ __global__ void coarse_coef_kernel(const uint64_t* __restrict__ fk, int64_t Ef, 
   }
 }
 
+// Coarse elements split into 8 fine children whose coefficients differ by more
+// than tol relative to their maximum (a or b): JAC_TYPE3_MULT_BLOCK's test
+// (examples/src/backend/omgJac.C:2167-2207, -tolToCoarsenMatProp default 1e-12).
+// flag[e] = 1 for those, with the children's a, b in child[16 e ..].
+__global__ void type1_detect_kernel(const uint64_t* __restrict__ fk, int64_t Ef, const double* __restrict__ fa,
+                                    const double* __restrict__ fb, const uint64_t* __restrict__ ck, int64_t Ec,
+                                    double tol, uint8_t* __restrict__ flag, double* __restrict__ child) {
+  for (int64_t e = gtid(); e < Ec; e += gstride()) {
+    const uint64_t m = okey_m(ck[e]);
+    const int64_t f = lower_bound(fk, Ef, okey(m, 0));
+    flag[e] = 0;
+    if (f + 8 > Ef || okey_m(fk[f]) != m || okey_l(fk[f]) == okey_l(ck[e])) continue;
+    double mx1 = fa[f], mn1 = fa[f], mx2 = fb[f], mn2 = fb[f];
+    for (int k = 1; k < 8; ++k) {
+      mx1 = fmax(mx1, fa[f + k]);
+      mn1 = fmin(mn1, fa[f + k]);
+      mx2 = fmax(mx2, fb[f + k]);
+      mn2 = fmin(mn2, fb[f + k]);
+    }
+    if (mx1 - mn1 <= tol * mx1 && mx2 - mn2 <= tol * mx2) continue;
+    flag[e] = 1;
+    for (int k = 0; k < 8; ++k) {
+      child[16 * e + k] = fa[f + k];
+      child[16 * e + 8 + k] = fb[f + k];
+    }
+  }
+}
+__global__ void gather16(const double* __restrict__ src, const uint32_t* __restrict__ idx, int64_t n,
+                         double* __restrict__ dst) {
+  for (int64_t i = gtid(); i < 16 * n; i += gstride()) dst[i] = src[16 * int64_t(idx[i / 16]) + i % 16];
+}
+__global__ void zero_elems(double* __restrict__ coef, int64_t E, const uint32_t* __restrict__ idx, int64_t n) {
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    coef[idx[i]] = 0.0;
+    coef[E + idx[i]] = 0.0;
+  }
+}
+
 // concatenation helpers for batches of meshes
 __global__ void copy_add_u32(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, int64_t n, uint32_t add) {
   for (int64_t i = gtid(); i < n; i += gstride()) dst[i] = src[i] + add;
@@ -444,6 +482,16 @@ struct Level {
   // 1 / element references, hanging share, mean log2 diagonal
   DBuf<float> sm_r, sm_nsum, sm_nmax, sm_refs, sm_hang;
   float sm_dlogbar = 0.f;
+  // coarse_op 1 (levels below the finest): the operator J from the finer
+  // level's coefficients = the averaged coefficients with the type-1 elements
+  // zeroed (coefJ) plus their children sums (t1); the Jacobi diagonal stays
+  // that of the averaged coefficients (the reference's B matrix)
+  Type1Set t1;
+  DBuf<double> coefJ;
+  DBuf<float> coefJ32;
+  const double* jcoef() const { return t1.n ? coefJ.p : nullptr; }
+  const float* jcoef32() const { return t1.n ? coefJ32.p : nullptr; }
+  const Type1Set* jset() const { return t1.n ? &t1 : nullptr; }
 };
 
 struct dg_damg {
@@ -616,7 +664,7 @@ dg_status setup_coarse(dg_damg* m) {
   for (int b = 0; b < nb; ++b)
     fill_row_blk<<<grid_for(m->cb_n[b], 256), 256, 0, m->s>>>(m->d_crow_blk.p, noff[b], noff[b + 1], uint32_t(b));
   DG_TRY(lapmass_assemble_dense(L.A.get(), m->Ainv.p, total, m->d_crow_blk.p, m->d_cb_off.p, m->d_cb_n.p,
-                                m->d_cb_aoff.p, m->s));
+                                m->d_cb_aoff.p, m->s, L.jcoef(), L.jset()));
   DBuf<double> colk;
   DG_TRY(colk.alloc(N));
   const dim3 g1(grid_for(maxn, 256), unsigned(nb)), g2(grid_for(maxn * maxn, 256), unsigned(nb));
@@ -627,6 +675,56 @@ dg_status setup_coarse(dg_damg* m) {
   }
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaStreamSynchronize(m->s));
+  return DG_OK;
+}
+
+// Type-1 set and J coefficients of level l (>= 1) from level l - 1.
+dg_status setup_type1(dg_damg* m, size_t l) {
+  cudaStream_t s = m->s;
+  Level& L = m->lv[l];
+  Level& F = m->lv[l - 1];
+  const int64_t Ec = L.da->E;
+  DBuf<uint8_t> flag;
+  DBuf<double> child;
+  DG_TRY(flag.alloc(Ec));
+  DG_TRY(child.alloc(16 * Ec));
+  const std::vector<int64_t>& fo = m->mesh_elem_off[l - 1];
+  const std::vector<int64_t>& co = m->mesh_elem_off[l];
+  for (int i = 0; i < m->nmesh; ++i) {
+    const int64_t ef = fo[i + 1] - fo[i], ec = co[i + 1] - co[i];
+    type1_detect_kernel<<<grid_for(ec, 256), 256, 0, s>>>(
+        F.da->ekey.p + fo[i], ef, F.A->coef.p + fo[i], F.A->coef.p + F.da->E + fo[i], L.da->ekey.p + co[i], ec,
+        1e-12, flag.p + co[i], child.p + 16 * co[i]);
+  }
+  DG_CUDA(cudaGetLastError());
+  std::vector<uint8_t> hf(static_cast<size_t>(Ec));
+  DG_CUDA(cudaMemcpyAsync(hf.data(), flag.p, Ec, cudaMemcpyDeviceToHost, s));
+  DG_CUDA(cudaStreamSynchronize(s));
+  std::vector<uint32_t> ids;
+  for (int64_t e = 0; e < Ec; ++e)
+    if (hf[size_t(e)]) ids.push_back(uint32_t(e));
+  L.t1.n = int64_t(ids.size());
+  if (!L.t1.n) return DG_OK;
+  const int64_t n = L.t1.n;
+  DG_TRY(L.t1.elem.alloc(n));
+  DG_CUDA(cudaMemcpyAsync(L.t1.elem.p, ids.data(), 4 * n, cudaMemcpyHostToDevice, s));
+  DG_TRY(L.t1.coef.alloc(16 * n));
+  gather16<<<grid_for(16 * n, 256), 256, 0, s>>>(child.p, L.t1.elem.p, n, L.t1.coef.p);
+  DG_TRY(L.coefJ.alloc(2 * Ec + kCoefPad));
+  DG_CUDA(cudaMemcpyAsync(L.coefJ.p, L.A->coef.p, 16 * Ec, cudaMemcpyDeviceToDevice, s));
+  zero_elems<<<grid_for(n, 256), 256, 0, s>>>(L.coefJ.p, Ec, L.t1.elem.p, n);
+  DG_CUDA(cudaGetLastError());
+  if (m->cfg.inner_prec != DG_PREC_F64) {
+    DG_TRY(L.coefJ32.alloc(2 * Ec + kCoefPad));
+    DG_TRY(convert_f64_to_f32(L.coefJ.p, L.coefJ32.p, 2 * Ec, s));
+    DG_TRY(L.t1.coef32.alloc(16 * n));
+    DG_TRY(convert_f64_to_f32(L.t1.coef.p, L.t1.coef32.p, 16 * n, s));
+    if (m->cfg.inner_prec == DG_PREC_F32_BF16COEF) {
+      DG_TRY(round_coef_bf16(L.coefJ32.p, 2 * Ec, s));
+      DG_TRY(round_coef_bf16(L.t1.coef32.p, 16 * n, s));
+    }
+  }
+  DG_CUDA(cudaStreamSynchronize(s));  // child is freed on return
   return DG_OK;
 }
 
@@ -674,6 +772,8 @@ dg_status set_operators(dg_damg* m, const double* coef) {
     L.A = std::move(A);
     DG_TRY(setup_level_vectors(L, s));
     if (m->cfg.inner_prec != DG_PREC_F64) DG_TRY(setup_level_f32(m, L, s));
+    L.t1.n = 0;
+    if (coef && l > 0 && m->cfg.coarse_op == 1) DG_TRY(setup_type1(m, l));
   }
   m->drop_graphs();  // operators changed: capture again on the next solve
   return setup_coarse(m);
@@ -696,8 +796,9 @@ dg_status vcycle(dg_damg* m, size_t l, const double* b, double* x) {
   // the residual are fused warp-tile operator applications
   if (m->cfg.nu_pre > 0) {
     jacobi_first<<<g, 256, 0, s>>>(x, b, L.dinv.p, w, n);
-    for (int k = 1; k < m->cfg.nu_pre; ++k) DG_TRY(lapmass_smooth_f64(L.A.get(), x, b, L.dinv.p, w, L.acc.p, s));
-    DG_TRY(lapmass_residual_f64(L.A.get(), x, b, L.t.p, L.acc.p, s));
+    for (int k = 1; k < m->cfg.nu_pre; ++k)
+      DG_TRY(lapmass_smooth_f64(L.A.get(), x, b, L.dinv.p, w, L.acc.p, s, L.jcoef(), L.jset()));
+    DG_TRY(lapmass_residual_f64(L.A.get(), x, b, L.t.p, L.acc.p, s, L.jcoef(), L.jset()));
   } else {
     DG_CUDA(cudaMemsetAsync(x, 0, 8 * n, s));
   }
@@ -706,7 +807,8 @@ dg_status vcycle(dg_damg* m, size_t l, const double* b, double* x) {
                                                             m->cfg.nu_pre > 0 ? (const double*)L.t.p : b, C.b.p);
   DG_TRY(vcycle(m, l + 1, C.b.p, C.x.p));
   prolong_add<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval.p, n, C.x.p, x);
-  for (int k = 0; k < m->cfg.nu_post; ++k) DG_TRY(lapmass_smooth_f64(L.A.get(), x, b, L.dinv.p, w, L.acc.p, s));
+  for (int k = 0; k < m->cfg.nu_post; ++k)
+    DG_TRY(lapmass_smooth_f64(L.A.get(), x, b, L.dinv.p, w, L.acc.p, s, L.jcoef(), L.jset()));
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }
@@ -728,8 +830,9 @@ dg_status vcycle32(dg_damg* m, size_t l, const float* b, float* x) {
   const float w = float(m->cfg.omega);
   if (m->cfg.nu_pre > 0) {
     jacobi_first<<<g, 256, 0, s>>>(x, b, L.dinv32.p, w, n);
-    for (int k = 1; k < m->cfg.nu_pre; ++k) DG_TRY(lapmass_smooth_f32(L.A.get(), x, b, L.dinv32.p, w, L.acc32.p, s));
-    DG_TRY(lapmass_residual_f32(L.A.get(), x, b, L.t32.p, L.acc32.p, s));
+    for (int k = 1; k < m->cfg.nu_pre; ++k)
+      DG_TRY(lapmass_smooth_f32(L.A.get(), x, b, L.dinv32.p, w, L.acc32.p, s, L.jcoef32(), L.jset()));
+    DG_TRY(lapmass_residual_f32(L.A.get(), x, b, L.t32.p, L.acc32.p, s, L.jcoef32(), L.jset()));
   } else {
     DG_CUDA(cudaMemsetAsync(x, 0, 4 * n, s));
   }
@@ -747,7 +850,7 @@ dg_status vcycle32(dg_damg* m, size_t l, const float* b, float* x) {
     }
   } else {
     for (int k = 0; k < m->cfg.nu_post; ++k)
-      DG_TRY(lapmass_smooth_f32(L.A.get(), x, b, L.dinv32.p, w, L.acc32.p, s));
+      DG_TRY(lapmass_smooth_f32(L.A.get(), x, b, L.dinv32.p, w, L.acc32.p, s, L.jcoef32(), L.jset()));
   }
   DG_CUDA(cudaGetLastError());
   return DG_OK;
@@ -834,6 +937,7 @@ void dg_damg_default_config(dg_damg_config* c) {
   c->maxit = 200;
   c->inner_prec = DG_PREC_F64;
   c->use_graph = 0;
+  c->coarse_op = 0;
 }
 
 }  // extern "C"
@@ -1289,6 +1393,24 @@ dg_status dg_damg_features(dg_damg* m, const double* r, float* F, float* scale) 
   DG_CUDA(cudaMemcpyAsync(&h, sc.p, 4, cudaMemcpyDeviceToHost, m->s));
   DG_CUDA(cudaStreamSynchronize(m->s));
   if (scale) *scale = h;
+  return DG_OK;
+}
+
+dg_status dg_damg_level_apply(dg_damg* m, int level, const double* x, double* y, int on_device) {
+  DG_CHECK(m && x && y && level >= 0 && size_t(level) < m->lv.size(), DG_EINVAL, "damg_level_apply: bad arguments");
+  Level& L = m->lv[size_t(level)];
+  DG_CHECK(L.A && L.A->kind == 0, DG_EINVAL, "damg_level_apply: no Laplacian-mass operator set");
+  const int64_t n = L.da->N;
+  const double* xd = x;
+  double* yd = y;
+  if (!on_device) {
+    DG_CUDA(cudaMemcpyAsync(L.x.p, x, 8 * n, cudaMemcpyHostToDevice, m->s));
+    xd = L.x.p;
+    yd = L.b.p;
+  }
+  DG_TRY(lapmass_apply_j_f64(L.A.get(), L.jcoef(), L.jset(), xd, yd, m->s));
+  if (!on_device) DG_CUDA(cudaMemcpyAsync(y, L.b.p, 8 * n, cudaMemcpyDeviceToHost, m->s));
+  DG_CUDA(cudaStreamSynchronize(m->s));
   return DG_OK;
 }
 

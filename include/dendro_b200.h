@@ -213,6 +213,12 @@ typedef struct dg_damg_config {
   int maxit;            /* outer iteration cap */
   int inner_prec;       /* dg_prec of the V-cycle (F64, or F32 inside FP64 outer) */
   int use_graph;        /* capture the V-cycle in a CUDA graph */
+  int coarse_op;        /* operators below the finest level: 0 from the level's averaged coefficients
+                           (Jacobian2 with ASSIGN_MAT_PROP_FINE_TO_COARSE, omgNeumann.C:73-113); 1 from the
+                           next finer level's coefficients (Jacobian3, examples/src/backend/omgJac.C:2139-2340:
+                           a coarse element whose 8 children's coefficients differ takes the sum of the
+                           children's operators, the type-1 stencils); the Jacobi diagonal is the averaged
+                           operator's either way, as the reference's B matrix */
 } dg_damg_config;
 
 typedef struct dg_solve_report {
@@ -262,6 +268,9 @@ dg_status dg_damg_restrict(dg_damg* m, int level, const double* rf, double* rc, 
 void dg_damg_destroy(dg_damg* m);
 
 /* PCApply of the multigrid preconditioner: one V-cycle on device vectors. */
+/* y = J x on one level (0 = finest): the operator the V-cycle smooths and
+ * takes residuals with on that level (MatMult of damg[l]->J). */
+dg_status dg_damg_level_apply(dg_damg* m, int level, const double* x, double* y, int on_device);
 dg_status dg_damg_vcycle(dg_damg* m, const double* b, double* x);
 
 /* ------------------------------------------------------- learned smoother --- */

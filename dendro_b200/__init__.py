@@ -13,7 +13,8 @@ Host-side mirror of the reference's interfaces on this path:
 All work runs in libdendro_b200.so (CUDA, sm_100a); importing this package
 does not load it until first use, and every use fails loudly without it.
 """
-from .api import (DA, DAMG, Elasticity, Jacobian2, Octree, balanceOctree, coarsenOctree,  # noqa: F401
+from .api import (DA, DAMG, DirichletJacobian, DirichletLaplacian, Elasticity, Jacobian2,  # noqa: F401
+                  Octree, balanceOctree, coarsenOctree,
                   deviceCheck, points2Octree, readDataPtsFromFile, readNodesFromFile, readPtsFromFile,
                   setDeviceWaitLimit, vecDot, writeDataPtsToFile, writeNodesToFile, writePtsToFile)
 from ._lib import DendroError, OCT_DTYPE  # noqa: F401

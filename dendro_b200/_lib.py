@@ -119,6 +119,7 @@ def lib():
         "dg_octree_read": ([C.c_char_p, PP], I),
         "dg_da_dump_mesh": ([P, C.c_char_p], I),
         "dg_damg_level_apply": ([P, I, P, P, I], I),
+        "dg_mat_create_dirichlet": ([P, I, P, PP], I),
         "dg_set_device_wait_limit": ([I64], I),
     }
     for name, (args, res) in sig.items():
@@ -146,6 +147,7 @@ def exported_symbols():
         "dg_vec_dot_noalloc", "dg_mat_kernel_count", "dg_mat_set_kernel", "dg_device_check",
         "dg_set_device_wait_limit", "dg_write_pts", "dg_read_pts", "dg_write_data_pts", "dg_read_data_pts",
         "dg_octree_write", "dg_octree_read", "dg_da_dump_mesh", "dg_damg_level_apply",
+        "dg_mat_create_dirichlet",
         "dg_mat_mult_multi", "dg_damg_set_tolerances",
     ]
 

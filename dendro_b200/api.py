@@ -273,6 +273,27 @@ class Elasticity(_Mat):
         super().__init__(da, h)
 
 
+class DirichletLaplacian(_Mat):
+    """CreateDirichletLaplacian / DirichletLaplacianMatMult (examples/src/backend/
+    omgJac.C:61, 859): h/2 L with unit coefficients, Dirichlet rows identity and
+    columns dropped; dirichlet [N] defaults to the domain-boundary nodes."""
+
+    _mass = 0
+
+    def __init__(self, da: DA, dirichlet=None):
+        h = C.c_void_p()
+        d = None if dirichlet is None else np.ascontiguousarray(dirichlet, np.uint8)
+        check(lib().dg_mat_create_dirichlet(da.h, self._mass, ptr(d), C.byref(h)), "mat_create_dirichlet")
+        super().__init__(da, h)
+
+
+class DirichletJacobian(DirichletLaplacian):
+    """CreateDirichletJacobian / DirichletJacobianMatMult (omgJac.C:166, 957):
+    h/2 L + h^3/8 M with unit coefficients, Dirichlet rows and columns as above."""
+
+    _mass = 1
+
+
 class DAMG:
     """ot::DAMG: level hierarchy + V-cycle preconditioned CG on the GPU."""
 

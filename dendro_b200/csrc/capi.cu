@@ -372,9 +372,29 @@ dg_status dg_mat_create_elasticity(dg_da* da, double mu, double lambda, const ui
   return DG_OK;
 }
 
+dg_status dg_mat_create_dirichlet(dg_da* da, int with_mass, const uint8_t* dirichlet, dg_mat** out) {
+  DG_CHECK(da && out, DG_EINVAL, "mat_create_dirichlet: bad arguments");
+  auto* A = new dg_mat();
+  A->da = da;
+  A->kind = with_mass ? 3 : 2;
+  A->dof = 1;
+  dg_status st = A->dirichlet.alloc(da->N);
+  if (!st) {
+    if (dirichlet) {
+      if (cudaMemcpy(A->dirichlet.p, dirichlet, da->N, cudaMemcpyHostToDevice) != cudaSuccess) st = DG_ECUDA;
+    } else {
+      st = node_boundary_flags(da, A->dirichlet.p, nullptr);
+    }
+  }
+  if (st) { delete A; return st; }
+  *out = A;
+  return DG_OK;
+}
+
 dg_status dg_mat_mult(dg_mat* A, const double* x, double* y, void* stream) {
   DG_CHECK(A && x && y, DG_EINVAL, "mat_mult: bad arguments");
   if (A->kind == 1) return elasticity_apply_f64(A, x, y, as_stream(stream));
+  if (A->kind >= 2) return dirichlet_apply_f64(A, x, y, as_stream(stream));
   return lapmass_apply_f64(A, x, y, as_stream(stream));
 }
 
@@ -387,6 +407,7 @@ dg_status dg_mat_mult_f32(dg_mat* A, const float* x, float* y, void* stream) {
 dg_status dg_mat_get_diagonal(dg_mat* A, double* d, void* stream) {
   DG_CHECK(A && d, DG_EINVAL, "mat_get_diagonal: bad arguments");
   if (A->kind == 1) return elasticity_diag(A, d, as_stream(stream));
+  if (A->kind >= 2) return dirichlet_diag(A, d, as_stream(stream));
   return lapmass_diag(A, d, as_stream(stream));
 }
 
@@ -411,7 +432,9 @@ dg_status dg_set_device_wait_limit(int64_t cycles) {
 int64_t dg_mat_size(const dg_mat* A) { return A ? int64_t(A->dof) * A->da->N : 0; }
 
 const char* dg_mat_kernel_name(const dg_mat* A, int prec) {
-  if (!A || A->kind != 0) return "elasticity";
+  if (!A) return "none";
+  if (A->kind == 1) return "elasticity";
+  if (A->kind >= 2) return "dirichlet";
   return matvec_variant_name(prec == DG_PREC_F64 ? A->da->tuned_f64 : A->da->tuned_f32);
 }
 

@@ -60,7 +60,7 @@ struct dg_mlp {
 
 struct dg_mat {
   dg_da* da = nullptr;
-  int kind = 0;  // 0 lap+mass, 1 elasticity
+  int kind = 0;  // 0 lap+mass, 1 elasticity, 2 Dirichlet Laplacian, 3 Dirichlet Jacobian
   int dof = 1;
   bool has_coef = false;
   dg::DBuf<double> coef;       // [2][E] (a then b), FP64
@@ -171,6 +171,9 @@ int matvec_variant_count();
 dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int nrhs, int split, cudaStream_t s);
 dg_status elasticity_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status elasticity_diag(const dg_mat* A, double* d, cudaStream_t s);
+// Dirichlet Laplacian (kind 2) / Jacobian (kind 3) on A->dirichlet node flags.
+dg_status dirichlet_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
+dg_status dirichlet_diag(const dg_mat* A, double* d, cudaStream_t s);
 // Dense assembled operator of a small level as row-major blocks, one per
 // independent mesh: node r belongs to block row_blk[r] with node offset
 // boff[b], size bn[b] and storage offset baoff[b].

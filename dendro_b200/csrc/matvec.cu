@@ -1447,6 +1447,69 @@ __global__ void set_dirichlet_diag(const uint8_t* __restrict__ dir, int64_t N, d
     if (dir[i]) d[3 * i] = d[3 * i + 1] = d[3 * i + 2] = 1.0;
 }
 
+// DirichletLaplacianMatMult / DirichletJacobianMatMult (examples/src/backend/
+// omgJac.C:859-1056): unit coefficients, h/2 L (+ h^3/8 M for the Jacobian);
+// the columns of Dirichlet nodes are dropped (their x entries enter as zero,
+// in node space, before the hanging interpolation) and their rows become the
+// identity (a pass after the elements).
+__global__ void __launch_bounds__(128) dirichlet_scalar_kernel(const uint32_t* __restrict__ nl,
+                                                               const uint32_t* __restrict__ meta,
+                                                               const uint8_t* __restrict__ dir, int64_t E,
+                                                               double mass, const double* __restrict__ x,
+                                                               double* __restrict__ y) {
+  for (int64_t e = gtid(); e < E; e += gstride()) {
+    const uint32_t m = meta[e];
+    const uint32_t c = meta_cnum(m), mask = meta_mask(m);
+    const double h = elem_h<double>(meta_lev(m));
+    uint32_t id[8];
+    bool bd[8];
+    double u[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      id[v] = __ldg(nl + int64_t(v) * E + e);
+      bd[v] = __ldg(dir + id[v]) != 0;
+      u[v] = bd[v] ? 0.0 : __ldg(x + id[v]);
+    }
+    if (mask) interp_hanging(u, c, mask);
+    lapmass_ref(u, h * 0.5, mass * h * h * h * 0.125);
+    if (mask) scatter_hanging(u, c, mask);
+#pragma unroll
+    for (int v = 0; v < 8; ++v)
+      if (!bd[v]) atomicAdd(y + id[v], u[v]);
+  }
+}
+__global__ void dirichlet_scalar_rows(const uint8_t* __restrict__ dir, int64_t N, const double* __restrict__ x,
+                                      double* __restrict__ y) {
+  for (int64_t i = gtid(); i < N; i += gstride())
+    if (dir[i]) y[i] = x[i];
+}
+// DirichletLaplacianMatGetDiagonal / DirichletJacobianMatGetDiagonal
+// (omgJac.C:1058-1160): one thread per (element, vertex).
+__global__ void dirichlet_scalar_diag_kernel(const uint32_t* __restrict__ nl, const uint32_t* __restrict__ meta,
+                                             const uint8_t* __restrict__ dir, int64_t E, double mass,
+                                             double* __restrict__ d) {
+  for (int64_t t = gtid(); t < E * 8; t += gstride()) {
+    const int64_t e = t >> 3;
+    const int j = int(t & 7);
+    const uint32_t node = nl[int64_t(j) * E + e];
+    if (dir[node]) continue;
+    const uint32_t m = meta[e];
+    const uint32_t c = meta_cnum(m), mask = meta_mask(m);
+    const double h = elem_h<double>(meta_lev(m));
+    double u[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) u[v] = v == j ? 1.0 : 0.0;
+    if (mask) interp_hanging(u, c, mask);
+    lapmass_ref(u, h * 0.5, mass * h * h * h * 0.125);
+    if (mask) scatter_hanging(u, c, mask);
+    atomicAdd(d + node, u[j]);
+  }
+}
+__global__ void set_dirichlet_diag1(const uint8_t* __restrict__ dir, int64_t N, double* __restrict__ d) {
+  for (int64_t i = gtid(); i < N; i += gstride())
+    if (dir[i]) d[i] = 1.0;
+}
+
 }  // namespace
 
 dg_status elasticity_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s) {
@@ -1455,6 +1518,28 @@ dg_status elasticity_apply_f64(const dg_mat* A, const double* x, double* y, cuda
   elasticity_kernel<<<grid_for(da->E, 128, 16), 128, 0, s>>>(da->nl.p, da->meta.p, A->dirichlet.p, da->E, A->mu,
                                                                A->lam, x, y);
   elasticity_dirichlet_rows<<<grid_for(da->N, 256), 256, 0, s>>>(A->dirichlet.p, da->N, x, y);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status dirichlet_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s) {
+  const dg_da* da = A->da;
+  const double mass = A->kind == 3 ? 1.0 : 0.0;
+  DG_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * da->N, s));
+  dirichlet_scalar_kernel<<<grid_for(da->E, 128, 16), 128, 0, s>>>(da->nl.p, da->meta.p, A->dirichlet.p, da->E, mass,
+                                                                     x, y);
+  dirichlet_scalar_rows<<<grid_for(da->N, 256), 256, 0, s>>>(A->dirichlet.p, da->N, x, y);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status dirichlet_diag(const dg_mat* A, double* d, cudaStream_t s) {
+  const dg_da* da = A->da;
+  const double mass = A->kind == 3 ? 1.0 : 0.0;
+  DG_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * da->N, s));
+  dirichlet_scalar_diag_kernel<<<grid_for(da->E * 8, 128, 16), 128, 0, s>>>(da->nl.p, da->meta.p, A->dirichlet.p,
+                                                                              da->E, mass, d);
+  set_dirichlet_diag1<<<grid_for(da->N, 256), 256, 0, s>>>(A->dirichlet.p, da->N, d);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }

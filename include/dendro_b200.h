@@ -166,6 +166,13 @@ dg_status dg_mat_create_elasticity(dg_da* da, double mu, double lambda, const ui
 
 /* MatMult (MATOP_MULT of the MatShell, omgNeumann.C:700-710): y = A x with
  * device pointers on the given CUDA stream (NULL = default stream). */
+/* CreateDirichletLaplacian / CreateDirichletJacobian with their MatMult and
+ * GetDiagonal (examples/src/backend/omgJac.C:61-269, 859-1160): unit
+ * coefficients, h/2 L (with_mass = 0) or h/2 L + h^3/8 M (with_mass = 1); the
+ * rows of the nodes flagged in dirichlet [N] are the identity and their
+ * columns are dropped.  dirichlet == NULL: the domain-boundary nodes
+ * (assignBoundaryFlags, src/oda/odaUtils.C:1054). */
+dg_status dg_mat_create_dirichlet(dg_da* da, int with_mass, const uint8_t* dirichlet, dg_mat** out);
 dg_status dg_mat_mult(dg_mat* A, const double* x, double* y, void* stream);
 /* FP32 inner-solver form of the same operator. */
 dg_status dg_mat_mult_f32(dg_mat* A, const float* x, float* y, void* stream);

@@ -653,6 +653,41 @@ int coarse_coef(const Mesh& F, const double* fc, const Mesh& C, std::vector<doub
   return 0;
 }
 
+// DirichletLaplacianMatMult / DirichletJacobianMatMult and their diagonals
+// (examples/src/backend/omgJac.C:859-1160): unit coefficients, h/2 L plus
+// h^3/8 M when mass is set; a Dirichlet row is the identity, a Dirichlet
+// column is skipped.
+void dirichlet_matvec(const Mesh& M, int mass, const uint8_t* bdy, const double* x, double* y) {
+  const Tables& T = tables();
+  std::fill(y, y + M.N, 0.0);
+  for (size_t e = 0; e < M.E; ++e) {
+    const double h = std::ldexp(1.0, 1 - int(M.elev[e]));
+    const double f1 = h / 2.0, f2 = mass ? h * h * h / 8.0 : 0.0;
+    const uint32_t* idx = &M.nlist[8 * e];
+    const uint32_t c = M.cnum[e], t = M.etype[e];
+    for (int k = 0; k < 8; ++k) {
+      if (bdy[idx[k]]) {
+        y[idx[k]] = x[idx[k]];
+        continue;
+      }
+      for (int j = 0; j < 8; ++j)
+        if (!bdy[idx[j]]) y[idx[k]] += (f1 * T.L[c][t][k][j] + f2 * T.Ms[c][t][k][j]) * x[idx[j]];
+    }
+  }
+}
+void dirichlet_diagonal(const Mesh& M, int mass, const uint8_t* bdy, double* d) {
+  const Tables& T = tables();
+  std::fill(d, d + M.N, 0.0);
+  for (size_t e = 0; e < M.E; ++e) {
+    const double h = std::ldexp(1.0, 1 - int(M.elev[e]));
+    const double f1 = h / 2.0, f2 = mass ? h * h * h / 8.0 : 0.0;
+    const uint32_t* idx = &M.nlist[8 * e];
+    const uint32_t c = M.cnum[e], t = M.etype[e];
+    for (int k = 0; k < 8; ++k)
+      d[idx[k]] = bdy[idx[k]] ? 1.0 : d[idx[k]] + f1 * T.L[c][t][k][k] + f2 * T.Ms[c][t][k][k];
+  }
+}
+
 // JAC_TYPE3_MULT_BLOCK (examples/src/backend/omgJac.C:2139-2233): the
 // operator of a coarse level from the next finer level's coefficients fc.
 // A coarse element that is also a fine element uses its coefficients with the
@@ -1012,6 +1047,12 @@ void orc_type1_stencils(double* L, double* M) {
   const Tables1& T = tables1();
   std::memcpy(L, T.L, sizeof T.L);
   std::memcpy(M, T.Ms, sizeof T.Ms);
+}
+void orc_dirichlet_matvec(void* m, int mass, const uint8_t* bdy, const double* x, double* y) {
+  dirichlet_matvec(*(Mesh*)m, mass, bdy, x, y);
+}
+void orc_dirichlet_diagonal(void* m, int mass, const uint8_t* bdy, double* d) {
+  dirichlet_diagonal(*(Mesh*)m, mass, bdy, d);
 }
 int orc_jacobian3(void* fine, const double* fc, void* coarse, const double* x, double* y) {
   return jacobian3(*(Mesh*)fine, fc, *(Mesh*)coarse, x, y);

@@ -67,6 +67,8 @@ def lib():
         L.orc_damg_level_apply.argtypes = [P, C.c_int, P, P]
         L.orc_type1_stencils.argtypes = [P, P]
         L.orc_jacobian3.argtypes = [P, P, P, P, P]
+        L.orc_dirichlet_matvec.argtypes = [P, C.c_int, P, P, P]
+        L.orc_dirichlet_diagonal.argtypes = [P, C.c_int, P, P]
         _lib = L
     return _lib
 
@@ -154,6 +156,20 @@ class Mesh:
         d = np.empty(self.N, np.float64)
         c = None if coef is None else np.ascontiguousarray(coef, np.float64)
         lib().orc_diagonal(self.h, _ptr(c), _ptr(d))
+        return d
+
+    def dirichlet_matvec(self, x, bdy, mass: bool):
+        """DirichletLaplacianMatMult (mass False) / DirichletJacobianMatMult."""
+        x = np.ascontiguousarray(x, np.float64)
+        b = np.ascontiguousarray(bdy, np.uint8)
+        y = np.empty_like(x)
+        lib().orc_dirichlet_matvec(self.h, int(mass), _ptr(b), _ptr(x), _ptr(y))
+        return y
+
+    def dirichlet_diagonal(self, bdy, mass: bool):
+        b = np.ascontiguousarray(bdy, np.uint8)
+        d = np.empty(self.N)
+        lib().orc_dirichlet_diagonal(self.h, int(mass), _ptr(b), _ptr(d))
         return d
 
     def elasticity_matvec(self, x, mu, lam, bdy=None):

@@ -25,6 +25,11 @@
 //       the Jacobian-3 context of that level: the next finer level's DA and
 //       its coefficients coef<l-1>.f64 (a, b per element), applied to
 //       jin<l>.f64 -> jout<l>.f64 (files in outdir)
+//   dendro_ref dirichlet <octs.u32> <maxDepth> <x.f64> <outdir>
+//       assignBoundaryFlags (src/oda/odaUtils.C:1054) -> bdy.u8 (nodal Vec),
+//       DirichletLaplacianMatMult / DirichletJacobianMatMult and their
+//       GetDiagonal (examples/src/backend/omgJac.C:859-1160) -> yL.f64, yJ.f64,
+//       dL.f64, dJ.f64
 //   dendro_ref io <octs.u32> <maxDepth> <pts.f64> <vals.f64> <outdir>
 //       the reference's file writers (src/oct/OctFunctions.C:313-440):
 //       writeNodesToFile -> octs.ot, writePtsToFile -> pts.pts,
@@ -267,6 +272,42 @@ int main(int argc, char** argv) {
       write_raw(dir + "/jout" + std::to_string(l) + ".f64", y.data(), y.size());
       coarse->user = saved;
     }
+    return 0;
+  }
+  if (mode == "dirichlet" && argc >= 6) {
+    unsigned D = atoi(argv[3]);
+    std::vector<ot::TreeNode> octs = read_octs(argv[2], D);
+    ot::DA da(octs, MPI_COMM_WORLD, MPI_COMM_WORLD, false);
+    createLmatType2(LaplacianType2Stencil);
+    createMmatType2(MassType2Stencil);
+    std::vector<double> x = read_raw<double>(argv[4]);
+    std::string dir = argv[5];
+    std::vector<unsigned char> flags;
+    ot::assignBoundaryFlags(&da, flags);
+    write_raw(dir + "/bdy.u8", flags.data(), flags.size());
+    DirichletJacData data;
+    std::memset((void*)&data, 0, sizeof(data));
+    da.vecGetBuffer<unsigned char>(flags, data.bdyArr, false, false, true, 1);
+    ot::DAMG damg = new ot::_p_DAMG;
+    std::memset((void*)damg, 0, sizeof(ot::_p_DAMG));
+    damg->da = &da;
+    damg->nlevels = 1;
+    damg->user = &data;
+    Mat J;
+    MatCreateShell(MPI_COMM_WORLD, int(x.size()), int(x.size()), PETSC_DETERMINE, PETSC_DETERMINE, damg, &J);
+    Vec in = make_vec(x), out = make_vec(x), dg = make_vec(x);
+    DirichletLaplacianMatMult(J, in, out);
+    std::vector<double> y = vec_data(out);
+    write_raw(dir + "/yL.f64", y.data(), y.size());
+    DirichletJacobianMatMult(J, in, out);
+    y = vec_data(out);
+    write_raw(dir + "/yJ.f64", y.data(), y.size());
+    DirichletLaplacianMatGetDiagonal(J, dg);
+    y = vec_data(dg);
+    write_raw(dir + "/dL.f64", y.data(), y.size());
+    DirichletJacobianMatGetDiagonal(J, dg);
+    y = vec_data(dg);
+    write_raw(dir + "/dJ.f64", y.data(), y.size());
     return 0;
   }
   if (mode == "io" && argc >= 7) {

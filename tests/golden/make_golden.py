@@ -10,6 +10,7 @@ tests read only them.
     python tests/golden/make_golden.py            # everything
     python tests/golden/make_golden.py --io-only  # the file-format fixtures io_*.npz
     python tests/golden/make_golden.py --jac3-only  # Jacobian3 fixture + stencil digests
+    python tests/golden/make_golden.py --dirichlet-only  # Dirichlet operator fixtures
 
 The file-format fixtures also run oracle/_ref/dendro_ref_dumpmesh, the
 reference's examples/src/drivers/dumpMesh.C built single-rank.
@@ -144,6 +145,18 @@ def transfer_fixture(tmp):
     np.savez_compressed(os.path.join(OUT, f"transfer_{name}.npz"), **rec)
 
 
+def dirichlet_fixture(tmp, name):
+    """The reference's boundary flags (assignBoundaryFlags) and its Dirichlet
+    Laplacian / Jacobian MatMult and GetDiagonal on the mesh case."""
+    z = np.load(os.path.join(OUT, f"mesh_{name}.npz"))
+    z["bal"].astype(np.uint32).tofile(os.path.join(tmp, "bal_d.u32"))
+    z["x"].tofile(os.path.join(tmp, "x_d.f64"))
+    run("dirichlet", os.path.join(tmp, "bal_d.u32"), int(z["depth"]), os.path.join(tmp, "x_d.f64"), tmp)
+    rd = lambda f, dt=np.float64: np.fromfile(os.path.join(tmp, f), dt)  # noqa: E731
+    np.savez_compressed(os.path.join(OUT, f"dirichlet_{name}.npz"), bdy=rd("bdy.u8", np.uint8), x=z["x"],
+                        yL=rd("yL.f64"), yJ=rd("yJ.f64"), dL=rd("dL.f64"), dJ=rd("dJ.f64"))
+
+
 def jac3_fixture(tmp):
     """Jacobian3MatMult (examples/src/backend/omgJac.C:2235) on the coarse
     levels of the transfer case's hierarchy, from the next finer level's
@@ -232,6 +245,11 @@ def main():
     if "--stencils-only" in sys.argv:
         stencil_digests()
         return
+    if "--dirichlet-only" in sys.argv:
+        with tempfile.TemporaryDirectory() as tmp:
+            for name in MESH_CASES:
+                dirichlet_fixture(tmp, name)
+        return
     if "--jac3-only" in sys.argv:
         with tempfile.TemporaryDirectory() as tmp:
             jac3_fixture(tmp)
@@ -248,6 +266,8 @@ def main():
             mesh_fixture(tmp, name)
         transfer_fixture(tmp)
         jac3_fixture(tmp)
+        for name in MESH_CASES:
+            dirichlet_fixture(tmp, name)
         for name in IO_CASES:
             io_fixture(tmp, name)
     stencil_digests()

@@ -40,6 +40,7 @@ WORKLOAD = "lognormal1m_d14"
 # summaries under profiles/ give the commands).  First matching prefix wins.
 TRAFFIC = {
     "warp-tile 32 elems, 3 CTAs/SM, ids and x of the next tile in flight": 337146106,
+    "warp-tile 32 elems, 5 CTAs/SM": 313580000 + 20210000,
     "warp-tile 32 elems, records by bulk copy": 336114385,
     "warp-tile": 332613888 + 21873408,
 }

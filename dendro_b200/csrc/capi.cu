@@ -139,7 +139,7 @@ int dg_device_count(void) {
 dg_status dg_points2octree(const double* pts, int64_t n, int pts_on_device, uint32_t max_depth, uint32_t max_num_pts,
                            dg_octree** out) {
   DG_CHECK(out && (pts || n == 0) && n >= 0, DG_EINVAL, "points2octree: bad arguments");
-  DG_CHECK(max_depth <= 19, DG_EDEPTH, "points2octree: maxDepth must be <= 19");
+  DG_CHECK(max_depth <= kMaxDepth, DG_EDEPTH, "points2octree: maxDepth must be <= 19");
   auto* t = new dg_octree();
   DBuf<double> dp;
   const double* src = pts;
@@ -156,7 +156,7 @@ dg_status dg_points2octree(const double* pts, int64_t n, int pts_on_device, uint
 
 dg_status dg_octree_from_octants(const dg_octant* octs, int64_t n, int on_device, uint32_t max_depth, dg_octree** out) {
   DG_CHECK(out && octs && n > 0, DG_EINVAL, "octree_from_octants: bad arguments");
-  DG_CHECK(max_depth <= 19, DG_EDEPTH, "octree_from_octants: maxDepth must be <= 19");
+  DG_CHECK(max_depth <= kMaxDepth, DG_EDEPTH, "octree_from_octants: maxDepth must be <= 19");
   DBuf<dg_octant> d;
   const dg_octant* src = octs;
   if (!on_device) {
@@ -231,7 +231,7 @@ dg_status dg_da_create_from_maps(int64_t E, int64_t N, uint32_t max_depth, const
                                  const uint32_t* elem_xyz, dg_da** out) {
   DG_CHECK(out && nlist && level && cnum && hmask && node_xyz && elem_xyz && E > 0 && N > 0, DG_EINVAL,
            "da_create_from_maps: bad arguments");
-  DG_CHECK(max_depth + 1 <= kMaxEmbeddedDepth, DG_EDEPTH, "da_create_from_maps: maxDepth must be <= 19");
+  DG_CHECK(max_depth + 1 <= kMaxEmbeddedDepth, DG_EDEPTH, "da_create_from_maps: maxDepth must be <= 18");
   auto* da = new dg_da();
   da->D = max_depth + 1;
   da->E = E;

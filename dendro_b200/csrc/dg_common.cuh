@@ -41,9 +41,13 @@ void set_error(const char* file, int line, const std::string& msg);
 constexpr uint32_t kLevelMask = 31u;
 constexpr uint32_t kBoundary = 64u;
 constexpr uint32_t kNode = 128u;
-// Deepest supported anchor depth (embedded depth, maxDepth + 1): 3*20 = 60
-// bits of Morton key + 4 bits free for the level tag in the low bits below.
-constexpr uint32_t kMaxEmbeddedDepth = 20;
+// Deepest supported depths.  A key is the Morton anchor shifted left by 5
+// with the level (up to the depth, 5 bits) below it: 3 depth + 5 <= 64 bits.
+// Octrees go to maxDepth 19 (62 bits); a mesh embeds its octree one level
+// deeper (addBoundaryNodesType1), so meshes go to maxDepth 18 (embedded
+// depth 19, 62 bits).
+constexpr uint32_t kMaxDepth = 19;
+constexpr uint32_t kMaxEmbeddedDepth = 19;
 
 // Morton key of an anchor: bits interleaved z>y>x within each triple, so that
 // integer order equals the reference's Morton comparator for distinct anchors

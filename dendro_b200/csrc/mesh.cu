@@ -403,7 +403,8 @@ static dg_status upload_etype_lut() {
 dg_status build_mesh(const dg_octree* tree, dg_da* da, cudaStream_t s) {
   const uint32_t D = tree->max_depth;
   const int64_t E = tree->n;
-  DG_CHECK(D + 1 <= kMaxEmbeddedDepth, DG_EDEPTH, "maxDepth above 19 is not supported");
+  DG_CHECK(D + 1 <= kMaxEmbeddedDepth, DG_EDEPTH,
+           "mesh: maxDepth above 18 is not supported (the embedded depth's keys would exceed 64 bits)");
   DG_CHECK(E >= 1, DG_EINVAL, "empty octree");
   DG_TRY(upload_etype_lut());
   const uint32_t Dp = D + 1;

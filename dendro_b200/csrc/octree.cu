@@ -258,7 +258,7 @@ static dg_status set_root(dg_octree* out, uint32_t D, cudaStream_t s) {
 }
 
 dg_status points_to_octree(const double* d_pts, int64_t n, uint32_t D, uint32_t m, dg_octree* out, cudaStream_t s) {
-  DG_CHECK(D + 1 <= kMaxEmbeddedDepth, DG_EDEPTH, "maxDepth above 19 is not supported");
+  DG_CHECK(D <= kMaxDepth, DG_EDEPTH, "maxDepth above 19 is not supported");
   DG_CHECK(m >= 1, DG_EINVAL, "maxNumPts must be >= 1");
   DG_CHECK(n >= 0, DG_EINVAL, "negative point count");
   if (D == 0 || n <= int64_t(m)) return set_root(out, D, s);  // Construct.C:884-888,915-919
@@ -302,7 +302,7 @@ dg_status points_to_octree(const double* d_pts, int64_t n, uint32_t D, uint32_t 
 dg_status balance_octree(const dg_octree* in, dg_octree* out, cudaStream_t s) {
   const uint32_t D = in->max_depth;
   const int64_t n = in->n;
-  DG_CHECK(D <= 19, DG_EDEPTH, "maxDepth above 19 is not supported");
+  DG_CHECK(D <= kMaxDepth, DG_EDEPTH, "maxDepth above 19 is not supported");
   if (n <= 1) {
     out->max_depth = D;
     DG_TRY(out->keys.alloc(n > 0 ? n : 1));

@@ -107,6 +107,7 @@ dg_status dg_octree_read(const char* path, dg_octree** out);
  * anchors (flagNodesType3, OctFunctions.C:1501) and builds the element->node
  * map with hanging masks, child numbers and element types (buildNodeList,
  * src/oda/private/odaBuildNlist.C:47-856).  The input octree is not consumed. */
+/* Meshes take octrees of maxDepth <= 18 (DG_EDEPTH above). */
 dg_status dg_da_create(const dg_octree* balanced, dg_da** out);
 
 /* Build a mesh from maps computed elsewhere (host arrays): nlist [E][8] node

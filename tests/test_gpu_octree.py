@@ -56,3 +56,55 @@ def test_unsorted_octants_rejected(gpu, oracle):
     lin = oracle.points2octree(pts, d, m)
     with pytest.raises(gpu.DendroError):
         gpu.Octree.from_octants(lin[::-1].copy(), d)
+
+
+def test_empty_point_set(gpu, oracle):
+    """No points: the complete octree is the root octant alone, as the oracle's."""
+    ref = oracle.points2octree(np.zeros((0, 3)), 6, 1)
+    t = gpu.points2Octree(np.zeros((0, 3)), 6, 1)
+    assert same(t.to_numpy(), ref)
+    assert same(gpu.balanceOctree(t).to_numpy(), oracle.balance(ref, 6))
+
+
+def deep_points(d):
+    from dendro_b200 import inputs as I
+    # two points one finest cell apart force leaves at level d
+    return np.concatenate([np.array([[0.5, 0.5, 0.5], [0.5 + 2.0 ** -d, 0.5, 0.5]]),
+                           I.clamp_unit(np.random.default_rng(3).uniform(0, 1, (200, 3)), d)])
+
+
+def test_deepest_supported_octree(gpu, oracle):
+    """Octrees go to maxDepth 19 (bit-exact); maxDepth 20 is refused with
+    DG_EDEPTH, and so is a mesh of a depth-19 octree (its embedded keys would
+    need 65 bits)."""
+    d = 19
+    pts = deep_points(d)
+    lin = oracle.points2octree(pts, d, 1)
+    assert (lin["lf"] & 31).max() == d
+    got = gpu.points2Octree(pts, d, 1)
+    assert same(got.to_numpy(), lin)
+    gb = gpu.balanceOctree(got)
+    assert same(gb.to_numpy(), oracle.balance(lin, d))
+    for call in (lambda: gpu.points2Octree(pts, 20, 1), lambda: gpu.DA(gb)):
+        with pytest.raises(gpu.DendroError) as err:
+            call()
+        assert err.value.status == 7  # DG_EDEPTH
+
+
+def test_deepest_supported_mesh(gpu, oracle):
+    """Meshes go to maxDepth 18 (embedded depth 19): octree, balance, mesh and
+    operator match the oracle with leaves at the deepest level."""
+    from dendro_b200 import inputs as I
+    d = 18
+    pts = deep_points(d)
+    lin = oracle.points2octree(pts, d, 1)
+    assert (lin["lf"] & 31).max() == d
+    bal = oracle.balance(lin, d)
+    gb = gpu.balanceOctree(gpu.points2Octree(pts, d, 1))
+    assert same(gb.to_numpy(), bal)
+    ref = oracle.Mesh(bal, d)
+    da = gpu.DA(gb)
+    assert (da.E, da.N) == (ref.E, ref.N)
+    x = I.uniform_rhs(ref.N, 4)
+    y, yr = gpu.Jacobian2(da).mult(x), ref.matvec(x)
+    assert np.linalg.norm(y - yr) <= 1e-12 * np.linalg.norm(yr)

@@ -64,6 +64,9 @@ def parse():
     p.add_argument("--vcycle-profile", metavar="WORKLOAD", default=None,
                    help="only: one FP64 and one FP32 V(2,2) cycle on WORKLOAD's hierarchy between "
                         "cudaProfilerStart/Stop (for ncu --profile-from-start off), then exit")
+    p.add_argument("--halo-profile", metavar="PARTS", type=int, default=0,
+                   help="only: split the matvec workload's mesh into PARTS parts (all on this GPU) and time "
+                        "each part's pack, independent and dependent operator launches, then exit")
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     return p.parse_args()
 
@@ -390,12 +393,69 @@ def run_vcycle_profile(workload):
     print(json.dumps({"vcycle_profile": out}), flush=True)
 
 
+def run_halo_profile(parts, workload):
+    """The matvec workload's mesh split into `parts` parts by the weighted
+    partition, every part on this GPU in turn: per part the launches one
+    rank makes per operator application (pack of the values its peers read,
+    the independent elements, the dependent elements with their gather and
+    scatter) timed with CUDA events after a 256 MB L2 flush (median of 20),
+    beside the whole mesh's operator.  The exchange itself needs several GPUs
+    and is reported as bytes per rank."""
+    import statistics
+
+    import torch
+
+    import dendro_b200 as dg
+    from dendro_b200 import inputs as I
+    from dendro_b200.halo import HaloDA, HaloJacobian2
+    pts, depth = build_workload(workload, 1.0)
+    da = dg.DA(dg.balanceOctree(dg.points2Octree(pts, depth, 1)))
+    coef = I.sphere_coefficients(da.elementCenters())
+    x = torch.tensor(I.uniform_rhs(da.N, 1), device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps=20):
+        for _ in range(3):
+            fn()
+        ts = []
+        for i in range(reps):
+            flush.fill_(i & 255)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return round(statistics.median(ts), 4)
+
+    A = dg.Jacobian2(da, coef)
+    y = torch.empty_like(x)
+    out = {"workload": workload, "elements": da.E, "nodes": da.N, "parts": parts,
+           "whole_ms": timed(lambda: A.mult(x, y)), "ranks": []}
+    for r in range(parts):
+        h = HaloDA(da, rank=r, nranks=parts)
+        op = HaloJacobian2(h, coef)
+        xl = h.local_vector(x[h.first_owned:h.first_owned + h.n_owned])
+        yl = torch.zeros_like(xl)
+        send = h.pack(xl)
+        out["ranks"].append({
+            "rank": r, "independent": len(h.independent), "dependent": len(h.dependent), "owned": h.n_owned,
+            "ghosts": h.n_ghost, "send_bytes": 8 * len(h.send_idx), "recv_bytes": 8 * h.n_ghost,
+            "pack_ms": timed(lambda: h.pack(xl, send)),
+            "independent_ms": timed(lambda: op._independent(xl, yl)),
+            "dependent_ms": timed(lambda: op._dependent(xl, yl))})
+        del op, h
+    print(json.dumps({"halo_profile": out}), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.vcycle_profile:
         return run_vcycle_profile(args.vcycle_profile)
+    if args.halo_profile:
+        return run_halo_profile(args.halo_profile, args.workload)
     if args.impl == "reference":
         return main_reference(args, rank, world)
     if world > 1:

@@ -121,6 +121,19 @@ def lib():
         "dg_damg_level_apply": ([P, I, P, P, I], I),
         "dg_mat_create_dirichlet": ([P, I, P, PP], I),
         "dg_set_device_wait_limit": ([I64], I),
+        "dg_partition_weighted": ([I64, P, I, P], I),
+        "dg_halo_create": ([I64, I64, U32, P, P, P, P, P, P, P, I, I, PP], I),
+        "dg_halo_create_from_da": ([P, P, I, I, PP], I),
+        "dg_halo_sizes": ([P, I64P, I64P, I64P, I64P, I64P, I64P], I),
+        "dg_halo_ranges": ([P, P, P], I),
+        "dg_halo_comm": ([P, P, P, P, P], I),
+        "dg_halo_part": ([P, I, P, P, P], I),
+        "dg_halo_local_da": ([P, I, PP], I),
+        "dg_halo_pack": ([P, P, P, I, P], I),
+        "dg_halo_accumulate": ([P, P, P, I, P], I),
+        "dg_halo_dep_gather": ([P, P, P, I, P], I),
+        "dg_halo_dep_scatter_add": ([P, P, P, I, P], I),
+        "dg_halo_destroy": ([P], None),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -149,6 +162,9 @@ def exported_symbols():
         "dg_octree_write", "dg_octree_read", "dg_da_dump_mesh", "dg_damg_level_apply",
         "dg_mat_create_dirichlet",
         "dg_mat_mult_multi", "dg_damg_set_tolerances",
+        "dg_partition_weighted", "dg_halo_create", "dg_halo_create_from_da", "dg_halo_sizes", "dg_halo_ranges",
+        "dg_halo_comm", "dg_halo_part", "dg_halo_local_da", "dg_halo_pack", "dg_halo_accumulate",
+        "dg_halo_dep_gather", "dg_halo_dep_scatter_add", "dg_halo_destroy",
     ]
 
 

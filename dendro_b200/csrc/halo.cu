@@ -1,0 +1,415 @@
+// One mesh over several ranks: the partition, one rank's halo, and the
+// kernels of its ghost exchange -- ot::DA with npes > 1 (include/oda/oda.h:500-512;
+// ReadFromGhostsBegin/End and WriteToGhostsBegin/End, include/oda/oda.txx:479-650).
+//
+// Elements are split into contiguous Morton ranges of equal weight by the rule
+// of par::partitionW (include/par/parUtils.txx:1011-1177).  A node belongs to
+// the rank whose range holds its anchor: node ids follow the Morton order of
+// the anchors, so every rank owns one contiguous id range, as the reference's
+// ranks own the nodes anchored at their octants.  A rank keeps every element
+// with a vertex it owns: its independent elements (all eight vertices owned)
+// and its dependent ones (the DEPENDENT loop of Jacobian2MatMult,
+// examples/src/backend/omgNeumann.C:517-523, which with the pre-ghost
+// elements of src/oda/private/odaBuildNlist.C:815-821 covers the partition
+// boundary).  One exchange of ghost node values, owner to reader, before the
+// dependent elements then makes y = A x complete on the owned nodes.
+//
+// Local node numbering of a rank: its owned nodes first (global id minus the
+// first owned id), then its ghost nodes in ascending global id, which groups
+// them by owner in rank order, so an all-to-all of the owners' packed values
+// lands directly after the owned nodes.  The independent elements form one
+// local mesh over the owned nodes; the dependent elements another over the
+// compact list of the local nodes they touch.
+//
+// The partition and the maps are host set-up and touch no GPU; the exchange
+// is a pack kernel, one all-to-all of the packed values and, for
+// accumulation to the owners, a gather-sum kernel in a fixed order.
+#include <algorithm>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "dg_internal.h"
+
+using dg::DBuf;
+
+struct dg_halo {
+  int nranks = 1, rank = 0;
+  uint32_t max_depth = 0;
+  std::vector<int64_t> elem_first, node_first;  // [nranks + 1]
+  int64_t n_own = 0;
+  std::vector<uint32_t> ghosts;                 // global ids, ascending
+  std::vector<int64_t> send_count, recv_count;  // per peer
+  std::vector<uint32_t> send_idx;               // local ids of owned nodes, by peer, then ascending
+  // 0: independent elements over the owned nodes; 1: dependent elements over `nodes`
+  struct Part {
+    std::vector<int64_t> elems;  // global element ids, ascending
+    std::vector<uint32_t> nl;    // [E][8] node ids of the part's mesh
+    std::vector<uint8_t> level, cnum, hmask;
+    std::vector<uint32_t> exyz, nxyz;
+    std::vector<uint32_t> nodes;  // dependent part: local ids of its nodes, ascending
+  } part[2];
+  // accumulation to owners: the positions of send_idx grouped by node
+  std::vector<uint32_t> acc_node, acc_ptr, acc_pos;
+  // device copies, uploaded on the first exchange call
+  int device = -1;
+  DBuf<uint32_t> d_send_idx, d_dep_nodes, d_acc_node, d_acc_ptr, d_acc_pos;
+};
+
+namespace {
+
+constexpr int kHaloThreads = 256;
+
+// par::partitionW (include/par/parUtils.txx:1130-1177) applied to a list held
+// whole: with s the inclusive scan of the weights, W their sum, avg = W / P
+// and extra = W % P, an item goes to rank 0 when s == 0, to (s - 1) / (avg + 1)
+// while s <= extra (avg + 1), else to (s - 1 - extra) / avg; with avg == 0
+// every item goes to rank 0.  The scan is monotone, so every rank receives one
+// contiguous range: first[r] .. first[r + 1].
+void partition_weighted(int64_t n, const uint32_t* w, int P, int64_t* first) {
+  std::vector<int64_t> cnt(P, 0);
+  int64_t W = 0;
+  for (int64_t i = 0; i < n; ++i) W += w ? int64_t(w[i]) : 1;
+  const int64_t avg = W / P, extra = W % P;
+  if (avg == 0) {
+    cnt[0] = n;
+  } else {
+    int64_t s = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      s += w ? int64_t(w[i]) : 1;
+      int64_t r = 0;
+      if (s != 0) r = s <= extra * (avg + 1) ? (s - 1) / (avg + 1) : (s - 1 - extra) / avg;
+      ++cnt[r];
+    }
+  }
+  first[0] = 0;
+  for (int r = 0; r < P; ++r) first[r + 1] = first[r] + cnt[r];
+}
+
+__global__ void __launch_bounds__(kHaloThreads)
+halo_gather(const uint32_t* __restrict__ idx, int64_t n, int dof, const double* __restrict__ x,
+            double* __restrict__ out) {
+  const int64_t total = n * dof;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t k = t / dof;
+    out[t] = x[int64_t(idx[k]) * dof + (t - k * dof)];
+  }
+}
+
+// y[idx[k]] += v[k] for idx[k] < limit (the indices are distinct)
+__global__ void __launch_bounds__(kHaloThreads)
+halo_scatter_add(const uint32_t* __restrict__ idx, int64_t n, int dof, int64_t limit, const double* __restrict__ v,
+                 double* __restrict__ y) {
+  const int64_t total = n * dof;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t k = t / dof;
+    const int64_t i = idx[k];
+    if (i < limit) y[i * dof + (t - k * dof)] += v[t];
+  }
+}
+
+// y[node[u]] += each received value of node u in turn, in peer order (the
+// order of WriteToGhostsEnd's loop over the scatter map, oda.txx:628-633)
+__global__ void __launch_bounds__(kHaloThreads)
+halo_accumulate(const uint32_t* __restrict__ node, const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ pos,
+                int64_t nu, int dof, const double* __restrict__ recv, double* __restrict__ y) {
+  const int64_t total = nu * dof;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t u = t / dof;
+    const int c = int(t - u * dof);
+    double* out = y + int64_t(node[u]) * dof + c;
+    double s = *out;
+    for (uint32_t j = ptr[u]; j < ptr[u + 1]; ++j) s += recv[int64_t(pos[j]) * dof + c];
+    *out = s;
+  }
+}
+
+template <class T>
+dg_status upload_vec(DBuf<T>& d, const std::vector<T>& h) {
+  DG_TRY(d.alloc(int64_t(h.size())));
+  if (!h.empty()) DG_CUDA(cudaMemcpy(d.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+  return DG_OK;
+}
+
+dg_status ensure_device(dg_halo* h) {
+  int dev = -1;
+  DG_CUDA(cudaGetDevice(&dev));
+  if (h->device == dev) return DG_OK;
+  DG_CHECK(h->device < 0, DG_EINVAL, "halo: used on a second device");
+  DG_TRY(upload_vec(h->d_send_idx, h->send_idx));
+  DG_TRY(upload_vec(h->d_dep_nodes, h->part[1].nodes));
+  DG_TRY(upload_vec(h->d_acc_node, h->acc_node));
+  DG_TRY(upload_vec(h->d_acc_ptr, h->acc_ptr));
+  DG_TRY(upload_vec(h->d_acc_pos, h->acc_pos));
+  h->device = dev;
+  return DG_OK;
+}
+
+template <class T>
+void gather_rows(std::vector<T>& out, const T* src, const std::vector<int64_t>& rows, int width) {
+  out.resize(rows.size() * width);
+  for (size_t i = 0; i < rows.size(); ++i)
+    for (int c = 0; c < width; ++c) out[i * width + c] = src[rows[i] * width + c];
+}
+
+}  // namespace
+
+extern "C" {
+
+dg_status dg_partition_weighted(int64_t n, const uint32_t* weights, int nranks, int64_t* first) {
+  DG_CHECK(n >= 0 && nranks >= 1 && first, DG_EINVAL, "partition_weighted: bad arguments");
+  partition_weighted(n, weights, nranks, first);
+  return DG_OK;
+}
+
+dg_status dg_halo_create(int64_t E, int64_t N, uint32_t max_depth, const uint32_t* nlist, const uint8_t* level,
+                         const uint8_t* cnum, const uint8_t* hmask, const uint32_t* node_xyz, const uint32_t* elem_xyz,
+                         const uint32_t* weights, int nranks, int rank, dg_halo** out) {
+  DG_CHECK(out && nlist && level && cnum && hmask && node_xyz && elem_xyz && E > 0 && N > 0, DG_EINVAL,
+           "halo_create: bad arguments");
+  DG_CHECK(nranks >= 1 && rank >= 0 && rank < nranks, DG_EINVAL, "halo_create: rank out of range");
+  DG_CHECK(N <= int64_t(UINT32_MAX), DG_EINVAL, "halo_create: too many nodes");
+  DG_CHECK(max_depth + 1 <= dg::kMaxEmbeddedDepth, DG_EDEPTH, "halo_create: maxDepth must be <= 18");
+  auto h = std::make_unique<dg_halo>();
+  const int P = nranks;
+  h->nranks = P;
+  h->rank = rank;
+  h->max_depth = max_depth;
+  h->elem_first.resize(P + 1);
+  partition_weighted(E, weights, P, h->elem_first.data());
+
+  // node ranges: the nodes whose anchors lie between the anchors of the first
+  // elements of consecutive non-empty ranks
+  std::vector<uint64_t> nk(N);
+  for (int64_t i = 0; i < N; ++i) nk[i] = dg::morton(node_xyz[3 * i], node_xyz[3 * i + 1], node_xyz[3 * i + 2]);
+  for (int64_t i = 1; i < N; ++i)
+    DG_CHECK(nk[i - 1] < nk[i], DG_EINVAL, "halo_create: node ids must follow the Morton order of their anchors");
+  auto& nf = h->node_first;
+  nf.assign(P + 1, 0);
+  nf[P] = N;
+  int first_nonempty = P;
+  for (int r = P - 1; r >= 0; --r) {
+    if (h->elem_first[r] == h->elem_first[r + 1]) {
+      nf[r] = nf[r + 1];
+      continue;
+    }
+    const int64_t e = h->elem_first[r];
+    const uint64_t key = dg::morton(elem_xyz[3 * e], elem_xyz[3 * e + 1], elem_xyz[3 * e + 2]);
+    nf[r] = std::min<int64_t>(std::lower_bound(nk.begin(), nk.end(), key) - nk.begin(), nf[r + 1]);
+    first_nonempty = r;
+  }
+  for (int r = 0; r <= first_nonempty && r <= P; ++r) nf[r] = 0;
+  std::vector<int32_t> owner(N);
+  for (int r = 0; r < P; ++r)
+    for (int64_t v = nf[r]; v < nf[r + 1]; ++v) owner[v] = r;
+
+  const int64_t n0 = nf[rank];
+  h->n_own = nf[rank + 1] - n0;
+  std::vector<int64_t>& ind = h->part[0].elems;
+  std::vector<int64_t>& dep = h->part[1].elems;
+  std::vector<uint32_t> ghost_refs;
+  std::vector<uint64_t> sends;  // peer << 32 | local id of an owned node
+  for (int64_t e = 0; e < E; ++e) {
+    const uint32_t* ids = nlist + 8 * e;
+    int ranks[8], nr = 0;
+    bool mine = false;
+    for (int k = 0; k < 8; ++k) {
+      DG_CHECK(ids[k] < uint64_t(N), DG_EINVAL, "halo_create: node id out of range");
+      const int q = owner[ids[k]];
+      mine |= q == rank;
+      bool seen = false;
+      for (int j = 0; j < nr; ++j) seen |= ranks[j] == q;
+      if (!seen) ranks[nr++] = q;
+    }
+    if (!mine) continue;
+    if (nr == 1) {
+      ind.push_back(e);
+      continue;
+    }
+    dep.push_back(e);
+    for (int k = 0; k < 8; ++k) {
+      if (owner[ids[k]] != rank) {
+        ghost_refs.push_back(ids[k]);
+        continue;
+      }
+      for (int j = 0; j < nr; ++j)
+        if (ranks[j] != rank) sends.push_back(uint64_t(ranks[j]) << 32 | uint64_t(ids[k] - n0));
+    }
+  }
+  std::sort(ghost_refs.begin(), ghost_refs.end());
+  ghost_refs.erase(std::unique(ghost_refs.begin(), ghost_refs.end()), ghost_refs.end());
+  h->ghosts = std::move(ghost_refs);
+  std::sort(sends.begin(), sends.end());
+  sends.erase(std::unique(sends.begin(), sends.end()), sends.end());
+  h->send_count.assign(P, 0);
+  h->recv_count.assign(P, 0);
+  h->send_idx.resize(sends.size());
+  for (size_t k = 0; k < sends.size(); ++k) {
+    ++h->send_count[sends[k] >> 32];
+    h->send_idx[k] = uint32_t(sends[k]);
+  }
+  for (uint32_t g : h->ghosts) ++h->recv_count[owner[g]];
+
+  // accumulation order: positions of send_idx by node, peers ascending within a node
+  {
+    std::vector<uint32_t> order(h->send_idx.size());
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return h->send_idx[a] < h->send_idx[b]; });
+    h->acc_pos = order;
+    h->acc_ptr.push_back(0);
+    for (size_t j = 0; j < order.size(); ++j) {
+      if (j == 0 || h->send_idx[order[j]] != h->send_idx[order[j - 1]]) {
+        if (j) h->acc_ptr.push_back(uint32_t(j));
+        h->acc_node.push_back(h->send_idx[order[j]]);
+      }
+    }
+    if (!order.empty()) h->acc_ptr.push_back(uint32_t(order.size()));
+  }
+
+  auto local_id = [&](uint32_t v) -> uint32_t {
+    if (owner[v] == rank) return uint32_t(v - n0);
+    return uint32_t(h->n_own + (std::lower_bound(h->ghosts.begin(), h->ghosts.end(), v) - h->ghosts.begin()));
+  };
+  auto global_id = [&](uint32_t l) -> uint32_t {
+    return l < h->n_own ? uint32_t(n0 + l) : h->ghosts[l - h->n_own];
+  };
+  for (int p = 0; p < 2; ++p) {
+    auto& pt = h->part[p];
+    gather_rows(pt.level, level, pt.elems, 1);
+    gather_rows(pt.cnum, cnum, pt.elems, 1);
+    gather_rows(pt.hmask, hmask, pt.elems, 1);
+    gather_rows(pt.exyz, elem_xyz, pt.elems, 3);
+    gather_rows(pt.nl, nlist, pt.elems, 8);
+    for (auto& v : pt.nl) v = local_id(v);
+  }
+  {
+    auto& pt = h->part[0];
+    pt.nxyz.assign(node_xyz + 3 * n0, node_xyz + 3 * (n0 + h->n_own));
+  }
+  {
+    auto& pt = h->part[1];
+    pt.nodes = pt.nl;
+    std::sort(pt.nodes.begin(), pt.nodes.end());
+    pt.nodes.erase(std::unique(pt.nodes.begin(), pt.nodes.end()), pt.nodes.end());
+    for (auto& v : pt.nl) v = uint32_t(std::lower_bound(pt.nodes.begin(), pt.nodes.end(), v) - pt.nodes.begin());
+    pt.nxyz.resize(3 * pt.nodes.size());
+    for (size_t i = 0; i < pt.nodes.size(); ++i) {
+      const uint32_t g = global_id(pt.nodes[i]);
+      for (int c = 0; c < 3; ++c) pt.nxyz[3 * i + c] = node_xyz[3 * int64_t(g) + c];
+    }
+  }
+  *out = h.release();
+  return DG_OK;
+}
+
+dg_status dg_halo_create_from_da(const dg_da* da, const uint32_t* weights, int nranks, int rank, dg_halo** out) {
+  DG_CHECK(da && out, DG_EINVAL, "halo_create_from_da: bad arguments");
+  const int64_t E = da->E, N = da->N;
+  std::vector<uint32_t> nl(8 * E), nxyz(3 * N), exyz(3 * E);
+  std::vector<uint8_t> hm(E), cn(E), lv(E);
+  DG_TRY(dg_da_export(da, nl.data(), hm.data(), cn.data(), nullptr, lv.data(), nxyz.data(), exyz.data(), nullptr));
+  return dg_halo_create(E, N, da->D - 1, nl.data(), lv.data(), cn.data(), hm.data(), nxyz.data(), exyz.data(), weights,
+                        nranks, rank, out);
+}
+
+dg_status dg_halo_sizes(const dg_halo* h, int64_t* n_owned, int64_t* n_ghost, int64_t* first_owned,
+                        int64_t* n_independent, int64_t* n_dependent, int64_t* n_dependent_nodes) {
+  DG_CHECK(h, DG_EINVAL, "halo_sizes: null halo");
+  if (n_owned) *n_owned = h->n_own;
+  if (n_ghost) *n_ghost = int64_t(h->ghosts.size());
+  if (first_owned) *first_owned = h->node_first[h->rank];
+  if (n_independent) *n_independent = int64_t(h->part[0].elems.size());
+  if (n_dependent) *n_dependent = int64_t(h->part[1].elems.size());
+  if (n_dependent_nodes) *n_dependent_nodes = int64_t(h->part[1].nodes.size());
+  return DG_OK;
+}
+
+dg_status dg_halo_ranges(const dg_halo* h, int64_t* elem_first, int64_t* node_first) {
+  DG_CHECK(h, DG_EINVAL, "halo_ranges: null halo");
+  if (elem_first) std::copy(h->elem_first.begin(), h->elem_first.end(), elem_first);
+  if (node_first) std::copy(h->node_first.begin(), h->node_first.end(), node_first);
+  return DG_OK;
+}
+
+dg_status dg_halo_comm(const dg_halo* h, int64_t* send_counts, int64_t* recv_counts, uint32_t* send_idx,
+                       uint32_t* ghosts) {
+  DG_CHECK(h, DG_EINVAL, "halo_comm: null halo");
+  if (send_counts) std::copy(h->send_count.begin(), h->send_count.end(), send_counts);
+  if (recv_counts) std::copy(h->recv_count.begin(), h->recv_count.end(), recv_counts);
+  if (send_idx) std::copy(h->send_idx.begin(), h->send_idx.end(), send_idx);
+  if (ghosts) std::copy(h->ghosts.begin(), h->ghosts.end(), ghosts);
+  return DG_OK;
+}
+
+dg_status dg_halo_part(const dg_halo* h, int which, int64_t* elems, uint32_t* nlist, uint32_t* nodes) {
+  DG_CHECK(h && (which == 0 || which == 1), DG_EINVAL, "halo_part: bad arguments");
+  const auto& pt = h->part[which];
+  if (elems) std::copy(pt.elems.begin(), pt.elems.end(), elems);
+  if (nlist) std::copy(pt.nl.begin(), pt.nl.end(), nlist);
+  if (nodes) std::copy(pt.nodes.begin(), pt.nodes.end(), nodes);
+  return DG_OK;
+}
+
+dg_status dg_halo_local_da(const dg_halo* h, int which, dg_da** out) {
+  DG_CHECK(h && out && (which == 0 || which == 1), DG_EINVAL, "halo_local_da: bad arguments");
+  const auto& pt = h->part[which];
+  DG_CHECK(!pt.elems.empty(), DG_EINVAL, "halo_local_da: the part has no elements");
+  const int64_t n = int64_t(pt.nxyz.size() / 3);
+  return dg_da_create_from_maps(int64_t(pt.elems.size()), n, h->max_depth, pt.nl.data(), pt.level.data(),
+                                pt.cnum.data(), pt.hmask.data(), pt.nxyz.data(), pt.exyz.data(), out);
+}
+
+dg_status dg_halo_pack(dg_halo* h, const double* x_local, double* send, int dof, void* stream) {
+  DG_CHECK(h && dof >= 1 && (h->send_idx.empty() || (x_local && send)), DG_EINVAL, "halo_pack: bad arguments");
+  DG_TRY(ensure_device(h));
+  const int64_t n = int64_t(h->send_idx.size());
+  if (n == 0) return DG_OK;
+  auto s = static_cast<cudaStream_t>(stream);
+  halo_gather<<<dg::grid_for(n * dof, kHaloThreads), kHaloThreads, 0, s>>>(h->d_send_idx.p, n, dof, x_local, send);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status dg_halo_accumulate(dg_halo* h, const double* recv, double* y_local, int dof, void* stream) {
+  DG_CHECK(h && dof >= 1 && (h->acc_node.empty() || (recv && y_local)), DG_EINVAL, "halo_accumulate: bad arguments");
+  DG_TRY(ensure_device(h));
+  const int64_t nu = int64_t(h->acc_node.size());
+  if (nu == 0) return DG_OK;
+  auto s = static_cast<cudaStream_t>(stream);
+  halo_accumulate<<<dg::grid_for(nu * dof, kHaloThreads), kHaloThreads, 0, s>>>(
+      h->d_acc_node.p, h->d_acc_ptr.p, h->d_acc_pos.p, nu, dof, recv, y_local);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status dg_halo_dep_gather(dg_halo* h, const double* x_local, double* x_dep, int dof, void* stream) {
+  DG_CHECK(h, DG_EINVAL, "halo_dep_gather: null halo");
+  const auto& nodes = h->part[1].nodes;
+  DG_CHECK(dof >= 1 && (nodes.empty() || (x_local && x_dep)), DG_EINVAL, "halo_dep_gather: bad arguments");
+  DG_TRY(ensure_device(h));
+  const int64_t n = int64_t(nodes.size());
+  if (n == 0) return DG_OK;
+  auto s = static_cast<cudaStream_t>(stream);
+  halo_gather<<<dg::grid_for(n * dof, kHaloThreads), kHaloThreads, 0, s>>>(h->d_dep_nodes.p, n, dof, x_local, x_dep);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status dg_halo_dep_scatter_add(dg_halo* h, const double* y_dep, double* y_local, int dof, void* stream) {
+  DG_CHECK(h, DG_EINVAL, "halo_dep_scatter_add: null halo");
+  const auto& nodes = h->part[1].nodes;
+  DG_CHECK(dof >= 1 && (nodes.empty() || (y_dep && y_local)), DG_EINVAL, "halo_dep_scatter_add: bad arguments");
+  DG_TRY(ensure_device(h));
+  const int64_t n = int64_t(nodes.size());
+  if (n == 0) return DG_OK;
+  auto s = static_cast<cudaStream_t>(stream);
+  halo_scatter_add<<<dg::grid_for(n * dof, kHaloThreads), kHaloThreads, 0, s>>>(h->d_dep_nodes.p, n, dof, h->n_own,
+                                                                               y_dep, y_local);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+void dg_halo_destroy(dg_halo* h) { delete h; }
+
+}  // extern "C"

@@ -45,6 +45,7 @@ typedef struct dg_da dg_da;         /* device-resident mesh (ot::DA)         */
 typedef struct dg_mat dg_mat;       /* operator on a mesh (PETSc MatShell)   */
 typedef struct dg_damg dg_damg;     /* multigrid hierarchy (ot::DAMG)        */
 typedef struct dg_mlp dg_mlp;       /* learned post-smoother (no reference counterpart) */
+typedef struct dg_halo dg_halo;     /* one rank's part of a partitioned mesh (ot::DA, npes > 1) */
 
 const char* dg_status_string(dg_status s);
 /* Copies the last error message of the calling thread into buf. */
@@ -280,6 +281,67 @@ void dg_damg_destroy(dg_damg* m);
  * takes residuals with on that level (MatMult of damg[l]->J). */
 dg_status dg_damg_level_apply(dg_damg* m, int level, const double* x, double* y, int on_device);
 dg_status dg_damg_vcycle(dg_damg* m, const double* b, double* x);
+
+/* ------------------------------------------------- partitioned meshes --- */
+
+/* par::partitionW (include/par/parUtils.txx:1011-1177) on a list held whole:
+ * n items with integer weights (NULL: 1 each) into nranks contiguous ranges
+ * of equal weight, the first W % nranks ranks one unit heavier; rank r gets
+ * items first[r] .. first[r+1] - 1 (first has nranks + 1 entries).  Host only. */
+dg_status dg_partition_weighted(int64_t n, const uint32_t* weights, int nranks, int64_t* first);
+
+/* One rank's part of a mesh split over nranks ranks: the DA that the
+ * reference builds per rank (ot::DA ctor, include/oda/oda.h:500-512, with
+ * the scatter maps of prepareAprioriCommMessagesInDAtype2,
+ * src/oda/private/odaFactory.C:199-460).  Elements are partitioned by
+ * dg_partition_weighted (weights per element, NULL: 1 each); a node belongs
+ * to the rank whose element range holds its anchor, so each rank owns a
+ * contiguous range of node ids.  The rank keeps every element with a vertex
+ * it owns: independent elements (all vertices owned) and dependent ones.
+ * Local node ids: owned nodes first, then ghost nodes ascending by global id
+ * (grouped by owner rank).  Inputs are the maps of dg_da_export (host
+ * arrays; node ids in the Morton order of their anchors).  Host only: no GPU
+ * is touched until the exchange calls below. */
+dg_status dg_halo_create(int64_t E, int64_t N, uint32_t max_depth, const uint32_t* nlist, const uint8_t* level,
+                         const uint8_t* cnum, const uint8_t* hmask, const uint32_t* node_xyz, const uint32_t* elem_xyz,
+                         const uint32_t* weights, int nranks, int rank, dg_halo** out);
+/* The same from a mesh on the GPU (exports its maps first). */
+dg_status dg_halo_create_from_da(const dg_da* da, const uint32_t* weights, int nranks, int rank, dg_halo** out);
+/* Sizes: owned and ghost nodes, the global id of the first owned node, the
+ * independent and dependent elements and the local nodes the dependent
+ * elements touch.  Any pointer may be NULL. */
+dg_status dg_halo_sizes(const dg_halo* h, int64_t* n_owned, int64_t* n_ghost, int64_t* first_owned,
+                        int64_t* n_independent, int64_t* n_dependent, int64_t* n_dependent_nodes);
+/* Element and node ranges of all ranks, [nranks + 1] each. */
+dg_status dg_halo_ranges(const dg_halo* h, int64_t* elem_first, int64_t* node_first);
+/* The exchange plan (m_uipSendProcs / m_uipSendCounts / m_uipScatterMap and
+ * m_uipRecvProcs / m_uipRecvCounts, include/oda/oda.h:426-438): values sent
+ * to and received from each rank [nranks]; the local ids of the owned nodes
+ * sent, by destination rank then ascending; the ghosts' global ids. */
+dg_status dg_halo_comm(const dg_halo* h, int64_t* send_counts, int64_t* recv_counts, uint32_t* send_idx,
+                       uint32_t* ghosts);
+/* A part's elements (which 0: independent, 1: dependent): global element ids
+ * [E_part], node ids [E_part][8] in the part's mesh (part 0: owned local ids;
+ * part 1: positions in its node list) and, for part 1, its node list (local
+ * ids, ascending). */
+dg_status dg_halo_part(const dg_halo* h, int which, int64_t* elems, uint32_t* nlist, uint32_t* nodes);
+/* The part's mesh on the current GPU (part 0 over the owned nodes, part 1
+ * over its node list); DG_EINVAL for a part without elements. */
+dg_status dg_halo_local_da(const dg_halo* h, int which, dg_da** out);
+/* ReadFromGhostsBegin's send buffer (include/oda/oda.txx:479-500):
+ * send[k] = x_local[send_idx[k]] for dof values per node; device pointers,
+ * asynchronous on `stream`.  The received values, concatenated by source
+ * rank, are x_local's ghost slots (x_local + dof * n_owned). */
+dg_status dg_halo_pack(dg_halo* h, const double* x_local, double* send, int dof, void* stream);
+/* WriteToGhostsEnd (include/oda/oda.txx:609-640): y_local[send_idx[k]] +=
+ * recv[k] for k in order, recv being the peers' ghost slots concatenated by
+ * source rank (what they send in WriteToGhostsBegin, oda.txx:566-605). */
+dg_status dg_halo_accumulate(dg_halo* h, const double* recv, double* y_local, int dof, void* stream);
+/* x_dep[i] = x_local[nodes[i]] over the dependent part's node list, and
+ * y_local[nodes[i]] += y_dep[i] for its owned nodes (ghost slots untouched). */
+dg_status dg_halo_dep_gather(dg_halo* h, const double* x_local, double* x_dep, int dof, void* stream);
+dg_status dg_halo_dep_scatter_add(dg_halo* h, const double* y_dep, double* y_local, int dof, void* stream);
+void dg_halo_destroy(dg_halo* h);
 
 /* ------------------------------------------------------- learned smoother --- */
 /* No reference counterpart (the reference smooths with damped Jacobi,

@@ -510,10 +510,13 @@ const Tables1& tables1() {
 // JAC_TYPE2_ELEM_MULT_BLOCK / JAC_TYPE2_MULT_BLOCK (examples/src/backend/
 // omgNeumann.C:468-530): y = sum_e (a_e h/2 L[c][t] + b_e h^3/8 M[c][t]) x_e,
 // h = 2^-(lev-1).  coef == nullptr means a = b = 1 (odaJac.C:271-288).
-void matvec(const Mesh& M, const double* coef, const double* x, double* y) {
+// matvec_elems adds the sum over the elements listed in `elems` (all of them
+// when elems is null) into y; matvec clears y first.
+void matvec_elems(const Mesh& M, const double* coef, const double* x, double* y, const int64_t* elems, int64_t ne) {
   const Tables& T = tables();
-  std::fill(y, y + M.N, 0.0);
-  for (size_t e = 0; e < M.E; ++e) {
+  const int64_t n = elems ? ne : int64_t(M.E);
+  for (int64_t i = 0; i < n; ++i) {
+    const size_t e = elems ? size_t(elems[i]) : size_t(i);
     double h = std::ldexp(1.0, 1 - int(M.elev[e]));
     double a = coef ? coef[2 * e] : 1.0, b = coef ? coef[2 * e + 1] : 1.0;
     double f1 = a * h / 2.0, f2 = b * h * h * h / 8.0;
@@ -523,6 +526,11 @@ void matvec(const Mesh& M, const double* coef, const double* x, double* y) {
       for (int j = 0; j < 8; ++j)
         y[idx[k]] += (f1 * T.L[c][t][k][j] + f2 * T.Ms[c][t][k][j]) * x[idx[j]];
   }
+}
+
+void matvec(const Mesh& M, const double* coef, const double* x, double* y) {
+  std::fill(y, y + M.N, 0.0);
+  matvec_elems(M, coef, x, y, nullptr, 0);
 }
 
 // JAC_TYPE2_ELEM_DIAG_BLOCK (omgNeumann.C:396-438).
@@ -941,6 +949,9 @@ void orc_mesh_export(void* m, uint32_t* nlist, uint8_t* hmask, uint8_t* cnum, ui
 
 void orc_matvec(void* m, const double* coef, const double* x, double* y) {
   matvec(*(Mesh*)m, coef, x, y);
+}
+void orc_matvec_elems(void* m, const double* coef, const double* x, double* y, const int64_t* elems, int64_t n) {
+  matvec_elems(*(Mesh*)m, coef, x, y, elems, n);
 }
 void orc_diagonal(void* m, const double* coef, double* d) { diagonal(*(Mesh*)m, coef, d); }
 void orc_elasticity_matvec(void* m, double mu, double lam, const uint8_t* bdy, const double* x, double* y) {

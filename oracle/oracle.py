@@ -48,6 +48,7 @@ def lib():
         L.orc_mesh_sizes.argtypes = [P, i64p, i64p, i64p]
         L.orc_mesh_export.argtypes = [P] * 9
         L.orc_matvec.argtypes = [P, P, P, P]
+        L.orc_matvec_elems.argtypes = [P, P, P, P, P, C.c_int64]
         L.orc_diagonal.argtypes = [P, P, P]
         L.orc_elasticity_matvec.argtypes = [P, C.c_double, C.c_double, P, P, P]
         L.orc_stencils.argtypes = [P, P, P]
@@ -150,6 +151,15 @@ class Mesh:
         y = np.empty(self.N, np.float64)
         c = None if coef is None else np.ascontiguousarray(coef, np.float64)
         lib().orc_matvec(self.h, _ptr(c), _ptr(x), _ptr(y))
+        return y
+
+    def matvec_elems(self, x, elems, coef=None):
+        """The matvec's sum over the listed elements only (global node ids)."""
+        x = np.ascontiguousarray(x, np.float64)
+        e = np.ascontiguousarray(elems, np.int64)
+        y = np.zeros(self.N, np.float64)
+        c = None if coef is None else np.ascontiguousarray(coef, np.float64)
+        lib().orc_matvec_elems(self.h, _ptr(c), _ptr(x), _ptr(y), _ptr(e), len(e))
         return y
 
     def diagonal(self, coef=None):
@@ -284,3 +294,31 @@ class DAMG:
         it = lib().orc_damg_pcg(self.h, _ptr(b), _ptr(x), rtol, maxit, _ptr(hist))
         n = abs(it)
         return x, it, hist[: n + 1]
+
+
+def partition_weighted(weights, nranks: int) -> np.ndarray:
+    """par::partitionW (include/par/parUtils.txx:1011-1177) for a list held by
+    one rank, as item ranges: rank r receives items first[r] .. first[r+1]-1.
+    The rule (parUtils.txx:1130-1150): with the inclusive weight scan s, the
+    total W, avgLoad = W // P and extra = W % P, an item goes to rank 0 when
+    s == 0, to (s - 1) // (avgLoad + 1) while s <= extra * (avgLoad + 1), else
+    to (s - 1 - extra) // avgLoad; with avgLoad == 0 all items go to rank 0
+    (parUtils.txx:1175-1176)."""
+    w = [int(v) for v in weights]
+    cnt = [0] * nranks
+    total = sum(w)
+    avg, extra = total // nranks, total % nranks
+    if avg == 0:
+        cnt[0] = len(w)
+    else:
+        s = 0
+        for v in w:
+            s += v
+            if s == 0:
+                r = 0
+            elif s <= extra * (avg + 1):
+                r = (s - 1) // (avg + 1)
+            else:
+                r = (s - 1 - extra) // avg
+            cnt[r] += 1
+    return np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)

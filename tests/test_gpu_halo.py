@@ -1,0 +1,103 @@
+"""Partitioned meshes on one GPU: every rank's part built in one process, the
+all-to-all between them done by the test from the product's pack kernel (no
+ranks wait on one another).  The owned rows of y = A x and of the diagonal
+against the oracle's whole-mesh results, the accumulation kernel against a
+sequential host sum, and the distributed operator and Jacobi CG on one rank."""
+import numpy as np
+import pytest
+
+from dendro_b200 import inputs as I
+from tests.cases import points
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def setup(gpu, oracle, name, P, weights=None):
+    from dendro_b200.halo import HaloDA
+    pts, d, m = points(name)
+    bal = oracle.balance(oracle.points2octree(pts, d, m), d)
+    da = gpu.DA(gpu.Octree.from_octants(bal, d))
+    ref = oracle.Mesh(bal, d)
+    H = [HaloDA(da, rank=r, nranks=P, weights=weights) for r in range(P)]
+    return da, ref, H
+
+
+def offsets(counts):
+    return np.concatenate([[0], np.cumsum(counts)])
+
+
+def emulate_read(H, xs):
+    """The all-to-all of read_from_ghosts, between the ranks' buffers."""
+    import torch
+    sends = [h.pack(x) for h, x in zip(H, xs)]
+    for r, h in enumerate(H):
+        parts = [sends[q][offsets(g.send_counts)[r]:offsets(g.send_counts)[r + 1]] for q, g in enumerate(H)]
+        xs[r][h.n_owned:] = torch.cat(parts)
+
+
+@pytest.mark.parametrize("name,P", [("gauss20k_d10", 2), ("lognormal20k_d12", 4), ("uniform8k_d9_m4", 3),
+                                    ("corner_points_d5", 5)])
+def test_partitioned_operator_matches_oracle(gpu, oracle, name, P):
+    import torch
+    from dendro_b200.halo import HaloJacobian2
+    da, ref, H = setup(gpu, oracle, name, P)
+    coef = I.sphere_coefficients(da.elementCenters())
+    x = I.uniform_rhs(ref.N, 21)
+    xs = [h.local_vector(x[h.first_owned:h.first_owned + h.n_owned]) for h in H]
+    emulate_read(H, xs)
+    for h, xl in zip(H, xs):
+        assert np.array_equal(xl.cpu().numpy(), x[h.local_to_global()])
+    ops = [HaloJacobian2(h, coef) for h in H]
+    y = np.concatenate([op.apply_local(xl)[:op.hda.n_owned].cpu().numpy() for op, xl in zip(ops, xs)])
+    assert rel(y, ref.matvec(x, coef)) < TOL
+    d = np.concatenate([op.getDiagonal().cpu().numpy() for op in ops])
+    assert rel(d, ref.diagonal(coef)) < TOL
+    # the whole-mesh operator on the GPU gives the same owned rows
+    yg = gpu.Jacobian2(da, coef).mult(torch.tensor(x, device="cuda")).cpu().numpy()
+    assert rel(y, yg) < TOL
+
+
+def test_accumulate_matches_sequential_sum(gpu, oracle):
+    """write_to_ghosts' accumulation: y[send_idx[k]] += recv[k] in order."""
+    import torch
+    _, _, H = setup(gpu, oracle, "lognormal20k_d12", 3)
+    rng = np.random.default_rng(5)
+    ys = [torch.tensor(rng.uniform(-1, 1, h.n_local), device="cuda") for h in H]
+    ghost = [y[h.n_owned:].clone() for h, y in zip(H, ys)]
+    for r, h in enumerate(H):
+        recv = torch.cat([ghost[q][offsets(g.recv_counts)[r]:offsets(g.recv_counts)[r + 1]]
+                          for q, g in enumerate(H)])
+        expect = ys[r].cpu().numpy().copy()
+        np.add.at(expect, h.send_idx.astype(np.int64), recv.cpu().numpy())
+        got = h.accumulate(recv, ys[r]).cpu().numpy()
+        assert np.array_equal(got, expect)
+
+
+def test_weighted_partition_and_one_rank_cg(gpu, oracle):
+    import torch
+    from dendro_b200.halo import HaloDA, HaloJacobian2, halo_cg
+    # element weights skew the ranges; the owned rows stay exact
+    pts, d, m = points("gauss20k_d10")
+    E = len(oracle.balance(oracle.points2octree(pts, d, m), d))
+    w = np.where(np.arange(E) < E // 4, 9, 1).astype(np.uint32)
+    da, ref, H = setup(gpu, oracle, "gauss20k_d10", 3, weights=w)
+    assert not np.array_equal(H[0].elem_first, HaloDA(da, rank=0, nranks=3).elem_first)
+    x = I.uniform_rhs(ref.N, 2)
+    xs = [h.local_vector(x[h.first_owned:h.first_owned + h.n_owned]) for h in H]
+    emulate_read(H, xs)
+    y = np.concatenate([HaloJacobian2(h).apply_local(xl)[:h.n_owned].cpu().numpy() for h, xl in zip(H, xs)])
+    assert rel(y, ref.matvec(x)) < TOL
+    # one rank: every element independent, mult without an exchange, CG to 1e-8
+    h1 = HaloDA(da, rank=0, nranks=1)
+    assert h1.n_ghost == 0 and len(h1.dependent) == 0 and len(h1.independent) == da.E
+    A = HaloJacobian2(h1)
+    b = I.uniform_rhs(ref.N, 3)
+    xs1, it, conv = halo_cg(A, torch.tensor(b, device="cuda"), rtol=1e-8, maxit=3000)
+    assert conv and it > 0
+    assert np.linalg.norm(ref.matvec(xs1.cpu().numpy()) - b) <= 1.01e-8 * np.linalg.norm(b)

@@ -397,8 +397,8 @@ def run_halo_profile(parts, workload):
     """The matvec workload's mesh split into `parts` parts by the weighted
     partition, every part on this GPU in turn: per part the launches one
     rank makes per operator application (pack of the values its peers read,
-    the independent elements, the dependent elements with their gather and
-    scatter) timed with CUDA events after a 256 MB L2 flush (median of 20),
+    the independent elements, the dependent elements added in place) timed
+    with CUDA events after a 256 MB L2 flush (median of 20),
     beside the whole mesh's operator.  The exchange itself needs several GPUs
     and is reported as bytes per rank."""
     import statistics

@@ -124,15 +124,14 @@ def lib():
         "dg_partition_weighted": ([I64, P, I, P], I),
         "dg_halo_create": ([I64, I64, U32, P, P, P, P, P, P, P, I, I, PP], I),
         "dg_halo_create_from_da": ([P, P, I, I, PP], I),
-        "dg_halo_sizes": ([P, I64P, I64P, I64P, I64P, I64P, I64P], I),
+        "dg_halo_sizes": ([P, I64P, I64P, I64P, I64P, I64P], I),
         "dg_halo_ranges": ([P, P, P], I),
         "dg_halo_comm": ([P, P, P, P, P], I),
-        "dg_halo_part": ([P, I, P, P, P], I),
+        "dg_halo_part": ([P, I, P, P], I),
         "dg_halo_local_da": ([P, I, PP], I),
         "dg_halo_pack": ([P, P, P, I, P], I),
         "dg_halo_accumulate": ([P, P, P, I, P], I),
-        "dg_halo_dep_gather": ([P, P, P, I, P], I),
-        "dg_halo_dep_scatter_add": ([P, P, P, I, P], I),
+        "dg_mat_mult_add": ([P, P, P, P], I),
         "dg_halo_destroy": ([P], None),
     }
     for name, (args, res) in sig.items():
@@ -164,7 +163,7 @@ def exported_symbols():
         "dg_mat_mult_multi", "dg_damg_set_tolerances",
         "dg_partition_weighted", "dg_halo_create", "dg_halo_create_from_da", "dg_halo_sizes", "dg_halo_ranges",
         "dg_halo_comm", "dg_halo_part", "dg_halo_local_da", "dg_halo_pack", "dg_halo_accumulate",
-        "dg_halo_dep_gather", "dg_halo_dep_scatter_add", "dg_halo_destroy",
+        "dg_halo_destroy", "dg_mat_mult_add",
     ]
 
 

@@ -214,6 +214,12 @@ class _Mat:
         check(lib().dg_mat_mult_host(self.h, ptr(xa), ptr(ya)), "mat_mult_host")
         return ya
 
+    def mult_add(self, x, y, stream=None):
+        """y += A x (FP64 device tensors, scalar operator)."""
+        s = None if stream is None else C.c_void_p(stream.cuda_stream)
+        check(lib().dg_mat_mult_add(self.h, ptr(x), ptr(y), s), "mat_mult_add")
+        return y
+
     def mult_multi(self, X, Y=None, split: int = 3, stream=None):
         """Y = A X for the columns of X, a CUDA float32 tensor [N, nrhs]
         (nrhs a multiple of 16), on the tensor cores (split 3: FP32-level

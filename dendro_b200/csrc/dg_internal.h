@@ -145,6 +145,7 @@ struct Type1Set {
 // zeroed, plus t1's children sums; coef == nullptr / t1 == nullptr: the
 // operator's own coefficients / no type-1 elements.
 dg_status lapmass_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
+dg_status lapmass_apply_add_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status lapmass_apply_j_f64(const dg_mat* A, const double* coef, const Type1Set* t1, const double* x, double* y,
                               cudaStream_t s);
 dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStream_t s);

@@ -18,8 +18,8 @@
 // first owned id), then its ghost nodes in ascending global id, which groups
 // them by owner in rank order, so an all-to-all of the owners' packed values
 // lands directly after the owned nodes.  The independent elements form one
-// local mesh over the owned nodes; the dependent elements another over the
-// compact list of the local nodes they touch.
+// local mesh over the owned nodes; the dependent elements another over all
+// local nodes, applied with y += A x into the local vector.
 //
 // The partition and the maps are host set-up and touch no GPU; the exchange
 // is a pack kernel, one all-to-all of the packed values and, for
@@ -41,19 +41,18 @@ struct dg_halo {
   std::vector<uint32_t> ghosts;                 // global ids, ascending
   std::vector<int64_t> send_count, recv_count;  // per peer
   std::vector<uint32_t> send_idx;               // local ids of owned nodes, by peer, then ascending
-  // 0: independent elements over the owned nodes; 1: dependent elements over `nodes`
+  // 0: independent elements over the owned nodes; 1: dependent elements over all local nodes
   struct Part {
     std::vector<int64_t> elems;  // global element ids, ascending
-    std::vector<uint32_t> nl;    // [E][8] node ids of the part's mesh
+    std::vector<uint32_t> nl;    // [E][8] local node ids
     std::vector<uint8_t> level, cnum, hmask;
     std::vector<uint32_t> exyz, nxyz;
-    std::vector<uint32_t> nodes;  // dependent part: local ids of its nodes, ascending
   } part[2];
   // accumulation to owners: the positions of send_idx grouped by node
   std::vector<uint32_t> acc_node, acc_ptr, acc_pos;
   // device copies, uploaded on the first exchange call
   int device = -1;
-  DBuf<uint32_t> d_send_idx, d_dep_nodes, d_acc_node, d_acc_ptr, d_acc_pos;
+  DBuf<uint32_t> d_send_idx, d_acc_node, d_acc_ptr, d_acc_pos;
 };
 
 namespace {
@@ -96,18 +95,6 @@ halo_gather(const uint32_t* __restrict__ idx, int64_t n, int dof, const double* 
   }
 }
 
-// y[idx[k]] += v[k] for idx[k] < limit (the indices are distinct)
-__global__ void __launch_bounds__(kHaloThreads)
-halo_scatter_add(const uint32_t* __restrict__ idx, int64_t n, int dof, int64_t limit, const double* __restrict__ v,
-                 double* __restrict__ y) {
-  const int64_t total = n * dof;
-  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t k = t / dof;
-    const int64_t i = idx[k];
-    if (i < limit) y[i * dof + (t - k * dof)] += v[t];
-  }
-}
-
 // y[node[u]] += each received value of node u in turn, in peer order (the
 // order of WriteToGhostsEnd's loop over the scatter map, oda.txx:628-633)
 __global__ void __launch_bounds__(kHaloThreads)
@@ -137,7 +124,6 @@ dg_status ensure_device(dg_halo* h) {
   if (h->device == dev) return DG_OK;
   DG_CHECK(h->device < 0, DG_EINVAL, "halo: used on a second device");
   DG_TRY(upload_vec(h->d_send_idx, h->send_idx));
-  DG_TRY(upload_vec(h->d_dep_nodes, h->part[1].nodes));
   DG_TRY(upload_vec(h->d_acc_node, h->acc_node));
   DG_TRY(upload_vec(h->d_acc_ptr, h->acc_ptr));
   DG_TRY(upload_vec(h->d_acc_pos, h->acc_pos));
@@ -271,9 +257,6 @@ dg_status dg_halo_create(int64_t E, int64_t N, uint32_t max_depth, const uint32_
     if (owner[v] == rank) return uint32_t(v - n0);
     return uint32_t(h->n_own + (std::lower_bound(h->ghosts.begin(), h->ghosts.end(), v) - h->ghosts.begin()));
   };
-  auto global_id = [&](uint32_t l) -> uint32_t {
-    return l < h->n_own ? uint32_t(n0 + l) : h->ghosts[l - h->n_own];
-  };
   for (int p = 0; p < 2; ++p) {
     auto& pt = h->part[p];
     gather_rows(pt.level, level, pt.elems, 1);
@@ -283,21 +266,12 @@ dg_status dg_halo_create(int64_t E, int64_t N, uint32_t max_depth, const uint32_
     gather_rows(pt.nl, nlist, pt.elems, 8);
     for (auto& v : pt.nl) v = local_id(v);
   }
+  h->part[0].nxyz.assign(node_xyz + 3 * n0, node_xyz + 3 * (n0 + h->n_own));
   {
-    auto& pt = h->part[0];
-    pt.nxyz.assign(node_xyz + 3 * n0, node_xyz + 3 * (n0 + h->n_own));
-  }
-  {
-    auto& pt = h->part[1];
-    pt.nodes = pt.nl;
-    std::sort(pt.nodes.begin(), pt.nodes.end());
-    pt.nodes.erase(std::unique(pt.nodes.begin(), pt.nodes.end()), pt.nodes.end());
-    for (auto& v : pt.nl) v = uint32_t(std::lower_bound(pt.nodes.begin(), pt.nodes.end(), v) - pt.nodes.begin());
-    pt.nxyz.resize(3 * pt.nodes.size());
-    for (size_t i = 0; i < pt.nodes.size(); ++i) {
-      const uint32_t g = global_id(pt.nodes[i]);
-      for (int c = 0; c < 3; ++c) pt.nxyz[3 * i + c] = node_xyz[3 * int64_t(g) + c];
-    }
+    auto& nx = h->part[1].nxyz;
+    nx = h->part[0].nxyz;
+    nx.reserve(3 * (h->n_own + h->ghosts.size()));
+    for (uint32_t g : h->ghosts) nx.insert(nx.end(), node_xyz + 3 * int64_t(g), node_xyz + 3 * int64_t(g) + 3);
   }
   *out = h.release();
   return DG_OK;
@@ -314,14 +288,13 @@ dg_status dg_halo_create_from_da(const dg_da* da, const uint32_t* weights, int n
 }
 
 dg_status dg_halo_sizes(const dg_halo* h, int64_t* n_owned, int64_t* n_ghost, int64_t* first_owned,
-                        int64_t* n_independent, int64_t* n_dependent, int64_t* n_dependent_nodes) {
+                        int64_t* n_independent, int64_t* n_dependent) {
   DG_CHECK(h, DG_EINVAL, "halo_sizes: null halo");
   if (n_owned) *n_owned = h->n_own;
   if (n_ghost) *n_ghost = int64_t(h->ghosts.size());
   if (first_owned) *first_owned = h->node_first[h->rank];
   if (n_independent) *n_independent = int64_t(h->part[0].elems.size());
   if (n_dependent) *n_dependent = int64_t(h->part[1].elems.size());
-  if (n_dependent_nodes) *n_dependent_nodes = int64_t(h->part[1].nodes.size());
   return DG_OK;
 }
 
@@ -342,12 +315,11 @@ dg_status dg_halo_comm(const dg_halo* h, int64_t* send_counts, int64_t* recv_cou
   return DG_OK;
 }
 
-dg_status dg_halo_part(const dg_halo* h, int which, int64_t* elems, uint32_t* nlist, uint32_t* nodes) {
+dg_status dg_halo_part(const dg_halo* h, int which, int64_t* elems, uint32_t* nlist) {
   DG_CHECK(h && (which == 0 || which == 1), DG_EINVAL, "halo_part: bad arguments");
   const auto& pt = h->part[which];
   if (elems) std::copy(pt.elems.begin(), pt.elems.end(), elems);
   if (nlist) std::copy(pt.nl.begin(), pt.nl.end(), nlist);
-  if (nodes) std::copy(pt.nodes.begin(), pt.nodes.end(), nodes);
   return DG_OK;
 }
 
@@ -379,33 +351,6 @@ dg_status dg_halo_accumulate(dg_halo* h, const double* recv, double* y_local, in
   auto s = static_cast<cudaStream_t>(stream);
   halo_accumulate<<<dg::grid_for(nu * dof, kHaloThreads), kHaloThreads, 0, s>>>(
       h->d_acc_node.p, h->d_acc_ptr.p, h->d_acc_pos.p, nu, dof, recv, y_local);
-  DG_CUDA(cudaGetLastError());
-  return DG_OK;
-}
-
-dg_status dg_halo_dep_gather(dg_halo* h, const double* x_local, double* x_dep, int dof, void* stream) {
-  DG_CHECK(h, DG_EINVAL, "halo_dep_gather: null halo");
-  const auto& nodes = h->part[1].nodes;
-  DG_CHECK(dof >= 1 && (nodes.empty() || (x_local && x_dep)), DG_EINVAL, "halo_dep_gather: bad arguments");
-  DG_TRY(ensure_device(h));
-  const int64_t n = int64_t(nodes.size());
-  if (n == 0) return DG_OK;
-  auto s = static_cast<cudaStream_t>(stream);
-  halo_gather<<<dg::grid_for(n * dof, kHaloThreads), kHaloThreads, 0, s>>>(h->d_dep_nodes.p, n, dof, x_local, x_dep);
-  DG_CUDA(cudaGetLastError());
-  return DG_OK;
-}
-
-dg_status dg_halo_dep_scatter_add(dg_halo* h, const double* y_dep, double* y_local, int dof, void* stream) {
-  DG_CHECK(h, DG_EINVAL, "halo_dep_scatter_add: null halo");
-  const auto& nodes = h->part[1].nodes;
-  DG_CHECK(dof >= 1 && (nodes.empty() || (y_dep && y_local)), DG_EINVAL, "halo_dep_scatter_add: bad arguments");
-  DG_TRY(ensure_device(h));
-  const int64_t n = int64_t(nodes.size());
-  if (n == 0) return DG_OK;
-  auto s = static_cast<cudaStream_t>(stream);
-  halo_scatter_add<<<dg::grid_for(n * dof, kHaloThreads), kHaloThreads, 0, s>>>(h->d_dep_nodes.p, n, dof, h->n_own,
-                                                                               y_dep, y_local);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }

@@ -1176,6 +1176,15 @@ dg_status lapmass_apply_f64(const dg_mat* A, const double* x, double* y, cudaStr
   return lapmass_launch<double, double>(da, da->tuned_f64, ca, cb, x, y, s);
 }
 
+// y += A x: the one-thread-per-element shape (launch shape 0), whose FP64
+// atomics add into y as it stands, so no clearing pass precedes it.
+dg_status lapmass_apply_add_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s) {
+  dg_da* da = A->da;
+  const double* ca = A->has_coef ? A->coef.p : nullptr;
+  const double* cb = A->has_coef ? A->coef.p + da->E : nullptr;
+  return launch_variant<double, double>(0, da, ca, cb, x, y, s);
+}
+
 dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStream_t s) {
   dg_da* da = A->da;
   const float* ca = A->has_coef ? A->coef32.p : nullptr;

@@ -13,7 +13,7 @@ torch.distributed (NCCL between GPUs, gloo on the host) per direction:
 ``HaloJacobian2.mult`` follows Jacobian2MatMult (examples/src/backend/
 omgNeumann.C:505-525): the exchange is started, the independent elements
 (all vertices owned) are applied while it is in flight, then the dependent
-ones.  Local vectors hold the owned nodes first, then the ghosts; after
+ones are added in place (one launch of y += A x over the local vector).  Local vectors hold the owned nodes first, then the ghosts; after
 ``mult`` the owned part of y is complete and its ghost slots are not defined.
 """
 from __future__ import annotations
@@ -68,9 +68,9 @@ class HaloDA:
                                                                               "node_xyz", "elem_xyz")],
                                        ptr(w), self.nranks, self.rank, C.byref(h)), "halo_create")
         self.h = h
-        v = [C.c_int64() for _ in range(6)]
+        v = [C.c_int64() for _ in range(5)]
         check(lib().dg_halo_sizes(self.h, *[C.byref(x) for x in v]), "halo_sizes")
-        (self.n_owned, self.n_ghost, self.first_owned, n_ind, n_dep, n_dep_nodes) = [x.value for x in v]
+        (self.n_owned, self.n_ghost, self.first_owned, n_ind, n_dep) = [x.value for x in v]
         self.n_local = self.n_owned + self.n_ghost
         P = self.nranks
         self.elem_first = np.empty(P + 1, np.int64)
@@ -84,12 +84,10 @@ class HaloDA:
         check(lib().dg_halo_comm(self.h, None, None, ptr(self.send_idx), ptr(self.ghosts)), "halo_comm")
         self.independent = np.empty(n_ind, np.int64)
         self.ind_nlist = np.empty((n_ind, 8), np.uint32)
-        check(lib().dg_halo_part(self.h, 0, ptr(self.independent), ptr(self.ind_nlist), None), "halo_part")
+        check(lib().dg_halo_part(self.h, 0, ptr(self.independent), ptr(self.ind_nlist)), "halo_part")
         self.dependent = np.empty(n_dep, np.int64)
         self.dep_nlist = np.empty((n_dep, 8), np.uint32)
-        self.dep_nodes = np.empty(n_dep_nodes, np.uint32)
-        check(lib().dg_halo_part(self.h, 1, ptr(self.dependent), ptr(self.dep_nlist), ptr(self.dep_nodes)),
-              "halo_part")
+        check(lib().dg_halo_part(self.h, 1, ptr(self.dependent), ptr(self.dep_nlist)), "halo_part")
         self.da_ind = self.da_dep = None
 
     def __del__(self):
@@ -146,19 +144,6 @@ class HaloDA:
         """WriteToGhostsEnd: add the peers' ghost contributions to the owned values."""
         check(lib().dg_halo_accumulate(self.h, ptr(recv), ptr(y_local), dof, self._stream(stream)),
               "halo_accumulate")
-        return y_local
-
-    def dep_gather(self, x_local, x_dep=None, dof: int = 1, stream=None):
-        import torch
-        if x_dep is None:
-            x_dep = torch.empty(len(self.dep_nodes) * dof, dtype=torch.float64, device=x_local.device)
-        check(lib().dg_halo_dep_gather(self.h, ptr(x_local), ptr(x_dep), dof, self._stream(stream)),
-              "halo_dep_gather")
-        return x_dep
-
-    def dep_scatter_add(self, y_dep, y_local, dof: int = 1, stream=None):
-        check(lib().dg_halo_dep_scatter_add(self.h, ptr(y_dep), ptr(y_local), dof, self._stream(stream)),
-              "halo_dep_scatter_add")
         return y_local
 
     # -------------------------------------------------------- exchanges ---
@@ -235,24 +220,20 @@ class HaloJacobian2:
 
     def _dependent(self, x_local, y_local):
         import torch
-        hda = self.hda
         if self.A_dep is not None:
-            stream = torch.cuda.current_stream()
-            x_dep = hda.dep_gather(x_local, stream=stream)
-            y_dep = self.A_dep.mult(x_dep, stream=stream)
-            hda.dep_scatter_add(y_dep, y_local, stream=stream)
+            self.A_dep.mult_add(x_local, y_local, stream=torch.cuda.current_stream())
         return y_local
 
     def getDiagonal(self):
         """Diagonal on the owned nodes [n_owned]."""
         import torch
         hda = self.hda
-        d = torch.zeros(hda.n_local, dtype=torch.float64, device="cuda")
+        d = torch.zeros(hda.n_owned, dtype=torch.float64, device="cuda")
         if self.A_ind is not None:
-            self.A_ind.getDiagonal(d[: hda.n_owned])
+            self.A_ind.getDiagonal(d)
         if self.A_dep is not None:
-            hda.dep_scatter_add(self.A_dep.getDiagonal(), d)
-        return d[: hda.n_owned]
+            d += self.A_dep.getDiagonal()[: hda.n_owned]
+        return d
 
 
 def halo_cg(A, b_owned, rtol: float = 1e-8, maxit: int = 1000, group=None):

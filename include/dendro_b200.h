@@ -176,6 +176,10 @@ dg_status dg_mat_create_elasticity(dg_da* da, double mu, double lambda, const ui
  * (assignBoundaryFlags, src/oda/odaUtils.C:1054). */
 dg_status dg_mat_create_dirichlet(dg_da* da, int with_mass, const uint8_t* dirichlet, dg_mat** out);
 dg_status dg_mat_mult(dg_mat* A, const double* x, double* y, void* stream);
+/* y += A x for the scalar operator (PETSc MatMultAdd with y as both the
+ * addend and the result), FP64, one launch and no clearing pass: the
+ * dependent elements of a partitioned mesh add into the local vector. */
+dg_status dg_mat_mult_add(dg_mat* A, const double* x, double* y, void* stream);
 /* FP32 inner-solver form of the same operator. */
 dg_status dg_mat_mult_f32(dg_mat* A, const float* x, float* y, void* stream);
 /* MATOP_GET_DIAGONAL (Jacobian2MatGetDiagonal, omgNeumann.C:442-465). */
@@ -309,9 +313,9 @@ dg_status dg_halo_create(int64_t E, int64_t N, uint32_t max_depth, const uint32_
 dg_status dg_halo_create_from_da(const dg_da* da, const uint32_t* weights, int nranks, int rank, dg_halo** out);
 /* Sizes: owned and ghost nodes, the global id of the first owned node, the
  * independent and dependent elements and the local nodes the dependent
- * elements touch.  Any pointer may be NULL. */
+ * Any pointer may be NULL. */
 dg_status dg_halo_sizes(const dg_halo* h, int64_t* n_owned, int64_t* n_ghost, int64_t* first_owned,
-                        int64_t* n_independent, int64_t* n_dependent, int64_t* n_dependent_nodes);
+                        int64_t* n_independent, int64_t* n_dependent);
 /* Element and node ranges of all ranks, [nranks + 1] each. */
 dg_status dg_halo_ranges(const dg_halo* h, int64_t* elem_first, int64_t* node_first);
 /* The exchange plan (m_uipSendProcs / m_uipSendCounts / m_uipScatterMap and
@@ -321,12 +325,11 @@ dg_status dg_halo_ranges(const dg_halo* h, int64_t* elem_first, int64_t* node_fi
 dg_status dg_halo_comm(const dg_halo* h, int64_t* send_counts, int64_t* recv_counts, uint32_t* send_idx,
                        uint32_t* ghosts);
 /* A part's elements (which 0: independent, 1: dependent): global element ids
- * [E_part], node ids [E_part][8] in the part's mesh (part 0: owned local ids;
- * part 1: positions in its node list) and, for part 1, its node list (local
- * ids, ascending). */
-dg_status dg_halo_part(const dg_halo* h, int which, int64_t* elems, uint32_t* nlist, uint32_t* nodes);
+ * [E_part] and their local node ids [E_part][8] (part 0: owned nodes only). */
+dg_status dg_halo_part(const dg_halo* h, int which, int64_t* elems, uint32_t* nlist);
 /* The part's mesh on the current GPU (part 0 over the owned nodes, part 1
- * over its node list); DG_EINVAL for a part without elements. */
+ * over all local nodes, so that dg_mat_mult_add adds its elements into a
+ * local vector in place); DG_EINVAL for a part without elements. */
 dg_status dg_halo_local_da(const dg_halo* h, int which, dg_da** out);
 /* ReadFromGhostsBegin's send buffer (include/oda/oda.txx:479-500):
  * send[k] = x_local[send_idx[k]] for dof values per node; device pointers,
@@ -337,10 +340,6 @@ dg_status dg_halo_pack(dg_halo* h, const double* x_local, double* send, int dof,
  * recv[k] for k in order, recv being the peers' ghost slots concatenated by
  * source rank (what they send in WriteToGhostsBegin, oda.txx:566-605). */
 dg_status dg_halo_accumulate(dg_halo* h, const double* recv, double* y_local, int dof, void* stream);
-/* x_dep[i] = x_local[nodes[i]] over the dependent part's node list, and
- * y_local[nodes[i]] += y_dep[i] for its owned nodes (ghost slots untouched). */
-dg_status dg_halo_dep_gather(dg_halo* h, const double* x_local, double* x_dep, int dof, void* stream);
-dg_status dg_halo_dep_scatter_add(dg_halo* h, const double* y_dep, double* y_local, int dof, void* stream);
 void dg_halo_destroy(dg_halo* h);
 
 /* ------------------------------------------------------- learned smoother --- */

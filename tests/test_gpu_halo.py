@@ -101,3 +101,22 @@ def test_weighted_partition_and_one_rank_cg(gpu, oracle):
     xs1, it, conv = halo_cg(A, torch.tensor(b, device="cuda"), rtol=1e-8, maxit=3000)
     assert conv and it > 0
     assert np.linalg.norm(ref.matvec(xs1.cpu().numpy()) - b) <= 1.01e-8 * np.linalg.norm(b)
+
+
+def test_mult_add(gpu, oracle):
+    """y += A x (the dependent elements' launch) against y + (A x)."""
+    import torch
+    pts, d, m = points("lognormal20k_d12")
+    bal = oracle.balance(oracle.points2octree(pts, d, m), d)
+    da = gpu.DA(gpu.Octree.from_octants(bal, d))
+    coef = I.sphere_coefficients(da.elementCenters())
+    A = gpu.Jacobian2(da, coef)
+    x = torch.tensor(I.uniform_rhs(da.N, 4), device="cuda")
+    y0 = torch.tensor(I.uniform_rhs(da.N, 5), device="cuda")
+    y = A.mult_add(x, y0.clone())
+    expect = y0.cpu().numpy() + oracle.Mesh(bal, d).matvec(x.cpu().numpy(), coef)
+    assert rel(y.cpu().numpy(), expect) < TOL
+    with pytest.raises(gpu.DendroError):
+        gpu.Elasticity(da, 0.4, 0.6).mult_add(torch.zeros(3 * da.N, dtype=torch.float64, device="cuda"),
+                                              torch.zeros(3 * da.N, dtype=torch.float64, device="cuda"))
+

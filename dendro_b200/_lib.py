@@ -132,6 +132,15 @@ def lib():
         "dg_halo_pack": ([P, P, P, I, P], I),
         "dg_halo_accumulate": ([P, P, P, I, P], I),
         "dg_mat_mult_add": ([P, P, P, P], I),
+        "dg_damg_transfer_export": ([P, I, I, I64P, P, P, P], I),
+        "dg_damg_level_coef": ([P, I, P], I),
+        "dg_damg_coarse_solve": ([P, P, P, P], I),
+        "dg_parcsr_create": ([I64, I64, P, P, P, P, P, I, I, PP], I),
+        "dg_parcsr_sizes": ([P, I64P, I64P, I64P, I64P], I),
+        "dg_parcsr_comm": ([P, P, P, P, P], I),
+        "dg_parcsr_pack": ([P, P, P, P], I),
+        "dg_parcsr_apply": ([P, P, P, P, I, P], I),
+        "dg_parcsr_destroy": ([P], None),
         "dg_halo_destroy": ([P], None),
     }
     for name, (args, res) in sig.items():
@@ -163,7 +172,9 @@ def exported_symbols():
         "dg_mat_mult_multi", "dg_damg_set_tolerances",
         "dg_partition_weighted", "dg_halo_create", "dg_halo_create_from_da", "dg_halo_sizes", "dg_halo_ranges",
         "dg_halo_comm", "dg_halo_part", "dg_halo_local_da", "dg_halo_pack", "dg_halo_accumulate",
-        "dg_halo_destroy", "dg_mat_mult_add",
+        "dg_halo_destroy", "dg_mat_mult_add", "dg_damg_transfer_export", "dg_damg_level_coef",
+        "dg_damg_coarse_solve", "dg_parcsr_create", "dg_parcsr_sizes", "dg_parcsr_comm", "dg_parcsr_pack",
+        "dg_parcsr_apply", "dg_parcsr_destroy",
     ]
 
 

@@ -55,6 +55,22 @@ struct dg_halo {
   DBuf<uint32_t> d_send_idx, d_acc_node, d_acc_ptr, d_acc_pos;
 };
 
+// Rows of a sparse matrix M (a transfer between two partitioned levels) that
+// one rank owns, with the columns it reads: owned columns first (global id
+// minus the first owned id), then ghost columns ascending by global id.
+struct dg_parcsr {
+  int nranks = 1, rank = 0;
+  int64_t row0 = 0, nrow = 0, col0 = 0, ncol_own = 0;
+  std::vector<uint32_t> ptr, col;
+  std::vector<double> val;
+  std::vector<uint32_t> ghosts;                 // global column ids, ascending
+  std::vector<int64_t> send_count, recv_count;  // per peer
+  std::vector<uint32_t> send_idx;               // owned columns the peers read, by peer, then ascending
+  int device = -1;
+  DBuf<uint32_t> d_ptr, d_col, d_send_idx;
+  DBuf<double> d_val;
+};
+
 namespace {
 
 constexpr int kHaloThreads = 256;
@@ -108,6 +124,22 @@ halo_accumulate(const uint32_t* __restrict__ node, const uint32_t* __restrict__ 
     double s = *out;
     for (uint32_t j = ptr[u]; j < ptr[u + 1]; ++j) s += recv[int64_t(pos[j]) * dof + c];
     *out = s;
+  }
+}
+
+// y[i] (+)= sum_k val[k] x[col[k]] over the rank's rows; a column below
+// nown reads the owned values, the rest the ghost values
+__global__ void __launch_bounds__(kHaloThreads)
+parcsr_spmv(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col, const double* __restrict__ val,
+            int64_t nrow, int64_t nown, const double* __restrict__ x_own, const double* __restrict__ x_ghost,
+            double* __restrict__ y, int add) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nrow; i += int64_t(gridDim.x) * blockDim.x) {
+    double s = add ? y[i] : 0.0;
+    for (uint32_t k = ptr[i]; k < ptr[i + 1]; ++k) {
+      const int64_t c = col[k];
+      s += val[k] * (c < nown ? x_own[c] : x_ghost[c - nown]);
+    }
+    y[i] = s;
   }
 }
 
@@ -356,5 +388,128 @@ dg_status dg_halo_accumulate(dg_halo* h, const double* recv, double* y_local, in
 }
 
 void dg_halo_destroy(dg_halo* h) { delete h; }
+
+dg_status dg_parcsr_create(int64_t nrows, int64_t ncols, const uint32_t* ptr, const uint32_t* col, const double* val,
+                           const int64_t* row_first, const int64_t* col_first, int nranks, int rank, dg_parcsr** out) {
+  DG_CHECK(out && ptr && row_first && col_first && nrows >= 0 && ncols >= 0, DG_EINVAL, "parcsr_create: bad arguments");
+  DG_CHECK(nranks >= 1 && rank >= 0 && rank < nranks, DG_EINVAL, "parcsr_create: rank out of range");
+  DG_CHECK(ncols <= int64_t(UINT32_MAX), DG_EINVAL, "parcsr_create: too many columns");
+  const int P = nranks;
+  DG_CHECK(row_first[0] == 0 && row_first[P] == nrows && col_first[0] == 0 && col_first[P] == ncols, DG_EINVAL,
+           "parcsr_create: ranges must cover the rows and the columns");
+  for (int r = 0; r < P; ++r)
+    DG_CHECK(row_first[r] <= row_first[r + 1] && col_first[r] <= col_first[r + 1], DG_EINVAL,
+             "parcsr_create: ranges must be ascending");
+  const int64_t nnz = ptr[nrows];
+  DG_CHECK(nnz == 0 || (col && val), DG_EINVAL, "parcsr_create: missing entries");
+  for (int64_t i = 0; i < nrows; ++i) DG_CHECK(ptr[i] <= ptr[i + 1], DG_EINVAL, "parcsr_create: bad row pointers");
+  for (int64_t k = 0; k < nnz; ++k) DG_CHECK(col[k] < uint64_t(ncols), DG_EINVAL, "parcsr_create: column out of range");
+  std::vector<int32_t> cown(ncols);
+  for (int r = 0; r < P; ++r)
+    for (int64_t c = col_first[r]; c < col_first[r + 1]; ++c) cown[c] = r;
+
+  auto pc = std::make_unique<dg_parcsr>();
+  pc->nranks = P;
+  pc->rank = rank;
+  pc->row0 = row_first[rank];
+  pc->nrow = row_first[rank + 1] - pc->row0;
+  pc->col0 = col_first[rank];
+  pc->ncol_own = col_first[rank + 1] - pc->col0;
+  std::vector<uint32_t> ghost_refs;
+  std::vector<uint64_t> sends;  // peer << 32 | local id of an owned column
+  for (int q = 0; q < P; ++q)
+    for (int64_t i = row_first[q]; i < row_first[q + 1]; ++i)
+      for (uint32_t k = ptr[i]; k < ptr[i + 1]; ++k) {
+        const int o = cown[col[k]];
+        if (q == rank && o != rank) ghost_refs.push_back(col[k]);
+        if (q != rank && o == rank) sends.push_back(uint64_t(q) << 32 | uint64_t(col[k] - pc->col0));
+      }
+  std::sort(ghost_refs.begin(), ghost_refs.end());
+  ghost_refs.erase(std::unique(ghost_refs.begin(), ghost_refs.end()), ghost_refs.end());
+  pc->ghosts = std::move(ghost_refs);
+  std::sort(sends.begin(), sends.end());
+  sends.erase(std::unique(sends.begin(), sends.end()), sends.end());
+  pc->send_count.assign(P, 0);
+  pc->recv_count.assign(P, 0);
+  pc->send_idx.resize(sends.size());
+  for (size_t k = 0; k < sends.size(); ++k) {
+    ++pc->send_count[sends[k] >> 32];
+    pc->send_idx[k] = uint32_t(sends[k]);
+  }
+  for (uint32_t g : pc->ghosts) ++pc->recv_count[cown[g]];
+  const uint32_t base = ptr[pc->row0];
+  pc->ptr.resize(pc->nrow + 1);
+  for (int64_t i = 0; i <= pc->nrow; ++i) pc->ptr[i] = ptr[pc->row0 + i] - base;
+  const int64_t lnnz = pc->ptr[pc->nrow];
+  pc->col.resize(lnnz);
+  pc->val.assign(val + base, val + base + lnnz);
+  for (int64_t k = 0; k < lnnz; ++k) {
+    const uint32_t c = col[base + k];
+    pc->col[k] = cown[c] == rank ? uint32_t(c - pc->col0)
+                                 : uint32_t(pc->ncol_own + (std::lower_bound(pc->ghosts.begin(), pc->ghosts.end(), c) -
+                                                            pc->ghosts.begin()));
+  }
+  *out = pc.release();
+  return DG_OK;
+}
+
+dg_status dg_parcsr_sizes(const dg_parcsr* pc, int64_t* n_rows, int64_t* n_cols_owned, int64_t* n_ghost,
+                          int64_t* nnz) {
+  DG_CHECK(pc, DG_EINVAL, "parcsr_sizes: null matrix");
+  if (n_rows) *n_rows = pc->nrow;
+  if (n_cols_owned) *n_cols_owned = pc->ncol_own;
+  if (n_ghost) *n_ghost = int64_t(pc->ghosts.size());
+  if (nnz) *nnz = int64_t(pc->col.size());
+  return DG_OK;
+}
+
+dg_status dg_parcsr_comm(const dg_parcsr* pc, int64_t* send_counts, int64_t* recv_counts, uint32_t* send_idx,
+                         uint32_t* ghosts) {
+  DG_CHECK(pc, DG_EINVAL, "parcsr_comm: null matrix");
+  if (send_counts) std::copy(pc->send_count.begin(), pc->send_count.end(), send_counts);
+  if (recv_counts) std::copy(pc->recv_count.begin(), pc->recv_count.end(), recv_counts);
+  if (send_idx) std::copy(pc->send_idx.begin(), pc->send_idx.end(), send_idx);
+  if (ghosts) std::copy(pc->ghosts.begin(), pc->ghosts.end(), ghosts);
+  return DG_OK;
+}
+
+static dg_status parcsr_device(dg_parcsr* pc) {
+  int dev = -1;
+  DG_CUDA(cudaGetDevice(&dev));
+  if (pc->device == dev) return DG_OK;
+  DG_CHECK(pc->device < 0, DG_EINVAL, "parcsr: used on a second device");
+  DG_TRY(upload_vec(pc->d_ptr, pc->ptr));
+  DG_TRY(upload_vec(pc->d_col, pc->col));
+  DG_TRY(upload_vec(pc->d_val, pc->val));
+  DG_TRY(upload_vec(pc->d_send_idx, pc->send_idx));
+  pc->device = dev;
+  return DG_OK;
+}
+
+dg_status dg_parcsr_pack(dg_parcsr* pc, const double* x_own, double* send, void* stream) {
+  DG_CHECK(pc && (pc->send_idx.empty() || (x_own && send)), DG_EINVAL, "parcsr_pack: bad arguments");
+  DG_TRY(parcsr_device(pc));
+  const int64_t n = int64_t(pc->send_idx.size());
+  if (n == 0) return DG_OK;
+  auto s = static_cast<cudaStream_t>(stream);
+  halo_gather<<<dg::grid_for(n, kHaloThreads), kHaloThreads, 0, s>>>(pc->d_send_idx.p, n, 1, x_own, send);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status dg_parcsr_apply(dg_parcsr* pc, const double* x_own, const double* x_ghost, double* y, int add,
+                          void* stream) {
+  DG_CHECK(pc && (pc->nrow == 0 || y) && (pc->ncol_own == 0 || x_own) && (pc->ghosts.empty() || x_ghost), DG_EINVAL,
+           "parcsr_apply: bad arguments");
+  DG_TRY(parcsr_device(pc));
+  if (pc->nrow == 0) return DG_OK;
+  auto s = static_cast<cudaStream_t>(stream);
+  parcsr_spmv<<<dg::grid_for(pc->nrow, kHaloThreads), kHaloThreads, 0, s>>>(
+      pc->d_ptr.p, pc->d_col.p, pc->d_val.p, pc->nrow, pc->ncol_own, x_own, x_ghost, y, add);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+void dg_parcsr_destroy(dg_parcsr* pc) { delete pc; }
 
 }  // extern "C"

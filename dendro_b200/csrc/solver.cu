@@ -1414,6 +1414,49 @@ dg_status dg_damg_level_apply(dg_damg* m, int level, const double* x, double* y,
   return DG_OK;
 }
 
+dg_status dg_damg_transfer_export(dg_damg* m, int level, int which, int64_t* nnz, uint32_t* ptr, uint32_t* col,
+                                  double* val) {
+  DG_CHECK(m && nnz && level >= 0 && size_t(level) + 1 < m->lv.size() && (which == 0 || which == 1), DG_EINVAL,
+           "damg_transfer_export: bad arguments");
+  const Level& L = m->lv[size_t(level)];
+  const int64_t rows = which == 0 ? L.da->N : m->lv[size_t(level) + 1].da->N;
+  const DBuf<uint32_t>& dp = which == 0 ? L.pptr : L.rptr;
+  const DBuf<uint32_t>& dc = which == 0 ? L.pcol : L.rcol;
+  const DBuf<double>& dv = which == 0 ? L.pval : L.rval;
+  uint32_t total = 0;
+  DG_CUDA(cudaMemcpy(&total, dp.p + rows, 4, cudaMemcpyDeviceToHost));
+  *nnz = total;
+  if (ptr) DG_CUDA(cudaMemcpy(ptr, dp.p, 4 * (rows + 1), cudaMemcpyDeviceToHost));
+  if (col) DG_CUDA(cudaMemcpy(col, dc.p, 4 * size_t(total), cudaMemcpyDeviceToHost));
+  if (val) DG_CUDA(cudaMemcpy(val, dv.p, 8 * size_t(total), cudaMemcpyDeviceToHost));
+  return DG_OK;
+}
+
+dg_status dg_damg_level_coef(dg_damg* m, int level, double* coef) {
+  DG_CHECK(m && coef && level >= 0 && size_t(level) < m->lv.size(), DG_EINVAL, "damg_level_coef: bad arguments");
+  const Level& L = m->lv[size_t(level)];
+  DG_CHECK(L.A && L.A->kind == 0, DG_EINVAL, "damg_level_coef: no Laplacian-mass operator set");
+  const int64_t E = L.da->E;
+  std::vector<double> soa(2 * E, 1.0);
+  if (L.A->has_coef) DG_CUDA(cudaMemcpy(soa.data(), L.A->coef.p, 16 * E, cudaMemcpyDeviceToHost));
+  for (int64_t e = 0; e < E; ++e) {
+    coef[2 * e] = soa[e];
+    coef[2 * e + 1] = soa[E + e];
+  }
+  return DG_OK;
+}
+
+dg_status dg_damg_coarse_solve(dg_damg* m, const double* b, double* x, void* stream) {
+  DG_CHECK(m && b && x && !m->lv.empty(), DG_EINVAL, "damg_coarse_solve: bad arguments");
+  DG_CHECK(m->lv.back().A, DG_EINVAL, "damg_coarse_solve: no operator set");
+  const int64_t n = m->lv.back().da->N;
+  auto s = static_cast<cudaStream_t>(stream);
+  dense_gemv<<<grid_for(n * 32, 256), 256, 0, s>>>(m->Ainv.p, n, m->d_crow_blk.p, m->d_cb_off.p, m->d_cb_n.p,
+                                                   m->d_cb_aoff.p, b, x);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
 dg_status dg_damg_vcycle(dg_damg* m, const double* b, double* x) {
   DG_CHECK(m && b && x, DG_EINVAL, "damg_vcycle: bad arguments");
   const int64_t n = m->lv[0].da->N;

@@ -46,6 +46,7 @@ typedef struct dg_mat dg_mat;       /* operator on a mesh (PETSc MatShell)   */
 typedef struct dg_damg dg_damg;     /* multigrid hierarchy (ot::DAMG)        */
 typedef struct dg_mlp dg_mlp;       /* learned post-smoother (no reference counterpart) */
 typedef struct dg_halo dg_halo;     /* one rank's part of a partitioned mesh (ot::DA, npes > 1) */
+typedef struct dg_parcsr dg_parcsr; /* one rank's rows of a sparse matrix between partitioned levels */
 
 const char* dg_status_string(dg_status s);
 /* Copies the last error message of the calling thread into buf. */
@@ -278,6 +279,19 @@ dg_da* dg_damg_level_da(dg_damg* m, int level); /* 0 = finest; owned by m */
 /* P (fine level l from level l+1) applied to host or device vectors. */
 dg_status dg_damg_prolong(dg_damg* m, int level, const double* xc, double* xf, int on_device);
 dg_status dg_damg_restrict(dg_damg* m, int level, const double* rf, double* rc, int on_device);
+/* The transfer matrices between level and level + 1 as CSR, copied to host
+ * memory: which 0 = P (rows: the nodes of level, columns: the nodes of
+ * level + 1; prolongMatVecType2, src/omg/ProlongMatVec.C:83-284), which 1 =
+ * R = P^T (rows: the nodes of level + 1).  *nnz receives the entry count;
+ * ptr [rows + 1], col and val [nnz] may be NULL (ask for nnz first). */
+dg_status dg_damg_transfer_export(dg_damg* m, int level, int which, int64_t* nnz, uint32_t* ptr, uint32_t* col,
+                                  double* val);
+/* The level's element coefficients (a, b per element, host [2 E_level]): the
+ * finest level's as set, the coarser ones averaged (omgNeumann.C:73-113). */
+dg_status dg_damg_level_coef(dg_damg* m, int level, double* coef);
+/* x = A_c^-1 b on the coarsest level (the dense inverse set up with the
+ * operators); device pointers [N_coarsest], asynchronous on `stream`. */
+dg_status dg_damg_coarse_solve(dg_damg* m, const double* b, double* x, void* stream);
 void dg_damg_destroy(dg_damg* m);
 
 /* PCApply of the multigrid preconditioner: one V-cycle on device vectors. */
@@ -341,6 +355,31 @@ dg_status dg_halo_pack(dg_halo* h, const double* x_local, double* send, int dof,
  * source rank (what they send in WriteToGhostsBegin, oda.txx:566-605). */
 dg_status dg_halo_accumulate(dg_halo* h, const double* recv, double* y_local, int dof, void* stream);
 void dg_halo_destroy(dg_halo* h);
+
+/* The rows of a sparse matrix that one rank owns, for products between two
+ * partitioned levels: the multigrid transfers of a partitioned hierarchy
+ * (prolongMatVecType2 / restrictMatVecType2, src/omg/ProlongMatVec.C:83-284,
+ * src/omg/RestrictMatVec.C:486-619, whose coarse values the reference reads
+ * with ReadFromGhosts and whose contributions it adds with WriteToGhosts).
+ * M is CSR on the host [nrows x ncols]; rank r owns rows row_first[r] ..
+ * row_first[r+1] - 1 and the input values of columns col_first[r] ..
+ * col_first[r+1] - 1 (both [nranks + 1]).  Host only until the calls below. */
+dg_status dg_parcsr_create(int64_t nrows, int64_t ncols, const uint32_t* ptr, const uint32_t* col, const double* val,
+                           const int64_t* row_first, const int64_t* col_first, int nranks, int rank, dg_parcsr** out);
+dg_status dg_parcsr_sizes(const dg_parcsr* pc, int64_t* n_rows, int64_t* n_cols_owned, int64_t* n_ghost,
+                          int64_t* nnz);
+/* The exchange plan: input values sent to / received from each rank, the
+ * owned columns sent (by destination rank, then ascending) and the ghost
+ * columns' global ids (ascending, so grouped by owner rank). */
+dg_status dg_parcsr_comm(const dg_parcsr* pc, int64_t* send_counts, int64_t* recv_counts, uint32_t* send_idx,
+                         uint32_t* ghosts);
+/* send[k] = x_own[send_idx[k]] (device pointers, asynchronous on `stream`). */
+dg_status dg_parcsr_pack(dg_parcsr* pc, const double* x_own, double* send, void* stream);
+/* y = M x (add = 0) or y += M x (add = 1) over the owned rows, x given as the
+ * owned input values and the received ghost values (device pointers). */
+dg_status dg_parcsr_apply(dg_parcsr* pc, const double* x_own, const double* x_ghost, double* y, int add,
+                          void* stream);
+void dg_parcsr_destroy(dg_parcsr* pc);
 
 /* ------------------------------------------------------- learned smoother --- */
 /* No reference counterpart (the reference smooths with damped Jacobi,

@@ -120,3 +120,77 @@ def test_mult_add(gpu, oracle):
         gpu.Elasticity(da, 0.4, 0.6).mult_add(torch.zeros(3 * da.N, dtype=torch.float64, device="cuda"),
                                               torch.zeros(3 * da.N, dtype=torch.float64, device="cuda"))
 
+
+
+def test_operator_and_cg_over_thread_ranks(gpu, oracle):
+    """mult with its exchange and Jacobi CG, the ranks run as threads on the
+    one GPU (exchanges and sums through the host)."""
+    import torch
+    from dendro_b200.halo import HaloDA, HaloJacobian2, halo_cg
+    from tests.threadcomm import ThreadComm, run_ranks
+    P = 3
+    pts, d, m = points("gauss20k_d10")
+    bal = oracle.balance(oracle.points2octree(pts, d, m), d)
+    da = gpu.DA(gpu.Octree.from_octants(bal, d))
+    ref = oracle.Mesh(bal, d)
+    coef = I.sphere_coefficients(da.elementCenters())
+    tc = ThreadComm(P)
+    H = [HaloDA(da, comm=tc.rank_comm(r)) for r in range(P)]
+    ops = [HaloJacobian2(h, coef) for h in H]
+    ops1 = [HaloJacobian2(h) for h in H]
+    x = I.uniform_rhs(ref.N, 31)
+    b = I.uniform_rhs(ref.N, 32)
+
+    def body(r):
+        h = H[r]
+        own = slice(h.first_owned, h.first_owned + h.n_owned)
+        y = ops[r].mult(h.local_vector(x[own]))[:h.n_owned].cpu().numpy()
+        y2 = ops[r].mult(h.local_vector(x[own]), overlap=False)[:h.n_owned].cpu().numpy()
+        xs, it, conv = halo_cg(ops1[r], torch.tensor(b[own], device="cuda"), rtol=1e-8, maxit=3000)
+        return y, y2, xs.cpu().numpy(), it, conv
+
+    res = run_ranks(P, body)
+    y_ref = ref.matvec(x, coef)
+    assert rel(np.concatenate([t[0] for t in res]), y_ref) < TOL
+    assert rel(np.concatenate([t[1] for t in res]), y_ref) < TOL
+    assert len({t[3] for t in res}) == 1 and all(t[4] for t in res)
+    xs = np.concatenate([t[2] for t in res])
+    assert np.linalg.norm(ref.matvec(xs) - b) <= 1.01e-8 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("name,P", [("gauss20k_d10", 2), ("lognormal20k_d12", 3)])
+def test_damg_over_thread_ranks(gpu, oracle, name, P):
+    """The partitioned V-cycle against the single-GPU V-cycle on the same
+    hierarchy, and the partitioned PCG's iterations and residual."""
+    import torch
+    from dendro_b200.halo import HaloDAMG
+    from dendro_b200.learned import vcycle
+    from tests.threadcomm import ThreadComm, run_ranks
+    pts, d, m = points(name)
+    bal = oracle.balance(oracle.points2octree(pts, d, m), d)
+    octree = gpu.Octree.from_octants(bal, d)
+    coef = I.sphere_coefficients(gpu.DA(octree).elementCenters())
+    single = gpu.DAMG(octree)
+    single.setKSP(coef)
+    b = I.uniform_rhs(int(single.N[0]), 41)
+    z_ref = vcycle(single, torch.tensor(b, device="cuda")).cpu().numpy()
+    _, rep = single.solve(b)
+    tc = ThreadComm(P)
+    M = [HaloDAMG(octree, coef, comm=tc.rank_comm(r)) for r in range(P)]
+    assert all(mm.nlevels == single.nlevels for mm in M)
+
+    def body(r):
+        own = slice(M[r].first_owned, M[r].first_owned + M[r].n_owned)
+        bo = torch.tensor(b[own], device="cuda")
+        z = M[r].vcycle(bo).cpu().numpy()
+        x, it, conv, rr = M[r].solve(bo, rtol=1e-8)
+        return z, x.cpu().numpy(), it, conv
+
+    res = run_ranks(P, body)
+    assert rel(np.concatenate([t[0] for t in res]), z_ref) < 1e-10
+    its = {t[2] for t in res}
+    assert len(its) == 1 and all(t[3] for t in res)
+    assert abs(its.pop() - rep["iterations"]) <= 1
+    x = np.concatenate([t[1] for t in res])
+    fine = oracle.Mesh(bal, d)
+    assert np.linalg.norm(fine.matvec(x, coef) - b) <= 1.01e-8 * np.linalg.norm(b)

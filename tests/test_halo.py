@@ -257,3 +257,38 @@ def test_jacobi_cg_over_gloo_ranks(oracle):
     assert np.linalg.norm(mesh.matvec(x) - b) <= 1.01e-8 * np.linalg.norm(b)
     _, it_ref = _jacobi_cg(mesh.matvec, mesh.diagonal(), b, 1e-8, 2000)
     assert abs(res[0][2] - it_ref) <= 1
+
+
+def test_parcsr_plan(oracle):
+    """The exchange plan of a row-partitioned sparse matrix: ghosts are the
+    columns a rank's rows read that it does not own, and what r sends to q is
+    what q receives from r, in q's ghost order."""
+    from dendro_b200.halo import ParCSR, partition_weighted
+    rng = np.random.default_rng(17)
+    nrows, ncols, P = 700, 400, 4
+    nnz_row = rng.integers(0, 9, nrows)
+    ptr_ = np.concatenate([[0], np.cumsum(nnz_row)]).astype(np.uint32)
+    col = np.concatenate([np.sort(rng.choice(ncols, k, replace=False)) for k in nnz_row]).astype(np.uint32)
+    val = rng.uniform(-1, 1, len(col))
+    rf, cf = partition_weighted(nrows, P), partition_weighted(ncols, P, rng.integers(1, 5, ncols))
+    mats = [ParCSR(ptr_, col, val, nrows, ncols, rf, cf, r, P) for r in range(P)]
+    owner = np.searchsorted(cf, np.arange(ncols), side="right") - 1
+    from dendro_b200._lib import lib, ptr
+    ghosts, sends = [], []
+    for r, pc in enumerate(mats):
+        assert pc.n_rows == rf[r + 1] - rf[r] and pc.n_cols_owned == cf[r + 1] - cf[r]
+        assert pc.nnz == ptr_[rf[r + 1]] - ptr_[rf[r]]
+        g = np.empty(pc.n_ghost, np.uint32)
+        s = np.empty(pc.n_send, np.uint32)
+        assert lib().dg_parcsr_comm(pc.h, None, None, ptr(s), ptr(g)) == 0
+        cols = col[ptr_[rf[r]]:ptr_[rf[r + 1]]]
+        assert np.array_equal(g, np.unique(cols[owner[cols] != r]))
+        assert np.array_equal(np.bincount(owner[g], minlength=P), pc.recv_counts)
+        ghosts.append(g)
+        sends.append(s)
+    for r, pc in enumerate(mats):
+        off = np.concatenate([[0], np.cumsum(pc.send_counts)])
+        for q, qc in enumerate(mats):
+            roff = np.concatenate([[0], np.cumsum(qc.recv_counts)])
+            assert np.array_equal(sends[r][off[q]:off[q + 1]].astype(np.int64) + cf[r],
+                                  ghosts[q][roff[r]:roff[r + 1]].astype(np.int64))

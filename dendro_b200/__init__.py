@@ -8,7 +8,9 @@ Host-side mirror of the reference's interfaces on this path:
 * ``Jacobian2`` / ``Elasticity`` operators (the MatShell callbacks of
   examples/src/backend/omgNeumann.C:533 and elasticityJac.C:212);
 * ``DAMG`` (``ot::DAMG``: DAMGCreateAndSetDA / DAMGSetKSP / DAMGSolve,
-  include/omg/omg.h:470-492).
+  include/omg/omg.h:470-492);
+* ``dendro_b200.halo``: one mesh and its hierarchy over several ranks
+  (``ot::DA`` / ``ot::DAMG`` with npes > 1).
 
 All work runs in libdendro_b200.so (CUDA, sm_100a); importing this package
 does not load it until first use, and every use fails loudly without it.

@@ -292,3 +292,41 @@ def test_parcsr_plan(oracle):
             roff = np.concatenate([[0], np.cumsum(qc.recv_counts)])
             assert np.array_equal(sends[r][off[q]:off[q + 1]].astype(np.int64) + cf[r],
                                   ghosts[q][roff[r]:roff[r + 1]].astype(np.int64))
+
+
+def _comm_worker(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        from dendro_b200.halo import TorchComm
+        c = TorchComm()
+        counts = [3, 0, 5][:world]
+        t = torch.arange(counts[rank], dtype=torch.float64) + 10 * rank
+        g = c.all_gather_v(t, counts)
+        s = c.all_reduce(torch.tensor([1.0 + rank], dtype=torch.float64))
+        out[rank] = (c.rank, c.size, g.tolist(), float(s.item()))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_torch_comm_over_gloo():
+    """The communicator's uneven gather and sum over gloo ranks."""
+    world = 3
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        procs = [ctx.Process(target=_comm_worker, args=(r, world, port, out)) for r in range(world)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(120)
+            assert p.exitcode == 0
+        res = dict(out)
+    for r in range(world):
+        assert res[r][:2] == (r, world)
+        assert res[r][2] == [0.0, 1.0, 2.0, 20.0, 21.0, 22.0, 23.0, 24.0]
+        assert res[r][3] == 6.0

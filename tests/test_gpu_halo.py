@@ -194,3 +194,43 @@ def test_damg_over_thread_ranks(gpu, oracle, name, P):
     x = np.concatenate([t[1] for t in res])
     fine = oracle.Mesh(bal, d)
     assert np.linalg.norm(fine.matvec(x, coef) - b) <= 1.01e-8 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("name,P", [("root", 2), ("corner_points_d5", 4)])
+def test_more_ranks_than_work(gpu, oracle, name, P):
+    """Ranks that own no nodes (the one-element mesh over 2 ranks; a
+    15-element mesh over 4, where one rank's elements anchor no node) still
+    take part in every exchange; the partitioned V-cycle and PCG match the
+    single-GPU ones."""
+    import torch
+    from dendro_b200.halo import HaloDAMG
+    from dendro_b200.learned import vcycle
+    from tests.threadcomm import ThreadComm, run_ranks
+    if name == "root":
+        d = 6
+        bal = oracle.points2octree(np.zeros((0, 3)), d, 1)
+    else:
+        pts, d, m = points(name)
+        bal = oracle.balance(oracle.points2octree(pts, d, m), d)
+    octree = gpu.Octree.from_octants(bal, d)
+    single = gpu.DAMG(octree)
+    single.setKSP()
+    b = I.uniform_rhs(int(single.N[0]), 51)
+    z_ref = vcycle(single, torch.tensor(b, device="cuda")).cpu().numpy()
+    tc = ThreadComm(P)
+    M = [HaloDAMG(octree, comm=tc.rank_comm(r)) for r in range(P)]
+    assert min(mm.n_owned for mm in M) == 0
+
+    def body(r):
+        own = slice(M[r].first_owned, M[r].first_owned + M[r].n_owned)
+        bo = torch.tensor(b[own], device="cuda")
+        z = M[r].vcycle(bo).cpu().numpy()
+        x, it, conv, _ = M[r].solve(bo, rtol=1e-8)
+        return z, x.cpu().numpy(), it, conv
+
+    res = run_ranks(P, body)
+    assert rel(np.concatenate([t[0] for t in res]), z_ref) < 1e-10
+    assert all(t[3] for t in res)
+    x = np.concatenate([t[1] for t in res])
+    fine = oracle.Mesh(bal, d)
+    assert np.linalg.norm(fine.matvec(x) - b) <= 1.01e-8 * np.linalg.norm(b)

@@ -58,6 +58,10 @@ struct dg_mlp {
   int step = 0;
 };
 
+namespace dg {
+struct HostPipe;  // streams, events and chunk plan of the pipelined host entry point (matvec.cu)
+}
+
 struct dg_mat {
   dg_da* da = nullptr;
   int kind = 0;  // 0 lap+mass, 1 elasticity, 2 Dirichlet Laplacian, 3 Dirichlet Jacobian
@@ -68,6 +72,7 @@ struct dg_mat {
   double mu = 0, lam = 0;
   dg::DBuf<uint8_t> dirichlet; // [N]
   dg::DBuf<double> host_x, host_y;  // device staging of dg_mat_mult_host, kept between calls
+  std::shared_ptr<dg::HostPipe> pipe;
 };
 
 namespace dg {
@@ -146,6 +151,9 @@ struct Type1Set {
 // operator's own coefficients / no type-1 elements.
 dg_status lapmass_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status lapmass_apply_add_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
+// y = A x for host x and y (staged in A->host_x / host_y) with the copies
+// pipelined against the operator; DG_ENOTIMPL when the mesh does not qualify
+dg_status lapmass_apply_host_pipelined_f64(dg_mat* A, const double* hx, double* hy);
 dg_status lapmass_apply_j_f64(const dg_mat* A, const double* coef, const Type1Set* t1, const double* x, double* y,
                               cudaStream_t s);
 dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStream_t s);

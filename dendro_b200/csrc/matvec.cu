@@ -16,10 +16,13 @@
 // eigenvectors (1,1) and (1,-1), so A = f1 K + f2 M = W diag(l) W / 8 with W
 // the 8-point Walsh-Hadamard transform and l depending only on the number of
 // (1,-1) factors; 56 flops per scalar element instead of 256.
+#include <algorithm>
 #include <cstddef>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <type_traits>
+#include <vector>
 
 #include "dg_internal.h"
 
@@ -1183,6 +1186,233 @@ dg_status lapmass_apply_add_f64(const dg_mat* A, const double* x, double* y, cud
   const double* ca = A->has_coef ? A->coef.p : nullptr;
   const double* cb = A->has_coef ? A->coef.p + da->E : nullptr;
   return launch_variant<double, double>(0, da, ca, cb, x, y, s);
+}
+
+// ---------------------------------------------------------------------------
+// Host entry point with the copies pipelined against the operator.  The warp
+// tiles are split into kPipeGroups consecutive groups.  x travels to the GPU
+// in node-order chunks on one stream -- the positive-boundary nodes first
+// (their anchors have a coordinate equal to the domain size, so their Morton
+// keys follow every other node's, yet tiles all along the curve read them) --
+// and each group's launch waits (stream event) for the chunk that completes
+// the nodes it reads.  After group g, the nodes below the smallest node any
+// later group touches are final and go back on a third stream while the
+// later groups run.  No kernel waits on a copy: the ordering is stream events.
+// For page-locked host buffers the whole pipeline is captured once into a CUDA
+// graph (per pair of buffers) and replayed, which removes the host cost of its
+// ~6 calls per group.
+struct HostPipe {
+  cudaStream_t sx = nullptr, sk = nullptr, sy = nullptr;
+  std::vector<cudaEvent_t> ex, ek;
+  cudaEvent_t efork = nullptr, ejx = nullptr, ejy = nullptr;
+  std::vector<int64_t> tile0;   // [G + 1] tile ranges of the groups
+  std::vector<int64_t> xend;    // [G] x [0, xend[g]) (and the tail) present before group g
+  std::vector<int64_t> yfinal;  // [G] y [0, yfinal[g]) final after group g
+  int64_t tail = 0;             // first positive-boundary node
+  int variant = -1;
+  cudaGraphExec_t exec = nullptr;  // captured pipeline for (gx, gy, gvariant)
+  const double* gx = nullptr;
+  double* gy = nullptr;
+  int gvariant = -1;
+  ~HostPipe() {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (auto e : ex) cudaEventDestroy(e);
+    for (auto e : ek) cudaEventDestroy(e);
+    if (efork) cudaEventDestroy(efork);
+    if (ejx) cudaEventDestroy(ejx);
+    if (ejy) cudaEventDestroy(ejy);
+    if (sx) cudaStreamDestroy(sx);
+    if (sk) cudaStreamDestroy(sk);
+    if (sy) cudaStreamDestroy(sy);
+  }
+};
+
+constexpr int kPipeGroups = 32;
+constexpr int64_t kPipeMinElements = int64_t(1) << 20;
+
+static dg_status build_host_pipe(const dg_da* da, HostPipe& P) {
+  const TileSet& ts = da->tiles_w;
+  const int64_t nt = ts.ntiles, N = da->N;
+  std::vector<uint32_t> tptr(nt + 1);
+  DG_CUDA(cudaMemcpy(tptr.data(), ts.ptr.p, 4 * (nt + 1), cudaMemcpyDeviceToHost));
+  std::vector<uint32_t> nodes(tptr[nt]);
+  DG_CUDA(cudaMemcpy(nodes.data(), ts.nodes.p, 4 * nodes.size(), cudaMemcpyDeviceToHost));
+  std::vector<uint64_t> nk(N);
+  DG_CUDA(cudaMemcpy(nk.data(), da->nkey.p, 8 * N, cudaMemcpyDeviceToHost));
+  const uint64_t tail_key = uint64_t(1) << (3 * (da->D - 1));
+  P.tail = std::lower_bound(nk.begin(), nk.end(), tail_key) - nk.begin();
+  const int G = kPipeGroups;
+  P.tile0.resize(G + 1);
+  for (int g = 0; g <= G; ++g) P.tile0[g] = nt * g / G;
+  std::vector<int64_t> lo(G, P.tail), hi(G, -1);
+  for (int g = 0; g < G; ++g)
+    for (uint32_t k = tptr[P.tile0[g]]; k < tptr[P.tile0[g + 1]]; ++k) {
+      const int64_t v = nodes[k] & 0x7fffffffu;
+      if (v >= P.tail) continue;
+      lo[g] = std::min(lo[g], v);
+      hi[g] = std::max(hi[g], v);
+    }
+  P.xend.resize(G);
+  int64_t run = 0;
+  for (int g = 0; g < G; ++g) {
+    run = std::max(run, hi[g] + 1);
+    P.xend[g] = g + 1 == G ? P.tail : std::min(run, P.tail);
+  }
+  P.yfinal.resize(G);
+  int64_t suffix = P.tail;
+  for (int g = G - 1; g >= 0; --g) {
+    P.yfinal[g] = suffix;
+    suffix = std::min(suffix, lo[g]);
+  }
+  for (int g = 1; g < G; ++g) P.yfinal[g] = std::max(P.yfinal[g], P.yfinal[g - 1]);
+  DG_CUDA(cudaStreamCreateWithFlags(&P.sx, cudaStreamNonBlocking));
+  DG_CUDA(cudaStreamCreateWithFlags(&P.sk, cudaStreamNonBlocking));
+  DG_CUDA(cudaStreamCreateWithFlags(&P.sy, cudaStreamNonBlocking));
+  P.ex.resize(G);
+  P.ek.resize(G);
+  for (int g = 0; g < G; ++g) {
+    DG_CUDA(cudaEventCreateWithFlags(&P.ex[g], cudaEventDisableTiming));
+    DG_CUDA(cudaEventCreateWithFlags(&P.ek[g], cudaEventDisableTiming));
+  }
+  DG_CUDA(cudaEventCreateWithFlags(&P.efork, cudaEventDisableTiming));
+  DG_CUDA(cudaEventCreateWithFlags(&P.ejx, cudaEventDisableTiming));
+  DG_CUDA(cudaEventCreateWithFlags(&P.ejy, cudaEventDisableTiming));
+  return DG_OK;
+}
+
+// One warp-tile launch over tiles [t0, t1): the per-element and per-tile
+// arrays are offset to the range; tile_ptr holds absolute offsets into the
+// node lists, so those stay whole.
+static dg_status launch_warp_range(int v, const dg_da* da, const double* ca, const double* cb, int64_t t0,
+                                   int64_t t1, const double* x, double* y, cudaStream_t s) {
+  const MatvecVariant& V = kVariants[v];
+  const TileSet& ts = da->tiles_w;
+  const int64_t e0 = t0 * kWarpTile;
+  const int64_t E = std::min<int64_t>(da->E, t1 * kWarpTile) - e0;
+  const int64_t nt = t1 - t0;
+  if (nt <= 0) return DG_OK;
+  const unsigned gw = grid_for(nt * 32, 32 * kWarpCta, V.per_sm);
+  const uint32_t* wm = ts.wmeta.p + e0;
+  const double* a = ca ? ca + e0 : nullptr;
+  const double* b = cb ? cb + e0 : nullptr;
+  const uint32_t* tp = ts.ptr.p + t0;
+  const uint2* e8 = reinterpret_cast<const uint2*>(ts.eloc8.p) + e0;
+  const uint8_t* r8 = ts.ref8.p + t0 * kWarpRefBytes;
+  if (V.kind == 4 && V.minb == 3)
+    lapmass_warp_pipe_kernel<double, double, 3><<<gw, 32 * kWarpCta, 0, s>>>(wm, a, b, E, nt, tp, ts.nodes.p, e8, r8,
+                                                                             x, y);
+  else if (V.kind == 4)
+    lapmass_warp_pipe_kernel<double, double, 4><<<gw, 32 * kWarpCta, 0, s>>>(wm, a, b, E, nt, tp, ts.nodes.p, e8, r8,
+                                                                             x, y);
+  else if (V.kind == 3)
+    lapmass_warp_kernel<double, double, 4, true><<<gw, 32 * kWarpCta, 0, s>>>(wm, a, b, E, nt, tp, ts.nodes.p, e8, r8,
+                                                                              x, y);
+  else if (V.minb == 6)
+    lapmass_warp_kernel<double, double, 6, false><<<gw, 32 * kWarpCta, 0, s>>>(wm, a, b, E, nt, tp, ts.nodes.p, e8,
+                                                                               r8, x, y);
+  else if (V.minb == 8)
+    lapmass_warp_kernel<double, double, 8, false><<<gw, 32 * kWarpCta, 0, s>>>(wm, a, b, E, nt, tp, ts.nodes.p, e8,
+                                                                               r8, x, y);
+  else
+    lapmass_warp_kernel<double, double, 5, false><<<gw, 32 * kWarpCta, 0, s>>>(wm, a, b, E, nt, tp, ts.nodes.p, e8,
+                                                                               r8, x, y);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+// The pipeline's copies and launches, enqueued on P's three streams (sk last
+// waits for sx and sy, so that sk alone marks the end).
+static dg_status enqueue_host_pipe(const dg_mat* A, HostPipe& P, const double* hx, double* hy) {
+  const dg_da* da = A->da;
+  const double* ca = A->has_coef ? A->coef.p : nullptr;
+  const double* cb = A->has_coef ? A->coef.p + da->E : nullptr;
+  double* dx = A->host_x.p;
+  double* dy = A->host_y.p;
+  const int64_t N = da->N;
+  const int G = kPipeGroups;
+  DG_CUDA(cudaEventRecord(P.efork, P.sk));
+  DG_CUDA(cudaStreamWaitEvent(P.sx, P.efork, 0));
+  DG_CUDA(cudaStreamWaitEvent(P.sy, P.efork, 0));
+  // x: the boundary tail, then the chunks in node order
+  if (P.tail < N) DG_CUDA(cudaMemcpyAsync(dx + P.tail, hx + P.tail, 8 * (N - P.tail), cudaMemcpyHostToDevice, P.sx));
+  int64_t xs = 0;
+  for (int g = 0; g < G; ++g) {
+    if (P.xend[g] > xs) {
+      DG_CUDA(cudaMemcpyAsync(dx + xs, hx + xs, 8 * (P.xend[g] - xs), cudaMemcpyHostToDevice, P.sx));
+      xs = P.xend[g];
+    }
+    DG_CUDA(cudaEventRecord(P.ex[g], P.sx));
+  }
+  DG_CUDA(cudaMemsetAsync(dy, 0, 8 * N, P.sk));
+  int64_t ys = 0;
+  for (int g = 0; g < G; ++g) {
+    DG_CUDA(cudaStreamWaitEvent(P.sk, P.ex[g], 0));
+    DG_TRY(launch_warp_range(P.variant, da, ca, cb, P.tile0[g], P.tile0[g + 1], dx, dy, P.sk));
+    DG_CUDA(cudaEventRecord(P.ek[g], P.sk));
+    DG_CUDA(cudaStreamWaitEvent(P.sy, P.ek[g], 0));
+    const int64_t ye = g + 1 == G ? N : P.yfinal[g];
+    if (ye > ys) {
+      DG_CUDA(cudaMemcpyAsync(hy + ys, dy + ys, 8 * (ye - ys), cudaMemcpyDeviceToHost, P.sy));
+      ys = ye;
+    }
+  }
+  DG_CUDA(cudaEventRecord(P.ejx, P.sx));
+  DG_CUDA(cudaEventRecord(P.ejy, P.sy));
+  DG_CUDA(cudaStreamWaitEvent(P.sk, P.ejx, 0));
+  DG_CUDA(cudaStreamWaitEvent(P.sk, P.ejy, 0));
+  return DG_OK;
+}
+
+static bool page_locked(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+dg_status lapmass_apply_host_pipelined_f64(dg_mat* A, const double* hx, double* hy) {
+  dg_da* da = A->da;
+  if (A->kind != 0 || da->E < kPipeMinElements || da->tiles_w.ntiles == 0 || da->tuned_f64 < 0) return DG_ENOTIMPL;
+  if (!A->pipe) {
+    auto P = std::make_shared<HostPipe>();
+    DG_TRY(build_host_pipe(da, *P));
+    A->pipe = P;
+  }
+  HostPipe& P = *A->pipe;
+  // the mesh's tuned shape when it is a plain warp-tile one, else the default
+  const int kind = kVariants[da->tuned_f64].kind;
+  P.variant = (kind >= 2 && kind <= 4) ? da->tuned_f64 : kDefaultVariant;
+  if (!(page_locked(hx) && page_locked(hy))) {
+    DG_TRY(enqueue_host_pipe(A, P, hx, hy));
+    DG_CUDA(cudaStreamSynchronize(P.sk));
+    return DG_OK;
+  }
+  if (!P.exec || P.gx != hx || P.gy != hy || P.gvariant != P.variant) {
+    if (P.exec) {
+      cudaGraphExecDestroy(P.exec);
+      P.exec = nullptr;
+    }
+    DG_CUDA(cudaStreamBeginCapture(P.sk, cudaStreamCaptureModeThreadLocal));
+    const dg_status st = enqueue_host_pipe(A, P, hx, hy);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(P.sk, &graph);
+    if (st != DG_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    DG_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&P.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    DG_CUDA(ie);
+    P.gx = hx;
+    P.gy = hy;
+    P.gvariant = P.variant;
+  }
+  DG_CUDA(cudaGraphLaunch(P.exec, P.sk));
+  DG_CUDA(cudaStreamSynchronize(P.sk));
+  return DG_OK;
 }
 
 dg_status lapmass_apply_f32(const dg_mat* A, const float* x, float* y, cudaStream_t s) {

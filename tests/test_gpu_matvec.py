@@ -115,3 +115,33 @@ def test_elasticity_diagonal_matches_unit_vectors(gpu, oracle):
     n = 3 * ref.N
     cols = np.array([ref.elasticity_matvec(np.eye(n)[j], mu, lam)[j] for j in range(n)])
     assert rel(d, cols) < TOL64
+
+
+def test_host_entry_point_pipelined(gpu, oracle):
+    """y = A x through the host entry point on a mesh of more than 2^20
+    elements (copies pipelined against launches over groups of tiles, replayed
+    from a CUDA graph for page-locked buffers) against the oracle: pageable and
+    page-locked buffers, new buffers (a new capture) and new values in the same
+    buffers (a replay)."""
+    import torch
+    pts = I.clamp_unit(I.lognormal_cloud(400000, 7), 12)
+    bal = gpu.balanceOctree(gpu.points2Octree(pts, 12, 1))
+    da = gpu.DA(bal)
+    assert da.E >= 1 << 20
+    coef = I.sphere_coefficients(da.elementCenters())
+    A = gpu.Jacobian2(da, coef)
+    ref = oracle.Mesh(bal.to_numpy(), 12)
+    for seed in (3, 4):
+        x = I.uniform_rhs(da.N, seed)
+        y_ref = ref.matvec(x, coef)
+        y_page = A.mult(x)                       # first call tunes, later calls pipeline
+        xp = torch.tensor(x).pin_memory()
+        yp = torch.empty(da.N, dtype=torch.float64).pin_memory()
+        A.mult(xp.numpy(), yp.numpy())
+        for y in (y_page, yp.numpy(), A.mult(x)):
+            assert np.linalg.norm(y - y_ref) / np.linalg.norm(y_ref) < 1e-12
+    x = I.uniform_rhs(da.N, 5)
+    xp.copy_(torch.from_numpy(x))
+    A.mult(xp.numpy(), yp.numpy())
+    y_ref = ref.matvec(x, coef)
+    assert np.linalg.norm(yp.numpy() - y_ref) / np.linalg.norm(y_ref) < 1e-12

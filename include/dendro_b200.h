@@ -186,7 +186,11 @@ dg_status dg_mat_mult_f32(dg_mat* A, const float* x, float* y, void* stream);
 /* MATOP_GET_DIAGONAL (Jacobian2MatGetDiagonal, omgNeumann.C:442-465). */
 dg_status dg_mat_get_diagonal(dg_mat* A, double* d, void* stream);
 /* Same as dg_mat_mult with host x and y: copies in, applies, copies out and
- * synchronises (the call a PETSc MatShell callback makes on host Vec arrays). */
+ * synchronises (the call a PETSc MatShell callback makes on host Vec arrays).
+ * On scalar meshes of more than 2^20 elements, after the first call, the
+ * copies run in chunks overlapped with the operator; with page-locked x and
+ * y the sequence is captured into a CUDA graph on first use of that pair of
+ * buffers and replayed on later calls. */
 dg_status dg_mat_mult_host(dg_mat* A, const double* x, double* y);
 /* Synchronise `stream`; DG_ETIMEOUT when a bounded device wait of an
  * operator kernel (the bulk-copy staged launch shape waits for its copies)

@@ -1198,9 +1198,9 @@ dg_status lapmass_apply_add_f64(const dg_mat* A, const double* x, double* y, cud
 // the nodes it reads.  After group g, the nodes below the smallest node any
 // later group touches are final and go back on a third stream while the
 // later groups run.  No kernel waits on a copy: the ordering is stream events.
-// For page-locked host buffers the whole pipeline is captured once into a CUDA
-// graph (per pair of buffers) and replayed, which removes the host cost of its
-// ~6 calls per group.
+// 16 groups measured fastest on the 4.7M-element benchmark mesh (8: 0.92-1.07,
+// 32: 0.97-0.99, 64: 1.08 ms per call); replaying the sequence from a CUDA
+// graph gave nothing measurable, so it is enqueued directly.
 struct HostPipe {
   cudaStream_t sx = nullptr, sk = nullptr, sy = nullptr;
   std::vector<cudaEvent_t> ex, ek;
@@ -1210,12 +1210,7 @@ struct HostPipe {
   std::vector<int64_t> yfinal;  // [G] y [0, yfinal[g]) final after group g
   int64_t tail = 0;             // first positive-boundary node
   int variant = -1;
-  cudaGraphExec_t exec = nullptr;  // captured pipeline for (gx, gy, gvariant)
-  const double* gx = nullptr;
-  double* gy = nullptr;
-  int gvariant = -1;
   ~HostPipe() {
-    if (exec) cudaGraphExecDestroy(exec);
     for (auto e : ex) cudaEventDestroy(e);
     for (auto e : ek) cudaEventDestroy(e);
     if (efork) cudaEventDestroy(efork);
@@ -1227,7 +1222,7 @@ struct HostPipe {
   }
 };
 
-constexpr int kPipeGroups = 32;
+constexpr int kPipeGroups = 16;
 constexpr int64_t kPipeMinElements = int64_t(1) << 20;
 
 static dg_status build_host_pipe(const dg_da* da, HostPipe& P) {
@@ -1363,15 +1358,6 @@ static dg_status enqueue_host_pipe(const dg_mat* A, HostPipe& P, const double* h
   return DG_OK;
 }
 
-static bool page_locked(const void* p) {
-  cudaPointerAttributes a{};
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeHost;
-}
-
 dg_status lapmass_apply_host_pipelined_f64(dg_mat* A, const double* hx, double* hy) {
   dg_da* da = A->da;
   if (A->kind != 0 || da->E < kPipeMinElements || da->tiles_w.ntiles == 0 || da->tuned_f64 < 0) return DG_ENOTIMPL;
@@ -1384,33 +1370,7 @@ dg_status lapmass_apply_host_pipelined_f64(dg_mat* A, const double* hx, double* 
   // the mesh's tuned shape when it is a plain warp-tile one, else the default
   const int kind = kVariants[da->tuned_f64].kind;
   P.variant = (kind >= 2 && kind <= 4) ? da->tuned_f64 : kDefaultVariant;
-  if (!(page_locked(hx) && page_locked(hy))) {
-    DG_TRY(enqueue_host_pipe(A, P, hx, hy));
-    DG_CUDA(cudaStreamSynchronize(P.sk));
-    return DG_OK;
-  }
-  if (!P.exec || P.gx != hx || P.gy != hy || P.gvariant != P.variant) {
-    if (P.exec) {
-      cudaGraphExecDestroy(P.exec);
-      P.exec = nullptr;
-    }
-    DG_CUDA(cudaStreamBeginCapture(P.sk, cudaStreamCaptureModeThreadLocal));
-    const dg_status st = enqueue_host_pipe(A, P, hx, hy);
-    cudaGraph_t graph = nullptr;
-    const cudaError_t ce = cudaStreamEndCapture(P.sk, &graph);
-    if (st != DG_OK) {
-      if (graph) cudaGraphDestroy(graph);
-      return st;
-    }
-    DG_CUDA(ce);
-    const cudaError_t ie = cudaGraphInstantiate(&P.exec, graph, 0);
-    cudaGraphDestroy(graph);
-    DG_CUDA(ie);
-    P.gx = hx;
-    P.gy = hy;
-    P.gvariant = P.variant;
-  }
-  DG_CUDA(cudaGraphLaunch(P.exec, P.sk));
+  DG_TRY(enqueue_host_pipe(A, P, hx, hy));
   DG_CUDA(cudaStreamSynchronize(P.sk));
   return DG_OK;
 }

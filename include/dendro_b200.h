@@ -188,9 +188,8 @@ dg_status dg_mat_get_diagonal(dg_mat* A, double* d, void* stream);
 /* Same as dg_mat_mult with host x and y: copies in, applies, copies out and
  * synchronises (the call a PETSc MatShell callback makes on host Vec arrays).
  * On scalar meshes of more than 2^20 elements, after the first call, the
- * copies run in chunks overlapped with the operator; with page-locked x and
- * y the sequence is captured into a CUDA graph on first use of that pair of
- * buffers and replayed on later calls. */
+ * copies run in chunks overlapped with the operator (page-locked x and y let
+ * the copies run asynchronously). */
 dg_status dg_mat_mult_host(dg_mat* A, const double* x, double* y);
 /* Synchronise `stream`; DG_ETIMEOUT when a bounded device wait of an
  * operator kernel (the bulk-copy staged launch shape waits for its copies)

@@ -119,10 +119,9 @@ def test_elasticity_diagonal_matches_unit_vectors(gpu, oracle):
 
 def test_host_entry_point_pipelined(gpu, oracle):
     """y = A x through the host entry point on a mesh of more than 2^20
-    elements (copies pipelined against launches over groups of tiles, replayed
-    from a CUDA graph for page-locked buffers) against the oracle: pageable and
-    page-locked buffers, new buffers (a new capture) and new values in the same
-    buffers (a replay)."""
+    elements (copies pipelined against launches over groups of tiles) against
+    the oracle: pageable and page-locked buffers, new buffers and new values
+    in the same buffers."""
     import torch
     pts = I.clamp_unit(I.lognormal_cloud(400000, 7), 12)
     bal = gpu.balanceOctree(gpu.points2Octree(pts, 12, 1))

@@ -146,10 +146,18 @@ def test_operator_and_cg_over_thread_ranks(gpu, oracle):
         own = slice(h.first_owned, h.first_owned + h.n_owned)
         y = ops[r].mult(h.local_vector(x[own]))[:h.n_owned].cpu().numpy()
         y2 = ops[r].mult(h.local_vector(x[own]), overlap=False)[:h.n_owned].cpu().numpy()
+        # WriteToGhosts: every ghost slot holds 1, the owners add what they receive
+        w = h.local_vector()
+        w[h.n_owned:] = 1.0
+        readers = h.write_to_ghosts(w)[:h.n_owned].cpu().numpy()
         xs, it, conv = halo_cg(ops1[r], torch.tensor(b[own], device="cuda"), rtol=1e-8, maxit=3000)
-        return y, y2, xs.cpu().numpy(), it, conv
+        return y, y2, xs.cpu().numpy(), it, conv, readers
 
     res = run_ranks(P, body)
+    holders = np.zeros(ref.N)
+    for h in H:
+        holders[h.ghosts.astype(np.int64)] += 1
+    assert np.array_equal(np.concatenate([t[5] for t in res]), holders) and holders.max() > 0
     y_ref = ref.matvec(x, coef)
     assert rel(np.concatenate([t[0] for t in res]), y_ref) < TOL
     assert rel(np.concatenate([t[1] for t in res]), y_ref) < TOL

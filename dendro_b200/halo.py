@@ -318,6 +318,8 @@ class ParCSR:
         ghost = torch.empty(self.n_ghost, dtype=torch.float64, device=dev)
         if self.comm is not None:
             self.comm.all_to_all_single(ghost, send, _splits(self.recv_counts), _splits(self.send_counts))
+        elif self.n_ghost or self.n_send:
+            raise RuntimeError("these rows read other ranks' values: a communicator is needed")
         if y is None:
             y = torch.empty(self.n_rows, dtype=torch.float64, device=dev)
         check(lib().dg_parcsr_apply(self.h, ptr(x_own), ptr(ghost), ptr(y), int(add), _stream()), "parcsr_apply")

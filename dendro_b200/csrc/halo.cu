@@ -143,6 +143,14 @@ parcsr_spmv(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col, 
   }
 }
 
+// x[i] += omega dinv[i] (b[i] - ax[i]): one damped Jacobi sweep's update
+__global__ void __launch_bounds__(kHaloThreads)
+jacobi_update(double* __restrict__ x, const double* __restrict__ b, const double* __restrict__ ax,
+              const double* __restrict__ dinv, double omega, int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    x[i] += omega * dinv[i] * (b[i] - ax[i]);
+}
+
 template <class T>
 dg_status upload_vec(DBuf<T>& d, const std::vector<T>& h) {
   DG_TRY(d.alloc(int64_t(h.size())));
@@ -511,5 +519,15 @@ dg_status dg_parcsr_apply(dg_parcsr* pc, const double* x_own, const double* x_gh
 }
 
 void dg_parcsr_destroy(dg_parcsr* pc) { delete pc; }
+
+dg_status dg_vec_jacobi_update(double* x, const double* b, const double* ax, const double* dinv, double omega,
+                               int64_t n, void* stream) {
+  DG_CHECK(n >= 0 && (n == 0 || (x && b && ax && dinv)), DG_EINVAL, "vec_jacobi_update: bad arguments");
+  if (n == 0) return DG_OK;
+  jacobi_update<<<dg::grid_for(n, kHaloThreads), kHaloThreads, 0, static_cast<cudaStream_t>(stream)>>>(x, b, ax, dinv,
+                                                                                                     omega, n);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
 
 }  // extern "C"

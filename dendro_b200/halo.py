@@ -388,8 +388,9 @@ class HaloDAMG:
 
     def _smooth(self, L, x_loc, b):
         n = L["hda"].n_owned
-        r = b - L["A"].mult(x_loc)[:n]
-        x_loc[:n].addcmul_(L["dinv"], r, value=self.omega)
+        ax = L["A"].mult(x_loc)
+        check(lib().dg_vec_jacobi_update(ptr(x_loc), ptr(b), ptr(ax), ptr(L["dinv"]), self.omega, n, _stream()),
+              "vec_jacobi_update")
 
     def vcycle(self, b, l: int = 0):
         """z = V(b) on level l from the owned values b [n_owned]."""

@@ -436,6 +436,13 @@ dg_status dg_vec_dot(const double* x, const double* y, int64_t n, double* result
  * other host threads) race on it and must be serialised by the caller. */
 dg_status dg_vec_dot_noalloc(const double* x, const double* y, int64_t n, double* result, void* stream);
 
+/* One damped Jacobi update, x[i] += omega dinv[i] (b[i] - ax[i]) (the
+ * V-cycle's smoother step, Richardson with Jacobi, bin/options:187-194), for
+ * callers that apply the operator themselves (the partitioned hierarchy);
+ * device pointers, asynchronous on `stream`. */
+dg_status dg_vec_jacobi_update(double* x, const double* b, const double* ax, const double* dinv, double omega,
+                               int64_t n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -330,3 +330,35 @@ def test_torch_comm_over_gloo():
         assert res[r][:2] == (r, world)
         assert res[r][2] == [0.0, 1.0, 2.0, 20.0, 21.0, 22.0, 23.0, 24.0]
         assert res[r][3] == 6.0
+
+
+def test_halo_and_parcsr_reject_bad_input(oracle):
+    """Bad ranks, node ids out of Morton order, ranges that do not cover the
+    rows, columns out of range: DG_EINVAL with no GPU touched."""
+    from dendro_b200._lib import DendroError
+    from dendro_b200.halo import HaloDA, ParCSR
+    mesh, maps, d = oracle_maps(oracle, "gauss2k_d8")
+    with pytest.raises(DendroError):
+        HaloDA(maps=maps, max_depth=d, rank=3, nranks=3)
+    with pytest.raises(DendroError):
+        HaloDA(maps=maps, max_depth=d, rank=-1, nranks=2)
+    bad = dict(maps)
+    bad["node_xyz"] = maps["node_xyz"][::-1].copy()          # anchors out of Morton order
+    with pytest.raises(DendroError):
+        HaloDA(maps=bad, max_depth=d, rank=0, nranks=2)
+    bad = dict(maps)
+    bad["nlist"] = maps["nlist"].copy()
+    bad["nlist"][5, 3] = mesh.N                              # node id out of range
+    with pytest.raises(DendroError):
+        HaloDA(maps=bad, max_depth=d, rank=0, nranks=2)
+    ptr_ = np.array([0, 2, 3], np.uint32)
+    col = np.array([0, 3, 1], np.uint32)
+    val = np.ones(3)
+    with pytest.raises(DendroError):                         # row ranges do not reach the last row
+        ParCSR(ptr_, col, val, 2, 4, [0, 1, 1], [0, 2, 4], 0, 2)
+    with pytest.raises(DendroError):                         # column 3 beyond 3 columns
+        ParCSR(ptr_, col, val, 2, 3, [0, 1, 2], [0, 2, 3], 0, 2)
+    with pytest.raises(DendroError):                         # descending column ranges
+        ParCSR(ptr_, col, val, 2, 4, [0, 1, 2], [0, 3, 2], 0, 2)
+    pc = ParCSR(ptr_, col, val, 2, 4, [0, 1, 2], [0, 2, 4], 1, 2)
+    assert (pc.n_rows, pc.n_cols_owned, pc.n_ghost, pc.nnz) == (1, 2, 1, 1)

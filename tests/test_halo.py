@@ -362,3 +362,20 @@ def test_halo_and_parcsr_reject_bad_input(oracle):
         ParCSR(ptr_, col, val, 2, 4, [0, 1, 2], [0, 3, 2], 0, 2)
     pc = ParCSR(ptr_, col, val, 2, 4, [0, 1, 2], [0, 2, 4], 1, 2)
     assert (pc.n_rows, pc.n_cols_owned, pc.n_ghost, pc.nnz) == (1, 2, 1, 1)
+
+
+def test_single_rank_defaults(oracle):
+    """Without a process group the communicator is one rank: every element is
+    independent, nothing is sent, and the collectives pass values through."""
+    import torch
+    from dendro_b200.halo import HaloDA, TorchComm
+    c = TorchComm()
+    assert (c.rank, c.size) == (0, 1)
+    t = torch.arange(4, dtype=torch.float64)
+    out = torch.empty(0, dtype=torch.float64)
+    assert c.all_to_all_single(out, torch.empty(0, dtype=torch.float64), [0], [0]) is None
+    assert torch.equal(c.all_reduce(t.clone()), t) and torch.equal(c.all_gather_v(t, [4]), t)
+    mesh, maps, d = oracle_maps(oracle, "gauss2k_d8")
+    h = HaloDA(maps=maps, max_depth=d)
+    assert (h.rank, h.nranks, h.n_ghost, len(h.dependent)) == (0, 1, 0, 0)
+    assert h.n_owned == mesh.N and len(h.independent) == mesh.E and len(h.send_idx) == 0

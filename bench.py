@@ -84,10 +84,10 @@ class ClockSampler:
     """nvidia-smi samples during the timed region."""
 
     def __init__(self, gpu_index: int):
+        import tempfile
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+        self.path = os.path.join(tempfile.mkdtemp(prefix="dg_clocks_"), f"clocks_gpu{gpu_index}.csv")
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(gpu_index),

@@ -534,6 +534,10 @@ constexpr long long kDefaultWaitLimit = 1ll << 31;  // clock64 cycles, about a s
 static long long g_wait_limit = kDefaultWaitLimit;
 
 __device__ int g_wait_status;  // DG_ETIMEOUT once a bounded wait has run out
+// Set when, after such a timeout, the bounded wait for the warp's copies
+// still in flight ran out as well: the warp returned with copies pending, so
+// they may have landed in shared memory that a later block already owned.
+__device__ int g_drain_gave_up;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -769,7 +773,10 @@ __global__ void __launch_bounds__(32 * kTmaWarps, MINB) lapmass_warp_tma_kernel(
       const long long drain = wait_limit > (1ll << 31) ? wait_limit : (1ll << 31);
       const long long t0 = clock64();
       while ((pend0 && !mbar_test(&W.bar[0], par0)) || (pend1 && !mbar_test(&W.bar[1], par1)))
-        if (clock64() - t0 > drain) break;
+        if (clock64() - t0 > drain) {
+          atomicExch(&g_drain_gave_up, 1);
+          break;
+        }
     }
     __syncwarp();
   }
@@ -1160,11 +1167,17 @@ void set_wait_limit(long long cycles) { g_wait_limit = cycles > 0 ? cycles : kDe
 
 dg_status device_wait_status(cudaStream_t s) {
   DG_CUDA(cudaStreamSynchronize(s));
-  int v = 0;
+  int v = 0, drained = 0;
   DG_CUDA(cudaMemcpyFromSymbol(&v, g_wait_status, sizeof(int)));
-  if (v) {
+  DG_CUDA(cudaMemcpyFromSymbol(&drained, g_drain_gave_up, sizeof(int)));
+  if (v || drained) {
     const int z = 0;
     DG_CUDA(cudaMemcpyToSymbol(g_wait_status, &z, sizeof(int)));
+    DG_CUDA(cudaMemcpyToSymbol(g_drain_gave_up, &z, sizeof(int)));
+    DG_CHECK(!drained, DG_ETIMEOUT,
+             "a bounded device wait of an operator kernel ran out and the copies it had in flight did not land "
+             "in time either: shared memory of later blocks may have been overwritten, so every result computed "
+             "since the last check is void");
     DG_CHECK(false, DG_ETIMEOUT, "a bounded device wait of an operator kernel ran out");
   }
   return DG_OK;
@@ -1358,9 +1371,23 @@ static dg_status enqueue_host_pipe(const dg_mat* A, HostPipe& P, const double* h
   return DG_OK;
 }
 
+// True when p is page-locked host memory (registered or allocated by CUDA):
+// only then do asynchronous copies from / to it overlap with kernels.
+static bool page_locked(const void* p) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
 dg_status lapmass_apply_host_pipelined_f64(dg_mat* A, const double* hx, double* hy) {
   dg_da* da = A->da;
   if (A->kind != 0 || da->E < kPipeMinElements || da->tiles_w.ntiles == 0 || da->tuned_f64 < 0) return DG_ENOTIMPL;
+  // pageable buffers: each chunk copy would block the host until its group
+  // has run, serialising the pipeline, so the caller copies, applies, copies
+  if (!page_locked(hx) || !page_locked(hy)) return DG_ENOTIMPL;
   if (!A->pipe) {
     auto P = std::make_shared<HostPipe>();
     DG_TRY(build_host_pipe(da, *P));

@@ -71,6 +71,10 @@ std::mutex g_noalloc_mu;
 double* g_noalloc_addr[kMaxDevices] = {nullptr};
 
 // Device address of g_noalloc_partials on the current device (looked up once).
+// The address belongs to the device's primary context at the time of the
+// lookup: cudaDeviceReset destroys that context and the module holding the
+// array, after which the cached address is stale, so a process that resets a
+// device must not call dg_vec_dot_noalloc on it again.
 dg_status noalloc_scratch(double** out) {
   int dev = 0;
   DG_CUDA(cudaGetDevice(&dev));

@@ -109,15 +109,24 @@ class HaloDA:
         self.comm = comm
         self.rank = comm.rank if rank is None else int(rank)
         self.nranks = comm.size if nranks is None else int(nranks)
-        w = None if weights is None else np.ascontiguousarray(weights, np.uint32)
+        w = None if weights is None else np.ascontiguousarray(weights, np.uint32).reshape(-1)
         h = C.c_void_p()
         if da is not None:
+            if w is not None and len(w) != da.E:
+                raise ValueError(f"weights has {len(w)} entries, the mesh has {da.E} elements")
             check(lib().dg_halo_create_from_da(da.h, ptr(w), self.nranks, self.rank, C.byref(h)), "halo_create")
         else:
             m = {k: np.ascontiguousarray(maps[k], dt) for k, dt in
                  (("nlist", np.uint32), ("level", np.uint8), ("cnum", np.uint8), ("hmask", np.uint8),
                   ("node_xyz", np.uint32), ("elem_xyz", np.uint32))}
             E, N = len(m["level"]), len(m["node_xyz"])
+            if m["nlist"].size != 8 * E or m["node_xyz"].size != 3 * N or m["elem_xyz"].size != 3 * E:
+                raise ValueError("maps: nlist must hold 8 ids per element, node_xyz and elem_xyz 3 coordinates "
+                                 "per node / element")
+            if len(m["cnum"]) != E or len(m["hmask"]) != E:
+                raise ValueError("maps: level, cnum and hmask must have one entry per element")
+            if w is not None and len(w) != E:
+                raise ValueError(f"weights has {len(w)} entries, the mesh has {E} elements")
             check(lib().dg_halo_create(E, N, max_depth, *[ptr(m[k]) for k in ("nlist", "level", "cnum", "hmask",
                                                                               "node_xyz", "elem_xyz")],
                                        ptr(w), self.nranks, self.rank, C.byref(h)), "halo_create")
@@ -292,6 +301,12 @@ class ParCSR:
         v = np.ascontiguousarray(val, np.float64)
         rf = np.ascontiguousarray(row_first, np.int64)
         cf = np.ascontiguousarray(col_first, np.int64)
+        if len(rf) != nranks + 1 or len(cf) != nranks + 1:
+            raise ValueError("row_first and col_first need nranks + 1 entries")
+        if len(p) != nrows + 1:
+            raise ValueError(f"ptr has {len(p)} entries, expected nrows + 1 = {nrows + 1}")
+        if nrows and (len(c) < int(p[-1]) or len(v) < int(p[-1])):
+            raise ValueError(f"col / val hold {len(c)} / {len(v)} entries, ptr[-1] = {int(p[-1])}")
         h = C.c_void_p()
         check(lib().dg_parcsr_create(nrows, ncols, ptr(p), ptr(c), ptr(v), ptr(rf), ptr(cf), nranks, rank,
                                      C.byref(h)), "parcsr_create")

@@ -188,13 +188,18 @@ dg_status dg_mat_get_diagonal(dg_mat* A, double* d, void* stream);
 /* Same as dg_mat_mult with host x and y: copies in, applies, copies out and
  * synchronises (the call a PETSc MatShell callback makes on host Vec arrays).
  * On scalar meshes of more than 2^20 elements, after the first call, the
- * copies run in chunks overlapped with the operator (page-locked x and y let
- * the copies run asynchronously). */
+ * copies run in chunks overlapped with the operator when x and y are both
+ * page-locked (cudaHostAlloc / cudaHostRegister); with pageable buffers the
+ * call copies x in, applies the operator and copies y out, one after another. */
 dg_status dg_mat_mult_host(dg_mat* A, const double* x, double* y);
 /* Synchronise `stream`; DG_ETIMEOUT when a bounded device wait of an
  * operator kernel (the bulk-copy staged launch shape waits for its copies)
  * has run out since the last check, which clears it.  The results of the
- * launches concerned are not valid.  dg_mat_mult_host and dg_damg_solve make
+ * launches concerned are not valid.  When, after such a timeout, the copies
+ * still in flight did not land within a second bounded wait either, the
+ * error message says so: a copy may then have written into shared memory
+ * that a later block of any kernel owned, and every result computed since the
+ * last check is void.  dg_mat_mult_host and dg_damg_solve make
  * the same check.  No reference counterpart: PETSc's MatMult reports errors
  * through its return code (Jacobian2MatMult, omgNeumann.C:533-556, returns 0). */
 dg_status dg_device_check(void* stream);
@@ -433,7 +438,10 @@ dg_status dg_vec_dot(const double* x, const double* y, int64_t n, double* result
  * device current), so make that first call before any stream capture.  The
  * result is written asynchronously on `stream` (no synchronisation).  All
  * calls share the one array: calls that overlap on the GPU (other streams,
- * other host threads) race on it and must be serialised by the caller. */
+ * other host threads) race on it and must be serialised by the caller.  The
+ * looked-up address belongs to the device's current context: after
+ * cudaDeviceReset on a device, do not call this function on that device
+ * again in the same process (the cached address would be stale). */
 dg_status dg_vec_dot_noalloc(const double* x, const double* y, int64_t n, double* result, void* stream);
 
 /* One damped Jacobi update, x[i] += omega dinv[i] (b[i] - ax[i]) (the

@@ -1,5 +1,6 @@
 """Compile the reference's own octree / mesh / operator / transfer sources
-(from /root/reference, read-only) into oracle/_ref/, single-rank, against
+(from the reference tree named by $DENDRO_REFERENCE, default /root/reference;
+read-only) into oracle/_ref/, single-rank, against
 the project-written MPI and PETSc stand-ins in oracle/ref_build/shim.
 
 The reference at its HEAD forces Hilbert ordering inside TreeNode::operator<
@@ -8,7 +9,7 @@ build therefore uses a copy of TreeNode.h / TreeNode.txx, generated into
 oracle/_ref/patched/ by this script, with those five lines removed so that
 the Morton comparator is used throughout.  A copy of include/hilbert/rotation.h
 gets one more byte in two sprintf buffers (the Hilbert tables that every
-TreeNode constructor reads overflow them by the terminator).  Nothing under /root/reference is
+TreeNode constructor reads overflow them by the terminator).  Nothing in the reference tree is
 modified and nothing it contains is committed.
 
 Outputs (git-ignored; they travel to the GPU box with the snapshot):
@@ -22,7 +23,7 @@ import shutil
 import subprocess
 import sys
 
-REF = "/root/reference"
+REF = os.environ.get("DENDRO_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(os.path.dirname(HERE), "_ref")
 
@@ -41,6 +42,20 @@ SOURCES = [
 INCLUDE_DIRS = ["include", "include/oct", "include/oda", "include/omg", "include/par", "include/seq",
                 "include/omp_par", "include/binOps", "include/point", "include/hilbert", "include/test",
                 "include/sys", "include/fem", "include/pc", "examples/include"]
+
+
+# Optimisation per source file.  With the mesh set-up built at -O2 or above
+# the reference crashes inside DA_blockPartStage2 (src/oda/odaPartition.C:302,
+# called from DA_FactoryPart3): odaFactory.C and odaPartition.C at -O1 are
+# enough for a DA built directly, omg.C at -O1 as well for the DAs that
+# DAMGCreateAndSetDA builds.  These are one-time set-up; everything else, the
+# operator, diagonal and transfer loops that the CPU baselines time included,
+# is built at -O3.
+LOW_OPT = {"src/oda/odaPartition.C", "src/oda/private/odaFactory.C", "src/omg/omg.C"}
+
+
+def opt_level(src):
+    return "-O1" if src in LOW_OPT else "-O3"
 
 
 def patched_headers():
@@ -74,7 +89,7 @@ def main():
     os.makedirs(os.path.join(OUT, "obj"), exist_ok=True)
     pdir = patched_headers()
     inc = ["-I" + os.path.join(HERE, "shim"), "-I" + pdir] + ["-I" + os.path.join(REF, d) for d in INCLUDE_DIRS]
-    flags = ["-O1", "-g", "-std=c++11", "-fopenmp", "-w", "-fpermissive", "-D__USE_PVT_DA_IN_MG__", "-D__SILENT_MODE__",
+    flags = ["-g", "-std=c++11", "-fopenmp", "-w", "-fpermissive", "-D__USE_PVT_DA_IN_MG__", "-D__SILENT_MODE__",
              "-include", os.path.join(pdir, "rotation.h"), "-include", os.path.join(pdir, "TreeNode.h")]
     objs, procs = [], []
     for src in SOURCES + [os.path.join(HERE, "ref_driver.cpp"), os.path.join(HERE, "dump_stubs.cpp"),
@@ -86,7 +101,8 @@ def main():
                                                              *[os.path.getmtime(os.path.join(HERE, "shim", f))
                                                                for f in os.listdir(os.path.join(HERE, "shim"))]):
             continue
-        procs.append((subprocess.Popen(["g++", *flags, *inc, "-c", path, "-o", obj], stdout=subprocess.PIPE,
+        procs.append((subprocess.Popen(["g++", opt_level(src), *flags, *inc, "-c", path, "-o", obj],
+                                       stdout=subprocess.PIPE,
                                        stderr=subprocess.STDOUT), src))
     bad = []
     for p, src in procs:

@@ -39,7 +39,7 @@ from oracle import oracle as O  # noqa: E402
 OUT = os.path.dirname(os.path.abspath(__file__))
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "dendro_ref")
 REF_CWD = os.path.join(ROOT, "oracle", "_ref", "stencils")
-STENCILS = "/root/reference/Stencils"
+STENCILS = os.path.join(os.environ.get("DENDRO_REFERENCE", "/root/reference"), "Stencils")
 
 MU, LAM = 1.0 / (2.0 * 1.3), 0.3 / (1.3 * 0.4)  # E = 1, nu = 0.3
 

@@ -362,6 +362,22 @@ def test_halo_and_parcsr_reject_bad_input(oracle):
         ParCSR(ptr_, col, val, 2, 4, [0, 1, 2], [0, 3, 2], 0, 2)
     pc = ParCSR(ptr_, col, val, 2, 4, [0, 1, 2], [0, 2, 4], 1, 2)
     assert (pc.n_rows, pc.n_cols_owned, pc.n_ghost, pc.nnz) == (1, 2, 1, 1)
+    # short host arrays are refused before the library reads them
+    for bad_args in ((ptr_[:2], col, val, 2, 4, [0, 1, 2], [0, 2, 4], 1, 2),   # ptr shorter than nrows + 1
+                     (ptr_, col[:2], val, 2, 4, [0, 1, 2], [0, 2, 4], 1, 2),   # col shorter than ptr[-1]
+                     (ptr_, col, val[:1], 2, 4, [0, 1, 2], [0, 2, 4], 1, 2),   # val shorter than ptr[-1]
+                     (ptr_, col, val, 2, 4, [0, 2], [0, 2, 4], 1, 2),          # row_first without nranks + 1
+                     (ptr_, col, val, 2, 4, [0, 1, 2], [0, 4], 1, 2)):         # col_first without nranks + 1
+        with pytest.raises(ValueError):
+            ParCSR(*bad_args)
+    E = len(maps["level"])
+    with pytest.raises(ValueError):                          # one weight short
+        HaloDA(maps=maps, max_depth=d, rank=0, nranks=2, weights=np.ones(E - 1, np.uint32))
+    for key in ("nlist", "cnum", "hmask", "elem_xyz"):
+        bad = dict(maps)
+        bad[key] = maps[key][:-1]                            # maps that disagree in length
+        with pytest.raises(ValueError):
+            HaloDA(maps=bad, max_depth=d, rank=0, nranks=2)
 
 
 def test_single_rank_defaults(oracle):

@@ -343,22 +343,31 @@ def run_multi(dev, steps, nrhs=64):
 
 
 def cpu_baseline(octs, depth, coef, x, seconds):
-    """Reference CPU matvec on the same mesh, timed on this host."""
+    """Reference-form CPU matvec (the oracle's restatement) on the same mesh,
+    timed on this host; also returns its y, the parity check of the GPU's."""
     from oracle import oracle as O
-    kind = "port"
-    ref_bin = os.path.join(ROOT, "oracle", "_ref", "dendro_ref_matvec")
     mesh = O.Mesh(octs, depth)
     t0 = time.perf_counter()
     n = 0
     while True:
-        mesh.matvec(x, coef)
+        y = mesh.matvec(x, coef)
         n += 1
         if time.perf_counter() - t0 >= seconds:
             break
     dt = time.perf_counter() - t0
-    del ref_bin
-    return {"value": mesh.N * n / dt / 1e9, "unit": "GDoF/s", "cores": 1, "kind": kind,
-            "sample": f"{n} full matvecs of the same mesh (E={mesh.E}, N={mesh.N}) in {dt:.1f} s, 1 thread"}
+    return {"value": mesh.N * n / dt / 1e9, "unit": "GDoF/s", "cores": 1, "kind": "port",
+            "sample": f"{n} full matvecs of the same mesh (E={mesh.E}, N={mesh.N}) in {dt:.1f} s, 1 thread"}, y
+
+
+def rel_err(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300))
+
+
+def reference_y_path(workload):
+    """Where the reference arm leaves one y of the compiled reference for the
+    GPU arm run after it on the same host (the two arms run back to back)."""
+    import tempfile
+    return os.path.join(tempfile.gettempdir(), f"dendro_b200_reference_y_{workload}.f64")
 
 
 def run_vcycle_profile(workload):
@@ -487,7 +496,16 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         octs = r["bal"].to_numpy()
-        line["cpu_baseline"] = cpu_baseline(octs, r["depth"], r["coef"], r["x"], args.cpu_seconds)
+        line["cpu_baseline"], y_port = cpu_baseline(octs, r["depth"], r["coef"], r["x"], args.cpu_seconds)
+        # results check on the benchmark mesh itself: the GPU's y against the
+        # oracle's and, when the reference arm ran before on this host, the
+        # compiled reference's Jacobian2MatMult on the same mesh and vector
+        parity = {"vs_oracle_rel_err": rel_err(r["y"], y_port), "tolerance": 1e-12}
+        yp = reference_y_path(args.workload)
+        if os.path.exists(yp) and os.path.getsize(yp) == 8 * r["N"]:
+            parity["vs_reference_rel_err"] = rel_err(r["y"], np.fromfile(yp))
+        parity["ok"] = all(v <= 1e-12 for k, v in parity.items() if k.endswith("rel_err"))
+        line["parity"] = parity
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -535,8 +553,8 @@ def main_reference(args, rank, world):
     reps = max(1, min(args.steps, 30))
     line = {"metric": METRIC, "unit": "GDoF/s", "n_gpus": world, "higher_is_better": True, "impl": "reference",
             "dtype": "f64", "data": "synthetic (seeded point cloud)", "warmup": 1,
-            "config": {"workload": args.workload, "elements": E, "nodes": N,
-                       "operator": "FP64 -div(a grad u)+u, a=1e4 in r<0.25"}}
+            "config": {"workload": args.workload, "points": int(1048576 * args.scale), "maxDepth": depth,
+                       "elements": E, "nodes": N, "operator": "FP64 -div(a grad u)+u, a=1e4 in r<0.25"}}
     if os.path.exists(REF_BIN):
         procs = ref_processes()
         tmp = tempfile.mkdtemp(prefix="dg_ref_")
@@ -549,12 +567,19 @@ def main_reference(args, rank, world):
                                  os.path.join(tmp, "x.f64"), os.path.join(tmp, "coef.f64"),
                                  os.path.join(tmp, f"y{p}.f64"), str(reps)], cwd=REF_STENCILS,
                                 stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True) for p in range(procs)]
-        per = []
-        for pr in run:
+        per, ok = [], []
+        for p, pr in enumerate(run):
             _, err = pr.communicate()
             if pr.returncode == 0:
                 per.append(float(err.strip().splitlines()[-1]))
+                ok.append(p)
         if per:
+            # one y of the reference: checked against the oracle here and kept
+            # for the GPU arm, which runs next on this host
+            y_ref = np.fromfile(os.path.join(tmp, f"y{ok[0]}.f64"))
+            y_port = O.Mesh(octs, depth).matvec(x, coef)
+            line["parity"] = {"oracle_vs_reference_rel_err": rel_err(y_port, y_ref), "tolerance": 1e-12}
+            y_ref.tofile(reference_y_path(args.workload))
             v = sum(N / t for t in per) / 1e9
             line.update({"value": round(v, 5), "steps": reps, "ms_per_step": round(1e3 * float(np.mean(per)), 3),
                          "cpu_baseline": {"value": round(v, 5), "unit": "GDoF/s", "cores": len(per),

@@ -34,7 +34,7 @@ class SolveReport(C.Structure):
 class DamgConfig(C.Structure):
     _fields_ = [("nlevels", C.c_int), ("nu_pre", C.c_int), ("nu_post", C.c_int), ("omega", C.c_double),
                 ("rtol", C.c_double), ("maxit", C.c_int), ("inner_prec", C.c_int), ("use_graph", C.c_int),
-                ("coarse_op", C.c_int)]
+                ("coarse_op", C.c_int), ("dof", C.c_int), ("mu", C.c_double), ("lambda_", C.c_double)]
 
 
 _lib = None

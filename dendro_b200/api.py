@@ -305,16 +305,22 @@ class DAMG:
 
     def __init__(self, finest, nlevels: int = 30, nu_pre: int = 2, nu_post: int = 2,
                  omega: float = 2.0 / 3.0, rtol: float = 1e-8, maxit: int = 200, inner_prec: int = 0,
-                 use_graph: bool = False, coarse_op: int = 0):
+                 use_graph: bool = False, coarse_op: int = 0, dof: int = 1, mu: float = 1.0, lam: float = 1.0):
         """`finest` is one balanced Octree, or a list of them for the batched
         form (independent meshes solved together, one launch per kernel).
         coarse_op 1: operators below the finest level from the next finer
-        level's coefficients (Jacobian3) instead of the level's averaged ones."""
+        level's coefficients (Jacobian3) instead of the level's averaged ones.
+        dof 3 (DAMGCreateAndSetDA's dof): linear elasticity with Lame
+        parameters mu, lam on every level, each level's boundary nodes
+        Dirichlet (examples/src/drivers/newElasSolver.C); vectors are
+        node-major [N][3]."""
         cfg = DamgConfig()
         lib().dg_damg_default_config(C.byref(cfg))
         cfg.nlevels, cfg.nu_pre, cfg.nu_post, cfg.omega = nlevels, nu_pre, nu_post, omega
         cfg.rtol, cfg.maxit, cfg.inner_prec, cfg.use_graph = rtol, maxit, inner_prec, int(use_graph)
         cfg.coarse_op = int(coarse_op)
+        cfg.dof, cfg.mu, cfg.lambda_ = int(dof), float(mu), float(lam)
+        self.dof = int(dof)
         h = C.c_void_p()
         if isinstance(finest, (list, tuple)):
             arr = (C.c_void_p * len(finest))(*[t.h.value for t in finest])
@@ -396,7 +402,7 @@ class DAMG:
 
     def restrict(self, level: int, rf: np.ndarray) -> np.ndarray:
         rf = np.ascontiguousarray(rf, np.float64)
-        rc = np.empty(int(self.N[level + 1]))
+        rc = np.empty(self.dof * int(self.N[level + 1]))
         check(lib().dg_damg_restrict(self.h, level, ptr(rf), ptr(rc), 0), "damg_restrict")
         return rc
 

@@ -30,6 +30,29 @@ struct TileSet {
   DBuf<uint32_t> shared;     // ascending ids of the nodes several tiles reference
   int64_t nshared = 0;
 };
+// Elements grouped by parent octant for the octet operator kernel (octet.cuh):
+// one entry per parent with at least one leaf child, in Morton order of the
+// parents.  Arrays are lattice-point / child major so that consecutive
+// octets are consecutive words.
+struct OctetSet {
+  int64_t n = 0;
+  DBuf<uint32_t> meta;  // [n] level of the children (embedded) | child mask << 8
+  DBuf<uint32_t> id;    // [27][n] node id of each lattice point, kNoNode when it hangs or no present child has it
+  DBuf<uint32_t> elem;  // [8][n] element id of each present child (kNoNode when absent)
+  // chunks of kOctChunk consecutive octets, staged through shared memory by
+  // the chunked kernel: per chunk the ascending ids of the nodes its octets
+  // touch (bit 31: another chunk touches the node too) and the range of
+  // element ids of its children; per octet the chunk-local index of each
+  // lattice node (0xffff: none) and of each present child's element.
+  int64_t nchunk = 0;
+  uint32_t max_nodes = 0, max_erange = 0;
+  DBuf<uint32_t> cptr;    // [nchunk + 1]
+  DBuf<uint32_t> cnodes;  // [cptr[nchunk]]
+  DBuf<uint32_t> cel;     // [2 nchunk]: first element id, element range length
+  DBuf<uint16_t> lidx;    // [27][n]
+  DBuf<uint16_t> lelem;   // [8][n]
+};
+constexpr int kOctChunk = 128;  // octets per chunk (one per thread of the chunked kernel)
 }  // namespace dg
 
 struct dg_octree {
@@ -49,6 +72,7 @@ struct dg_da {
   // operator's (kWarpTile elements per tile, built with the mesh) and the
   // multi-right-hand-side one's (kMultiTile elements per tile, built on first use)
   dg::TileSet tiles_w, tiles_mr;
+  dg::OctetSet octs;  // elements grouped by parent (octet operator kernel)
   // operator launch shape picked by the autotuner on first use (-1: not yet)
   int tuned_f64 = -1, tuned_f32 = -1;
 };
@@ -130,6 +154,7 @@ dg_status build_mesh(const dg_octree* tree, dg_da* da, cudaStream_t s);
 void set_wait_limit(long long cycles);
 dg_status device_wait_status(cudaStream_t s);
 dg_status build_tiles(dg_da* da, cudaStream_t s);  // da->tiles_w (kWarpTile)
+dg_status build_octets(dg_da* da, cudaStream_t s);  // da->octs (octet.cu)
 dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s);
 // Hanging mask of element type t (0..17) for child number c
 // (include/oda/cnumEtypes.h:19-229).
@@ -180,6 +205,9 @@ int matvec_variant_count();
 dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int nrhs, int split, cudaStream_t s);
 dg_status elasticity_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status elasticity_diag(const dg_mat* A, double* d, cudaStream_t s);
+// Dense row-major (3 N) x (3 N) matrix of the elasticity operator, Dirichlet
+// rows the identity (the coarsest level of the dof-3 multigrid).
+dg_status elasticity_assemble_dense(const dg_mat* A, double* dense, cudaStream_t s);
 // Dirichlet Laplacian (kind 2) / Jacobian (kind 3) on A->dirichlet node flags.
 dg_status dirichlet_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status dirichlet_diag(const dg_mat* A, double* d, cudaStream_t s);

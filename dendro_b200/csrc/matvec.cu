@@ -21,10 +21,12 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
 #include "dg_internal.h"
+#include "octet.cuh"
 
 namespace dg {
 
@@ -506,6 +508,180 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_pipe_kernel(
     }
     __syncwarp();
     if (has_next) cur = nxt;
+  }
+}
+
+// ------------------------------------------------------------ octet form --
+// The arithmetic of one octet (octet.cuh) on its 27 lattice values xv: the
+// points flagged in `none` (no node: hanging, or not a vertex of a present
+// child) are filled from their corners; every present child's element
+// operator is applied with compile-time lattice indices; the sums of the
+// hanging points are folded back onto their corners (T^T).  yv receives the
+// 27 lattice sums (meaningful at the points with a node).  coef(c, f1, f2)
+// scales child c's two factors by its coefficients.
+template <class T, class Coef>
+__device__ __forceinline__ void octet_apply(T (&xv)[27], T (&yv)[27], uint32_t none, uint32_t m, Coef coef) {
+#pragma unroll
+  for (int p = 0; p < 27; ++p) {
+    if (oct_free(p) == 1) {
+      const int s0 = oct_s0(p);
+      if ((none >> p) & 1u) xv[p] = (xv[p - s0] + xv[p + s0]) * T(0.5);
+    } else if (oct_free(p) == 2) {
+      const int s0 = oct_s0(p), s1 = oct_s1(p);
+      if ((none >> p) & 1u)
+        xv[p] = ((xv[p - s0 - s1] + xv[p + s0 - s1]) + (xv[p - s0 + s1] + xv[p + s0 + s1])) * T(0.25);
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < 27; ++p) yv[p] = T(0);
+  const uint32_t cm = ometa_cmask(m);
+  const T h = elem_h<T>(ometa_lev(m));
+  const T g1 = h * T(0.5), g2 = h * h * h * T(0.125);
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    if ((cm >> c) & 1u) {
+      T f1 = g1, f2 = g2;
+      coef(c, f1, f2);
+      T u[8];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) u[v] = xv[oct_lat(c, v)];
+      lapmass_ref(u, f1, f2);
+#pragma unroll
+      for (int v = 0; v < 8; ++v) yv[oct_lat(c, v)] += u[v];
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < 27; ++p) {
+    if (oct_free(p) == 1) {
+      const int s0 = oct_s0(p);
+      const T w = ((none >> p) & 1u) ? yv[p] * T(0.5) : T(0);
+      yv[p - s0] += w;
+      yv[p + s0] += w;
+    } else if (oct_free(p) == 2) {
+      const int s0 = oct_s0(p), s1 = oct_s1(p);
+      const T w = ((none >> p) & 1u) ? yv[p] * T(0.25) : T(0);
+      yv[p - s0 - s1] += w;
+      yv[p + s0 - s1] += w;
+      yv[p - s0 + s1] += w;
+      yv[p + s0 + s1] += w;
+    }
+  }
+}
+
+// One thread per octet, x and y in global memory: the octet's nodes gathered
+// from x, each node's sum added into y (which must be zero or hold the
+// values to add to) with one global reduction; the centre of an octet with
+// all 8 children present belongs to no other element and leaves with a store.
+template <class T, class CT, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_kernel(
+    int64_t n, const uint32_t* __restrict__ ometa, const uint32_t* __restrict__ oid,
+    const uint32_t* __restrict__ oelem, const CT* __restrict__ ca, const CT* __restrict__ cb,
+    const T* __restrict__ x, T* __restrict__ y) {
+  for (int64_t o = gtid(); o < n; o += gstride()) {
+    const uint32_t m = __ldg(ometa + o);
+    uint32_t id[27], none = 0;
+    T xv[27], yv[27];
+#pragma unroll
+    for (int p = 0; p < 27; ++p) {
+      id[p] = __ldg(oid + int64_t(p) * n + o);
+      none |= id[p] == kNoNode ? (1u << p) : 0u;
+    }
+#pragma unroll
+    for (int p = 0; p < 27; ++p) xv[p] = id[p] != kNoNode ? __ldg(x + id[p]) : T(0);
+    octet_apply<T>(xv, yv, none, m, [&](int c, T& f1, T& f2) {
+      if (ca) {
+        const uint32_t e = __ldg(oelem + int64_t(c) * n + o);
+        f1 *= T(__ldg(ca + e));
+        f2 *= T(__ldg(cb + e));
+      }
+    });
+    const uint32_t cm = ometa_cmask(m);
+#pragma unroll
+    for (int p = 0; p < 27; ++p) {
+      const bool node = id[p] != kNoNode;
+      T* dst = y + (node ? id[p] : 0u);
+      if (p == 13) {
+        st_if(dst, yv[p], node && cm == 255u);
+        red_add_if(dst, yv[p], node && cm != 255u);
+      } else {
+        red_add_if(dst, yv[p], node && yv[p] != T(0));
+      }
+    }
+  }
+}
+
+// Chunked octet kernel: a CTA of kOctChunk threads per chunk of kOctChunk
+// consecutive octets (OctetSet chunks).  x at the chunk's nodes (ascending
+// ids: mostly contiguous runs) and the coefficients of the chunk's element
+// range are staged in shared memory with coalesced loads; every thread works
+// its octet from shared memory and adds its 27 lattice sums into the chunk's
+// shared accumulator (shared-memory atomics: octets of one chunk share
+// nodes); then the chunk's sums leave with coalesced stores (nodes no other
+// chunk touches) or global reductions.  Chunks whose element range exceeds
+// the staged coefficient window read their coefficients from global memory.
+template <class T, class CT, int MINB>
+__global__ void __launch_bounds__(kOctChunk, MINB) lapmass_octchunk_kernel(
+    int64_t n, int64_t nchunk, uint32_t node_cap, uint32_t coef_cap, const uint32_t* __restrict__ ometa,
+    const uint16_t* __restrict__ lidx, const uint16_t* __restrict__ lelem, const uint32_t* __restrict__ cptr,
+    const uint32_t* __restrict__ cnodes, const uint32_t* __restrict__ cel, const CT* __restrict__ ca,
+    const CT* __restrict__ cb, const T* __restrict__ x, T* __restrict__ y) {
+  extern __shared__ __align__(16) unsigned char oc_smem[];
+  T* sx = reinterpret_cast<T*>(oc_smem);
+  T* sy = sx + node_cap;
+  T* sa = sy + node_cap;
+  T* sb = sa + coef_cap;
+  for (int64_t q = blockIdx.x; q < nchunk; q += gridDim.x) {
+    const uint32_t p0 = __ldg(cptr + q), nn = __ldg(cptr + q + 1) - p0;
+    const uint32_t e0 = __ldg(cel + 2 * q), ne = __ldg(cel + 2 * q + 1);
+    const bool staged = ca && ne <= coef_cap;
+    for (uint32_t k = threadIdx.x; k < nn; k += kOctChunk) {
+      sx[k] = __ldg(x + (__ldg(cnodes + p0 + k) & 0x7fffffffu));
+      sy[k] = T(0);
+    }
+    if (staged)
+      for (uint32_t k = threadIdx.x; k < ne; k += kOctChunk) {
+        sa[k] = T(__ldg(ca + e0 + k));
+        sb[k] = T(__ldg(cb + e0 + k));
+      }
+    __syncthreads();
+    const int64_t o = q * kOctChunk + threadIdx.x;
+    if (o < n) {
+      const uint32_t m = __ldg(ometa + o);
+      uint32_t none = 0;
+      uint16_t li[27];
+      T xv[27], yv[27];
+#pragma unroll
+      for (int p = 0; p < 27; ++p) {
+        li[p] = __ldg(lidx + int64_t(p) * n + o);
+        none |= li[p] == 0xffffu ? (1u << p) : 0u;
+      }
+#pragma unroll
+      for (int p = 0; p < 27; ++p) xv[p] = li[p] != 0xffffu ? sx[li[p]] : T(0);
+      octet_apply<T>(xv, yv, none, m, [&](int c, T& f1, T& f2) {
+        if (ca) {
+          const uint32_t le = __ldg(lelem + int64_t(c) * n + o);
+          if (staged) {
+            f1 *= sa[le];
+            f2 *= sb[le];
+          } else {
+            f1 *= T(__ldg(ca + e0 + le));
+            f2 *= T(__ldg(cb + e0 + le));
+          }
+        }
+      });
+#pragma unroll
+      for (int p = 0; p < 27; ++p)
+        if (li[p] != 0xffffu && yv[p] != T(0)) atomicAdd(sy + li[p], yv[p]);
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < nn; k += kOctChunk) {
+      const uint32_t id = __ldg(cnodes + p0 + k);
+      T* dst = y + (id & 0x7fffffffu);
+      const T v = sy[k];
+      st_if(dst, v, !(id >> 31));
+      red_add_if(dst, v, (id >> 31) && v != T(0));
+    }
+    __syncthreads();  // the buffers are reused by the next chunk
   }
 }
 
@@ -1001,7 +1177,8 @@ __global__ void type1_dense_kernel(const uint32_t* __restrict__ nl, const uint32
 struct MatvecVariant {
   int block, per_sm;  // threads per CTA, CTAs per SM in the grid (0: one thread per element)
   int kind;           // 0 atomic (BLOCK, MINB), 2 warp-tile, 3 + records prefetched, 4 + ids and x too,
-                      // 5 records staged by bulk copies
+                      // 5 records staged by bulk copies, 6 octet (one thread per parent octant),
+                      // 7 octet chunks staged through shared memory
   int minb;
   const char* name;
 };
@@ -1017,7 +1194,31 @@ constexpr MatvecVariant kVariants[] = {
     {32 * kTmaWarps, 5, 5, 5, "warp-tile 32 elems, records by bulk copy, 5 CTAs of 4 warps/SM"},
     {32 * kTmaWarps, 6, 5, 6, "warp-tile 32 elems, records by bulk copy, 6 CTAs of 4 warps/SM"},
     {32 * kTmaWarps, 7, 5, 7, "warp-tile 32 elems, records by bulk copy, 7 CTAs of 4 warps/SM"},
+    {128, 3, 6, 3, "octet b128, 3 CTAs/SM"},
+    {128, 4, 6, 4, "octet b128, 4 CTAs/SM"},
+    {256, 2, 6, 2, "octet b256, 2 CTAs/SM"},
+    {64, 8, 6, 8, "octet b64, 8 CTAs/SM"},
+    {kOctChunk, 2, 7, 2, "octet chunks of 128, 2 CTAs/SM"},
+    {kOctChunk, 3, 7, 3, "octet chunks of 128, 3 CTAs/SM"},
+    {kOctChunk, 4, 7, 4, "octet chunks of 128, 4 CTAs/SM"},
 };
+// Coefficients of at most this many consecutive elements are staged per chunk.
+constexpr uint32_t kOctCoefCap = 2048;
+// Largest shared-memory need of the chunked kernel, in values: x and sums of
+// at most 27 kOctChunk nodes, and kOctCoefCap coefficient pairs.
+constexpr size_t kOctChunkSmemMax = 2 * 27 * kOctChunk + 2 * kOctCoefCap;
+
+// Raise a kernel's dynamic shared-memory limit once (the first launch of
+// each kernel, normally the autotuner's, outside any stream capture).
+static dg_status allow_dynamic_smem(const void* kern, size_t bytes) {
+  static std::mutex mu;
+  static std::vector<const void*> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (std::find(done.begin(), done.end(), kern) != done.end()) return DG_OK;
+  DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+  done.push_back(kern);
+  return DG_OK;
+}
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 
 template <class T, class CT>
@@ -1026,7 +1227,32 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
   const MatvecVariant& V = kVariants[v];
   const unsigned g = V.per_sm ? grid_for(da->E, V.block, V.per_sm)
                               : unsigned((da->E + V.block - 1) / V.block > 0 ? (da->E + V.block - 1) / V.block : 1);
-  if (V.kind == 5) {
+  if (V.kind == 7) {
+    const OctetSet& O = da->octs;
+    const uint32_t coef_cap = ca ? std::min(O.max_erange, kOctCoefCap) : 0u;
+    const size_t smem = sizeof(T) * (2 * size_t(O.max_nodes) + 2 * size_t(coef_cap));
+    const unsigned gq = unsigned(std::min<int64_t>(O.nchunk, int64_t(sm_count()) * V.per_sm));
+    auto go = [&](auto kern) -> dg_status {
+      DG_TRY(allow_dynamic_smem(reinterpret_cast<const void*>(kern), kOctChunkSmemMax * sizeof(T)));
+      kern<<<gq, kOctChunk, smem, s>>>(O.n, O.nchunk, O.max_nodes, coef_cap, O.meta.p, O.lidx.p, O.lelem.p,
+                                       O.cptr.p, O.cnodes.p, O.cel.p, ca, cb, x, y);
+      return DG_OK;
+    };
+    if (V.minb == 2) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 2>));
+    else if (V.minb == 3) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 3>));
+    else DG_TRY(go(lapmass_octchunk_kernel<T, CT, 4>));
+  } else if (V.kind == 6) {
+    const OctetSet& O = da->octs;
+    const unsigned go = grid_for(O.n, V.block, V.per_sm);
+    if (V.block == 128 && V.minb == 3)
+      lapmass_octet_kernel<T, CT, 128, 3><<<go, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
+    else if (V.block == 128)
+      lapmass_octet_kernel<T, CT, 128, 4><<<go, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
+    else if (V.block == 256)
+      lapmass_octet_kernel<T, CT, 256, 2><<<go, 256, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
+    else
+      lapmass_octet_kernel<T, CT, 64, 8><<<go, 64, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
+  } else if (V.kind == 5) {
     const TileSet& ts = da->tiles_w;
     const unsigned gt = grid_for(ts.ntiles * 32, 32 * kTmaWarps, V.per_sm);
     const uint2* e8 = reinterpret_cast<const uint2*>(ts.eloc8.p);
@@ -1082,7 +1308,8 @@ static int forced_variant() {
     const char* e = getenv("DG_MATVEC_KERNEL");
     v = -1;
     if (e && *e) {
-      const int kind = !strcmp(e, "atomic") ? 0 : !strcmp(e, "warp") ? 2 : -1;
+      const int kind = !strcmp(e, "atomic") ? 0 : !strcmp(e, "warp") ? 2 : !strcmp(e, "octet") ? 6
+                     : !strcmp(e, "chunk") ? 7 : -1;
       if (kind >= 0) {
         for (int i = kNumVariants - 1; i >= 0; --i)
           if (kVariants[i].kind == kind) v = i;
@@ -1126,7 +1353,9 @@ static dg_status pick_variant(const dg_da* da, int& choice, const CT* ca, const 
     DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
     DG_TRY((launch_variant<T, CT>(0, da, ca, cb, x, y, s)));
     for (int v = 0; v < kNumVariants; ++v) {
-      if (kVariants[v].kind >= 2 && da->tiles_w.ntiles == 0) continue;
+      if (kVariants[v].kind >= 2 && kVariants[v].kind <= 5 && da->tiles_w.ntiles == 0) continue;
+      if (kVariants[v].kind == 6 && da->octs.n == 0) continue;
+      if (kVariants[v].kind == 7 && da->octs.nchunk == 0) continue;
       for (int trial = 0; trial < 2; ++trial) {
         DG_CUDA(cudaMemsetAsync(flush.p, trial + 1, flush_bytes, s));
         DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
@@ -1668,6 +1897,58 @@ __global__ void elasticity_diag_kernel(const uint32_t* __restrict__ nl, const ui
   }
 }
 
+// Dense assembly of the operator on a small level (the coarsest level of the
+// dof-3 multigrid): per element and non-hanging, non-Dirichlet column (node,
+// component) the element operator applied to that unit vector, scattered into
+// the non-Dirichlet rows of the row-major n3 x n3 matrix (n3 = 3 N).
+__global__ void elasticity_dense_kernel(const uint32_t* __restrict__ nl, const uint32_t* __restrict__ meta,
+                                        const uint8_t* __restrict__ dir, int64_t E, double mu, double lam,
+                                        int64_t n3, double* __restrict__ Ad) {
+  for (int64_t t = gtid(); t < E * 24; t += gstride()) {
+    const int64_t e = t / 24;
+    const int j = int(t - e * 24), jn = j / 3, jd = j % 3;
+    const uint32_t m = meta[e];
+    const uint32_t lev = meta_lev(m), c = meta_cnum(m), mask = meta_mask(m);
+    if ((mask >> jn) & 1u) continue;  // a hanging vertex is no column of its own
+    const uint32_t node = nl[int64_t(jn) * E + e];
+    if (dir[node]) continue;
+    const double fac = elem_h<double>(lev) / 2.0;
+    double u[3][8], r[3][8];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int v = 0; v < 8; ++v) u[a][v] = (a == jd && v == jn) ? 1.0 : 0.0;
+    if (mask)
+      for (int a = 0; a < 3; ++a) interp_hanging(u[a], c, mask);
+    const double wl = mu * fac, wg = (mu + lam) * fac;
+    for (int a = 0; a < 3; ++a) lapmass_ref_to(u[a], wl, 0.0, r[a]);
+    graddiv_block<0, 0>(u[0], wg, r[0]);
+    graddiv_block<0, 1>(u[1], wg, r[0]);
+    graddiv_block<0, 2>(u[2], wg, r[0]);
+    graddiv_block<1, 0>(u[0], wg, r[1]);
+    graddiv_block<1, 1>(u[1], wg, r[1]);
+    graddiv_block<1, 2>(u[2], wg, r[1]);
+    graddiv_block<2, 0>(u[0], wg, r[2]);
+    graddiv_block<2, 1>(u[1], wg, r[2]);
+    graddiv_block<2, 2>(u[2], wg, r[2]);
+    if (mask)
+      for (int a = 0; a < 3; ++a) scatter_hanging(r[a], c, mask);
+    const int64_t col = 3 * int64_t(node) + jd;
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t rn = nl[int64_t(k) * E + e];
+      if (dir[rn]) continue;
+      for (int a = 0; a < 3; ++a)
+        if (r[a][k] != 0.0) atomicAdd(Ad + (3 * int64_t(rn) + a) * n3 + col, r[a][k]);
+    }
+  }
+}
+__global__ void elasticity_dense_dirichlet(const uint8_t* __restrict__ dir, int64_t N, double* __restrict__ Ad) {
+  const int64_t n3 = 3 * N;
+  for (int64_t i = gtid(); i < N; i += gstride())
+    if (dir[i])
+      for (int a = 0; a < 3; ++a) Ad[(3 * i + a) * n3 + 3 * i + a] = 1.0;
+}
+
 __global__ void set_dirichlet_diag(const uint8_t* __restrict__ dir, int64_t N, double* __restrict__ d) {
   for (int64_t i = gtid(); i < N; i += gstride())
     if (dir[i]) d[3 * i] = d[3 * i + 1] = d[3 * i + 2] = 1.0;
@@ -1766,6 +2047,17 @@ dg_status dirichlet_diag(const dg_mat* A, double* d, cudaStream_t s) {
   dirichlet_scalar_diag_kernel<<<grid_for(da->E * 8, 128, 16), 128, 0, s>>>(da->nl.p, da->meta.p, A->dirichlet.p,
                                                                               da->E, mass, d);
   set_dirichlet_diag1<<<grid_for(da->N, 256), 256, 0, s>>>(A->dirichlet.p, da->N, d);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status elasticity_assemble_dense(const dg_mat* A, double* dense, cudaStream_t s) {
+  const dg_da* da = A->da;
+  const int64_t n3 = 3 * da->N;
+  DG_CUDA(cudaMemsetAsync(dense, 0, sizeof(double) * n3 * n3, s));
+  elasticity_dense_kernel<<<grid_for(da->E * 24, 128, 16), 128, 0, s>>>(da->nl.p, da->meta.p, A->dirichlet.p, da->E,
+                                                                         A->mu, A->lam, n3, dense);
+  elasticity_dense_dirichlet<<<grid_for(da->N, 256), 256, 0, s>>>(A->dirichlet.p, da->N, dense);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }

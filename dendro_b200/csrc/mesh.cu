@@ -451,7 +451,8 @@ dg_status build_mesh(const dg_octree* tree, dg_da* da, cudaStream_t s) {
   DG_CHECK(!(herr & 1u), DG_EUNBALANCED, "hanging vertex without a parent node: octree not 2:1 balanced");
   DG_CHECK(!(herr & 2u), DG_EUNBALANCED, "hanging configuration outside the 18 element types");
   da->ekey = std::move(ekey);
-  return build_tiles(da, s);
+  DG_TRY(build_tiles(da, s));
+  return build_octets(da, s);
 }
 
 template <int TE>

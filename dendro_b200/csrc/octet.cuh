@@ -1,0 +1,58 @@
+// Octet form of the Laplacian + mass operator (Jacobian2MatMult,
+// examples/src/backend/omgNeumann.C:468-557): one thread per parent octant.
+//
+// Every leaf element is child c of a parent octant P.  The 8 children of P
+// share the 3 x 3 x 3 lattice of P's corners, edge midpoints, face centres
+// and centre (lattice point p = x + 3 y + 9 z, x, y, z in {0, 1, 2}); vertex v
+// of child c is lattice point c + v per axis.  An "octet" is a parent with at
+// least one leaf child; a child mask says which children are elements (the
+// others are refined further and belong to deeper octets).  Per octet the
+// mesh stores the node id of every lattice point that is a node of a present
+// child, and kNoNode for points that hang or that no present child touches.
+//
+// Hanging points are the reference's hanging vertices (the 2:1 balanced
+// octree's vertices that lie inside an edge or face of a coarser element,
+// odaBuildNlist.C): an edge midpoint of P takes the mean of its edge's two
+// corners, a face centre the mean of its face's four corners, exactly the
+// interpolation T of the per-element stencils (`T^T L T`, handleType2Stencils.C).
+// Corners of P are never hanging (a coarser neighbour of a child is at most
+// P's size and aligned with P), and the centre is interior to P.
+//
+// The thread gathers x at the octet's nodes once, fills the hanging points,
+// applies each present child's element operator with compile-time lattice
+// indices (all values stay in registers), accumulates the 27 lattice sums,
+// folds the hanging points' sums back onto their corners (T^T) and adds each
+// node's sum into y with one FP64/FP32 global reduction -- the sums over the
+// octet's own children are done in registers, not in memory.
+#pragma once
+
+#include "dg_internal.h"
+
+namespace dg {
+
+constexpr uint32_t kNoNode = 0xffffffffu;
+
+// Lattice point of vertex v of child c.
+__host__ __device__ constexpr int oct_lat(int c, int v) {
+  return ((c & 1) + (v & 1)) + 3 * (((c >> 1) & 1) + ((v >> 1) & 1)) + 9 * (((c >> 2) & 1) + ((v >> 2) & 1));
+}
+// Coordinate a (0 x, 1 y, 2 z) of lattice point p, and its stride.
+__host__ __device__ constexpr int oct_coord(int p, int a) { return a == 0 ? p % 3 : a == 1 ? (p / 3) % 3 : p / 9; }
+__host__ __device__ constexpr int oct_stride(int a) { return a == 0 ? 1 : a == 1 ? 3 : 9; }
+// Number of coordinates equal to 1: 0 corner, 1 edge midpoint, 2 face centre, 3 centre.
+__host__ __device__ constexpr int oct_free(int p) {
+  return (oct_coord(p, 0) == 1) + (oct_coord(p, 1) == 1) + (oct_coord(p, 2) == 1);
+}
+// The two free axes' strides of a face centre (or the one of an edge midpoint in s0).
+__host__ __device__ constexpr int oct_s0(int p) {
+  return oct_coord(p, 0) == 1 ? 1 : oct_coord(p, 1) == 1 ? 3 : 9;
+}
+__host__ __device__ constexpr int oct_s1(int p) {
+  return oct_coord(p, 2) == 1 ? 9 : oct_coord(p, 1) == 1 ? 3 : 1;
+}
+
+// Per-octet word: level of the children (embedded) | child mask << 8.
+__host__ __device__ __forceinline__ uint32_t ometa_lev(uint32_t m) { return m & 31u; }
+__host__ __device__ __forceinline__ uint32_t ometa_cmask(uint32_t m) { return (m >> 8) & 255u; }
+
+}  // namespace dg

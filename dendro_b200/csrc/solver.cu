@@ -237,6 +237,53 @@ __global__ void restrict_gather(const uint32_t* __restrict__ rptr, const uint32_
     rc[c] = acc;
   }
 }
+// The dof-3 forms: the scalar transfer applied to each of the 3 interleaved
+// components (node-major [N][3]), as the reference's transfer loops apply
+// the same R entry to every dof (RestrictMatVec.C:109-115, ProlongMatVec.C).
+__global__ void prolong_add3(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+                             const double* __restrict__ val, int64_t Nf, const double* __restrict__ xc,
+                             double* __restrict__ xf) {
+  for (int64_t f = gtid(); f < Nf; f += gstride()) {
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (uint32_t k = ptr[f]; k < ptr[f + 1]; ++k) {
+      const double w = val[k];
+      const int64_t c = 3 * int64_t(col[k]);
+      s0 += w * xc[c];
+      s1 += w * xc[c + 1];
+      s2 += w * xc[c + 2];
+    }
+    xf[3 * f] += s0;
+    xf[3 * f + 1] += s1;
+    xf[3 * f + 2] += s2;
+  }
+}
+__global__ void restrict_gather3(const uint32_t* __restrict__ rptr, const uint32_t* __restrict__ rcol,
+                                 const double* __restrict__ rval, int64_t Nc, const double* __restrict__ rf,
+                                 double* __restrict__ rc) {
+  for (int64_t c = gtid(); c < Nc; c += gstride()) {
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (uint32_t k = rptr[c]; k < rptr[c + 1]; ++k) {
+      const double w = rval[k];
+      const int64_t f = 3 * int64_t(rcol[k]);
+      s0 += w * rf[f];
+      s1 += w * rf[f + 1];
+      s2 += w * rf[f + 2];
+    }
+    rc[3 * c] = s0;
+    rc[3 * c + 1] = s1;
+    rc[3 * c + 2] = s2;
+  }
+}
+// x += omega dinv (b - t), elementwise (the dof-3 sweep after the operator)
+__global__ void jacobi_update(double* __restrict__ x, const double* __restrict__ b, const double* __restrict__ dinv,
+                              const double* __restrict__ t, double omega, int64_t n) {
+  for (int64_t i = gtid(); i < n; i += gstride()) x[i] += omega * dinv[i] * (b[i] - t[i]);
+}
+__global__ void residual_update(const double* __restrict__ b, const double* __restrict__ t, double* __restrict__ r,
+                                int64_t n) {
+  for (int64_t i = gtid(); i < n; i += gstride()) r[i] = b[i] - t[i];
+}
+
 // transpose of P: keys (coarse column << 32 | entry index) and counts per column
 __global__ void ptrans_keys(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col, int64_t Nf,
                             uint64_t* __restrict__ keys, uint32_t* __restrict__ frow, uint32_t* __restrict__ cnt) {
@@ -333,6 +380,163 @@ __global__ void gj_elim(double* __restrict__ A, const int64_t* __restrict__ bn, 
     Ab[t] = (j == k ? 0.0 : Ab[t]) - ck[i] * Ab[k * n + j];
   }
 }
+// Blocked Gauss-Jordan inversion of one SPD matrix A (n x n, row-major, in
+// place) for coarse levels too large for one pivot per launch: per pivot
+// block K of kGjB rows (P = A[K,K], row panel R = A[K,J], column panel
+// C = A[I,K], the rest S = A[I,J]) one sweep replaces
+//   P <- P^-1,  R <- P^-1 R,  S <- S - C (P^-1 R),  C <- -C P^-1,
+// which after every block has been swept leaves A^-1 (the block form of the
+// scalar sweep of gj_col / gj_row / gj_elim).  SPD keeps every pivot block
+// invertible without pivoting.  The S update is the n^2 kGjB multiply-add
+// product that carries the cost: 64 x 64 output tiles, 4 x 4 per thread,
+// the panels staged through shared memory.
+constexpr int kGjB = 64;
+
+// P^-1 of the pivot block into Pinv (kb x kb, leading dimension kGjB), by the
+// unblocked sweep in shared memory (one CTA of 256 threads).
+__global__ void __launch_bounds__(256) gjb_pivot(const double* __restrict__ A, int64_t n, int64_t k0, int kb,
+                                                 double* __restrict__ Pinv) {
+  __shared__ double P[kGjB][kGjB + 1];
+  __shared__ double ck[kGjB];
+  for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+    const int i = t / kb, j = t - i * kb;
+    P[i][j] = A[(k0 + i) * n + k0 + j];
+  }
+  __syncthreads();
+  for (int k = 0; k < kb; ++k) {
+    if (threadIdx.x < kb) ck[threadIdx.x] = P[threadIdx.x][k];
+    __syncthreads();
+    const double piv = ck[k];
+    if (threadIdx.x < kb) P[k][threadIdx.x] = (threadIdx.x == k ? 1.0 : P[k][threadIdx.x]) / piv;
+    __syncthreads();
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+      const int i = t / kb, j = t - i * kb;
+      if (i != k) P[i][j] = (j == k ? 0.0 : P[i][j]) - ck[i] * P[k][j];
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+    const int i = t / kb, j = t - i * kb;
+    Pinv[i * kGjB + j] = P[i][j];
+  }
+}
+
+// R <- P^-1 R: CTA = one strip of 64 columns outside the pivot block.
+__global__ void __launch_bounds__(256) gjb_row(double* __restrict__ A, int64_t n, int64_t k0, int kb,
+                                               const double* __restrict__ Pinv) {
+  extern __shared__ double gj_smem[];  // two kGjB x (kGjB + 1) panels
+  double(*Pi)[kGjB + 1] = reinterpret_cast<double(*)[kGjB + 1]>(gj_smem);
+  double(*R)[kGjB + 1] = reinterpret_cast<double(*)[kGjB + 1]>(gj_smem + kGjB * (kGjB + 1));
+  const int64_t j0 = int64_t(blockIdx.x) * kGjB;
+  if (j0 == k0) return;  // the pivot block's own columns
+  for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
+    const int i = t / kGjB, j = t - i * kGjB;
+    Pi[i][j] = (i < kb && j < kb) ? Pinv[i * kGjB + j] : 0.0;
+    R[i][j] = (i < kb && j0 + j < n) ? A[(k0 + i) * n + j0 + j] : 0.0;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
+    const int i = t / kGjB, j = t - i * kGjB;
+    if (i >= kb || j0 + j >= n) continue;
+    double acc = 0;
+    for (int k = 0; k < kb; ++k) acc += Pi[i][k] * R[k][j];
+    A[(k0 + i) * n + j0 + j] = acc;
+  }
+}
+
+// S <- S - C R for every 64 x 64 tile outside the pivot rows and columns
+// (blockIdx.x: column tile, blockIdx.y: row tile).
+__global__ void __launch_bounds__(256) gjb_update(double* __restrict__ A, int64_t n, int64_t k0, int kb) {
+  extern __shared__ double gj_smem[];
+  double(*Cs)[kGjB + 2] = reinterpret_cast<double(*)[kGjB + 2]>(gj_smem);                      // Cs[k][row]
+  double(*Rs)[kGjB + 2] = reinterpret_cast<double(*)[kGjB + 2]>(gj_smem + kGjB * (kGjB + 2));  // Rs[k][col]
+  const int64_t i0 = int64_t(blockIdx.y) * kGjB, j0 = int64_t(blockIdx.x) * kGjB;
+  if (i0 == k0 || j0 == k0) return;
+  for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
+    const int r = t / kGjB, k = t - r * kGjB;
+    Cs[k][r] = (k < kb && i0 + r < n) ? A[(i0 + r) * n + k0 + k] : 0.0;
+    Rs[r][k] = (r < kb && j0 + k < n) ? A[(k0 + r) * n + j0 + k] : 0.0;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0;
+  for (int k = 0; k < kb; ++k) {
+    double cv[4], rv[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) cv[a] = Cs[k][ty + 16 * a];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) rv[b] = Rs[k][tx + 16 * b];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] += cv[a] * rv[b];
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int64_t i = i0 + ty + 16 * a;
+    if (i >= n) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int64_t j = j0 + tx + 16 * b;
+      if (j < n) A[i * n + j] -= acc[a][b];
+    }
+  }
+}
+
+// C <- -C P^-1 for the rows outside the pivot block (one 64-row strip per
+// CTA), and the pivot block <- P^-1 (the CTA of the pivot rows).
+__global__ void __launch_bounds__(256) gjb_col(double* __restrict__ A, int64_t n, int64_t k0, int kb,
+                                               const double* __restrict__ Pinv) {
+  extern __shared__ double gj_smem[];
+  double(*Pi)[kGjB + 1] = reinterpret_cast<double(*)[kGjB + 1]>(gj_smem);
+  double(*Cb)[kGjB + 1] = reinterpret_cast<double(*)[kGjB + 1]>(gj_smem + kGjB * (kGjB + 1));
+  const int64_t i0 = int64_t(blockIdx.x) * kGjB;
+  if (i0 == k0) {
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+      const int i = t / kb, j = t - i * kb;
+      A[(k0 + i) * n + k0 + j] = Pinv[i * kGjB + j];
+    }
+    return;
+  }
+  for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
+    const int i = t / kGjB, j = t - i * kGjB;
+    Pi[i][j] = (i < kb && j < kb) ? Pinv[i * kGjB + j] : 0.0;
+    Cb[i][j] = (i0 + i < n && j < kb) ? A[(i0 + i) * n + k0 + j] : 0.0;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
+    const int i = t / kGjB, j = t - i * kGjB;
+    if (i0 + i >= n || j >= kb) continue;
+    double acc = 0;
+    for (int k = 0; k < kb; ++k) acc += Cb[i][k] * Pi[k][j];
+    A[(i0 + i) * n + k0 + j] = -acc;
+  }
+}
+
+dg_status gj_invert_blocked(double* A, int64_t n, cudaStream_t s) {
+  DBuf<double> pinv;
+  DG_TRY(pinv.alloc(kGjB * kGjB));
+  const unsigned nt = unsigned((n + kGjB - 1) / kGjB);
+  const int sm1 = int(sizeof(double)) * 2 * kGjB * (kGjB + 1), sm2 = int(sizeof(double)) * 2 * kGjB * (kGjB + 2);
+  DG_CUDA(cudaFuncSetAttribute(gjb_row, cudaFuncAttributeMaxDynamicSharedMemorySize, sm1));
+  DG_CUDA(cudaFuncSetAttribute(gjb_col, cudaFuncAttributeMaxDynamicSharedMemorySize, sm1));
+  DG_CUDA(cudaFuncSetAttribute(gjb_update, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
+  for (int64_t k0 = 0; k0 < n; k0 += kGjB) {
+    const int kb = int(std::min<int64_t>(kGjB, n - k0));
+    gjb_pivot<<<1, 256, 0, s>>>(A, n, k0, kb, pinv.p);
+    gjb_row<<<nt, 256, sm1, s>>>(A, n, k0, kb, pinv.p);
+    gjb_update<<<dim3(nt, nt), 256, sm2, s>>>(A, n, k0, kb);
+    gjb_col<<<nt, 256, sm1, s>>>(A, n, k0, kb, pinv.p);
+  }
+  DG_CUDA(cudaGetLastError());
+  DG_CUDA(cudaStreamSynchronize(s));  // pinv is freed on return
+  return DG_OK;
+}
+
 // x = Ainv b with block-diagonal Ainv, one warp per row
 __global__ void dense_gemv(const double* __restrict__ A, int64_t N, const uint32_t* __restrict__ row_blk,
                            const int64_t* __restrict__ boff, const int64_t* __restrict__ bn,
@@ -590,14 +794,15 @@ dg_status build_restriction(Level& F, int64_t Nc, cudaStream_t s) {
 }
 
 dg_status setup_level_vectors(Level& L, cudaStream_t s) {
-  const int64_t N = L.da->N;
+  const int64_t N = int64_t(L.A->dof) * L.da->N;
   DG_TRY(L.dinv.alloc(N));
   DG_TRY(L.x.alloc(N));
   DG_TRY(L.b.alloc(N));
   DG_TRY(L.t.alloc(N));
   DG_TRY(L.acc.alloc(N));
   DG_CUDA(cudaMemsetAsync(L.acc.p, 0, 8 * N, s));
-  DG_TRY(lapmass_diag(L.A.get(), L.dinv.p, s));
+  if (L.A->kind == 1) DG_TRY(elasticity_diag(L.A.get(), L.dinv.p, s));
+  else DG_TRY(lapmass_diag(L.A.get(), L.dinv.p, s));
   invert<<<grid_for(N, 256), 256, 0, s>>>(L.dinv.p, N);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
@@ -636,8 +841,36 @@ __global__ void fill_row_blk(uint32_t* __restrict__ rb, int64_t n0, int64_t n1, 
   for (int64_t i = n0 + gtid(); i < n1; i += gstride()) rb[i] = b;
 }
 
+// The dense inverse of the coarsest operator: up to kMaxCoarseNodes nodes per
+// mesh (8.6 GB of FP64 at the limit); one mesh above kGjBlockedFrom nodes is
+// inverted by the blocked sweep, smaller or batched meshes one pivot per launch.
+constexpr int64_t kMaxCoarseNodes = 32768;
+constexpr int64_t kGjBlockedFrom = 1024;
+dg_status gj_invert(dg_damg* m, int64_t maxn, int nb);
+
 dg_status setup_coarse(dg_damg* m) {
   Level& L = m->lv.back();
+  if (L.A->kind == 1) {
+    // dof 3: one mesh, one dense block over its 3 N unknowns
+    const int64_t n3 = 3 * L.da->N;
+    DG_CHECK(n3 <= kMaxCoarseNodes, DG_EINVAL,
+             "coarsest level too large for the dense direct solve (> 32768 unknowns of one mesh)");
+    m->cb_off.assign(1, 0);
+    m->cb_n.assign(1, n3);
+    m->cb_aoff.assign(1, 0);
+    m->nc = n3;
+    DG_TRY(m->Ainv.alloc(n3 * n3));
+    DG_TRY(m->d_cb_off.alloc(1));
+    DG_TRY(m->d_cb_n.alloc(1));
+    DG_TRY(m->d_cb_aoff.alloc(1));
+    DG_TRY(m->d_crow_blk.alloc(n3));
+    DG_CUDA(cudaMemcpyAsync(m->d_cb_off.p, m->cb_off.data(), 8, cudaMemcpyHostToDevice, m->s));
+    DG_CUDA(cudaMemcpyAsync(m->d_cb_n.p, m->cb_n.data(), 8, cudaMemcpyHostToDevice, m->s));
+    DG_CUDA(cudaMemcpyAsync(m->d_cb_aoff.p, m->cb_aoff.data(), 8, cudaMemcpyHostToDevice, m->s));
+    DG_CUDA(cudaMemsetAsync(m->d_crow_blk.p, 0, 4 * n3, m->s));
+    DG_TRY(elasticity_assemble_dense(L.A.get(), m->Ainv.p, m->s));
+    return gj_invert(m, n3, 1);
+  }
   const int64_t N = L.da->N;
   const std::vector<int64_t>& noff = m->mesh_node_off.back();
   const int nb = int(noff.size()) - 1;
@@ -647,7 +880,8 @@ dg_status setup_coarse(dg_damg* m) {
   int64_t total = 0, maxn = 0;
   for (int b = 0; b < nb; ++b) {
     m->cb_n[b] = noff[b + 1] - noff[b];
-    DG_CHECK(m->cb_n[b] <= 16384, DG_EINVAL, "coarsest level too large for the dense direct solve (> 16384 nodes)");
+    DG_CHECK(m->cb_n[b] <= kMaxCoarseNodes, DG_EINVAL,
+             "coarsest level too large for the dense direct solve (> 32768 nodes of one mesh)");
     m->cb_aoff[b] = total;
     total += m->cb_n[b] * m->cb_n[b];
     maxn = m->cb_n[b] > maxn ? m->cb_n[b] : maxn;
@@ -665,6 +899,14 @@ dg_status setup_coarse(dg_damg* m) {
     fill_row_blk<<<grid_for(m->cb_n[b], 256), 256, 0, m->s>>>(m->d_crow_blk.p, noff[b], noff[b + 1], uint32_t(b));
   DG_TRY(lapmass_assemble_dense(L.A.get(), m->Ainv.p, total, m->d_crow_blk.p, m->d_cb_off.p, m->d_cb_n.p,
                                 m->d_cb_aoff.p, m->s, L.jcoef(), L.jset()));
+  return gj_invert(m, maxn, nb);
+}
+
+// The dense inverse of the coarsest operator in m->Ainv: the blocked sweep
+// for one large block, else one pivot per launch over all blocks.
+dg_status gj_invert(dg_damg* m, int64_t maxn, int nb) {
+  if (nb == 1 && maxn > kGjBlockedFrom) return gj_invert_blocked(m->Ainv.p, maxn, m->s);
+  const int64_t N = m->nc;
   DBuf<double> colk;
   DG_TRY(colk.alloc(N));
   const dim3 g1(grid_for(maxn, 256), unsigned(nb)), g2(grid_for(maxn * maxn, 256), unsigned(nb));
@@ -728,7 +970,34 @@ dg_status setup_type1(dg_damg* m, size_t l) {
   return DG_OK;
 }
 
+// dof 3: ElasticityMatMult on every level with that level's boundary nodes
+// (assignBoundaryFlags) as its Dirichlet nodes (SetElasticityContexts,
+// examples/src/backend/elasticityJac.C:396-480).
+dg_status set_elasticity_operators(dg_damg* m) {
+  cudaStream_t s = m->s;
+  for (size_t l = 0; l < m->lv.size(); ++l) {
+    Level& L = m->lv[l];
+    auto A = std::make_unique<dg_mat>();
+    A->da = L.da.get();
+    A->kind = 1;
+    A->dof = 3;
+    A->mu = m->cfg.mu;
+    A->lam = m->cfg.lambda;
+    DG_TRY(A->dirichlet.alloc(L.da->N));
+    DG_TRY(node_boundary_flags(L.da.get(), A->dirichlet.p, s));
+    L.A = std::move(A);
+    DG_TRY(setup_level_vectors(L, s));
+    L.t1.n = 0;
+  }
+  m->drop_graphs();
+  return setup_coarse(m);
+}
+
 dg_status set_operators(dg_damg* m, const double* coef) {
+  if (m->cfg.dof == 3) {
+    DG_CHECK(!coef, DG_EINVAL, "damg: dof 3 (elasticity) takes no Laplacian-mass coefficients");
+    return set_elasticity_operators(m);
+  }
   cudaStream_t s = m->s;
   for (size_t l = 0; l < m->lv.size(); ++l) {
     Level& L = m->lv[l];
@@ -779,8 +1048,54 @@ dg_status set_operators(dg_damg* m, const double* coef) {
   return setup_coarse(m);
 }
 
+// The level operator y = A x (FP64): Laplacian + mass, or elasticity.
+dg_status level_op(const Level& L, const double* x, double* y, cudaStream_t s) {
+  if (L.A->kind == 1) return elasticity_apply_f64(L.A.get(), x, y, s);
+  return lapmass_apply_f64(L.A.get(), x, y, s);
+}
+
+// The dof-3 V(nu_pre, nu_post) cycle: the same Richardson-Jacobi steps as the
+// scalar one (zero initial guess, first sweep x = omega D^-1 b), with the
+// elasticity operator and the transfers applied per component.
+dg_status vcycle3(dg_damg* m, size_t l, const double* b, double* x) {
+  cudaStream_t s = m->s;
+  Level& L = m->lv[l];
+  const int64_t nn = L.da->N, n = 3 * nn;
+  const unsigned g = grid_for(n, 256, 16);
+  if (l + 1 == m->lv.size()) {
+    dense_gemv<<<grid_for(n * 32, 256), 256, 0, s>>>(m->Ainv.p, n, m->d_crow_blk.p, m->d_cb_off.p, m->d_cb_n.p,
+                                                     m->d_cb_aoff.p, b, x);
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+  }
+  const double w = m->cfg.omega;
+  if (m->cfg.nu_pre > 0) {
+    jacobi_first<<<g, 256, 0, s>>>(x, b, L.dinv.p, w, n);
+    for (int k = 1; k < m->cfg.nu_pre; ++k) {
+      DG_TRY(elasticity_apply_f64(L.A.get(), x, L.t.p, s));
+      jacobi_update<<<g, 256, 0, s>>>(x, b, L.dinv.p, L.t.p, w, n);
+    }
+    DG_TRY(elasticity_apply_f64(L.A.get(), x, L.acc.p, s));
+    residual_update<<<g, 256, 0, s>>>(b, L.acc.p, L.t.p, n);
+  } else {
+    DG_CUDA(cudaMemsetAsync(x, 0, 8 * n, s));
+  }
+  Level& C = m->lv[l + 1];
+  restrict_gather3<<<grid_for(C.da->N, 256, 16), 256, 0, s>>>(L.rptr.p, L.rcol.p, L.rval.p, C.da->N,
+                                                             m->cfg.nu_pre > 0 ? (const double*)L.t.p : b, C.b.p);
+  DG_TRY(vcycle3(m, l + 1, C.b.p, C.x.p));
+  prolong_add3<<<grid_for(nn, 256, 16), 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval.p, nn, C.x.p, x);
+  for (int k = 0; k < m->cfg.nu_post; ++k) {
+    DG_TRY(elasticity_apply_f64(L.A.get(), x, L.t.p, s));
+    jacobi_update<<<g, 256, 0, s>>>(x, b, L.dinv.p, L.t.p, w, n);
+  }
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
 // z = V(b) on level l (x of level l holds the result)
 dg_status vcycle(dg_damg* m, size_t l, const double* b, double* x) {
+  if (m->cfg.dof == 3) return vcycle3(m, l, b, x);
   cudaStream_t s = m->s;
   Level& L = m->lv[l];
   const int64_t n = L.da->N;
@@ -859,7 +1174,7 @@ dg_status vcycle32(dg_damg* m, size_t l, const float* b, float* x) {
 // z = M^-1 r on the finest level: the FP64 V-cycle, or the FP32 one between
 // conversions of r and z.
 dg_status precond_body(dg_damg* m) {
-  if (m->cfg.inner_prec == DG_PREC_F64) return vcycle(m, 0, m->r.p, m->z.p);
+  if (m->cfg.inner_prec == DG_PREC_F64 || m->cfg.dof == 3) return vcycle(m, 0, m->r.p, m->z.p);
   const int64_t n = m->lv[0].da->N;
   const unsigned g = grid_for(n, 256);
   convert<double, float><<<g, 256, 0, m->s>>>(m->r.p, m->r32.p, n);
@@ -938,6 +1253,9 @@ void dg_damg_default_config(dg_damg_config* c) {
   c->inner_prec = DG_PREC_F64;
   c->use_graph = 0;
   c->coarse_op = 0;
+  c->dof = 1;
+  c->mu = 1.0;
+  c->lambda = 1.0;
 }
 
 }  // extern "C"
@@ -995,7 +1313,7 @@ dg_status extend_hierarchy(std::vector<Level>& lv, size_t L, cudaStream_t s) {
 }
 
 dg_status finish_create(dg_damg* m) {
-  const int64_t N = m->lv[0].da->N;
+  const int64_t N = int64_t(m->cfg.dof) * m->lv[0].da->N;
   DG_TRY(m->r.alloc(N));
   DG_TRY(m->z.alloc(N));
   DG_TRY(m->p.alloc(N));
@@ -1091,6 +1409,9 @@ dg_status dg_damg_create_batch(const dg_octree* const* finest, int count, const 
   auto m = std::make_unique<dg_damg>();
   if (cfg) m->cfg = *cfg; else dg_damg_default_config(&m->cfg);
   DG_CHECK(m->cfg.nlevels >= 1, DG_EINVAL, "damg_create: nlevels must be >= 1");
+  DG_CHECK(m->cfg.dof == 1 || m->cfg.dof == 3, DG_EINVAL, "damg_create: dof must be 1 or 3");
+  DG_CHECK(m->cfg.dof == 1 || (count == 1 && m->cfg.inner_prec == DG_PREC_F64 && m->cfg.coarse_op == 0),
+           DG_ENOTIMPL, "damg_create: dof 3 (elasticity) is one mesh with the FP64 V-cycle and coarse_op 0");
   DG_CUDA(cudaStreamCreateWithFlags(&m->s, cudaStreamNonBlocking));
   cudaStream_t s = m->s;
   m->nmesh = count;
@@ -1182,7 +1503,8 @@ dg_status dg_damg_prolong(dg_damg* m, int level, const double* xc, double* xf, i
   DG_CHECK(m && level >= 0 && level + 1 < int(m->lv.size()), DG_EINVAL, "damg_prolong: bad level");
   Level& F = m->lv[level];
   Level& C = m->lv[level + 1];
-  const int64_t nf = F.da->N, nc = C.da->N;
+  const int dof = m->cfg.dof;
+  const int64_t nf = dof * F.da->N, nc = dof * C.da->N;
   DBuf<double> dc, df;
   const double* pc = xc;
   double* pf = xf;
@@ -1195,7 +1517,10 @@ dg_status dg_damg_prolong(dg_damg* m, int level, const double* xc, double* xf, i
     pf = df.p;
   }
   if (on_device) DG_CUDA(cudaDeviceSynchronize());
-  prolong_add<<<grid_for(nf, 256), 256, 0, m->s>>>(F.pptr.p, F.pcol.p, F.pval.p, nf, pc, pf);
+  if (dof == 3)
+    prolong_add3<<<grid_for(F.da->N, 256), 256, 0, m->s>>>(F.pptr.p, F.pcol.p, F.pval.p, F.da->N, pc, pf);
+  else
+    prolong_add<<<grid_for(nf, 256), 256, 0, m->s>>>(F.pptr.p, F.pcol.p, F.pval.p, nf, pc, pf);
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaStreamSynchronize(m->s));
   if (!on_device) DG_CUDA(cudaMemcpy(xf, df.p, 8 * nf, cudaMemcpyDeviceToHost));
@@ -1206,7 +1531,8 @@ dg_status dg_damg_restrict(dg_damg* m, int level, const double* rf, double* rc, 
   DG_CHECK(m && level >= 0 && level + 1 < int(m->lv.size()), DG_EINVAL, "damg_restrict: bad level");
   Level& F = m->lv[level];
   Level& C = m->lv[level + 1];
-  const int64_t nf = F.da->N, nc = C.da->N;
+  const int dof = m->cfg.dof;
+  const int64_t nf = dof * F.da->N, nc = dof * C.da->N;
   DBuf<double> dc, df;
   const double* pf = rf;
   double* pc = rc;
@@ -1218,7 +1544,10 @@ dg_status dg_damg_restrict(dg_damg* m, int level, const double* rf, double* rc, 
     pc = dc.p;
   }
   if (on_device) DG_CUDA(cudaDeviceSynchronize());
-  restrict_gather<<<grid_for(nc, 256, 16), 256, 0, m->s>>>(F.rptr.p, F.rcol.p, F.rval.p, nc, pf, pc);
+  if (dof == 3)
+    restrict_gather3<<<grid_for(C.da->N, 256, 16), 256, 0, m->s>>>(F.rptr.p, F.rcol.p, F.rval.p, C.da->N, pf, pc);
+  else
+    restrict_gather<<<grid_for(nc, 256, 16), 256, 0, m->s>>>(F.rptr.p, F.rcol.p, F.rval.p, nc, pf, pc);
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaStreamSynchronize(m->s));
   if (!on_device) DG_CUDA(cudaMemcpy(rc, dc.p, 8 * nc, cudaMemcpyDeviceToHost));
@@ -1230,7 +1559,7 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
   DG_CHECK(m && b && x, DG_EINVAL, "damg_solve: bad arguments");
   cudaStream_t s = m->s;
   Level& L = m->lv[0];
-  const int64_t n = L.da->N;
+  const int64_t n = int64_t(m->cfg.dof) * L.da->N;
   const unsigned g = grid_for(n, 256);
   DBuf<double> db, dx;
   const double* pb = b;
@@ -1283,7 +1612,7 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
     DG_CUDA(cudaMemcpyAsync(m->p.p, m->z.p, 8 * n, cudaMemcpyDeviceToDevice, s));
     DG_TRY(dot(m, m->r.p, m->z.p, n, sc + 1));
     for (it = 1; it <= m->cfg.maxit; ++it) {
-      DG_TRY(lapmass_apply_f64(L.A.get(), m->p.p, m->q.p, s));
+      DG_TRY(level_op(L, m->p.p, m->q.p, s));
       DG_TRY(dot(m, m->p.p, m->q.p, n, sc + 2));
       cg_update<<<kRedBlocks, 256, 0, s>>>(px, m->r.p, m->p.p, m->q.p, n, sc + 1, sc + 2, m->part.p);
       finish_sum<<<1, 256, 0, s>>>(m->part.p, kRedBlocks, sc + 3);
@@ -1363,6 +1692,7 @@ dg_status dg_vec_dot(const double* x, const double* y, int64_t n, double* result
 
 dg_status dg_damg_set_smoother(dg_damg* m, dg_mlp* mlp, int sweeps, double fallback_ratio) {
   DG_CHECK(m && sweeps >= 1 && fallback_ratio > 0, DG_EINVAL, "damg_set_smoother: bad arguments");
+  DG_CHECK(!mlp || m->cfg.dof == 1, DG_ENOTIMPL, "damg_set_smoother: the learned smoother is scalar (dof 1)");
   DG_CHECK(!mlp || m->cfg.inner_prec != DG_PREC_F64, DG_EINVAL,
            "damg_set_smoother: the learned smoother runs in the FP32 inner V-cycle (inner_prec F32)");
   if (mlp) DG_TRY(ensure_smoother_data(m));
@@ -1399,8 +1729,8 @@ dg_status dg_damg_features(dg_damg* m, const double* r, float* F, float* scale) 
 dg_status dg_damg_level_apply(dg_damg* m, int level, const double* x, double* y, int on_device) {
   DG_CHECK(m && x && y && level >= 0 && size_t(level) < m->lv.size(), DG_EINVAL, "damg_level_apply: bad arguments");
   Level& L = m->lv[size_t(level)];
-  DG_CHECK(L.A && L.A->kind == 0, DG_EINVAL, "damg_level_apply: no Laplacian-mass operator set");
-  const int64_t n = L.da->N;
+  DG_CHECK(L.A, DG_EINVAL, "damg_level_apply: no operator set");
+  const int64_t n = int64_t(L.A->dof) * L.da->N;
   const double* xd = x;
   double* yd = y;
   if (!on_device) {
@@ -1408,7 +1738,8 @@ dg_status dg_damg_level_apply(dg_damg* m, int level, const double* x, double* y,
     xd = L.x.p;
     yd = L.b.p;
   }
-  DG_TRY(lapmass_apply_j_f64(L.A.get(), L.jcoef(), L.jset(), xd, yd, m->s));
+  if (L.A->kind == 1) DG_TRY(elasticity_apply_f64(L.A.get(), xd, yd, m->s));
+  else DG_TRY(lapmass_apply_j_f64(L.A.get(), L.jcoef(), L.jset(), xd, yd, m->s));
   if (!on_device) DG_CUDA(cudaMemcpyAsync(y, L.b.p, 8 * n, cudaMemcpyDeviceToHost, m->s));
   DG_CUDA(cudaStreamSynchronize(m->s));
   return DG_OK;
@@ -1449,7 +1780,7 @@ dg_status dg_damg_level_coef(dg_damg* m, int level, double* coef) {
 dg_status dg_damg_coarse_solve(dg_damg* m, const double* b, double* x, void* stream) {
   DG_CHECK(m && b && x && !m->lv.empty(), DG_EINVAL, "damg_coarse_solve: bad arguments");
   DG_CHECK(m->lv.back().A, DG_EINVAL, "damg_coarse_solve: no operator set");
-  const int64_t n = m->lv.back().da->N;
+  const int64_t n = int64_t(m->cfg.dof) * m->lv.back().da->N;
   auto s = static_cast<cudaStream_t>(stream);
   dense_gemv<<<grid_for(n * 32, 256), 256, 0, s>>>(m->Ainv.p, n, m->d_crow_blk.p, m->d_cb_off.p, m->d_cb_n.p,
                                                    m->d_cb_aoff.p, b, x);
@@ -1459,7 +1790,7 @@ dg_status dg_damg_coarse_solve(dg_damg* m, const double* b, double* x, void* str
 
 dg_status dg_damg_vcycle(dg_damg* m, const double* b, double* x) {
   DG_CHECK(m && b && x, DG_EINVAL, "damg_vcycle: bad arguments");
-  const int64_t n = m->lv[0].da->N;
+  const int64_t n = int64_t(m->cfg.dof) * m->lv[0].da->N;
   DG_CUDA(cudaDeviceSynchronize());
   DG_CUDA(cudaMemcpyAsync(m->r.p, b, 8 * n, cudaMemcpyDeviceToDevice, m->s));
   DG_TRY(precond_body(m));

@@ -241,6 +241,12 @@ typedef struct dg_damg_config {
                            a coarse element whose 8 children's coefficients differ takes the sum of the
                            children's operators, the type-1 stencils); the Jacobi diagonal is the averaged
                            operator's either way, as the reference's B matrix */
+  int dof;              /* degrees of freedom per node (DAMGCreateAndSetDA's dof, include/omg/omg.h:470-473):
+                           1 the Laplacian + mass operator; 3 linear elasticity (ElasticityMatMult,
+                           examples/src/backend/elasticityJac.C:130-230) on every level with that level's
+                           boundary nodes as Dirichlet nodes, as examples/src/drivers/newElasSolver.C:279-361
+                           sets it up (FP64 V-cycle, single mesh, coarse_op 0) */
+  double mu, lambda;    /* Lame parameters of the dof-3 operator (SetElasticityContexts defaults: 1, 1) */
 } dg_damg_config;
 
 typedef struct dg_solve_report {

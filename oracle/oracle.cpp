@@ -770,10 +770,23 @@ struct Level {
   std::vector<double> r, b, x, t;
 };
 
+// Profile (envelope) Cholesky of a sparse SPD matrix in reverse Cuthill-McKee
+// order: row i of L holds columns first[i] .. i, and the factor never fills
+// outside that envelope.  Used for coarsest levels too large for the dense
+// factor; PETSc's coarse LU (bin/options: -mg_coarse_pc_type lu) is a sparse
+// direct solve as well, so the two agree up to rounding.
+struct Envelope {
+  size_t n = 0;
+  std::vector<uint32_t> perm, iperm;  // perm[new] = old, iperm[old] = new
+  std::vector<size_t> first, start;   // per row: first column, offset of L[i][first[i]] in val
+  std::vector<double> val;
+};
+
 struct Hierarchy {
   std::vector<Level> lv;  // lv[0] finest
   int coarse_op = 0;      // 1: levels below the finest apply Jacobian3 (J); diag stays type 2 (B)
   std::vector<double> chol;  // dense Cholesky of the coarsest operator
+  Envelope env;              // or its envelope Cholesky (large coarsest levels)
   size_t nc = 0;
   int nu_pre = 2, nu_post = 2;
   double omega = 2.0 / 3.0;
@@ -790,10 +803,166 @@ void level_apply(const Hierarchy& H, size_t l, const double* x, double* y) {
   matvec(L.mesh, L.coef.empty() ? nullptr : L.coef.data(), x, y);
 }
 
+// Node adjacency of a mesh: two nodes are coupled when an element lists both
+// (a hanging vertex's interpolation nodes are among its element's 8 listed
+// nodes, so the element couples exactly its listed nodes).
+std::vector<std::vector<uint32_t>> node_graph(const Mesh& M) {
+  std::vector<std::vector<uint32_t>> adj(M.N);
+  for (size_t e = 0; e < M.E; ++e)
+    for (int a = 0; a < 8; ++a)
+      for (int b = 0; b < 8; ++b) adj[M.nlist[8 * e + a]].push_back(M.nlist[8 * e + b]);
+  for (auto& v : adj) {
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+  }
+  return adj;
+}
+
+// Reverse Cuthill-McKee order, component by component, each started from a
+// pseudo-peripheral node (the last node reached by a BFS from a minimum-degree
+// node).
+std::vector<uint32_t> rcm_order(const std::vector<std::vector<uint32_t>>& adj) {
+  const size_t n = adj.size();
+  std::vector<uint32_t> order;
+  order.reserve(n);
+  std::vector<char> seen(n, 0);
+  std::vector<uint32_t> queue;
+  auto bfs = [&](uint32_t s, std::vector<char>& mark, std::vector<uint32_t>& out) {
+    out.clear();
+    out.push_back(s);
+    mark[s] = 1;
+    for (size_t h = 0; h < out.size(); ++h) {
+      const uint32_t u = out[h];
+      std::vector<uint32_t> nb;
+      for (uint32_t w : adj[u])
+        if (!mark[w]) {
+          mark[w] = 1;
+          nb.push_back(w);
+        }
+      std::sort(nb.begin(), nb.end(), [&](uint32_t a, uint32_t b) {
+        return adj[a].size() != adj[b].size() ? adj[a].size() < adj[b].size() : a < b;
+      });
+      out.insert(out.end(), nb.begin(), nb.end());
+    }
+  };
+  for (size_t s0 = 0; s0 < n; ++s0) {
+    if (seen[s0]) continue;
+    // the component of s0 and its minimum-degree node
+    std::vector<char> mark(seen);
+    bfs(uint32_t(s0), mark, queue);
+    uint32_t start = queue[0];
+    for (uint32_t u : queue)
+      if (adj[u].size() < adj[start].size()) start = u;
+    mark = seen;
+    bfs(start, mark, queue);
+    start = queue.back();
+    mark = seen;
+    bfs(start, mark, queue);
+    for (uint32_t u : queue) seen[u] = 1;
+    order.insert(order.end(), queue.begin(), queue.end());
+  }
+  std::reverse(order.begin(), order.end());
+  return order;
+}
+
+// Assemble the coarsest operator by probing (columns of one colour of a
+// distance-2 colouring share one product with the level operator) into the
+// envelope of its RCM order, then factor in place.
+int envelope_factor(Hierarchy& H) {
+  const size_t l = H.lv.size() - 1;
+  const Mesh& M = H.lv[l].mesh;
+  const size_t n = M.N;
+  Envelope& V = H.env;
+  std::vector<std::vector<uint32_t>> adj = node_graph(M);
+  V.n = n;
+  V.perm = rcm_order(adj);
+  V.iperm.assign(n, 0);
+  for (size_t i = 0; i < n; ++i) V.iperm[V.perm[i]] = uint32_t(i);
+  V.first.assign(n, 0);
+  V.start.assign(n + 1, 0);
+  for (size_t i = 0; i < n; ++i) {
+    size_t f = i;
+    for (uint32_t w : adj[V.perm[i]]) f = std::min<size_t>(f, V.iperm[w]);
+    V.first[i] = f;
+    V.start[i + 1] = V.start[i] + (i - f + 1);
+  }
+  V.val.assign(V.start[n], 0.0);
+  // distance-2 colouring, greedy in node order
+  std::vector<int> colour(n, -1);
+  int ncol = 0;
+  std::vector<int> used;
+  for (size_t j = 0; j < n; ++j) {
+    used.clear();
+    for (uint32_t i : adj[j])
+      for (uint32_t k : adj[i])
+        if (colour[k] >= 0) used.push_back(colour[k]);
+    std::sort(used.begin(), used.end());
+    int c = 0;
+    for (int u : used) {
+      if (u == c) ++c;
+      else if (u > c) break;
+    }
+    colour[j] = c;
+    ncol = std::max(ncol, c + 1);
+  }
+  std::vector<double> e(n), y(n);
+  for (int c = 0; c < ncol; ++c) {
+    for (size_t j = 0; j < n; ++j) e[j] = colour[j] == c ? 1.0 : 0.0;
+    level_apply(H, l, e.data(), y.data());
+    for (size_t j = 0; j < n; ++j) {
+      if (colour[j] != c) continue;
+      const size_t pj = V.iperm[j];
+      for (uint32_t i : adj[j]) {  // column j: A[i][j] = y[i]
+        const size_t pi = V.iperm[i];
+        if (pj <= pi) V.val[V.start[pi] + (pj - V.first[pi])] = y[i];
+      }
+    }
+  }
+  // row-oriented Cholesky inside the envelope
+  for (size_t i = 0; i < n; ++i) {
+    double* Li = &V.val[V.start[i]] - V.first[i];  // Li[k], k in [first[i], i]
+    for (size_t j = V.first[i]; j < i; ++j) {
+      const double* Lj = &V.val[V.start[j]] - V.first[j];
+      double t = Li[j];
+      for (size_t k = std::max(V.first[i], V.first[j]); k < j; ++k) t -= Li[k] * Lj[k];
+      Li[j] = t / Lj[j];
+    }
+    double d = Li[i];
+    for (size_t k = V.first[i]; k < i; ++k) d -= Li[k] * Li[k];
+    if (!(d > 0)) return -1;
+    Li[i] = std::sqrt(d);
+  }
+  return 0;
+}
+
+void envelope_solve(const Envelope& V, const double* b, double* x) {
+  const size_t n = V.n;
+  std::vector<double> w(n);
+  for (size_t i = 0; i < n; ++i) w[i] = b[V.perm[i]];
+  for (size_t i = 0; i < n; ++i) {  // L w' = w
+    const double* Li = &V.val[V.start[i]] - V.first[i];
+    double t = w[i];
+    for (size_t k = V.first[i]; k < i; ++k) t -= Li[k] * w[k];
+    w[i] = t / Li[i];
+  }
+  for (size_t i = n; i-- > 0;) {  // L^T x = w', column by column
+    const double* Li = &V.val[V.start[i]] - V.first[i];
+    w[i] /= Li[i];
+    for (size_t k = V.first[i]; k < i; ++k) w[k] -= Li[k] * w[i];
+  }
+  for (size_t i = 0; i < n; ++i) x[V.perm[i]] = w[i];
+}
+
+// Coarsest levels above this many nodes use the envelope factor.
+constexpr size_t kDenseCoarseMax = 4096;
+
 int assemble_and_factor(Hierarchy& H) {
   Level& L = H.lv.back();
   size_t n = L.mesh.N;
   H.nc = n;
+  H.env = Envelope();
+  H.chol.clear();
+  if (n > kDenseCoarseMax) return envelope_factor(H);
   H.chol.assign(n * n, 0.0);
   std::vector<double> e(n, 0.0), col(n);
   for (size_t j = 0; j < n; ++j) {
@@ -819,6 +988,10 @@ int assemble_and_factor(Hierarchy& H) {
 }
 
 void chol_solve(const Hierarchy& H, const double* b, double* x) {
+  if (H.env.n) {
+    envelope_solve(H.env, b, x);
+    return;
+  }
   size_t n = H.nc;
   const double* A = H.chol.data();
   for (size_t i = 0; i < n; ++i) {

@@ -22,6 +22,8 @@ operators and the transfers.
 """
 from __future__ import annotations
 
+import hashlib
+import math
 import os
 import shutil
 import subprocess
@@ -215,6 +217,49 @@ def io_fixture(tmp, name):
                         nl=rd("m_NL_0_1.out"), el=rd("m_EL_0_1.out"), m=rd("m_M_0_1.out"))
 
 
+CFG1 = "gauss131k_d10"  # 131,072 points N(0.5, 0.1) (seed 0), maxDepth 10
+CFG1_PROJECTIONS = 4
+
+
+def digest(a):
+    """sha256 of an array's uint32 bytes (C order)."""
+    return hashlib.sha256(np.ascontiguousarray(a, np.uint32).tobytes()).hexdigest()
+
+
+def projections(y, k=CFG1_PROJECTIONS, seed=77):
+    """y projected on k seeded unit vectors (a size-independent check of y)."""
+    g = np.random.default_rng(seed).normal(size=(k, len(y)))
+    g /= np.linalg.norm(g, axis=1, keepdims=True)
+    return np.array([math.fsum(gi * y) for gi in g])
+
+
+def cfg1_fixture(tmp):
+    """The reference at the full size of the small configuration: its balance of
+    the oracle's linear octree, its DA maps and one Jacobian2MatMult with
+    constant coefficients (x = U[-1, 1], seed 1), kept as digests (sha256 of the
+    integer arrays; norm, sum and seeded projections of y) because the arrays
+    themselves run to tens of megabytes."""
+    pts, depth = I.workload_points(CFG1)
+    lin = O.points2octree(pts, depth, 1)
+    octs_to_u32(lin).tofile(os.path.join(tmp, "lin.u32"))
+    run("balance", os.path.join(tmp, "lin.u32"), depth, tmp)
+    bal = read_octs(os.path.join(tmp, "bal.u32"))
+    bal.tofile(os.path.join(tmp, "bal_in.u32"))
+    run("mesh", os.path.join(tmp, "bal_in.u32"), depth, tmp)
+    elem = np.fromfile(os.path.join(tmp, "elem.u32"), np.uint32).reshape(-1, 14)
+    node_xyz = np.fromfile(os.path.join(tmp, "node_xyz.u32"), np.uint32).reshape(-1, 3)
+    N = len(node_xyz)
+    x = I.uniform_rhs(N, 1)
+    x.tofile(os.path.join(tmp, "x.f64"))
+    run("matvec", os.path.join(tmp, "bal_in.u32"), depth, os.path.join(tmp, "x.f64"), "none",
+        os.path.join(tmp, "y.f64"))
+    y = np.fromfile(os.path.join(tmp, "y.f64"))
+    np.savez_compressed(os.path.join(OUT, f"cfg1_{CFG1}.npz"), depth=depth, n_lin=len(lin), n_bal=len(bal),
+                        E=len(elem), N=N, bal_sha=digest(bal), maps_sha=digest(elem[:, 3:]),
+                        node_sha=digest(node_xyz), y_norm=np.linalg.norm(y), y_sum=math.fsum(y),
+                        y_proj=projections(y))
+
+
 def table_digest(a):
     """Checksums of each (child number, type) table: sum, sum of squares,
     sum of magnitudes and a position-weighted sum."""
@@ -255,6 +300,10 @@ def main():
             jac3_fixture(tmp)
         stencil_digests()
         return
+    if "--cfg1-only" in sys.argv:
+        with tempfile.TemporaryDirectory() as tmp:
+            cfg1_fixture(tmp)
+        return
     if "--io-only" in sys.argv:
         with tempfile.TemporaryDirectory() as tmp:
             for name in IO_CASES:
@@ -270,6 +319,7 @@ def main():
             dirichlet_fixture(tmp, name)
         for name in IO_CASES:
             io_fixture(tmp, name)
+        cfg1_fixture(tmp)
     stencil_digests()
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):

@@ -575,6 +575,25 @@ void elasticity_matvec(const Mesh& M, double mu, double lam, const uint8_t* bdy,
   }
 }
 
+// ELASTICITY_DIAG_BLOCK (examples/src/backend/elasticityJac.C:60-100): the
+// diagonal of the element tables; 1 on Dirichlet rows.
+void elasticity_diagonal(const Mesh& M, double mu, double lam, const uint8_t* bdy, double* d) {
+  const Tables& T = tables();
+  std::fill(d, d + 3 * M.N, 0.0);
+  for (size_t e = 0; e < M.E; ++e) {
+    double fac = std::ldexp(1.0, 1 - int(M.elev[e])) / 2.0;
+    const uint32_t* idx = &M.nlist[8 * e];
+    uint32_t c = M.cnum[e], t = M.etype[e];
+    for (int k = 0; k < 8; ++k) {
+      if (bdy[idx[k]]) continue;
+      for (int p = 0; p < 3; ++p)
+        d[3 * idx[k] + p] += mu * fac * T.L[c][t][k][k] + (mu + lam) * fac * T.GD[c][t][3 * k + p][3 * k + p];
+    }
+  }
+  for (size_t i = 0; i < M.N; ++i)
+    if (bdy[i]) d[3 * i] = d[3 * i + 1] = d[3 * i + 2] = 1.0;
+}
+
 // ---------------------------------------------------------------- transfer --
 // Prolongation P (fine nodes x coarse nodes): the coarse conforming FE
 // function evaluated at each fine node, i.e. what prolongMatVecType1
@@ -632,6 +651,23 @@ void restrict_(const CSR& P, size_t nf, size_t nc, const double* rf, double* rc)
   std::fill(rc, rc + nc, 0.0);
   for (size_t f = 0; f < nf; ++f)
     for (int64_t k = P.ptr[f]; k < P.ptr[f + 1]; ++k) rc[P.col[k]] += P.val[k] * rf[f];
+}
+// The same transfers on dof interleaved components, each component moved by
+// the scalar entries: the reference's transfer loops apply one R entry to
+// every dof (RestrictMatVec.C:109-115); its elasticity driver creates the
+// transfers before the suppressed-DOF arrays exist (DAMGSetUp inside
+// DAMGCreateAndSetDA, omg.C:2167, copies their null pointers, omg.C:2259-2260),
+// so no Dirichlet dof is suppressed.
+void prolong_add_dof(const CSR& P, size_t nf, int dof, const double* xc, double* xf) {
+  for (size_t f = 0; f < nf; ++f)
+    for (int64_t k = P.ptr[f]; k < P.ptr[f + 1]; ++k)
+      for (int d = 0; d < dof; ++d) xf[dof * f + d] += P.val[k] * xc[size_t(dof) * P.col[k] + d];
+}
+void restrict_dof(const CSR& P, size_t nf, size_t nc, int dof, const double* rf, double* rc) {
+  std::fill(rc, rc + dof * nc, 0.0);
+  for (size_t f = 0; f < nf; ++f)
+    for (int64_t k = P.ptr[f]; k < P.ptr[f + 1]; ++k)
+      for (int d = 0; d < dof; ++d) rc[size_t(dof) * P.col[k] + d] += P.val[k] * rf[dof * f + d];
 }
 
 // Coefficients of a coarse level (ASSIGN_MAT_PROP_FINE_TO_COARSE_ELEM_BLOCK,
@@ -788,6 +824,8 @@ struct Hierarchy {
   std::vector<double> chol;  // dense Cholesky of the coarsest operator
   Envelope env;              // or its envelope Cholesky (large coarsest levels)
   size_t nc = 0;
+  int dof = 1;               // 3: linear elasticity on every level, its boundary nodes Dirichlet
+  double mu = 1.0, lam = 1.0;
   int nu_pre = 2, nu_post = 2;
   double omega = 2.0 / 3.0;
 };
@@ -796,6 +834,10 @@ struct Hierarchy {
 // coarse_op 1 below the finest level Jacobian3 from the finer level's.
 void level_apply(const Hierarchy& H, size_t l, const double* x, double* y) {
   const Level& L = H.lv[l];
+  if (H.dof == 3) {
+    elasticity_matvec(L.mesh, H.mu, H.lam, L.mesh.node_bdy.data(), x, y);
+    return;
+  }
   if (H.coarse_op == 1 && l > 0 && !H.lv[l - 1].coef.empty()) {
     jacobian3(H.lv[l - 1].mesh, H.lv[l - 1].coef.data(), L.mesh, x, y);
     return;
@@ -806,11 +848,14 @@ void level_apply(const Hierarchy& H, size_t l, const double* x, double* y) {
 // Node adjacency of a mesh: two nodes are coupled when an element lists both
 // (a hanging vertex's interpolation nodes are among its element's 8 listed
 // nodes, so the element couples exactly its listed nodes).
-std::vector<std::vector<uint32_t>> node_graph(const Mesh& M) {
-  std::vector<std::vector<uint32_t>> adj(M.N);
+std::vector<std::vector<uint32_t>> node_graph(const Mesh& M, int dof = 1) {
+  std::vector<std::vector<uint32_t>> adj(M.N * dof);
   for (size_t e = 0; e < M.E; ++e)
     for (int a = 0; a < 8; ++a)
-      for (int b = 0; b < 8; ++b) adj[M.nlist[8 * e + a]].push_back(M.nlist[8 * e + b]);
+      for (int b = 0; b < 8; ++b)
+        for (int p = 0; p < dof; ++p)
+          for (int q = 0; q < dof; ++q)
+            adj[size_t(dof) * M.nlist[8 * e + a] + p].push_back(uint32_t(dof * M.nlist[8 * e + b] + q));
   for (auto& v : adj) {
     std::sort(v.begin(), v.end());
     v.erase(std::unique(v.begin(), v.end()), v.end());
@@ -871,9 +916,9 @@ std::vector<uint32_t> rcm_order(const std::vector<std::vector<uint32_t>>& adj) {
 int envelope_factor(Hierarchy& H) {
   const size_t l = H.lv.size() - 1;
   const Mesh& M = H.lv[l].mesh;
-  const size_t n = M.N;
+  const size_t n = M.N * H.dof;
   Envelope& V = H.env;
-  std::vector<std::vector<uint32_t>> adj = node_graph(M);
+  std::vector<std::vector<uint32_t>> adj = node_graph(M, H.dof);
   V.n = n;
   V.perm = rcm_order(adj);
   V.iperm.assign(n, 0);
@@ -958,7 +1003,7 @@ constexpr size_t kDenseCoarseMax = 4096;
 
 int assemble_and_factor(Hierarchy& H) {
   Level& L = H.lv.back();
-  size_t n = L.mesh.N;
+  size_t n = L.mesh.N * H.dof;
   H.nc = n;
   H.env = Envelope();
   H.chol.clear();
@@ -1008,7 +1053,7 @@ void chol_solve(const Hierarchy& H, const double* b, double* x) {
 
 void vcycle(Hierarchy& H, size_t l, const double* b, double* x) {
   Level& L = H.lv[l];
-  size_t n = L.mesh.N;
+  size_t n = L.mesh.N * H.dof;
   if (l + 1 == H.lv.size()) {
     chol_solve(H, b, x);
     return;
@@ -1021,9 +1066,9 @@ void vcycle(Hierarchy& H, size_t l, const double* b, double* x) {
   level_apply(H, l, x, L.t.data());
   for (size_t i = 0; i < n; ++i) L.r[i] = b[i] - L.t[i];
   Level& C = H.lv[l + 1];
-  restrict_(L.P, n, C.mesh.N, L.r.data(), C.b.data());
+  restrict_dof(L.P, L.mesh.N, C.mesh.N, H.dof, L.r.data(), C.b.data());
   vcycle(H, l + 1, C.b.data(), C.x.data());
-  prolong_add(L.P, n, C.x.data(), x);
+  prolong_add_dof(L.P, L.mesh.N, H.dof, C.x.data(), x);
   for (int s = 0; s < H.nu_post; ++s) {
     level_apply(H, l, x, L.t.data());
     for (size_t i = 0; i < n; ++i) x[i] += H.omega * (b[i] - L.t[i]) / L.diag[i];
@@ -1165,9 +1210,20 @@ int orc_coarse_coef(void* fine, const double* fc, void* coarse, double* cc) {
 // Build the multigrid hierarchy (DAMGCreateAndSetDA, src/omg/omg.C:1306-1420):
 // coarsen + balance per level until nlevels or a level below 500 octants.
 // coef_mode 0: a = b = 1; 1: per-element coefficients given for the finest.
+void* orc_damg_create_dof(const orc_octant* finest, int64_t n, uint32_t maxDepth, int nlevels,
+                          const double* coef, int dof, double mu, double lam, int* status, int* levels_out);
 void* orc_damg_create(const orc_octant* finest, int64_t n, uint32_t maxDepth, int nlevels,
                       const double* coef, int* status, int* levels_out) {
+  return orc_damg_create_dof(finest, n, maxDepth, nlevels, coef, 1, 1.0, 1.0, status, levels_out);
+}
+// dof 3: ElasticityMatMult on every level with that level's boundary nodes
+// Dirichlet (SetElasticityContexts, examples/src/backend/elasticityJac.C:396-480).
+void* orc_damg_create_dof(const orc_octant* finest, int64_t n, uint32_t maxDepth, int nlevels,
+                          const double* coef, int dof, double mu, double lam, int* status, int* levels_out) {
   Hierarchy* H = new Hierarchy();
+  H->dof = dof;
+  H->mu = mu;
+  H->lam = lam;
   std::vector<std::vector<Oct>> trees;
   trees.push_back(from_c(finest, n));
   int idx = -1;
@@ -1194,9 +1250,12 @@ void* orc_damg_create(const orc_octant* finest, int64_t n, uint32_t maxDepth, in
   }
   for (size_t l = 0; l < H->lv.size(); ++l) {
     Level& L = H->lv[l];
-    size_t N = L.mesh.N;
+    size_t N = L.mesh.N * dof;
     L.diag.resize(N);
-    diagonal(L.mesh, L.coef.empty() ? nullptr : L.coef.data(), L.diag.data());
+    if (dof == 3)
+      elasticity_diagonal(L.mesh, mu, lam, L.mesh.node_bdy.data(), L.diag.data());
+    else
+      diagonal(L.mesh, L.coef.empty() ? nullptr : L.coef.data(), L.diag.data());
     L.r.assign(N, 0);
     L.b.assign(N, 0);
     L.x.assign(N, 0);
@@ -1259,8 +1318,7 @@ void orc_damg_vcycle(void* h, const double* b, double* x) {
 int orc_damg_pcg(void* h, const double* b, double* x, double rtol, int maxit, double* history) {
   Hierarchy* H = (Hierarchy*)h;
   Level& L = H->lv[0];
-  size_t n = L.mesh.N;
-  const double* cf = L.coef.empty() ? nullptr : L.coef.data();
+  size_t n = L.mesh.N * H->dof;
   std::vector<double> r(b, b + n), z(n), p(n), q(n);
   std::fill(x, x + n, 0.0);
   double bn = std::sqrt(dot(b, b, n));
@@ -1270,7 +1328,7 @@ int orc_damg_pcg(void* h, const double* b, double* x, double rtol, int maxit, do
   p = z;
   double rz = dot(r.data(), z.data(), n);
   for (int it = 1; it <= maxit; ++it) {
-    matvec(L.mesh, cf, p.data(), q.data());
+    level_apply(*H, 0, p.data(), q.data());
     double alpha = rz / dot(p.data(), q.data(), n);
     for (size_t i = 0; i < n; ++i) {
       x[i] += alpha * p[i];

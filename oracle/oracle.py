@@ -58,6 +58,9 @@ def lib():
         L.orc_damg_create.argtypes = [P, C.c_int64, C.c_uint32, C.c_int, P, C.POINTER(C.c_int),
                                       C.POINTER(C.c_int)]
         L.orc_damg_create.restype = P
+        L.orc_damg_create_dof.argtypes = [P, C.c_int64, C.c_uint32, C.c_int, P, C.c_int, C.c_double, C.c_double,
+                                          C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.orc_damg_create_dof.restype = P
         L.orc_damg_destroy.argtypes = [P]
         L.orc_damg_level_sizes.argtypes = [P, P, P]
         L.orc_damg_level_mesh.argtypes = [P, C.c_int]
@@ -247,12 +250,16 @@ def coarse_coef(fine: Mesh, fine_coef, coarse: Mesh):
 class DAMG:
     """Oracle multigrid hierarchy + FP64 PCG/V(2,2) solver."""
 
-    def __init__(self, finest: np.ndarray, max_depth: int, nlevels: int, coef=None):
+    def __init__(self, finest: np.ndarray, max_depth: int, nlevels: int, coef=None, dof: int = 1,
+                 mu: float = 1.0, lam: float = 1.0):
+        """dof 3: linear elasticity (mu, lam) on every level, each level's
+        boundary nodes Dirichlet, as the reference's elasticity driver."""
         finest = np.ascontiguousarray(finest, OCT_DTYPE)
         st, nl = C.c_int(), C.c_int()
         c = None if coef is None else np.ascontiguousarray(coef, np.float64)
-        self.h = lib().orc_damg_create(_ptr(finest), len(finest), max_depth, nlevels, _ptr(c),
-                                       C.byref(st), C.byref(nl))
+        self.dof = int(dof)
+        self.h = lib().orc_damg_create_dof(_ptr(finest), len(finest), max_depth, nlevels, _ptr(c), self.dof,
+                                           float(mu), float(lam), C.byref(st), C.byref(nl))
         if not self.h:
             raise ValueError("oracle DAMG create failed: %d" % st.value)
         self.nlevels = nl.value

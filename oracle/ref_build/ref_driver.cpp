@@ -19,6 +19,10 @@
 //       DAMGCreateAndSetDA + DAMGSetUp; per level the node anchors, and the
 //       restriction / prolongation of the vectors level<l>_in.f64 /
 //       coarse<l>_in.f64 found in outdir
+//   dendro_ref elastic_transfer <octs.u32> <maxDepth> <nlevels> <outdir>
+//       the elasticity solver's hierarchy (dof 3, suppressed DOFs, elasticity
+//       contexts); per level the boundary flags, and the restriction /
+//       prolongation of 3-dof vectors level<l>_in.f64 / coarse<l>_in.f64
 //   dendro_ref jac3 <octs.u32> <maxDepth> <nlevels> <outdir>
 //       DAMGCreateAndSetDA + DAMGSetUp, then per coarse level l (1 = next to
 //       the finest) Jacobian3MatMult (examples/src/backend/omgJac.C:2235) with
@@ -442,6 +446,45 @@ int main(int argc, char** argv) {
       VecDuplicate(vf, &of);
       MatMult(fine->R, vf, oc);           // restriction
       MatMultTranspose(fine->R, vc, of);  // prolongation
+      std::vector<double> r = vec_data(oc), p = vec_data(of);
+      write_raw(dir + "/restrict" + std::to_string(l) + ".f64", r.data(), r.size());
+      write_raw(dir + "/prolong" + std::to_string(l) + ".f64", p.data(), p.size());
+    }
+    return 0;
+  }
+  if (mode == "elastic_transfer" && argc >= 6) {
+    // The elasticity solver's set-up order (examples/src/drivers/newElasSolver.C:
+    // DAMGCreateAndSetDA with dof 3, DAMGCreateSuppressedDOFs,
+    // SetElasticityContexts), then the restriction / prolongation of 3-dof
+    // vectors level<l>_in.f64 / coarse<l>_in.f64 -> restrict<l>.f64 /
+    // prolong<l>.f64, and each level's boundary flags bdy<l>.u8
+    unsigned D = atoi(argv[3]);
+    int nlevels = atoi(argv[4]);
+    std::string dir = argv[5];
+    std::vector<ot::TreeNode> octs = read_octs(argv[2], D);
+    ot::DAMG* damg = NULL;
+    ot::DAMG_Initialize(MPI_COMM_WORLD);
+    ot::DAMGCreateAndSetDA(MPI_COMM_WORLD, nlevels, NULL, &damg, octs, 3, 1.5, false, true);
+    ot::DAMGCreateSuppressedDOFs(damg);
+    SetElasticityContexts(damg);
+    FILE* f = fopen((dir + "/levels.txt").c_str(), "w");
+    fprintf(f, "%d\n", nlevels);
+    fclose(f);
+    for (int l = 0; l < nlevels; ++l) {
+      ot::DA* da = damg[nlevels - 1 - l]->da;
+      std::vector<unsigned char> bdy;
+      assignBoundaryFlags(da, bdy);
+      write_raw(dir + "/bdy" + std::to_string(l) + ".u8", bdy.data(), bdy.size());
+    }
+    for (int l = 0; l + 1 < nlevels; ++l) {
+      ot::DAMG fine = damg[nlevels - 1 - l];
+      std::vector<double> xf = read_raw<double>(dir + "/level" + std::to_string(l) + "_in.f64");
+      std::vector<double> xc = read_raw<double>(dir + "/coarse" + std::to_string(l) + "_in.f64");
+      Vec vf = make_vec(xf), vc = make_vec(xc), of, oc;
+      VecDuplicate(vc, &oc);
+      VecDuplicate(vf, &of);
+      MatMult(fine->R, vf, oc);
+      MatMultTranspose(fine->R, vc, of);
       std::vector<double> r = vec_data(oc), p = vec_data(of);
       write_raw(dir + "/restrict" + std::to_string(l) + ".f64", r.data(), r.size());
       write_raw(dir + "/prolong" + std::to_string(l) + ".f64", p.data(), p.size());

@@ -147,6 +147,30 @@ def transfer_fixture(tmp):
     np.savez_compressed(os.path.join(OUT, f"transfer_{name}.npz"), **rec)
 
 
+def elastic_transfer_fixture(tmp):
+    """The reference's intergrid transfers of 3-dof vectors in the elasticity
+    solver's set-up order (dof 3, suppressed DOFs, elasticity contexts) and
+    each level's boundary flags, on the transfer case's hierarchy."""
+    name, nlevels = TRANSFER_CASE
+    pts, depth = MESH_CASES[name]()
+    bal = O.balance(O.points2octree(pts, depth, 1), depth)
+    octs_to_u32(bal).tofile(os.path.join(tmp, "bal_e.u32"))
+    dm = O.DAMG(bal, depth, nlevels)
+    rec = {"depth": depth, "nlevels": dm.nlevels, "bal": octs_to_u32(bal)}
+    for l in range(dm.nlevels - 1):
+        xf = np.random.default_rng(60 + l).uniform(-1, 1, 3 * int(dm.N[l]))
+        xc = np.random.default_rng(70 + l).uniform(-1, 1, 3 * int(dm.N[l + 1]))
+        xf.tofile(os.path.join(tmp, f"level{l}_in.f64"))  # inputs are regenerated from the seeds
+        xc.tofile(os.path.join(tmp, f"coarse{l}_in.f64"))
+    run("elastic_transfer", os.path.join(tmp, "bal_e.u32"), depth, nlevels, tmp)
+    for l in range(dm.nlevels):
+        rec[f"bdy{l}"] = np.fromfile(os.path.join(tmp, f"bdy{l}.u8"), np.uint8)
+    for l in range(dm.nlevels - 1):
+        rec[f"restrict{l}"] = np.fromfile(os.path.join(tmp, f"restrict{l}.f64"))
+        rec[f"prolong{l}"] = np.fromfile(os.path.join(tmp, f"prolong{l}.f64"))
+    np.savez_compressed(os.path.join(OUT, f"elastic_transfer_{name}.npz"), **rec)
+
+
 def dirichlet_fixture(tmp, name):
     """The reference's boundary flags (assignBoundaryFlags) and its Dirichlet
     Laplacian / Jacobian MatMult and GetDiagonal on the mesh case."""
@@ -300,6 +324,10 @@ def main():
             jac3_fixture(tmp)
         stencil_digests()
         return
+    if "--elastic-only" in sys.argv:
+        with tempfile.TemporaryDirectory() as tmp:
+            elastic_transfer_fixture(tmp)
+        return
     if "--cfg1-only" in sys.argv:
         with tempfile.TemporaryDirectory() as tmp:
             cfg1_fixture(tmp)
@@ -320,6 +348,7 @@ def main():
         for name in IO_CASES:
             io_fixture(tmp, name)
         cfg1_fixture(tmp)
+        elastic_transfer_fixture(tmp)
     stencil_digests()
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):

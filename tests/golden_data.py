@@ -100,3 +100,14 @@ def reference_matvec(bal_u32, depth, x, coef=None):
                            timeout=1200)
         assert r.returncode == 0, r.stderr[-2000:]
         return np.fromfile(os.path.join(tmp, "y.f64"))
+
+
+def elastic_inputs(g, sizes):
+    """The seeded 3-dof inputs of the elastic transfer fixture (fine, coarse)
+    per level, as make_golden.py drew them; sizes = node counts per level."""
+    out = []
+    for l in range(int(g["nlevels"]) - 1):
+        xf = np.random.default_rng(60 + l).uniform(-1, 1, 3 * int(sizes[l]))
+        xc = np.random.default_rng(70 + l).uniform(-1, 1, 3 * int(sizes[l + 1]))
+        out.append((xf, xc))
+    return out

@@ -61,6 +61,7 @@ typedef const char* PetscRandomType;
 #define PETSC_ERR_ARG_WRONG 62
 #define PETSC_ERR_SUP 56
 #define PETSC_ERR_MEM 55
+#define PETSC_ERR_LIB 76
 #define PETSC_ERR_USER 83
 #define PETSC_ERR_ARG_OUTOFRANGE 63
 #define PETSC_MAX_PATH_LEN 4096

@@ -59,6 +59,7 @@ def parse():
     p.add_argument("--no-solve", action="store_true")
     p.add_argument("--no-multi", action="store_true")
     p.add_argument("--no-batch", action="store_true")
+    p.add_argument("--no-cfg1", action="store_true")
     p.add_argument("--solve-workload", default="lognormal4m_d16")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--vcycle-profile", metavar="WORKLOAD", default=None,
@@ -199,7 +200,8 @@ def run_dendro(args, rank, world):
     kernel = A.kernel_name(0)
     multi = None if args.no_multi else run_multi(dev, min(args.steps, 50))
     batch = None if args.no_batch else run_batch(dev)
-    return dict(multi=multi, batch=batch, kernel=kernel, E=E, N=N, setup_s=setup_s, ms_per_step=ms_per_step, gdofs=gdofs, achieved=achieved, peak=peak,
+    cfg1 = None if args.no_cfg1 else run_cfg1(dev)
+    return dict(multi=multi, batch=batch, cfg1=cfg1, kernel=kernel, E=E, N=N, setup_s=setup_s, ms_per_step=ms_per_step, gdofs=gdofs, achieved=achieved, peak=peak,
                 peak_kind=peak_kind, alg_bytes=alg_bytes, clocks=clk, e2e=e2e, solve=solve, bal=bal, depth=depth,
                 coef=coef, x=x.cpu().numpy(), y=y.cpu().numpy())
 
@@ -267,6 +269,48 @@ def run_solve(dev, workload):
         "mixed_fp32_omega09": "mixed_fp32 with Jacobi damping omega 0.9",
         "mixed_fp32_learned": "mixed_fp32 with the trained MLP post-smoother on the finest level, Jacobi fallback "
                               "when the FP64 residual stalls"}
+    return out
+
+
+def run_cfg1(dev, matvecs=100):
+    """The small configuration in full on the GPU, with the set-up stages of
+    examples/src/drivers/tstMatVec.C:165-275 timed one by one: 131,072
+    Gaussian points (seed 0), maxDepth 10 -> points2Octree, 2:1 balance, the
+    mesh; 100 operator applications (a = b = 1); PCG with the 4-level V(2,2)
+    damped-Jacobi cycle (omega 2/3) to 1e-8 with f = U[-1, 1] (seed 1)."""
+    import torch
+
+    import dendro_b200 as dg
+    from dendro_b200 import inputs as I
+    pts, depth = build_workload("gauss131k_d10", 1.0)
+    out = {"workload": "gauss131k_d10"}
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return r, time.perf_counter() - t
+    lin, out["points2octree_s"] = timed(lambda: dg.points2Octree(pts, depth, 1))
+    bal, out["balance_s"] = timed(lambda: dg.balanceOctree(lin))
+    da, out["da_build_s"] = timed(lambda: dg.DA(bal))
+    out.update({"elements": da.E, "nodes": da.N})
+    A = dg.Jacobian2(da)
+    x = torch.tensor(I.uniform_rhs(da.N, 1), device=dev)
+    y = torch.empty_like(x)
+    for _ in range(3):
+        A.mult(x, y)
+    _, t = timed(lambda: [A.mult(x, y) for _ in range(matvecs)])
+    out["matvec_ms"] = round(1e3 * t / matvecs, 4)
+    out["matvec_gdofs"] = round(da.N * matvecs / t / 1e9, 3)
+    m = dg.DAMG(bal, nlevels=4)
+    b = torch.tensor(I.uniform_rhs(da.N, 1), device=dev)
+    m.solve(b)
+    xs, rep = m.solve(b)
+    out["pcg"] = {"levels": m.nlevels, "coarse_nodes": int(m.N[-1]), "iterations": rep["iterations"],
+                  "rel_residual": rep["rel_residual"], "solve_ms": round(rep["solve_ms"], 3)}
+    for k in ("points2octree_s", "balance_s", "da_build_s"):
+        out[k] = round(out[k], 4)
     return out
 
 
@@ -492,6 +536,7 @@ def main():
         "matvec_kernel": r["kernel"],
         "multi_rhs": r["multi"],
         "batch": r["batch"],
+        "cfg1": r["cfg1"],
         "setup_s": round(r["setup_s"], 3),
     }
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -526,6 +571,55 @@ def ref_processes(mem_per_proc_gb: float = 2.0, cap: int = 64) -> int:
     except Exception:
         avail = 8.0
     return max(1, min(cores, cap, int(avail * 0.6 / mem_per_proc_gb)))
+
+
+def reference_cfg1(matvecs=20):
+    """The small configuration on the CPU: the reference's own balance, DA
+    construction and Jacobian2MatMult (the compiled reference; its OpenMP
+    loops on every host core), and the oracle's restatement of the 4-level
+    V(2,2) PCG solve to 1e-8 (PETSc's CG and PCMG are not in the reference
+    tree).  The linear octree comes from the oracle: the reference's
+    points2Octree does not finish at this size."""
+    import tempfile
+
+    from dendro_b200 import inputs as I
+    from oracle import oracle as O
+    pts, depth = build_workload("gauss131k_d10", 1.0)
+    out = {"workload": "gauss131k_d10", "omp_threads": os.cpu_count()}
+    t = time.perf_counter()
+    lin = O.points2octree(pts, depth, 1)
+    out["points2octree_s_port"] = round(time.perf_counter() - t, 4)
+    tmp = tempfile.mkdtemp(prefix="dg_cfg1_")
+    np.stack([lin["x"], lin["y"], lin["z"], lin["lf"] & 31], 1).astype(np.uint32).tofile(os.path.join(tmp, "lin.u32"))
+    env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count()))
+    if os.path.exists(REF_BIN):
+        r = subprocess.run([REF_BIN, "timings", os.path.join(tmp, "lin.u32"), str(depth)], cwd=REF_STENCILS,
+                           capture_output=True, text=True, env=env, timeout=1800)
+        if r.returncode == 0:
+            nb, ne, tb, td = r.stderr.strip().splitlines()[-1].split()
+            out.update({"balance_s": float(tb), "da_build_s": float(td), "elements": int(ne)})
+    bal = O.balance(lin, depth)
+    mesh = O.Mesh(bal, depth)
+    x = I.uniform_rhs(mesh.N, 1)
+    out["nodes"] = mesh.N
+    if os.path.exists(REF_BIN):
+        np.stack([bal["x"], bal["y"], bal["z"], bal["lf"] & 31], 1).astype(np.uint32).tofile(os.path.join(tmp, "bal.u32"))
+        x.tofile(os.path.join(tmp, "x.f64"))
+        r = subprocess.run([REF_BIN, "matvec", os.path.join(tmp, "bal.u32"), str(depth), os.path.join(tmp, "x.f64"),
+                            "none", os.path.join(tmp, "y.f64"), str(matvecs)], cwd=REF_STENCILS, capture_output=True,
+                           text=True, timeout=1800)
+        if r.returncode == 0:
+            tm = float(r.stderr.strip().splitlines()[-1])
+            out["matvec_ms"] = round(1e3 * tm, 3)
+            out["matvec_gdofs"] = round(mesh.N / tm / 1e9, 5)
+            out["matvec_cores"] = 1
+    H = O.DAMG(bal, depth, 4)
+    b = I.uniform_rhs(mesh.N, 1)
+    t = time.perf_counter()
+    _, it, hist = H.pcg(b, 1e-8, 100)
+    out["pcg_port"] = {"levels": H.nlevels, "coarse_nodes": int(H.N[-1]), "iterations": int(it),
+                       "rel_residual": float(hist[-1]), "solve_s": round(time.perf_counter() - t, 3), "cores": 1}
+    return out
 
 
 def main_reference(args, rank, world):
@@ -589,6 +683,8 @@ def main_reference(args, rank, world):
                                                     f"(E={E}, N={N}) after one untimed"}})
             line["e2e"] = {"value": line["value"], "unit": "GDoF/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+            if not args.no_cfg1:
+                line["cfg1"] = reference_cfg1()
             print(json.dumps(line), flush=True)
             return
         mesh = O.Mesh(octs, depth)

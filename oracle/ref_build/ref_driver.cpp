@@ -7,6 +7,9 @@
 //       ot::points2Octree, ot::balanceOctree (incCorner), ot::coarsenOctree
 //   dendro_ref balance <octs.u32> <maxDepth> <outdir>
 //       ot::balanceOctree (incCorner) and ot::coarsenOctree of a linear octree
+//   dendro_ref timings <lin.u32> <maxDepth>
+//       seconds of ot::balanceOctree and of the DA construction (stderr:
+//       balanced octants, elements, balance s, DA s)
 //   dendro_ref mesh    <octs.u32> <maxDepth> <outdir>
 //       ot::DA maps: per element anchor, level, child number, hanging mask and
 //       the 8 node ids (Vec order), plus the node anchors
@@ -237,6 +240,21 @@ int main(int argc, char** argv) {
     write_octs(dir + "/bal.u32", bal);
     ot::coarsenOctree(bal, coarse);
     write_octs(dir + "/coarse.u32", coarse);
+    return 0;
+  }
+  if (mode == "timings" && argc >= 4) {
+    // the set-up stages of examples/src/drivers/tstMatVec.C:165-275 on a
+    // linear octree: balanceOctree, then the DA; seconds on stderr
+    unsigned D = atoi(argv[3]);
+    std::vector<ot::TreeNode> lin = read_octs(argv[2], D), bal;
+    auto t0 = std::chrono::steady_clock::now();
+    ot::balanceOctree(lin, bal, 3, D, true, MPI_COMM_WORLD, NULL, NULL);
+    auto t1 = std::chrono::steady_clock::now();
+    const size_t nbal = bal.size();
+    ot::DA da(bal, MPI_COMM_WORLD, MPI_COMM_WORLD, false);
+    auto t2 = std::chrono::steady_clock::now();
+    fprintf(stderr, "%zu %u %.6f %.6f\n", nbal, da.getElementSize(),
+            std::chrono::duration<double>(t1 - t0).count(), std::chrono::duration<double>(t2 - t1).count());
     return 0;
   }
   if (mode == "jac3" && argc >= 6) {

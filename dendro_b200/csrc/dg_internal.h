@@ -51,6 +51,7 @@ struct OctetSet {
   DBuf<uint32_t> cel;     // [2 nchunk]: first element id, element range length
   DBuf<uint16_t> lidx;    // [27][n]
   DBuf<uint16_t> lelem;   // [8][n]
+  DBuf<uint16_t> lnl;     // [8][E]: per element, the chunk-local index of each vertex's node (the DA's nl)
 };
 constexpr int kOctChunk = 128;  // octets per chunk (one per thread of the chunked kernel)
 }  // namespace dg

@@ -1851,6 +1851,103 @@ __global__ void __launch_bounds__(128) elasticity_kernel(const uint32_t* __restr
   }
 }
 
+// Chunked form (the octet chunks of the mesh, OctetSet): a CTA per chunk
+// stages x at the chunk's nodes (3 components) and their Dirichlet flags in
+// shared memory with coalesced loads, applies every element of the chunk's
+// octets (one thread per element, the same element arithmetic as above) with
+// x read from shared memory and the 24 results added into a shared
+// accumulator, then writes the chunk's node sums with stores (nodes no other
+// chunk touches) or global reductions.  Dirichlet rows are set afterwards by
+// elasticity_dirichlet_rows, as for the kernel above.
+constexpr int kElasChunkThreads = 256;
+__global__ void __launch_bounds__(kElasChunkThreads, 2) elasticity_chunk_kernel(
+    int64_t n, int64_t nchunk, uint32_t node_cap, const uint32_t* __restrict__ oelem, const uint16_t* __restrict__ lnl,
+    const uint32_t* __restrict__ cptr, const uint32_t* __restrict__ cnodes, const uint32_t* __restrict__ meta,
+    const uint8_t* __restrict__ dir, int64_t E, double mu, double lam, const double* __restrict__ x,
+    double* __restrict__ y) {
+  extern __shared__ __align__(16) unsigned char el_smem[];
+  double* sx = reinterpret_cast<double*>(el_smem);
+  double* sy = sx + 3 * size_t(node_cap);
+  uint8_t* sd = reinterpret_cast<uint8_t*>(sy + 3 * size_t(node_cap));
+  for (int64_t q = blockIdx.x; q < nchunk; q += gridDim.x) {
+    const uint32_t p0 = __ldg(cptr + q), nn = __ldg(cptr + q + 1) - p0;
+    for (uint32_t k = threadIdx.x; k < nn; k += kElasChunkThreads) {
+      const uint32_t id = __ldg(cnodes + p0 + k) & 0x7fffffffu;
+      sd[k] = __ldg(dir + id);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        sx[3 * k + a] = __ldg(x + 3 * int64_t(id) + a);
+        sy[3 * k + a] = 0.0;
+      }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 8 * kOctChunk; i += kElasChunkThreads) {
+      const int c = i / kOctChunk;
+      const int64_t o = q * kOctChunk + (i - c * kOctChunk);
+      if (o >= n) continue;
+      const uint32_t e = __ldg(oelem + int64_t(c) * n + o);
+      if (e == kNoNode) continue;
+      const uint32_t m = __ldg(meta + e);
+      const uint32_t lev = meta_lev(m), cn = meta_cnum(m), mask = meta_mask(m);
+      const double fac = elem_h<double>(lev) / 2.0;
+      uint32_t li[8];
+      bool bd[8];
+      double u0[8], u1[8], u2[8];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) {
+        li[v] = __ldg(lnl + int64_t(v) * E + e);
+        bd[v] = sd[li[v]] != 0;
+        u0[v] = bd[v] ? 0.0 : sx[3 * li[v]];
+        u1[v] = bd[v] ? 0.0 : sx[3 * li[v] + 1];
+        u2[v] = bd[v] ? 0.0 : sx[3 * li[v] + 2];
+      }
+      if (mask) {
+        interp_hanging(u0, cn, mask);
+        interp_hanging(u1, cn, mask);
+        interp_hanging(u2, cn, mask);
+      }
+      double r0[8], r1[8], r2[8];
+      const double wl = mu * fac, wg = (mu + lam) * fac;
+      lapmass_ref_to(u0, wl, 0.0, r0);
+      lapmass_ref_to(u1, wl, 0.0, r1);
+      lapmass_ref_to(u2, wl, 0.0, r2);
+      graddiv_block<0, 0>(u0, wg, r0);
+      graddiv_block<0, 1>(u1, wg, r0);
+      graddiv_block<0, 2>(u2, wg, r0);
+      graddiv_block<1, 0>(u0, wg, r1);
+      graddiv_block<1, 1>(u1, wg, r1);
+      graddiv_block<1, 2>(u2, wg, r1);
+      graddiv_block<2, 0>(u0, wg, r2);
+      graddiv_block<2, 1>(u1, wg, r2);
+      graddiv_block<2, 2>(u2, wg, r2);
+      if (mask) {
+        scatter_hanging(r0, cn, mask);
+        scatter_hanging(r1, cn, mask);
+        scatter_hanging(r2, cn, mask);
+      }
+#pragma unroll
+      for (int v = 0; v < 8; ++v) {
+        if (bd[v]) continue;
+        double* t = sy + 3 * li[v];
+        if (r0[v] != 0.0) atomicAdd(t, r0[v]);
+        if (r1[v] != 0.0) atomicAdd(t + 1, r1[v]);
+        if (r2[v] != 0.0) atomicAdd(t + 2, r2[v]);
+      }
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < nn; k += kElasChunkThreads) {
+      const uint32_t id = __ldg(cnodes + p0 + k);
+      double* dst = y + 3 * int64_t(id & 0x7fffffffu);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        st_if(dst + a, sy[3 * k + a], !(id >> 31));
+        red_add_if(dst + a, sy[3 * k + a], (id >> 31) && sy[3 * k + a] != 0.0);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 __global__ void elasticity_dirichlet_rows(const uint8_t* __restrict__ dir, int64_t N, const double* __restrict__ x,
                                           double* __restrict__ y) {
   for (int64_t i = gtid(); i < N; i += gstride())
@@ -2019,11 +2116,32 @@ __global__ void set_dirichlet_diag1(const uint8_t* __restrict__ dir, int64_t N, 
 
 }  // namespace
 
+// DG_ELASTICITY_KERNEL=element keeps the one-thread-per-element kernel (testing).
+static bool elasticity_chunks_off() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("DG_ELASTICITY_KERNEL");
+    v = (e && !strcmp(e, "element")) ? 1 : 0;
+  }
+  return v == 1;
+}
+
 dg_status elasticity_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s) {
   const dg_da* da = A->da;
   DG_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * 3 * da->N, s));
-  elasticity_kernel<<<grid_for(da->E, 128, 16), 128, 0, s>>>(da->nl.p, da->meta.p, A->dirichlet.p, da->E, A->mu,
-                                                               A->lam, x, y);
+  const OctetSet& O = da->octs;
+  if (O.nchunk > 0 && O.lnl.p && !elasticity_chunks_off()) {
+    const size_t smem = 6 * sizeof(double) * O.max_nodes + O.max_nodes;
+    DG_TRY(allow_dynamic_smem(reinterpret_cast<const void*>(elasticity_chunk_kernel),
+                              (6 * sizeof(double) + 1) * 27 * kOctChunk));
+    const unsigned g = unsigned(std::min<int64_t>(O.nchunk, int64_t(sm_count()) * 4));
+    elasticity_chunk_kernel<<<g, kElasChunkThreads, smem, s>>>(O.n, O.nchunk, O.max_nodes, O.elem.p, O.lnl.p,
+                                                               O.cptr.p, O.cnodes.p, da->meta.p, A->dirichlet.p,
+                                                               da->E, A->mu, A->lam, x, y);
+  } else {
+    elasticity_kernel<<<grid_for(da->E, 128, 16), 128, 0, s>>>(da->nl.p, da->meta.p, A->dirichlet.p, da->E, A->mu,
+                                                                 A->lam, x, y);
+  }
   elasticity_dirichlet_rows<<<grid_for(da->N, 256), 256, 0, s>>>(A->dirichlet.p, da->N, x, y);
   DG_CUDA(cudaGetLastError());
   return DG_OK;

@@ -208,7 +208,9 @@ __global__ void __launch_bounds__(kChunkThreads) chunk_emit(int64_t n, const uin
                                                             uint32_t* __restrict__ cnodes,
                                                             uint32_t* __restrict__ ncount,
                                                             uint16_t* __restrict__ lidx,
-                                                            uint16_t* __restrict__ lelem) {
+                                                            uint16_t* __restrict__ lelem,
+                                                            const uint32_t* __restrict__ nl, int64_t E,
+                                                            uint16_t* __restrict__ lnl) {
   __shared__ uint32_t keys[kChunkKeys];
   __shared__ uint32_t uniq[kChunkKeys];
   __shared__ uint32_t tsum[kChunkThreads];
@@ -265,7 +267,25 @@ __global__ void __launch_bounds__(kChunkThreads) chunk_emit(int64_t n, const uin
     const int64_t g = int64_t(cc) * n + o0 + j;
     const uint32_t e = oelem[g];
     lelem[g] = e == kNoNode ? uint16_t(0xffffu) : uint16_t(e - e0);
+    if (e == kNoNode) continue;
+    // the element's 8 nodes as listed by the DA (a hanging vertex lists the
+    // parent's vertex node, a corner of the octet and so in the chunk's list)
+    for (int v = 0; v < 8; ++v) {
+      const uint32_t id = nl[int64_t(v) * E + e];
+      int lo = 0, hi = nu;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (uniq[mid] < id) lo = mid + 1;
+        else hi = mid;
+      }
+      lnl[int64_t(v) * E + e] = uint16_t(lo < nu && uniq[lo] == id ? lo : 0xffff);
+    }
   }
+}
+
+__global__ void count_u16_ffff(const uint16_t* __restrict__ a, int64_t n, uint32_t* __restrict__ out) {
+  for (int64_t i = gtid(); i < n; i += gstride())
+    if (a[i] == 0xffffu) atomicAdd(out, 1u);
 }
 
 __global__ void chunk_flag_shared(uint32_t* __restrict__ cnodes, int64_t total, const uint32_t* __restrict__ ncount) {
@@ -306,15 +326,25 @@ dg_status build_chunks(dg_da* da, cudaStream_t s) {
   DG_TRY(O.cnodes.alloc(int64_t(hp[nq]) > 0 ? int64_t(hp[nq]) : 1));
   DG_TRY(O.lidx.alloc(27 * n));
   DG_TRY(O.lelem.alloc(8 * n));
+  DG_TRY(O.lnl.alloc(8 * da->E));
+  DG_CUDA(cudaMemsetAsync(O.lnl.p, 0xff, 2 * 8 * da->E, s));
   DBuf<uint32_t> ncount;
   DG_TRY(ncount.alloc(da->N));
   DG_CUDA(cudaMemsetAsync(ncount.p, 0, 4 * da->N, s));
   DG_CUDA(cudaMemcpyAsync(O.cptr.p, hp.data(), 4 * (nq + 1), cudaMemcpyHostToDevice, s));
   chunk_emit<<<unsigned(nq), kChunkThreads, 0, s>>>(n, O.id.p, O.elem.p, O.cptr.p, O.cel.p, O.cnodes.p, ncount.p,
-                                                     O.lidx.p, O.lelem.p);
+                                                     O.lidx.p, O.lelem.p, da->nl.p, da->E, O.lnl.p);
+  // every node an element lists must be in its chunk's list
+  DBuf<uint32_t> miss;
+  DG_TRY(miss.alloc(1));
+  DG_CUDA(cudaMemsetAsync(miss.p, 0, 4, s));
+  count_u16_ffff<<<grid_for(8 * da->E, 256), 256, 0, s>>>(O.lnl.p, 8 * da->E, miss.p);
+  uint32_t hmiss = 0;
+  DG_CUDA(cudaMemcpyAsync(&hmiss, miss.p, 4, cudaMemcpyDeviceToHost, s));
   chunk_flag_shared<<<grid_for(hp[nq], 256), 256, 0, s>>>(O.cnodes.p, hp[nq], ncount.p);
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaStreamSynchronize(s));
+  DG_CHECK(!hmiss, DG_EUNBALANCED, "octet chunks: an element's node is missing from its chunk's node list");
   O.nchunk = nq;
   O.max_nodes = mx;
   O.max_erange = mr;

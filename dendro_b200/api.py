@@ -223,7 +223,9 @@ class _Mat:
     def mult_multi(self, X, Y=None, split: int = 3, stream=None):
         """Y = A X for the columns of X, a CUDA float32 tensor [N, nrhs]
         (nrhs a multiple of 16), on the tensor cores (split 3: FP32-level
-        accuracy from three TF32 products; 1: one TF32 product)."""
+        accuracy from three TF32 products; 1: one TF32 product), or with
+        split 0 in the octet form on the CUDA cores (exact FP32 products;
+        nrhs a multiple of 32)."""
         import torch
         if not (X.is_cuda and X.dtype == torch.float32 and X.dim() == 2 and X.is_contiguous()):
             raise TypeError("X must be a contiguous CUDA float32 tensor [N, nrhs]")

@@ -35,56 +35,6 @@ namespace {
 __device__ __forceinline__ int64_t gtid() { return blockIdx.x * int64_t(blockDim.x) + threadIdx.x; }
 __device__ __forceinline__ int64_t gstride() { return int64_t(gridDim.x) * blockDim.x; }
 
-// h = 2^-(lev-1) for embedded level lev (omgNeumann.C:470-471).
-template <class T>
-__device__ __forceinline__ T elem_h(uint32_t lev) {
-  return T(__longlong_as_double(int64_t(1023 + 1 - int(lev)) << 52));
-}
-
-// In-place 8-point Walsh-Hadamard transform over the vertex bits x=1, y=2, z=4.
-template <class T>
-__device__ __forceinline__ void wht8(T (&u)[8]) {
-#pragma unroll
-  for (int B = 1; B < 8; B <<= 1)
-#pragma unroll
-    for (int v = 0; v < 8; ++v)
-      if (!(v & B)) {
-        const T a = u[v], b = u[v | B];
-        u[v] = a + b;
-        u[v | B] = a - b;
-      }
-}
-
-// u <- (f1 K + f2 M) u on the reference cube, K = K1(x)M1(x)M1 + M1(x)K1(x)M1
-// + M1(x)M1(x)K1 and M = M1(x)M1(x)M1.  In the Walsh basis M1 -> diag(1, 1/3)
-// and K1 -> diag(0, 1), so a component with n (1,-1) factors is scaled by
-// f2 3^-n + f1 n 3^(1-n); the 1/8 of the inverse transform is folded in.
-template <class T>
-__device__ __forceinline__ void lapmass_ref(T (&u)[8], T f1, T f2) {
-  wht8(u);
-  const T l0 = f2 * T(0.125);
-  const T l1 = (f2 * T(1.0 / 3.0) + f1) * T(0.125);
-  const T l2 = (f2 * T(1.0 / 9.0) + f1 * T(2.0 / 3.0)) * T(0.125);
-  const T l3 = (f2 * T(1.0 / 27.0) + f1 * T(1.0 / 3.0)) * T(0.125);
-  u[0] *= l0;
-  u[1] *= l1;
-  u[2] *= l1;
-  u[4] *= l1;
-  u[3] *= l2;
-  u[5] *= l2;
-  u[6] *= l2;
-  u[7] *= l3;
-  wht8(u);
-}
-
-// r = (f1 K + f2 M) u, u unchanged.
-template <class T>
-__device__ __forceinline__ void lapmass_ref_to(const T (&u)[8], T f1, T f2, T (&r)[8]) {
-#pragma unroll
-  for (int v = 0; v < 8; ++v) r[v] = u[v];
-  lapmass_ref(r, f1, f2);
-}
-
 // Hanging interpolation u_vertex = T u_node, in place.  A hanging vertex i
 // takes the mean of the nodes j that differ from i only on the axes where i
 // and the child number c differ (2 nodes on an edge, 4 on a face).  All array
@@ -512,62 +462,6 @@ __global__ void __launch_bounds__(32 * kWarpCta, MINB) lapmass_warp_pipe_kernel(
 }
 
 // ------------------------------------------------------------ octet form --
-// The arithmetic of one octet (octet.cuh) on its 27 lattice values xv: the
-// points flagged in `none` (no node: hanging, or not a vertex of a present
-// child) are filled from their corners; every present child's element
-// operator is applied with compile-time lattice indices; the sums of the
-// hanging points are folded back onto their corners (T^T).  yv receives the
-// 27 lattice sums (meaningful at the points with a node).  coef(c, f1, f2)
-// scales child c's two factors by its coefficients.
-template <class T, class Coef>
-__device__ __forceinline__ void octet_apply(T (&xv)[27], T (&yv)[27], uint32_t none, uint32_t m, Coef coef) {
-#pragma unroll
-  for (int p = 0; p < 27; ++p) {
-    if (oct_free(p) == 1) {
-      const int s0 = oct_s0(p);
-      if ((none >> p) & 1u) xv[p] = (xv[p - s0] + xv[p + s0]) * T(0.5);
-    } else if (oct_free(p) == 2) {
-      const int s0 = oct_s0(p), s1 = oct_s1(p);
-      if ((none >> p) & 1u)
-        xv[p] = ((xv[p - s0 - s1] + xv[p + s0 - s1]) + (xv[p - s0 + s1] + xv[p + s0 + s1])) * T(0.25);
-    }
-  }
-#pragma unroll
-  for (int p = 0; p < 27; ++p) yv[p] = T(0);
-  const uint32_t cm = ometa_cmask(m);
-  const T h = elem_h<T>(ometa_lev(m));
-  const T g1 = h * T(0.5), g2 = h * h * h * T(0.125);
-#pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    if ((cm >> c) & 1u) {
-      T f1 = g1, f2 = g2;
-      coef(c, f1, f2);
-      T u[8];
-#pragma unroll
-      for (int v = 0; v < 8; ++v) u[v] = xv[oct_lat(c, v)];
-      lapmass_ref(u, f1, f2);
-#pragma unroll
-      for (int v = 0; v < 8; ++v) yv[oct_lat(c, v)] += u[v];
-    }
-  }
-#pragma unroll
-  for (int p = 0; p < 27; ++p) {
-    if (oct_free(p) == 1) {
-      const int s0 = oct_s0(p);
-      const T w = ((none >> p) & 1u) ? yv[p] * T(0.5) : T(0);
-      yv[p - s0] += w;
-      yv[p + s0] += w;
-    } else if (oct_free(p) == 2) {
-      const int s0 = oct_s0(p), s1 = oct_s1(p);
-      const T w = ((none >> p) & 1u) ? yv[p] * T(0.25) : T(0);
-      yv[p - s0 - s1] += w;
-      yv[p + s0 - s1] += w;
-      yv[p - s0 + s1] += w;
-      yv[p + s0 + s1] += w;
-    }
-  }
-}
-
 // One thread per octet, x and y in global memory: the octet's nodes gathered
 // from x, each node's sum added into y (which must be zero or hold the
 // values to add to) with one global reduction; the centre of an octet with

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "dg_internal.h"
+#include "octet.cuh"
 
 namespace dg {
 
@@ -508,13 +509,63 @@ std::vector<float> frame_stencil_tables() {
   return out;
 }
 
+// Octet form on the CUDA cores: a warp per (octet, 32 right-hand sides), one
+// lane per right-hand side.  Each lane holds its column's 27 lattice values
+// of the octet in registers and runs the octet arithmetic of the scalar
+// kernel (octet_apply: hanging points, the children's Walsh-form element
+// operators, T^T) in FP32; the octet's node ids, level and coefficients are
+// the same for the whole warp (broadcast loads), and the X rows read and the
+// Y rows added are 32 consecutive floats per node (one 128-byte access per
+// node and warp).  Y must be zero on entry (the sums leave with global
+// reductions; the centre of a full octet with a store).  Exact FP32 products:
+// no TF32 rounding, so `split` does not apply.
+__global__ void __launch_bounds__(128) mrhs_octet_kernel(int64_t n, const uint32_t* __restrict__ ometa,
+                                                         const uint32_t* __restrict__ oid,
+                                                         const uint32_t* __restrict__ oelem,
+                                                         const float* __restrict__ ca, const float* __restrict__ cb,
+                                                         int R, const float* __restrict__ X, float* __restrict__ Y) {
+  const int lane = threadIdx.x & 31;
+  const int nb = R / 32;
+  const int64_t tasks = n * nb;
+  for (int64_t t = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; t < tasks;
+       t += (int64_t(gridDim.x) * blockDim.x) >> 5) {
+    const int64_t o = t / nb;
+    const int col = int(t - o * nb) * 32 + lane;
+    const uint32_t m = __ldg(ometa + o);
+    uint32_t id[27], none = 0;
+    float xv[27], yv[27];
+#pragma unroll
+    for (int p = 0; p < 27; ++p) {
+      id[p] = __ldg(oid + int64_t(p) * n + o);
+      none |= id[p] == kNoNode ? (1u << p) : 0u;
+    }
+#pragma unroll
+    for (int p = 0; p < 27; ++p) xv[p] = id[p] != kNoNode ? __ldg(X + int64_t(id[p]) * R + col) : 0.f;
+    octet_apply<float>(xv, yv, none, m, [&](int c, float& f1, float& f2) {
+      if (ca) {
+        const uint32_t e = __ldg(oelem + int64_t(c) * n + o);
+        f1 *= __ldg(ca + e);
+        f2 *= __ldg(cb + e);
+      }
+    });
+    const uint32_t cm = ometa_cmask(m);
+#pragma unroll
+    for (int p = 0; p < 27; ++p) {
+      if (id[p] == kNoNode) continue;
+      float* dst = Y + int64_t(id[p]) * R + col;
+      if (p == 13 && cm == 255u) *dst = yv[p];
+      else if (yv[p] != 0.f) atomicAdd(dst, yv[p]);
+    }
+  }
+}
+
 }  // namespace
 
 dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int R, int split, cudaStream_t s) {
   dg_da* da = A->da;
   DG_CHECK(A->kind == 0, DG_EINVAL, "mat_mult_multi: scalar operator expected");
   DG_CHECK(R > 0 && R % kRC == 0, DG_EINVAL, "mat_mult_multi: nrhs must be a positive multiple of 16");
-  DG_CHECK(split == 1 || split == 3, DG_EINVAL, "mat_mult_multi: split must be 1 or 3");
+  DG_CHECK(split == 0 || split == 1 || split == 3, DG_EINVAL, "mat_mult_multi: split must be 0, 1 or 3");
   DG_CHECK((reinterpret_cast<uintptr_t>(X) & 15) == 0 && (reinterpret_cast<uintptr_t>(Y) & 15) == 0, DG_EINVAL,
            "mat_mult_multi: X and Y must be 16-byte aligned");
   static float4* tbls[64] = {};  // one table per device, kept for the process
@@ -532,13 +583,24 @@ dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int R, int split
   const float* ca = A->has_coef ? A->coef32.p : nullptr;
   const float* cb = A->has_coef ? A->coef32.p + da->E : nullptr;
   static int form = -1;
-  if (form < 0) {  // DG_MRHS_KERNEL: block (default, 32 per pass) | block64 | direct | stage | cta
+  if (form < 0) {  // DG_MRHS_KERNEL: block (default, 32 per pass) | block64 | direct | stage | cta | octet
     const char* e = getenv("DG_MRHS_KERNEL");
     form = (e && !strcmp(e, "cta"))       ? 2
            : (e && !strcmp(e, "stage"))   ? 1
            : (e && !strcmp(e, "direct"))  ? 0
            : (e && !strcmp(e, "block64")) ? 4
+           : (e && !strcmp(e, "octet"))   ? 5
                                           : 3;
+  }
+  if (split == 0 || form == 5) {
+    DG_CHECK(R % 32 == 0 && da->octs.n > 0, DG_EINVAL, "mat_mult_multi: the octet form takes nrhs a multiple of 32");
+    const OctetSet& O = da->octs;
+    DG_CUDA(cudaMemsetAsync(Y, 0, sizeof(float) * size_t(da->N) * R, s));
+    const int64_t warps = O.n * (R / 32);
+    const unsigned grid = unsigned(std::min<int64_t>((warps + 3) / 4, int64_t(sm_count()) * 16));
+    mrhs_octet_kernel<<<grid, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, R, X, Y);
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
   }
   if (form >= 3 && R % 32 == 0) {
     static float4* ftbls[64] = {};  // frame tables, one per device, kept for the process

@@ -27,6 +27,7 @@
 #pragma once
 
 #include "dg_internal.h"
+#include "element.cuh"
 
 namespace dg {
 
@@ -54,5 +55,61 @@ __host__ __device__ constexpr int oct_s1(int p) {
 // Per-octet word: level of the children (embedded) | child mask << 8.
 __host__ __device__ __forceinline__ uint32_t ometa_lev(uint32_t m) { return m & 31u; }
 __host__ __device__ __forceinline__ uint32_t ometa_cmask(uint32_t m) { return (m >> 8) & 255u; }
+
+// The arithmetic of one octet on its 27 lattice values xv: the
+// points flagged in `none` (no node: hanging, or not a vertex of a present
+// child) are filled from their corners; every present child's element
+// operator is applied with compile-time lattice indices; the sums of the
+// hanging points are folded back onto their corners (T^T).  yv receives the
+// 27 lattice sums (meaningful at the points with a node).  coef(c, f1, f2)
+// scales child c's two factors by its coefficients.
+template <class T, class Coef>
+__device__ __forceinline__ void octet_apply(T (&xv)[27], T (&yv)[27], uint32_t none, uint32_t m, Coef coef) {
+#pragma unroll
+  for (int p = 0; p < 27; ++p) {
+    if (oct_free(p) == 1) {
+      const int s0 = oct_s0(p);
+      if ((none >> p) & 1u) xv[p] = (xv[p - s0] + xv[p + s0]) * T(0.5);
+    } else if (oct_free(p) == 2) {
+      const int s0 = oct_s0(p), s1 = oct_s1(p);
+      if ((none >> p) & 1u)
+        xv[p] = ((xv[p - s0 - s1] + xv[p + s0 - s1]) + (xv[p - s0 + s1] + xv[p + s0 + s1])) * T(0.25);
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < 27; ++p) yv[p] = T(0);
+  const uint32_t cm = ometa_cmask(m);
+  const T h = elem_h<T>(ometa_lev(m));
+  const T g1 = h * T(0.5), g2 = h * h * h * T(0.125);
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    if ((cm >> c) & 1u) {
+      T f1 = g1, f2 = g2;
+      coef(c, f1, f2);
+      T u[8];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) u[v] = xv[oct_lat(c, v)];
+      lapmass_ref(u, f1, f2);
+#pragma unroll
+      for (int v = 0; v < 8; ++v) yv[oct_lat(c, v)] += u[v];
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < 27; ++p) {
+    if (oct_free(p) == 1) {
+      const int s0 = oct_s0(p);
+      const T w = ((none >> p) & 1u) ? yv[p] * T(0.5) : T(0);
+      yv[p - s0] += w;
+      yv[p + s0] += w;
+    } else if (oct_free(p) == 2) {
+      const int s0 = oct_s0(p), s1 = oct_s1(p);
+      const T w = ((none >> p) & 1u) ? yv[p] * T(0.25) : T(0);
+      yv[p - s0 - s1] += w;
+      yv[p + s0 - s1] += w;
+      yv[p - s0 + s1] += w;
+      yv[p + s0 + s1] += w;
+    }
+  }
+}
 
 }  // namespace dg

@@ -220,7 +220,9 @@ int dg_mat_kernel_count(void);
  * of 16.  The element contraction runs on the tensor cores with TF32 inputs
  * and FP32 accumulation; split = 3 splits each input into a TF32 high part and
  * a TF32 remainder (three products, FP32-level accuracy), split = 1 uses one
- * TF32 product.  Scalar Laplacian + mass operators only. */
+ * TF32 product; split = 0 runs the octet form on the CUDA cores instead (a
+ * warp per element parent and 32 right-hand sides, exact FP32 products;
+ * nrhs a multiple of 32).  Scalar Laplacian + mass operators only. */
 dg_status dg_mat_mult_multi(dg_mat* A, const float* X, float* Y, int nrhs, int split, void* stream);
 dg_status dg_mat_set_kernel(dg_mat* A, int prec, int variant);
 void dg_mat_destroy(dg_mat* A);

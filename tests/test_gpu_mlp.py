@@ -75,24 +75,51 @@ def test_learned_smoother_in_flexible_pcg(gpu, oracle):
     assert np.linalg.norm(fm.matvec(x) - b) <= 1.01e-8 * np.linalg.norm(b)
 
 
-def test_trained_smoother_gain_is_measured(gpu, oracle):
-    """Train briefly on pairs from the plain solver, then compare iterations
-    with and without the learned post-smoother on the same system."""
+def test_trained_smoother_gain_is_measured(gpu):
+    """The committed trained network (the benchmark's) as the finest-level
+    post-smoother of the FP32 V-cycle in flexible PCG, against the same cycle
+    with damped Jacobi post-smoothing (2 sweeps) and with none, on a 262,144-
+    point log-normal octree (maxDepth 14, the training distribution):
+      * the network has learned something: it needs fewer iterations to 1e-8
+        than the cycle without post-smoothing;
+      * its solve time against Jacobi's is the product of the measured
+        iteration ratio and per-cycle cost ratio (within 25 %), so the
+        measured gain (or loss) is explained by those two numbers, which the
+        test reports: the network costs more per application than the two
+        Jacobi sweeps it replaces and does not cut the iteration count below
+        theirs, so it does not pay on this hardware."""
+    import torch
+
     from dendro_b200 import inputs as I
-    from dendro_b200 import learned as Lrn
-    net, hist = Lrn.train(n_pairs=60, steps_per_pair=2, batch=16384, mesh_points=(15000,), log=None)
-    assert np.mean(hist[-10:]) < 0.5 * np.mean(hist[:3])
-    pts, d, m = points("lognormal20k_d12")
-    bal = oracle.balance(oracle.points2octree(pts, d, m), d)
-    b = I.uniform_rhs(len(bal), 9)
-    res = {}
-    for tag in ("jacobi", "learned"):
-        mg = gpu.DAMG(gpu.Octree.from_octants(bal, d), inner_prec=1)
+    from dendro_b200.learned import MLP, WEIGHTS, vcycle
+    pts = I.clamp_unit(I.lognormal_cloud(262144, 11), 14)
+    bal = gpu.balanceOctree(gpu.points2Octree(pts, 14, 1))
+    net = MLP(np.load(WEIGHTS))
+    out = {}
+    for tag, kw in (("jacobi", {}), ("none", {"nu_post": 0}), ("learned", {})):
+        mg = gpu.DAMG(bal, inner_prec=1, use_graph=True, **kw)
         if tag == "learned":
             mg.setSmoother(net)
-        bb = I.uniform_rhs(int(mg.N[0]), 9)
-        _, rep = mg.solve(bb)
-        assert rep["converged"]
-        res[tag] = rep
-    print("iterations jacobi", res["jacobi"]["iterations"], "learned", res["learned"]["iterations"],
-          "fallbacks", res["learned"]["smoother_fallbacks"])
+        b = torch.tensor(I.uniform_rhs(int(mg.N[0]), 9), device="cuda")
+        mg.solve(b)
+        reps = [mg.solve(b)[1] for _ in range(3)]
+        rep = min(reps, key=lambda r: r["solve_ms"])
+        assert rep["converged"], (tag, rep)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(3):
+            vcycle(mg, b)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(10):
+            vcycle(mg, b)
+        e1.record()
+        torch.cuda.synchronize()
+        out[tag] = dict(iterations=rep["iterations"], solve_ms=rep["solve_ms"], cycle_ms=e0.elapsed_time(e1) / 10,
+                        fallbacks=rep["smoother_fallbacks"])
+        del mg
+    print("learned smoother:", out)
+    assert out["learned"]["iterations"] < out["none"]["iterations"]
+    model = (out["learned"]["iterations"] * out["learned"]["cycle_ms"]) / (
+        out["jacobi"]["iterations"] * out["jacobi"]["cycle_ms"])
+    measured = out["learned"]["solve_ms"] / out["jacobi"]["solve_ms"]
+    assert abs(measured / model - 1) < 0.25, (measured, model)

@@ -88,6 +88,7 @@ def lib():
         "dg_damg_create": ([P, C.POINTER(DamgConfig), PP], I),
         "dg_damg_set_lapmass": ([P, P], I),
         "dg_damg_solve": ([P, P, P, I, C.POINTER(SolveReport)], I),
+        "dg_damg_solve_multi": ([P, P, P, I, I, C.POINTER(SolveReport)], I),
         "dg_damg_levels": ([P], I),
         "dg_damg_level_sizes": ([P, P, P], I),
         "dg_damg_level_da": ([P, I], P),
@@ -161,7 +162,7 @@ def exported_symbols():
         "dg_da_export", "dg_da_element_centers", "dg_da_destroy", "dg_mat_create_lapmass",
         "dg_mat_create_elasticity", "dg_mat_mult", "dg_mat_mult_f32", "dg_mat_get_diagonal",
         "dg_mat_mult_host", "dg_mat_size", "dg_mat_kernel_name", "dg_mat_destroy", "dg_damg_default_config", "dg_damg_create",
-        "dg_damg_set_lapmass", "dg_damg_solve", "dg_damg_levels", "dg_damg_level_sizes", "dg_damg_level_da",
+        "dg_damg_set_lapmass", "dg_damg_solve", "dg_damg_solve_multi", "dg_damg_levels", "dg_damg_level_sizes", "dg_damg_level_da",
         "dg_damg_prolong", "dg_damg_restrict", "dg_damg_destroy", "dg_vec_dot",
         "dg_damg_create_batch", "dg_damg_batch_count", "dg_damg_batch_offsets", "dg_damg_vcycle",
         "dg_mlp_param_count", "dg_mlp_create", "dg_mlp_get_params", "dg_mlp_set_params", "dg_mlp_forward",

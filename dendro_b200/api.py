@@ -377,6 +377,26 @@ class DAMG:
         return x, dict(iterations=rep.iterations, converged=bool(rep.converged), rel_residual=rep.rel_residual,
                        solve_ms=rep.solve_ms, smoother_fallbacks=rep.smoother_fallbacks)
 
+    def solve_multi(self, B, X=None, allow_unconverged: bool = False):
+        """Many right-hand sides at once: B [N, nrhs] FP64 (nrhs 32, 64, 128 or
+        256; CUDA tensor or numpy), one flexible PCG per column around one
+        V-cycle per iteration for all columns.  Returns (X, report dict)."""
+        rep = SolveReport()
+        R = int(B.shape[1])
+        if _is_device(B):
+            import torch
+            B = B.contiguous()
+            X = torch.empty_like(B) if X is None else X
+            st = lib().dg_damg_solve_multi(self.h, ptr(B), ptr(X), R, 1, C.byref(rep))
+        else:
+            Ba = np.ascontiguousarray(B, np.float64)
+            X = np.empty_like(Ba) if X is None else X
+            st = lib().dg_damg_solve_multi(self.h, ptr(Ba), ptr(X), R, 0, C.byref(rep))
+        if not (allow_unconverged and st == 4):
+            check(st, "damg_solve_multi")
+        return X, dict(iterations=rep.iterations, converged=bool(rep.converged), rel_residual=rep.rel_residual,
+                       solve_ms=rep.solve_ms)
+
     def setSmoother(self, mlp=None, sweeps: int = 2, fallback_ratio: float = 0.7):
         """Finest-level post-smoother: a learned MLP (dendro_b200.learned.MLP)
         or None for damped Jacobi; needs the FP32 inner V-cycle (inner_prec=1)."""

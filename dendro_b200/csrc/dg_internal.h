@@ -204,6 +204,11 @@ int matvec_variant_count();
 // Y = A X for nrhs vectors (node-major [N][nrhs], FP32) on the tensor cores;
 // split 1: TF32 products, 3: high/low TF32 split (FP32-level accuracy).
 dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int nrhs, int split, cudaStream_t s);
+// Y = A X in the octet form (CUDA cores) in FP32 or FP64, node-major [N][R],
+// R a multiple of 32; coef = the operator's coefficients in that precision
+// ([2][E], a then b; ignored when the operator has none).
+template <class T>
+dg_status mrhs_octet_apply(const dg_mat* A, const T* coef, const T* X, T* Y, int R, cudaStream_t s);
 dg_status elasticity_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status elasticity_diag(const dg_mat* A, double* d, cudaStream_t s);
 // Dense row-major (3 N) x (3 N) matrix of the elasticity operator, Dirichlet

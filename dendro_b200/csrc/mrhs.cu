@@ -519,11 +519,12 @@ std::vector<float> frame_stencil_tables() {
 // node and warp).  Y must be zero on entry (the sums leave with global
 // reductions; the centre of a full octet with a store).  Exact FP32 products:
 // no TF32 rounding, so `split` does not apply.
+template <class T>
 __global__ void __launch_bounds__(128) mrhs_octet_kernel(int64_t n, const uint32_t* __restrict__ ometa,
                                                          const uint32_t* __restrict__ oid,
                                                          const uint32_t* __restrict__ oelem,
-                                                         const float* __restrict__ ca, const float* __restrict__ cb,
-                                                         int R, const float* __restrict__ X, float* __restrict__ Y) {
+                                                         const T* __restrict__ ca, const T* __restrict__ cb,
+                                                         int R, const T* __restrict__ X, T* __restrict__ Y) {
   const int lane = threadIdx.x & 31;
   const int nb = R / 32;
   const int64_t tasks = n * nb;
@@ -533,15 +534,15 @@ __global__ void __launch_bounds__(128) mrhs_octet_kernel(int64_t n, const uint32
     const int col = int(t - o * nb) * 32 + lane;
     const uint32_t m = __ldg(ometa + o);
     uint32_t id[27], none = 0;
-    float xv[27], yv[27];
+    T xv[27], yv[27];
 #pragma unroll
     for (int p = 0; p < 27; ++p) {
       id[p] = __ldg(oid + int64_t(p) * n + o);
       none |= id[p] == kNoNode ? (1u << p) : 0u;
     }
 #pragma unroll
-    for (int p = 0; p < 27; ++p) xv[p] = id[p] != kNoNode ? __ldg(X + int64_t(id[p]) * R + col) : 0.f;
-    octet_apply<float>(xv, yv, none, m, [&](int c, float& f1, float& f2) {
+    for (int p = 0; p < 27; ++p) xv[p] = id[p] != kNoNode ? __ldg(X + int64_t(id[p]) * R + col) : T(0);
+    octet_apply<T>(xv, yv, none, m, [&](int c, T& f1, T& f2) {
       if (ca) {
         const uint32_t e = __ldg(oelem + int64_t(c) * n + o);
         f1 *= __ldg(ca + e);
@@ -552,14 +553,32 @@ __global__ void __launch_bounds__(128) mrhs_octet_kernel(int64_t n, const uint32
 #pragma unroll
     for (int p = 0; p < 27; ++p) {
       if (id[p] == kNoNode) continue;
-      float* dst = Y + int64_t(id[p]) * R + col;
+      T* dst = Y + int64_t(id[p]) * R + col;
       if (p == 13 && cm == 255u) *dst = yv[p];
-      else if (yv[p] != 0.f) atomicAdd(dst, yv[p]);
+      else if (yv[p] != T(0)) atomicAdd(dst, yv[p]);
     }
   }
 }
 
 }  // namespace
+
+template <class T>
+dg_status mrhs_octet_apply(const dg_mat* A, const T* coef, const T* X, T* Y, int R, cudaStream_t s) {
+  const dg_da* da = A->da;
+  const OctetSet& O = da->octs;
+  DG_CHECK(A->kind == 0 && R % 32 == 0 && O.n > 0, DG_EINVAL, "multi-RHS octet operator: bad arguments");
+  DG_CUDA(cudaMemsetAsync(Y, 0, sizeof(T) * size_t(da->N) * R, s));
+  const T* ca = A->has_coef ? coef : nullptr;
+  const T* cb = A->has_coef ? coef + da->E : nullptr;
+  const int64_t warps = O.n * (R / 32);
+  const unsigned grid = unsigned(std::min<int64_t>((warps + 3) / 4, int64_t(sm_count()) * 16));
+  mrhs_octet_kernel<T><<<grid, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, R, X, Y);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+template dg_status mrhs_octet_apply<float>(const dg_mat*, const float*, const float*, float*, int, cudaStream_t);
+template dg_status mrhs_octet_apply<double>(const dg_mat*, const double*, const double*, double*, int,
+                                            cudaStream_t);
 
 dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int R, int split, cudaStream_t s) {
   dg_da* da = A->da;
@@ -598,7 +617,7 @@ dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int R, int split
     DG_CUDA(cudaMemsetAsync(Y, 0, sizeof(float) * size_t(da->N) * R, s));
     const int64_t warps = O.n * (R / 32);
     const unsigned grid = unsigned(std::min<int64_t>((warps + 3) / 4, int64_t(sm_count()) * 16));
-    mrhs_octet_kernel<<<grid, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, R, X, Y);
+    mrhs_octet_kernel<float><<<grid, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, R, X, Y);
     DG_CUDA(cudaGetLastError());
     return DG_OK;
   }

@@ -1674,6 +1674,332 @@ dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, d
 
 void dg_damg_destroy(dg_damg* m) { delete m; }
 
+}  // extern "C"
+
+// ------------------------------------------------------ multi-RHS solve ---
+// R right-hand sides solved together (BASELINE's batched form: many right-
+// hand sides on one mesh): node-major [N][R] blocks, one flexible PCG per
+// column in FP64 (its own step lengths, frozen once it has converged) around
+// one V-cycle per iteration for all columns -- the operator applications of
+// every level are the octet multi-RHS kernel (a warp per parent octant and
+// 32 columns), the smoother, residual and transfers elementwise or per row
+// over the R columns, the coarsest level the dense inverse times the block.
+namespace {
+
+template <class T>
+__global__ void mv_jacobi_first(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ dinv, T omega,
+                                int64_t n, int R) {
+  for (int64_t i = gtid(); i < n; i += gstride()) x[i] = omega * dinv[i / R] * b[i];
+}
+template <class T>
+__global__ void mv_jacobi_update(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ dinv,
+                                 const T* __restrict__ t, T omega, int64_t n, int R) {
+  for (int64_t i = gtid(); i < n; i += gstride()) x[i] += omega * dinv[i / R] * (b[i] - t[i]);
+}
+template <class T>
+__global__ void mv_residual(const T* __restrict__ b, const T* __restrict__ t, T* __restrict__ r, int64_t n) {
+  for (int64_t i = gtid(); i < n; i += gstride()) r[i] = b[i] - t[i];
+}
+// rc[c][:] = sum_k R[c][k] rf[k][:]  (thread per (row, column): coalesced rows)
+template <class T>
+__global__ void mv_restrict(const uint32_t* __restrict__ rptr, const uint32_t* __restrict__ rcol,
+                            const T* __restrict__ rval, int64_t Nc, int R, const T* __restrict__ rf,
+                            T* __restrict__ rc) {
+  for (int64_t i = gtid(); i < Nc * R; i += gstride()) {
+    const int64_t c = i / R;
+    const int j = int(i - c * R);
+    T acc = T(0);
+    for (uint32_t k = rptr[c]; k < rptr[c + 1]; ++k) acc += rval[k] * rf[int64_t(rcol[k]) * R + j];
+    rc[i] = acc;
+  }
+}
+template <class T>
+__global__ void mv_prolong_add(const uint32_t* __restrict__ pptr, const uint32_t* __restrict__ pcol,
+                               const T* __restrict__ pval, int64_t Nf, int R, const T* __restrict__ xc,
+                               T* __restrict__ xf) {
+  for (int64_t i = gtid(); i < Nf * R; i += gstride()) {
+    const int64_t f = i / R;
+    const int j = int(i - f * R);
+    T acc = T(0);
+    for (uint32_t k = pptr[f]; k < pptr[f + 1]; ++k) acc += pval[k] * xc[int64_t(pcol[k]) * R + j];
+    xf[i] += acc;
+  }
+}
+// x = Ainv b for a block of R columns (one dense block: a single mesh)
+__global__ void mv_coarse(const double* __restrict__ Ainv, int64_t n, int R, const double* __restrict__ b,
+                          double* __restrict__ x) {
+  for (int64_t i = gtid(); i < n * R; i += gstride()) {
+    const int64_t r = i / R;
+    const int j = int(i - r * R);
+    const double* a = Ainv + r * n;
+    double acc = 0;
+    for (int64_t k = 0; k < n; ++k) acc += a[k] * b[k * R + j];
+    x[i] = acc;
+  }
+}
+template <class A, class B>
+__global__ void mv_convert(const A* __restrict__ a, B* __restrict__ b, int64_t n) {
+  for (int64_t i = gtid(); i < n; i += gstride()) b[i] = B(a[i]);
+}
+// Column sums of a[i][j] b[i][j] over the N rows: per block R partial sums
+// (256 / R rows at a time), then one pass over the blocks.
+constexpr int kMvDotBlocks = 592;
+__global__ void __launch_bounds__(256) mv_dot_partial(const double* __restrict__ a, const double* __restrict__ b,
+                                                      int64_t N, int R, double* __restrict__ part) {
+  __shared__ double acc[256];
+  const int rows = 256 / R, j = int(threadIdx.x) % R, r0 = int(threadIdx.x) / R;
+  double v = 0;
+  for (int64_t i = int64_t(blockIdx.x) * rows + r0; i < N; i += int64_t(gridDim.x) * rows)
+    v += a[i * R + j] * b[i * R + j];
+  acc[threadIdx.x] = v;
+  __syncthreads();
+  if (threadIdx.x < R) {
+    double t = 0;
+    for (int k = 0; k < rows; ++k) t += acc[k * R + threadIdx.x];
+    part[int64_t(blockIdx.x) * R + threadIdx.x] = t;
+  }
+}
+__global__ void mv_dot_finish(const double* __restrict__ part, int nb, int R, double* __restrict__ out) {
+  for (int j = threadIdx.x; j < R; j += blockDim.x) {
+    double t = 0;
+    for (int k = 0; k < nb; ++k) t += part[int64_t(k) * R + j];
+    out[j] = t;
+  }
+}
+// per-column PCG steps: y += s a[j] x; p = z + b[j] p
+__global__ void mv_axpy(double* __restrict__ y, const double* __restrict__ x, const double* __restrict__ a,
+                        double sgn, int64_t n, int R) {
+  for (int64_t i = gtid(); i < n; i += gstride()) y[i] += sgn * a[i % R] * x[i];
+}
+__global__ void mv_direction(double* __restrict__ p, const double* __restrict__ z, const double* __restrict__ b,
+                             int64_t n, int R) {
+  for (int64_t i = gtid(); i < n; i += gstride()) p[i] = z[i] + b[i % R] * p[i];
+}
+// alpha = rz / pq and the flexible beta = (rz_new - (r, z_old)) / rz, zero for
+// converged columns (done[j]); rz <- rz_new
+__global__ void mv_alpha(const double* __restrict__ rz, const double* __restrict__ pq,
+                         const uint8_t* __restrict__ done, double* __restrict__ alpha, int R) {
+  for (int j = threadIdx.x; j < R; j += blockDim.x) alpha[j] = (done[j] || pq[j] == 0) ? 0.0 : rz[j] / pq[j];
+}
+__global__ void mv_beta(const double* __restrict__ rzn, const double* __restrict__ rzo, double* __restrict__ rz,
+                        const uint8_t* __restrict__ done, double* __restrict__ beta, int R, int flexible) {
+  for (int j = threadIdx.x; j < R; j += blockDim.x) {
+    const double num = flexible ? rzn[j] - rzo[j] : rzn[j];
+    beta[j] = (done[j] || rz[j] == 0) ? 0.0 : num / rz[j];
+    rz[j] = rzn[j];
+  }
+}
+
+// Work blocks of every level for one right-hand-side count R.
+template <class T>
+struct MultiLevels {
+  std::vector<DBuf<T>> x, b, t;
+};
+
+template <class T>
+dg_status vcycle_multi(dg_damg* m, size_t l, const T* b, T* x, int R, MultiLevels<T>& W, DBuf<double>& cb,
+                       DBuf<double>& cx) {
+  cudaStream_t s = m->s;
+  Level& L = m->lv[l];
+  const int64_t N = L.da->N, n = N * R;
+  const unsigned g = grid_for(n, 256, 16);
+  if (l + 1 == m->lv.size()) {
+    if constexpr (sizeof(T) == 8) {
+      mv_coarse<<<grid_for(n, 256, 16), 256, 0, s>>>(m->Ainv.p, N, R, b, x);
+    } else {
+      mv_convert<float, double><<<g, 256, 0, s>>>(b, cb.p, n);
+      mv_coarse<<<grid_for(n, 256, 16), 256, 0, s>>>(m->Ainv.p, N, R, cb.p, cx.p);
+      mv_convert<double, float><<<g, 256, 0, s>>>(cx.p, x, n);
+    }
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+  }
+  const T* dinv;
+  const T* coef;
+  const T *pval, *rval;
+  if constexpr (sizeof(T) == 8) {
+    dinv = L.dinv.p;
+    coef = L.A->coef.p;
+    pval = L.pval.p;
+    rval = L.rval.p;
+  } else {
+    dinv = L.dinv32.p;
+    coef = L.A->coef32.p;
+    pval = L.pval32.p;
+    rval = L.rval32.p;
+  }
+  const T w = T(m->cfg.omega);
+  T* t = W.t[l].p;
+  if (m->cfg.nu_pre > 0) {
+    mv_jacobi_first<T><<<g, 256, 0, s>>>(x, b, dinv, w, n, R);
+    for (int k = 1; k < m->cfg.nu_pre; ++k) {
+      DG_TRY(mrhs_octet_apply<T>(L.A.get(), coef, x, t, R, s));
+      mv_jacobi_update<T><<<g, 256, 0, s>>>(x, b, dinv, t, w, n, R);
+    }
+    DG_TRY(mrhs_octet_apply<T>(L.A.get(), coef, x, t, R, s));
+    mv_residual<T><<<g, 256, 0, s>>>(b, t, t, n);
+  } else {
+    DG_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * n, s));
+  }
+  Level& C = m->lv[l + 1];
+  const int64_t Nc = C.da->N;
+  mv_restrict<T><<<grid_for(Nc * R, 256, 16), 256, 0, s>>>(L.rptr.p, L.rcol.p, rval, Nc, R,
+                                                           m->cfg.nu_pre > 0 ? (const T*)t : b, W.b[l + 1].p);
+  DG_TRY(vcycle_multi<T>(m, l + 1, W.b[l + 1].p, W.x[l + 1].p, R, W, cb, cx));
+  mv_prolong_add<T><<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, pval, N, R, W.x[l + 1].p, x);
+  for (int k = 0; k < m->cfg.nu_post; ++k) {
+    DG_TRY(mrhs_octet_apply<T>(L.A.get(), coef, x, t, R, s));
+    mv_jacobi_update<T><<<g, 256, 0, s>>>(x, b, dinv, t, w, n, R);
+  }
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+template <class T>
+dg_status alloc_multi_levels(dg_damg* m, int R, MultiLevels<T>& W) {
+  const size_t L = m->lv.size();
+  W.x.resize(L);
+  W.b.resize(L);
+  W.t.resize(L);
+  for (size_t l = 0; l < L; ++l) {
+    const int64_t n = m->lv[l].da->N * int64_t(R);
+    DG_TRY(W.x[l].alloc(n));
+    DG_TRY(W.b[l].alloc(n));
+    DG_TRY(W.t[l].alloc(n));
+  }
+  return DG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+dg_status dg_damg_solve_multi(dg_damg* m, const double* B, double* X, int nrhs, int on_device,
+                              dg_solve_report* rep) {
+  DG_CHECK(m && B && X, DG_EINVAL, "damg_solve_multi: bad arguments");
+  const int R = nrhs;
+  DG_CHECK(R > 0 && R % 32 == 0 && R <= 256 && 256 % R == 0, DG_EINVAL,
+           "damg_solve_multi: nrhs must be 32, 64, 128 or 256");
+  DG_CHECK(m->cfg.dof == 1 && m->nmesh == 1 && m->cfg.coarse_op == 0, DG_ENOTIMPL,
+           "damg_solve_multi: one mesh, the scalar operator, coarse_op 0");
+  DG_CHECK(m->lv.back().da->N <= 32768, DG_EINVAL, "damg_solve_multi: coarsest level too large");
+  for (const Level& L : m->lv) DG_CHECK(L.da->octs.n > 0, DG_EINVAL, "damg_solve_multi: mesh without octets");
+  cudaStream_t s = m->s;
+  const Level& L0 = m->lv[0];
+  const int64_t N = L0.da->N, n = N * R;
+  const bool f32 = m->cfg.inner_prec != DG_PREC_F64;
+  if (on_device) DG_CUDA(cudaDeviceSynchronize());
+  DBuf<double> b, x, r, z, zo, p, q, part, sc, cb, cx;
+  DBuf<float> r32, z32;
+  DBuf<uint8_t> done;
+  for (DBuf<double>* v : {&b, &x, &r, &z, &zo, &p, &q}) DG_TRY(v->alloc(n));
+  DG_TRY(part.alloc(int64_t(kMvDotBlocks) * R));
+  DG_TRY(sc.alloc(8 * int64_t(R)));  // bb, rz, pq, rr, rzn, rzo, alpha, beta
+  DG_TRY(done.alloc(R));
+  const int64_t nc = m->lv.back().da->N * int64_t(R);
+  DG_TRY(cb.alloc(nc));
+  DG_TRY(cx.alloc(nc));
+  MultiLevels<float> W32;
+  MultiLevels<double> W64;
+  if (f32) {
+    DG_TRY(alloc_multi_levels<float>(m, R, W32));
+    DG_TRY(r32.alloc(n));
+    DG_TRY(z32.alloc(n));
+  } else {
+    DG_TRY(alloc_multi_levels<double>(m, R, W64));
+  }
+  double* bb = sc.p;
+  double *rz = sc.p + R, *pq = sc.p + 2 * R, *rr = sc.p + 3 * R, *rzn = sc.p + 4 * R, *rzo = sc.p + 5 * R;
+  double *alpha = sc.p + 6 * R, *beta = sc.p + 7 * R;
+  DG_CUDA(cudaMemcpyAsync(b.p, B, 8 * n, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  DG_CUDA(cudaMemsetAsync(done.p, 0, R, s));
+  DG_CUDA(cudaStreamSynchronize(s));
+  auto dots = [&](const double* u, const double* v, double* out) -> dg_status {
+    mv_dot_partial<<<kMvDotBlocks, 256, 0, s>>>(u, v, N, R, part.p);
+    mv_dot_finish<<<1, 256, 0, s>>>(part.p, kMvDotBlocks, R, out);
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+  };
+  const unsigned g = grid_for(n, 256, 16);
+  auto precond = [&]() -> dg_status {
+    if (f32) {
+      mv_convert<double, float><<<g, 256, 0, s>>>(r.p, r32.p, n);
+      DG_TRY(vcycle_multi<float>(m, 0, r32.p, z32.p, R, W32, cb, cx));
+      mv_convert<float, double><<<g, 256, 0, s>>>(z32.p, z.p, n);
+      DG_CUDA(cudaGetLastError());
+      return DG_OK;
+    }
+    return vcycle_multi<double>(m, 0, r.p, z.p, R, W64, cb, cx);
+  };
+  cudaEvent_t e0, e1;
+  DG_CUDA(cudaEventCreate(&e0));
+  DG_CUDA(cudaEventCreate(&e1));
+  DG_CUDA(cudaEventRecord(e0, s));
+  DG_CUDA(cudaMemsetAsync(x.p, 0, 8 * n, s));
+  DG_CUDA(cudaMemcpyAsync(r.p, b.p, 8 * n, cudaMemcpyDeviceToDevice, s));
+  DG_TRY(dots(b.p, b.p, bb));
+  std::vector<double> hbb(R), hrr(R);
+  std::vector<uint8_t> hdone(R, 0);
+  DG_CUDA(cudaMemcpyAsync(hbb.data(), bb, 8 * R, cudaMemcpyDeviceToHost, s));
+  DG_TRY(precond());
+  DG_CUDA(cudaMemcpyAsync(p.p, z.p, 8 * n, cudaMemcpyDeviceToDevice, s));
+  DG_TRY(dots(r.p, z.p, rz));
+  const int flexible = f32 ? 1 : 0;
+  int it = 0;
+  double worst = 1.0;
+  bool conv = false;
+  DG_CUDA(cudaStreamSynchronize(s));
+  for (int j = 0; j < R; ++j)
+    if (hbb[j] == 0) hdone[j] = 1;
+  for (it = 1; it <= m->cfg.maxit; ++it) {
+    DG_TRY(mrhs_octet_apply<double>(L0.A.get(), L0.A->coef.p, p.p, q.p, R, s));
+    DG_TRY(dots(p.p, q.p, pq));
+    mv_alpha<<<1, 256, 0, s>>>(rz, pq, done.p, alpha, R);
+    mv_axpy<<<g, 256, 0, s>>>(x.p, p.p, alpha, 1.0, n, R);
+    mv_axpy<<<g, 256, 0, s>>>(r.p, q.p, alpha, -1.0, n, R);
+    DG_TRY(dots(r.p, r.p, rr));
+    DG_CUDA(cudaMemcpyAsync(hrr.data(), rr, 8 * R, cudaMemcpyDeviceToHost, s));
+    DG_CUDA(cudaStreamSynchronize(s));
+    worst = 0;
+    bool all = true;
+    for (int j = 0; j < R; ++j) {
+      const double rel = hbb[j] > 0 ? std::sqrt(hrr[j] / hbb[j]) : 0.0;
+      if (!(rel == rel)) worst = rel;
+      else worst = std::max(worst, rel);
+      if (rel <= m->cfg.rtol) hdone[j] = 1;
+      all = all && hdone[j];
+    }
+    if (!(worst == worst)) break;
+    if (all) {
+      conv = true;
+      break;
+    }
+    DG_CUDA(cudaMemcpyAsync(done.p, hdone.data(), R, cudaMemcpyHostToDevice, s));
+    DG_CUDA(cudaMemcpyAsync(zo.p, z.p, 8 * n, cudaMemcpyDeviceToDevice, s));
+    DG_TRY(precond());
+    DG_TRY(dots(r.p, z.p, rzn));
+    if (flexible) DG_TRY(dots(r.p, zo.p, rzo));
+    mv_beta<<<1, 256, 0, s>>>(rzn, rzo, rz, done.p, beta, R, flexible);
+    mv_direction<<<g, 256, 0, s>>>(p.p, z.p, beta, n, R);
+  }
+  DG_CUDA(cudaEventRecord(e1, s));
+  DG_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  DG_CUDA(cudaMemcpyAsync(X, x.p, 8 * n, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+  DG_CUDA(cudaStreamSynchronize(s));
+  if (rep) {
+    rep->iterations = it > m->cfg.maxit ? m->cfg.maxit : it;
+    rep->converged = conv ? 1 : 0;
+    rep->rel_residual = worst;
+    rep->solve_ms = ms;
+    rep->smoother_fallbacks = 0;
+  }
+  return conv ? DG_OK : DG_ENOTCONVERGED;
+}
+
 dg_status dg_vec_dot(const double* x, const double* y, int64_t n, double* result, void* stream) {
   DG_CHECK(result && n >= 0 && (n == 0 || (x && y)), DG_EINVAL, "vec_dot: bad arguments");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

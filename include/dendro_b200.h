@@ -285,6 +285,18 @@ dg_status dg_damg_set_lapmass(dg_damg* m, const double* coef);
 /* DAMGSolve (omg.h:492; omg.C:1121-1169): CG with V(nu_pre, nu_post)
  * preconditioning.  b and x are host arrays when on_device = 0. */
 dg_status dg_damg_solve(dg_damg* m, const double* b, double* x, int on_device, dg_solve_report* rep);
+
+/* Many right-hand sides on one mesh, solved together: B and X node-major
+ * [N][nrhs] FP64 (nrhs 32, 64, 128 or 256), one flexible PCG per column in
+ * FP64 around one V-cycle per iteration for all columns (the cycle in the
+ * configuration's inner precision; its operator applications are the octet
+ * multi-right-hand-side kernel).  Stops when every column's relative residual
+ * is at or below rtol; rep: iterations, the largest relative residual, device
+ * time.  One mesh, the scalar operator, coarse_op 0.  No reference
+ * counterpart (the reference solves one Vec at a time, DAMGSolve,
+ * include/omg/omg.h:492). */
+dg_status dg_damg_solve_multi(dg_damg* m, const double* B, double* X, int nrhs, int on_device,
+                              dg_solve_report* rep);
 /* Relative residual target and iteration limit of later solves (the
  * reference sets them through PETSc, KSPSetTolerances / -ksp_rtol,
  * bin/options:50-53). */

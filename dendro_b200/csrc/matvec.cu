@@ -504,6 +504,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_kernel(
   }
 }
 
+constexpr int kStageBatch = 8;  // node values each thread has in flight while staging a chunk
+
 // Chunked octet kernel: a CTA of kOctChunk threads per chunk of kOctChunk
 // consecutive octets (OctetSet chunks).  x at the chunk's nodes (ascending
 // ids: mostly contiguous runs) and the coefficients of the chunk's element
@@ -528,14 +530,47 @@ __global__ void __launch_bounds__(kOctChunk, MINB) lapmass_octchunk_kernel(
     const uint32_t p0 = __ldg(cptr + q), nn = __ldg(cptr + q + 1) - p0;
     const uint32_t e0 = __ldg(cel + 2 * q), ne = __ldg(cel + 2 * q + 1);
     const bool staged = ca && ne <= coef_cap;
-    for (uint32_t k = threadIdx.x; k < nn; k += kOctChunk) {
-      sx[k] = __ldg(x + (__ldg(cnodes + p0 + k) & 0x7fffffffu));
-      sy[k] = T(0);
+    // staging in batches of kStageBatch per thread: the node ids of a batch,
+    // then their x values, each batch's loads independent of one another
+    for (uint32_t k0 = threadIdx.x; k0 < nn; k0 += kStageBatch * kOctChunk) {
+      uint32_t id[kStageBatch];
+      T v[kStageBatch];
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const uint32_t k = k0 + u * kOctChunk;
+        id[u] = k < nn ? (__ldg(cnodes + p0 + k) & 0x7fffffffu) : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const uint32_t k = k0 + u * kOctChunk;
+        v[u] = k < nn ? __ldg(x + id[u]) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const uint32_t k = k0 + u * kOctChunk;
+        if (k < nn) {
+          sx[k] = v[u];
+          sy[k] = T(0);
+        }
+      }
     }
     if (staged)
-      for (uint32_t k = threadIdx.x; k < ne; k += kOctChunk) {
-        sa[k] = T(__ldg(ca + e0 + k));
-        sb[k] = T(__ldg(cb + e0 + k));
+      for (uint32_t k0 = threadIdx.x; k0 < ne; k0 += kStageBatch * kOctChunk) {
+        T a[kStageBatch], b[kStageBatch];
+#pragma unroll
+        for (int u = 0; u < kStageBatch; ++u) {
+          const uint32_t k = k0 + u * kOctChunk;
+          a[u] = k < ne ? T(__ldg(ca + e0 + k)) : T(0);
+          b[u] = k < ne ? T(__ldg(cb + e0 + k)) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < kStageBatch; ++u) {
+          const uint32_t k = k0 + u * kOctChunk;
+          if (k < ne) {
+            sa[k] = a[u];
+            sb[k] = b[u];
+          }
+        }
       }
     __syncthreads();
     const int64_t o = q * kOctChunk + threadIdx.x;
@@ -1765,13 +1800,32 @@ __global__ void __launch_bounds__(kElasChunkThreads, 2) elasticity_chunk_kernel(
   uint8_t* sd = reinterpret_cast<uint8_t*>(sy + 3 * size_t(node_cap));
   for (int64_t q = blockIdx.x; q < nchunk; q += gridDim.x) {
     const uint32_t p0 = __ldg(cptr + q), nn = __ldg(cptr + q + 1) - p0;
-    for (uint32_t k = threadIdx.x; k < nn; k += kElasChunkThreads) {
-      const uint32_t id = __ldg(cnodes + p0 + k) & 0x7fffffffu;
-      sd[k] = __ldg(dir + id);
+    for (uint32_t k0 = threadIdx.x; k0 < nn; k0 += 4 * kElasChunkThreads) {
+      uint32_t id[4];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        sx[3 * k + a] = __ldg(x + 3 * int64_t(id) + a);
-        sy[3 * k + a] = 0.0;
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t k = k0 + u * kElasChunkThreads;
+        id[u] = k < nn ? (__ldg(cnodes + p0 + k) & 0x7fffffffu) : 0u;
+      }
+      double v[4][3];
+      uint8_t dv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const bool in = k0 + u * kElasChunkThreads < nn;
+        dv[u] = in ? __ldg(dir + id[u]) : uint8_t(0);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) v[u][a] = in ? __ldg(x + 3 * int64_t(id[u]) + a) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t k = k0 + u * kElasChunkThreads;
+        if (k >= nn) continue;
+        sd[k] = dv[u];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          sx[3 * k + a] = v[u][a];
+          sy[3 * k + a] = 0.0;
+        }
       }
     }
     __syncthreads();

@@ -256,6 +256,9 @@ dg_status dg_da_create_from_maps(int64_t E, int64_t N, uint32_t max_depth, const
   if (!st) st = upload(da->ekey, ek.data(), E);
   if (!st) st = upload(da->nkey, nk.data(), N);
   if (!st) st = build_tiles(da, nullptr);
+  // octets: the corners a hanging vertex needs are nodes its own element
+  // lists, so a mesh of any subset of elements has them
+  if (!st) st = build_octets(da, nullptr);
   if (st) { delete da; return st; }
   *out = da;
   return DG_OK;

@@ -65,6 +65,11 @@ __global__ void octet_fill(const uint64_t* __restrict__ ekey, int64_t E, uint32_
                         9 * (((c >> 2) & 1u) + ((v >> 2) & 1)));
       if ((mask >> v) & 1u) {
         hb |= 1u << p;
+        // the DA lists a hanging vertex v as the parent's vertex v, the
+        // octet corner at lattice point 2 v, one of the corners its
+        // interpolation reads
+        const int pc = 2 * (v & 1) + 6 * ((v >> 1) & 1) + 18 * ((v >> 2) & 1);
+        oid[int64_t(pc) * n + o] = nl[int64_t(v) * E + e];
       } else {
         nb |= 1u << p;
         oid[int64_t(p) * n + o] = nl[int64_t(v) * E + e];
@@ -75,9 +80,9 @@ __global__ void octet_fill(const uint64_t* __restrict__ ekey, int64_t E, uint32_
   }
 }
 
-// Corners needed by hanging points and not set by a present child: their node
-// ids from the node anchors.  Also checks that no lattice point is both
-// hanging for one child and a node for another, and that no corner hangs.
+// Checks that no lattice point is both hanging for one child and a node for
+// another and that no corner hangs; corners a hanging point needs and no
+// element listed (none expected) are looked up among the node anchors.
 __global__ void octet_corners(const uint64_t* __restrict__ okeys, int64_t n, uint32_t Dp,
                               const uint64_t* __restrict__ nkey, int64_t N, const uint32_t* __restrict__ hang,
                               const uint32_t* __restrict__ node, uint32_t* __restrict__ oid,
@@ -101,7 +106,10 @@ __global__ void octet_corners(const uint64_t* __restrict__ okeys, int64_t n, uin
         need |= 1u << (qx + 3 * qy + 9 * qz);
       }
     }
-    need &= ~nb;
+    // corners still without an id (none: every element lists its hanging
+    // vertices' corners) are looked up among the node anchors
+    for (int p = 0; p < 27; ++p)
+      if (((need >> p) & 1u) && oid[int64_t(p) * n + o] != kNoNode) need &= ~(1u << p);
     if (!need) continue;
     const uint64_t k = okeys[o];
     const uint32_t pl = okey_l(k);

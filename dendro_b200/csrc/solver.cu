@@ -1365,6 +1365,8 @@ dg_status concat_das(const std::vector<dg_da*>& in, dg_da* out, cudaStream_t s) 
     no += d->N;
   }
   DG_CUDA(cudaGetLastError());
+  // no octet tables: the meshes' parent keys coincide across the batch, so
+  // the octet kernels are not offered for a concatenated level
   return build_tiles(out, s);
 }
 

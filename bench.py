@@ -64,6 +64,7 @@ def parse():
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--no-cfg1", action="store_true")
     p.add_argument("--no-elasticity", action="store_true")
+    p.add_argument("--no-partitioned", action="store_true")
     p.add_argument("--solve-workload", default="lognormal4m_d16")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--vcycle-profile", metavar="WORKLOAD", default=None,
@@ -204,9 +205,11 @@ def run_dendro(args, rank, world):
 
     # the partitioned path with one rank: the same mesh through the
     # partitioned operator (what --gpus N > 1 times), for comparison
-    part = run_partitioned(args, dev, bal, coef, x, 1, min(args.steps, 50), args.warmup)
-    part = {"ms_per_step": round(part["ms_per_step"], 5),
-            "gdofs": round(N / (part["ms_per_step"] * 1e-3) / 1e9, 4)}
+    part = None
+    if not args.no_partitioned:
+        part = run_partitioned(args, dev, bal, coef, x, 1, min(args.steps, 50), args.warmup)
+        part = {"ms_per_step": round(part["ms_per_step"], 5),
+                "gdofs": round(N / (part["ms_per_step"] * 1e-3) / 1e9, 4)}
     solve = None if args.no_solve else run_solve(dev, args.solve_workload)
     kernel = A.kernel_name(0)
     multi = None if args.no_multi else run_multi(dev, min(args.steps, 50))

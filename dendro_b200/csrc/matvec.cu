@@ -1943,9 +1943,9 @@ __global__ void elasticity_diag_kernel(const uint32_t* __restrict__ nl, const ui
 }
 
 // Dense assembly of the operator on a small level (the coarsest level of the
-// dof-3 multigrid): per element and non-hanging, non-Dirichlet column (node,
-// component) the element operator applied to that unit vector, scattered into
-// the non-Dirichlet rows of the row-major n3 x n3 matrix (n3 = 3 N).
+// dof-3 multigrid): per element and non-Dirichlet column (node, component)
+// the element operator applied to that unit vector, scattered into the
+// non-Dirichlet rows of the row-major n3 x n3 matrix (n3 = 3 N).
 __global__ void elasticity_dense_kernel(const uint32_t* __restrict__ nl, const uint32_t* __restrict__ meta,
                                         const uint8_t* __restrict__ dir, int64_t E, double mu, double lam,
                                         int64_t n3, double* __restrict__ Ad) {
@@ -1954,7 +1954,8 @@ __global__ void elasticity_dense_kernel(const uint32_t* __restrict__ nl, const u
     const int j = int(t - e * 24), jn = j / 3, jd = j % 3;
     const uint32_t m = meta[e];
     const uint32_t lev = meta_lev(m), c = meta_cnum(m), mask = meta_mask(m);
-    if ((mask >> jn) & 1u) continue;  // a hanging vertex is no column of its own
+    // a hanging vertex's slot holds the parent-corner node the DA lists
+    // there, so every one of the 8 slots is a column
     const uint32_t node = nl[int64_t(jn) * E + e];
     if (dir[node]) continue;
     const double fac = elem_h<double>(lev) / 2.0;

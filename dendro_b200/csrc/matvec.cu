@@ -614,6 +614,137 @@ __global__ void __launch_bounds__(kOctChunk, MINB) lapmass_octchunk_kernel(
   }
 }
 
+// Lean chunked octet kernel: the same staging and flush as
+// lapmass_octchunk_kernel, but no 27-value register arrays -- each child's 8
+// vertex values are read from the staged x on demand (a hanging point as the
+// mean of its corners), and the child's 8 results go straight into the
+// chunk's shared accumulator (a hanging point's share onto its corners), so
+// a thread holds only the 27 local indices and one element: far fewer
+// registers and more resident chunks per SM, for 64 shared-memory atomics per
+// complete octet instead of 27.
+template <class T>
+__device__ __forceinline__ T lean_value(const T* sx, const uint16_t (&li)[27], int p) {
+  if (oct_free(p) == 1) {
+    const int s0 = oct_s0(p);
+    if (li[p] == 0xffffu) return (sx[li[p - s0]] + sx[li[p + s0]]) * T(0.5);
+  } else if (oct_free(p) == 2) {
+    const int s0 = oct_s0(p), s1 = oct_s1(p);
+    if (li[p] == 0xffffu)
+      return ((sx[li[p - s0 - s1]] + sx[li[p + s0 - s1]]) + (sx[li[p - s0 + s1]] + sx[li[p + s0 + s1]])) * T(0.25);
+  }
+  return sx[li[p]];
+}
+template <class T>
+__device__ __forceinline__ void lean_add(T* sy, const uint16_t (&li)[27], int p, T v) {
+  if (oct_free(p) == 1) {
+    const int s0 = oct_s0(p);
+    if (li[p] == 0xffffu) {
+      const T w = v * T(0.5);
+      atomicAdd(sy + li[p - s0], w);
+      atomicAdd(sy + li[p + s0], w);
+      return;
+    }
+  } else if (oct_free(p) == 2) {
+    const int s0 = oct_s0(p), s1 = oct_s1(p);
+    if (li[p] == 0xffffu) {
+      const T w = v * T(0.25);
+      atomicAdd(sy + li[p - s0 - s1], w);
+      atomicAdd(sy + li[p + s0 - s1], w);
+      atomicAdd(sy + li[p - s0 + s1], w);
+      atomicAdd(sy + li[p + s0 + s1], w);
+      return;
+    }
+  }
+  atomicAdd(sy + li[p], v);
+}
+
+template <class T, class CT, int MINB>
+__global__ void __launch_bounds__(kOctChunk, MINB) lapmass_octchunk_lean_kernel(
+    int64_t n, int64_t nchunk, uint32_t node_cap, uint32_t coef_cap, const uint32_t* __restrict__ ometa,
+    const uint16_t* __restrict__ lidx, const uint16_t* __restrict__ lelem, const uint32_t* __restrict__ cptr,
+    const uint32_t* __restrict__ cnodes, const uint32_t* __restrict__ cel, const CT* __restrict__ ca,
+    const CT* __restrict__ cb, const T* __restrict__ x, T* __restrict__ y) {
+  extern __shared__ __align__(16) unsigned char oc_smem[];
+  T* sx = reinterpret_cast<T*>(oc_smem);
+  T* sy = sx + node_cap;
+  T* sa = sy + node_cap;
+  T* sb = sa + coef_cap;
+  for (int64_t q = blockIdx.x; q < nchunk; q += gridDim.x) {
+    const uint32_t p0 = __ldg(cptr + q), nn = __ldg(cptr + q + 1) - p0;
+    const uint32_t e0 = __ldg(cel + 2 * q), ne = __ldg(cel + 2 * q + 1);
+    const bool staged = ca && ne <= coef_cap;
+    for (uint32_t k0 = threadIdx.x; k0 < nn; k0 += kStageBatch * kOctChunk) {
+      uint32_t id[kStageBatch];
+      T v[kStageBatch];
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const uint32_t k = k0 + u * kOctChunk;
+        id[u] = k < nn ? (__ldg(cnodes + p0 + k) & 0x7fffffffu) : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const uint32_t k = k0 + u * kOctChunk;
+        v[u] = k < nn ? __ldg(x + id[u]) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const uint32_t k = k0 + u * kOctChunk;
+        if (k < nn) {
+          sx[k] = v[u];
+          sy[k] = T(0);
+        }
+      }
+    }
+    if (staged)
+      for (uint32_t k = threadIdx.x; k < ne; k += kOctChunk) {
+        sa[k] = T(__ldg(ca + e0 + k));
+        sb[k] = T(__ldg(cb + e0 + k));
+      }
+    __syncthreads();
+    const int64_t o = q * kOctChunk + threadIdx.x;
+    if (o < n) {
+      const uint32_t m = __ldg(ometa + o);
+      const uint32_t cm = ometa_cmask(m);
+      uint16_t li[27];
+#pragma unroll
+      for (int p = 0; p < 27; ++p) li[p] = __ldg(lidx + int64_t(p) * n + o);
+      const T h = elem_h<T>(ometa_lev(m));
+      const T g1 = h * T(0.5), g2 = h * h * h * T(0.125);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if ((cm >> c) & 1u) {
+          T f1 = g1, f2 = g2;
+          if (ca) {
+            const uint32_t le = __ldg(lelem + int64_t(c) * n + o);
+            if (staged) {
+              f1 *= sa[le];
+              f2 *= sb[le];
+            } else {
+              f1 *= T(__ldg(ca + e0 + le));
+              f2 *= T(__ldg(cb + e0 + le));
+            }
+          }
+          T u[8];
+#pragma unroll
+          for (int v = 0; v < 8; ++v) u[v] = lean_value<T>(sx, li, oct_lat(c, v));
+          lapmass_ref(u, f1, f2);
+#pragma unroll
+          for (int v = 0; v < 8; ++v) lean_add<T>(sy, li, oct_lat(c, v), u[v]);
+        }
+      }
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < nn; k += kOctChunk) {
+      const uint32_t id = __ldg(cnodes + p0 + k);
+      T* dst = y + (id & 0x7fffffffu);
+      const T v = sy[k];
+      st_if(dst, v, !(id >> 31));
+      red_add_if(dst, v, (id >> 31) && v != T(0));
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------- bulk-copy staging --
 // The warp-tile operator with its tile records staged by the copy engine:
 // one lane per warp issues cp.async.bulk copies of a tile's contiguous
@@ -1107,7 +1238,7 @@ struct MatvecVariant {
   int block, per_sm;  // threads per CTA, CTAs per SM in the grid (0: one thread per element)
   int kind;           // 0 atomic (BLOCK, MINB), 2 warp-tile, 3 + records prefetched, 4 + ids and x too,
                       // 5 records staged by bulk copies, 6 octet (one thread per parent octant),
-                      // 7 octet chunks staged through shared memory
+                      // 7 octet chunks staged through shared memory, 8 the same, lean
   int minb;
   const char* name;
 };
@@ -1130,6 +1261,8 @@ constexpr MatvecVariant kVariants[] = {
     {kOctChunk, 2, 7, 2, "octet chunks of 128, 2 CTAs/SM"},
     {kOctChunk, 3, 7, 3, "octet chunks of 128, 3 CTAs/SM"},
     {kOctChunk, 4, 7, 4, "octet chunks of 128, 4 CTAs/SM"},
+    {kOctChunk, 6, 8, 6, "octet chunks of 128, lean, 6 CTAs/SM"},
+    {kOctChunk, 8, 8, 8, "octet chunks of 128, lean, 8 CTAs/SM"},
 };
 // Coefficients of at most this many consecutive elements are staged per chunk.
 constexpr uint32_t kOctCoefCap = 2048;
@@ -1156,7 +1289,20 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
   const MatvecVariant& V = kVariants[v];
   const unsigned g = V.per_sm ? grid_for(da->E, V.block, V.per_sm)
                               : unsigned((da->E + V.block - 1) / V.block > 0 ? (da->E + V.block - 1) / V.block : 1);
-  if (V.kind == 7) {
+  if (V.kind == 8) {
+    const OctetSet& O = da->octs;
+    const uint32_t coef_cap = ca ? std::min(O.max_erange, kOctCoefCap) : 0u;
+    const size_t smem = sizeof(T) * (2 * size_t(O.max_nodes) + 2 * size_t(coef_cap));
+    const unsigned gq = unsigned(std::min<int64_t>(O.nchunk, int64_t(sm_count()) * V.per_sm));
+    auto go = [&](auto kern) -> dg_status {
+      DG_TRY(allow_dynamic_smem(reinterpret_cast<const void*>(kern), kOctChunkSmemMax * sizeof(T)));
+      kern<<<gq, kOctChunk, smem, s>>>(O.n, O.nchunk, O.max_nodes, coef_cap, O.meta.p, O.lidx.p, O.lelem.p,
+                                       O.cptr.p, O.cnodes.p, O.cel.p, ca, cb, x, y);
+      return DG_OK;
+    };
+    if (V.minb == 6) DG_TRY(go(lapmass_octchunk_lean_kernel<T, CT, 6>));
+    else DG_TRY(go(lapmass_octchunk_lean_kernel<T, CT, 8>));
+  } else if (V.kind == 7) {
     const OctetSet& O = da->octs;
     const uint32_t coef_cap = ca ? std::min(O.max_erange, kOctCoefCap) : 0u;
     const size_t smem = sizeof(T) * (2 * size_t(O.max_nodes) + 2 * size_t(coef_cap));
@@ -1284,7 +1430,7 @@ static dg_status pick_variant(const dg_da* da, int& choice, const CT* ca, const 
     for (int v = 0; v < kNumVariants; ++v) {
       if (kVariants[v].kind >= 2 && kVariants[v].kind <= 5 && da->tiles_w.ntiles == 0) continue;
       if (kVariants[v].kind == 6 && da->octs.n == 0) continue;
-      if (kVariants[v].kind == 7 && da->octs.nchunk == 0) continue;
+      if ((kVariants[v].kind == 7 || kVariants[v].kind == 8) && da->octs.nchunk == 0) continue;
       for (int trial = 0; trial < 2; ++trial) {
         DG_CUDA(cudaMemsetAsync(flush.p, trial + 1, flush_bytes, s));
         DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));

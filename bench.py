@@ -573,6 +573,13 @@ def rel_err(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300))
 
 
+def octree_digest(octs):
+    """sha256 of the octants (x, y, z, level) as uint32, in order."""
+    import hashlib
+    a = np.stack([octs["x"], octs["y"], octs["z"], octs["lf"] & 31], 1).astype(np.uint32)
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
 def reference_y_path(workload):
     """Where the reference arm leaves one y of the compiled reference for the
     GPU arm run after it on the same host (the two arms run back to back)."""
@@ -719,7 +726,12 @@ def main():
         yp = reference_y_path(args.workload)
         if os.path.exists(yp) and os.path.getsize(yp) == 8 * r["N"]:
             parity["vs_reference_rel_err"] = rel_err(r["y"], np.fromfile(yp))
-        parity["ok"] = all(v <= 1e-12 for k, v in parity.items() if k.endswith("rel_err"))
+        # the GPU's balanced octree against the oracle's, built from the same
+        # points by the reference arm (its digest, left beside its y)
+        if os.path.exists(yp + ".octree"):
+            parity["octree_equals_oracle"] = open(yp + ".octree").read().strip() == octree_digest(octs)
+        parity["ok"] = all(v <= 1e-12 for k, v in parity.items() if k.endswith("rel_err")) and \
+            parity.get("octree_equals_oracle", True)
         line["parity"] = parity
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -844,6 +856,8 @@ def main_reference(args, rank, world):
             y_port = O.Mesh(octs, depth).matvec(x, coef)
             line["parity"] = {"oracle_vs_reference_rel_err": rel_err(y_port, y_ref), "tolerance": 1e-12}
             y_ref.tofile(reference_y_path(args.workload))
+            with open(reference_y_path(args.workload) + ".octree", "w") as f:
+                f.write(octree_digest(octs))
             v = sum(N / t for t in per) / 1e9
             line.update({"value": round(v, 5), "steps": reps, "ms_per_step": round(1e3 * float(np.mean(per)), 3),
                          "cpu_baseline": {"value": round(v, 5), "unit": "GDoF/s", "cores": len(per),

@@ -660,19 +660,26 @@ __device__ __forceinline__ void lean_add(T* sy, const uint16_t (&li)[27], int p,
 
 template <class T, class CT, int MINB>
 __global__ void __launch_bounds__(kOctChunk, MINB) lapmass_octchunk_lean_kernel(
-    int64_t n, int64_t nchunk, uint32_t node_cap, uint32_t coef_cap, const uint32_t* __restrict__ ometa,
+    int64_t n, int64_t nchunk, uint32_t node_cap, const uint32_t* __restrict__ ometa,
     const uint16_t* __restrict__ lidx, const uint16_t* __restrict__ lelem, const uint32_t* __restrict__ cptr,
     const uint32_t* __restrict__ cnodes, const uint32_t* __restrict__ cel, const CT* __restrict__ ca,
     const CT* __restrict__ cb, const T* __restrict__ x, T* __restrict__ y) {
   extern __shared__ __align__(16) unsigned char oc_smem[];
   T* sx = reinterpret_cast<T*>(oc_smem);
   T* sy = sx + node_cap;
-  T* sa = sy + node_cap;
-  T* sb = sa + coef_cap;
   for (int64_t q = blockIdx.x; q < nchunk; q += gridDim.x) {
     const uint32_t p0 = __ldg(cptr + q), nn = __ldg(cptr + q + 1) - p0;
-    const uint32_t e0 = __ldg(cel + 2 * q), ne = __ldg(cel + 2 * q + 1);
-    const bool staged = ca && ne <= coef_cap;
+    const uint32_t e0 = __ldg(cel + 2 * q);
+    const int64_t o = q * kOctChunk + threadIdx.x;
+    // this thread's octet records, issued before the staging so that their
+    // latency overlaps it
+    uint32_t m = 0;
+    uint16_t li[27];
+    if (o < n) {
+      m = __ldg(ometa + o);
+#pragma unroll
+      for (int p = 0; p < 27; ++p) li[p] = __ldg(lidx + int64_t(p) * n + o);
+    }
     for (uint32_t k0 = threadIdx.x; k0 < nn; k0 += kStageBatch * kOctChunk) {
       uint32_t id[kStageBatch];
       T v[kStageBatch];
@@ -695,34 +702,19 @@ __global__ void __launch_bounds__(kOctChunk, MINB) lapmass_octchunk_lean_kernel(
         }
       }
     }
-    if (staged)
-      for (uint32_t k = threadIdx.x; k < ne; k += kOctChunk) {
-        sa[k] = T(__ldg(ca + e0 + k));
-        sb[k] = T(__ldg(cb + e0 + k));
-      }
     __syncthreads();
-    const int64_t o = q * kOctChunk + threadIdx.x;
     if (o < n) {
-      const uint32_t m = __ldg(ometa + o);
       const uint32_t cm = ometa_cmask(m);
-      uint16_t li[27];
-#pragma unroll
-      for (int p = 0; p < 27; ++p) li[p] = __ldg(lidx + int64_t(p) * n + o);
       const T h = elem_h<T>(ometa_lev(m));
       const T g1 = h * T(0.5), g2 = h * h * h * T(0.125);
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
         if ((cm >> c) & 1u) {
           T f1 = g1, f2 = g2;
-          if (ca) {
+          if (ca) {  // used once per element: read through L1, not staged
             const uint32_t le = __ldg(lelem + int64_t(c) * n + o);
-            if (staged) {
-              f1 *= sa[le];
-              f2 *= sb[le];
-            } else {
-              f1 *= T(__ldg(ca + e0 + le));
-              f2 *= T(__ldg(cb + e0 + le));
-            }
+            f1 *= T(__ldg(ca + e0 + le));
+            f2 *= T(__ldg(cb + e0 + le));
           }
           T u[8];
 #pragma unroll
@@ -1263,6 +1255,7 @@ constexpr MatvecVariant kVariants[] = {
     {kOctChunk, 4, 7, 4, "octet chunks of 128, 4 CTAs/SM"},
     {kOctChunk, 6, 8, 6, "octet chunks of 128, lean, 6 CTAs/SM"},
     {kOctChunk, 8, 8, 8, "octet chunks of 128, lean, 8 CTAs/SM"},
+    {kOctChunk, 5, 8, 5, "octet chunks of 128, lean, 5 CTAs/SM"},
 };
 // Coefficients of at most this many consecutive elements are staged per chunk.
 constexpr uint32_t kOctCoefCap = 2048;
@@ -1291,16 +1284,16 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
                               : unsigned((da->E + V.block - 1) / V.block > 0 ? (da->E + V.block - 1) / V.block : 1);
   if (V.kind == 8) {
     const OctetSet& O = da->octs;
-    const uint32_t coef_cap = ca ? std::min(O.max_erange, kOctCoefCap) : 0u;
-    const size_t smem = sizeof(T) * (2 * size_t(O.max_nodes) + 2 * size_t(coef_cap));
+    const size_t smem = sizeof(T) * 2 * size_t(O.max_nodes);
     const unsigned gq = unsigned(std::min<int64_t>(O.nchunk, int64_t(sm_count()) * V.per_sm));
     auto go = [&](auto kern) -> dg_status {
       DG_TRY(allow_dynamic_smem(reinterpret_cast<const void*>(kern), kOctChunkSmemMax * sizeof(T)));
-      kern<<<gq, kOctChunk, smem, s>>>(O.n, O.nchunk, O.max_nodes, coef_cap, O.meta.p, O.lidx.p, O.lelem.p,
-                                       O.cptr.p, O.cnodes.p, O.cel.p, ca, cb, x, y);
+      kern<<<gq, kOctChunk, smem, s>>>(O.n, O.nchunk, O.max_nodes, O.meta.p, O.lidx.p, O.lelem.p, O.cptr.p,
+                                       O.cnodes.p, O.cel.p, ca, cb, x, y);
       return DG_OK;
     };
     if (V.minb == 6) DG_TRY(go(lapmass_octchunk_lean_kernel<T, CT, 6>));
+    else if (V.minb == 5) DG_TRY(go(lapmass_octchunk_lean_kernel<T, CT, 5>));
     else DG_TRY(go(lapmass_octchunk_lean_kernel<T, CT, 8>));
   } else if (V.kind == 7) {
     const OctetSet& O = da->octs;

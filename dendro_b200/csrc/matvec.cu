@@ -737,6 +737,133 @@ __global__ void __launch_bounds__(kOctChunk, MINB) lapmass_octchunk_lean_kernel(
   }
 }
 
+// Pipelined chunked octet kernel: the chunked kernel with its staging moved
+// off the critical path.  A CTA walks its chunks i = 0, 1, 2, ... (chunk
+// blockIdx.x + i gridDim.x); while it works chunk i, the x gathers of chunk
+// i + 1 (cp.async, 4 or 8 bytes each, from the node ids already in shared
+// memory) and the node ids of chunk i + 2 (cp.async) are in flight.  Shared
+// memory: node ids in three slots (i: flush, i + 1: gathering, i + 2:
+// arriving), x in two, the accumulator in one.  Coefficients are read
+// through L1 (each is used once).
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <class T>
+__device__ __forceinline__ void octchunk_issue_ids(uint32_t* ib, const uint32_t* __restrict__ cnodes, uint32_t p0,
+                                                   uint32_t nn) {
+  for (uint32_t k = threadIdx.x; k < nn; k += kOctChunk) cp_async4(ib + k, cnodes + p0 + k);
+}
+template <class T>
+__device__ __forceinline__ void octchunk_issue_x(T* xb, const uint32_t* ib, const T* __restrict__ x, uint32_t nn) {
+  for (uint32_t k = threadIdx.x; k < nn; k += kOctChunk) {
+    const T* src = x + (ib[k] & 0x7fffffffu);
+    if constexpr (sizeof(T) == 8) cp_async8(xb + k, src);
+    else cp_async4(xb + k, src);
+  }
+}
+
+template <class T, class CT, int MINB>
+__global__ void __launch_bounds__(kOctChunk, MINB) lapmass_octchunk_pipe_kernel(
+    int64_t n, int64_t nchunk, uint32_t node_cap, const uint32_t* __restrict__ ometa,
+    const uint16_t* __restrict__ lidx, const uint16_t* __restrict__ lelem, const uint32_t* __restrict__ cptr,
+    const uint32_t* __restrict__ cnodes, const uint32_t* __restrict__ cel, const CT* __restrict__ ca,
+    const CT* __restrict__ cb, const T* __restrict__ x, T* __restrict__ y) {
+  extern __shared__ __align__(16) unsigned char oc_smem[];
+  T* xb0 = reinterpret_cast<T*>(oc_smem);
+  T* xb1 = xb0 + node_cap;
+  T* sy = xb1 + node_cap;
+  uint32_t* ib0 = reinterpret_cast<uint32_t*>(sy + node_cap);
+  uint32_t* ib1 = ib0 + node_cap;
+  uint32_t* ib2 = ib1 + node_cap;
+  const int64_t G = gridDim.x;
+  int64_t q = blockIdx.x;
+  if (q >= nchunk) return;
+  // prologue: ids of chunks 0 and 1, then x of chunk 0
+  {
+    const uint32_t a0 = __ldg(cptr + q), a1 = __ldg(cptr + q + 1);
+    octchunk_issue_ids<T>(ib0, cnodes, a0, a1 - a0);
+    if (q + G < nchunk) {
+      const uint32_t b0 = __ldg(cptr + q + G), b1 = __ldg(cptr + q + G + 1);
+      octchunk_issue_ids<T>(ib1, cnodes, b0, b1 - b0);
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    octchunk_issue_x<T>(xb0, ib0, x, a1 - a0);
+    cp_async_commit();
+    for (uint32_t k = threadIdx.x; k < node_cap; k += kOctChunk) sy[k] = T(0);
+    cp_async_wait_all();
+    __syncthreads();
+  }
+  for (int i = 0; q < nchunk; ++i, q += G) {
+    T* xc = (i & 1) ? xb1 : xb0;
+    T* xn = (i & 1) ? xb0 : xb1;
+    uint32_t* ic = (i % 3 == 0) ? ib0 : (i % 3 == 1) ? ib1 : ib2;  // chunk i
+    uint32_t* in1 = (i % 3 == 0) ? ib1 : (i % 3 == 1) ? ib2 : ib0;  // chunk i + 1
+    uint32_t* in2 = (i % 3 == 0) ? ib2 : (i % 3 == 1) ? ib0 : ib1;  // chunk i + 2
+    const uint32_t p0 = __ldg(cptr + q), nn = __ldg(cptr + q + 1) - p0;
+    const uint32_t e0 = __ldg(cel + 2 * q);
+    // 1. in flight during this chunk: x of chunk i + 1, ids of chunk i + 2
+    if (q + G < nchunk) {
+      const uint32_t c0 = __ldg(cptr + q + G), c1 = __ldg(cptr + q + G + 1);
+      octchunk_issue_x<T>(xn, in1, x, c1 - c0);
+    }
+    if (q + 2 * G < nchunk) {
+      const uint32_t d0 = __ldg(cptr + q + 2 * G), d1 = __ldg(cptr + q + 2 * G + 1);
+      octchunk_issue_ids<T>(in2, cnodes, d0, d1 - d0);
+    }
+    cp_async_commit();
+    // 2. this chunk's octets
+    const int64_t o = q * kOctChunk + threadIdx.x;
+    if (o < n) {
+      const uint32_t m = __ldg(ometa + o);
+      uint32_t none = 0;
+      uint16_t li[27];
+      T xv[27], yv[27];
+#pragma unroll
+      for (int p = 0; p < 27; ++p) {
+        li[p] = __ldg(lidx + int64_t(p) * n + o);
+        none |= li[p] == 0xffffu ? (1u << p) : 0u;
+      }
+#pragma unroll
+      for (int p = 0; p < 27; ++p) xv[p] = li[p] != 0xffffu ? xc[li[p]] : T(0);
+      octet_apply<T>(xv, yv, none, m, [&](int c, T& f1, T& f2) {
+        if (ca) {
+          const uint32_t le = __ldg(lelem + int64_t(c) * n + o);
+          f1 *= T(__ldg(ca + e0 + le));
+          f2 *= T(__ldg(cb + e0 + le));
+        }
+      });
+#pragma unroll
+      for (int p = 0; p < 27; ++p)
+        if (li[p] != 0xffffu && yv[p] != T(0)) atomicAdd(sy + li[p], yv[p]);
+    }
+    __syncthreads();
+    // 3. this chunk's sums leave; the accumulator is zeroed for the next
+    for (uint32_t k = threadIdx.x; k < nn; k += kOctChunk) {
+      const uint32_t id = ic[k];
+      T* dst = y + (id & 0x7fffffffu);
+      const T v = sy[k];
+      sy[k] = T(0);
+      st_if(dst, v, !(id >> 31));
+      red_add_if(dst, v, (id >> 31) && v != T(0));
+    }
+    // 4. the next chunk's x and the ids after it have landed
+    cp_async_wait_all();
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------- bulk-copy staging --
 // The warp-tile operator with its tile records staged by the copy engine:
 // one lane per warp issues cp.async.bulk copies of a tile's contiguous
@@ -1230,7 +1357,8 @@ struct MatvecVariant {
   int block, per_sm;  // threads per CTA, CTAs per SM in the grid (0: one thread per element)
   int kind;           // 0 atomic (BLOCK, MINB), 2 warp-tile, 3 + records prefetched, 4 + ids and x too,
                       // 5 records staged by bulk copies, 6 octet (one thread per parent octant),
-                      // 7 octet chunks staged through shared memory, 8 the same, lean
+                      // 7 octet chunks staged through shared memory, 8 the same, lean,
+                      // 9 the same with the staging of the next chunks in flight (cp.async)
   int minb;
   const char* name;
 };
@@ -1256,6 +1384,8 @@ constexpr MatvecVariant kVariants[] = {
     {kOctChunk, 6, 8, 6, "octet chunks of 128, lean, 6 CTAs/SM"},
     {kOctChunk, 8, 8, 8, "octet chunks of 128, lean, 8 CTAs/SM"},
     {kOctChunk, 5, 8, 5, "octet chunks of 128, lean, 5 CTAs/SM"},
+    {kOctChunk, 3, 9, 3, "octet chunks of 128, pipelined staging, 3 CTAs/SM"},
+    {kOctChunk, 4, 9, 4, "octet chunks of 128, pipelined staging, 4 CTAs/SM"},
 };
 // Coefficients of at most this many consecutive elements are staged per chunk.
 constexpr uint32_t kOctCoefCap = 2048;
@@ -1282,7 +1412,20 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
   const MatvecVariant& V = kVariants[v];
   const unsigned g = V.per_sm ? grid_for(da->E, V.block, V.per_sm)
                               : unsigned((da->E + V.block - 1) / V.block > 0 ? (da->E + V.block - 1) / V.block : 1);
-  if (V.kind == 8) {
+  if (V.kind == 9) {
+    const OctetSet& O = da->octs;
+    const size_t smem = (3 * sizeof(T) + 3 * sizeof(uint32_t)) * size_t(O.max_nodes);
+    const unsigned gq = unsigned(std::min<int64_t>(O.nchunk, int64_t(sm_count()) * V.per_sm));
+    auto go = [&](auto kern) -> dg_status {
+      DG_TRY(allow_dynamic_smem(reinterpret_cast<const void*>(kern),
+                                (3 * sizeof(T) + 3 * sizeof(uint32_t)) * 27 * kOctChunk));
+      kern<<<gq, kOctChunk, smem, s>>>(O.n, O.nchunk, O.max_nodes, O.meta.p, O.lidx.p, O.lelem.p, O.cptr.p,
+                                       O.cnodes.p, O.cel.p, ca, cb, x, y);
+      return DG_OK;
+    };
+    if (V.minb == 3) DG_TRY(go(lapmass_octchunk_pipe_kernel<T, CT, 3>));
+    else DG_TRY(go(lapmass_octchunk_pipe_kernel<T, CT, 4>));
+  } else if (V.kind == 8) {
     const OctetSet& O = da->octs;
     const size_t smem = sizeof(T) * 2 * size_t(O.max_nodes);
     const unsigned gq = unsigned(std::min<int64_t>(O.nchunk, int64_t(sm_count()) * V.per_sm));
@@ -1423,7 +1566,7 @@ static dg_status pick_variant(const dg_da* da, int& choice, const CT* ca, const 
     for (int v = 0; v < kNumVariants; ++v) {
       if (kVariants[v].kind >= 2 && kVariants[v].kind <= 5 && da->tiles_w.ntiles == 0) continue;
       if (kVariants[v].kind == 6 && da->octs.n == 0) continue;
-      if ((kVariants[v].kind == 7 || kVariants[v].kind == 8) && da->octs.nchunk == 0) continue;
+      if (kVariants[v].kind >= 7 && da->octs.nchunk == 0) continue;
       for (int trial = 0; trial < 2; ++trial) {
         DG_CUDA(cudaMemsetAsync(flush.p, trial + 1, flush_bytes, s));
         DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));

@@ -480,13 +480,24 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_kernel(
       id[p] = __ldg(oid + int64_t(p) * n + o);
       none |= id[p] == kNoNode ? (1u << p) : 0u;
     }
+    T fa[8], fb[8];
+    if (ca) {
+      const uint32_t cm0 = ometa_cmask(m);
+      uint32_t el[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) el[c] = ((cm0 >> c) & 1u) ? __ldg(oelem + int64_t(c) * n + o) : 0u;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        fa[c] = ((cm0 >> c) & 1u) ? T(__ldg(ca + el[c])) : T(0);
+        fb[c] = ((cm0 >> c) & 1u) ? T(__ldg(cb + el[c])) : T(0);
+      }
+    }
 #pragma unroll
     for (int p = 0; p < 27; ++p) xv[p] = id[p] != kNoNode ? __ldg(x + id[p]) : T(0);
     octet_apply<T>(xv, yv, none, m, [&](int c, T& f1, T& f2) {
       if (ca) {
-        const uint32_t e = __ldg(oelem + int64_t(c) * n + o);
-        f1 *= T(__ldg(ca + e));
-        f2 *= T(__ldg(cb + e));
+        f1 *= fa[c];
+        f2 *= fb[c];
       }
     });
     const uint32_t cm = ometa_cmask(m);
@@ -584,17 +595,22 @@ __global__ void __launch_bounds__(kOctChunk, MINB) lapmass_octchunk_kernel(
         li[p] = __ldg(lidx + int64_t(p) * n + o);
         none |= li[p] == 0xffffu ? (1u << p) : 0u;
       }
+      uint32_t le[8];
+      if (ca) {
+        const uint32_t cm = ometa_cmask(m);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) le[c] = ((cm >> c) & 1u) ? __ldg(lelem + int64_t(c) * n + o) : 0u;
+      }
 #pragma unroll
       for (int p = 0; p < 27; ++p) xv[p] = li[p] != 0xffffu ? sx[li[p]] : T(0);
       octet_apply<T>(xv, yv, none, m, [&](int c, T& f1, T& f2) {
         if (ca) {
-          const uint32_t le = __ldg(lelem + int64_t(c) * n + o);
           if (staged) {
-            f1 *= sa[le];
-            f2 *= sb[le];
+            f1 *= sa[le[c]];
+            f2 *= sb[le[c]];
           } else {
-            f1 *= T(__ldg(ca + e0 + le));
-            f2 *= T(__ldg(cb + e0 + le));
+            f1 *= T(__ldg(ca + e0 + le[c]));
+            f2 *= T(__ldg(cb + e0 + le[c]));
           }
         }
       });
@@ -835,13 +851,27 @@ __global__ void __launch_bounds__(kOctChunk, MINB) lapmass_octchunk_pipe_kernel(
         li[p] = __ldg(lidx + int64_t(p) * n + o);
         none |= li[p] == 0xffffu ? (1u << p) : 0u;
       }
+      // the children's coefficients, all issued before the arithmetic (a
+      // load inside the predicated child loop would expose its round trip
+      // once per child)
+      T fa[8], fb[8];
+      if (ca) {
+        const uint32_t cm = ometa_cmask(m);
+        uint32_t le[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) le[c] = ((cm >> c) & 1u) ? __ldg(lelem + int64_t(c) * n + o) : 0u;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          fa[c] = ((cm >> c) & 1u) ? T(__ldg(ca + e0 + le[c])) : T(0);
+          fb[c] = ((cm >> c) & 1u) ? T(__ldg(cb + e0 + le[c])) : T(0);
+        }
+      }
 #pragma unroll
       for (int p = 0; p < 27; ++p) xv[p] = li[p] != 0xffffu ? xc[li[p]] : T(0);
       octet_apply<T>(xv, yv, none, m, [&](int c, T& f1, T& f2) {
         if (ca) {
-          const uint32_t le = __ldg(lelem + int64_t(c) * n + o);
-          f1 *= T(__ldg(ca + e0 + le));
-          f2 *= T(__ldg(cb + e0 + le));
+          f1 *= fa[c];
+          f2 *= fb[c];
         }
       });
 #pragma unroll

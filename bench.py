@@ -38,16 +38,15 @@ sys.path.insert(0, ROOT)
 
 METRIC = "time to FP64 rel. residual 1e-8 & matvec GDoF/s: chosen vs plain FP64, 1 B200"
 WORKLOAD = "lognormal1m_d14"
-# DRAM bytes (read + write) of one operator launch on the default workload,
-# from one ncu capture per kernel (profiles/lapmass_warp_lognormal1m_d14.md)
-# DRAM bytes per operator launch on the bench mesh, by launch shape (ncu:
-# dram__bytes.sum.per_second x gpu__time_duration.sum of one launch; the
-# summaries under profiles/ give the commands).  First matching prefix wins.
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one operator
+# launch on the default workload, per launch shape, each from a one-kernel
+# ncu capture of that shape (profiles/lapmass_traffic_lognormal1m_d14.md
+# gives the commands); a shape without a capture reports null.
 TRAFFIC = {
-    "warp-tile 32 elems, 3 CTAs/SM, ids and x of the next tile in flight": 337146106,
-    "warp-tile 32 elems, 5 CTAs/SM": 313580000 + 20210000,
-    "warp-tile 32 elems, records by bulk copy": 336114385,
-    "warp-tile": 332613888 + 21873408,
+    "warp-tile 32 elems, 5 CTAs/SM": 313494528 + 19637248,
+    "warp-tile 32 elems, 3 CTAs/SM, ids and x of the next tile in flight": 313441024 + 19751680,
+    "octet b128, 4 CTAs/SM": 217575168 + 18488576,
+    "octet b256, 2 CTAs/SM": 217540864 + 18269184,
 }
 
 
@@ -701,8 +700,7 @@ def main():
                    f"one mesh partitioned over {world} GPUs (SFC-weighted element ranges, ghost exchange over NCCL)"},
         "roofline": {"bound": "hbm", "achieved": round(r["achieved"], 1), "peak": r["peak"], "unit": "GB/s",
                      "frac": round(r["achieved"] / r["peak"], 4),
-                     "traffic": next((v for k, v in TRAFFIC.items() if r["kernel"].startswith(k)), None)
-                     if args.workload == WORKLOAD and args.scale == 1.0 else None,
+                     "traffic": TRAFFIC.get(r["kernel"]) if args.workload == WORKLOAD and args.scale == 1.0 else None,
                      "peak_source": r["peak_kind"], "algorithmic_bytes": int(r["alg_bytes"])},
         "e2e": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r["e2e"].items()},
         "gpu_launches": args.steps,

@@ -52,8 +52,14 @@ struct OctetSet {
   DBuf<uint16_t> lidx;    // [27][n]
   DBuf<uint16_t> lelem;   // [8][n]
   DBuf<uint16_t> lnl;     // [8][E]: per element, the chunk-local index of each vertex's node (the DA's nl)
+  // [n + 1][kOctRec] per octet (and a padding octet without children): the
+  // 27 lattice node ids, the mask of lattice points without a node, the meta
+  // word, 3 words of padding -- one 128-byte record read by the lane-per-child
+  // operator and the tensor-memory multi-RHS kernel
+  DBuf<uint32_t> rec;
 };
 constexpr int kOctChunk = 128;  // octets per chunk (one per thread of the chunked kernel)
+constexpr int kOctRec = 32;     // words per octet record
 }  // namespace dg
 
 struct dg_octree {
@@ -97,6 +103,7 @@ struct dg_mat {
   double mu = 0, lam = 0;
   dg::DBuf<uint8_t> dirichlet; // [N]
   dg::DBuf<double> host_x, host_y;  // device staging of dg_mat_mult_host, kept between calls
+  mutable dg::DBuf<float> tc_coef;  // [octets + 1][16] element scale factors of the tensor-memory multi-RHS kernel
   std::shared_ptr<dg::HostPipe> pipe;
 };
 
@@ -153,6 +160,7 @@ dg_status build_mesh(const dg_octree* tree, dg_da* da, cudaStream_t s);
 // cycles (<= 0: the default) and the check that synchronises s and reports
 // DG_ETIMEOUT (then clears it) when a wait has run out.
 void set_wait_limit(long long cycles);
+long long wait_limit();  // clock cycles a bounded device wait may take
 dg_status device_wait_status(cudaStream_t s);
 dg_status build_tiles(dg_da* da, cudaStream_t s);  // da->tiles_w (kWarpTile)
 dg_status build_octets(dg_da* da, cudaStream_t s);  // da->octs (octet.cu)
@@ -209,6 +217,11 @@ dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int nrhs, int sp
 // ([2][E], a then b; ignored when the operator has none).
 template <class T>
 dg_status mrhs_octet_apply(const dg_mat* A, const T* coef, const T* X, T* Y, int R, cudaStream_t s);
+// Multi-RHS operator on tcgen05 (mrhs_tc.cu): nrhs a multiple of 64, passes 1
+// (TF32 products) or 3 (hi/lo split, FP32-level).
+dg_status mrhs_tc_apply(const dg_mat* A, const float* X, float* Y, int R, int passes, cudaStream_t s);
+// DG_ETIMEOUT (then cleared) when a bounded wait of that kernel ran out.
+dg_status mrhs_tc_take_status();
 dg_status elasticity_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status elasticity_diag(const dg_mat* A, double* d, cudaStream_t s);
 // Dense row-major (3 N) x (3 N) matrix of the elasticity operator, Dirichlet

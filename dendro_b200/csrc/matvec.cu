@@ -515,6 +515,118 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_kernel(
   }
 }
 
+// Octet form with a child per lane: the 8 lanes 8g .. 8g + 7 of a warp work
+// the 8 children of one parent octant (4 octets per warp), lane c child c.
+// A lane holds its child's 8 vertex values in the child's mirrored frame
+// f = v ^ c, in which f_a = 0 is the parent's outer face on axis a and
+// f_a = 1 the middle plane that child c shares with child c ^ (1 << a); the
+// element operator is unchanged by the relabelling (its entries depend on
+// popcount(v ^ w) only).  In that frame:
+//  * vertex f is lattice point sum_a (c_a ? 2 - f_a : f_a) 3^a; a hanging
+//    vertex reads x at its far corner, the parent corner f ^ c (the DA's
+//    node for a hanging vertex), and takes the mean of the values at the
+//    frame vertices j that are bit subsets of f (2 on an edge, 4 on a face:
+//    the interpolation of the hanging-node stencils, handleType2Stencils.C);
+//  * the lattice sums over the children sharing a point are a butterfly: on
+//    axis a the 4 values with f_a = 1 are exchanged with lane c ^ (1 << a)
+//    at the same frame index (one shuffle each), so after the three axes
+//    every sharer holds the point's full sum;
+//  * the transpose of the interpolation is local: a hanging point's sum
+//    goes, times 1/2 (edge) or 1/4 (face), to frame vertex 0 (the parent
+//    corner c) of every child at one of its corners, each of which holds the
+//    point;
+//  * each node's sum leaves once, from the lowest-numbered present child
+//    that shares it.
+// The octet's record (octet.cuh, 128 bytes) gives the node ids, the mask of
+// points without a node and the level; a lane keeps 8 values, 8 ids and its
+// two scale factors, so many warps fit on an SM.
+template <class T, class CT, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) lapmass_octlane_kernel(
+    int64_t n, const uint32_t* __restrict__ orec, const uint32_t* __restrict__ oelem, const CT* __restrict__ ca,
+    const CT* __restrict__ cb, const T* __restrict__ x, T* __restrict__ y) {
+  const int lane = threadIdx.x & 31, c = lane & 7;
+  const int cx = c & 1, cy = (c >> 1) & 1, cz = c >> 2;
+  const int64_t nw = gstride() >> 5;
+  for (int64_t ob = (gtid() >> 5) * 4; ob < n; ob += nw * 4) {
+    const int64_t o = ob + (lane >> 3);
+    const uint32_t* r = orec + (o < n ? o : n) * kOctRec;
+    const uint32_t none = __ldg(r + 27), m = __ldg(r + 28);
+    const uint32_t cm = ometa_cmask(m);
+    const bool present = (cm >> c) & 1u;
+    // lattice index of frame vertex f, and of the parent corner f ^ c
+    const int base = 2 * (cx + 3 * cy + 9 * cz);
+    const int dx = cx ? -1 : 1, dy = cy ? -3 : 3, dz = cz ? -9 : 9;
+    uint32_t hang = 0;
+    T u[8];
+#pragma unroll
+    for (int f = 0; f < 8; ++f) {
+      const int L = base + (f & 1) * dx + ((f >> 1) & 1) * dy + (f >> 2) * dz;
+      const int F = 2 * (((f ^ c) & 1) + 3 * (((f ^ c) >> 1) & 1) + 9 * ((f ^ c) >> 2));
+      const bool h = (f != 0 && f != 7) && ((none >> L) & 1u);
+      hang |= h ? (1u << f) : 0u;
+      const uint32_t id = present ? __ldg(r + (h ? F : L)) : kNoNode;
+      u[f] = id != kNoNode ? __ldg(x + id) : T(0);
+    }
+    T f1 = T(0), f2 = T(0);
+    if (present) {
+      const T hh = elem_h<T>(ometa_lev(m));
+      f1 = hh * T(0.5);
+      f2 = hh * hh * hh * T(0.125);
+      if (ca) {
+        const uint32_t e = __ldg(oelem + int64_t(c) * n + o);
+        f1 *= T(__ldg(ca + e));
+        f2 *= T(__ldg(cb + e));
+      }
+    }
+    // hanging vertices from the raw values: faces first (they read the raw
+    // edge values), then edges
+#pragma unroll
+    for (int f = 3; f < 7; ++f) {
+      if (f == 4) continue;
+      const int b0 = f & -f, b1 = f ^ b0;
+      if ((hang >> f) & 1u) u[f] = ((u[0] + u[f]) + (u[b0] + u[b1])) * T(0.25);
+    }
+#pragma unroll
+    for (int f = 1; f <= 4; f <<= 1)
+      if ((hang >> f) & 1u) u[f] = (u[0] + u[f]) * T(0.5);
+    lapmass_ref(u, f1, f2);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int f = 0; f < 8; ++f)
+        if ((f >> a) & 1) u[f] += __shfl_xor_sync(0xffffffffu, u[f], 1 << a);
+    T fold = T(0);
+#pragma unroll
+    for (int f = 1; f < 7; ++f) {
+      const T w = (f == 1 || f == 2 || f == 4) ? T(0.5) : T(0.25);
+      fold += ((hang >> f) & 1u) ? u[f] * w : T(0);
+    }
+    u[0] += fold;
+    // sharers of frame vertex f: c with the bits of f replaced by any
+    // subset; the node ids are read again from the record (L1) so that they
+    // do not occupy registers during the arithmetic
+#pragma unroll
+    for (int f = 0; f < 8; ++f) {
+      uint32_t subsets = 0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if ((q & ~f) == 0) subsets |= 1u << q;
+      const uint32_t ps = (subsets << (c & ~f)) & cm;
+      const bool mine = present && !((hang >> f) & 1u) && (ps & ((1u << c) - 1u)) == 0u;
+      const int L = base + (f & 1) * dx + ((f >> 1) & 1) * dy + (f >> 2) * dz;
+      const uint32_t id = mine ? __ldg(r + L) : kNoNode;
+      const bool owner = id != kNoNode;
+      T* dst = y + (owner ? id : 0u);
+      if (f == 7) {
+        st_if(dst, u[f], owner && cm == 255u);
+        red_add_if(dst, u[f], owner && cm != 255u);
+      } else {
+        red_add_if(dst, u[f], owner);
+      }
+    }
+  }
+}
+
 constexpr int kStageBatch = 8;  // node values each thread has in flight while staging a chunk
 
 // Chunked octet kernel: a CTA of kOctChunk threads per chunk of kOctChunk
@@ -1388,7 +1500,8 @@ struct MatvecVariant {
   int kind;           // 0 atomic (BLOCK, MINB), 2 warp-tile, 3 + records prefetched, 4 + ids and x too,
                       // 5 records staged by bulk copies, 6 octet (one thread per parent octant),
                       // 7 octet chunks staged through shared memory, 8 the same, lean,
-                      // 9 the same with the staging of the next chunks in flight (cp.async)
+                      // 9 the same with the staging of the next chunks in flight (cp.async),
+                      // 10 octet lanes (a child per lane, 8 lanes per parent octant)
   int minb;
   const char* name;
 };
@@ -1416,6 +1529,10 @@ constexpr MatvecVariant kVariants[] = {
     {kOctChunk, 5, 8, 5, "octet chunks of 128, lean, 5 CTAs/SM"},
     {kOctChunk, 3, 9, 3, "octet chunks of 128, pipelined staging, 3 CTAs/SM"},
     {kOctChunk, 4, 9, 4, "octet chunks of 128, pipelined staging, 4 CTAs/SM"},
+    {256, 4, 10, 4, "octet lanes b256, 4 CTAs/SM"},
+    {256, 6, 10, 6, "octet lanes b256, 6 CTAs/SM"},
+    {128, 12, 10, 12, "octet lanes b128, 12 CTAs/SM"},
+    {256, 5, 10, 5, "octet lanes b256, 5 CTAs/SM"},
 };
 // Coefficients of at most this many consecutive elements are staged per chunk.
 constexpr uint32_t kOctCoefCap = 2048;
@@ -1482,6 +1599,17 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
     if (V.minb == 2) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 2>));
     else if (V.minb == 3) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 3>));
     else DG_TRY(go(lapmass_octchunk_kernel<T, CT, 4>));
+  } else if (V.kind == 10) {
+    const OctetSet& O = da->octs;
+    const unsigned gl = grid_for(8 * O.n, V.block, V.per_sm);
+    if (V.block == 128)
+      lapmass_octlane_kernel<T, CT, 128, 12><<<gl, 128, 0, s>>>(O.n, O.rec.p, O.elem.p, ca, cb, x, y);
+    else if (V.minb == 4)
+      lapmass_octlane_kernel<T, CT, 256, 4><<<gl, 256, 0, s>>>(O.n, O.rec.p, O.elem.p, ca, cb, x, y);
+    else if (V.minb == 5)
+      lapmass_octlane_kernel<T, CT, 256, 5><<<gl, 256, 0, s>>>(O.n, O.rec.p, O.elem.p, ca, cb, x, y);
+    else
+      lapmass_octlane_kernel<T, CT, 256, 6><<<gl, 256, 0, s>>>(O.n, O.rec.p, O.elem.p, ca, cb, x, y);
   } else if (V.kind == 6) {
     const OctetSet& O = da->octs;
     const unsigned go = grid_for(O.n, V.block, V.per_sm);
@@ -1550,7 +1678,7 @@ static int forced_variant() {
     v = -1;
     if (e && *e) {
       const int kind = !strcmp(e, "atomic") ? 0 : !strcmp(e, "warp") ? 2 : !strcmp(e, "octet") ? 6
-                     : !strcmp(e, "chunk") ? 7 : -1;
+                     : !strcmp(e, "chunk") ? 7 : !strcmp(e, "lanes") ? 10 : -1;
       if (kind >= 0) {
         for (int i = kNumVariants - 1; i >= 0; --i)
           if (kVariants[i].kind == kind) v = i;
@@ -1595,8 +1723,8 @@ static dg_status pick_variant(const dg_da* da, int& choice, const CT* ca, const 
     DG_TRY((launch_variant<T, CT>(0, da, ca, cb, x, y, s)));
     for (int v = 0; v < kNumVariants; ++v) {
       if (kVariants[v].kind >= 2 && kVariants[v].kind <= 5 && da->tiles_w.ntiles == 0) continue;
-      if (kVariants[v].kind == 6 && da->octs.n == 0) continue;
-      if (kVariants[v].kind >= 7 && da->octs.nchunk == 0) continue;
+      if ((kVariants[v].kind == 6 || kVariants[v].kind == 10) && da->octs.n == 0) continue;
+      if (kVariants[v].kind >= 7 && kVariants[v].kind <= 9 && da->octs.nchunk == 0) continue;
       for (int trial = 0; trial < 2; ++trial) {
         DG_CUDA(cudaMemsetAsync(flush.p, trial + 1, flush_bytes, s));
         DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
@@ -1634,9 +1762,11 @@ static dg_status lapmass_launch(dg_da* da, int& choice, const CT* ca, const CT* 
 int matvec_variant_count() { return kNumVariants; }
 
 void set_wait_limit(long long cycles) { g_wait_limit = cycles > 0 ? cycles : kDefaultWaitLimit; }
+long long wait_limit() { return g_wait_limit; }
 
 dg_status device_wait_status(cudaStream_t s) {
   DG_CUDA(cudaStreamSynchronize(s));
+  DG_TRY(mrhs_tc_take_status());
   int v = 0, drained = 0;
   DG_CUDA(cudaMemcpyFromSymbol(&v, g_wait_status, sizeof(int)));
   DG_CUDA(cudaMemcpyFromSymbol(&drained, g_drain_gave_up, sizeof(int)));

@@ -584,9 +584,11 @@ dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int R, int split
   dg_da* da = A->da;
   DG_CHECK(A->kind == 0, DG_EINVAL, "mat_mult_multi: scalar operator expected");
   DG_CHECK(R > 0 && R % kRC == 0, DG_EINVAL, "mat_mult_multi: nrhs must be a positive multiple of 16");
-  DG_CHECK(split == 0 || split == 1 || split == 3, DG_EINVAL, "mat_mult_multi: split must be 0, 1 or 3");
+  DG_CHECK(split == 0 || split == 1 || split == 3 || split == 4 || split == 5, DG_EINVAL,
+           "mat_mult_multi: split must be 0, 1, 3, 4 or 5");
   DG_CHECK((reinterpret_cast<uintptr_t>(X) & 15) == 0 && (reinterpret_cast<uintptr_t>(Y) & 15) == 0, DG_EINVAL,
            "mat_mult_multi: X and Y must be 16-byte aligned");
+  if (split >= 4) return mrhs_tc_apply(A, X, Y, R, split == 4 ? 1 : 3, s);
   static float4* tbls[64] = {};  // one table per device, kept for the process
   int dev = 0;
   DG_CUDA(cudaGetDevice(&dev));

@@ -361,6 +361,25 @@ dg_status build_chunks(dg_da* da, cudaStream_t s) {
 
 }  // namespace
 
+// Per octet one 128-byte record (and a padding octet at index n with no
+// children): the 27 lattice node ids, the mask of lattice points without a
+// node, the meta word, three words of padding.
+__global__ void octet_records(int64_t n, const uint32_t* __restrict__ ometa, const uint32_t* __restrict__ oid,
+                              uint32_t* __restrict__ rec) {
+  for (int64_t o = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; o <= n; o += int64_t(gridDim.x) * blockDim.x) {
+    uint32_t* r = rec + o * kOctRec;
+    uint32_t none = 0;
+    for (int p = 0; p < 27; ++p) {
+      const uint32_t id = o < n ? oid[int64_t(p) * n + o] : kNoNode;
+      r[p] = id;
+      none |= id == kNoNode ? (1u << p) : 0u;
+    }
+    r[27] = none;
+    r[28] = o < n ? ometa[o] : 0u;
+    r[29] = r[30] = r[31] = 0u;
+  }
+}
+
 dg_status build_octets(dg_da* da, cudaStream_t s) {
   const int64_t E = da->E;
   const uint32_t Dp = da->D;
@@ -397,6 +416,9 @@ dg_status build_octets(dg_da* da, cudaStream_t s) {
   DG_CHECK(!(herr & 1u), DG_EUNBALANCED, "octets: element without its parent entry");
   DG_CHECK(!(herr & 2u), DG_EUNBALANCED, "octets: a lattice point hangs for one child and is a node for another");
   DG_CHECK(!(herr & 4u), DG_EUNBALANCED, "octets: a parent corner needed by a hanging point is not a node");
+  DG_TRY(O.rec.alloc((n + 1) * kOctRec));
+  octet_records<<<grid_for(n + 1, 256), 256, 0, s>>>(n, O.meta.p, O.id.p, O.rec.p);
+  DG_CUDA(cudaGetLastError());
   return build_chunks(da, s);
 }
 

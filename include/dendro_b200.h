@@ -220,7 +220,11 @@ int dg_mat_kernel_count(void);
  * of 16.  The element contraction runs on the tensor cores with TF32 inputs
  * and FP32 accumulation; split = 3 splits each input into a TF32 high part and
  * a TF32 remainder (three products, FP32-level accuracy), split = 1 uses one
- * TF32 product; split = 0 runs the octet form on the CUDA cores instead (a
+ * TF32 product (both with mma.sync on the warp tiles); split = 5 and split = 4
+ * are the same two precisions on the 5th-generation tensor cores (tcgen05.mma
+ * with accumulators in tensor memory: per pair of element parents their
+ * assembled 27 x 27 lattice matrix times the lattice rows of X; nrhs a
+ * multiple of 64); split = 0 runs the octet form on the CUDA cores instead (a
  * warp per element parent and 32 right-hand sides, exact FP32 products;
  * nrhs a multiple of 32).  Scalar Laplacian + mass operators only. */
 dg_status dg_mat_mult_multi(dg_mat* A, const float* X, float* Y, int nrhs, int split, void* stream);

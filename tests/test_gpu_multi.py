@@ -1,6 +1,7 @@
-"""Multi-right-hand-side operator (on the tensor cores, split 3 / 1, and in
-the octet form on the CUDA cores, split 0) against the oracle's FP64
-operator applied column by column."""
+"""Multi-right-hand-side operator (mma.sync on the warp tiles, split 3 / 1;
+tcgen05 with tensor-memory accumulators on octet pairs, split 5 / 4; the
+octet form on the CUDA cores, split 0) against the oracle's FP64 operator
+applied column by column."""
 import numpy as np
 import pytest
 
@@ -23,7 +24,8 @@ def setup(gpu, oracle, name):
 # 32-wide block kernel (DG_MRHS_KERNEL=block64: 64-wide where they divide)
 @pytest.mark.parametrize("name,nrhs,coef", [("lognormal20k_d12", 32, True), ("gauss20k_d10", 16, False),
                                              ("corner_points_d5", 48, True), ("lognormal20k_d12", 64, True),
-                                             ("gauss20k_d10", 96, False), ("uniform8k_d9_m4", 64, False)])
+                                             ("gauss20k_d10", 96, False), ("uniform8k_d9_m4", 64, False),
+                                             ("gauss20k_d10", 128, True), ("single_point", 64, True)])
 def test_multi_rhs_matches_oracle(gpu, oracle, name, nrhs, coef):
     import torch
     ref, da = setup(gpu, oracle, name)
@@ -32,7 +34,8 @@ def test_multi_rhs_matches_oracle(gpu, oracle, name, nrhs, coef):
     X = np.random.default_rng(6).uniform(-1, 1, (ref.N, nrhs))
     Yr = np.stack([ref.matvec(X[:, j], c) for j in range(nrhs)], 1)
     Xd = torch.tensor(X, dtype=torch.float32, device="cuda")
-    forms = ((3, TOL_SPLIT3), (1, TOL_SPLIT1)) + (((0, TOL_SPLIT3),) if nrhs % 32 == 0 else ())
+    forms = ((3, TOL_SPLIT3), (1, TOL_SPLIT1)) + (((0, TOL_SPLIT3),) if nrhs % 32 == 0 else ()) + \
+        (((5, TOL_SPLIT3), (4, TOL_SPLIT1)) if nrhs % 64 == 0 else ())
     for split, tol in forms:
         Y = A.mult_multi(Xd, split=split).double().cpu().numpy()
         err = np.linalg.norm(Y - Yr, axis=0) / np.linalg.norm(Yr, axis=0)
@@ -45,3 +48,5 @@ def test_multi_rhs_rejects_bad_shapes(gpu, oracle):
     A = gpu.Jacobian2(da)
     with pytest.raises(gpu.DendroError):
         A.mult_multi(torch.zeros((ref.N, 20), dtype=torch.float32, device="cuda"))
+    with pytest.raises(gpu.DendroError):  # the tensor-memory form takes multiples of 64
+        A.mult_multi(torch.zeros((ref.N, 32), dtype=torch.float32, device="cuda"), split=4)

@@ -501,8 +501,8 @@ def run_multi(dev, steps, nrhs=64):
     Y = torch.empty_like(X)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
-    out = {"workload": "uniform512k_d12", "elements": E, "nodes": N, "nrhs": nrhs}
-    for split in (0, 3, 1):
+    out = {"workload": "uniform512k_d12", "elements": E, "nodes": N, "nrhs": nrhs, "octets": da.octets}
+    for split in (0, 3, 1, 5, 4):
         for _ in range(3):
             A.mult_multi(X, Y, split=split)
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
@@ -514,12 +514,16 @@ def run_multi(dev, steps, nrhs=64):
         torch.cuda.synchronize()
         ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
         alg = 36 * E + 2 * 4 * nrhs * N  # element record + X read + Y written (FP32)
-        tag = "octet_cuda_cores" if split == 0 else f"split{split}"
+        tag = {0: "octet_cuda_cores", 5: "tcgen05_split5", 4: "tcgen05_split4"}.get(split, f"split{split}")
         out[tag] = {"ms": round(ms, 4), "gdofs": round(N * nrhs / (ms * 1e-3) / 1e9, 3),
                     "achieved_gbs": round(alg / (ms * 1e-3) / 1e9, 1),
                     "frac_of_hbm": round(alg / (ms * 1e-3) / 1e9 / measured_peaks()[0], 4)}
-        if split:
+        if split in (1, 3):  # m16n8k8 per element and 32 right-hand sides: 2 * 64 * nrhs flops per element
             out[tag]["tensor_tflops"] = round(2 * 64 * nrhs * E * split / (ms * 1e-3) / 1e12, 2)
+        elif split in (4, 5):  # per pair of octets and 64 right-hand sides: M 128 x N 64 x K 32 per pass
+            passes = 1 if split == 4 else 3
+            flops = 2 * 128 * 64 * 32 * passes * ((da.octets + 1) // 2) * (nrhs // 64)
+            out[tag]["tensor_tflops"] = round(flops / (ms * 1e-3) / 1e12, 2)
     out["algorithmic_bytes"] = int(36 * E + 8 * nrhs * N)
     # the 64 right-hand sides solved together to FP64 relative residual 1e-8
     # (flexible PCG per column, FP64 outer, one FP32 V-cycle for all columns),
@@ -546,6 +550,10 @@ def run_multi(dev, steps, nrhs=64):
                               "(octet multi-RHS operator on every level), dense FP64 coarse solve"}
     out["method"] = {"split3/split1": "mma.sync m16n8k8 TF32, 32 right-hand sides per element pass on the warp "
                                        "tiles (split3: hi/lo TF32 split, three products), FP32 accumulation",
+                     "tcgen05_split5/split4": "tcgen05.mma kind::tf32, accumulators in tensor memory: per pair of "
+                                              "element parents the assembled 27 x 27 lattice matrices times the "
+                                              "lattice values of 64 right-hand sides (M 128, N 64, K 32; split5: "
+                                              "hi/lo split, three passes)",
                      "octet_cuda_cores": "a warp per (parent octant, 32 right-hand sides), Walsh-form element "
                                          "operators in FP32 registers, coalesced rows of X and Y"}
     return out

@@ -137,6 +137,7 @@ class DA:
         check(lib().dg_da_sizes(self.h, C.byref(E), C.byref(N), C.byref(P)), "da_sizes")
         self.E, self.N, self.P = E.value, N.value, P.value
         self.maxDepth = int(lib().dg_da_max_depth(self.h))  # embedded depth
+        self.octets = int(lib().dg_da_octets(self.h))  # parent octants with leaf children
 
     @classmethod
     def from_maps(cls, max_depth, nlist, level, cnum, hmask, node_xyz, elem_xyz) -> "DA":
@@ -223,9 +224,11 @@ class _Mat:
     def mult_multi(self, X, Y=None, split: int = 3, stream=None):
         """Y = A X for the columns of X, a CUDA float32 tensor [N, nrhs]
         (nrhs a multiple of 16), on the tensor cores (split 3: FP32-level
-        accuracy from three TF32 products; 1: one TF32 product), or with
-        split 0 in the octet form on the CUDA cores (exact FP32 products;
-        nrhs a multiple of 32)."""
+        accuracy from three TF32 products; 1: one TF32 product; 5 and 4: the
+        same two precisions with tcgen05 and tensor-memory accumulators on
+        pairs of element parents, nrhs a multiple of 64), or with split 0 in
+        the octet form on the CUDA cores (exact FP32 products; nrhs a multiple
+        of 32)."""
         import torch
         if not (X.is_cuda and X.dtype == torch.float32 and X.dim() == 2 and X.is_contiguous()):
             raise TypeError("X must be a contiguous CUDA float32 tensor [N, nrhs]")

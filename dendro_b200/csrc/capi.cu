@@ -274,6 +274,8 @@ dg_status dg_da_sizes(const dg_da* da, int64_t* elements, int64_t* nodes, int64_
 
 uint32_t dg_da_max_depth(const dg_da* da) { return da ? da->D : 0; }
 
+int64_t dg_da_octets(const dg_da* da) { return da ? da->octs.n : 0; }
+
 dg_status dg_da_export(const dg_da* da, uint32_t* nlist, uint8_t* hmask, uint8_t* cnum, uint8_t* etype, uint8_t* level,
                        uint32_t* node_xyz, uint32_t* elem_xyz, uint8_t* node_bdy) {
   DG_CHECK(da, DG_EINVAL, "da_export: null mesh");

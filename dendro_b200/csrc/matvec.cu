@@ -627,6 +627,130 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_octlane_kernel(
   }
 }
 
+// Octet form with a column of two children per lane: the 4 lanes 4g .. 4g + 3
+// of a warp work one parent octant (8 octets per warp); lane q = (qx, qy)
+// holds the two children c = q (lower half, z bit 0) and c = q + 4 (upper),
+// i.e. the 12 lattice points with x in {qx, qx + 1}, y in {qy, qy + 1} and
+// z in {0, 1, 2}.  Lane point i = fx + 2 fy + 4 z, mirrored on x and y
+// (lattice coordinate qx ? 2 - fx : fx, the same for y), so that fx = 1 /
+// fy = 1 are the planes shared with lane q ^ 1 / q ^ 2 and z = 1 the plane the
+// lane's two children share.  Per octet a lane
+//  * reads x at its 12 points, a hanging point (no node in the record) as the
+//    mean of its 2 or 4 parent corners (the interpolation T of the
+//    hanging-node stencils, handleType2Stencils.C);
+//  * applies the two children's element operators (points 0..7 and 4..11;
+//    the operator is unchanged by the mirroring) and adds their results;
+//  * sums the shared planes with the neighbour lanes (one shuffle per value
+//    on x, one on y): every sharer then holds the full lattice sum;
+//  * folds each hanging point's sum, times 1/2 (edge) or 1/4 (face), onto
+//    its corners in the lane's own range (every lane holding one of the
+//    corners also holds the point);
+//  * adds each node's sum into y once, from the sharer with qx = 0 / qy = 0 on
+//    the shared axes.
+// A lane keeps 12 values, so the kernel runs at twice the warps per SM of
+// the one-thread-per-octet form with about the same instructions per element.
+template <class T, class CT, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) lapmass_octquad_kernel(
+    int64_t n, const uint32_t* __restrict__ orec, const uint32_t* __restrict__ oelem, const CT* __restrict__ ca,
+    const CT* __restrict__ cb, const T* __restrict__ x, T* __restrict__ y) {
+  const int lane = threadIdx.x & 31, q = lane & 3, qx = q & 1, qy = q >> 1;
+  const int base = (qx ? 2 : 0) + (qy ? 6 : 0), sx = qx ? -1 : 1, sy = qy ? -3 : 3;
+  const int64_t nw = gstride() >> 5;
+  for (int64_t ob = (gtid() >> 5) * 8; ob < n; ob += nw * 8) {
+    const int64_t o = ob + (lane >> 2);
+    const uint32_t* r = orec + (o < n ? o : n) * kOctRec;
+    const uint32_t none = __ldg(r + 27), m = __ldg(r + 28);
+    const uint32_t cm = ometa_cmask(m);
+    uint32_t hang = 0;
+    T u[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+      const int L = base + sx * (i & 1) + sy * ((i >> 1) & 1) + 9 * (i >> 2);
+      const bool h = (none >> L) & 1u;
+      hang |= h ? (1u << i) : 0u;
+      const uint32_t id = h ? kNoNode : __ldg(r + L);
+      u[i] = id != kNoNode ? __ldg(x + id) : T(0);
+    }
+    if (hang) {
+#pragma unroll
+      for (int i = 0; i < 12; ++i) {
+        const int fx = i & 1, fy = (i >> 1) & 1, z = i >> 2;
+        const int nf = fx + fy + (z == 1);
+        if (nf == 0 || nf == 3 || !((hang >> i) & 1u)) continue;
+        const int L = base + sx * fx + sy * fy + 9 * z;
+        // corners: L -/+ the lattice stride of each free axis (1, 3, 9); a
+        // point that no present child has may have corners without nodes
+        const int s0 = fx ? 1 : fy ? 3 : 9;
+        const int s1 = nf == 2 ? ((fx && fy) ? 3 : 9) : 0;
+        auto xat = [&](int Lc) {
+          const uint32_t id = __ldg(r + Lc);
+          return id != kNoNode ? __ldg(x + id) : T(0);
+        };
+        if (nf == 1) u[i] = (xat(L - s0) + xat(L + s0)) * T(0.5);
+        else u[i] = ((xat(L - s0 - s1) + xat(L + s0 - s1)) + (xat(L - s0 + s1) + xat(L + s0 + s1))) * T(0.25);
+      }
+    }
+    T f1[2] = {T(0), T(0)}, f2[2] = {T(0), T(0)};
+    const T hh = elem_h<T>(ometa_lev(m));
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int c = q + 4 * k;
+      if ((cm >> c) & 1u) {
+        f1[k] = hh * T(0.5);
+        f2[k] = hh * hh * hh * T(0.125);
+        if (ca) {
+          const uint32_t e = __ldg(oelem + int64_t(c) * n + o);
+          f1[k] *= T(__ldg(ca + e));
+          f2[k] *= T(__ldg(cb + e));
+        }
+      }
+    }
+    T lo[8], up[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      lo[v] = u[v];
+      up[v] = u[v + 4];
+    }
+    lapmass_ref(lo, f1[0], f2[0]);
+    lapmass_ref(up, f1[1], f2[1]);
+#pragma unroll
+    for (int i = 0; i < 12; ++i) u[i] = (i < 8 ? lo[i] : T(0)) + (i >= 4 ? up[i - 4] : T(0));
+#pragma unroll
+    for (int i = 0; i < 12; ++i)
+      if (i & 1) u[i] += __shfl_xor_sync(0xffffffffu, u[i], 1);
+#pragma unroll
+    for (int i = 0; i < 12; ++i)
+      if (i & 2) u[i] += __shfl_xor_sync(0xffffffffu, u[i], 2);
+    if (hang) {
+#pragma unroll
+      for (int i = 0; i < 12; ++i) {
+        const int fx = i & 1, fy = (i >> 1) & 1, z = i >> 2;
+        const int nf = fx + fy + (z == 1);
+        if (nf == 0 || nf == 3) continue;
+        const T w = ((hang >> i) & 1u) ? u[i] * (nf == 1 ? T(0.5) : T(0.25)) : T(0);
+        // its corners in this lane's range are the parent corners of the
+        // lane's column, points 0 (z = 0) and 8 (z = 2)
+        if (z != 2) u[0] += w;
+        if (z != 0) u[8] += w;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+      const bool mine = (!(i & 1) || !qx) && (!(i & 2) || !qy) && !((hang >> i) & 1u);
+      const int L = base + sx * (i & 1) + sy * ((i >> 1) & 1) + 9 * (i >> 2);
+      const uint32_t id = mine ? __ldg(r + L) : kNoNode;
+      const bool go = id != kNoNode && u[i] != T(0);
+      T* dst = y + (go ? id : 0u);
+      if (i == 7) {  // the parent's centre: only this octet's children touch it when all 8 are leaves
+        st_if(dst, u[i], go && cm == 255u);
+        red_add_if(dst, u[i], go && cm != 255u);
+      } else {
+        red_add_if(dst, u[i], go);
+      }
+    }
+  }
+}
+
 constexpr int kStageBatch = 8;  // node values each thread has in flight while staging a chunk
 
 // Chunked octet kernel: a CTA of kOctChunk threads per chunk of kOctChunk
@@ -1501,7 +1625,8 @@ struct MatvecVariant {
                       // 5 records staged by bulk copies, 6 octet (one thread per parent octant),
                       // 7 octet chunks staged through shared memory, 8 the same, lean,
                       // 9 the same with the staging of the next chunks in flight (cp.async),
-                      // 10 octet lanes (a child per lane, 8 lanes per parent octant)
+                      // 10 octet lanes (a child per lane, 8 lanes per parent octant),
+                      // 11 octet quads (a column of two children per lane, 4 lanes per octant)
   int minb;
   const char* name;
 };
@@ -1530,9 +1655,7 @@ constexpr MatvecVariant kVariants[] = {
     {kOctChunk, 3, 9, 3, "octet chunks of 128, pipelined staging, 3 CTAs/SM"},
     {kOctChunk, 4, 9, 4, "octet chunks of 128, pipelined staging, 4 CTAs/SM"},
     {256, 4, 10, 4, "octet lanes b256, 4 CTAs/SM"},
-    {256, 6, 10, 6, "octet lanes b256, 6 CTAs/SM"},
-    {128, 12, 10, 12, "octet lanes b128, 12 CTAs/SM"},
-    {256, 5, 10, 5, "octet lanes b256, 5 CTAs/SM"},
+    {256, 4, 11, 4, "octet quads b256, 4 CTAs/SM"},
 };
 // Coefficients of at most this many consecutive elements are staged per chunk.
 constexpr uint32_t kOctCoefCap = 2048;
@@ -1599,17 +1722,14 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
     if (V.minb == 2) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 2>));
     else if (V.minb == 3) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 3>));
     else DG_TRY(go(lapmass_octchunk_kernel<T, CT, 4>));
+  } else if (V.kind == 11) {
+    const OctetSet& O = da->octs;
+    lapmass_octquad_kernel<T, CT, 256, 4><<<grid_for(4 * O.n, 256, V.per_sm), 256, 0, s>>>(O.n, O.rec.p, O.elem.p,
+                                                                                          ca, cb, x, y);
   } else if (V.kind == 10) {
     const OctetSet& O = da->octs;
-    const unsigned gl = grid_for(8 * O.n, V.block, V.per_sm);
-    if (V.block == 128)
-      lapmass_octlane_kernel<T, CT, 128, 12><<<gl, 128, 0, s>>>(O.n, O.rec.p, O.elem.p, ca, cb, x, y);
-    else if (V.minb == 4)
-      lapmass_octlane_kernel<T, CT, 256, 4><<<gl, 256, 0, s>>>(O.n, O.rec.p, O.elem.p, ca, cb, x, y);
-    else if (V.minb == 5)
-      lapmass_octlane_kernel<T, CT, 256, 5><<<gl, 256, 0, s>>>(O.n, O.rec.p, O.elem.p, ca, cb, x, y);
-    else
-      lapmass_octlane_kernel<T, CT, 256, 6><<<gl, 256, 0, s>>>(O.n, O.rec.p, O.elem.p, ca, cb, x, y);
+    lapmass_octlane_kernel<T, CT, 256, 4><<<grid_for(8 * O.n, 256, V.per_sm), 256, 0, s>>>(O.n, O.rec.p, O.elem.p,
+                                                                                          ca, cb, x, y);
   } else if (V.kind == 6) {
     const OctetSet& O = da->octs;
     const unsigned go = grid_for(O.n, V.block, V.per_sm);
@@ -1678,7 +1798,7 @@ static int forced_variant() {
     v = -1;
     if (e && *e) {
       const int kind = !strcmp(e, "atomic") ? 0 : !strcmp(e, "warp") ? 2 : !strcmp(e, "octet") ? 6
-                     : !strcmp(e, "chunk") ? 7 : !strcmp(e, "lanes") ? 10 : -1;
+                     : !strcmp(e, "chunk") ? 7 : !strcmp(e, "lanes") ? 10 : !strcmp(e, "quads") ? 11 : -1;
       if (kind >= 0) {
         for (int i = kNumVariants - 1; i >= 0; --i)
           if (kVariants[i].kind == kind) v = i;
@@ -1723,7 +1843,7 @@ static dg_status pick_variant(const dg_da* da, int& choice, const CT* ca, const 
     DG_TRY((launch_variant<T, CT>(0, da, ca, cb, x, y, s)));
     for (int v = 0; v < kNumVariants; ++v) {
       if (kVariants[v].kind >= 2 && kVariants[v].kind <= 5 && da->tiles_w.ntiles == 0) continue;
-      if ((kVariants[v].kind == 6 || kVariants[v].kind == 10) && da->octs.n == 0) continue;
+      if ((kVariants[v].kind == 6 || kVariants[v].kind >= 10) && da->octs.n == 0) continue;
       if (kVariants[v].kind >= 7 && kVariants[v].kind <= 9 && da->octs.nchunk == 0) continue;
       for (int trial = 0; trial < 2; ++trial) {
         DG_CUDA(cudaMemsetAsync(flush.p, trial + 1, flush_bytes, s));

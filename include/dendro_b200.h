@@ -123,6 +123,9 @@ dg_status dg_da_create_from_maps(int64_t E, int64_t N, uint32_t max_depth, const
  * include/oda/oda.h:668-684) and positive-boundary pseudo-octants. */
 dg_status dg_da_sizes(const dg_da* da, int64_t* elements, int64_t* nodes, int64_t* pseudo_octants);
 uint32_t dg_da_max_depth(const dg_da* da); /* embedded depth (maxDepth + 1) */
+/* Parent octants with at least one leaf child: the units of the octet
+ * operator kernels (no reference counterpart; 0 for batched meshes). */
+int64_t dg_da_octets(const dg_da* da);
 
 /* Copy the maps to host memory; any pointer may be NULL.  nlist [E][8]
  * (getNodeIndices, include/oda/oda.txx:1111), hmask [E]

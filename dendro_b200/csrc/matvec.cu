@@ -1645,7 +1645,7 @@ constexpr MatvecVariant kVariants[] = {
     {128, 3, 6, 3, "octet b128, 3 CTAs/SM"},
     {128, 4, 6, 4, "octet b128, 4 CTAs/SM"},
     {256, 2, 6, 2, "octet b256, 2 CTAs/SM"},
-    {64, 8, 6, 8, "octet b64, 8 CTAs/SM"},
+    {128, 5, 6, 5, "octet b128, 5 CTAs/SM"},
     {kOctChunk, 2, 7, 2, "octet chunks of 128, 2 CTAs/SM"},
     {kOctChunk, 3, 7, 3, "octet chunks of 128, 3 CTAs/SM"},
     {kOctChunk, 4, 7, 4, "octet chunks of 128, 4 CTAs/SM"},
@@ -1735,12 +1735,12 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
     const unsigned go = grid_for(O.n, V.block, V.per_sm);
     if (V.block == 128 && V.minb == 3)
       lapmass_octet_kernel<T, CT, 128, 3><<<go, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
+    else if (V.block == 128 && V.minb == 5)
+      lapmass_octet_kernel<T, CT, 128, 5><<<go, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
     else if (V.block == 128)
       lapmass_octet_kernel<T, CT, 128, 4><<<go, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
-    else if (V.block == 256)
-      lapmass_octet_kernel<T, CT, 256, 2><<<go, 256, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
     else
-      lapmass_octet_kernel<T, CT, 64, 8><<<go, 64, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
+      lapmass_octet_kernel<T, CT, 256, 2><<<go, 256, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
   } else if (V.kind == 5) {
     const TileSet& ts = da->tiles_w;
     const unsigned gt = grid_for(ts.ntiles * 32, 32 * kTmaWarps, V.per_sm);

@@ -37,9 +37,9 @@
 // no-op for kind::tf32 on this hardware: the accumulator was left untouched.)
 // The epilogue reads each thread's row of D (32 lattice columns of one octet
 // and one right-hand side) with tcgen05.ld, folds the hanging points' sums
-// onto their corners (T^T) and adds each node's value into Y with a global
-// reduction; the 32 lanes of a warp hold 32 consecutive right-hand sides, so
-// every reduction instruction covers 128 contiguous bytes.
+// onto their corners (T^T), stages the pair's 2 x 27 lattice rows in shared
+// memory and adds them into Y with 16-byte global reductions (4 consecutive
+// right-hand sides of one node per lane).
 //
 // Passes: 1 = TF32 products of the FP32 inputs; 3 = each input split into a
 // TF32 high part and its remainder, D = A_hi B_hi + A_lo B_hi + A_hi B_lo
@@ -144,10 +144,21 @@ __device__ __forceinline__ bool bar_try(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for phase `parity`: false once `limit` clock cycles have passed.
+// Bounded wait for phase `parity`: false once `limit` clock cycles have
+// passed.  Each try suspends the thread in hardware (up to a 0.1 ms hint)
+// until the phase completes, so the wait issues few instructions.
+__device__ __forceinline__ bool bar_try_suspend(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(su32(bar)), "r"(parity), "r"(100000u)
+      : "memory");
+  return ok != 0;
+}
 __device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity, long long limit) {
   const long long t0 = clock64();
-  while (!bar_try(bar, parity))
+  while (!bar_try_suspend(bar, parity))
     if (clock64() - t0 > limit) return false;
   return true;
 }
@@ -219,7 +230,7 @@ __global__ void __launch_bounds__(kTcThreads) mrhs_tc_kernel(int64_t npairs, int
   auto B_lo = [&](int st) { return sbase + uint32_t(st * L::kStage + 2 * kTcAbytes + kTcBbytes); };
 
   const int64_t items = npairs * ncb;
-  if (int64_t(blockIdx.x) >= items) return;
+  if (int64_t(blockIdx.x) * ((items + gridDim.x - 1) / gridDim.x) >= items) return;
 
   // operands start at zero: rows 27..31, the zero entries of Klat and the
   // rows of untouched lattice points are never written again
@@ -253,7 +264,11 @@ __global__ void __launch_bounds__(kTcThreads) mrhs_tc_kernel(int64_t npairs, int
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  auto item_of = [&](int64_t k) { return int64_t(blockIdx.x) + k * int64_t(gridDim.x); };
+  // each CTA works a contiguous range of pairs (neighbours on the curve
+  // share nodes, so their reductions meet in L2)
+  const int64_t per = (items + gridDim.x - 1) / gridDim.x;
+  const int64_t first = int64_t(blockIdx.x) * per, last = first + per < items ? first + per : items;
+  auto item_of = [&](int64_t k) { return first + k < last ? first + k : items; };
   // records of local item k into meta slot k % 3
   auto issue_meta = [&](int64_t k) {
     const int64_t it = item_of(k);
@@ -386,10 +401,28 @@ __global__ void __launch_bounds__(kTcThreads) mrhs_tc_kernel(int64_t npairs, int
         v[p + s0 + s1] += h;
       }
     }
+    // the lattice sums through the stage's A buffer (its MMA has completed),
+    // then out as 16-byte reductions: 4 consecutive right-hand sides of one
+    // node per lane
+    tc_fence_before();
+    const uint32_t sbuf = A_hi(st);
 #pragma unroll
-    for (int p = 0; p < 27; ++p) {
-      const uint32_t id = M.rec[o][p];
-      if (id != kNoNode && v[p] != 0.f) atomicAdd(Y + int64_t(id) * R + cb * kTcRhs + r, v[p]);
+    for (int p = 0; p < 27; ++p)
+      asm volatile("st.shared.f32 [%0], %1;" ::"r"(sbuf + uint32_t(((o * 27 + p) * kTcRhs + r) * 4)), "f"(v[p])
+                   : "memory");
+    __syncthreads();
+    for (int j = t; j < 2 * 27 * (kTcRhs / 4); j += kTcThreads) {
+      const int oo = j / (27 * (kTcRhs / 4)), rem = j % (27 * (kTcRhs / 4)), p = rem / (kTcRhs / 4),
+                r4 = rem % (kTcRhs / 4);
+      const uint32_t id = M.rec[oo][p];
+      if (id == kNoNode) continue;
+      float4 a;
+      asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+                   : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w)
+                   : "r"(sbuf + uint32_t(((oo * 27 + p) * kTcRhs + 4 * r4) * 4)));
+      float* dst = Y + int64_t(id) * R + cb * kTcRhs + 4 * r4;
+      asm volatile("red.global.add.v4.f32 [%0], {%1,%2,%3,%4};" ::"l"(dst), "f"(a.x), "f"(a.y), "f"(a.z), "f"(a.w)
+                   : "memory");
     }
     tc_fence_before();
   };
@@ -500,10 +533,11 @@ dg_status mrhs_tc_apply(const dg_mat* A, const float* X, float* Y, int R, int pa
     static bool attr3 = false;
     if (!attr3) {
       DG_CUDA(cudaFuncSetAttribute(mrhs_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      DG_CUDA(cudaFuncSetAttribute(mrhs_tc_kernel<3>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   int(cudaSharedmemCarveoutMaxShared)));
       attr3 = true;
     }
-    DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mrhs_tc_kernel<3>, kTcThreads, bytes));
-    per_sm = std::max(1, std::min(per_sm, 512 / kTcTmemCols));
+    per_sm = std::min(512 / kTcTmemCols, (227 << 10) / (bytes + 1024));
     const unsigned grid = unsigned(std::min<int64_t>(items, int64_t(sm_count()) * per_sm));
     mrhs_tc_kernel<3><<<grid, kTcThreads, bytes, s>>>(npairs, ncb, O.rec.p, A->tc_coef.p, R, X, Y,
                                                        wait_limit());
@@ -512,10 +546,11 @@ dg_status mrhs_tc_apply(const dg_mat* A, const float* X, float* Y, int R, int pa
     static bool attr1 = false;
     if (!attr1) {
       DG_CUDA(cudaFuncSetAttribute(mrhs_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      DG_CUDA(cudaFuncSetAttribute(mrhs_tc_kernel<1>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   int(cudaSharedmemCarveoutMaxShared)));
       attr1 = true;
     }
-    DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mrhs_tc_kernel<1>, kTcThreads, bytes));
-    per_sm = std::max(1, std::min(per_sm, 512 / kTcTmemCols));
+    per_sm = std::min(512 / kTcTmemCols, (227 << 10) / (bytes + 1024));
     const unsigned grid = unsigned(std::min<int64_t>(items, int64_t(sm_count()) * per_sm));
     mrhs_tc_kernel<1><<<grid, kTcThreads, bytes, s>>>(npairs, ncb, O.rec.p, A->tc_coef.p, R, X, Y,
                                                        wait_limit());

@@ -515,6 +515,102 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_kernel(
   }
 }
 
+// The one-thread-per-octet form with the next octet's words in flight: each
+// thread copies the 27 node ids, 8 element ids and the meta word of the
+// octet it works next (grid stride ahead) into its own shared-memory slot with
+// 4-byte cp.async while it works the current one, so an octet's x gathers
+// and coefficient loads issue at once, without the round trip for the ids,
+// and the ids are read from shared memory (not held in registers) when the
+// sums leave.  Slots are private to a thread: its own cp.async.wait_group is
+// the only synchronisation.
+constexpr int kOctPfWords = 36;  // 27 node ids, 8 element ids, meta
+template <class T, class CT, int BLOCK, int MINB, bool HOIST = true>
+__global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_pf_kernel(
+    int64_t n, const uint32_t* __restrict__ ometa, const uint32_t* __restrict__ oid,
+    const uint32_t* __restrict__ oelem, const CT* __restrict__ ca, const CT* __restrict__ cb,
+    const T* __restrict__ x, T* __restrict__ y) {
+  __shared__ uint32_t sw[2][kOctPfWords][BLOCK];  // [slot][word][thread]: a warp's accesses are consecutive words
+  const int tid = threadIdx.x;
+  const int64_t stride = gstride();
+  auto fetch = [&](int64_t oo, int slot) {
+    if (oo < n) {
+#pragma unroll
+      for (int p = 0; p < 27; ++p)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                         static_cast<uint32_t>(__cvta_generic_to_shared(&sw[slot][p][tid]))),
+                     "l"(oid + int64_t(p) * n + oo)
+                     : "memory");
+      if (ca) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                           static_cast<uint32_t>(__cvta_generic_to_shared(&sw[slot][27 + c][tid]))),
+                       "l"(oelem + int64_t(c) * n + oo)
+                       : "memory");
+      }
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                       static_cast<uint32_t>(__cvta_generic_to_shared(&sw[slot][35][tid]))),
+                   "l"(ometa + oo)
+                   : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  int64_t o = gtid();
+  fetch(o, 0);
+  for (int it = 0; o < n; o += stride, ++it) {
+    const int sl = it & 1;
+    fetch(o + stride, sl ^ 1);
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
+    const uint32_t m = sw[sl][35][tid];
+    const uint32_t cm0 = ometa_cmask(m);
+    // HOIST: all 16 coefficients loaded with the x gathers (more loads in
+    // flight); otherwise each child's pair is loaded when its operator runs
+    // (fewer registers)
+    T fa[HOIST ? 8 : 1], fb[HOIST ? 8 : 1];
+    if (HOIST && ca) {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const uint32_t e = sw[sl][27 + c][tid];
+        fa[c] = ((cm0 >> c) & 1u) ? T(__ldg(ca + e)) : T(0);
+        fb[c] = ((cm0 >> c) & 1u) ? T(__ldg(cb + e)) : T(0);
+      }
+    }
+    uint32_t none = 0;
+    T xv[27], yv[27];
+#pragma unroll
+    for (int p = 0; p < 27; ++p) {
+      const uint32_t id = sw[sl][p][tid];
+      none |= id == kNoNode ? (1u << p) : 0u;
+      xv[p] = id != kNoNode ? __ldg(x + id) : T(0);
+    }
+    octet_apply<T>(xv, yv, none, m, [&](int c, T& f1, T& f2) {
+      if (ca) {
+        if (HOIST) {
+          f1 *= fa[c];
+          f2 *= fb[c];
+        } else {
+          const uint32_t e = sw[sl][27 + c][tid];
+          f1 *= T(__ldg(ca + e));
+          f2 *= T(__ldg(cb + e));
+        }
+      }
+    });
+#pragma unroll
+    for (int p = 0; p < 27; ++p) {
+      const uint32_t id = sw[sl][p][tid];
+      const bool node = id != kNoNode;
+      T* dst = y + (node ? id : 0u);
+      if (p == 13) {
+        st_if(dst, yv[p], node && cm0 == 255u);
+        red_add_if(dst, yv[p], node && cm0 != 255u);
+      } else {
+        red_add_if(dst, yv[p], node && yv[p] != T(0));
+      }
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 // Octet form with a child per lane: the 8 lanes 8g .. 8g + 7 of a warp work
 // the 8 children of one parent octant (4 octets per warp), lane c child c.
 // A lane holds its child's 8 vertex values in the child's mirrored frame
@@ -534,7 +630,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_kernel(
 //  * the transpose of the interpolation is local: a hanging point's sum
 //    goes, times 1/2 (edge) or 1/4 (face), to frame vertex 0 (the parent
 //    corner c) of every child at one of its corners, each of which holds the
-//    point;
+//    point (a lane whose child is not an element of the mesh still holds it
+//    after the butterfly, and adds its corner's sum);
 //  * each node's sum leaves once, from the lowest-numbered present child
 //    that shares it.
 // The octet's record (octet.cuh, 128 bytes) gives the node ids, the mask of
@@ -612,7 +709,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_octlane_kernel(
       for (int q = 0; q < 8; ++q)
         if ((q & ~f) == 0) subsets |= 1u << q;
       const uint32_t ps = (subsets << (c & ~f)) & cm;
-      const bool mine = present && !((hang >> f) & 1u) && (ps & ((1u << c) - 1u)) == 0u;
+      // f = 0 (the parent corner c) belongs to this lane alone; it may hold
+      // folded sums even when child c is not an element of this mesh (an
+      // element subset of a partitioned mesh leaves children out)
+      const bool mine = (present || (f == 0 && u[0] != T(0))) && !((hang >> f) & 1u) &&
+                        (ps & ((1u << c) - 1u)) == 0u;
       const int L = base + (f & 1) * dx + ((f >> 1) & 1) * dy + (f >> 2) * dz;
       const uint32_t id = mine ? __ldg(r + L) : kNoNode;
       const bool owner = id != kNoNode;
@@ -1626,7 +1727,9 @@ struct MatvecVariant {
                       // 7 octet chunks staged through shared memory, 8 the same, lean,
                       // 9 the same with the staging of the next chunks in flight (cp.async),
                       // 10 octet lanes (a child per lane, 8 lanes per parent octant),
-                      // 11 octet quads (a column of two children per lane, 4 lanes per octant)
+                      // 11 octet quads (a column of two children per lane, 4 lanes per octant),
+                      // 12 octet with the next octet's ids in flight (cp.async), 13 the same
+                      // with each child's coefficients loaded when its operator runs
   int minb;
   const char* name;
 };
@@ -1656,6 +1759,11 @@ constexpr MatvecVariant kVariants[] = {
     {kOctChunk, 4, 9, 4, "octet chunks of 128, pipelined staging, 4 CTAs/SM"},
     {256, 4, 10, 4, "octet lanes b256, 4 CTAs/SM"},
     {256, 4, 11, 4, "octet quads b256, 4 CTAs/SM"},
+    {128, 4, 12, 4, "octet b128, next ids in flight, 4 CTAs/SM"},
+    {128, 5, 12, 5, "octet b128, next ids in flight, 5 CTAs/SM"},
+    {128, 4, 13, 4, "octet b128, next ids in flight, coefficients per child, 4 CTAs/SM"},
+    {128, 5, 13, 5, "octet b128, next ids in flight, coefficients per child, 5 CTAs/SM"},
+    {128, 6, 13, 6, "octet b128, next ids in flight, coefficients per child, 6 CTAs/SM"},
 };
 // Coefficients of at most this many consecutive elements are staged per chunk.
 constexpr uint32_t kOctCoefCap = 2048;
@@ -1722,6 +1830,22 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
     if (V.minb == 2) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 2>));
     else if (V.minb == 3) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 3>));
     else DG_TRY(go(lapmass_octchunk_kernel<T, CT, 4>));
+  } else if (V.kind == 13) {
+    const OctetSet& O = da->octs;
+    const unsigned gp = grid_for(O.n, 128, V.per_sm);
+    if (V.minb == 6)
+      lapmass_octet_pf_kernel<T, CT, 128, 6, false><<<gp, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
+    else if (V.minb == 5)
+      lapmass_octet_pf_kernel<T, CT, 128, 5, false><<<gp, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
+    else
+      lapmass_octet_pf_kernel<T, CT, 128, 4, false><<<gp, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
+  } else if (V.kind == 12) {
+    const OctetSet& O = da->octs;
+    const unsigned gp = grid_for(O.n, 128, V.per_sm);
+    if (V.minb == 5)
+      lapmass_octet_pf_kernel<T, CT, 128, 5><<<gp, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
+    else
+      lapmass_octet_pf_kernel<T, CT, 128, 4><<<gp, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
   } else if (V.kind == 11) {
     const OctetSet& O = da->octs;
     lapmass_octquad_kernel<T, CT, 256, 4><<<grid_for(4 * O.n, 256, V.per_sm), 256, 0, s>>>(O.n, O.rec.p, O.elem.p,
@@ -1843,7 +1967,7 @@ static dg_status pick_variant(const dg_da* da, int& choice, const CT* ca, const 
     DG_TRY((launch_variant<T, CT>(0, da, ca, cb, x, y, s)));
     for (int v = 0; v < kNumVariants; ++v) {
       if (kVariants[v].kind >= 2 && kVariants[v].kind <= 5 && da->tiles_w.ntiles == 0) continue;
-      if ((kVariants[v].kind == 6 || kVariants[v].kind >= 10) && da->octs.n == 0) continue;
+      if ((kVariants[v].kind == 6 || kVariants[v].kind >= 10) && da->octs.n == 0) continue;  // octet forms
       if (kVariants[v].kind >= 7 && kVariants[v].kind <= 9 && da->octs.nchunk == 0) continue;
       for (int trial = 0; trial < 2; ++trial) {
         DG_CUDA(cudaMemsetAsync(flush.p, trial + 1, flush_bytes, s));

@@ -79,6 +79,28 @@ def test_accumulate_matches_sequential_sum(gpu, oracle):
         assert np.array_equal(got, expect)
 
 
+@pytest.mark.parametrize("name,P", [("lognormal20k_d12", 4), ("gauss20k_d10", 2)])
+def test_partitioned_every_launch_shape(gpu, oracle, name, P):
+    """Each operator kernel, fixed in turn, on the independent and dependent
+    element subsets of every part: octets there lack children that the
+    other subset (or another rank) holds, while their hanging points still
+    fold onto those children's corners."""
+    from dendro_b200.halo import HaloJacobian2
+    da, ref, H = setup(gpu, oracle, name, P)
+    coef = I.sphere_coefficients(da.elementCenters())
+    x = I.uniform_rhs(ref.N, 21)
+    xs = [h.local_vector(x[h.first_owned:h.first_owned + h.n_owned]) for h in H]
+    emulate_read(H, xs)
+    ops = [HaloJacobian2(h, coef) for h in H]
+    y_ref = ref.matvec(x, coef)
+    mats = [A for op in ops for A in (op.A_ind, op.A_dep) if A is not None]
+    for v in range(mats[0].kernel_count()):
+        for A in mats:
+            A.set_kernel(v, 0)
+        y = np.concatenate([op.apply_local(xl)[:op.hda.n_owned].cpu().numpy() for op, xl in zip(ops, xs)])
+        assert rel(y, y_ref) < TOL, (v, mats[0].kernel_name(0))
+
+
 def test_weighted_partition_and_one_rank_cg(gpu, oracle):
     import torch
     from dendro_b200.halo import HaloDA, HaloJacobian2, halo_cg

@@ -47,6 +47,7 @@ TRAFFIC = {
     "warp-tile 32 elems, 3 CTAs/SM, ids and x of the next tile in flight": 313441024 + 19751680,
     "octet b128, 4 CTAs/SM": 217575168 + 18488576,
     "octet b256, 2 CTAs/SM": 217540864 + 18269184,
+    "octet b128, next ids in flight, 4 CTAs/SM": 217420288 + 15001600,
 }
 
 

@@ -611,6 +611,117 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_pf_kernel(
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// The same with x in flight too: per thread the words of the octet two grid
+// strides ahead and the x values (8- or 4-byte cp.async gathers) of the
+// next one are copied while it works the current one, whose x is read from
+// its shared slot; only the coefficients are read straight from global
+// memory.  Shared memory per thread: 3 word slots + 2 value slots.
+template <class T, class CT, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_pfx_kernel(
+    int64_t n, const uint32_t* __restrict__ ometa, const uint32_t* __restrict__ oid,
+    const uint32_t* __restrict__ oelem, const CT* __restrict__ ca, const CT* __restrict__ cb,
+    const T* __restrict__ x, T* __restrict__ y) {
+  extern __shared__ __align__(16) unsigned char pfx_smem[];
+  uint32_t(*sw)[kOctPfWords][BLOCK] = reinterpret_cast<uint32_t(*)[kOctPfWords][BLOCK]>(pfx_smem);
+  T(*sx)[27][BLOCK] = reinterpret_cast<T(*)[27][BLOCK]>(pfx_smem + sizeof(uint32_t) * 3 * kOctPfWords * BLOCK);
+  const int tid = threadIdx.x;
+  const int64_t stride = gstride();
+  auto fetch_words = [&](int64_t oo, int slot) {
+    if (oo < n) {
+#pragma unroll
+      for (int p = 0; p < 27; ++p)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                         static_cast<uint32_t>(__cvta_generic_to_shared(&sw[slot][p][tid]))),
+                     "l"(oid + int64_t(p) * n + oo)
+                     : "memory");
+      if (ca) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                           static_cast<uint32_t>(__cvta_generic_to_shared(&sw[slot][27 + c][tid]))),
+                       "l"(oelem + int64_t(c) * n + oo)
+                       : "memory");
+      }
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                       static_cast<uint32_t>(__cvta_generic_to_shared(&sw[slot][35][tid]))),
+                   "l"(ometa + oo)
+                   : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  auto fetch_x = [&](int64_t oo, int wslot, int xslot) {
+    if (oo < n) {
+#pragma unroll
+      for (int p = 0; p < 27; ++p) {
+        const uint32_t id = sw[wslot][p][tid];
+        const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(&sx[xslot][p][tid]));
+        if (id != kNoNode) {
+          if (sizeof(T) == 8)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(x + id) : "memory");
+          else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(x + id) : "memory");
+        } else {
+          sx[xslot][p][tid] = T(0);
+        }
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  int64_t o = gtid();
+  fetch_words(o, 0);
+  fetch_words(o + stride, 1);
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+  fetch_x(o, 0, 0);
+  for (int it = 0; o < n; o += stride, ++it) {
+    const int ws = it % 3, xs = it & 1;
+    fetch_words(o + 2 * stride, (it + 2) % 3);
+    asm volatile("cp.async.wait_group 2;" ::: "memory");  // words of the next octet
+    fetch_x(o + stride, (it + 1) % 3, xs ^ 1);
+    asm volatile("cp.async.wait_group 2;" ::: "memory");  // x of this octet
+    const uint32_t m = sw[ws][35][tid];
+    const uint32_t cm0 = ometa_cmask(m);
+    T fa[8], fb[8];
+    if (ca) {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const uint32_t e = sw[ws][27 + c][tid];
+        fa[c] = ((cm0 >> c) & 1u) ? T(__ldg(ca + e)) : T(0);
+        fb[c] = ((cm0 >> c) & 1u) ? T(__ldg(cb + e)) : T(0);
+      }
+    }
+    uint32_t none = 0;
+    T xv[27], yv[27];
+#pragma unroll
+    for (int p = 0; p < 27; ++p) {
+      none |= sw[ws][p][tid] == kNoNode ? (1u << p) : 0u;
+      xv[p] = sx[xs][p][tid];
+    }
+    octet_apply<T>(xv, yv, none, m, [&](int c, T& f1, T& f2) {
+      if (ca) {
+        f1 *= fa[c];
+        f2 *= fb[c];
+      }
+    });
+#pragma unroll
+    for (int p = 0; p < 27; ++p) {
+      const uint32_t id = sw[ws][p][tid];
+      const bool node = id != kNoNode;
+      T* dst = y + (node ? id : 0u);
+      if (p == 13) {
+        st_if(dst, yv[p], node && cm0 == 255u);
+        red_add_if(dst, yv[p], node && cm0 != 255u);
+      } else {
+        red_add_if(dst, yv[p], node && yv[p] != T(0));
+      }
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+template <class T, int BLOCK>
+constexpr size_t octet_pfx_smem() {
+  return sizeof(uint32_t) * 3 * kOctPfWords * BLOCK + sizeof(T) * 2 * 27 * BLOCK;
+}
+
 // Octet form with a child per lane: the 8 lanes 8g .. 8g + 7 of a warp work
 // the 8 children of one parent octant (4 octets per warp), lane c child c.
 // A lane holds its child's 8 vertex values in the child's mirrored frame
@@ -1729,7 +1840,8 @@ struct MatvecVariant {
                       // 10 octet lanes (a child per lane, 8 lanes per parent octant),
                       // 11 octet quads (a column of two children per lane, 4 lanes per octant),
                       // 12 octet with the next octet's ids in flight (cp.async), 13 the same
-                      // with each child's coefficients loaded when its operator runs
+                      // with each child's coefficients loaded when its operator runs, 14 the
+                      // words two octets ahead and x one octet ahead in flight
   int minb;
   const char* name;
 };
@@ -1764,6 +1876,7 @@ constexpr MatvecVariant kVariants[] = {
     {128, 4, 13, 4, "octet b128, next ids in flight, coefficients per child, 4 CTAs/SM"},
     {128, 5, 13, 5, "octet b128, next ids in flight, coefficients per child, 5 CTAs/SM"},
     {128, 6, 13, 6, "octet b128, next ids in flight, coefficients per child, 6 CTAs/SM"},
+    {128, 2, 14, 2, "octet b128, next ids and x in flight, 2 CTAs/SM"},
 };
 // Coefficients of at most this many consecutive elements are staged per chunk.
 constexpr uint32_t kOctCoefCap = 2048;
@@ -1830,6 +1943,12 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
     if (V.minb == 2) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 2>));
     else if (V.minb == 3) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 3>));
     else DG_TRY(go(lapmass_octchunk_kernel<T, CT, 4>));
+  } else if (V.kind == 14) {
+    const OctetSet& O = da->octs;
+    const unsigned gp = grid_for(O.n, 128, V.per_sm);
+    auto kern = lapmass_octet_pfx_kernel<T, CT, 128, 2>;
+    DG_TRY(allow_dynamic_smem(reinterpret_cast<const void*>(kern), octet_pfx_smem<T, 128>()));
+    kern<<<gp, 128, octet_pfx_smem<T, 128>(), s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
   } else if (V.kind == 13) {
     const OctetSet& O = da->octs;
     const unsigned gp = grid_for(O.n, 128, V.per_sm);

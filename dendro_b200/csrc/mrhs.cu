@@ -560,6 +560,76 @@ __global__ void __launch_bounds__(128) mrhs_octet_kernel(int64_t n, const uint32
   }
 }
 
+// The same with the next task's octet words in flight: each warp copies the
+// 27 node ids, the meta word and the 8 element ids of the task one grid
+// stride ahead into its own shared-memory slot (4-byte cp.async, one word
+// per lane) while it works the current task, so the X row loads of a task
+// issue without the round trip for its ids.
+constexpr int kMoWords = 36;  // 27 node ids, meta, 8 element ids
+template <class T>
+__global__ void __launch_bounds__(128) mrhs_octet_pf_kernel(int64_t n, const uint32_t* __restrict__ ometa,
+                                                            const uint32_t* __restrict__ oid,
+                                                            const uint32_t* __restrict__ oelem,
+                                                            const T* __restrict__ ca, const T* __restrict__ cb,
+                                                            int R, const T* __restrict__ X, T* __restrict__ Y) {
+  __shared__ uint32_t slot[4][2][kMoWords];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nb = R / 32;
+  const int64_t tasks = n * nb;
+  const int64_t wstride = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  auto fetch = [&](int64_t t, int sl) {
+    if (t < tasks) {
+      const int64_t o = t / nb;
+      for (int k = lane; k < kMoWords; k += 32) {
+        const uint32_t* src = k < 27 ? oid + int64_t(k) * n + o : k == 27 ? ometa + o : oelem + int64_t(k - 28) * n + o;
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                         static_cast<uint32_t>(__cvta_generic_to_shared(&slot[w][sl][k]))),
+                     "l"(src)
+                     : "memory");
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  int64_t t = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+  fetch(t, 0);
+  for (int it = 0; t < tasks; t += wstride, ++it) {
+    const int sl = it & 1;
+    __syncwarp();  // every lane is done with the slot the next fetch overwrites
+    fetch(t + wstride, sl ^ 1);
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
+    __syncwarp();  // the whole slot of this task has landed
+    const uint32_t* W = slot[w][sl];
+    const int64_t o = t / nb;
+    const int col = int(t - o * nb) * 32 + lane;
+    const uint32_t m = W[27];
+    uint32_t none = 0;
+    T xv[27], yv[27];
+#pragma unroll
+    for (int p = 0; p < 27; ++p) {
+      const uint32_t id = W[p];
+      none |= id == kNoNode ? (1u << p) : 0u;
+      xv[p] = id != kNoNode ? __ldg(X + int64_t(id) * R + col) : T(0);
+    }
+    octet_apply<T>(xv, yv, none, m, [&](int c, T& f1, T& f2) {
+      if (ca) {
+        const uint32_t e = W[28 + c];
+        f1 *= __ldg(ca + e);
+        f2 *= __ldg(cb + e);
+      }
+    });
+    const uint32_t cm = ometa_cmask(m);
+#pragma unroll
+    for (int p = 0; p < 27; ++p) {
+      const uint32_t id = W[p];
+      if (id == kNoNode) continue;
+      T* dst = Y + int64_t(id) * R + col;
+      if (p == 13 && cm == 255u) *dst = yv[p];
+      else if (yv[p] != T(0)) atomicAdd(dst, yv[p]);
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 }  // namespace
 
 template <class T>
@@ -572,7 +642,7 @@ dg_status mrhs_octet_apply(const dg_mat* A, const T* coef, const T* X, T* Y, int
   const T* cb = A->has_coef ? coef + da->E : nullptr;
   const int64_t warps = O.n * (R / 32);
   const unsigned grid = unsigned(std::min<int64_t>((warps + 3) / 4, int64_t(sm_count()) * 16));
-  mrhs_octet_kernel<T><<<grid, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, R, X, Y);
+  mrhs_octet_pf_kernel<T><<<grid, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, R, X, Y);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }
@@ -619,7 +689,7 @@ dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int R, int split
     DG_CUDA(cudaMemsetAsync(Y, 0, sizeof(float) * size_t(da->N) * R, s));
     const int64_t warps = O.n * (R / 32);
     const unsigned grid = unsigned(std::min<int64_t>((warps + 3) / 4, int64_t(sm_count()) * 16));
-    mrhs_octet_kernel<float><<<grid, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, R, X, Y);
+    mrhs_octet_pf_kernel<float><<<grid, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, R, X, Y);
     DG_CUDA(cudaGetLastError());
     return DG_OK;
   }

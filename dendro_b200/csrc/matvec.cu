@@ -2527,21 +2527,117 @@ __device__ __forceinline__ void graddiv_block(const double (&u)[8], double w, do
   for (int v = 0; v < 8; ++v) r[v] += w * t[v];
 }
 
-// y = mu h/2 (K x I3) x + (mu + lambda) h/2 GD x per element; Dirichlet nodes
-// contribute nothing (columns skipped) and receive nothing (rows handled by
-// elasticity_dirichlet_rows).  x, y are node-major [N][3].
+// The element in its child-number frame (frame vertex f = vertex f ^ c): the
+// hanging vertices are the frame vertices of the frame mask, a hanging frame
+// vertex interpolates the raw values at its bit subsets (faces from the raw
+// edge values, then edges), and T^T sends w_i r_i to every bit subset of a
+// hanging i.  Reflecting axis a negates d/dx_a, so the grad-div block (A, B)
+// of the frame is the reference block times s_A s_B (s_a = -1 on the axes
+// the child number reflects); K and M are unchanged.  The element operator
+// itself runs in the Walsh basis, where it is diagonal plus one shifted term
+// per off-diagonal block (below).
+__device__ __forceinline__ void frame_interp(double (&u)[8], uint32_t fm) {
+#pragma unroll
+  for (int f = 3; f < 7; ++f) {
+    if (f == 4) continue;
+    const int b0 = f & -f, b1 = f ^ b0;
+    if ((fm >> f) & 1u) u[f] = ((u[0] + u[f]) + (u[b0] + u[b1])) * 0.25;
+  }
+#pragma unroll
+  for (int f = 1; f <= 4; f <<= 1)
+    if ((fm >> f) & 1u) u[f] = (u[0] + u[f]) * 0.5;
+}
+__device__ __forceinline__ void frame_scatter(double (&r)[8], uint32_t fm) {
+  double w[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const double wt = (i == 1 || i == 2 || i == 4) ? 0.5 : 0.25;
+    w[i] = (i != 0 && i != 7 && ((fm >> i) & 1u)) ? r[i] * wt : 0.0;
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    double t = ((fm >> j) & 1u) ? 0.0 : r[j];
+#pragma unroll
+    for (int i = 1; i < 7; ++i)
+      if ((i & j) == j) t += w[i];
+    r[j] = t;
+  }
+}
+// r = the element's 24 results in the frame from its 24 raw frame values.
+__device__ __forceinline__ void elasticity_frame(double (&u0)[8], double (&u1)[8], double (&u2)[8], uint32_t fm,
+                                                 uint32_t cn, double wl, double wg, double (&r0)[8],
+                                                 double (&r1)[8], double (&r2)[8]) {
+  if (fm) {
+    frame_interp(u0, fm);
+    frame_interp(u1, fm);
+    frame_interp(u2, fm);
+  }
+  // In the Walsh basis (per axis u^ = (u0 + u1, u0 - u1)) the 1D factors are
+  // M1 = diag(1, 1/3), K1 = diag(0, 1), int phi'_k phi_j: u^_1 <- -u^_0 and
+  // int phi_k phi'_j: u^_0 <- -u^_1, so every grad-div block (A, B), A != B,
+  // is one term per Walsh index w with bit A set and bit B clear:
+  // r^_A[w] += m_C(w) u^_B[w ^ bit A ^ bit B] (the two -1 cancel; C the third
+  // axis, m_a(w) = 1/3 if bit a of w is set, else 1); the diagonal blocks and
+  // mu K are diagonal: mu K eigenvalue n 3^(1-n) (n = popcount w), block
+  // (A, A) [bit A of w] times m of the other two axes.  r = WHT(r^) / 8.
+  wht8(u0);
+  wht8(u1);
+  wht8(u2);
+  const double s0 = (cn & 1u) ? -1.0 : 1.0, s1 = (cn & 2u) ? -1.0 : 1.0, s2 = (cn & 4u) ? -1.0 : 1.0;
+  const double g01 = wg * s0 * s1, g02 = wg * s0 * s2, g12 = wg * s1 * s2;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) {
+    const int n = (w & 1) + ((w >> 1) & 1) + (w >> 2);
+    const double kap = n == 0 ? 0.0 : n == 1 ? 1.0 : n == 2 ? 2.0 / 3.0 : 1.0 / 3.0;
+    const double m0 = (w & 1) ? 1.0 / 3.0 : 1.0, m1 = (w & 2) ? 1.0 / 3.0 : 1.0, m2 = (w & 4) ? 1.0 / 3.0 : 1.0;
+    double a0 = wl * kap * u0[w], a1 = wl * kap * u1[w], a2 = wl * kap * u2[w];
+    if (w & 1) a0 += wg * (m1 * m2) * u0[w];
+    if (w & 2) a1 += wg * (m0 * m2) * u1[w];
+    if (w & 4) a2 += wg * (m0 * m1) * u2[w];
+    if ((w & 1) && !(w & 2)) a0 += g01 * m2 * u1[w ^ 3];
+    if ((w & 1) && !(w & 4)) a0 += g02 * m1 * u2[w ^ 5];
+    if ((w & 2) && !(w & 1)) a1 += g01 * m2 * u0[w ^ 3];
+    if ((w & 2) && !(w & 4)) a1 += g12 * m0 * u2[w ^ 6];
+    if ((w & 4) && !(w & 1)) a2 += g02 * m1 * u0[w ^ 5];
+    if ((w & 4) && !(w & 2)) a2 += g12 * m0 * u1[w ^ 6];
+    r0[w] = a0 * 0.125;
+    r1[w] = a1 * 0.125;
+    r2[w] = a2 * 0.125;
+  }
+  wht8(r0);
+  wht8(r1);
+  wht8(r2);
+  if (fm) {
+    frame_scatter(r0, fm);
+    frame_scatter(r1, fm);
+    frame_scatter(r2, fm);
+  }
+}
+__device__ __forceinline__ uint32_t frame_mask(uint32_t mask, uint32_t cn) {
+  uint32_t fm = 0;
+#pragma unroll
+  for (int f = 0; f < 8; ++f) fm |= ((mask >> (uint32_t(f) ^ cn)) & 1u) << f;
+  return fm;
+}
+
+// y = mu h/2 (K x I3) x + (mu + lambda) h/2 GD x per element (worked in the
+// element's child-number frame); Dirichlet nodes contribute nothing (columns
+// skipped) and receive nothing (rows handled by elasticity_dirichlet_rows).
+// x, y are node-major [N][3].
 __global__ void __launch_bounds__(128) elasticity_kernel(const uint32_t* __restrict__ nl, const uint32_t* __restrict__ meta,
                                                          const uint8_t* __restrict__ dir, int64_t E, double mu, double lam,
                                                          const double* __restrict__ x, double* __restrict__ y) {
   for (int64_t e = gtid(); e < E; e += gstride()) {
     const uint32_t m = meta[e];
-    const uint32_t lev = meta_lev(m), c = meta_cnum(m), mask = meta_mask(m);
+    const uint32_t lev = meta_lev(m), c = meta_cnum(m);
+    const uint32_t fm = frame_mask(meta_mask(m), c);
     const double fac = elem_h<double>(lev) / 2.0;
+    // in the child-number frame: frame vertex v is vertex v ^ c
     uint32_t id[8];
     bool bd[8];
 #pragma unroll
     for (int v = 0; v < 8; ++v) {
-      id[v] = __ldg(nl + int64_t(v) * E + e);
+      id[v] = __ldg(nl + int64_t(uint32_t(v) ^ c) * E + e);
       bd[v] = __ldg(dir + id[v]) != 0;
     }
     double u0[8], u1[8], u2[8];
@@ -2551,30 +2647,8 @@ __global__ void __launch_bounds__(128) elasticity_kernel(const uint32_t* __restr
       u1[v] = bd[v] ? 0.0 : __ldg(x + 3 * int64_t(id[v]) + 1);
       u2[v] = bd[v] ? 0.0 : __ldg(x + 3 * int64_t(id[v]) + 2);
     }
-    if (mask) {
-      interp_hanging(u0, c, mask);
-      interp_hanging(u1, c, mask);
-      interp_hanging(u2, c, mask);
-    }
     double r0[8], r1[8], r2[8];
-    const double wl = mu * fac, wg = (mu + lam) * fac;
-    lapmass_ref_to(u0, wl, 0.0, r0);
-    lapmass_ref_to(u1, wl, 0.0, r1);
-    lapmass_ref_to(u2, wl, 0.0, r2);
-    graddiv_block<0, 0>(u0, wg, r0);
-    graddiv_block<0, 1>(u1, wg, r0);
-    graddiv_block<0, 2>(u2, wg, r0);
-    graddiv_block<1, 0>(u0, wg, r1);
-    graddiv_block<1, 1>(u1, wg, r1);
-    graddiv_block<1, 2>(u2, wg, r1);
-    graddiv_block<2, 0>(u0, wg, r2);
-    graddiv_block<2, 1>(u1, wg, r2);
-    graddiv_block<2, 2>(u2, wg, r2);
-    if (mask) {
-      scatter_hanging(r0, c, mask);
-      scatter_hanging(r1, c, mask);
-      scatter_hanging(r2, c, mask);
-    }
+    elasticity_frame(u0, u1, u2, fm, c, mu * fac, (mu + lam) * fac, r0, r1, r2);
 #pragma unroll
     for (int v = 0; v < 8; ++v) {
       if (bd[v]) continue;
@@ -2641,43 +2715,23 @@ __global__ void __launch_bounds__(kElasChunkThreads, 2) elasticity_chunk_kernel(
       const uint32_t e = __ldg(oelem + int64_t(c) * n + o);
       if (e == kNoNode) continue;
       const uint32_t m = __ldg(meta + e);
-      const uint32_t lev = meta_lev(m), cn = meta_cnum(m), mask = meta_mask(m);
+      const uint32_t lev = meta_lev(m), cn = meta_cnum(m);
+      const uint32_t fm = frame_mask(meta_mask(m), cn);
       const double fac = elem_h<double>(lev) / 2.0;
+      // frame vertex v is vertex v ^ cn: its node's chunk-local index
       uint32_t li[8];
       bool bd[8];
       double u0[8], u1[8], u2[8];
 #pragma unroll
       for (int v = 0; v < 8; ++v) {
-        li[v] = __ldg(lnl + int64_t(v) * E + e);
+        li[v] = __ldg(lnl + int64_t(uint32_t(v) ^ cn) * E + e);
         bd[v] = sd[li[v]] != 0;
         u0[v] = bd[v] ? 0.0 : sx[3 * li[v]];
         u1[v] = bd[v] ? 0.0 : sx[3 * li[v] + 1];
         u2[v] = bd[v] ? 0.0 : sx[3 * li[v] + 2];
       }
-      if (mask) {
-        interp_hanging(u0, cn, mask);
-        interp_hanging(u1, cn, mask);
-        interp_hanging(u2, cn, mask);
-      }
       double r0[8], r1[8], r2[8];
-      const double wl = mu * fac, wg = (mu + lam) * fac;
-      lapmass_ref_to(u0, wl, 0.0, r0);
-      lapmass_ref_to(u1, wl, 0.0, r1);
-      lapmass_ref_to(u2, wl, 0.0, r2);
-      graddiv_block<0, 0>(u0, wg, r0);
-      graddiv_block<0, 1>(u1, wg, r0);
-      graddiv_block<0, 2>(u2, wg, r0);
-      graddiv_block<1, 0>(u0, wg, r1);
-      graddiv_block<1, 1>(u1, wg, r1);
-      graddiv_block<1, 2>(u2, wg, r1);
-      graddiv_block<2, 0>(u0, wg, r2);
-      graddiv_block<2, 1>(u1, wg, r2);
-      graddiv_block<2, 2>(u2, wg, r2);
-      if (mask) {
-        scatter_hanging(r0, cn, mask);
-        scatter_hanging(r1, cn, mask);
-        scatter_hanging(r2, cn, mask);
-      }
+      elasticity_frame(u0, u1, u2, fm, cn, mu * fac, (mu + lam) * fac, r0, r1, r2);
 #pragma unroll
       for (int v = 0; v < 8; ++v) {
         if (bd[v]) continue;

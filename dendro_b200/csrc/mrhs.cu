@@ -513,58 +513,15 @@ std::vector<float> frame_stencil_tables() {
 // lane per right-hand side.  Each lane holds its column's 27 lattice values
 // of the octet in registers and runs the octet arithmetic of the scalar
 // kernel (octet_apply: hanging points, the children's Walsh-form element
-// operators, T^T) in FP32; the octet's node ids, level and coefficients are
-// the same for the whole warp (broadcast loads), and the X rows read and the
-// Y rows added are 32 consecutive floats per node (one 128-byte access per
-// node and warp).  Y must be zero on entry (the sums leave with global
+// operators, T^T) in FP32; the octet's node ids, meta word and element ids
+// are the same for the whole warp, and the X rows read and the Y rows added
+// are 32 consecutive floats per node (one 128-byte access per node and
+// warp).  Each warp copies those 36 words of the task one grid stride ahead
+// into its own shared-memory slot (4-byte cp.async, one word per lane) while
+// it works the current task, so the X row loads of a task issue without the
+// round trip for its ids.  Y must be zero on entry (the sums leave with global
 // reductions; the centre of a full octet with a store).  Exact FP32 products:
 // no TF32 rounding, so `split` does not apply.
-template <class T>
-__global__ void __launch_bounds__(128) mrhs_octet_kernel(int64_t n, const uint32_t* __restrict__ ometa,
-                                                         const uint32_t* __restrict__ oid,
-                                                         const uint32_t* __restrict__ oelem,
-                                                         const T* __restrict__ ca, const T* __restrict__ cb,
-                                                         int R, const T* __restrict__ X, T* __restrict__ Y) {
-  const int lane = threadIdx.x & 31;
-  const int nb = R / 32;
-  const int64_t tasks = n * nb;
-  for (int64_t t = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; t < tasks;
-       t += (int64_t(gridDim.x) * blockDim.x) >> 5) {
-    const int64_t o = t / nb;
-    const int col = int(t - o * nb) * 32 + lane;
-    const uint32_t m = __ldg(ometa + o);
-    uint32_t id[27], none = 0;
-    T xv[27], yv[27];
-#pragma unroll
-    for (int p = 0; p < 27; ++p) {
-      id[p] = __ldg(oid + int64_t(p) * n + o);
-      none |= id[p] == kNoNode ? (1u << p) : 0u;
-    }
-#pragma unroll
-    for (int p = 0; p < 27; ++p) xv[p] = id[p] != kNoNode ? __ldg(X + int64_t(id[p]) * R + col) : T(0);
-    octet_apply<T>(xv, yv, none, m, [&](int c, T& f1, T& f2) {
-      if (ca) {
-        const uint32_t e = __ldg(oelem + int64_t(c) * n + o);
-        f1 *= __ldg(ca + e);
-        f2 *= __ldg(cb + e);
-      }
-    });
-    const uint32_t cm = ometa_cmask(m);
-#pragma unroll
-    for (int p = 0; p < 27; ++p) {
-      if (id[p] == kNoNode) continue;
-      T* dst = Y + int64_t(id[p]) * R + col;
-      if (p == 13 && cm == 255u) *dst = yv[p];
-      else if (yv[p] != T(0)) atomicAdd(dst, yv[p]);
-    }
-  }
-}
-
-// The same with the next task's octet words in flight: each warp copies the
-// 27 node ids, the meta word and the 8 element ids of the task one grid
-// stride ahead into its own shared-memory slot (4-byte cp.async, one word
-// per lane) while it works the current task, so the X row loads of a task
-// issue without the round trip for its ids.
 constexpr int kMoWords = 36;  // 27 node ids, meta, 8 element ids
 template <class T>
 __global__ void __launch_bounds__(128) mrhs_octet_pf_kernel(int64_t n, const uint32_t* __restrict__ ometa,

@@ -1900,6 +1900,16 @@ constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 template <class T, class CT>
 static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* cb, const T* x, T* y,
                                 cudaStream_t s) {
+  // a shape fixed by the caller that this mesh cannot run (no octets, no
+  // octet chunks or no warp tiles, e.g. a batch of meshes) falls back to
+  // the element kernel rather than leaving y unwritten
+  {
+    const int k = kVariants[v].kind;
+    const bool no_oct = (k == 6 || k >= 10) && da->octs.n == 0;
+    const bool no_chunk = k >= 7 && k <= 9 && da->octs.nchunk == 0;
+    const bool no_tile = k >= 2 && k <= 5 && da->tiles_w.ntiles == 0;
+    if (no_oct || no_chunk || no_tile) v = 0;
+  }
   const MatvecVariant& V = kVariants[v];
   const unsigned g = V.per_sm ? grid_for(da->E, V.block, V.per_sm)
                               : unsigned((da->E + V.block - 1) / V.block > 0 ? (da->E + V.block - 1) / V.block : 1);

@@ -611,6 +611,218 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_pf_kernel(
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// The next-ids-in-flight octet kernel worked in two halves to keep fewer
+// lattice values live: the lower children (z bit 0) on lattice planes z = 0
+// and 1, then the upper ones on planes 1 and 2.  Plane 0's sums are complete
+// after the lower half (only those children touch it) and leave then, except
+// its four corners, which still receive the folds of hanging points of plane
+// 1 (vertical edges and faces); plane 1 interpolates its hanging points from
+// the plane-2 corners, read with the lower half.  Peak: 22 x values and 18
+// sums (instead of 27 + 27), so more warps fit.
+template <class T, class CT, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_pf2_kernel(
+    int64_t n, const uint32_t* __restrict__ ometa, const uint32_t* __restrict__ oid,
+    const uint32_t* __restrict__ oelem, const CT* __restrict__ ca, const CT* __restrict__ cb,
+    const T* __restrict__ x, T* __restrict__ y) {
+  __shared__ uint32_t sw[2][kOctPfWords][BLOCK];
+  const int tid = threadIdx.x;
+  const int64_t stride = gstride();
+  auto fetch = [&](int64_t oo, int slot) {
+    if (oo < n) {
+#pragma unroll
+      for (int p = 0; p < 27; ++p)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                         static_cast<uint32_t>(__cvta_generic_to_shared(&sw[slot][p][tid]))),
+                     "l"(oid + int64_t(p) * n + oo)
+                     : "memory");
+      if (ca) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                           static_cast<uint32_t>(__cvta_generic_to_shared(&sw[slot][27 + c][tid]))),
+                       "l"(oelem + int64_t(c) * n + oo)
+                       : "memory");
+      }
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                       static_cast<uint32_t>(__cvta_generic_to_shared(&sw[slot][35][tid]))),
+                   "l"(ometa + oo)
+                   : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // plane-2 corners, lattice 18, 20, 24, 26, in c2[0..3]
+  constexpr int kC2[4] = {18, 20, 24, 26};
+  int64_t o = gtid();
+  fetch(o, 0);
+  for (int it = 0; o < n; o += stride, ++it) {
+    const int sl = it & 1;
+    fetch(o + stride, sl ^ 1);
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
+    const uint32_t m = sw[sl][35][tid];
+    const uint32_t cm = ometa_cmask(m);
+    uint32_t none = 0;
+#pragma unroll
+    for (int p = 0; p < 27; ++p) none |= sw[sl][p][tid] == kNoNode ? (1u << p) : 0u;
+    auto xat = [&](int p) {
+      const uint32_t id = sw[sl][p][tid];
+      return id != kNoNode ? T(__ldg(x + id)) : T(0);
+    };
+    const T hh = elem_h<T>(ometa_lev(m));
+    const T g1 = hh * T(0.5), g2 = hh * hh * hh * T(0.125);
+    auto child = [&](int c, T (&u)[8]) {
+      T f1 = g1, f2 = g2;
+      if (ca) {
+        const uint32_t e = sw[sl][27 + c][tid];
+        f1 *= T(__ldg(ca + e));
+        f2 *= T(__ldg(cb + e));
+      }
+      lapmass_ref(u, f1, f2);
+    };
+    // ---- lower half: planes 0, 1 (lattice 0..17) and the plane-2 corners
+    T xa[18], c2[4];
+#pragma unroll
+    for (int p = 0; p < 18; ++p) xa[p] = xat(p);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c2[k] = xat(kC2[k]);
+    auto xlow = [&](int q) -> T { return q < 18 ? xa[q] : c2[q == 18 ? 0 : q == 20 ? 1 : q == 24 ? 2 : 3]; };
+#pragma unroll
+    for (int p = 0; p < 18; ++p) {
+      if (oct_free(p) == 1) {
+        const int s0 = oct_s0(p);
+        if ((none >> p) & 1u) xa[p] = (xlow(p - s0) + xlow(p + s0)) * T(0.5);
+      } else if (oct_free(p) == 2) {
+        const int s0 = oct_s0(p), s1 = oct_s1(p);
+        if ((none >> p) & 1u)
+          xa[p] = ((xlow(p - s0 - s1) + xlow(p + s0 - s1)) + (xlow(p - s0 + s1) + xlow(p + s0 + s1))) * T(0.25);
+      }
+    }
+    T ya[18];
+#pragma unroll
+    for (int p = 0; p < 18; ++p) ya[p] = T(0);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if ((cm >> c) & 1u) {
+        T u[8];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) u[v] = xa[oct_lat(c, v)];
+        child(c, u);
+#pragma unroll
+        for (int v = 0; v < 8; ++v) ya[oct_lat(c, v)] += u[v];
+      }
+    }
+    // plane 0's hanging points fold onto plane-0 corners; its other node
+    // sums leave now, its corners are kept for the folds of plane 1
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+      if (oct_free(p) == 1) {
+        const int s0 = oct_s0(p);
+        const T w = ((none >> p) & 1u) ? ya[p] * T(0.5) : T(0);
+        ya[p - s0] += w;
+        ya[p + s0] += w;
+      } else if (oct_free(p) == 2) {
+        const int s0 = oct_s0(p), s1 = oct_s1(p);
+        const T w = ((none >> p) & 1u) ? ya[p] * T(0.25) : T(0);
+        ya[p - s0 - s1] += w;
+        ya[p + s0 - s1] += w;
+        ya[p - s0 + s1] += w;
+        ya[p + s0 + s1] += w;
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+      if (oct_free(p) == 0) continue;  // corners: later
+      const uint32_t id = sw[sl][p][tid];
+      const bool node = id != kNoNode;
+      red_add_if(y + (node ? id : 0u), ya[p], node && ya[p] != T(0));
+    }
+    T yc0[4] = {ya[0], ya[2], ya[6], ya[8]};
+    // ---- upper half: planes 1, 2 (lattice 9..26)
+    T xb[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const int p = 18 + q;
+      xb[q] = p == 18 ? c2[0] : p == 20 ? c2[1] : p == 24 ? c2[2] : p == 26 ? c2[3] : xat(p);
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const int p = 18 + q;
+      if (oct_free(p) == 1) {
+        const int s0 = oct_s0(p);
+        if ((none >> p) & 1u) xb[q] = (xb[q - s0] + xb[q + s0]) * T(0.5);
+      } else if (oct_free(p) == 2) {
+        const int s0 = oct_s0(p), s1 = oct_s1(p);
+        if ((none >> p) & 1u)
+          xb[q] = ((xb[q - s0 - s1] + xb[q + s0 - s1]) + (xb[q - s0 + s1] + xb[q + s0 + s1])) * T(0.25);
+      }
+    }
+    T yb[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) yb[q] = T(0);
+#pragma unroll
+    for (int c = 4; c < 8; ++c) {
+      if ((cm >> c) & 1u) {
+        T u[8];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+          const int p = oct_lat(c, v);
+          u[v] = p < 18 ? xa[p] : xb[p - 18];
+        }
+        child(c, u);
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+          const int p = oct_lat(c, v);
+          if (p < 18) ya[p] += u[v];
+          else yb[p - 18] += u[v];
+        }
+      }
+    }
+    // folds of planes 1 and 2: a corner q is plane 0 (yc0), plane 2 (yb)
+    auto addc = [&](int q, T w) {
+      if (q < 9) yc0[q == 0 ? 0 : q == 2 ? 1 : q == 6 ? 2 : 3] += w;
+      else if (q >= 18) yb[q - 18] += w;
+      else ya[q] += w;
+    };
+#pragma unroll
+    for (int p = 9; p < 27; ++p) {
+      const T yp = p < 18 ? ya[p] : yb[p - 18];
+      if (oct_free(p) == 1) {
+        const int s0 = oct_s0(p);
+        const T w = ((none >> p) & 1u) ? yp * T(0.5) : T(0);
+        addc(p - s0, w);
+        addc(p + s0, w);
+      } else if (oct_free(p) == 2) {
+        const int s0 = oct_s0(p), s1 = oct_s1(p);
+        const T w = ((none >> p) & 1u) ? yp * T(0.25) : T(0);
+        addc(p - s0 - s1, w);
+        addc(p + s0 - s1, w);
+        addc(p - s0 + s1, w);
+        addc(p + s0 + s1, w);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int p = k == 0 ? 0 : k == 1 ? 2 : k == 2 ? 6 : 8;
+      const uint32_t id = sw[sl][p][tid];
+      const bool node = id != kNoNode;
+      red_add_if(y + (node ? id : 0u), yc0[k], node && yc0[k] != T(0));
+    }
+#pragma unroll
+    for (int p = 9; p < 27; ++p) {
+      const T yp = p < 18 ? ya[p] : yb[p - 18];
+      const uint32_t id = sw[sl][p][tid];
+      const bool node = id != kNoNode;
+      T* dst = y + (node ? id : 0u);
+      if (p == 13) {
+        st_if(dst, yp, node && cm == 255u);
+        red_add_if(dst, yp, node && cm != 255u);
+      } else {
+        red_add_if(dst, yp, node && yp != T(0));
+      }
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 // The same with x in flight too: per thread the words of the octet two grid
 // strides ahead and the x values (8- or 4-byte cp.async gathers) of the
 // next one are copied while it works the current one, whose x is read from
@@ -1841,7 +2053,8 @@ struct MatvecVariant {
                       // 11 octet quads (a column of two children per lane, 4 lanes per octant),
                       // 12 octet with the next octet's ids in flight (cp.async), 13 the same
                       // with each child's coefficients loaded when its operator runs, 14 the
-                      // words two octets ahead and x one octet ahead in flight
+                      // words two octets ahead and x one octet ahead in flight, 15 next ids
+                      // in flight, the octet worked in two halves
   int minb;
   const char* name;
 };
@@ -1877,6 +2090,8 @@ constexpr MatvecVariant kVariants[] = {
     {128, 5, 13, 5, "octet b128, next ids in flight, coefficients per child, 5 CTAs/SM"},
     {128, 6, 13, 6, "octet b128, next ids in flight, coefficients per child, 6 CTAs/SM"},
     {128, 2, 14, 2, "octet b128, next ids and x in flight, 2 CTAs/SM"},
+    {128, 4, 15, 4, "octet b128, next ids in flight, two halves, 4 CTAs/SM"},
+    {128, 5, 15, 5, "octet b128, next ids in flight, two halves, 5 CTAs/SM"},
 };
 // Coefficients of at most this many consecutive elements are staged per chunk.
 constexpr uint32_t kOctCoefCap = 2048;
@@ -1953,6 +2168,13 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
     if (V.minb == 2) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 2>));
     else if (V.minb == 3) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 3>));
     else DG_TRY(go(lapmass_octchunk_kernel<T, CT, 4>));
+  } else if (V.kind == 15) {
+    const OctetSet& O = da->octs;
+    const unsigned gp = grid_for(O.n, 128, V.per_sm);
+    if (V.minb == 5)
+      lapmass_octet_pf2_kernel<T, CT, 128, 5><<<gp, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
+    else
+      lapmass_octet_pf2_kernel<T, CT, 128, 4><<<gp, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
   } else if (V.kind == 14) {
     const OctetSet& O = da->octs;
     const unsigned gp = grid_for(O.n, 128, V.per_sm);

@@ -135,18 +135,19 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
 __device__ __forceinline__ void bar_init(uint64_t* bar) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(bar)) : "memory");
 }
-__device__ __forceinline__ bool bar_try(uint64_t* bar, uint32_t parity) {
+// Bounded wait for phase `parity`: false once `limit` clock cycles have
+// passed.  A non-blocking test first, then tries that suspend the thread in
+// hardware (up to a 0.1 ms hint) until the phase completes, so the wait
+// issues few instructions and a limit shorter than one try still ends it.
+__device__ __forceinline__ bool bar_test(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
       : "=r"(ok)
       : "r"(su32(bar)), "r"(parity)
       : "memory");
   return ok != 0;
 }
-// Bounded wait for phase `parity`: false once `limit` clock cycles have
-// passed.  Each try suspends the thread in hardware (up to a 0.1 ms hint)
-// until the phase completes, so the wait issues few instructions.
 __device__ __forceinline__ bool bar_try_suspend(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -158,9 +159,11 @@ __device__ __forceinline__ bool bar_try_suspend(uint64_t* bar, uint32_t parity) 
 }
 __device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity, long long limit) {
   const long long t0 = clock64();
-  while (!bar_try_suspend(bar, parity))
+  while (true) {
+    if (bar_test(bar, parity)) return true;
     if (clock64() - t0 > limit) return false;
-  return true;
+    if (bar_try_suspend(bar, parity)) return true;
+  }
 }
 
 __device__ __forceinline__ float tf32_hi(float x) {
@@ -469,8 +472,10 @@ __global__ void __launch_bounds__(kTcThreads) mrhs_tc_kernel(int64_t npairs, int
   if (!ok) {
     if (t == 0) atomicExch(&g_tc_status, int(DG_ETIMEOUT));
     // the chain of the item that timed out may still run: wait for its
-    // commit once more (bounded) before the tensor memory goes back
-    bar_wait(&bar[pending & 1], uint32_t((pending >> 1) & 1), limit);
+    // commit once more before the tensor memory goes back, bounded by at
+    // least about a second whatever limit the caller set
+    const long long drain = limit > (1ll << 31) ? limit : (1ll << 31);
+    bar_wait(&bar[pending & 1], uint32_t((pending >> 1) & 1), drain);
   }
   tc_fence_before();
   __syncthreads();

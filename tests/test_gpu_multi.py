@@ -50,3 +50,29 @@ def test_multi_rhs_rejects_bad_shapes(gpu, oracle):
         A.mult_multi(torch.zeros((ref.N, 20), dtype=torch.float32, device="cuda"))
     with pytest.raises(gpu.DendroError):  # the tensor-memory form takes multiples of 64
         A.mult_multi(torch.zeros((ref.N, 32), dtype=torch.float32, device="cuda"), split=4)
+
+
+def test_tensor_memory_form_wait_limit_reports_timeout(gpu, oracle):
+    """A one-cycle limit makes every CTA of the tcgen05 form give up on its
+    first accumulator wait: it records DG_ETIMEOUT, waits for the MMAs it
+    issued, frees its tensor memory and returns; the check reports it once,
+    and with the default limit restored the same launch is correct."""
+    import torch
+    ref, da = setup(gpu, oracle, "lognormal20k_d12")
+    A = gpu.Jacobian2(da)
+    X = torch.tensor(np.random.default_rng(8).uniform(-1, 1, (ref.N, 64)), dtype=torch.float32, device="cuda")
+    Y0 = A.mult_multi(X, split=4).clone()
+    gpu.deviceCheck()
+    try:
+        gpu.setDeviceWaitLimit(1)
+        A.mult_multi(X, split=4)
+        with pytest.raises(gpu.DendroError) as err:
+            gpu.deviceCheck()
+        assert err.value.status == 5  # DG_ETIMEOUT
+    finally:
+        gpu.setDeviceWaitLimit(0)
+    gpu.deviceCheck()  # cleared by the check that reported it
+    Y = A.mult_multi(X, split=4)
+    gpu.deviceCheck()
+    assert torch.isfinite(Y).all()
+    assert (torch.linalg.norm(Y - Y0) / torch.linalg.norm(Y0)).item() < 1e-6

@@ -48,6 +48,7 @@ TRAFFIC = {
     "octet b128, 4 CTAs/SM": 217575168 + 18488576,
     "octet b256, 2 CTAs/SM": 217540864 + 18269184,
     "octet b128, next ids in flight, 4 CTAs/SM": 217420288 + 15001600,
+    "octet b128, next ids in flight, two halves, 4 CTAs/SM": 217417472 + 15151104,
 }
 
 

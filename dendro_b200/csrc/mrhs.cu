@@ -587,6 +587,97 @@ __global__ void __launch_bounds__(128) mrhs_octet_pf_kernel(int64_t n, const uin
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// Octet chunks with the chunk's sums in shared memory: a CTA per (chunk of
+// kOctChunk octets, 32 right-hand sides).  Its warps work the chunk's octets
+// as the octet kernel above does (a lane per right-hand side, the next
+// octet's words in flight), but add each octet's lattice sums into the
+// chunk's rows in shared memory (shared atomics: lanes hit 32 distinct
+// words of one row); then each node's row leaves once -- a store for a node
+// no other chunk touches, a global reduction for the others.  The global
+// reductions per node fall from one per octet touching it to one per chunk.
+template <class T, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS, 1) mrhs_chunk_kernel(
+    int64_t n, int64_t nchunk, const uint32_t* __restrict__ ometa, const uint32_t* __restrict__ oid,
+    const uint16_t* __restrict__ lidx, const uint32_t* __restrict__ oelem, const uint32_t* __restrict__ cptr,
+    const uint32_t* __restrict__ cnodes, const T* __restrict__ ca, const T* __restrict__ cb, int R,
+    const T* __restrict__ X, T* __restrict__ Y) {
+  extern __shared__ __align__(16) unsigned char mc_smem[];
+  uint32_t(*slot)[2][kMoWords] = reinterpret_cast<uint32_t(*)[2][kMoWords]>(mc_smem);
+  T* sy = reinterpret_cast<T*>(mc_smem + sizeof(uint32_t) * WARPS * 2 * kMoWords);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int ng = R / 32;
+  const int64_t items = nchunk * ng;
+  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
+    const int64_t q = it / ng;
+    const int col = int(it - q * ng) * 32 + lane;
+    const uint32_t p0 = __ldg(cptr + q), nn = __ldg(cptr + q + 1) - p0;
+    for (uint32_t i = threadIdx.x; i < nn * 32; i += 32 * WARPS) sy[i] = T(0);
+    __syncthreads();
+    const int64_t o0 = q * kOctChunk;
+    const int cnt = int(n - o0 < kOctChunk ? n - o0 : kOctChunk);
+    auto fetch = [&](int j, int sl) {
+      if (j < cnt) {
+        const int64_t o = o0 + j;
+        for (int k = lane; k < kMoWords; k += 32) {
+          const uint32_t* src = k < 27 ? oid + int64_t(k) * n + o : k == 27 ? ometa + o : oelem + int64_t(k - 28) * n + o;
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                           static_cast<uint32_t>(__cvta_generic_to_shared(&slot[w][sl][k]))),
+                       "l"(src)
+                       : "memory");
+        }
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    fetch(w, 0);
+    for (int j = w, i = 0; j < cnt; j += WARPS, ++i) {
+      const int sl = i & 1;
+      __syncwarp();
+      fetch(j + WARPS, sl ^ 1);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+      __syncwarp();
+      const uint32_t* W = slot[w][sl];
+      const int64_t o = o0 + j;
+      const uint32_t m = W[27];
+      uint32_t none = 0;
+      T xv[27], yv[27];
+#pragma unroll
+      for (int p = 0; p < 27; ++p) {
+        const uint32_t id = W[p];
+        none |= id == kNoNode ? (1u << p) : 0u;
+        xv[p] = id != kNoNode ? __ldg(X + int64_t(id) * R + col) : T(0);
+      }
+      octet_apply<T>(xv, yv, none, m, [&](int c, T& f1, T& f2) {
+        if (ca) {
+          const uint32_t e = W[28 + c];
+          f1 *= __ldg(ca + e);
+          f2 *= __ldg(cb + e);
+        }
+      });
+#pragma unroll
+      for (int p = 0; p < 27; ++p) {
+        if ((none >> p) & 1u) continue;
+        const uint32_t li = __ldg(lidx + int64_t(p) * n + o);
+        if (yv[p] != T(0)) atomicAdd(sy + size_t(li) * 32 + lane, yv[p]);
+      }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    for (uint32_t k = w; k < nn; k += WARPS) {
+      const uint32_t id = __ldg(cnodes + p0 + k);
+      const T v = sy[size_t(k) * 32 + lane];
+      T* dst = Y + int64_t(id & 0x7fffffffu) * R + col;
+      if (!(id >> 31)) *dst = v;
+      else if (v != T(0)) atomicAdd(dst, v);
+    }
+    __syncthreads();
+  }
+}
+constexpr int kMcWarps = 16;
+template <class T>
+constexpr size_t mrhs_chunk_smem(uint32_t max_nodes) {
+  return sizeof(uint32_t) * kMcWarps * 2 * kMoWords + sizeof(T) * 32 * size_t(max_nodes);
+}
+
 }  // namespace
 
 template <class T>
@@ -597,6 +688,28 @@ dg_status mrhs_octet_apply(const dg_mat* A, const T* coef, const T* X, T* Y, int
   DG_CUDA(cudaMemsetAsync(Y, 0, sizeof(T) * size_t(da->N) * R, s));
   const T* ca = A->has_coef ? coef : nullptr;
   const T* cb = A->has_coef ? coef + da->E : nullptr;
+  // chunks whose rows fit in shared memory: the chunked form (one CTA per SM)
+  const size_t csmem = mrhs_chunk_smem<T>(O.max_nodes);
+  // DG_MRHS_OCTET=chunk: the chunked form (measured slower than the direct
+  // one on the 64-RHS benchmark mesh: one CTA per SM and a barrier per chunk)
+  static int chunked = -1;
+  if (chunked < 0) {
+    const char* e = getenv("DG_MRHS_OCTET");
+    chunked = (e && !strcmp(e, "chunk")) ? 1 : 0;
+  }
+  if (chunked && O.nchunk > 0 && csmem <= size_t(220) << 10) {
+    static bool attr[2] = {false, false};
+    auto kern = mrhs_chunk_kernel<T, kMcWarps>;
+    if (!attr[sizeof(T) == 8]) {
+      DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(size_t(220) << 10)));
+      attr[sizeof(T) == 8] = true;
+    }
+    const unsigned grid = unsigned(std::min<int64_t>(O.nchunk * (R / 32), int64_t(sm_count())));
+    kern<<<grid, 32 * kMcWarps, csmem, s>>>(O.n, O.nchunk, O.meta.p, O.id.p, O.lidx.p, O.elem.p, O.cptr.p,
+                                            O.cnodes.p, ca, cb, R, X, Y);
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+  }
   const int64_t warps = O.n * (R / 32);
   const unsigned grid = unsigned(std::min<int64_t>((warps + 3) / 4, int64_t(sm_count()) * 16));
   mrhs_octet_pf_kernel<T><<<grid, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, R, X, Y);
@@ -642,13 +755,7 @@ dg_status mrhs_apply(const dg_mat* A, const float* X, float* Y, int R, int split
   }
   if (split == 0 || form == 5) {
     DG_CHECK(R % 32 == 0 && da->octs.n > 0, DG_EINVAL, "mat_mult_multi: the octet form takes nrhs a multiple of 32");
-    const OctetSet& O = da->octs;
-    DG_CUDA(cudaMemsetAsync(Y, 0, sizeof(float) * size_t(da->N) * R, s));
-    const int64_t warps = O.n * (R / 32);
-    const unsigned grid = unsigned(std::min<int64_t>((warps + 3) / 4, int64_t(sm_count()) * 16));
-    mrhs_octet_pf_kernel<float><<<grid, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, R, X, Y);
-    DG_CUDA(cudaGetLastError());
-    return DG_OK;
+    return mrhs_octet_apply<float>(A, A->has_coef ? A->coef32.p : nullptr, X, Y, R, s);
   }
   if (form >= 3 && R % 32 == 0) {
     static float4* ftbls[64] = {};  // frame tables, one per device, kept for the process

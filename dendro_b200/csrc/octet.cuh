@@ -63,17 +63,30 @@ __host__ __device__ __forceinline__ uint32_t ometa_cmask(uint32_t m) { return (m
 // hanging points are folded back onto their corners (T^T).  yv receives the
 // 27 lattice sums (meaningful at the points with a node).  coef(c, f1, f2)
 // scales child c's two factors by its coefficients.
+// Lattice points that can hang: the 12 edge midpoints and 6 face centres.
+__host__ __device__ constexpr uint32_t oct_hangable() {
+  uint32_t m = 0;
+  for (int p = 0; p < 27; ++p)
+    if (oct_free(p) == 1 || oct_free(p) == 2) m |= 1u << p;
+  return m;
+}
+
 template <class T, class Coef>
 __device__ __forceinline__ void octet_apply(T (&xv)[27], T (&yv)[27], uint32_t none, uint32_t m, Coef coef) {
+  // octets without a point to fill skip the interpolation and the fold (a
+  // branch, uniform when a warp works one octet)
+  const bool fill = (none & oct_hangable()) != 0u;
+  if (fill) {
 #pragma unroll
-  for (int p = 0; p < 27; ++p) {
-    if (oct_free(p) == 1) {
-      const int s0 = oct_s0(p);
-      if ((none >> p) & 1u) xv[p] = (xv[p - s0] + xv[p + s0]) * T(0.5);
-    } else if (oct_free(p) == 2) {
-      const int s0 = oct_s0(p), s1 = oct_s1(p);
-      if ((none >> p) & 1u)
-        xv[p] = ((xv[p - s0 - s1] + xv[p + s0 - s1]) + (xv[p - s0 + s1] + xv[p + s0 + s1])) * T(0.25);
+    for (int p = 0; p < 27; ++p) {
+      if (oct_free(p) == 1) {
+        const int s0 = oct_s0(p);
+        if ((none >> p) & 1u) xv[p] = (xv[p - s0] + xv[p + s0]) * T(0.5);
+      } else if (oct_free(p) == 2) {
+        const int s0 = oct_s0(p), s1 = oct_s1(p);
+        if ((none >> p) & 1u)
+          xv[p] = ((xv[p - s0 - s1] + xv[p + s0 - s1]) + (xv[p - s0 + s1] + xv[p + s0 + s1])) * T(0.25);
+      }
     }
   }
 #pragma unroll
@@ -94,20 +107,22 @@ __device__ __forceinline__ void octet_apply(T (&xv)[27], T (&yv)[27], uint32_t n
       for (int v = 0; v < 8; ++v) yv[oct_lat(c, v)] += u[v];
     }
   }
+  if (fill) {
 #pragma unroll
-  for (int p = 0; p < 27; ++p) {
-    if (oct_free(p) == 1) {
-      const int s0 = oct_s0(p);
-      const T w = ((none >> p) & 1u) ? yv[p] * T(0.5) : T(0);
-      yv[p - s0] += w;
-      yv[p + s0] += w;
-    } else if (oct_free(p) == 2) {
-      const int s0 = oct_s0(p), s1 = oct_s1(p);
-      const T w = ((none >> p) & 1u) ? yv[p] * T(0.25) : T(0);
-      yv[p - s0 - s1] += w;
-      yv[p + s0 - s1] += w;
-      yv[p - s0 + s1] += w;
-      yv[p + s0 + s1] += w;
+    for (int p = 0; p < 27; ++p) {
+      if (oct_free(p) == 1) {
+        const int s0 = oct_s0(p);
+        const T w = ((none >> p) & 1u) ? yv[p] * T(0.5) : T(0);
+        yv[p - s0] += w;
+        yv[p + s0] += w;
+      } else if (oct_free(p) == 2) {
+        const int s0 = oct_s0(p), s1 = oct_s1(p);
+        const T w = ((none >> p) & 1u) ? yv[p] * T(0.25) : T(0);
+        yv[p - s0 - s1] += w;
+        yv[p + s0 - s1] += w;
+        yv[p - s0 + s1] += w;
+        yv[p + s0 + s1] += w;
+      }
     }
   }
 }

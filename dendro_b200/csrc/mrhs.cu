@@ -587,6 +587,105 @@ __global__ void __launch_bounds__(128) mrhs_octet_pf_kernel(int64_t n, const uin
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// Two FP32 values in one 64-bit register, worked by the packed FP32
+// instructions of sm_100 (add / sub / mul .f32x2): the octet arithmetic runs
+// on two right-hand sides per instruction.
+struct F2 {
+  uint64_t v;
+  __device__ __forceinline__ F2() {}
+  __device__ __forceinline__ F2(double s) {
+    const uint64_t u = __float_as_uint(float(s));
+    v = (u << 32) | u;
+  }
+  __device__ __forceinline__ F2& operator+=(F2 b) {
+    asm("add.rn.f32x2 %0, %0, %1;" : "+l"(v) : "l"(b.v));
+    return *this;
+  }
+  __device__ __forceinline__ F2& operator*=(F2 b) {
+    asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(v) : "l"(b.v));
+    return *this;
+  }
+};
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return a += b; }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return a *= b; }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
+  F2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ bool nonzero(F2 a) { return (a.v & 0x7fffffff7fffffffull) != 0ull; }
+
+// The octet form with two right-hand sides per lane (64 per warp): X rows
+// read as 8-byte pairs, Y rows added with 8-byte vector reductions, the
+// element arithmetic on packed pairs.  nrhs a multiple of 64.
+__global__ void __launch_bounds__(128) mrhs_octet_pair_kernel(int64_t n, const uint32_t* __restrict__ ometa,
+                                                              const uint32_t* __restrict__ oid,
+                                                              const uint32_t* __restrict__ oelem,
+                                                              const float* __restrict__ ca,
+                                                              const float* __restrict__ cb, int R,
+                                                              const float* __restrict__ X, float* __restrict__ Y) {
+  __shared__ uint32_t slot[4][2][kMoWords];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nb = R / 64;
+  const int64_t tasks = n * nb;
+  const int64_t wstride = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  auto fetch = [&](int64_t t, int sl) {
+    if (t < tasks) {
+      const int64_t o = t / nb;
+      for (int k = lane; k < kMoWords; k += 32) {
+        const uint32_t* src = k < 27 ? oid + int64_t(k) * n + o : k == 27 ? ometa + o : oelem + int64_t(k - 28) * n + o;
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                         static_cast<uint32_t>(__cvta_generic_to_shared(&slot[w][sl][k]))),
+                     "l"(src)
+                     : "memory");
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  int64_t t = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+  fetch(t, 0);
+  for (int it = 0; t < tasks; t += wstride, ++it) {
+    const int sl = it & 1;
+    __syncwarp();
+    fetch(t + wstride, sl ^ 1);
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
+    __syncwarp();
+    const uint32_t* W = slot[w][sl];
+    const int64_t o = t / nb;
+    const int col = int(t - o * nb) * 64 + 2 * lane;
+    const uint32_t m = W[27];
+    uint32_t none = 0;
+    F2 xv[27], yv[27];
+#pragma unroll
+    for (int p = 0; p < 27; ++p) {
+      const uint32_t id = W[p];
+      none |= id == kNoNode ? (1u << p) : 0u;
+      xv[p].v = id != kNoNode ? __ldg(reinterpret_cast<const unsigned long long*>(X + int64_t(id) * R + col))
+                              : 0ull;
+    }
+    octet_apply<F2>(xv, yv, none, m, [&](int c, F2& f1, F2& f2) {
+      if (ca) {
+        const uint32_t e = W[28 + c];
+        f1 *= F2(__ldg(ca + e));
+        f2 *= F2(__ldg(cb + e));
+      }
+    });
+    const uint32_t cm = ometa_cmask(m);
+#pragma unroll
+    for (int p = 0; p < 27; ++p) {
+      const uint32_t id = W[p];
+      if (id == kNoNode) continue;
+      float* dst = Y + int64_t(id) * R + col;
+      const float a = __uint_as_float(uint32_t(yv[p].v)), b = __uint_as_float(uint32_t(yv[p].v >> 32));
+      if (p == 13 && cm == 255u)
+        asm volatile("st.global.v2.f32 [%0], {%1, %2};" ::"l"(dst), "f"(a), "f"(b) : "memory");
+      else if (nonzero(yv[p]))
+        asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(dst), "f"(a), "f"(b) : "memory");
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 // Octet chunks with the chunk's sums in shared memory: a CTA per (chunk of
 // kOctChunk octets, 32 right-hand sides).  Its warps work the chunk's octets
 // as the octet kernel above does (a lane per right-hand side, the next
@@ -707,6 +806,21 @@ dg_status mrhs_octet_apply(const dg_mat* A, const T* coef, const T* X, T* Y, int
     const unsigned grid = unsigned(std::min<int64_t>(O.nchunk * (R / 32), int64_t(sm_count())));
     kern<<<grid, 32 * kMcWarps, csmem, s>>>(O.n, O.nchunk, O.meta.p, O.id.p, O.lidx.p, O.elem.p, O.cptr.p,
                                             O.cnodes.p, ca, cb, R, X, Y);
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+  }
+  static int pairs = -1;  // DG_MRHS_OCTET=single: one right-hand side per lane
+  if (pairs < 0) {
+    const char* e = getenv("DG_MRHS_OCTET");
+    pairs = (e && !strcmp(e, "single")) ? 0 : 1;
+  }
+  if (sizeof(T) == 4 && pairs && R % 64 == 0) {
+    const int64_t warps = O.n * (R / 64);
+    const unsigned grid = unsigned(std::min<int64_t>((warps + 3) / 4, int64_t(sm_count()) * 16));
+    mrhs_octet_pair_kernel<<<grid, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p,
+                                                reinterpret_cast<const float*>(ca),
+                                                reinterpret_cast<const float*>(cb), R,
+                                                reinterpret_cast<const float*>(X), reinterpret_cast<float*>(Y));
     DG_CUDA(cudaGetLastError());
     return DG_OK;
   }

@@ -183,10 +183,17 @@ using Vec16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
 constexpr int kVecU = 4;
 template <class T>
 __global__ void jacobi_from_v(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ dinv,
-                              T* __restrict__ t, T omega, int64_t nv) {
+                              T* __restrict__ t, T omega, int64_t nv, int64_t n) {
   using V = Vec16<T>;
   constexpr int W = 16 / sizeof(T);
   const int64_t S = gstride();
+  // the last n - nv * W (< W) entries, by the first threads
+  if (nv * W + gtid() < n) {
+    const int64_t j = nv * W + gtid();
+    const T tj = t[j];
+    t[j] = T(0);
+    x[j] += omega * dinv[j] * (b[j] - tj);
+  }
   for (int64_t i0 = gtid(); i0 < nv; i0 += S * kVecU) {
     V tv[kVecU], xv[kVecU], bv[kVecU], dv[kVecU];
 #pragma unroll
@@ -218,10 +225,17 @@ __global__ void jacobi_from_v(T* __restrict__ x, const T* __restrict__ b, const 
   }
 }
 template <class T>
-__global__ void residual_from_v(const T* __restrict__ b, T* __restrict__ t, T* __restrict__ r, int64_t nv) {
+__global__ void residual_from_v(const T* __restrict__ b, T* __restrict__ t, T* __restrict__ r, int64_t nv,
+                                int64_t n) {
   using V = Vec16<T>;
   constexpr int W = 16 / sizeof(T);
   const int64_t S = gstride();
+  if (nv * W + gtid() < n) {
+    const int64_t j = nv * W + gtid();
+    const T tj = t[j];
+    t[j] = T(0);
+    r[j] = b[j] - tj;
+  }
   for (int64_t i0 = gtid(); i0 < nv; i0 += S * kVecU) {
     V tv[kVecU], bv[kVecU];
 #pragma unroll
@@ -2672,10 +2686,10 @@ static dg_status smooth_sweep(const dg_mat* A, const CT* coef, T* x, const T* b,
   const int64_t n = A->da->N;
   constexpr int W = 16 / sizeof(T);
   const int64_t nv = (aligned16(x) && aligned16(b) && aligned16(dinv) && aligned16(t)) ? n / W : 0;
-  if (nv) jacobi_from_v<T><<<grid_for((nv + kVecU - 1) / kVecU, 256, 8), 256, 0, s>>>(x, b, dinv, t, omega, nv);
-  if (n > nv * W)
-    jacobi_from<T><<<grid_for(n - nv * W, 256, 16), 256, 0, s>>>(x + nv * W, b + nv * W, dinv + nv * W, t + nv * W,
-                                                                omega, n - nv * W);
+  if (nv)
+    jacobi_from_v<T><<<grid_for((nv + kVecU - 1) / kVecU, 256, 8), 256, 0, s>>>(x, b, dinv, t, omega, nv, n);
+  else if (n)
+    jacobi_from<T><<<grid_for(n, 256, 16), 256, 0, s>>>(x, b, dinv, t, omega, n);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }
@@ -2688,9 +2702,10 @@ static dg_status residual(const dg_mat* A, const CT* coef, const T* x, const T* 
   const int64_t n = A->da->N;
   constexpr int W = 16 / sizeof(T);
   const int64_t nv = (aligned16(b) && aligned16(t) && aligned16(r)) ? n / W : 0;
-  if (nv) residual_from_v<T><<<grid_for((nv + kVecU - 1) / kVecU, 256, 8), 256, 0, s>>>(b, t, r, nv);
-  if (n > nv * W)
-    residual_from<T><<<grid_for(n - nv * W, 256, 16), 256, 0, s>>>(b + nv * W, t + nv * W, r + nv * W, n - nv * W);
+  if (nv)
+    residual_from_v<T><<<grid_for((nv + kVecU - 1) / kVecU, 256, 8), 256, 0, s>>>(b, t, r, nv, n);
+  else if (n)
+    residual_from<T><<<grid_for(n, 256, 16), 256, 0, s>>>(b, t, r, n);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }

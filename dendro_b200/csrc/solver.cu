@@ -237,6 +237,45 @@ __global__ void restrict_gather(const uint32_t* __restrict__ rptr, const uint32_
     rc[c] = acc;
   }
 }
+// The same two products with the weights as 8-bit codes k = 128 w.  The
+// weights are dyadic (trilinear interpolation at a coarse element's corners,
+// edge midpoints, face centres and centre, with the hanging corners' halves
+// and quarters folded in), so k is exact; code * x is w * x scaled by 128
+// exactly, every partial sum is the uncoded one scaled by 128, and the final
+// scaling by 1/128 gives the uncoded result bit for bit while each entry
+// moves 5 bytes instead of 12 (FP64) or 8 (FP32).
+constexpr double kWeightCode = 128.0;
+template <class T>
+__global__ void prolong_add_coded(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+                                  const uint8_t* __restrict__ code, int64_t Nf, const T* __restrict__ xc,
+                                  T* __restrict__ xf) {
+  #pragma unroll 4
+  for (int64_t f = gtid(); f < Nf; f += gstride()) {
+    T s = 0;
+    for (uint32_t k = ptr[f]; k < ptr[f + 1]; ++k) s += T(code[k]) * xc[col[k]];
+    xf[f] += s * T(1.0 / kWeightCode);
+  }
+}
+template <class T>
+__global__ void restrict_gather_coded(const uint32_t* __restrict__ rptr, const uint32_t* __restrict__ rcol,
+                                      const uint8_t* __restrict__ code, int64_t Nc, const T* __restrict__ rf,
+                                      T* __restrict__ rc) {
+  for (int64_t c = gtid(); c < Nc; c += gstride()) {
+    T acc = T(0);
+    for (uint32_t k = rptr[c]; k < rptr[c + 1]; ++k) acc += T(code[k]) * rf[rcol[k]];
+    rc[c] = acc * T(1.0 / kWeightCode);
+  }
+}
+// k = 128 w for every weight; flags a weight that has no exact code.
+__global__ void weight_codes(const double* __restrict__ w, int64_t n, uint8_t* __restrict__ code,
+                             uint32_t* __restrict__ bad) {
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    const double k = w[i] * kWeightCode;
+    const bool ok = k >= 0.0 && k <= 255.0 && k == floor(k);
+    if (!ok) atomicOr(bad, 1u);
+    code[i] = ok ? uint8_t(k) : uint8_t(0);
+  }
+}
 // The dof-3 forms: the scalar transfer applied to each of the 3 interleaved
 // components (node-major [N][3]), as the reference's transfer loops apply
 // the same R entry to every dof (RestrictMatVec.C:109-115, ProlongMatVec.C).
@@ -707,6 +746,9 @@ struct Level {
   // (CSR over the coarse nodes, entries in fine-node order)
   DBuf<uint32_t> pptr, pcol, rptr, rcol;
   DBuf<double> pval, rval;
+  // the weights of P and R as exact 8-bit codes (empty when a weight has
+  // none; the transfers then read pval / rval)
+  DBuf<uint8_t> pcode, rcode;
   // FP32 inner V-cycle
   DBuf<float> dinv32, x32, b32, t32, pval32, rval32, acc32;
   // learned smoother data (finest level): residual, neighbour stats,
@@ -818,6 +860,52 @@ dg_status build_restriction(Level& F, int64_t Nc, cudaStream_t s) {
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaStreamSynchronize(s));
   return DG_OK;
+}
+
+// The 8-bit weight codes of P and R (kept only when every weight has one).
+dg_status build_weight_codes(Level& F, cudaStream_t s) {
+  const int64_t nnz = F.pval.n;
+  if (!nnz || F.rval.n != nnz) return DG_OK;
+  DBuf<uint32_t> bad;
+  DG_TRY(bad.alloc(1));
+  DG_CUDA(cudaMemsetAsync(bad.p, 0, 4, s));
+  DG_TRY(F.pcode.alloc(nnz));
+  DG_TRY(F.rcode.alloc(nnz));
+  weight_codes<<<grid_for(nnz, 256), 256, 0, s>>>(F.pval.p, nnz, F.pcode.p, bad.p);
+  weight_codes<<<grid_for(nnz, 256), 256, 0, s>>>(F.rval.p, nnz, F.rcode.p, bad.p);
+  DG_CUDA(cudaGetLastError());
+  uint32_t hbad = 0;
+  DG_CUDA(cudaMemcpyAsync(&hbad, bad.p, 4, cudaMemcpyDeviceToHost, s));
+  DG_CUDA(cudaStreamSynchronize(s));
+  if (hbad) {
+    F.pcode.reset();
+    F.rcode.reset();
+  }
+  return DG_OK;
+}
+
+// rc = R rf and xf += P xc for the scalar hierarchy in FP64 or FP32, by the
+// weight codes where the level has them.
+template <class T>
+void restrict_level(const Level& F, int64_t Nc, const T* rf, T* rc, cudaStream_t s) {
+  const unsigned g = grid_for(Nc, 256, 16);
+  if (F.rcode.n) {
+    restrict_gather_coded<T><<<g, 256, 0, s>>>(F.rptr.p, F.rcol.p, F.rcode.p, Nc, rf, rc);
+  } else if constexpr (sizeof(T) == 8) {
+    restrict_gather<T><<<g, 256, 0, s>>>(F.rptr.p, F.rcol.p, F.rval.p, Nc, rf, rc);
+  } else {
+    restrict_gather<T><<<g, 256, 0, s>>>(F.rptr.p, F.rcol.p, F.rval32.p, Nc, rf, rc);
+  }
+}
+template <class T>
+void prolong_level(const Level& F, int64_t Nf, const T* xc, T* xf, cudaStream_t s, unsigned g) {
+  if (F.pcode.n) {
+    prolong_add_coded<T><<<g, 256, 0, s>>>(F.pptr.p, F.pcol.p, F.pcode.p, Nf, xc, xf);
+  } else if constexpr (sizeof(T) == 8) {
+    prolong_add<T><<<g, 256, 0, s>>>(F.pptr.p, F.pcol.p, F.pval.p, Nf, xc, xf);
+  } else {
+    prolong_add<T><<<g, 256, 0, s>>>(F.pptr.p, F.pcol.p, F.pval32.p, Nf, xc, xf);
+  }
 }
 
 dg_status setup_level_vectors(Level& L, cudaStream_t s) {
@@ -1145,10 +1233,9 @@ dg_status vcycle(dg_damg* m, size_t l, const double* b, double* x) {
     DG_CUDA(cudaMemsetAsync(x, 0, 8 * n, s));
   }
   Level& C = m->lv[l + 1];
-  restrict_gather<<<grid_for(C.da->N, 256, 16), 256, 0, s>>>(L.rptr.p, L.rcol.p, L.rval.p, C.da->N,
-                                                            m->cfg.nu_pre > 0 ? (const double*)L.t.p : b, C.b.p);
+  restrict_level<double>(L, C.da->N, m->cfg.nu_pre > 0 ? (const double*)L.t.p : b, C.b.p, s);
   DG_TRY(vcycle(m, l + 1, C.b.p, C.x.p));
-  prolong_add<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval.p, n, C.x.p, x);
+  prolong_level<double>(L, n, C.x.p, x, s, g);
   for (int k = 0; k < m->cfg.nu_post; ++k)
     DG_TRY(lapmass_smooth_f64(L.A.get(), x, b, L.dinv.p, w, L.acc.p, s, L.jcoef(), L.jset()));
   DG_CUDA(cudaGetLastError());
@@ -1179,10 +1266,9 @@ dg_status vcycle32(dg_damg* m, size_t l, const float* b, float* x) {
     DG_CUDA(cudaMemsetAsync(x, 0, 4 * n, s));
   }
   Level& C = m->lv[l + 1];
-  restrict_gather<<<grid_for(C.da->N, 256, 16), 256, 0, s>>>(L.rptr.p, L.rcol.p, L.rval32.p, C.da->N,
-                                                            m->cfg.nu_pre > 0 ? (const float*)L.t32.p : b, C.b32.p);
+  restrict_level<float>(L, C.da->N, m->cfg.nu_pre > 0 ? (const float*)L.t32.p : b, C.b32.p, s);
   DG_TRY(vcycle32(m, l + 1, C.b32.p, C.x32.p));
-  prolong_add<<<g, 256, 0, s>>>(L.pptr.p, L.pcol.p, L.pval32.p, n, C.x32.p, x);
+  prolong_level<float>(L, n, C.x32.p, x, s, g);
   if (l == 0 && m->mlp && m->mlp_active) {
     const float level_feat = 0.f;  // finest level
     for (int k = 0; k < m->mlp_sweeps; ++k) {
@@ -1358,7 +1444,10 @@ dg_status finish_create(dg_damg* m) {
   for (int i = 0; i < m->nmesh; ++i)
     fill_u16<<<grid_for(no[i + 1] - no[i], 256), 256, 0, m->s>>>(m->d_node_mesh.p, no[i], no[i + 1], uint16_t(i));
   DG_CUDA(cudaGetLastError());
-  for (size_t l = 0; l + 1 < m->lv.size(); ++l) DG_TRY(build_restriction(m->lv[l], m->lv[l + 1].da->N, m->s));
+  for (size_t l = 0; l + 1 < m->lv.size(); ++l) {
+    DG_TRY(build_restriction(m->lv[l], m->lv[l + 1].da->N, m->s));
+    DG_TRY(build_weight_codes(m->lv[l], m->s));
+  }
   return set_operators(m, nullptr);
 }
 
@@ -1549,7 +1638,7 @@ dg_status dg_damg_prolong(dg_damg* m, int level, const double* xc, double* xf, i
   if (dof == 3)
     prolong_add3<<<grid_for(F.da->N, 256), 256, 0, m->s>>>(F.pptr.p, F.pcol.p, F.pval.p, F.da->N, pc, pf);
   else
-    prolong_add<<<grid_for(nf, 256), 256, 0, m->s>>>(F.pptr.p, F.pcol.p, F.pval.p, nf, pc, pf);
+    prolong_level<double>(F, nf, pc, pf, m->s, grid_for(nf, 256));
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaStreamSynchronize(m->s));
   if (!on_device) DG_CUDA(cudaMemcpy(xf, df.p, 8 * nf, cudaMemcpyDeviceToHost));
@@ -1576,7 +1665,7 @@ dg_status dg_damg_restrict(dg_damg* m, int level, const double* rf, double* rc, 
   if (dof == 3)
     restrict_gather3<<<grid_for(C.da->N, 256, 16), 256, 0, m->s>>>(F.rptr.p, F.rcol.p, F.rval.p, C.da->N, pf, pc);
   else
-    restrict_gather<<<grid_for(nc, 256, 16), 256, 0, m->s>>>(F.rptr.p, F.rcol.p, F.rval.p, nc, pf, pc);
+    restrict_level<double>(F, nc, pf, pc, m->s);
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaStreamSynchronize(m->s));
   if (!on_device) DG_CUDA(cudaMemcpy(rc, dc.p, 8 * nc, cudaMemcpyDeviceToHost));

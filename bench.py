@@ -66,6 +66,7 @@ def parse():
     p.add_argument("--no-cfg1", action="store_true")
     p.add_argument("--no-elasticity", action="store_true")
     p.add_argument("--no-partitioned", action="store_true")
+    p.add_argument("--no-cmap", action="store_true")
     p.add_argument("--solve-workload", default="lognormal4m_d16")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--vcycle-profile", metavar="WORKLOAD", default=None,
@@ -211,15 +212,53 @@ def run_dendro(args, rank, world):
         part = run_partitioned(args, dev, bal, coef, x, 1, min(args.steps, 50), args.warmup)
         part = {"ms_per_step": round(part["ms_per_step"], 5),
                 "gdofs": round(N / (part["ms_per_step"] * 1e-3) / 1e9, 4)}
-    solve = None if args.no_solve else run_solve(dev, args.solve_workload)
     kernel = A.kernel_name(0)
+    cmap = None if args.no_cmap else run_cmap(A, da, x, y, flush, stream, min(args.steps, 20))
+    solve = None if args.no_solve else run_solve(dev, args.solve_workload)
     multi = None if args.no_multi else run_multi(dev, min(args.steps, 50))
     batch = None if args.no_batch else run_batch(dev)
     cfg1 = None if args.no_cfg1 else run_cfg1(dev)
     elastic = None if args.no_elasticity else run_elasticity(dev, bal)
-    return dict(elasticity=elastic, partitioned_one_rank=part, multi=multi, batch=batch, cfg1=cfg1, kernel=kernel, E=E, N=N, setup_s=setup_s, ms_per_step=ms_per_step, gdofs=gdofs, achieved=achieved, peak=peak,
+    return dict(cmap=cmap, elasticity=elastic, partitioned_one_rank=part, multi=multi, batch=batch, cfg1=cfg1, kernel=kernel, E=E, N=N, setup_s=setup_s, ms_per_step=ms_per_step, gdofs=gdofs, achieved=achieved, peak=peak,
                 peak_kind=peak_kind, alg_bytes=alg_bytes, clocks=clk, e2e=e2e, solve=solve, bal=bal, depth=depth,
                 coef=coef, x=x.cpu().numpy(), y=y.cpu().numpy())
+
+
+def run_cmap(A, da, x, y_default, flush, stream, steps):
+    """The compressed element map on the benchmark mesh: its bytes per element, and the element
+    kernel reading it against the same kernel reading the raw map (FP64 and FP32, L2 flushed)."""
+    import torch
+    t0 = time.time()
+    nbytes = da.compressMaps()
+    torch.cuda.synchronize()
+    build_ms = (time.time() - t0) * 1e3
+    shape = None
+    for v in range(A.kernel_count()):
+        A.set_kernel(v, 0)
+        if "compressed map" in A.kernel_name(0):
+            shape = v
+    out = {"bytes_per_element": round(nbytes / da.E, 3), "raw_bytes_per_element": 32,
+           "wide_tiles": da.compressedMapBytes()[1], "build_ms": round(build_ms, 2)}
+    for prec, name in ((0, "f64"), (1, "f32")):
+        xx = x if prec == 0 else x.float()
+        yy = torch.empty_like(xx)
+        for tag, v in (("compressed", shape), ("raw", 0)):
+            A.set_kernel(v, prec)
+            for _ in range(3):
+                A.mult(xx, yy, stream)
+            ts = []
+            for i in range(steps):
+                flush.fill_(float(i))
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                A.mult(xx, yy, stream)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            out[f"{name}_{tag}_ms"] = round(float(np.median(ts)), 4)
+            if prec == 0 and tag == "compressed":
+                out["vs_default_rel_err"] = rel_err(yy.cpu().numpy(), y_default.cpu().numpy())
+    return out
 
 
 def run_partitioned(args, dev, bal, coef, x_full, world, steps, warmup):
@@ -722,6 +761,7 @@ def main():
         "batch": r["batch"],
         "cfg1": r["cfg1"],
         "elasticity": r.get("elasticity"),
+        "compressed_map": r.get("cmap"),
         "setup_s": round(r["setup_s"], 3),
     }
     if rank == 0 and world == 1 and not args.no_cpu:

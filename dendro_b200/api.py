@@ -172,6 +172,24 @@ class DA:
               "da_export")
         return out
 
+    def compressMaps(self, quotient_bits: int = 16) -> int:
+        """Build the compressed element map (the DA's compressLut option); returns its bytes.
+        The operator's autotuner then also times the element kernel that reads it."""
+        check(lib().dg_da_compress_maps(self.h, int(quotient_bits)), "da_compress_maps")
+        return self.compressedMapBytes()[0]
+
+    def compressedMapBytes(self):
+        """(bytes of the compressed map or 0, tiles stored with 32-bit quotients)."""
+        w = C.c_int64()
+        b = int(lib().dg_da_compressed_map_bytes(self.h, C.byref(w)))
+        return b, w.value
+
+    def decompressMaps(self) -> np.ndarray:
+        """The element map [E, 8] decoded from the compressed form on the GPU."""
+        out = np.empty((self.E, 8), np.uint32)
+        check(lib().dg_da_decompress_maps(self.h, ptr(out)), "da_decompress_maps")
+        return out
+
     def elementCenters(self) -> np.ndarray:
         """CalculateCenters (examples/src/backend/omgNeumann.C:788-820), [E, 3] in [0,1]."""
         c = np.empty((self.E, 3))

@@ -276,6 +276,32 @@ uint32_t dg_da_max_depth(const dg_da* da) { return da ? da->D : 0; }
 
 int64_t dg_da_octets(const dg_da* da) { return da ? da->octs.n : 0; }
 
+dg_status dg_da_compress_maps(dg_da* da, int quotient_bits) {
+  DG_CHECK(da, DG_EINVAL, "compress_maps: null mesh");
+  DG_TRY(build_cmap(da, quotient_bits, 0));
+  DG_CUDA(cudaDeviceSynchronize());
+  return DG_OK;
+}
+
+int64_t dg_da_compressed_map_bytes(const dg_da* da, int64_t* wide_tiles) {
+  if (wide_tiles) *wide_tiles = da ? da->cmap.wide_tiles : 0;
+  return (da && da->cmap.qbits) ? da->cmap.bytes() : 0;
+}
+
+dg_status dg_da_decompress_maps(const dg_da* da, uint32_t* nlist) {
+  DG_CHECK(da && nlist, DG_EINVAL, "decompress_maps: bad arguments");
+  const int64_t E = da->E;
+  if (!E) return DG_OK;
+  DBuf<uint32_t> d;
+  DG_TRY(d.alloc(8 * E));
+  DG_TRY(cmap_decode(da, d.p, 0));
+  std::vector<uint32_t> nl(8 * E);
+  DG_CUDA(cudaMemcpy(nl.data(), d.p, 4 * 8 * E, cudaMemcpyDeviceToHost));
+  for (int64_t e = 0; e < E; ++e)
+    for (int v = 0; v < 8; ++v) nlist[8 * e + v] = nl[int64_t(v) * E + e];
+  return DG_OK;
+}
+
 dg_status dg_da_export(const dg_da* da, uint32_t* nlist, uint8_t* hmask, uint8_t* cnum, uint8_t* etype, uint8_t* level,
                        uint32_t* node_xyz, uint32_t* elem_xyz, uint8_t* node_bdy) {
   DG_CHECK(da, DG_EINVAL, "da_export: null mesh");

@@ -58,6 +58,18 @@ struct OctetSet {
   // operator and the tensor-memory multi-RHS kernel
   DBuf<uint32_t> rec;
 };
+// Compressed element-to-node map (cmap.cuh), built on request.
+struct CompressedMap {
+  int64_t ntiles = 0;    // tiles of 32 consecutive elements
+  int qbits = 0;         // narrow quotient width (bits), 0 when not built
+  int64_t wide_tiles = 0;
+  DBuf<uint2> rem;       // [E] remainder bytes, vertex order
+  DBuf<uint8_t> qmask;   // [E] vertices with a quotient
+  DBuf<uint32_t> base;   // [ntiles] smallest node id of the tile
+  DBuf<uint32_t> qoff;   // [ntiles] first quotient word | kCmapWide
+  DBuf<uint16_t> quot;   // quotient words
+  int64_t bytes() const { return 8 * rem.n + qmask.n + 4 * base.n + 4 * qoff.n + 2 * quot.n; }
+};
 constexpr int kOctChunk = 128;  // octets per chunk (one per thread of the chunked kernel)
 constexpr int kOctRec = 32;     // words per octet record
 }  // namespace dg
@@ -80,6 +92,7 @@ struct dg_da {
   // multi-right-hand-side one's (kMultiTile elements per tile, built on first use)
   dg::TileSet tiles_w, tiles_mr;
   dg::OctetSet octs;  // elements grouped by parent (octet operator kernel)
+  dg::CompressedMap cmap;  // compressed element map (on request)
   // operator launch shape picked by the autotuner on first use (-1: not yet)
   int tuned_f64 = -1, tuned_f32 = -1;
 };
@@ -164,6 +177,10 @@ long long wait_limit();  // clock cycles a bounded device wait may take
 dg_status device_wait_status(cudaStream_t s);
 dg_status build_tiles(dg_da* da, cudaStream_t s);  // da->tiles_w (kWarpTile)
 dg_status build_octets(dg_da* da, cudaStream_t s);  // da->octs (octet.cu)
+// da->cmap with narrow quotients of qbits (1..16) bits (cmap.cu); nl_out
+// [8][E] receives the map decoded from it
+dg_status build_cmap(dg_da* da, int qbits, cudaStream_t s);
+dg_status cmap_decode(const dg_da* da, uint32_t* nl_out, cudaStream_t s);
 dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s);
 // Hanging mask of element type t (0..17) for child number c
 // (include/oda/cnumEtypes.h:19-229).

@@ -25,6 +25,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "cmap.cuh"
 #include "dg_internal.h"
 #include "octet.cuh"
 
@@ -138,6 +139,41 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_kernel(const uint32_t* __
 #pragma unroll
     for (int v = 0; v < 8; ++v) id[v] = __ldg(nl + int64_t(v) * E + e);
     xor_perm(id, c);  // child-number frame: id[j] is the node of vertex j ^ c
+#pragma unroll
+    for (int j = 0; j < 8; ++j) u[j] = __ldg(x + id[j]);
+    const uint32_t mp = xor_perm_mask(mask, c);
+    if (mp) interp_frame(u, mp);
+    lapmass_ref(u, f1, f2);
+    if (mp) scatter_frame(u, mp);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) atomicAdd(y + id[j], u[j]);
+  }
+}
+
+// The element kernel on the compressed element map: a warp per tile of 32
+// consecutive elements decodes its lanes' node ids (cmap.cuh), then each lane
+// gathers, applies and scatters its element as lapmass_kernel does.  The map
+// moves about 12 bytes per element instead of 32.
+template <class T, class CT, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) lapmass_cmap_kernel(CMapView M, int64_t ntiles,
+                                                                   const uint32_t* __restrict__ meta,
+                                                                   const CT* __restrict__ ca,
+                                                                   const CT* __restrict__ cb, const T* __restrict__ x,
+                                                                   T* __restrict__ y) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const int64_t nw = int64_t(gridDim.x) * (BLOCK / 32);
+  for (int64_t t = (int64_t(blockIdx.x) * BLOCK + threadIdx.x) >> 5; t < ntiles; t += nw) {
+    uint32_t id[8];
+    cmap_ids(M, t, lane, id);
+    const int64_t e = t * 32 + lane;
+    if (e >= M.E) continue;
+    const uint32_t m = __ldg(meta + e);
+    const uint32_t lev = meta_lev(m), c = meta_cnum(m), mask = meta_mask(m);
+    const T h = elem_h<T>(lev);
+    const T a = ca ? T(ca[e]) : T(1), b = cb ? T(cb[e]) : T(1);
+    const T f1 = a * h / T(2), f2 = b * h * h * h / T(8);
+    T u[8];
+    xor_perm(id, c);
 #pragma unroll
     for (int j = 0; j < 8; ++j) u[j] = __ldg(x + id[j]);
     const uint32_t mp = xor_perm_mask(mask, c);
@@ -2101,7 +2137,8 @@ struct MatvecVariant {
                       // 12 octet with the next octet's ids in flight (cp.async), 13 the same
                       // with each child's coefficients loaded when its operator runs, 14 the
                       // words two octets ahead and x one octet ahead in flight, 15 next ids
-                      // in flight, the octet worked in two halves
+                      // in flight, the octet worked in two halves, 16 the element kernel on
+                      // the compressed element map
   int minb;
   const char* name;
 };
@@ -2139,6 +2176,7 @@ constexpr MatvecVariant kVariants[] = {
     {128, 2, 14, 2, "octet b128, next ids and x in flight, 2 CTAs/SM"},
     {128, 4, 15, 4, "octet b128, next ids in flight, two halves, 4 CTAs/SM"},
     {128, 5, 15, 5, "octet b128, next ids in flight, two halves, 5 CTAs/SM"},
+    {256, 8, 16, 4, "element, compressed map, b256, 8 CTAs/SM"},
 };
 // Coefficients of at most this many consecutive elements are staged per chunk.
 constexpr uint32_t kOctCoefCap = 2048;
@@ -2159,6 +2197,16 @@ static dg_status allow_dynamic_smem(const void* kern, size_t bytes) {
 }
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 
+// Whether the mesh has the structure a launch shape of this kind reads:
+// octets, octet chunks, warp tiles or the compressed map.
+static bool variant_runs(int k, const dg_da* da) {
+  if (k == 16) return da->cmap.qbits != 0;
+  if ((k == 6 || k >= 10) && da->octs.n == 0) return false;
+  if (k >= 7 && k <= 9 && da->octs.nchunk == 0) return false;
+  if (k >= 2 && k <= 5 && da->tiles_w.ntiles == 0) return false;
+  return true;
+}
+
 template <class T, class CT>
 static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* cb, const T* x, T* y,
                                 cudaStream_t s) {
@@ -2166,16 +2214,17 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
   // octet chunks or no warp tiles, e.g. a batch of meshes) falls back to
   // the element kernel rather than leaving y unwritten
   {
-    const int k = kVariants[v].kind;
-    const bool no_oct = (k == 6 || k >= 10) && da->octs.n == 0;
-    const bool no_chunk = k >= 7 && k <= 9 && da->octs.nchunk == 0;
-    const bool no_tile = k >= 2 && k <= 5 && da->tiles_w.ntiles == 0;
-    if (no_oct || no_chunk || no_tile) v = 0;
+    if (!variant_runs(kVariants[v].kind, da)) v = 0;
   }
   const MatvecVariant& V = kVariants[v];
   const unsigned g = V.per_sm ? grid_for(da->E, V.block, V.per_sm)
                               : unsigned((da->E + V.block - 1) / V.block > 0 ? (da->E + V.block - 1) / V.block : 1);
-  if (V.kind == 9) {
+  if (V.kind == 16) {
+    const CompressedMap& C = da->cmap;
+    const CMapView M{C.rem.p, C.qmask.p, C.base.p, C.qoff.p, C.quot.p, da->E};
+    lapmass_cmap_kernel<T, CT, 256, 4><<<grid_for(C.ntiles * 32, 256, V.per_sm), 256, 0, s>>>(
+        M, C.ntiles, da->meta.p, ca, cb, x, y);
+  } else if (V.kind == 9) {
     const OctetSet& O = da->octs;
     const size_t smem = (3 * sizeof(T) + 3 * sizeof(uint32_t)) * size_t(O.max_nodes);
     const unsigned gq = unsigned(std::min<int64_t>(O.nchunk, int64_t(sm_count()) * V.per_sm));
@@ -2320,7 +2369,8 @@ static int forced_variant() {
     v = -1;
     if (e && *e) {
       const int kind = !strcmp(e, "atomic") ? 0 : !strcmp(e, "warp") ? 2 : !strcmp(e, "octet") ? 6
-                     : !strcmp(e, "chunk") ? 7 : !strcmp(e, "lanes") ? 10 : !strcmp(e, "quads") ? 11 : -1;
+                     : !strcmp(e, "chunk") ? 7 : !strcmp(e, "lanes") ? 10 : !strcmp(e, "quads") ? 11
+                     : !strcmp(e, "cmap") ? 16 : -1;
       if (kind >= 0) {
         for (int i = kNumVariants - 1; i >= 0; --i)
           if (kVariants[i].kind == kind) v = i;
@@ -2364,9 +2414,7 @@ static dg_status pick_variant(const dg_da* da, int& choice, const CT* ca, const 
     DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));
     DG_TRY((launch_variant<T, CT>(0, da, ca, cb, x, y, s)));
     for (int v = 0; v < kNumVariants; ++v) {
-      if (kVariants[v].kind >= 2 && kVariants[v].kind <= 5 && da->tiles_w.ntiles == 0) continue;
-      if ((kVariants[v].kind == 6 || kVariants[v].kind >= 10) && da->octs.n == 0) continue;  // octet forms
-      if (kVariants[v].kind >= 7 && kVariants[v].kind <= 9 && da->octs.nchunk == 0) continue;
+      if (!variant_runs(kVariants[v].kind, da)) continue;
       for (int trial = 0; trial < 2; ++trial) {
         DG_CUDA(cudaMemsetAsync(flush.p, trial + 1, flush_bytes, s));
         DG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * da->N, s));

@@ -127,6 +127,23 @@ uint32_t dg_da_max_depth(const dg_da* da); /* embedded depth (maxDepth + 1) */
  * operator kernels (no reference counterpart; 0 for batched meshes). */
 int64_t dg_da_octets(const dg_da* da);
 
+/* Compressed element map: the DA's compressLut option (the remainder and
+ * quotient arrays m_ucpLutRemainders / m_uspLutQuotients, include/oda/oda.h:
+ * 332-341, decoded by getNodeIndices, include/oda/oda.txx:1125-1300) in a
+ * warp-tile form: per tile of 32 elements the smallest node id, per element a
+ * byte remainder of each node's offset from it and a 16-bit quotient where the
+ * offset needs one (a tile whose quotients exceed quotient_bits bits keeps
+ * 32-bit quotients).  quotient_bits is 16 normally (1..16; smaller values make
+ * wide tiles for tests).  Once built, the operator's autotuner also times the
+ * element kernel that reads this map ("element, compressed map"). */
+dg_status dg_da_compress_maps(dg_da* da, int quotient_bits);
+/* Bytes of the compressed map (0 when not built); *wide_tiles (may be NULL)
+ * receives the number of tiles with 32-bit quotients. */
+int64_t dg_da_compressed_map_bytes(const dg_da* da, int64_t* wide_tiles);
+/* The element map decoded from the compressed form on the device, into host
+ * nlist [E][8] (the layout of dg_da_export). */
+dg_status dg_da_decompress_maps(const dg_da* da, uint32_t* nlist);
+
 /* Copy the maps to host memory; any pointer may be NULL.  nlist [E][8]
  * (getNodeIndices, include/oda/oda.txx:1111), hmask [E]
  * (getHangingNodeIndex, src/oda/oda.C:784), cnum [E] (getChildNumber,

@@ -52,6 +52,7 @@ def test_every_launch_shape(gpu, oracle, name):
     """Each operator kernel the autotuner may pick, fixed in turn, FP64 and FP32."""
     import torch
     ref, da = setup(gpu, oracle, name)
+    da.compressMaps()  # the compressed-map shape reads its own map, not a fallback
     coef = I.sphere_coefficients(da.elementCenters())
     x = I.uniform_rhs(ref.N, 5)
     y_ref = ref.matvec(x, coef)

@@ -8,6 +8,12 @@
 //
 //   matshell_driver lapmass <octs.u32> <maxDepth> <x.f64> <coef.f64|none> <y.f64> <d.f64>
 //   matshell_driver elastic <octs.u32> <maxDepth> <x.f64> <mu> <lambda> <y.f64> <d.f64>
+//   matshell_driver transfer <octs.u32> <maxDepth> <nlevels> <level> <xf.f64> <xc.f64> <out>
+//
+// The transfer mode builds the hierarchy, wraps R from `level` to level + 1
+// in a MatShell as DAMGSetUp does (src/omg/omg.C:2278-2283) and writes
+// MatMult (R xf), MatMultTranspose (P xc), MatMultAdd (1 + R xf) and
+// MatMultTransposeAdd (1 + P xc) to <out>.R / .P / .RA / .PA.
 //
 // Octant files hold 4 x uint32 per octant (x, y, z, level).
 #include <cstdio>
@@ -46,7 +52,66 @@ int fail(const char* where, dg_status st) {
 
 }  // namespace
 
+int run_transfer(int argc, char** argv) {
+  if (argc < 9) return 2;
+  PetscInitialize(&argc, &argv, nullptr, nullptr);
+  std::vector<uint32_t> raw = read_raw<uint32_t>(argv[2]);
+  const uint32_t depth = uint32_t(std::atoi(argv[3]));
+  const int nlevels = std::atoi(argv[4]), level = std::atoi(argv[5]);
+  std::vector<dg_octant> octs(raw.size() / 4);
+  for (size_t i = 0; i < octs.size(); ++i)
+    octs[i] = dg_octant{raw[4 * i], raw[4 * i + 1], raw[4 * i + 2], raw[4 * i + 3]};
+  dg_octree* tree = nullptr;
+  dg_damg* m = nullptr;
+  dg_status st = dg_octree_from_octants(octs.data(), int64_t(octs.size()), 0, depth, &tree);
+  if (st) return fail("octree", st);
+  dg_damg_config cfg;
+  dg_damg_default_config(&cfg);
+  cfg.nlevels = nlevels;
+  if ((st = dg_damg_create(tree, &cfg, &m))) return fail("damg", st);
+  Mat R;
+  if (dendro_b200::DgCreateRestrictionShell(PETSC_COMM_WORLD, m, level, 1, &R)) return 1;
+  const std::vector<double> xf = read_raw<double>(argv[6]), xc = read_raw<double>(argv[7]);
+  Vec vf, vc, rf, pc, one_c, one_f, ra, pa;
+  auto make = [](const std::vector<double>& v, Vec* out) {
+    VecCreateSeq(PETSC_COMM_WORLD, PetscInt(v.size()), out);
+    PetscScalar* p = nullptr;
+    VecGetArray(*out, &p);
+    std::memcpy(p, v.data(), sizeof(double) * v.size());
+    VecRestoreArray(*out, &p);
+  };
+  make(xf, &vf);
+  make(xc, &vc);
+  VecDuplicate(vc, &rf);
+  VecDuplicate(vf, &pc);
+  VecDuplicate(vc, &one_c);
+  VecDuplicate(vf, &one_f);
+  VecSet(one_c, 1.0);
+  VecSet(one_f, 1.0);
+  VecDuplicate(vc, &ra);
+  VecDuplicate(vf, &pa);
+  VecSet(pc, 7.0);  // overwritten by MatMultTranspose
+  if (MatMult(R, vf, rf) || MatMultTranspose(R, vc, pc) || MatMultAdd(R, vf, one_c, ra) ||
+      MatMultTransposeAdd(R, vc, one_f, pa))
+    return 1;
+  const std::string out = argv[8];
+  const std::pair<const char*, Vec> outs[] = {{".R", rf}, {".P", pc}, {".RA", ra}, {".PA", pa}};
+  for (const auto& o : outs) {
+    PetscScalar* p = nullptr;
+    VecGetArray(o.second, &p);
+    write_raw((out + o.first).c_str(), p, o.second->a.size());
+  }
+  ((PetscErrorCode(*)(Mat))R->op[MATOP_DESTROY])(R);
+  MatDestroy(&R);
+  for (Vec v : {vf, vc, rf, pc, one_c, one_f, ra, pa}) VecDestroy(&v);
+  dg_damg_destroy(m);
+  dg_octree_destroy(tree);
+  PetscFinalize();
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  if (argc > 1 && !std::strcmp(argv[1], "transfer")) return run_transfer(argc, argv);
   if (argc < 8) {
     std::fprintf(stderr, "bad arguments\n");
     return 2;

@@ -63,3 +63,26 @@ def test_matshell_through_matmult(gpu, oracle, tmp_path, name):
     g["x3"].tofile(x3)
     run("elastic", octs, d, x3, float(g["mu"]), float(g["lam"]), y, dg)
     assert rel(np.fromfile(y), g["y3"]) < 1e-12
+
+
+@pytest.mark.gpu
+def test_transfer_shell_through_matmult(gpu, tmp_path):
+    """R as a MatShell (src/omg/omg.C:2278-2283): MatMult restricts, MatMultTranspose
+    prolongs, the ADD forms add to another Vec; against the reference's own
+    restrictMatVecType1 / prolongMatVecType1 outputs."""
+    exe = build_driver(str(tmp_path))
+    g = load("transfer_gauss1k_d8")
+    d, nl = int(g["depth"]), int(g["nlevels"])
+    octs = str(tmp_path / "bal.u32")
+    g["bal"].astype(np.uint32).tofile(octs)
+    for l in range(nl - 1):
+        xf, xc, out = str(tmp_path / "xf.f64"), str(tmp_path / "xc.f64"), str(tmp_path / f"t{l}")
+        g[f"xf{l}"].tofile(xf)
+        g[f"xc{l}"].tofile(xc)
+        r = subprocess.run([exe, "transfer", octs, str(d), str(nl), str(l), xf, xc, out],
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-3000:]
+        assert rel(np.fromfile(out + ".R"), g[f"restrict{l}"]) < 1e-12
+        assert rel(np.fromfile(out + ".P"), g[f"prolong{l}"]) < 1e-12
+        assert rel(np.fromfile(out + ".RA") - 1.0, g[f"restrict{l}"]) < 1e-12
+        assert rel(np.fromfile(out + ".PA") - 1.0, g[f"prolong{l}"]) < 1e-12

@@ -11,6 +11,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <memory>
 #include <vector>
 
@@ -866,6 +868,9 @@ dg_status build_restriction(Level& F, int64_t Nc, cudaStream_t s) {
 dg_status build_weight_codes(Level& F, cudaStream_t s) {
   const int64_t nnz = F.pval.n;
   if (!nnz || F.rval.n != nnz) return DG_OK;
+  // DG_TRANSFER_CODES=0 keeps the FP64 / FP32 weights (to compare the two forms)
+  if (const char* e = getenv("DG_TRANSFER_CODES"))
+    if (!strcmp(e, "0")) return DG_OK;
   DBuf<uint32_t> bad;
   DG_TRY(bad.alloc(1));
   DG_CUDA(cudaMemsetAsync(bad.p, 0, 4, s));

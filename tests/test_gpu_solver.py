@@ -108,3 +108,18 @@ def test_solve_with_unaligned_device_vectors(gpu, oracle):
     _, rep1 = mg.solve(bb[1:], xx[1:])
     assert rep0["converged"] and rep1["converged"]
     assert float(torch.linalg.norm(x0 - xx[1:])) <= 1e-12 * float(torch.linalg.norm(x0))
+
+
+def test_transfer_codes_bit_identical(gpu, oracle, monkeypatch):
+    """The 8-bit weight codes of P and R give the FP64 weights' results bit for bit."""
+    pts, d, m = points("lognormal20k_d12")
+    bal = oracle.balance(oracle.points2octree(pts, d, m), d)
+    coded = gpu.DAMG(gpu.Octree.from_octants(bal, d), nlevels=4)
+    monkeypatch.setenv("DG_TRANSFER_CODES", "0")
+    plain = gpu.DAMG(gpu.Octree.from_octants(bal, d), nlevels=4)
+    for l in range(coded.nlevels - 1):
+        xf = I.uniform_rhs(int(coded.N[l]), 30 + l)
+        xc = I.uniform_rhs(int(coded.N[l + 1]), 40 + l)
+        assert np.array_equal(coded.restrict(l, xf), plain.restrict(l, xf))
+        xf0 = I.uniform_rhs(int(coded.N[l]), 50 + l)
+        assert np.array_equal(coded.prolong(l, xc, xf0.copy()), plain.prolong(l, xc, xf0.copy()))

@@ -75,6 +75,9 @@ def parse():
     p.add_argument("--halo-profile", metavar="PARTS", type=int, default=0,
                    help="only: split the matvec workload's mesh into PARTS parts (all on this GPU) and time "
                         "each part's pack, independent and dependent operator launches, then exit")
+    p.add_argument("--cmap-profile", metavar="WORKLOAD", default=None,
+                   help="only: the element kernel on the compressed and on the raw element map, FP64 and FP32, "
+                        "one launch each between cudaProfilerStart/Stop, then exit")
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     return p.parse_args()
 
@@ -667,6 +670,45 @@ def run_vcycle_profile(workload):
     print(json.dumps({"vcycle_profile": out}), flush=True)
 
 
+def run_cmap_profile(workload):
+    """The element kernel on the compressed element map and on the raw map, FP64 then FP32, one
+    launch each between cudaProfilerStart / cudaProfilerStop (for ncu --profile-from-start off),
+    after a warm-up launch of each; prints their times (CUDA events)."""
+    import torch
+
+    import dendro_b200 as dg
+    from dendro_b200 import inputs as I
+    pts, depth = build_workload(workload, 1.0)
+    da = dg.DA(dg.balanceOctree(dg.points2Octree(pts, depth, 1)))
+    nbytes = da.compressMaps()
+    A = dg.Jacobian2(da, I.sphere_coefficients(da.elementCenters()))
+    shape = None
+    for v in range(A.kernel_count()):
+        A.set_kernel(v, 0)
+        if "compressed map" in A.kernel_name(0):
+            shape = v
+    x64 = torch.tensor(I.uniform_rhs(da.N, 3), device="cuda")
+    out = {"workload": workload, "elements": da.E, "nodes": da.N, "map_bytes_per_element": round(nbytes / da.E, 3)}
+    x32 = x64.float()
+    y64, y32 = torch.empty_like(x64), torch.empty_like(x32)
+    runs = [(p, tag, v) for p in (0, 1) for tag, v in (("compressed", shape), ("raw", 0))]
+    for prec, tag, v in runs:
+        A.set_kernel(v, prec)
+        A.mult(x64, y64) if prec == 0 else A.mult(x32, y32)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    for prec, tag, v in runs:
+        A.set_kernel(v, prec)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        A.mult(x64, y64) if prec == 0 else A.mult(x32, y32)
+        e1.record()
+        torch.cuda.synchronize()
+        out[f"{'f64' if prec == 0 else 'f32'}_{tag}_ms"] = round(e0.elapsed_time(e1), 4)
+    torch.cuda.profiler.stop()
+    print(json.dumps({"cmap_profile": out}), flush=True)
+
+
 def run_halo_profile(parts, workload):
     """The matvec workload's mesh split into `parts` parts by the weighted
     partition, every part on this GPU in turn: per part the launches one
@@ -728,6 +770,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     if args.vcycle_profile:
         return run_vcycle_profile(args.vcycle_profile)
+    if args.cmap_profile:
+        return run_cmap_profile(args.cmap_profile)
     if args.halo_profile:
         return run_halo_profile(args.halo_profile, args.workload)
     if args.impl == "reference":

@@ -607,7 +607,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_kernel(
 // sums leave.  Slots are private to a thread: its own cp.async.wait_group is
 // the only synchronisation.
 constexpr int kOctPfWords = 36;  // 27 node ids, 8 element ids, meta
-template <class T, class CT, int BLOCK, int MINB, bool HOIST = true>
+template <class T, class CT, int BLOCK, int MINB, bool HOIST = true, bool FAST = false>
 __global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_pf_kernel(
     int64_t n, const uint32_t* __restrict__ ometa, const uint32_t* __restrict__ oid,
     const uint32_t* __restrict__ oelem, const CT* __restrict__ ca, const CT* __restrict__ cb,
@@ -666,7 +666,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_pf_kernel(
       none |= id == kNoNode ? (1u << p) : 0u;
       xv[p] = id != kNoNode ? __ldg(x + id) : T(0);
     }
-    octet_apply<T>(xv, yv, none, m, [&](int c, T& f1, T& f2) {
+    auto scale = [&](int c, T& f1, T& f2) {
       if (ca) {
         if (HOIST) {
           f1 *= fa[c];
@@ -677,7 +677,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_octet_pf_kernel(
           f2 *= T(__ldg(cb + e));
         }
       }
-    });
+    };
+    // FAST: a warp whose octets all have 8 children and no point to fill
+    // takes the compile-time form of the arithmetic
+    if (FAST && __all_sync(__activemask(), cm0 == 255u && (none & oct_hangable()) == 0u))
+      octet_apply<T, true>(xv, yv, none, m, scale);
+    else
+      octet_apply<T>(xv, yv, none, m, scale);
 #pragma unroll
     for (int p = 0; p < 27; ++p) {
       const uint32_t id = sw[sl][p][tid];
@@ -2138,7 +2144,8 @@ struct MatvecVariant {
                       // with each child's coefficients loaded when its operator runs, 14 the
                       // words two octets ahead and x one octet ahead in flight, 15 next ids
                       // in flight, the octet worked in two halves, 16 the element kernel on
-                      // the compressed element map
+                      // the compressed element map, 17 as 12 with a compile-time form for
+                      // warps of complete octets without points to fill
   int minb;
   const char* name;
 };
@@ -2177,6 +2184,7 @@ constexpr MatvecVariant kVariants[] = {
     {128, 4, 15, 4, "octet b128, next ids in flight, two halves, 4 CTAs/SM"},
     {128, 5, 15, 5, "octet b128, next ids in flight, two halves, 5 CTAs/SM"},
     {256, 8, 16, 4, "element, compressed map, b256, 8 CTAs/SM"},
+    {128, 4, 17, 4, "octet b128, next ids in flight, complete-warp fast path, 4 CTAs/SM"},
 };
 // Coefficients of at most this many consecutive elements are staged per chunk.
 constexpr uint32_t kOctCoefCap = 2048;
@@ -2264,6 +2272,10 @@ static dg_status launch_variant(int v, const dg_da* da, const CT* ca, const CT* 
     if (V.minb == 2) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 2>));
     else if (V.minb == 3) DG_TRY(go(lapmass_octchunk_kernel<T, CT, 3>));
     else DG_TRY(go(lapmass_octchunk_kernel<T, CT, 4>));
+  } else if (V.kind == 17) {
+    const OctetSet& O = da->octs;
+    const unsigned gp = grid_for(O.n, 128, V.per_sm);
+    lapmass_octet_pf_kernel<T, CT, 128, 4, true, true><<<gp, 128, 0, s>>>(O.n, O.meta.p, O.id.p, O.elem.p, ca, cb, x, y);
   } else if (V.kind == 15) {
     const OctetSet& O = da->octs;
     const unsigned gp = grid_for(O.n, 128, V.per_sm);

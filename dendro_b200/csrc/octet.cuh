@@ -71,11 +71,13 @@ __host__ __device__ constexpr uint32_t oct_hangable() {
   return m;
 }
 
-template <class T, class Coef>
+// FULL: the caller knows that all 8 children are present and that no point
+// needs filling (a compile-time child loop and no fill or fold).
+template <class T, bool FULL = false, class Coef>
 __device__ __forceinline__ void octet_apply(T (&xv)[27], T (&yv)[27], uint32_t none, uint32_t m, Coef coef) {
   // octets without a point to fill skip the interpolation and the fold (a
   // branch, uniform when a warp works one octet)
-  const bool fill = (none & oct_hangable()) != 0u;
+  const bool fill = !FULL && (none & oct_hangable()) != 0u;
   if (fill) {
 #pragma unroll
     for (int p = 0; p < 27; ++p) {
@@ -91,12 +93,12 @@ __device__ __forceinline__ void octet_apply(T (&xv)[27], T (&yv)[27], uint32_t n
   }
 #pragma unroll
   for (int p = 0; p < 27; ++p) yv[p] = T(0);
-  const uint32_t cm = ometa_cmask(m);
+  const uint32_t cm = FULL ? 255u : ometa_cmask(m);
   const T h = elem_h<T>(ometa_lev(m));
   const T g1 = h * T(0.5), g2 = h * h * h * T(0.125);
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
-    if ((cm >> c) & 1u) {
+    if (FULL || ((cm >> c) & 1u)) {
       T f1 = g1, f2 = g2;
       coef(c, f1, f2);
       T u[8];

@@ -49,6 +49,8 @@ TRAFFIC = {
     "octet b256, 2 CTAs/SM": 217540864 + 18269184,
     "octet b128, next ids in flight, 4 CTAs/SM": 217420288 + 15001600,
     "octet b128, next ids in flight, two halves, 4 CTAs/SM": 217417472 + 15151104,
+    "octet b128, next ids in flight, two halves, 5 CTAs/SM": 217705984 + 17701376,
+    "octet b128, next ids in flight, complete-warp fast path, 4 CTAs/SM": 217558784 + 15632640,
 }
 
 

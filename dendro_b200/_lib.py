@@ -69,6 +69,7 @@ def lib():
         "dg_da_sizes": ([P, I64P, I64P, I64P], I),
         "dg_da_octets": ([P], C.c_int64),
         "dg_da_compress_maps": ([P, I], I),
+        "dg_da_load_vector": ([P, P, P, I], I),
         "dg_da_compressed_map_bytes": ([P, I64P], C.c_int64),
         "dg_da_decompress_maps": ([P, P], I),
         "dg_da_max_depth": ([P], U32),
@@ -163,7 +164,7 @@ def exported_symbols():
         "dg_status_string", "dg_last_error", "dg_device_count", "dg_points2octree", "dg_octree_from_octants",
         "dg_balance_octree", "dg_coarsen_octree", "dg_octree_size", "dg_octree_max_depth", "dg_octree_export",
         "dg_octree_destroy", "dg_da_create", "dg_da_create_from_maps", "dg_da_sizes", "dg_da_max_depth", "dg_da_octets",
-        "dg_da_compress_maps", "dg_da_compressed_map_bytes", "dg_da_decompress_maps",
+        "dg_da_compress_maps", "dg_da_compressed_map_bytes", "dg_da_decompress_maps", "dg_da_load_vector",
         "dg_da_export", "dg_da_element_centers", "dg_da_destroy", "dg_mat_create_lapmass",
         "dg_mat_create_elasticity", "dg_mat_mult", "dg_mat_mult_f32", "dg_mat_get_diagonal",
         "dg_mat_mult_host", "dg_mat_size", "dg_mat_kernel_name", "dg_mat_destroy", "dg_damg_default_config", "dg_damg_create",

@@ -172,6 +172,21 @@ class DA:
               "da_export")
         return out
 
+    def loadVector(self, force, b=None):
+        """ComputeRHS_omgNeumann (omgNeumann.C:749-785): the force sampled at the element
+        centres (elementCenters order) -> the load vector b [N].  Device tensors stay on
+        the device; numpy arrays go through host copies."""
+        if _is_device(force):
+            import torch
+            if b is None:
+                b = torch.empty(self.N, dtype=torch.float64, device=force.device)
+            check(lib().dg_da_load_vector(self.h, ptr(force), ptr(b), 1), "da_load_vector")
+            return b
+        f = np.ascontiguousarray(force, np.float64)
+        out = np.empty(self.N, np.float64)
+        check(lib().dg_da_load_vector(self.h, ptr(f), ptr(out), 0), "da_load_vector")
+        return out
+
     def compressMaps(self, quotient_bits: int = 16) -> int:
         """Build the compressed element map (the DA's compressLut option); returns its bytes.
         The operator's autotuner then also times the element kernel that reads it."""

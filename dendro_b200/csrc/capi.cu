@@ -276,6 +276,22 @@ uint32_t dg_da_max_depth(const dg_da* da) { return da ? da->D : 0; }
 
 int64_t dg_da_octets(const dg_da* da) { return da ? da->octs.n : 0; }
 
+dg_status dg_da_load_vector(const dg_da* da, const double* force, double* b, int on_device) {
+  DG_CHECK(da && force && b, DG_EINVAL, "da_load_vector: bad arguments");
+  if (on_device) {
+    DG_TRY(load_vector(da, force, b, 0));
+    DG_CUDA(cudaDeviceSynchronize());
+    return DG_OK;
+  }
+  DBuf<double> df, db;
+  DG_TRY(df.alloc(da->E));
+  DG_TRY(db.alloc(da->N));
+  if (da->E) DG_CUDA(cudaMemcpy(df.p, force, 8 * size_t(da->E), cudaMemcpyHostToDevice));
+  DG_TRY(load_vector(da, df.p, db.p, 0));
+  if (da->N) DG_CUDA(cudaMemcpy(b, db.p, 8 * size_t(da->N), cudaMemcpyDeviceToHost));
+  return DG_OK;
+}
+
 dg_status dg_da_compress_maps(dg_da* da, int quotient_bits) {
   DG_CHECK(da, DG_EINVAL, "compress_maps: null mesh");
   DG_TRY(build_cmap(da, quotient_bits, 0));

@@ -181,6 +181,8 @@ dg_status build_octets(dg_da* da, cudaStream_t s);  // da->octs (octet.cu)
 // [8][E] receives the map decoded from it
 dg_status build_cmap(dg_da* da, int qbits, cudaStream_t s);
 dg_status cmap_decode(const dg_da* da, uint32_t* nl_out, cudaStream_t s);
+// b = the load vector of a force sampled at the element centres (matvec.cu)
+dg_status load_vector(const dg_da* da, const double* force, double* b, cudaStream_t s);
 dg_status build_tile_set(const dg_da* da, int te, TileSet& ts, cudaStream_t s);
 // Hanging mask of element type t (0..17) for child number c
 // (include/oda/cnumEtypes.h:19-229).

@@ -150,6 +150,32 @@ __global__ void __launch_bounds__(BLOCK, MINB) lapmass_kernel(const uint32_t* __
   }
 }
 
+// Load vector (ComputeRHS_omgNeumann, examples/src/backend/omgNeumann.C:
+// 749-785): b += f_e h^3 / 8 T^T 1 per element, the force sampled at the
+// element's centre times the integrals of its vertices' shape functions
+// (RHSType2Stencil), the hanging vertices' shares moved to their nodes by the
+// frame fold.
+__global__ void load_vector_kernel(const uint32_t* __restrict__ nl, const uint32_t* __restrict__ meta,
+                                   const double* __restrict__ force, int64_t E, double* __restrict__ b) {
+  for (int64_t e = gtid(); e < E; e += gstride()) {
+    const uint32_t m = meta[e];
+    const uint32_t c = meta_cnum(m);
+    const double h = elem_h<double>(meta_lev(m));
+    const double w = force[e] * h * h * h * 0.125;
+    uint32_t id[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) id[v] = __ldg(nl + int64_t(v) * E + e);
+    xor_perm(id, c);
+    double u[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) u[j] = w;
+    const uint32_t mp = xor_perm_mask(meta_mask(m), c);
+    if (mp) scatter_frame(u, mp);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) atomicAdd(b + id[j], u[j]);
+  }
+}
+
 // The element kernel on the compressed element map: a warp per tile of 32
 // consecutive elements decodes its lanes' node ids (cmap.cuh), then each lane
 // gathers, applies and scatters its element as lapmass_kernel does.  The map
@@ -2701,6 +2727,13 @@ dg_status lapmass_apply_host_pipelined_f64(dg_mat* A, const double* hx, double* 
   P.variant = (kind >= 2 && kind <= 4) ? da->tuned_f64 : kDefaultVariant;
   DG_TRY(enqueue_host_pipe(A, P, hx, hy));
   DG_CUDA(cudaStreamSynchronize(P.sk));
+  return DG_OK;
+}
+
+dg_status load_vector(const dg_da* da, const double* force, double* b, cudaStream_t s) {
+  DG_CUDA(cudaMemsetAsync(b, 0, 8 * size_t(da->N), s));
+  if (da->E) load_vector_kernel<<<grid_for(da->E, 256, 8), 256, 0, s>>>(da->nl.p, da->meta.p, force, da->E, b);
+  DG_CUDA(cudaGetLastError());
   return DG_OK;
 }
 

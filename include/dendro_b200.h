@@ -127,6 +127,13 @@ uint32_t dg_da_max_depth(const dg_da* da); /* embedded depth (maxDepth + 1) */
  * operator kernels (no reference counterpart; 0 for batched meshes). */
 int64_t dg_da_octets(const dg_da* da);
 
+/* Load vector of the Neumann problem (ComputeRHS_omgNeumann,
+ * examples/src/backend/omgNeumann.C:749-785): force [E] sampled at the
+ * element centres (the order of dg_da_element_centers), b [N] =
+ * sum over elements of force_e h^3/8 RHSType2Stencil[childNum][elemType]
+ * at the element's nodes.  Host or device arrays (on_device). */
+dg_status dg_da_load_vector(const dg_da* da, const double* force, double* b, int on_device);
+
 /* Compressed element map: the DA's compressLut option (the remainder and
  * quotient arrays m_ucpLutRemainders / m_uspLutQuotients, include/oda/oda.h:
  * 332-341, decoded by getNodeIndices, include/oda/oda.txx:1125-1300) in a

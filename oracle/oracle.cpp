@@ -414,12 +414,18 @@ void hanging_T(uint32_t c, uint32_t mask, double T[8][8]) {
 
 struct Tables {
   double L[8][18][8][8], Ms[8][18][8][8], GD[8][18][24][24];
+  double Rhs[8][18][8];  // T^T 1: the shape functions' integrals on the reference cube per node slot
   Tables() {
     const RefMats& R = refmats();
     for (uint32_t c = 0; c < 8; ++c)
       for (int t = 0; t < 18; ++t) {
         double T[8][8];
         hanging_T(c, kEtypeMask[c][t], T);
+        for (int i = 0; i < 8; ++i) {
+          double r = 0;
+          for (int a = 0; a < 8; ++a) r += T[a][i];
+          Rhs[c][t][i] = r;
+        }
         for (int i = 0; i < 8; ++i)
           for (int j = 0; j < 8; ++j) {
             double l = 0, m = 0;
@@ -531,6 +537,21 @@ void matvec_elems(const Mesh& M, const double* coef, const double* x, double* y,
 void matvec(const Mesh& M, const double* coef, const double* x, double* y) {
   std::fill(y, y + M.N, 0.0);
   matvec_elems(M, coef, x, y, nullptr, 0);
+}
+
+// ComputeRHS_omgNeumann (examples/src/backend/omgNeumann.C:749-785): the
+// force sampled at each element's centre times RHSType2Stencil (the integral
+// of each vertex's shape function on the reference cube, hanging vertices'
+// shares moved to their nodes) times h^3 / 8, summed at the nodes.
+void load_vector(const Mesh& M, const double* force, double* b) {
+  const Tables& T = tables();
+  std::fill(b, b + M.N, 0.0);
+  for (size_t e = 0; e < M.E; ++e) {
+    const double h = std::ldexp(1.0, 1 - int(M.elev[e]));
+    const double fac = force[e] * h * h * h / 8.0;
+    const uint32_t c = M.cnum[e], t = M.etype[e];
+    for (int k = 0; k < 8; ++k) b[M.nlist[8 * e + k]] += T.Rhs[c][t][k] * fac;
+  }
 }
 
 // JAC_TYPE2_ELEM_DIAG_BLOCK (omgNeumann.C:396-438).
@@ -1172,6 +1193,9 @@ void orc_matvec_elems(void* m, const double* coef, const double* x, double* y, c
   matvec_elems(*(Mesh*)m, coef, x, y, elems, n);
 }
 void orc_diagonal(void* m, const double* coef, double* d) { diagonal(*(Mesh*)m, coef, d); }
+void orc_load_vector(void* m, const double* force, double* b) { load_vector(*(Mesh*)m, force, b); }
+// RHSType2Stencil as derived here, [8][18][8].
+void orc_rhs_table(double* R) { std::memcpy(R, tables().Rhs, sizeof(tables().Rhs)); }
 void orc_elasticity_matvec(void* m, double mu, double lam, const uint8_t* bdy, const double* x, double* y) {
   elasticity_matvec(*(Mesh*)m, mu, lam, bdy, x, y);
 }

@@ -50,6 +50,8 @@ def lib():
         L.orc_matvec.argtypes = [P, P, P, P]
         L.orc_matvec_elems.argtypes = [P, P, P, P, P, C.c_int64]
         L.orc_diagonal.argtypes = [P, P, P]
+        L.orc_load_vector.argtypes = [P, P, P]
+        L.orc_rhs_table.argtypes = [P]
         L.orc_elasticity_matvec.argtypes = [P, C.c_double, C.c_double, P, P, P]
         L.orc_stencils.argtypes = [P, P, P]
         L.orc_hanging_T.argtypes = [C.c_uint32, C.c_uint32, P]
@@ -165,6 +167,13 @@ class Mesh:
         lib().orc_matvec_elems(self.h, _ptr(c), _ptr(x), _ptr(y), _ptr(e), len(e))
         return y
 
+    def load_vector(self, force):
+        """ComputeRHS_omgNeumann (omgNeumann.C:749-785): force per element (at its centre) -> b."""
+        f = np.ascontiguousarray(force, np.float64)
+        b = np.empty(self.N, np.float64)
+        lib().orc_load_vector(self.h, _ptr(f), _ptr(b))
+        return b
+
     def diagonal(self, coef=None):
         d = np.empty(self.N, np.float64)
         c = None if coef is None else np.ascontiguousarray(coef, np.float64)
@@ -236,6 +245,13 @@ def prolongation(fine: Mesh, coarse: Mesh):
     for q in (p, c, v):
         lib().orc_free(q)
     return ptr, col, val
+
+
+def rhs_table() -> np.ndarray:
+    """RHSType2Stencil [childNum][elemType][vertex] as the oracle derives it (T^T 1)."""
+    out = np.empty((8, 18, 8))
+    lib().orc_rhs_table(_ptr(out))
+    return out
 
 
 def coarse_coef(fine: Mesh, fine_coef, coarse: Mesh):

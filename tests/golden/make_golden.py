@@ -293,6 +293,14 @@ def table_digest(a):
                      (a * w).sum(axis=(2, 3))], -1)
 
 
+def vector_digest(a):
+    """Checksums of each (child number, type) vector: sum, sum of squares, sum of
+    magnitudes and a position-weighted sum."""
+    m = a.shape[-1]
+    w = (7.0 * np.arange(m) + 1.0) / (10.0 * m)
+    return np.stack([a.sum(-1), (a * a).sum(-1), np.abs(a).sum(-1), (a * w).sum(-1)], -1)
+
+
 def stencil_digests():
     """Checksums of the reference's Laplacian, mass, grad-div and same-level
     restriction tables (Stencils/*Type2Stencils.inp)."""
@@ -301,6 +309,9 @@ def stencil_digests():
                           ("gd", "GDType2Stencils.inp", 24), ("rmat2", "RmatType2Stencils.inp", 8)):
         a = np.array(open(os.path.join(STENCILS, fname)).read().split(), float).reshape(8, 18, m, m)
         rec[tag] = table_digest(a)
+    # RHSType2Stencil [child][type][vertex] (ComputeRHS_omgNeumann's load table)
+    r = np.array(open(os.path.join(STENCILS, "RHSType2Stencils.inp")).read().split(), float).reshape(8, 18, 8)
+    rec["rhs"] = vector_digest(r)
     # type-1 tables [coarse child][type][fine child][8][8], digested per (type, fine child)
     for tag, fname in (("lap1", "LapType1Stencils.inp"), ("mass1", "MassType1Stencils.inp")):
         a = np.array(open(os.path.join(STENCILS, fname)).read().split(), float).reshape(8, 18 * 8, 8, 8)

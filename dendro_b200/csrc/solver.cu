@@ -1800,8 +1800,8 @@ void dg_damg_destroy(dg_damg* m) { delete m; }
 }  // extern "C"
 
 // ------------------------------------------------------ multi-RHS solve ---
-// R right-hand sides solved together (BASELINE's batched form: many right-
-// hand sides on one mesh): node-major [N][R] blocks, one flexible PCG per
+// R right-hand sides solved together (the batched form with many right-hand
+// sides on one mesh): node-major [N][R] blocks, one flexible PCG per
 // column in FP64 (its own step lengths, frozen once it has converged) around
 // one V-cycle per iteration for all columns -- the operator applications of
 // every level are the octet multi-RHS kernel (a warp per parent octant and

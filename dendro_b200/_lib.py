@@ -148,6 +148,11 @@ def lib():
         "dg_parcsr_apply": ([P, P, P, P, I, P], I),
         "dg_parcsr_destroy": ([P], None),
         "dg_vec_jacobi_update": ([P, P, P, P, C.c_double, I64, P], I),
+        "dg_vec_jacobi_update_f32": ([P, P, P, P, C.c_float, I64, P], I),
+        "dg_mat_mult_add_f32": ([P, P, P, P], I),
+        "dg_halo_pack_f32": ([P, P, P, I, P], I),
+        "dg_parcsr_pack_f32": ([P, P, P, P], I),
+        "dg_parcsr_apply_f32": ([P, P, P, P, I, P], I),
         "dg_halo_destroy": ([P], None),
     }
     for name, (args, res) in sig.items():
@@ -182,7 +187,8 @@ def exported_symbols():
         "dg_halo_comm", "dg_halo_part", "dg_halo_local_da", "dg_halo_pack", "dg_halo_accumulate",
         "dg_halo_destroy", "dg_mat_mult_add", "dg_damg_transfer_export", "dg_damg_level_coef",
         "dg_damg_coarse_solve", "dg_parcsr_create", "dg_parcsr_sizes", "dg_parcsr_comm", "dg_parcsr_pack",
-        "dg_parcsr_apply", "dg_parcsr_destroy", "dg_vec_jacobi_update",
+        "dg_parcsr_apply", "dg_parcsr_destroy", "dg_vec_jacobi_update", "dg_vec_jacobi_update_f32",
+        "dg_mat_mult_add_f32", "dg_halo_pack_f32", "dg_parcsr_pack_f32", "dg_parcsr_apply_f32",
     ]
 
 

@@ -249,9 +249,13 @@ class _Mat:
         return ya
 
     def mult_add(self, x, y, stream=None):
-        """y += A x (FP64 device tensors, scalar operator)."""
+        """y += A x (FP64 or FP32 device tensors, scalar operator)."""
+        import torch
         s = None if stream is None else C.c_void_p(stream.cuda_stream)
-        check(lib().dg_mat_mult_add(self.h, ptr(x), ptr(y), s), "mat_mult_add")
+        if x.dtype == torch.float32:
+            check(lib().dg_mat_mult_add_f32(self.h, ptr(x), ptr(y), s), "mat_mult_add_f32")
+        else:
+            check(lib().dg_mat_mult_add(self.h, ptr(x), ptr(y), s), "mat_mult_add")
         return y
 
     def mult_multi(self, X, Y=None, split: int = 3, stream=None):

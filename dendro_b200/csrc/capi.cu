@@ -451,6 +451,12 @@ dg_status dg_mat_mult_add(dg_mat* A, const double* x, double* y, void* stream) {
   return lapmass_apply_add_f64(A, x, y, as_stream(stream));
 }
 
+dg_status dg_mat_mult_add_f32(dg_mat* A, const float* x, float* y, void* stream) {
+  DG_CHECK(A && x && y, DG_EINVAL, "mat_mult_add_f32: bad arguments");
+  DG_CHECK(A->kind == 0, DG_ENOTIMPL, "mat_mult_add_f32: scalar operator only");
+  return lapmass_apply_add_f32(A, x, y, as_stream(stream));
+}
+
 dg_status dg_mat_mult_f32(dg_mat* A, const float* x, float* y, void* stream) {
   DG_CHECK(A && x && y, DG_EINVAL, "mat_mult_f32: bad arguments");
   DG_CHECK(A->kind == 0, DG_ENOTIMPL, "mat_mult_f32: scalar operator only");

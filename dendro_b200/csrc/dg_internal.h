@@ -204,6 +204,7 @@ struct Type1Set {
 // operator's own coefficients / no type-1 elements.
 dg_status lapmass_apply_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
 dg_status lapmass_apply_add_f64(const dg_mat* A, const double* x, double* y, cudaStream_t s);
+dg_status lapmass_apply_add_f32(const dg_mat* A, const float* x, float* y, cudaStream_t s);
 // y = A x for host x and y (staged in A->host_x / host_y) with the copies
 // pipelined against the operator; DG_ENOTIMPL when the mesh does not qualify
 dg_status lapmass_apply_host_pipelined_f64(dg_mat* A, const double* hx, double* hy);

@@ -69,6 +69,7 @@ struct dg_parcsr {
   int device = -1;
   DBuf<uint32_t> d_ptr, d_col, d_send_idx;
   DBuf<double> d_val;
+  DBuf<float> d_val32;  // FP32 copy of the entries, for the FP32 products
 };
 
 namespace {
@@ -101,9 +102,9 @@ void partition_weighted(int64_t n, const uint32_t* w, int P, int64_t* first) {
   for (int r = 0; r < P; ++r) first[r + 1] = first[r] + cnt[r];
 }
 
+template <class T>
 __global__ void __launch_bounds__(kHaloThreads)
-halo_gather(const uint32_t* __restrict__ idx, int64_t n, int dof, const double* __restrict__ x,
-            double* __restrict__ out) {
+halo_gather(const uint32_t* __restrict__ idx, int64_t n, int dof, const T* __restrict__ x, T* __restrict__ out) {
   const int64_t total = n * dof;
   for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
     const int64_t k = t / dof;
@@ -128,13 +129,14 @@ halo_accumulate(const uint32_t* __restrict__ node, const uint32_t* __restrict__ 
 }
 
 // y[i] (+)= sum_k val[k] x[col[k]] over the rank's rows; a column below
-// nown reads the owned values, the rest the ghost values
+// nown reads the owned values, the rest the ghost values (FP64 or FP32)
+template <class T>
 __global__ void __launch_bounds__(kHaloThreads)
-parcsr_spmv(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col, const double* __restrict__ val,
-            int64_t nrow, int64_t nown, const double* __restrict__ x_own, const double* __restrict__ x_ghost,
-            double* __restrict__ y, int add) {
+parcsr_spmv(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col, const T* __restrict__ val,
+            int64_t nrow, int64_t nown, const T* __restrict__ x_own, const T* __restrict__ x_ghost,
+            T* __restrict__ y, int add) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nrow; i += int64_t(gridDim.x) * blockDim.x) {
-    double s = add ? y[i] : 0.0;
+    T s = add ? y[i] : T(0);
     for (uint32_t k = ptr[i]; k < ptr[i + 1]; ++k) {
       const int64_t c = col[k];
       s += val[k] * (c < nown ? x_own[c] : x_ghost[c - nown]);
@@ -144,9 +146,10 @@ parcsr_spmv(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col, 
 }
 
 // x[i] += omega dinv[i] (b[i] - ax[i]): one damped Jacobi sweep's update
+template <class T>
 __global__ void __launch_bounds__(kHaloThreads)
-jacobi_update(double* __restrict__ x, const double* __restrict__ b, const double* __restrict__ ax,
-              const double* __restrict__ dinv, double omega, int64_t n) {
+jacobi_update(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ ax, const T* __restrict__ dinv,
+              T omega, int64_t n) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
     x[i] += omega * dinv[i] * (b[i] - ax[i]);
 }
@@ -383,6 +386,17 @@ dg_status dg_halo_pack(dg_halo* h, const double* x_local, double* send, int dof,
   return DG_OK;
 }
 
+dg_status dg_halo_pack_f32(dg_halo* h, const float* x_local, float* send, int dof, void* stream) {
+  DG_CHECK(h && dof >= 1 && (h->send_idx.empty() || (x_local && send)), DG_EINVAL, "halo_pack_f32: bad arguments");
+  DG_TRY(ensure_device(h));
+  const int64_t n = int64_t(h->send_idx.size());
+  if (n == 0) return DG_OK;
+  auto s = static_cast<cudaStream_t>(stream);
+  halo_gather<<<dg::grid_for(n * dof, kHaloThreads), kHaloThreads, 0, s>>>(h->d_send_idx.p, n, dof, x_local, send);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
 dg_status dg_halo_accumulate(dg_halo* h, const double* recv, double* y_local, int dof, void* stream) {
   DG_CHECK(h && dof >= 1 && (h->acc_node.empty() || (recv && y_local)), DG_EINVAL, "halo_accumulate: bad arguments");
   DG_TRY(ensure_device(h));
@@ -489,6 +503,7 @@ static dg_status parcsr_device(dg_parcsr* pc) {
   DG_TRY(upload_vec(pc->d_ptr, pc->ptr));
   DG_TRY(upload_vec(pc->d_col, pc->col));
   DG_TRY(upload_vec(pc->d_val, pc->val));
+  DG_TRY(upload_vec(pc->d_val32, std::vector<float>(pc->val.begin(), pc->val.end())));
   DG_TRY(upload_vec(pc->d_send_idx, pc->send_idx));
   pc->device = dev;
   return DG_OK;
@@ -518,11 +533,45 @@ dg_status dg_parcsr_apply(dg_parcsr* pc, const double* x_own, const double* x_gh
   return DG_OK;
 }
 
+dg_status dg_parcsr_pack_f32(dg_parcsr* pc, const float* x_own, float* send, void* stream) {
+  DG_CHECK(pc && (pc->send_idx.empty() || (x_own && send)), DG_EINVAL, "parcsr_pack_f32: bad arguments");
+  DG_TRY(parcsr_device(pc));
+  const int64_t n = int64_t(pc->send_idx.size());
+  if (n == 0) return DG_OK;
+  auto s = static_cast<cudaStream_t>(stream);
+  halo_gather<<<dg::grid_for(n, kHaloThreads), kHaloThreads, 0, s>>>(pc->d_send_idx.p, n, 1, x_own, send);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status dg_parcsr_apply_f32(dg_parcsr* pc, const float* x_own, const float* x_ghost, float* y, int add,
+                              void* stream) {
+  DG_CHECK(pc && (pc->nrow == 0 || y) && (pc->ncol_own == 0 || x_own) && (pc->ghosts.empty() || x_ghost), DG_EINVAL,
+           "parcsr_apply_f32: bad arguments");
+  DG_TRY(parcsr_device(pc));
+  if (pc->nrow == 0) return DG_OK;
+  auto s = static_cast<cudaStream_t>(stream);
+  parcsr_spmv<<<dg::grid_for(pc->nrow, kHaloThreads), kHaloThreads, 0, s>>>(
+      pc->d_ptr.p, pc->d_col.p, pc->d_val32.p, pc->nrow, pc->ncol_own, x_own, x_ghost, y, add);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
 void dg_parcsr_destroy(dg_parcsr* pc) { delete pc; }
 
 dg_status dg_vec_jacobi_update(double* x, const double* b, const double* ax, const double* dinv, double omega,
                                int64_t n, void* stream) {
   DG_CHECK(n >= 0 && (n == 0 || (x && b && ax && dinv)), DG_EINVAL, "vec_jacobi_update: bad arguments");
+  if (n == 0) return DG_OK;
+  jacobi_update<<<dg::grid_for(n, kHaloThreads), kHaloThreads, 0, static_cast<cudaStream_t>(stream)>>>(x, b, ax, dinv,
+                                                                                                     omega, n);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+dg_status dg_vec_jacobi_update_f32(float* x, const float* b, const float* ax, const float* dinv, float omega,
+                                   int64_t n, void* stream) {
+  DG_CHECK(n >= 0 && (n == 0 || (x && b && ax && dinv)), DG_EINVAL, "vec_jacobi_update_f32: bad arguments");
   if (n == 0) return DG_OK;
   jacobi_update<<<dg::grid_for(n, kHaloThreads), kHaloThreads, 0, static_cast<cudaStream_t>(stream)>>>(x, b, ax, dinv,
                                                                                                      omega, n);

@@ -2529,6 +2529,13 @@ dg_status lapmass_apply_add_f64(const dg_mat* A, const double* x, double* y, cud
   return launch_variant<double, double>(0, da, ca, cb, x, y, s);
 }
 
+dg_status lapmass_apply_add_f32(const dg_mat* A, const float* x, float* y, cudaStream_t s) {
+  dg_da* da = A->da;
+  const float* ca = A->has_coef ? A->coef32.p : nullptr;
+  const float* cb = A->has_coef ? A->coef32.p + da->E : nullptr;
+  return launch_variant<float, float>(0, da, ca, cb, x, y, s);
+}
+
 // ---------------------------------------------------------------------------
 // Host entry point with the copies pipelined against the operator.  The warp
 // tiles are split into kPipeGroups consecutive groups.  x travels to the GPU

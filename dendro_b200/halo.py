@@ -177,12 +177,14 @@ class HaloDA:
         return self.da_ind, self.da_dep
 
     # ------------------------------------------------------------ vectors ---
-    def local_vector(self, owned=None, dof: int = 1):
-        """A device vector in local layout (zeros, owned part from `owned`)."""
+    def local_vector(self, owned=None, dof: int = 1, dtype=None):
+        """A device vector in local layout (zeros, owned part from `owned`);
+        FP64 unless dtype says otherwise (torch.float32 for the FP32 cycle)."""
         import torch
-        x = torch.zeros(self.n_local * dof, dtype=torch.float64, device="cuda")
+        dt = torch.float64 if dtype is None else dtype
+        x = torch.zeros(self.n_local * dof, dtype=dt, device="cuda")
         if owned is not None:
-            x[: self.n_owned * dof].copy_(torch.as_tensor(owned, dtype=torch.float64).reshape(-1))
+            x[: self.n_owned * dof].copy_(torch.as_tensor(owned, dtype=dt).reshape(-1))
         return x
 
     # ----------------------------------------------------------- kernels ---
@@ -190,8 +192,11 @@ class HaloDA:
         """ReadFromGhostsBegin's send buffer: the owned values each peer reads."""
         import torch
         if send is None:
-            send = torch.empty(len(self.send_idx) * dof, dtype=torch.float64, device=x_local.device)
-        check(lib().dg_halo_pack(self.h, ptr(x_local), ptr(send), dof, _stream(stream)), "halo_pack")
+            send = torch.empty(len(self.send_idx) * dof, dtype=x_local.dtype, device=x_local.device)
+        if x_local.dtype == torch.float32:
+            check(lib().dg_halo_pack_f32(self.h, ptr(x_local), ptr(send), dof, _stream(stream)), "halo_pack_f32")
+        else:
+            check(lib().dg_halo_pack(self.h, ptr(x_local), ptr(send), dof, _stream(stream)), "halo_pack")
         return send
 
     def accumulate(self, recv, y_local, dof: int = 1, stream=None):
@@ -325,19 +330,23 @@ class ParCSR:
             self.h = None
 
     def mult(self, x_own, y=None, add: bool = False):
-        """y = M x (or y += M x) on the owned rows from the owned input values."""
+        """y = M x (or y += M x) on the owned rows from the owned input values
+        (FP64, or FP32 with the FP32 copy of the entries)."""
         import torch
-        dev = x_own.device
-        send = torch.empty(self.n_send, dtype=torch.float64, device=dev)
-        check(lib().dg_parcsr_pack(self.h, ptr(x_own), ptr(send), _stream()), "parcsr_pack")
-        ghost = torch.empty(self.n_ghost, dtype=torch.float64, device=dev)
+        dev, dt = x_own.device, x_own.dtype
+        f32 = dt == torch.float32
+        send = torch.empty(self.n_send, dtype=dt, device=dev)
+        check((lib().dg_parcsr_pack_f32 if f32 else lib().dg_parcsr_pack)(self.h, ptr(x_own), ptr(send), _stream()),
+              "parcsr_pack")
+        ghost = torch.empty(self.n_ghost, dtype=dt, device=dev)
         if self.comm is not None:
             self.comm.all_to_all_single(ghost, send, _splits(self.recv_counts), _splits(self.send_counts))
         elif self.n_ghost or self.n_send:
             raise RuntimeError("these rows read other ranks' values: a communicator is needed")
         if y is None:
-            y = torch.empty(self.n_rows, dtype=torch.float64, device=dev)
-        check(lib().dg_parcsr_apply(self.h, ptr(x_own), ptr(ghost), ptr(y), int(add), _stream()), "parcsr_apply")
+            y = torch.empty(self.n_rows, dtype=dt, device=dev)
+        apply = lib().dg_parcsr_apply_f32 if f32 else lib().dg_parcsr_apply
+        check(apply(self.h, ptr(x_own), ptr(ghost), ptr(y), int(add), _stream()), "parcsr_apply")
         return y
 
 
@@ -352,11 +361,17 @@ class HaloDAMG:
     owned values; CG as DAMGSolve's (src/omg/omg.C:1121-1169).
 
     The hierarchy is built whole on every rank (set-up); each rank then keeps
-    and applies only its parts.  coarse_op 0 (averaged coefficients) only."""
+    and applies only its parts.  coarse_op 0 (averaged coefficients) only.
+
+    inner_prec 1 runs the V-cycle in FP32 (operators on the FP32 coefficient
+    copies, smoother, transfers and exchanges in FP32, the gathered coarsest
+    level solved in FP64) inside an FP64 flexible CG, as the single-GPU
+    mixed-precision solver does."""
 
     def __init__(self, octree, coef=None, comm=None, nlevels: int = 30, nu_pre: int = 2, nu_post: int = 2,
-                 omega: float = 2.0 / 3.0):
+                 omega: float = 2.0 / 3.0, inner_prec: int = 0):
         import torch
+        self.inner_prec = int(inner_prec)
         self.comm = TorchComm() if comm is None else comm
         rank, P = self.comm.rank, self.comm.size
         self.m = DAMG(octree, nlevels=nlevels, nu_pre=nu_pre, nu_post=nu_post, omega=omega)
@@ -371,7 +386,8 @@ class HaloDAMG:
             check(lib().dg_damg_level_coef(self.m.h, l, ptr(c)), "damg_level_coef")
             A = HaloJacobian2(hda, c) if l + 1 < self.nlevels else None
             dinv = None if A is None else 1.0 / A.getDiagonal()
-            self.levels.append(dict(hda=hda, A=A, dinv=dinv, N=da.N))
+            dinv32 = None if dinv is None else dinv.float()
+            self.levels.append(dict(hda=hda, A=A, dinv=dinv, dinv32=dinv32, N=da.N))
         self.P, self.R = [], []
         for l in range(self.nlevels - 1):
             nf, ncs = int(self.m.N[l]), int(self.m.N[l + 1])
@@ -402,23 +418,34 @@ class HaloDAMG:
         return self.levels[0]["hda"].first_owned
 
     def _smooth(self, L, x_loc, b):
+        import torch
         n = L["hda"].n_owned
         ax = L["A"].mult(x_loc)
-        check(lib().dg_vec_jacobi_update(ptr(x_loc), ptr(b), ptr(ax), ptr(L["dinv"]), self.omega, n, _stream()),
-              "vec_jacobi_update")
+        if x_loc.dtype == torch.float32:
+            check(lib().dg_vec_jacobi_update_f32(ptr(x_loc), ptr(b), ptr(ax), ptr(L["dinv32"]), self.omega, n,
+                                                 _stream()), "vec_jacobi_update_f32")
+        else:
+            check(lib().dg_vec_jacobi_update(ptr(x_loc), ptr(b), ptr(ax), ptr(L["dinv"]), self.omega, n,
+                                             _stream()), "vec_jacobi_update")
 
     def vcycle(self, b, l: int = 0):
-        """z = V(b) on level l from the owned values b [n_owned]."""
+        """z = V(b) on level l from the owned values b [n_owned], in b's
+        precision (FP32 b: the FP32 cycle, its coarsest level solved in FP64)."""
+        import torch
         L = self.levels[l]
         hda = L["hda"]
+        f32 = b.dtype == torch.float32
         if l + 1 == self.nlevels:
             full = self.comm.all_gather_v(b, self.coarse_counts).contiguous()
+            if f32:
+                full = full.double()
             check(lib().dg_damg_coarse_solve(self.m.h, ptr(full), ptr(self._xc), _stream()), "damg_coarse_solve")
-            return self._xc[hda.first_owned:hda.first_owned + hda.n_owned].clone()
+            z = self._xc[hda.first_owned:hda.first_owned + hda.n_owned].clone()
+            return z.float() if f32 else z
         n = hda.n_owned
-        x_loc = hda.local_vector()
+        x_loc = hda.local_vector(dtype=b.dtype)
         if self.nu_pre > 0:
-            x_loc[:n].copy_(self.omega * L["dinv"] * b)
+            x_loc[:n].copy_(self.omega * (L["dinv32"] if f32 else L["dinv"]) * b)
             for _ in range(self.nu_pre - 1):
                 self._smooth(L, x_loc, b)
             r = b - L["A"].mult(x_loc)[:n]
@@ -444,7 +471,12 @@ class HaloDAMG:
         bnorm = hda.dot(b, b) ** 0.5
         if bnorm == 0:
             return x, 0, True, 0.0
-        z = self.vcycle(r)
+        # the FP32 cycle is not exactly the same linear map from one call to
+        # the next (FP32 rounding), so CG takes the flexible (Polak-Ribiere)
+        # direction update: beta = z_new . (r_new - r_old) / (z_old . r_old)
+        flexible = self.inner_prec == 1
+        pre = (lambda v: self.vcycle(v.float()).double()) if flexible else self.vcycle
+        z = pre(r)
         p_loc = hda.local_vector()
         p_loc[:n].copy_(z)
         rz = hda.dot(r, z)
@@ -454,13 +486,15 @@ class HaloDAMG:
             q = A.mult(p_loc)[:n]
             alpha = rz / hda.dot(p_loc, q)
             x.add_(p_loc[:n], alpha=alpha)
+            r_old = r.clone() if flexible else None
             r.add_(q, alpha=-alpha)
             rel = hda.dot(r, r) ** 0.5 / bnorm
             if rel <= rtol:
                 return x, it, True, rel
-            z = self.vcycle(r)
+            z = pre(r)
             rz_new = hda.dot(r, z)
-            p_loc[:n].mul_(rz_new / rz).add_(z)
+            beta = (rz_new - hda.dot(r_old, z)) / rz if flexible else rz_new / rz
+            p_loc[:n].mul_(beta).add_(z)
             rz = rz_new
         return x, it, False, rel
 

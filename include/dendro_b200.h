@@ -210,6 +210,9 @@ dg_status dg_mat_mult(dg_mat* A, const double* x, double* y, void* stream);
 dg_status dg_mat_mult_add(dg_mat* A, const double* x, double* y, void* stream);
 /* FP32 inner-solver form of the same operator. */
 dg_status dg_mat_mult_f32(dg_mat* A, const float* x, float* y, void* stream);
+/* y += A x in FP32 (the FP32 coefficient copy): the dependent elements of a
+ * partitioned mesh in the FP32 inner V-cycle. */
+dg_status dg_mat_mult_add_f32(dg_mat* A, const float* x, float* y, void* stream);
 /* MATOP_GET_DIAGONAL (Jacobian2MatGetDiagonal, omgNeumann.C:442-465). */
 dg_status dg_mat_get_diagonal(dg_mat* A, double* d, void* stream);
 /* Same as dg_mat_mult with host x and y: copies in, applies, copies out and
@@ -409,6 +412,8 @@ dg_status dg_halo_local_da(const dg_halo* h, int which, dg_da** out);
  * asynchronous on `stream`.  The received values, concatenated by source
  * rank, are x_local's ghost slots (x_local + dof * n_owned). */
 dg_status dg_halo_pack(dg_halo* h, const double* x_local, double* send, int dof, void* stream);
+/* The same for FP32 vectors (the FP32 inner V-cycle's exchanges). */
+dg_status dg_halo_pack_f32(dg_halo* h, const float* x_local, float* send, int dof, void* stream);
 /* WriteToGhostsEnd (include/oda/oda.txx:609-640): y_local[send_idx[k]] +=
  * recv[k] for k in order, recv being the peers' ghost slots concatenated by
  * source rank (what they send in WriteToGhostsBegin, oda.txx:566-605). */
@@ -438,6 +443,11 @@ dg_status dg_parcsr_pack(dg_parcsr* pc, const double* x_own, double* send, void*
  * owned input values and the received ghost values (device pointers). */
 dg_status dg_parcsr_apply(dg_parcsr* pc, const double* x_own, const double* x_ghost, double* y, int add,
                           void* stream);
+/* The same two in FP32 (vectors and an FP32 copy of M's entries; the
+ * transfers' weights are dyadic, so the copy is exact). */
+dg_status dg_parcsr_pack_f32(dg_parcsr* pc, const float* x_own, float* send, void* stream);
+dg_status dg_parcsr_apply_f32(dg_parcsr* pc, const float* x_own, const float* x_ghost, float* y, int add,
+                              void* stream);
 void dg_parcsr_destroy(dg_parcsr* pc);
 
 /* ------------------------------------------------------- learned smoother --- */
@@ -501,6 +511,9 @@ dg_status dg_vec_dot_noalloc(const double* x, const double* y, int64_t n, double
  * device pointers, asynchronous on `stream`. */
 dg_status dg_vec_jacobi_update(double* x, const double* b, const double* ax, const double* dinv, double omega,
                                int64_t n, void* stream);
+/* The same update in FP32. */
+dg_status dg_vec_jacobi_update_f32(float* x, const float* b, const float* ax, const float* dinv, float omega,
+                                   int64_t n, void* stream);
 
 #ifdef __cplusplus
 }

@@ -226,6 +226,50 @@ def test_damg_over_thread_ranks(gpu, oracle, name, P):
     assert np.linalg.norm(fine.matvec(x, coef) - b) <= 1.01e-8 * np.linalg.norm(b)
 
 
+@pytest.mark.parametrize("name,P", [("gauss20k_d10", 2), ("lognormal20k_d12", 3)])
+def test_damg_fp32_over_thread_ranks(gpu, oracle, name, P):
+    """The partitioned FP32 inner V-cycle against the single-GPU FP32 and FP64
+    V-cycles (FP32 tolerance, 2e-5), and its FP64 flexible PCG against the
+    single-GPU mixed-precision solve (iterations +-1, FP64 residual)."""
+    import torch
+    from dendro_b200.halo import HaloDAMG
+    from dendro_b200.learned import vcycle
+    from tests.threadcomm import ThreadComm, run_ranks
+    pts, d, m = points(name)
+    bal = oracle.balance(oracle.points2octree(pts, d, m), d)
+    octree = gpu.Octree.from_octants(bal, d)
+    coef = I.sphere_coefficients(gpu.DA(octree).elementCenters())
+    single64 = gpu.DAMG(octree)
+    single64.setKSP(coef)
+    single32 = gpu.DAMG(octree, inner_prec=1)
+    single32.setKSP(coef)
+    b = I.uniform_rhs(int(single64.N[0]), 43)
+    bd = torch.tensor(b, device="cuda")
+    z64 = vcycle(single64, bd).cpu().numpy()
+    z32 = vcycle(single32, bd).cpu().numpy()
+    _, rep = single32.solve(b)
+    tc = ThreadComm(P)
+    M = [HaloDAMG(octree, coef, comm=tc.rank_comm(r), inner_prec=1) for r in range(P)]
+
+    def body(r):
+        own = slice(M[r].first_owned, M[r].first_owned + M[r].n_owned)
+        bo = torch.tensor(b[own], device="cuda")
+        z = M[r].vcycle(bo.float())
+        assert z.dtype == torch.float32
+        x, it, conv, rr = M[r].solve(bo, rtol=1e-8)
+        return z.double().cpu().numpy(), x.cpu().numpy(), it, conv
+
+    res = run_ranks(P, body)
+    z = np.concatenate([t[0] for t in res])
+    assert rel(z, z32) < 2e-5 and rel(z, z64) < 2e-5
+    its = {t[2] for t in res}
+    assert len(its) == 1 and all(t[3] for t in res)
+    assert abs(its.pop() - rep["iterations"]) <= 1
+    x = np.concatenate([t[1] for t in res])
+    fine = oracle.Mesh(bal, d)
+    assert np.linalg.norm(fine.matvec(x, coef) - b) <= 1.01e-8 * np.linalg.norm(b)
+
+
 @pytest.mark.parametrize("name,P", [("root", 2), ("corner_points_d5", 4)])
 def test_more_ranks_than_work(gpu, oracle, name, P):
     """Ranks that own no nodes (the one-element mesh over 2 ranks; a
